@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark of the distance-driven fan-beam projector pair on B200.
+
+Workload (the batched 2D fan-beam workload): 64 independent 512x512 slices at
+0.7 mm, 888-channel arc detector (1.2858 mm pitch at 1085.6 mm), source at
+595 mm, each slice with a seeded uneven view count in [576, 1152] over 360
+degrees; random-ellipse phantoms.  One step = DD forward projection of every
+view of every slice followed by the matched (exact-transpose) backprojection
+of that sinogram -- the projector work of one OS-SQS pass.
+
+Metric: Gray/s = 1e9 footprint updates per second, where an update is one
+ray-line integration of the forward projector (nominal count
+views x channels x lines, the reference's loop count) or one pixel-view
+integration of the backprojector (views x pixels).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 is launched with torch.distributed.run (one process per GPU); every
+rank processes its own batch (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DD proj+BP Gray/s & % HBM roofline; OS-SQS time-to-RMSE learned vs TV, 1 B200"
+UNIT = "Gray/s"
+BYTES_PER_UPDATE = 8          # two FP32 prefix samples per footprint
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--slices", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def workload(rank, nslices):
+    from reconnet_b200 import phantom as P
+    geom = P.geom_cfg1()
+    counts = P.cfg1_view_counts(nslices, seed=1 + rank)
+    angles = np.concatenate([P.uniform_angles(int(n)) for n in counts])
+    rng = np.random.default_rng(100 + rank)
+    imgs = np.stack([P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng) for _ in range(nslices)])
+    return geom, counts, angles, imgs
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` on this workload from the committed
+    ncu summary (profiles/ncu_dram_bytes.txt: `<kernel> <bytes_per_launch>`)."""
+    p = os.path.join(ROOT, "profiles", "ncu_dram_bytes.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(geom, counts, angles, target_s=12.0):
+    """FP32 OpenMP port of the oracle on one slice of the workload, with the
+    view subset sized for about `target_s` seconds; returns (Gray/s, threads, desc)."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    n0 = int(counts[0])
+    ang0 = angles[:n0]
+    img = workload_first_image(geom)
+
+    def run(nv):
+        sel = ang0[:: max(1, n0 // nv)][:nv].copy()
+        t0 = time.perf_counter()
+        p = O.fan_fp(img, sel, geom, geom.nu, 1, dtype=np.float32)
+        O.fan_bp(p, sel, geom, (geom.nx, geom.ny, 1), 2, dtype=np.float32)
+        dt = time.perf_counter() - t0
+        upd = sel.size * (geom.nu * geom.ny + geom.nx * geom.ny)
+        return upd, dt, sel.size
+
+    upd, dt, nv = run(4)
+    per_view = dt / max(nv, 1)
+    nv = int(max(4, min(n0, target_s / max(per_view, 1e-6))))
+    upd, dt, nv = run(nv)
+    desc = (f"1 slice 512x512, 888 ch, {nv} of its {n0} views: FP + matched BP, FP32 OpenMP port of the "
+            f"oracle, {threads} threads, {dt:.1f} s")
+    return upd / dt / 1e9, threads, desc
+
+
+def workload_first_image(geom):
+    from reconnet_b200 import phantom as P
+    rng = np.random.default_rng(100)
+    return P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
+
+
+def run_reference(args):
+    """Reference arm: the CPU port of the reference DD loop on the host cores
+    (rank 0 only), plus the reference's own CUDA library (built from its
+    sources into oracle/_ref) on the same GPU for context."""
+    rank, local, world = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    geom, counts, angles, imgs = workload(0, args.slices)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    n0 = int(counts[0])
+    # per step: one slice, a view subset sized for ~4 s (pilot-calibrated)
+    img = imgs[0][None, :, :, None, None]
+
+    def step(nv):
+        sel = angles[:n0][:: max(1, n0 // nv)][:nv].copy()
+        p = O.fan_fp(img, sel, geom, geom.nu, 1, dtype=np.float32)
+        O.fan_bp(p, sel, geom, (geom.nx, geom.ny, 1), 2, dtype=np.float32)
+        return sel.size * (geom.nu * geom.ny + geom.nx * geom.ny)
+
+    t0 = time.perf_counter()
+    step(4)
+    per_view = (time.perf_counter() - t0) / 4
+    nv = int(max(4, min(n0, 4.0 / max(per_view, 1e-6))))
+    for _ in range(args.warmup):
+        step(nv)
+    upd, t0 = 0, time.perf_counter()
+    for _ in range(args.steps):
+        upd += step(nv)
+    dt = time.perf_counter() - t0
+    value = upd / dt / 1e9
+    sample = (f"per step: 1 slice 512x512, 888 ch, {nv} of its {n0} views, FP + matched BP; FP32 OpenMP port of "
+              f"the reference DD loop (the reference has no CPU path), {threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded random-ellipse phantoms",
+            "config": {"workload": "batched 2D fan-beam DD FP + matched BP (bounded CPU sample per step)",
+                       "slices": args.slices, "nx": geom.nx, "ny": geom.ny, "nu": geom.nu},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["reference_gpu"] = reference_gpu(geom, counts, angles, imgs, min(3, args.steps))
+    print(json.dumps(line), flush=True)
+
+
+def reference_gpu(geom, counts, angles, imgs, steps):
+    """The reference CUDA library on the full workload, called as its Python
+    wrapper does (python/ReconNet_no_tf.py:133-200): per slice, FP then BP
+    through cDistanceDrivenFan{Projection,Backprojection} with host arrays."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libreconnet_ref.so")
+    if not os.path.exists(path):
+        return {"unavailable": "reference library not built (make -C oracle ref)"}
+    import ctypes
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    lib = make_golden.load_ref(path)
+    p = make_golden.p
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    sinos = [np.zeros((1, geom.nu, int(n), 1, 1), np.float32) for n in counts]
+    bps = [np.zeros((1, geom.nx, geom.ny, 1, 1), np.float32) for _ in counts]
+    imgs5 = [np.ascontiguousarray(im[None, :, :, None, None]) for im in imgs]
+    angs = [np.ascontiguousarray(angles[offs[s]:offs[s + 1]]) for s in range(len(counts))]
+
+    def one_step():
+        for s, n in enumerate(counts):
+            a = (1, 1, geom.nx, geom.ny, 1, geom.dx, geom.dy, geom.dz, geom.nu, int(n), 1, geom.da, geom.dv,
+                 0.0, 0.0, geom.dsd, geom.dso, 0)
+            lib.cDistanceDrivenFanProjection(p(sinos[s]), p(imgs5[s]), p(angs[s]), *a)
+            lib.cDistanceDrivenFanBackprojection(p(bps[s]), p(sinos[s]), p(angs[s]), *a)
+
+    one_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_step()
+    dt = (time.perf_counter() - t0) / steps
+    upd = int(np.sum(counts)) * (geom.nu * geom.ny + geom.nx * geom.ny)
+    return {"value": upd / dt / 1e9, "unit": UNIT, "ms_per_step": dt * 1e3, "steps": steps,
+            "note": "reference CUDA kernels (ReconNet4D_no_tf sources built for sm_100a into oracle/_ref), "
+                    "per-slice host calls FP + iterative BP incl. its per-call allocation and copies, same B200"}
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from reconnet_b200.torch_ops import FanPlan
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    geom, counts, angles, imgs = workload(rank, args.slices)
+    plan = FanPlan(geom, angles, nbatches=args.slices, nview_per_slice=counts, device=dev)
+    x = torch.from_numpy(imgs).to(dev)
+    p = torch.empty(plan.sino_shape, device=dev)
+    b = torch.empty(plan.img_shape, device=dev)
+    fp_upd, bp_upd = plan.fp_updates(), plan.bp_updates()
+    updates = fp_upd + bp_upd
+
+    def step():
+        plan.project(x, out=p)
+        plan.backproject(p, 2, out=b)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    plan.check()
+    torch.cuda.synchronize()
+
+    # ---- device-timed region ----
+    barrier()
+    torch.cuda.synchronize()
+    l0 = plan.launches()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+    barrier()
+    launches = plan.launches() - l0
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = updates * world / (ms_step * 1e-3) / 1e9
+    plan.check()
+
+    # ---- per-kernel timing (CUDA events around each launch) for the roofline ----
+    plan.set_timing(True)
+    prof_steps = 3
+    for _ in range(prof_steps):
+        step()
+    kt, _ = plan.read_timing()
+    plan.set_timing(False)
+    fp_ms = kt["fp"][0] / max(kt["fp"][1], 1)
+    bp_ms = kt["bp"][0] / max(kt["bp"][1], 1)
+    dominant = "fan_fp_kernel" if kt["fp"][0] >= kt["bp"][0] else "fan_bp_kernel"
+    io_bytes = 4 * (x.numel() + p.numel())
+    if dominant == "fan_fp_kernel":
+        alg_bytes, dur_ms = BYTES_PER_UPDATE * fp_upd + io_bytes, fp_ms
+    else:
+        alg_bytes, dur_ms = BYTES_PER_UPDATE * bp_upd + io_bytes, bp_ms
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (dur_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": ncu_traffic(dominant), "kernel": dominant, "peak_kind": peak_kind,
+                "alg_bytes_per_launch": alg_bytes, "launch_ms": dur_ms,
+                "kernels_ms": {k: (v[0] / max(v[1], 1)) for k, v in kt.items() if v[1]},
+                "model": f"{BYTES_PER_UPDATE} B per footprint update + 4 B per image/sinogram element"}
+
+    # ---- end to end through the public API with host buffers ----
+    xh = torch.from_numpy(imgs).pin_memory()
+    bh = torch.empty(plan.img_shape, dtype=torch.float32).pin_memory()
+    xs = torch.empty_like(x)
+
+    def e2e_step():
+        xs.copy_(xh, non_blocking=True)
+        plan.project(xs, out=p)
+        plan.backproject(p, 2, out=b)
+        bh.copy_(b, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(st)
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": updates * world / (ms_e2e / e2e_steps * 1e-3) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": int(xh.numel() * 4), "d2h_bytes_per_step": int(bh.numel() * 4),
+           "ms_per_step": ms_e2e / e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, desc = cpu_baseline_sample(geom, counts, angles)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded random-ellipse phantoms (10 ellipses, 5-120 mm, 0-0.04/mm)",
+                "config": {"workload": "batched 2D fan-beam DD forward projection + matched backprojection: "
+                                       f"{args.slices} slices 512x512 @0.7 mm, 888 ch @1.2858 mm, "
+                                       "views U[576,1152] per slice over 360 deg",
+                           "slices_per_gpu": args.slices, "total_views_per_gpu": int(plan.total_views),
+                           "fp_updates_per_step": fp_upd, "bp_updates_per_step": bp_upd,
+                           "l2": "inputs larger than L2 (64 MB image batch, "
+                                 f"{p.numel() * 4 / 1e6:.0f} MB sinogram, ~1.2 GB scratch per step)",
+                           "parallelism": f"dp{world} (independent slice batches)"},
+                "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clk.summary()}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    del plan
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * reconnet_b200 -- B200-native (sm_100a) distance-driven CT projector library.
+ *
+ * C ABI only: plain pointers, sizes and scalars; no C++ or torch types.
+ *
+ * Two layers:
+ *   1. Drop-in entry points with the reference's names and signatures
+ *      (host pointers, synchronous).  Each replaces the reference function
+ *      cited beside it (paths are relative to the wudufan/ReconNet tree).
+ *   2. A native device API: device pointers, caller-chosen CUDA stream, no
+ *      implicit device synchronisation, int status codes, and a plan object
+ *      that owns geometry tables and scratch so repeated calls allocate
+ *      nothing.
+ *
+ * Conventions (same as the reference):
+ *   image    [nBatches][nx][ny][nz][nChannels]   float32, C order
+ *   sinogram [nBatches][nu][nview][nv][nChannels] float32, C order
+ *   angles in radians; da (angular detector pitch) = du_mm / dsd.
+ *
+ * typeProjector for the fan backprojector:
+ *   0  iterative backprojection of the reference (length pre-weight),
+ *   1  FBP backprojection of the reference (distance weight),
+ *   2  matched backprojection: the exact transpose of the forward projector
+ *      (not in the reference; used by OS-SQS and the autograd backward).
+ *
+ * Errors: native functions return RN_OK (0) or an RN_ERR_* code and set a
+ * thread-local message readable with rn_last_error().  The reference-named
+ * functions keep their void/float returns and also set rn_last_error();
+ * rn_last_status() returns the code of the most recent call on the thread.
+ */
+#ifndef RECONNET_B200_H
+#define RECONNET_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RN_OK 0
+#define RN_ERR_ARG 1         /* invalid argument or unsupported geometry */
+#define RN_ERR_CUDA 2        /* CUDA runtime error */
+#define RN_ERR_ALLOC 3       /* device allocation failed */
+#define RN_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define RN_ERR_NOT_READY 5   /* library not initialised for this device */
+
+#define RN_TYPE_ITERATIVE 0
+#define RN_TYPE_FBP 1
+#define RN_TYPE_MATCHED 2
+
+const char* rn_last_error(void);
+int rn_last_status(void);
+int rn_version(void);
+
+/* ------------------------------------------------------------------------
+ * Reference-named drop-in entry points (host pointers, synchronous).
+ * ------------------------------------------------------------------------ */
+
+/* replaces ReconNet4D/Projector.cu:12 */
+int SetDevice(int device);
+
+/* replaces ReconNet4D/DistanceDriven.cu:386-439 (prj is overwritten) */
+void cDistanceDrivenFanProjection(float* prj, const float* img, const float* deg, int nBatches, int nChannels,
+                                  int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
+                                  float da, float dv, float off_a, float off_v, float dsd, float dso,
+                                  int typeProjector);
+
+/* replaces ReconNet4D/DistanceDriven.cu:793-846 (img is overwritten, as the
+ * reference zeroes its device copy before accumulating) */
+void cDistanceDrivenFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels,
+                                      int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview,
+                                      int nv, float da, float dv, float off_a, float off_v, float dsd, float dso,
+                                      int typeProjector);
+
+/* replaces ReconNet4D/DistanceDriven3D.cu:346-407 */
+void cDistanceDrivenTomoProjection(float* prj, const float* img, const float* detCenter, const float* src,
+                                   int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz,
+                                   float cx, float cy, float cz, int nu, int nview, int nv, float du, float dv,
+                                   float off_u, float off_v);
+
+/* replaces ReconNet4D/DistanceDriven3D.cu:666-727 */
+void cDistanceDrivenTomoBackprojection(float* img, const float* prj, const float* detCenter, const float* src,
+                                       int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy,
+                                       float dz, float cx, float cy, float cz, int nu, int nview, int nv, float du,
+                                       float dv, float off_u, float off_v);
+
+/* replaces ReconNet4D/Filter.cu:432-474 (equiangular fan ramp filter) */
+void cFilterFanFilter(float* pFPrj, const float* pPrj, int nBatches, int nChannels, int nu, int nview, int nv,
+                      float da, float dv, float off_a, float off_v, float dsd, float dso, int typeFilter,
+                      int typeProjector);
+
+/* replaces ReconNet4D/Filter.cu:476-518 (equispaced parallel ramp filter) */
+void cFilterParallelFilter(float* pFPrj, const float* pPrj, int nBatches, int nChannels, int nu, int nview, int nv,
+                           float da, float dv, float off_a, float off_v, float dsd, float dso, int typeFilter,
+                           int typeProjector);
+
+/* replaces ReconNet4D/ossqs.cu:12-161.  Same arguments; the projector is the
+ * DD fan pair (forward + the backprojector selected by typeProjector), and the
+ * last subset holds views [startView, nview) instead of the reference's
+ * nview - nviewPerSubset. */
+void cOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
+            const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels,
+            int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
+            float off_a, float off_v, float dsd, float dso, int typeProjector, float lambda);
+
+/* replaces ReconNet4D/TotalVariation.cu:70-142; the TV value is summed in FP64 */
+float cTVSQS2D(float* grad, float* norm, const float* img, int nx, int ny);
+
+/* ------------------------------------------------------------------------
+ * Native device API.
+ * ------------------------------------------------------------------------ */
+
+/* Geometry; field names and meaning follow Projector (ReconNet4D/Projector.h:10-37).
+ * du is the angular pitch (da) for the fan projector. */
+typedef struct RnFanGeom {
+    int nBatches, nChannels;
+    int nx, ny, nz;
+    float dx, dy, dz;
+    float cx, cy, cz;
+    int nu, nview, nv;
+    float du, dv, off_u, off_v;
+    float dsd, dso;
+} RnFanGeom;
+
+typedef struct rn_fan_plan rn_fan_plan;
+
+/* Plan for the reference layout: image [B][nx][ny][nz][C], sinogram
+ * [B][nu][nview][nv][C], one angle list (host_deg, nview floats) shared by
+ * all batches.  Builds device geometry tables and scratch on `stream`. */
+int rn_fan_plan_create(rn_fan_plan** plan, const RnFanGeom* g, const float* host_deg, void* stream);
+
+/* Plan for a ragged batch of independent 2D slices (the batched OS-SQS
+ * workload): g->nBatches slices of [nx][ny] stored back to back; slice s has
+ * nview_per_slice[s] views with angles host_deg[view_offset(s) + k], and its
+ * sinogram [nu][nview_s] starts at float offset nu * view_offset(s) of a
+ * packed sinogram buffer, where view_offset(s) = sum of nview over earlier
+ * slices.  nz, nv, nChannels must be 1. */
+int rn_fan_plan_create_ragged(rn_fan_plan** plan, const RnFanGeom* g, const int* nview_per_slice,
+                              const float* host_deg, void* stream);
+
+int rn_fan_plan_destroy(rn_fan_plan* plan);
+
+/* Total number of views in the plan (sum over slices for ragged plans). */
+int64_t rn_fan_plan_total_views(const rn_fan_plan* plan);
+
+/* Forward projection, device pointers, stream-ordered; prj is overwritten. */
+int rn_fan_project(rn_fan_plan* plan, float* d_prj, const float* d_img, void* stream);
+
+/* Backprojection; typeProjector as above.  accumulate = 0 overwrites img,
+ * 1 adds to it (the reference class-level Backprojection accumulates). */
+int rn_fan_backproject(rn_fan_plan* plan, float* d_img, const float* d_prj, int typeProjector, int accumulate,
+                       void* stream);
+
+/* Device-side error word of the plan's kernels (bounded waits that gave up):
+ * synchronises `stream`, returns RN_OK or RN_ERR_TIMEOUT, clears the word. */
+int rn_fan_plan_check(rn_fan_plan* plan, void* stream);
+
+/* Instrumentation.  rn_fan_plan_set_timing(plan, 1) brackets every kernel
+ * launch of the plan with CUDA events on its stream; rn_fan_plan_read_timing
+ * synchronises on them and returns, per kernel kind (0 line prologue,
+ * 1 forward projection, 2 edge tables, 3 backprojection, 4 other), the summed
+ * milliseconds and launch counts since the last read, plus the total number of
+ * kernels the plan has launched. */
+int rn_fan_plan_set_timing(rn_fan_plan* plan, int enable);
+int rn_fan_plan_read_timing(rn_fan_plan* plan, float* ms, int* counts, int nkinds, long long* launches);
+
+/* Ramp filter on device pointers (fan = 1 equiangular / 0 parallel); same
+ * parameters as cFilterFanFilter. */
+int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int nu, int nview, int nv, float da,
+              float off_a, float dsd, float dso, int typeFilter, int fan, void* stream);
+
+/* TV surrogate on a batch of S slices [S][nx][ny]; grad/norm may be NULL;
+ * d_tv (may be NULL) receives S FP64 TV values. */
+int rn_tv_sqs(float* d_grad, float* d_norm, double* d_tv, const float* d_img, int nslices, int nx, int ny,
+              void* stream);
+
+/* One OS-SQS subset update on all slices of a plan (device pointers):
+ *   x_out = clamp(x_in - lambda * (nSubsets * A_s^T W_s (A_s x_in - b_s) + beta * grad_tv(x_in))
+ *                  / (normImg + beta * norm_tv(x_in) + 1e-6), lb, ub)
+ * `subset_plan` is a plan holding only the subset's views (same slice
+ * layout); d_prj_s / d_w_s are the subset's measured and weight sinograms in
+ * that plan's layout.  x_out must not alias x_in. */
+int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x_in, const float* d_prj_s,
+                      const float* d_w_s, const float* d_norm_img, float lambda, float beta, int nSubsets, float lb,
+                      float ub, int typeProjector, void* stream);
+
+/* Tomosynthesis DD on device pointers (same arguments as the reference-named
+ * host functions above plus a caller-provided FP64 scratch d_sat whose size
+ * rn_tomo_sat_bytes reports: fp_bytes for projection, bp_bytes for
+ * backprojection).  detCenter / src are [nview][3] device arrays. */
+int rn_tomo_sat_bytes(int nx, int ny, int nz, int nu, int nview, int nv, size_t* fp_bytes, size_t* bp_bytes);
+int rn_tomo_project(float* d_prj, const float* d_img, const float* d_detCenter, const float* d_src, double* d_sat,
+                    int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, float cx,
+                    float cy, float cz, int nu, int nview, int nv, float du, float dv, float off_u, float off_v,
+                    void* stream);
+int rn_tomo_backproject(float* d_img, const float* d_prj, const float* d_detCenter, const float* d_src, double* d_sat,
+                        int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, float cx,
+                        float cy, float cz, int nu, int nview, int nv, float du, float dv, float off_u, float off_v,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RECONNET_B200_H */

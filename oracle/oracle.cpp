@@ -1,0 +1,745 @@
+// ============================================================================
+// TEST INFRASTRUCTURE -- NOT PART OF THE PRODUCT.
+//
+// CPU oracle for the ReconNet distance-driven (DD) hot path.  Only the test
+// suite, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs
+// may load this library; the shipped library (reconnet_b200) never links or
+// calls it.
+//
+// Every function restates one reference kernel (file:line given beside it).
+// The reference fetches prefix sums through CUDA texture objects with linear
+// filtering; here those fetches are emulated with the same addressing rules
+// (texel-centre convention, border / clamp per dimension) but with exact
+// interpolation weights, so the oracle is the "ideal" version of the
+// reference arithmetic.  All functions are templated on the accumulation type
+// T: T = double is the FP64 oracle used for parity, T = float is the FP32
+// OpenMP port used as the timed CPU baseline.
+//
+// The matched backprojector (typeProjector == 2) is not a reference kernel:
+// it is the mechanical transpose of the FP restatement below (scatter into
+// adjoint prefix arrays, then suffix sums), so <Ax, y> == <x, A^T y> holds to
+// rounding.
+// ============================================================================
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// PI as the reference defines it (ReconNet4D/Projector.h:5).
+const double kRefPi = 3.141592657;
+
+struct Fan {
+    int nb, nc, nx, ny, nz;
+    double dx, dy, dz;
+    int nu, nview, nv;
+    double du, dv, off_u, off_v, dsd, dso;
+};
+
+inline int64_t img_index(const Fan& g, int b, int ix, int iy, int iz, int c) {
+    return ((((int64_t)b * g.nx + ix) * g.ny + iy) * g.nz + iz) * g.nc + c;
+}
+inline int64_t prj_index(const Fan& g, int b, int iu, int iview, int iv, int c) {
+    return ((((int64_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + c;
+}
+
+// View split of DistanceDriven.cu:299-312 (|cos| > |sin| -> rays run along y,
+// the "X" kernels integrate along x on every image row).
+inline bool x_class(float deg) {
+    double d = (double)deg;
+    return std::fabs(std::cos(d)) > std::fabs(std::sin(d));
+}
+
+// Channel angle of detector cell iu, DistanceDriven.cu:83.
+inline double chan_angle(const Fan& g, double iu) {
+    return (-(iu - (g.nu - 1) / 2.0) - g.off_u) * g.du;
+}
+
+// Weight quantisation of the emulated texture unit: 0 = exact weights (the
+// oracle proper), 1 = weights rounded to 1/256, 2 = truncated to 1/256 (the
+// 8-bit fractional weights of CUDA linear filtering, to compare against the
+// reference's own texture-based kernels).
+static int g_tex_quant = 0;
+
+// One texture dimension with linear filtering: coordinate c in texel-centre
+// convention -> (i0, w) such that value = (1-w)*T[i0] + w*T[i0+1].
+inline void tex_split(double c, int& i0, double& w) {
+    double b = c - 0.5;
+    double f = std::floor(b);
+    i0 = (int)f;
+    w = b - f;
+    if (g_tex_quant == 1) w = std::floor(w * 256.0 + 0.5) / 256.0;
+    else if (g_tex_quant == 2) w = std::floor(w * 256.0) / 256.0;
+    if (w >= 1.0) { i0 += 1; w = 0.0; }
+}
+
+// Prefix arrays of one (batch, channel) image, the layouts of
+// AccumulateKernelX/Y (DistanceDriven.cu:23-60):
+//   PX[x][y][z], x in [0, nx]   (sum over i < x along x)
+//   PY[x][y][z], y in [0, ny]   (sum over j < y along y)
+template <typename T>
+void build_prefix(const Fan& g, const float* img, int b, int c, std::vector<T>& PX, std::vector<T>& PY) {
+    PX.assign((size_t)(g.nx + 1) * g.ny * g.nz, T(0));
+    PY.assign((size_t)g.nx * (g.ny + 1) * g.nz, T(0));
+    for (int iy = 0; iy < g.ny; iy++)
+        for (int iz = 0; iz < g.nz; iz++) {
+            T acc = 0;
+            for (int ix = 0; ix < g.nx; ix++) {
+                acc += (T)img[img_index(g, b, ix, iy, iz, c)];
+                PX[((size_t)(ix + 1) * g.ny + iy) * g.nz + iz] = acc;
+            }
+        }
+    for (int ix = 0; ix < g.nx; ix++)
+        for (int iz = 0; iz < g.nz; iz++) {
+            T acc = 0;
+            for (int iy = 0; iy < g.ny; iy++) {
+                acc += (T)img[img_index(g, b, ix, iy, iz, c)];
+                PY[((size_t)ix * (g.ny + 1) + (iy + 1)) * g.nz + iz] = acc;
+            }
+        }
+}
+
+// Emulation of tex3D over a 3D array with extents (W, H, D) =
+// (width, height, depth), element (w, h, d) at data[(d*H + h)*W + w].
+// mode[k] = 0 border (zero outside), 1 clamp.  Exact weights.
+template <typename T>
+struct Tex3 {
+    const T* data;
+    int W, H, D;
+    int mode[3];
+    inline T at(int w, int h, int d) const {
+        if (mode[0] == 0) { if (w < 0 || w >= W) return T(0); } else { w = std::min(std::max(w, 0), W - 1); }
+        if (mode[1] == 0) { if (h < 0 || h >= H) return T(0); } else { h = std::min(std::max(h, 0), H - 1); }
+        if (mode[2] == 0) { if (d < 0 || d >= D) return T(0); } else { d = std::min(std::max(d, 0), D - 1); }
+        return data[((size_t)d * H + h) * W + w];
+    }
+    inline T fetch(double cw, double ch, double cd) const {
+        int w0, h0, d0;
+        double fw, fh, fd;
+        tex_split(cw, w0, fw);
+        tex_split(ch, h0, fh);
+        tex_split(cd, d0, fd);
+        T acc = 0;
+        for (int a = 0; a < 2; a++) {
+            double ww = a ? fw : 1 - fw;
+            if (ww == 0) continue;
+            for (int bb = 0; bb < 2; bb++) {
+                double wh = bb ? fh : 1 - fh;
+                if (wh == 0) continue;
+                for (int cc = 0; cc < 2; cc++) {
+                    double wd = cc ? fd : 1 - fd;
+                    if (wd == 0) continue;
+                    acc += (T)(ww * wh * wd) * at(w0 + a, h0 + bb, d0 + cc);
+                }
+            }
+        }
+        return acc;
+    }
+    // Transpose of fetch: scatter v into the texels fetch() would read.
+    inline void scatter(T* adj, double cw, double ch, double cd, T v) const {
+        int w0, h0, d0;
+        double fw, fh, fd;
+        tex_split(cw, w0, fw);
+        tex_split(ch, h0, fh);
+        tex_split(cd, d0, fd);
+        for (int a = 0; a < 2; a++) {
+            double ww = a ? fw : 1 - fw;
+            if (ww == 0) continue;
+            for (int bb = 0; bb < 2; bb++) {
+                double wh = bb ? fh : 1 - fh;
+                if (wh == 0) continue;
+                for (int cc = 0; cc < 2; cc++) {
+                    double wd = cc ? fd : 1 - fd;
+                    if (wd == 0) continue;
+                    int w = w0 + a, h = h0 + bb, d = d0 + cc;
+                    if (mode[0] == 0) { if (w < 0 || w >= W) continue; } else { w = std::min(std::max(w, 0), W - 1); }
+                    if (mode[1] == 0) { if (h < 0 || h >= H) continue; } else { h = std::min(std::max(h, 0), H - 1); }
+                    if (mode[2] == 0) { if (d < 0 || d >= D) continue; } else { d = std::min(std::max(d, 0), D - 1); }
+                    adj[((size_t)d * H + h) * W + w] += (T)(ww * wh * wd) * v;
+                }
+            }
+        }
+    }
+};
+
+// Per-ray geometry of DDFPFanKernelX/Y (DistanceDriven.cu:81-113 / :149-179),
+// in image coordinates with the origin at the corner of pixel 0
+// (PhysicsToImg, DistanceDriven.cu:14-20; cx = cy = cz = 0 for the fan API).
+struct FanRay {
+    double sx, sy;      // source
+    double r1, r2;      // slopes of the two cell-edge rays (dx/dy for X, dy/dx for Y)
+    double lenw;        // dy/|cos(deg-a)| or dx/|sin(deg-a)|
+    double zc;          // texture coordinate along z
+    bool xcls;
+};
+
+inline FanRay fan_ray(const Fan& g, float degf, int iu, int iv) {
+    FanRay R;
+    double deg = degf;
+    double c = std::cos(deg), s = std::sin(deg);
+    double a = chan_angle(g, iu);
+    double z = (iv - (g.nv - 1) / 2.0 + g.off_v) * g.dv;
+    double srcx = g.dso * s, srcy = -g.dso * c;
+    double e1x = g.dsd * std::sin(a - g.du / 2), e1y = -g.dso + g.dsd * std::cos(a - g.du / 2);
+    double e2x = g.dsd * std::sin(a + g.du / 2), e2y = -g.dso + g.dsd * std::cos(a + g.du / 2);
+    double d1x = e1x * c - e1y * s, d1y = e1x * s + e1y * c;
+    double d2x = e2x * c - e2y * s, d2y = e2x * s + e2y * c;
+    R.sx = srcx / g.dx + g.nx / 2.0;
+    R.sy = srcy / g.dy + g.ny / 2.0;
+    d1x = d1x / g.dx + g.nx / 2.0;
+    d1y = d1y / g.dy + g.ny / 2.0;
+    d2x = d2x / g.dx + g.nx / 2.0;
+    d2y = d2y / g.dy + g.ny / 2.0;
+    R.zc = z / g.dz + g.nz / 2.0;
+    R.xcls = x_class(degf);
+    if (R.xcls) {
+        R.r1 = (d1x - R.sx) / (d1y - R.sy);
+        R.r2 = (d2x - R.sx) / (d2y - R.sy);
+        R.lenw = g.dy / std::fabs(std::cos(deg - a));
+    } else {
+        R.r1 = (d1y - R.sy) / (d1x - R.sx);
+        R.r2 = (d2y - R.sy) / (d2x - R.sx);
+        R.lenw = g.dx / std::fabs(std::sin(deg - a));
+    }
+    return R;
+}
+
+// --------------------------------------------------------------------------
+// DD fan forward projection: DDFPFanKernelX/Y, DistanceDriven.cu:64-196,
+// driven as in DistanceDrivenFan::Projection :198-384.
+// Texture layouts (:234-271): AccX extents (nz, ny, nx+1), modes
+// (border, border, clamp); AccY extents (nz, ny+1, nx), modes
+// (border, clamp, border).
+// --------------------------------------------------------------------------
+template <typename T>
+void fan_fp(T* prj, const float* img, const float* deg, const Fan& g) {
+    for (int b = 0; b < g.nb; b++)
+        for (int c = 0; c < g.nc; c++) {
+            std::vector<T> PX, PY;
+            build_prefix<T>(g, img, b, c, PX, PY);
+            Tex3<T> tx{PX.data(), g.nz, g.ny, g.nx + 1, {0, 0, 1}};
+            Tex3<T> ty{PY.data(), g.nz, g.ny + 1, g.nx, {0, 1, 0}};
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+            for (int iview = 0; iview < g.nview; iview++)
+                for (int iu = 0; iu < g.nu; iu++)
+                    for (int iv = 0; iv < g.nv; iv++) {
+                        FanRay R = fan_ray(g, deg[iview], iu, iv);
+                        T val = 0;
+                        if (R.xcls) {
+                            for (int iy = 0; iy < g.ny; iy++) {
+                                double x1 = R.sx + R.r1 * (iy - R.sy);
+                                double x2 = R.sx + R.r2 * (iy - R.sy);
+                                T d = tx.fetch(R.zc, iy, x2 + 0.5) - tx.fetch(R.zc, iy, x1 + 0.5);
+                                val += d / (T)(x2 - x1);
+                            }
+                        } else {
+                            for (int ix = 0; ix < g.nx; ix++) {
+                                double y1 = R.sy + R.r1 * (ix - R.sx);
+                                double y2 = R.sy + R.r2 * (ix - R.sx);
+                                T d = ty.fetch(R.zc, y2 + 0.5, ix) - ty.fetch(R.zc, y1 + 0.5, ix);
+                                val += d / (T)(y2 - y1);
+                            }
+                        }
+                        prj[prj_index(g, b, iu, iview, iv, c)] = val * (T)R.lenw;
+                    }
+        }
+}
+
+// --------------------------------------------------------------------------
+// Matched DD fan backprojection: the exact transpose of fan_fp above (not a
+// reference kernel).  Scatter into adjoint prefix arrays, then suffix sums
+// (the transpose of the prefix sums of build_prefix).
+// --------------------------------------------------------------------------
+template <typename T>
+void fan_bp_matched(T* img, const float* prj, const float* deg, const Fan& g) {
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    size_t nPX = (size_t)(g.nx + 1) * g.ny * g.nz, nPY = (size_t)g.nx * (g.ny + 1) * g.nz;
+    for (int b = 0; b < g.nb; b++)
+        for (int c = 0; c < g.nc; c++) {
+            std::vector<T> aPX((size_t)nthreads * nPX, T(0)), aPY((size_t)nthreads * nPY, T(0));
+            Tex3<T> tx{nullptr, g.nz, g.ny, g.nx + 1, {0, 0, 1}};
+            Tex3<T> ty{nullptr, g.nz, g.ny + 1, g.nx, {0, 1, 0}};
+#pragma omp parallel
+            {
+                int tid = 0;
+#ifdef _OPENMP
+                tid = omp_get_thread_num();
+#endif
+                T* myX = aPX.data() + (size_t)tid * nPX;
+                T* myY = aPY.data() + (size_t)tid * nPY;
+#pragma omp for schedule(dynamic, 1) collapse(2)
+                for (int iview = 0; iview < g.nview; iview++)
+                    for (int iu = 0; iu < g.nu; iu++)
+                        for (int iv = 0; iv < g.nv; iv++) {
+                            FanRay R = fan_ray(g, deg[iview], iu, iv);
+                            T w = (T)prj[prj_index(g, b, iu, iview, iv, c)] * (T)R.lenw;
+                            if (w == T(0)) continue;
+                            if (R.xcls) {
+                                for (int iy = 0; iy < g.ny; iy++) {
+                                    double x1 = R.sx + R.r1 * (iy - R.sy);
+                                    double x2 = R.sx + R.r2 * (iy - R.sy);
+                                    T s = w / (T)(x2 - x1);
+                                    tx.scatter(myX, R.zc, iy, x2 + 0.5, s);
+                                    tx.scatter(myX, R.zc, iy, x1 + 0.5, -s);
+                                }
+                            } else {
+                                for (int ix = 0; ix < g.nx; ix++) {
+                                    double y1 = R.sy + R.r1 * (ix - R.sx);
+                                    double y2 = R.sy + R.r2 * (ix - R.sx);
+                                    T s = w / (T)(y2 - y1);
+                                    ty.scatter(myY, R.zc, y2 + 0.5, ix, s);
+                                    ty.scatter(myY, R.zc, y1 + 0.5, ix, -s);
+                                }
+                            }
+                        }
+            }
+            for (int t = 1; t < nthreads; t++) {
+                for (size_t i = 0; i < nPX; i++) aPX[i] += aPX[(size_t)t * nPX + i];
+                for (size_t i = 0; i < nPY; i++) aPY[i] += aPY[(size_t)t * nPY + i];
+            }
+            // P[k] = sum_{i<k} img[i]  =>  adj_img[i] = sum_{k>i} adj_P[k]
+            for (int ix = 0; ix < g.nx; ix++)
+                for (int iy = 0; iy < g.ny; iy++)
+                    for (int iz = 0; iz < g.nz; iz++) img[img_index(g, b, ix, iy, iz, c)] = 0;
+            for (int iy = 0; iy < g.ny; iy++)
+                for (int iz = 0; iz < g.nz; iz++) {
+                    T acc = 0;
+                    for (int k = g.nx; k >= 1; k--) {
+                        acc += aPX[((size_t)k * g.ny + iy) * g.nz + iz];
+                        img[img_index(g, b, k - 1, iy, iz, c)] += acc;
+                    }
+                }
+            for (int ix = 0; ix < g.nx; ix++)
+                for (int iz = 0; iz < g.nz; iz++) {
+                    T acc = 0;
+                    for (int k = g.ny; k >= 1; k--) {
+                        acc += aPY[((size_t)ix * (g.ny + 1) + k) * g.nz + iz];
+                        img[img_index(g, b, ix, k - 1, iz, c)] += acc;
+                    }
+                }
+        }
+}
+
+// --------------------------------------------------------------------------
+// Reference-mode DD fan backprojection: PreweightBPKernelX/Y
+// (DistanceDriven.cu:441-477), u-prefix (AccumulateKernelX reused, :746-756),
+// DDBPFanKernelX/Y (:500-614) with GetProjectionOnDetector (:479) and
+// GetFBPWeight (:487).  typeProjector == 1 -> FBP weighting, no pre-weight.
+// AccU texture (:653-675): extents (nv, nview, nu+1), modes
+// (border, border, clamp).
+// --------------------------------------------------------------------------
+template <typename T>
+void fan_bp_ref(T* img, const float* prj, const float* deg, const Fan& g, int typeProjector) {
+    const bool isFBP = (typeProjector == 1);
+    std::vector<char> xcls(g.nview);
+    std::vector<double> cs(g.nview), sn(g.nview);
+    for (int v = 0; v < g.nview; v++) {
+        xcls[v] = x_class(deg[v]);
+        cs[v] = std::cos((double)deg[v]);
+        sn[v] = std::sin((double)deg[v]);
+    }
+    for (int b = 0; b < g.nb; b++)
+        for (int c = 0; c < g.nc; c++) {
+            // weighted sinogram and its prefix along u: U[u][view][v], u in [0, nu]
+            std::vector<T> U((size_t)(g.nu + 1) * g.nview * g.nv, T(0));
+            for (int iview = 0; iview < g.nview; iview++)
+                for (int iv = 0; iv < g.nv; iv++) {
+                    T acc = 0;
+                    for (int iu = 0; iu < g.nu; iu++) {
+                        T p = (T)prj[prj_index(g, b, iu, iview, iv, c)];
+                        if (!isFBP) {
+                            double a = chan_angle(g, iu);
+                            double dd = (double)deg[iview] - a;
+                            p *= xcls[iview] ? (T)(g.dy / std::fabs(std::cos(dd))) : (T)(g.dx / std::fabs(std::sin(dd)));
+                        }
+                        acc += p;
+                        U[((size_t)(iu + 1) * g.nview + iview) * g.nv + iv] = acc;
+                    }
+                }
+            Tex3<T> tu{U.data(), g.nv, g.nview, g.nu + 1, {0, 0, 1}};
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int ix = 0; ix < g.nx; ix++)
+                for (int iy = 0; iy < g.ny; iy++)
+                    for (int iz = 0; iz < g.nz; iz++) {
+                        double x = (ix - (g.nx - 1) / 2.0) * g.dx;
+                        double y = (iy - (g.ny - 1) / 2.0) * g.dy;
+                        double ivf = (iz - (g.nz - 1) / 2.0) * g.dz / g.dv + g.off_v + (g.nv - 1.0) / 2.0;
+                        T val = 0;
+                        for (int iview = 0; iview < g.nview; iview++) {
+                            double cd = cs[iview], sd = sn[iview];
+                            double px1, py1, px2, py2;
+                            if (xcls[iview]) {
+                                px1 = x - g.dx / 2; py1 = y; px2 = x + g.dx / 2; py2 = y;
+                            } else {
+                                px1 = x; py1 = y - g.dy / 2; px2 = x; py2 = y + g.dy / 2;
+                            }
+                            auto proj = [&](double px, double py) {
+                                double rx = px * cd + py * sd;
+                                double ry = -px * sd + py * cd;
+                                double a = std::atan(rx / (ry + g.dso));
+                                return -(a / g.du + g.off_u) + g.nu / 2.0;
+                            };
+                            double a1 = proj(px1, py1), a2 = proj(px2, py2);
+                            if (a1 > a2) std::swap(a1, a2);
+                            T v = (tu.fetch(ivf + 0.5, iview + 0.5, a2 + 0.5) - tu.fetch(ivf + 0.5, iview + 0.5, a1 + 0.5)) / (T)(a2 - a1);
+                            if (isFBP) {
+                                double rx = x * cd + y * sd;
+                                double ry = -x * sd + y * cd;
+                                v *= (T)(g.dso * g.dso / (rx * rx + (g.dso + ry) * (g.dso + ry)));
+                            }
+                            val += v;
+                        }
+                        img[img_index(g, b, ix, iy, iz, c)] = val;
+                    }
+        }
+}
+
+// --------------------------------------------------------------------------
+// Ramp filter: getRamp (Filter.cu:66-214) and cFilterFan::Filter (:216-342) /
+// cFilterParallel::Filter (:344-430).  The reference convolves through cuFFT
+// with zero padding to L = 2nu-1; the output window it keeps (offset nu-1) is
+// an exact linear convolution, restated here directly in T precision.
+// --------------------------------------------------------------------------
+void dft(std::vector<std::complex<double>>& a, bool inverse) {
+    size_t n = a.size();
+    std::vector<std::complex<double>> out(n);
+    double sgn = inverse ? 1.0 : -1.0;
+    for (size_t k = 0; k < n; k++) {
+        std::complex<double> acc = 0;
+        for (size_t j = 0; j < n; j++) {
+            double ang = sgn * 2.0 * M_PI * (double)((k * j) % n) / (double)n;
+            acc += a[j] * std::complex<double>(std::cos(ang), std::sin(ang));
+        }
+        out[k] = acc;
+    }
+    a.swap(out);
+}
+
+// Real spatial-domain kernel h[0..L-1] (offset k = i - (nu-1)), the
+// real part of ifft(fft(ramp) * window) of getRamp.
+std::vector<double> ramp_kernel(int nu, double da, int typeFilter, bool equispace) {
+    int L = 2 * nu - 1;
+    std::vector<std::complex<double>> r(L);
+    for (int i = 0; i < L; i++) {
+        int k = i - (nu - 1);
+        double v;
+        if (k == 0) v = 1.0 / (4 * da * da);
+        else if (k % 2 != 0) {
+            if (equispace) v = -1.0 / (kRefPi * kRefPi * (double)k * k * da * da);
+            else { double s = std::sin(k * da); v = -1.0 / (kRefPi * kRefPi * s * s); }
+        } else v = 0;
+        r[i] = v;
+    }
+    if (typeFilter >= 1 && typeFilter <= 3) {
+        dft(r, false);
+        for (int i = 0; i < L; i++) {
+            double w;
+            if (typeFilter == 1) w = 0.54 + 0.46 * std::cos(2 * kRefPi * i / (double)(L - 1));
+            else if (typeFilter == 2) w = 0.5 + 0.5 * std::cos(2 * kRefPi * i / (double)(L - 1));
+            else w = std::fabs(std::cos(kRefPi * i / (double)(L - 1)));
+            r[i] *= w;
+        }
+        dft(r, true);
+        for (int i = 0; i < L; i++) r[i] /= (double)L;
+    }
+    std::vector<double> h(L);
+    for (int i = 0; i < L; i++) h[i] = r[i].real();
+    return h;
+}
+
+template <typename T>
+void filter_sino(T* out, const float* prj, int nb, int nc, int nu, int nview, int nv, double da, double off_a,
+                 double dsd, double dso, int typeFilter, bool fan) {
+    std::vector<double> h = ramp_kernel(nu, da, typeFilter, !fan);
+    std::vector<double> pw(nu, 1.0);
+    double scale;
+    if (fan) {
+        for (int i = 0; i < nu; i++) pw[i] = std::cos(((i - (nu - 1) / 2.0) - off_a) * da);
+        scale = kRefPi / nview * da / dso;
+    } else {
+        scale = kRefPi / nview * da;
+    }
+    (void)dsd;
+#pragma omp parallel for collapse(3) schedule(static)
+    for (int b = 0; b < nb; b++)
+        for (int iview = 0; iview < nview; iview++)
+            for (int iv = 0; iv < nv; iv++)
+                for (int c = 0; c < nc; c++) {
+                    std::vector<T> x(nu);
+                    for (int j = 0; j < nu; j++)
+                        x[j] = (T)prj[((((size_t)b * nu + j) * nview + iview) * nv + iv) * nc + c] * (T)pw[j];
+                    for (int iu = 0; iu < nu; iu++) {
+                        T acc = 0;
+                        for (int j = 0; j < nu; j++) acc += x[j] * (T)h[nu - 1 + iu - j];
+                        out[((((size_t)b * nu + iu) * nview + iview) * nv + iv) * nc + c] = acc * (T)scale;
+                    }
+                }
+}
+
+// --------------------------------------------------------------------------
+// TV surrogate: TVSQSKernel (TotalVariation.cu:9-68), zero padding at the
+// border, eps = 1e-6; cTVSQS2D (:70-142) returns sum(var).
+// --------------------------------------------------------------------------
+template <typename T>
+double tv_sqs(T* grad, T* norm, const float* img, int nx, int ny) {
+    double tv = 0;
+#pragma omp parallel for reduction(+ : tv) schedule(static)
+    for (int ix = 0; ix < nx; ix++)
+        for (int iy = 0; iy < ny; iy++) {
+            size_t ind = (size_t)ix * ny + iy;
+            T x = img[ind];
+            T dx0 = ix == 0 ? x : x - (T)img[ind - ny];
+            T dx1 = ix == nx - 1 ? x : x - (T)img[ind + ny];
+            T dy0 = iy == 0 ? x : x - (T)img[ind - 1];
+            T dy1 = iy == ny - 1 ? x : x - (T)img[ind + 1];
+            const T eps = (T)1e-6f;
+            T t0 = std::sqrt(dx0 * dx0 + eps), t1 = std::sqrt(dx1 * dx1 + eps);
+            T t2 = std::sqrt(dy0 * dy0 + eps), t3 = std::sqrt(dy1 * dy1 + eps);
+            if (grad) grad[ind] = (dx0 / t0 + dx1 / t1 + dy0 / t2 + dy1 / t3) / 2;
+            if (norm) norm[ind] = 1 / t0 + 1 / t1 + 1 / t2 + 1 / t3;
+            tv += (double)((t0 + t1 + t2 + t3) / 2);
+        }
+    return tv;
+}
+
+// --------------------------------------------------------------------------
+// Tomosynthesis DD: DistanceDrivenTomo::ProjectionTomo / BackprojectionTomo
+// (DistanceDriven3D.cu:37-343, :409-663).  detU = (1,0,0), detV = (0,1,0).
+// --------------------------------------------------------------------------
+struct Tomo {
+    int nb, nc, nx, ny, nz;
+    double dx, dy, dz, cx, cy, cz;
+    int nu, nview, nv;
+    double du, dv, off_u, off_v;
+};
+
+// Clamp_float + InterpolateXY (DistanceDriven3D.cu:75-135): x clamped to
+// [0, n-1] (n = nx+1) at and beyond n, bilinear on a (n0 x n1) grid.
+template <typename T>
+inline T sat_interp(const T* acc, double x, double y, int n0, int n1, int stride0, int stride1) {
+    if (x < 0) x = 0; else if (x >= n0) x = n0 - 1;
+    if (y < 0) y = 0; else if (y >= n1) y = n1 - 1;
+    int i0 = (int)x, j0 = (int)y;
+    int i1 = std::min(i0 + 1, n0 - 1), j1 = std::min(j0 + 1, n1 - 1);
+    double wx = x - i0, wy = y - j0;
+    return (T)(acc[(size_t)i0 * stride0 + (size_t)j0 * stride1] * (1 - wx) * (1 - wy) +
+               acc[(size_t)i1 * stride0 + (size_t)j0 * stride1] * wx * (1 - wy) +
+               acc[(size_t)i0 * stride0 + (size_t)j1 * stride1] * (1 - wx) * wy +
+               acc[(size_t)i1 * stride0 + (size_t)j1 * stride1] * wx * wy);
+}
+
+template <typename T>
+void tomo_fp(T* prj, const float* img, const float* detCenter, const float* src, const Tomo& g) {
+    size_t nacc = (size_t)(g.nx + 1) * (g.ny + 1) * g.nz;
+    for (int b = 0; b < g.nb; b++)
+        for (int c = 0; c < g.nc; c++) {
+            // SAT acc[x][y][z], x in [0,nx], y in [0,ny]  (AccumulateXYAlongX/Y, :37-73)
+            std::vector<T> acc(nacc, T(0));
+            for (int iz = 0; iz < g.nz; iz++)
+                for (int ix = 0; ix < g.nx; ix++)
+                    for (int iy = 0; iy < g.ny; iy++) {
+                        T v = (T)img[((((size_t)b * g.nx + ix) * g.ny + iy) * g.nz + iz) * g.nc + c];
+                        size_t o = ((size_t)(ix + 1) * (g.ny + 1) + (iy + 1)) * g.nz + iz;
+                        acc[o] = v + acc[((size_t)ix * (g.ny + 1) + (iy + 1)) * g.nz + iz] +
+                                 acc[((size_t)(ix + 1) * (g.ny + 1) + iy) * g.nz + iz] -
+                                 acc[((size_t)ix * (g.ny + 1) + iy) * g.nz + iz];
+                    }
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+            for (int iview = 0; iview < g.nview; iview++)
+                for (int iu = 0; iu < g.nu; iu++)
+                    for (int iv = 0; iv < g.nv; iv++) {
+                        const float* dc = detCenter + 3 * iview;
+                        const float* sp = src + 3 * iview;
+                        double u = (iu - g.off_u - (g.nu - 1) / 2.0) * g.du;
+                        double v = (iv - g.off_v - (g.nv - 1) / 2.0) * g.dv;
+                        auto toimg = [&](double px, double py, double pz, double& ox, double& oy, double& oz) {
+                            ox = (px - g.cx) / g.dx + g.nx / 2.0;
+                            oy = (py - g.cy) / g.dy + g.ny / 2.0;
+                            oz = (pz - g.cz) / g.dz + g.nz / 2.0;
+                        };
+                        double x1x, x1y, x1z, x2x, x2y, x2z, y1x, y1y, y1z, y2x, y2y, y2z, sx, sy, sz;
+                        toimg(dc[0] + u - g.du / 2, dc[1] + v, dc[2], x1x, x1y, x1z);
+                        toimg(dc[0] + u + g.du / 2, dc[1] + v, dc[2], x2x, x2y, x2z);
+                        toimg(dc[0] + u, dc[1] + v - g.dv / 2, dc[2], y1x, y1y, y1z);
+                        toimg(dc[0] + u, dc[1] + v + g.dv / 2, dc[2], y2x, y2y, y2z);
+                        toimg(sp[0], sp[1], sp[2], sx, sy, sz);
+                        if (x1x > x2x) { std::swap(x1x, x2x); std::swap(x1y, x2y); std::swap(x1z, x2z); }
+                        if (y1y > y2y) { std::swap(y1x, y2x); std::swap(y1y, y2y); std::swap(y1z, y2z); }
+                        double rx1 = (x1x - sx) / (x1z - sz), rx2 = (x2x - sx) / (x2z - sz);
+                        double ry1 = (y1y - sy) / (y1z - sz), ry2 = (y2y - sy) / (y2z - sz);
+                        T val = 0;
+                        for (int iz = 0; iz < g.nz; iz++) {
+                            double xa = sx + rx1 * (iz - sz), xb = sx + rx2 * (iz - sz);
+                            double ya = sy + ry1 * (iz - sz), yb = sy + ry2 * (iz - sz);
+                            const T* a = acc.data() + iz;
+                            int s0 = (g.ny + 1) * g.nz, s1 = g.nz;
+                            T q = sat_interp(a, xb, yb, g.nx + 1, g.ny + 1, s0, s1) + sat_interp(a, xa, ya, g.nx + 1, g.ny + 1, s0, s1) -
+                                  sat_interp(a, xb, ya, g.nx + 1, g.ny + 1, s0, s1) - sat_interp(a, xa, yb, g.nx + 1, g.ny + 1, s0, s1);
+                            val += q / (T)((xb - xa) * (yb - ya));
+                        }
+                        double dstx = dc[0] + u, dsty = dc[1] + v, dstz = dc[2];
+                        double ddx = sp[0] - dstx, ddy = sp[1] - dsty, ddz = sp[2] - dstz;
+                        val *= (T)(g.dz / std::fabs(ddz) * std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz));
+                        prj[((((size_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + c] = val;
+                    }
+        }
+}
+
+template <typename T>
+void tomo_bp(T* img, const float* prj, const float* detCenter, const float* src, const Tomo& g) {
+    size_t nacc = (size_t)(g.nu + 1) * g.nview * (g.nv + 1);
+    for (int b = 0; b < g.nb; b++)
+        for (int c = 0; c < g.nc; c++) {
+            // Pre-weight (PreweightBPCartKernelXY :409-431) + SAT over (u, v) per view
+            // (AccumulateUVAlongU/V :437-474): acc[u][view][v], u in [0,nu], v in [0,nv].
+            std::vector<T> acc(nacc, T(0));
+            for (int iview = 0; iview < g.nview; iview++) {
+                const float* dc = detCenter + 3 * iview;
+                const float* sp = src + 3 * iview;
+                for (int iu = 0; iu < g.nu; iu++)
+                    for (int iv = 0; iv < g.nv; iv++) {
+                        double u = (iu - g.off_u - (g.nu - 1) / 2.0) * g.du;
+                        double v = (iv - g.off_v - (g.nv - 1) / 2.0) * g.dv;
+                        double ddx = sp[0] - (dc[0] + u), ddy = sp[1] - (dc[1] + v), ddz = sp[2] - dc[2];
+                        T w = (T)prj[((((size_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + c] *
+                              (T)(g.dz / std::fabs(ddz) * std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz));
+                        size_t o = ((size_t)(iu + 1) * g.nview + iview) * (g.nv + 1) + (iv + 1);
+                        acc[o] = w + acc[((size_t)iu * g.nview + iview) * (g.nv + 1) + (iv + 1)] +
+                                 acc[((size_t)(iu + 1) * g.nview + iview) * (g.nv + 1) + iv] -
+                                 acc[((size_t)iu * g.nview + iview) * (g.nv + 1) + iv];
+                    }
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int ix = 0; ix < g.nx; ix++)
+                for (int iy = 0; iy < g.ny; iy++)
+                    for (int iz = 0; iz < g.nz; iz++) {
+                        double x = (ix - (g.nx - 1) / 2.0) * g.dx + g.cx;
+                        double y = (iy - (g.ny - 1) / 2.0) * g.dy + g.cy;
+                        double z = (iz - (g.nz - 1) / 2.0) * g.dz + g.cz;
+                        T val = 0;
+                        for (int iview = 0; iview < g.nview; iview++) {
+                            const float* dc = detCenter + 3 * iview;
+                            const float* sp = src + 3 * iview;
+                            // ProjectConeToDetCart (:478-489)
+                            auto pu = [&](double px, double pz) {
+                                double r = (dc[2] - sp[2]) / (pz - sp[2]);
+                                double uu = sp[0] - dc[0] + r * (px - sp[0]);
+                                return uu / g.du + g.off_u + (g.nu - 1) / 2.0;
+                            };
+                            auto pv = [&](double py, double pz) {
+                                double r = (dc[2] - sp[2]) / (pz - sp[2]);
+                                double vv = sp[1] - dc[1] + r * (py - sp[1]);
+                                return vv / g.dv + g.off_v + (g.nv - 1) / 2.0;
+                            };
+                            double u1 = pu(x - g.dx / 2, z), u2 = pu(x + g.dx / 2, z);
+                            double v1 = pv(y - g.dy / 2, z), v2 = pv(y + g.dy / 2, z);
+                            const T* a = acc.data() + (size_t)iview * (g.nv + 1);
+                            int s0 = g.nview * (g.nv + 1), s1 = 1;
+                            T q = sat_interp(a, u2, v2, g.nu + 1, g.nv + 1, s0, s1) - sat_interp(a, u2, v1, g.nu + 1, g.nv + 1, s0, s1) +
+                                  sat_interp(a, u1, v1, g.nu + 1, g.nv + 1, s0, s1) - sat_interp(a, u1, v2, g.nu + 1, g.nv + 1, s0, s1);
+                            val += q / (T)((u2 - u1) * (v2 - v1));
+                        }
+                        img[((((size_t)b * g.nx + ix) * g.ny + iy) * g.nz + iz) * g.nc + c] = val;
+                    }
+        }
+}
+
+inline Fan make_fan(int nb, int nc, int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
+                    float da, float dv, float off_a, float off_v, float dsd, float dso) {
+    Fan g;
+    g.nb = nb; g.nc = nc; g.nx = nx; g.ny = ny; g.nz = nz;
+    g.dx = dx; g.dy = dy; g.dz = dz;
+    g.nu = nu; g.nview = nview; g.nv = nv;
+    g.du = da; g.dv = dv; g.off_u = off_a; g.off_v = off_v; g.dsd = dsd; g.dso = dso;
+    return g;
+}
+
+inline Tomo make_tomo(int nb, int nc, int nx, int ny, int nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                      int nu, int nview, int nv, float du, float dv, float off_u, float off_v) {
+    Tomo g;
+    g.nb = nb; g.nc = nc; g.nx = nx; g.ny = ny; g.nz = nz;
+    g.dx = dx; g.dy = dy; g.dz = dz; g.cx = cx; g.cy = cy; g.cz = cz;
+    g.nu = nu; g.nview = nview; g.nv = nv;
+    g.du = du; g.dv = dv; g.off_u = off_u; g.off_v = off_v;
+    return g;
+}
+
+}  // namespace
+
+#define FAN_ARGS                                                                                                  \
+    int nb, int nc, int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da,    \
+        float dv, float off_a, float off_v, float dsd, float dso
+#define FAN_PASS nb, nc, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso
+#define TOMO_ARGS                                                                                                  \
+    int nb, int nc, int nx, int ny, int nz, float dx, float dy, float dz, float cx, float cy, float cz, int nu,   \
+        int nview, int nv, float du, float dv, float off_u, float off_v
+#define TOMO_PASS nb, nc, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nview, nv, du, dv, off_u, off_v
+
+extern "C" {
+
+int oracle_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void oracle_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int oracle_view_is_x(float deg) { return x_class(deg) ? 1 : 0; }
+
+void oracle_set_tex_quant(int mode) { g_tex_quant = mode; }
+
+void oracle_fan_fp_f64(double* prj, const float* img, const float* deg, FAN_ARGS) {
+    fan_fp<double>(prj, img, deg, make_fan(FAN_PASS));
+}
+void oracle_fan_fp_f32(float* prj, const float* img, const float* deg, FAN_ARGS) {
+    fan_fp<float>(prj, img, deg, make_fan(FAN_PASS));
+}
+// typeProjector: 0 iterative (reference), 1 FBP (reference), 2 matched transpose
+void oracle_fan_bp_f64(double* img, const float* prj, const float* deg, FAN_ARGS, int typeProjector) {
+    Fan g = make_fan(FAN_PASS);
+    if (typeProjector == 2) fan_bp_matched<double>(img, prj, deg, g);
+    else fan_bp_ref<double>(img, prj, deg, g, typeProjector);
+}
+void oracle_fan_bp_f32(float* img, const float* prj, const float* deg, FAN_ARGS, int typeProjector) {
+    Fan g = make_fan(FAN_PASS);
+    if (typeProjector == 2) fan_bp_matched<float>(img, prj, deg, g);
+    else fan_bp_ref<float>(img, prj, deg, g, typeProjector);
+}
+void oracle_ramp_kernel(double* h, int nu, float da, int typeFilter, int equispace) {
+    std::vector<double> k = ramp_kernel(nu, da, typeFilter, equispace != 0);
+    std::memcpy(h, k.data(), sizeof(double) * k.size());
+}
+void oracle_filter_f64(double* out, const float* prj, int nb, int nc, int nu, int nview, int nv, float da, float dv,
+                       float off_a, float off_v, float dsd, float dso, int typeFilter, int fan) {
+    (void)dv; (void)off_v;
+    filter_sino<double>(out, prj, nb, nc, nu, nview, nv, da, off_a, dsd, dso, typeFilter, fan != 0);
+}
+double oracle_tv_sqs_f64(double* grad, double* norm, const float* img, int nx, int ny) {
+    return tv_sqs<double>(grad, norm, img, nx, ny);
+}
+void oracle_tomo_fp_f64(double* prj, const float* img, const float* detCenter, const float* src, TOMO_ARGS) {
+    tomo_fp<double>(prj, img, detCenter, src, make_tomo(TOMO_PASS));
+}
+void oracle_tomo_bp_f64(double* img, const float* prj, const float* detCenter, const float* src, TOMO_ARGS) {
+    tomo_bp<double>(img, prj, detCenter, src, make_tomo(TOMO_PASS));
+}
+
+}  // extern "C"

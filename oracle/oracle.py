@@ -1,0 +1,212 @@
+"""TEST INFRASTRUCTURE -- the CPU oracle for the DD hot path (not product code).
+
+ctypes wrapper over ``oracle/liboracle.so`` (built from ``oracle/oracle.cpp`` by
+``oracle/Makefile``).  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline / reference legs of ``bench.py`` may import this module.
+
+Array conventions are the reference's (python/ReconNet_no_tf.py:133-200):
+images are ``[B, nx, ny, nz, C]`` and sinograms ``[B, nu, nview, nv, C]``, C-order.
+Geometry objects only need the attributes ``dx dy dz da dv off_a off_v dsd dso``
+(fan) or ``dx dy dz cx cy cz du dv off_u off_v`` (tomo).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_f = ctypes.c_float
+_i = ctypes.c_int
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+_FAN = [_i, _i, _i, _i, _i, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f, _f, _f]
+_TOMO = [_i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f]
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (gcc, OpenMP)."""
+    src = os.path.join(_HERE, "oracle.cpp")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.oracle_num_threads.restype = _i
+        L.oracle_set_num_threads.argtypes = [_i]
+        L.oracle_view_is_x.argtypes = [_f]
+        L.oracle_view_is_x.restype = _i
+        L.oracle_set_tex_quant.argtypes = [_i]
+        L.oracle_fan_fp_f64.argtypes = [_dp, _fp, _fp] + _FAN
+        L.oracle_fan_fp_f32.argtypes = [_fp, _fp, _fp] + _FAN
+        L.oracle_fan_bp_f64.argtypes = [_dp, _fp, _fp] + _FAN + [_i]
+        L.oracle_fan_bp_f32.argtypes = [_fp, _fp, _fp] + _FAN + [_i]
+        L.oracle_ramp_kernel.argtypes = [_dp, _i, _f, _i, _i]
+        L.oracle_filter_f64.argtypes = [_dp, _fp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i]
+        L.oracle_tv_sqs_f64.argtypes = [_dp, _dp, _fp, _i, _i]
+        L.oracle_tv_sqs_f64.restype = ctypes.c_double
+        L.oracle_tomo_fp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
+        L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
+        _lib = L
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
+
+
+def set_tex_quant(mode: int) -> None:
+    """0 exact texture weights (default), 1 rounded / 2 truncated to 1/256."""
+    lib().oracle_set_tex_quant(int(mode))
+
+
+def view_is_x(deg: float) -> bool:
+    return bool(lib().oracle_view_is_x(float(deg)))
+
+
+def _fan_args(g, img_shape, sino_shape):
+    B, nx, ny, nz, C = img_shape
+    _, nu, nview, nv, _ = sino_shape
+    return (B, C, nx, ny, nz, g.dx, g.dy, g.dz, nu, nview, nv, g.da, g.dv, g.off_a, g.off_v, g.dsd, g.dso)
+
+
+def fan_fp(img, angles, g, nu, nv=None, dtype=np.float64):
+    """DD fan forward projection (DistanceDriven.cu:64-384), exact texture lerp."""
+    img = _f32(img)
+    ang = _f32(angles)
+    B, nx, ny, nz, C = img.shape
+    nv = nz if nv is None else nv
+    out = np.zeros((B, nu, ang.size, nv, C), dtype=dtype)
+    args = _fan_args(g, img.shape, out.shape)
+    if dtype == np.float64:
+        lib().oracle_fan_fp_f64(_ptr(out, ctypes.c_double), _ptr(img, _f), _ptr(ang, _f), *args)
+    else:
+        lib().oracle_fan_fp_f32(_ptr(out, _f), _ptr(img, _f), _ptr(ang, _f), *args)
+    return out
+
+
+def fan_bp(sino, angles, g, img_shape, type_projector=0, dtype=np.float64):
+    """DD fan backprojection.  type 0/1: reference DDBPFanKernelX/Y
+    (DistanceDriven.cu:441-791); type 2: exact transpose of ``fan_fp``."""
+    sino = _f32(sino)
+    ang = _f32(angles)
+    B, nu, nview, nv, C = sino.shape
+    nx, ny, nz = img_shape
+    out = np.zeros((B, nx, ny, nz, C), dtype=dtype)
+    args = _fan_args(g, out.shape, sino.shape)
+    if dtype == np.float64:
+        lib().oracle_fan_bp_f64(_ptr(out, ctypes.c_double), _ptr(sino, _f), _ptr(ang, _f), *args, int(type_projector))
+    else:
+        lib().oracle_fan_bp_f32(_ptr(out, _f), _ptr(sino, _f), _ptr(ang, _f), *args, int(type_projector))
+    return out
+
+
+def ramp_kernel(nu, da, type_filter=0, equispace=False):
+    """Spatial filter kernel of getRamp (Filter.cu:66-214), length 2nu-1."""
+    h = np.zeros(2 * nu - 1, np.float64)
+    lib().oracle_ramp_kernel(_ptr(h, ctypes.c_double), int(nu), float(da), int(type_filter), int(bool(equispace)))
+    return h
+
+
+def filter_sino(sino, g, type_filter=0, fan=True):
+    """cFilterFan::Filter / cFilterParallel::Filter (Filter.cu:216-430)."""
+    sino = _f32(sino)
+    B, nu, nview, nv, C = sino.shape
+    out = np.zeros(sino.shape, np.float64)
+    lib().oracle_filter_f64(_ptr(out, ctypes.c_double), _ptr(sino, _f), B, C, nu, nview, nv, g.da, g.dv, g.off_a,
+                            g.off_v, g.dsd, g.dso, int(type_filter), int(bool(fan)))
+    return out
+
+
+def tv_sqs(img2d):
+    """TVSQSKernel + cTVSQS2D (TotalVariation.cu:9-142); img2d is [nx, ny]."""
+    img = _f32(img2d)
+    nx, ny = img.shape
+    grad = np.zeros((nx, ny), np.float64)
+    norm = np.zeros((nx, ny), np.float64)
+    tv = lib().oracle_tv_sqs_f64(_ptr(grad, ctypes.c_double), _ptr(norm, ctypes.c_double), _ptr(img, _f), nx, ny)
+    return grad, norm, float(tv)
+
+
+def _tomo_args(g, img_shape, prj_shape):
+    B, nx, ny, nz, C = img_shape
+    _, nu, nview, nv, _ = prj_shape
+    return (B, C, nx, ny, nz, g.dx, g.dy, g.dz, g.cx, g.cy, g.cz, nu, nview, nv, g.du, g.dv, g.off_u, g.off_v)
+
+
+def tomo_fp(img, det_center, src, g, nu, nv):
+    """DistanceDrivenTomo::ProjectionTomo (DistanceDriven3D.cu:139-343)."""
+    img = _f32(img)
+    dc = _f32(det_center)
+    sp = _f32(src)
+    B, nx, ny, nz, C = img.shape
+    out = np.zeros((B, nu, dc.shape[0], nv, C), np.float64)
+    lib().oracle_tomo_fp_f64(_ptr(out, ctypes.c_double), _ptr(img, _f), _ptr(dc, _f), _ptr(sp, _f),
+                             *_tomo_args(g, img.shape, out.shape))
+    return out
+
+
+def tomo_bp(prj, det_center, src, g, img_shape):
+    """DistanceDrivenTomo::BackprojectionTomo (DistanceDriven3D.cu:409-663)."""
+    prj = _f32(prj)
+    dc = _f32(det_center)
+    sp = _f32(src)
+    B, nu, nview, nv, C = prj.shape
+    nx, ny, nz = img_shape
+    out = np.zeros((B, nx, ny, nz, C), np.float64)
+    lib().oracle_tomo_bp_f64(_ptr(out, ctypes.c_double), _ptr(prj, _f), _ptr(dc, _f), _ptr(sp, _f),
+                             *_tomo_args(g, out.shape, prj.shape))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# OS-SQS composition (ossqs.cu:91-149 arithmetic with the DD projector, a TV
+# term from TotalVariation.cu, explicit subset view lists).
+# ---------------------------------------------------------------------------
+def sqs_subset_update(x, sino, wsino, norm_img, angles, views, g, n_subsets, lam=1.0, beta=0.0,
+                      lb=-np.inf, ub=np.inf, bp_type=2):
+    """One ordered-subset SQS step on a [nx, ny] slice (2D, B = C = 1).
+
+    x_new = clamp(x - lam * (M * A_s^T W_s (A_s x - b_s) + beta * grad_tv(x))
+                        / (norm_img + beta * norm_tv(x) + 1e-6), lb, ub)
+    ``sino``/``wsino`` are [nu, nview]; ``views`` lists the subset's view indices.
+    """
+    x = np.asarray(x, np.float32)
+    nx, ny = x.shape
+    nu = sino.shape[0]
+    views = np.asarray(views)
+    ang = np.asarray(angles, np.float32)[views]
+    fp = fan_fp(x[None, :, :, None, None], ang, g, nu, 1)[0, :, :, 0, 0]
+    r = (fp - sino[:, views].astype(np.float64)) * wsino[:, views].astype(np.float64)
+    bp = fan_bp(r.astype(np.float32)[None, :, :, None, None], ang, g, (nx, ny, 1), bp_type)[0, :, :, 0, 0]
+    num = n_subsets * bp
+    den = np.asarray(norm_img, np.float64) + 1e-6
+    if beta > 0:
+        grad, norm, _ = tv_sqs(x)
+        num = num + beta * grad
+        den = den + beta * norm
+    xn = x.astype(np.float64) - lam * num / den
+    return np.clip(xn, lb, ub)

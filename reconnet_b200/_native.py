@@ -1,0 +1,111 @@
+"""ctypes binding of ``libreconnet_b200.so`` (the C ABI in include/reconnet_b200.h).
+
+The library is loaded from ``reconnet_b200/_lib``; if it is missing this
+module raises at import time -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libreconnet_b200.so")
+
+RN_OK = 0
+RN_ERR_ARG = 1
+RN_ERR_CUDA = 2
+RN_ERR_ALLOC = 3
+RN_ERR_TIMEOUT = 4
+RN_TYPE_ITERATIVE = 0
+RN_TYPE_FBP = 1
+RN_TYPE_MATCHED = 2
+
+_f = ctypes.c_float
+_i = ctypes.c_int
+_fp = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+
+class RnFanGeom(ctypes.Structure):
+    """Mirror of ``RnFanGeom`` (fields of Projector, ReconNet4D/Projector.h:10-37)."""
+    _fields_ = [("nBatches", _i), ("nChannels", _i), ("nx", _i), ("ny", _i), ("nz", _i),
+                ("dx", _f), ("dy", _f), ("dz", _f), ("cx", _f), ("cy", _f), ("cz", _f),
+                ("nu", _i), ("nview", _i), ("nv", _i),
+                ("du", _f), ("dv", _f), ("off_u", _f), ("off_v", _f), ("dsd", _f), ("dso", _f)]
+
+
+class ReconNetError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"reconnet_b200 error {code}: {msg}")
+        self.code = code
+
+
+_FAN = [_i, _i, _i, _i, _i, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i]
+_TOMO = [_i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f]
+_FILT = [_i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i]
+
+# name -> (restype, argtypes); every entry point of include/reconnet_b200.h
+SIGNATURES = {
+    "rn_last_error": (ctypes.c_char_p, []),
+    "rn_last_status": (_i, []),
+    "rn_version": (_i, []),
+    "SetDevice": (_i, [_i]),
+    "cDistanceDrivenFanProjection": (None, [_fp, _fp, _fp] + _FAN),
+    "cDistanceDrivenFanBackprojection": (None, [_fp, _fp, _fp] + _FAN),
+    "cDistanceDrivenTomoProjection": (None, [_fp, _fp, _fp, _fp] + _TOMO),
+    "cDistanceDrivenTomoBackprojection": (None, [_fp, _fp, _fp, _fp] + _TOMO),
+    "cFilterFanFilter": (None, [_fp, _fp] + _FILT),
+    "cFilterParallelFilter": (None, [_fp, _fp] + _FILT),
+    "cOSSQS": (None, [_fp, _fp, _fp, _fp, _fp, _fp, _f, _f, _i, _i] + _FAN[:-1] + [_i, _f]),
+    "cTVSQS2D": (_f, [_fp, _fp, _fp, _i, _i]),
+    "rn_fan_plan_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnFanGeom), _fp, _vp]),
+    "rn_fan_plan_create_ragged": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnFanGeom),
+                                       ctypes.POINTER(_i), _fp, _vp]),
+    "rn_fan_plan_destroy": (_i, [_vp]),
+    "rn_fan_plan_total_views": (ctypes.c_int64, [_vp]),
+    "rn_fan_project": (_i, [_vp, _vp, _vp, _vp]),
+    "rn_fan_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
+    "rn_fan_plan_check": (_i, [_vp, _vp]),
+    "rn_fan_plan_set_timing": (_i, [_vp, _i]),
+    "rn_fan_plan_read_timing": (_i, [_vp, _fp, ctypes.POINTER(_i), _i, ctypes.POINTER(ctypes.c_longlong)]),
+    "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
+    "rn_tv_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
+    "rn_fan_sqs_update": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _f, _f, _i, _vp]),
+    "rn_tomo_sat_bytes": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_size_t),
+                               ctypes.POINTER(ctypes.c_size_t)]),
+    "rn_tomo_project": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),
+    "rn_tomo_backproject": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"reconnet_b200 native library not built ({LIB_PATH}); run `python -m reconnet_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    s = lib.rn_last_error()
+    return s.decode() if s else ""
+
+
+def check(status: int) -> None:
+    """Raise ReconNetError if a native call returned a non-zero status."""
+    if status != RN_OK:
+        raise ReconNetError(status, last_error())
+
+
+def check_last() -> None:
+    """Raise if the most recent reference-named (void) call failed."""
+    st = lib.rn_last_status()
+    if st != RN_OK:
+        raise ReconNetError(st, last_error())

@@ -1,0 +1,845 @@
+// Distance-driven fan-beam projector pair for sm_100a.
+//
+// Forward projection (restates DDFPFanKernelX/Y, ReconNet4D/DistanceDriven.cu:64-196):
+//   prj(u, view) = L_u * sum_lines [P_l(x_{u+1}(l)) - P_l(x_u(l))] / (x_{u+1}(l) - x_u(l))
+// where l runs over the image rows (X-class views) or columns (Y-class),
+// x_e(l) is where the ray through detector-cell edge e crosses line l, and
+// P_l is the exact integral of the line's pixel values from 0 to x.  The
+// reference samples its prefix texture at row *boundaries* with a 50/50
+// blend of the two neighbouring rows (tex3D at integer y, border mode); the
+// line arrays built here are exactly those blended rows.
+//
+// Design:
+//   * line prologue: one warp per line, FP64 prefix split into hi/lo floats
+//     (so prefix differences keep full precision), written once per call;
+//   * FP kernel: one CTA per (slice, view class, 4 views); lines are staged
+//     into shared memory in chunks with bulk async copies (cp.async.bulk +
+//     mbarrier, double buffered); each thread integrates whole rays across
+//     the staged lines; per-ray accumulators live in shared memory;
+//   * BP: edge tables (FP64 prefix of the weighted sinogram, hi/lo) built per
+//     call, then a gather-form kernel (no atomics): each thread owns a 4x4
+//     pixel block and accumulates all views in registers; per-view table
+//     windows are staged with bulk async copies.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "rn_device.cuh"
+#include "rn_internal.h"
+
+namespace rn {
+
+// ---------------------------------------------------------------------------
+// Tunables.
+// ---------------------------------------------------------------------------
+constexpr int kFpThreads = 512;
+constexpr int kFpViews = 4;          // views per FP CTA
+constexpr int kFpMaxLines = 16;      // lines per staged chunk (upper bound)
+constexpr int kSmemBudget = 227 * 1024;
+
+constexpr int kBpThreads = 256;      // 16 x 16 threads
+constexpr int kBpTile = 64;          // pixels per CTA side (4 x 4 per thread)
+constexpr int kBpViews = 8;          // views per staged chunk
+
+__host__ __device__ inline long long align4(long long v) { return (v + 3) & ~3ll; }
+
+// ---------------------------------------------------------------------------
+// Geometry: per-edge slopes r_e (FP64).  X-class: r = tan(gamma_e - theta)*dy/dx
+// (= (D.x - S.x)/(D.y - S.y) in image units, DistanceDriven.cu:89-113);
+// Y-class: r = cot(gamma_e - theta)*dx/dy.
+// ---------------------------------------------------------------------------
+__global__ void edge_slope_kernel(double* edges, const double2* view_cs, const int* view_x, const double2* edge_sc,
+                                  int total_views, int nu, double dx, double dy) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long n = (long long)total_views * (nu + 1);
+    if (i >= n) return;
+    int v = (int)(i / (nu + 1));
+    int e = (int)(i - (long long)v * (nu + 1));
+    double2 cs = view_cs[v];     // (cos theta, sin theta)
+    double2 sc = edge_sc[e];     // (sin gamma, cos gamma)
+    double sn = sc.x * cs.x - sc.y * cs.y;   // sin(gamma - theta)
+    double cn = sc.y * cs.x + sc.x * cs.y;   // cos(gamma - theta)
+    edges[i] = view_x[v] ? (sn * dy) / (cn * dx) : (cn * dx) / (sn * dy);
+}
+
+// ---------------------------------------------------------------------------
+// Line prologue: for each FP slice, X lines (image rows, boundary l between
+// rows l-1 and l) and Y lines (columns).  Entry k of a line holds the prefix
+// P[k] = sum_{i<k} a_i as (hi, lo) and the value a_k (a_n = 0).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_incl_scan(double v) {
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double t = __shfl_up_sync(full, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
+                                 FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int per_slice = d.ny + d.nx;
+    if (warp >= ns * per_slice) return;
+    int si = warp / per_slice;
+    int li = warp - si * per_slice;
+    const FpSlice fs = fps[s_begin + si];
+    bool xl = li < d.ny;
+    int l = xl ? li : li - d.ny;
+    int n = xl ? d.nx : d.ny;
+    int lp = xl ? d.lpx : d.lpy;
+    long long base = (long long)si * slot_elems + (xl ? (long long)l * d.lpx : (long long)d.ny * d.lpx + (long long)l * d.lpy);
+    float2* ohl = hl + base;
+    float* ola = la + base;
+    double carry = 0.0;
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        int k = k0 + lane;
+        double a = 0.0;
+        if (k < n) {
+            // blended value of rows (l-1, l) [X] or columns (l-1, l) [Y] at position k
+            float s = 0.f;
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                float w = fs.img_w[j];
+                if (w == 0.f) continue;
+                const float* p = img + fs.img_off[j];
+                float v1, v0 = 0.f;
+                if (xl) {
+                    v1 = __ldg(p + (long long)k * d.isx + (long long)l * d.isy);
+                    if (l > 0) v0 = __ldg(p + (long long)k * d.isx + (long long)(l - 1) * d.isy);
+                } else {
+                    v1 = __ldg(p + (long long)l * d.isx + (long long)k * d.isy);
+                    if (l > 0) v0 = __ldg(p + (long long)(l - 1) * d.isx + (long long)k * d.isy);
+                }
+                s += w * (0.5f * v0 + 0.5f * v1);
+            }
+            a = (double)s;
+        }
+        double incl = warp_incl_scan(a);
+        double excl = carry + incl - a;
+        if (k < n) {
+            ohl[k] = split_double(excl);
+            ola[k] = (float)a;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    // entry n and padding up to lp: P = total, a = 0
+    for (int k = n + lane; k < lp; k += 32) {
+        ohl[k] = split_double(carry);
+        ola[k] = 0.f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP kernel.
+// ---------------------------------------------------------------------------
+struct FpParams {
+    const ViewGeo* views;
+    const double* edges;
+    const float2* cell;
+    const int* perm;
+    const GeoSet* sets;
+    const FpSlice* fps;
+    const int4* work;
+    const float2* hl;
+    const float* la;
+    long long slot_elems;
+    int slot_base;     // first FP slice of the current wave
+    float* prj;
+    int* err;
+    FanDims d;
+    int R;             // lines per chunk
+};
+
+__global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int4 w = p.work[blockIdx.x];
+    const int s = w.x, xcls = w.y, vbegin = w.z, vcount = w.w;
+    const FpSlice fs = p.fps[s];
+    const GeoSet gs = p.sets[fs.set];
+    const int nu = p.d.nu;
+    const int nlines = xcls ? p.d.ny : p.d.nx;
+    const int n = xcls ? p.d.nx : p.d.ny;
+    const int lp = xcls ? p.d.lpx : p.d.lpy;
+    const int R = p.R;
+    const long long slot = (long long)(s - p.slot_base) * p.slot_elems + (xcls ? 0ll : (long long)p.d.ny * p.d.lpx);
+    const float2* ghl = p.hl + slot;
+    const float* gla = p.la + slot;
+
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+    int* s_gv = reinterpret_cast<int*>(smem + 16);                  // kFpViews
+    int* s_vl = s_gv + kFpViews;                                    // set-local view index
+    double* s_par = reinterpret_cast<double*>(smem + 64);           // kFpViews
+    double* s_perp = s_par + kFpViews;                              // kFpViews
+    float* s_g = reinterpret_cast<float*>(smem + 128);              // kFpViews * kFpMaxLines
+    float* s_acc = s_g + kFpViews * kFpMaxLines;                    // kFpViews * nu
+    size_t off = 128 + sizeof(float) * (kFpViews * kFpMaxLines + align4((long long)kFpViews * nu));
+    off = (off + 127) & ~size_t(127);
+    float2* bhl[2];
+    float* bla[2];
+    const size_t hl_bytes = (size_t)R * lp * sizeof(float2);
+    const size_t la_bytes = (size_t)R * lp * sizeof(float);
+    bhl[0] = reinterpret_cast<float2*>(smem + off);
+    bla[0] = reinterpret_cast<float*>(smem + off + hl_bytes);
+    bhl[1] = reinterpret_cast<float2*>(smem + off + hl_bytes + la_bytes);
+    bla[1] = reinterpret_cast<float*>(smem + off + 2 * hl_bytes + la_bytes);
+
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    if (tid < vcount) {
+        int vl = p.perm[gs.view_off + vbegin + tid];
+        int gv = gs.view_off + vl;
+        s_vl[tid] = vl;
+        s_gv[tid] = gv;
+        s_par[tid] = p.views[gv].par;
+        s_perp[tid] = p.views[gv].perp;
+    }
+    const int nrays = vcount * nu;
+    for (int i = tid; i < nrays; i += kFpThreads) s_acc[i] = 0.f;
+    __syncthreads();
+
+    const int nchunks = (nlines + R - 1) / R;
+    auto issue = [&](int c) {
+        int b = c & 1;
+        int l0 = c * R;
+        int rc = min(R, nlines - l0);
+        uint32_t bh = (uint32_t)((size_t)rc * lp * sizeof(float2));
+        uint32_t ba = (uint32_t)((size_t)rc * lp * sizeof(float));
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&bars[b], bh + ba);
+        bulk_g2s(bhl[b], ghl + (long long)l0 * lp, bh, &bars[b]);
+        bulk_g2s(bla[b], gla + (long long)l0 * lp, ba, &bars[b]);
+    };
+    if (tid == 0) issue(0);
+
+    const float fn = (float)n;
+    bool ok = true;
+    for (int c = 0; c < nchunks; c++) {
+        const int b = c & 1;
+        const int l0 = c * R;
+        const int rc = min(R, nlines - l0);
+        if (tid == 0 && c + 1 < nchunks) issue(c + 1);
+        // per-view 1/(line - perp) for this chunk
+        if (tid < vcount * R) {
+            int v = tid / R, j = tid - (tid / R) * R;
+            s_g[v * kFpMaxLines + j] = (float)(1.0 / ((double)(l0 + j) - s_perp[v]));
+        }
+        if (!mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1))) {
+            ok = false;
+        }
+        __syncthreads();
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
+            break;
+        }
+        const float2* HL = bhl[b];
+        const float* LA = bla[b];
+        for (int ray = tid; ray < nrays; ray += kFpThreads) {
+            const int v = ray / nu;
+            const int u = ray - v * nu;
+            const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
+            const double ra = ed[u], rb = ed[u + 1];
+            const double t0 = (double)l0 - s_perp[v];
+            const double par = s_par[v];
+            const float Xa = (float)(par + ra * t0), Xb = (float)(par + rb * t0);
+            const float fra = (float)ra, frb = (float)rb;
+            const float* g = s_g + v * kFpMaxLines;
+            float acc = 0.f;
+            float jf = 0.f;
+            for (int j = 0; j < rc; j++, jf += 1.f) {
+                float xa = fminf(fmaxf(fmaf(fra, jf, Xa), 0.f), fn);
+                float xb = fminf(fmaxf(fmaf(frb, jf, Xb), 0.f), fn);
+                float fa, fb;
+                int ka = floor_frac(xa, fa);
+                int kb = floor_frac(xb, fb);
+                const float2 ha = HL[j * lp + ka];
+                const float2 hb = HL[j * lp + kb];
+                const float aa = LA[j * lp + ka];
+                const float ab = LA[j * lp + kb];
+                float dP = (hb.x - ha.x) + ((hb.y - ha.y) + (fb * ab - fa * aa));
+                acc = fmaf(dP, g[j], acc);
+            }
+            s_acc[ray] += acc;
+        }
+        __syncthreads();
+    }
+    if (!ok) return;
+
+    // epilogue: scale by L_u / (r_{u+1} - r_u) and store
+    const float lenA = xcls ? p.d.dy : p.d.dx;
+    for (int ray = tid; ray < nrays; ray += kFpThreads) {
+        const int v = ray / nu;
+        const int u = ray - v * nu;
+        const int gv = s_gv[v];
+        const double* ed = p.edges + (long long)gv * (nu + 1);
+        const float dr = (float)(ed[u + 1] - ed[u]);
+        const ViewGeo& vg = p.views[gv];
+        const float2 cs = p.cell[u];   // (cos a, sin a)
+        float L = xcls ? lenA / fabsf(vg.cosd * cs.x + vg.sind * cs.y) : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
+        float val = s_acc[ray] * (L / dr);
+        p.prj[fs.prj_off + (long long)u * fs.su + (long long)s_vl[v] * fs.sview] = val;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BP edge tables.  One warp per (BP slice, view); 8 consecutive views per CTA
+// so that the u-strided sinogram reads of neighbouring views share sectors.
+//   matched (type 2): W_u = prj * L_u; entry e < nu = {Qhi, Qlo, W_e/(r_{e+1}-r_e), r_e}
+//   reference (0/1):  W_u = prj * (L_u if type 0); entry k <= nu = {Uhi, Ulo, W_k, 0}
+// with Q/U the FP64 prefix over u.
+// ---------------------------------------------------------------------------
+__global__ void fan_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin,
+                                 int ns, const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
+                                 const double* __restrict__ edges, const float2* __restrict__ cell, FanDims d,
+                                 int type, float4* __restrict__ tab, long long tab_base) {
+    int warp = threadIdx.x >> 5;
+    int lane = threadIdx.x & 31;
+    int si = blockIdx.y;
+    if (si >= ns) return;
+    const BpSlice bs = bps[s_begin + si];
+    const GeoSet gs = sets[bs.set];
+    int vl = blockIdx.x * 8 + warp;
+    if (vl >= gs.nview) return;
+    int gv = gs.view_off + vl;
+    const ViewGeo vg = views[gv];
+    const int nu = d.nu;
+    const double* ed = edges + (long long)gv * (nu + 1);
+    float4* out = tab + (bs.table_off - tab_base) + (long long)vl * (nu + 1);
+    const float lenA = vg.xcls ? d.dy : d.dx;
+    double carry = 0.0;
+    for (int u0 = 0; u0 < nu; u0 += 32) {
+        int u = u0 + lane;
+        double W = 0.0;
+        if (u < nu) {
+            float s = 0.f;
+#pragma unroll
+            for (int j = 0; j < kBpMix; j++) {
+                float wj = bs.prj_w[j];
+                if (wj == 0.f) continue;
+                s += wj * __ldg(prj + bs.prj_off[j] + (long long)u * bs.su + (long long)vl * bs.sview);
+            }
+            if (type != RN_TYPE_FBP) {
+                float2 cs = cell[u];
+                float L = vg.xcls ? lenA / fabsf(vg.cosd * cs.x + vg.sind * cs.y)
+                                  : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
+                s *= L;
+            }
+            W = (double)s;
+        }
+        double incl = warp_incl_scan(W);
+        double excl = carry + incl - W;
+        if (u < nu) {
+            float2 q = split_double(excl);
+            if (type == RN_TYPE_MATCHED) {
+                double dr = ed[u + 1] - ed[u];
+                out[u] = make_float4(q.x, q.y, (float)(W / dr), (float)ed[u]);
+            } else {
+                out[u] = make_float4(q.x, q.y, (float)W, 0.f);
+            }
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) {
+        float2 q = split_double(carry);
+        out[nu] = make_float4(q.x, q.y, 0.f, type == RN_TYPE_MATCHED ? (float)ed[nu] : 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BP kernels.
+// ---------------------------------------------------------------------------
+struct BpParams {
+    const ViewGeo* views;
+    const GeoSet* sets;
+    const BpSlice* bps;
+    const float4* tab;
+    long long tab_base;
+    int s_begin;
+    float* img;
+    int* err;
+    FanDims d;
+    int accumulate;
+    int type;
+    int tiles_x, tiles_y;
+    int win;           // staged table entries per view
+};
+
+// Edge index t of the matched parametrisation at lattice point
+// (line l, position q): slope r = (q - par) / (l - perp).
+__device__ __forceinline__ float matched_t(const ViewGeo& vg, float r) {
+    return vg.tA + vg.tB * atanf(vg.kappa * r);
+}
+
+// Reference detector coordinate of a physical point (GetProjectionOnDetector,
+// DistanceDriven.cu:479-485, and the mapping at :530-533).
+__device__ __forceinline__ float ref_t(float px, float py, float c, float s, const FanDims& d) {
+    float rx = px * c + py * s;
+    float ry = -px * s + py * c;
+    float a = atanf(rx / (ry + d.dso));
+    return -(a / d.du + d.off_u) + d.nu * 0.5f;
+}
+
+struct BpShared {
+    uint64_t bars[2];
+    int elo[2][kBpViews];
+    int gv[2][kBpViews];
+};
+
+template <bool kMatched>
+__global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    BpShared* sh = reinterpret_cast<BpShared*>(smem);
+    float4* buf[2];
+    size_t off = (sizeof(BpShared) + 127) & ~size_t(127);
+    buf[0] = reinterpret_cast<float4*>(smem + off);
+    buf[1] = buf[0] + kBpViews * p.win;
+
+    const int tiles_per_slice = p.tiles_x * p.tiles_y;
+    const int si = blockIdx.x / tiles_per_slice;
+    const int ti = blockIdx.x - si * tiles_per_slice;
+    const int tyi = ti / p.tiles_x;
+    const int txi = ti - tyi * p.tiles_x;
+    const BpSlice bs = p.bps[p.s_begin + si];
+    const GeoSet gs = p.sets[bs.set];
+    const float4* gtab = p.tab + (bs.table_off - p.tab_base);
+    const int nu = p.d.nu, nx = p.d.nx, ny = p.d.ny;
+    const int tid = threadIdx.x;
+    const int X0 = txi * kBpTile, Y0 = tyi * kBpTile;            // CTA pixel origin
+    const int x0 = X0 + (tid & 15) * 4, y0 = Y0 + (tid >> 4) * 4; // thread pixel origin
+    const int tabn = nu + 1;
+
+    if (tid == 0) {
+        mbar_init(&sh->bars[0], 1);
+        mbar_init(&sh->bars[1], 1);
+        fence_mbar_init();
+    }
+
+    // window of table entries touched by the CTA tile for view vl
+    auto window = [&](int vl) -> int {
+        const ViewGeo vg = p.views[gs.view_off + vl];
+        float tmin = 1e30f, tmax = -1e30f;
+#pragma unroll
+        for (int cx = 0; cx < 2; cx++)
+#pragma unroll
+            for (int cy = 0; cy < 2; cy++) {
+                float t;
+                if (kMatched) {
+                    float X = (float)(X0 + cx * kBpTile), Y = (float)(Y0 + cy * kBpTile);
+                    float l = vg.xcls ? Y : X, q = vg.xcls ? X : Y;
+                    float r = (q - (float)vg.par) / (l - (float)vg.perp);
+                    t = matched_t(vg, r);
+                } else {
+                    float px = ((float)(X0 + cx * kBpTile) - 0.5f - (nx - 1) * 0.5f) * p.d.dx;
+                    float py = ((float)(Y0 + cy * kBpTile) - 0.5f - (ny - 1) * 0.5f) * p.d.dy;
+                    t = ref_t(px, py, vg.cosd, vg.sind, p.d);
+                }
+                tmin = fminf(tmin, t);
+                tmax = fmaxf(tmax, t);
+            }
+        int lo = (int)floorf(tmin) - 2;
+        lo = max(0, min(lo, tabn - p.win));
+        return lo;
+    };
+
+    const int nchunks = (gs.nview + kBpViews - 1) / kBpViews;
+    auto prep = [&](int c) {   // threads < kBpViews compute windows for chunk c
+        if (tid < kBpViews) {
+            int vl = c * kBpViews + tid;
+            int b = c & 1;
+            if (vl < gs.nview) {
+                sh->elo[b][tid] = window(vl);
+                sh->gv[b][tid] = gs.view_off + vl;
+            }
+        }
+    };
+    auto issue = [&](int c) {
+        int b = c & 1;
+        int vc = min(kBpViews, gs.nview - c * kBpViews);
+        uint32_t total = 0;
+        int cnt = min(p.win, tabn);
+        total = (uint32_t)(vc * cnt * sizeof(float4));
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&sh->bars[b], total);
+        for (int v = 0; v < vc; v++) {
+            int vl = c * kBpViews + v;
+            bulk_g2s(buf[b] + v * p.win, gtab + (long long)vl * tabn + sh->elo[b][v],
+                     (uint32_t)(cnt * sizeof(float4)), &sh->bars[b]);
+        }
+    };
+
+    prep(0);
+    __syncthreads();
+    if (tid == 0) issue(0);
+
+    float acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+
+    bool ok = true;
+    for (int c = 0; c < nchunks; c++) {
+        const int b = c & 1;
+        if (c + 1 < nchunks) prep(c + 1);
+        __syncthreads();
+        if (tid == 0 && c + 1 < nchunks) issue(c + 1);
+        if (!mbar_wait(&sh->bars[b], (uint32_t)((c >> 1) & 1))) ok = false;
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
+            ok = false;
+            break;
+        }
+        const int vc = min(kBpViews, gs.nview - c * kBpViews);
+        for (int v = 0; v < vc; v++) {
+            const ViewGeo vg = p.views[sh->gv[b][v]];
+            const float4* T = buf[b] + v * p.win;
+            const int elo = sh->elo[b][v];
+            const int cnt = min(p.win, tabn);
+            if (kMatched) {
+                // lattice lines: rows (X) or columns (Y); positions along them
+                const int L0 = vg.xcls ? y0 : x0;
+                const int Q0 = vg.xcls ? x0 : y0;
+                const int nl = vg.xcls ? ny : nx;
+                const float par = (float)vg.par, perp = (float)vg.perp;
+                const int emax = min(nu - 1, elo + cnt - 1);
+                float dprev[4];
+#pragma unroll
+                for (int li = 0; li < 5; li++) {
+                    const int l = L0 + li;
+                    const float g = 1.0f / ((float)l - perp);
+                    float fh[5], fl[5];
+#pragma unroll
+                    for (int qi = 0; qi < 5; qi++) {
+                        float r = ((float)(Q0 + qi) - par) * g;
+                        float t = matched_t(vg, r);
+                        int e = (int)floorf(t);
+                        e = min(max(e, elo), emax);
+                        float rc = fminf(fmaxf(r, vg.rmin), vg.rmax);
+                        float4 E = T[e - elo];
+                        fh[qi] = E.x;
+                        fl[qi] = fmaf(E.z, rc - E.w, E.y);
+                    }
+                    float dcur[4];
+#pragma unroll
+                    for (int qi = 0; qi < 4; qi++) dcur[qi] = (fh[qi + 1] - fh[qi]) + (fl[qi + 1] - fl[qi]);
+                    if (li > 0) {
+                        const float m = (l < nl) ? 1.f : 0.f;   // line l exists?
+#pragma unroll
+                        for (int qi = 0; qi < 4; qi++) {
+                            float v2 = vg.sigma * 0.5f * (dprev[qi] + m * dcur[qi]);
+                            if (vg.xcls) acc[qi][li - 1] += v2;
+                            else acc[li - 1][qi] += v2;
+                        }
+                    }
+#pragma unroll
+                    for (int qi = 0; qi < 4; qi++) dprev[qi] = dcur[qi];
+                }
+            } else {
+                // reference DDBPFanKernelX/Y: pixel edges at the pixel centre line
+                const float cs = vg.cosd, sn = vg.sind;
+                const int kmax = min(nu, elo + cnt - 1);
+#pragma unroll
+                for (int li = 0; li < 4; li++) {
+                    float tq[5], uh[5], ul[5];
+#pragma unroll
+                    for (int qi = 0; qi < 5; qi++) {
+                        float px, py;
+                        if (vg.xcls) {
+                            px = ((float)(x0 + qi) - 0.5f - (nx - 1) * 0.5f) * p.d.dx;
+                            py = ((float)(y0 + li) - (ny - 1) * 0.5f) * p.d.dy;
+                        } else {
+                            px = ((float)(x0 + li) - (nx - 1) * 0.5f) * p.d.dx;
+                            py = ((float)(y0 + qi) - 0.5f - (ny - 1) * 0.5f) * p.d.dy;
+                        }
+                        float t = ref_t(px, py, cs, sn, p.d);
+                        float tc = fminf(fmaxf(t, 0.f), (float)nu);
+                        float fr;
+                        int k = floor_frac(tc, fr);
+                        k = min(max(k, elo), kmax);
+                        fr = tc - (float)k;
+                        float4 E = T[k - elo];
+                        tq[qi] = t;
+                        uh[qi] = E.x;
+                        ul[qi] = fmaf(fr, E.z, E.y);
+                    }
+#pragma unroll
+                    for (int qi = 0; qi < 4; qi++) {
+                        float dU = (uh[qi + 1] - uh[qi]) + (ul[qi + 1] - ul[qi]);
+                        float val = dU / (tq[qi + 1] - tq[qi]);
+                        int ax = vg.xcls ? qi : li, ay = vg.xcls ? li : qi;
+                        if (p.type == RN_TYPE_FBP) {
+                            float px = ((float)(x0 + ax) - (nx - 1) * 0.5f) * p.d.dx;
+                            float py = ((float)(y0 + ay) - (ny - 1) * 0.5f) * p.d.dy;
+                            float rx = px * cs + py * sn;
+                            float ry = -px * sn + py * cs;
+                            float dd = p.d.dso + ry;
+                            val *= p.d.dso * p.d.dso / (rx * rx + dd * dd);
+                        }
+                        if (vg.xcls) acc[qi][li] += val;
+                        else acc[li][qi] += val;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok) return;
+
+    float* out = p.img + bs.img_off;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) {
+            int ix = x0 + a, iy = y0 + bb;
+            if (ix < nx && iy < ny) {
+                float* q = out + (long long)ix * p.d.isx + (long long)iy * p.d.isy;
+                *q = p.accumulate ? (*q + acc[a][bb]) : acc[a][bb];
+            }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+static size_t fp_smem_bytes(int nu, int lp, int R) {
+    size_t off = 128 + sizeof(float) * (kFpViews * kFpMaxLines + align4((long long)kFpViews * nu));
+    off = (off + 127) & ~size_t(127);
+    return off + 2 * (size_t)R * lp * (sizeof(float2) + sizeof(float));
+}
+
+static size_t bp_smem_bytes(int win) {
+    return ((sizeof(BpShared) + 127) & ~size_t(127)) + 2 * (size_t)kBpViews * win * sizeof(float4);
+}
+
+int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
+    const RnFanGeom& g = p->g;
+    const int nu = g.nu;
+    const int64_t V = p->total_views;
+    const double du = g.du, off_u = g.off_u;
+
+    // per-edge (sin, cos) of the fan angle gamma_e; edge e sits at
+    // a_e + du/2 of cell e (DistanceDriven.cu:83,90)
+    std::vector<double2> esc(nu + 1);
+    for (int e = 0; e <= nu; e++) {
+        double gam = (-((double)e - 0.5 - (nu - 1) / 2.0) - off_u) * du;
+        esc[e] = make_double2(std::sin(gam), std::cos(gam));
+    }
+    std::vector<float2> cell(nu);
+    for (int u = 0; u < nu; u++) {
+        double a = (-((double)u - (nu - 1) / 2.0) - off_u) * du;
+        cell[u] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+
+    std::vector<ViewGeo> vg(V);
+    std::vector<double2> vcs(V);
+    std::vector<int> vx(V);
+    std::vector<int> perm(V);
+    auto slope = [&](int xc, double c, double s, int e) {
+        double sn = esc[e].x * c - esc[e].y * s;
+        double cn = esc[e].y * c + esc[e].x * s;
+        return xc ? (sn * g.dy) / (cn * g.dx) : (cn * g.dx) / (sn * g.dy);
+    };
+    for (size_t si = 0; si < p->h_sets.size(); si++) {
+        GeoSet& gs = p->h_sets[si];
+        int nxv = 0;
+        for (int k = 0; k < gs.nview; k++) {
+            int v = gs.view_off + k;
+            double th = (double)host_deg[v];
+            double c = std::cos(th), s = std::sin(th);
+            int xc = std::fabs(c) > std::fabs(s) ? 1 : 0;
+            double sx = (g.dso * s - g.cx) / g.dx + g.nx / 2.0;
+            double sy = (-g.dso * c - g.cy) / g.dy + g.ny / 2.0;
+            ViewGeo& q = vg[v];
+            q.xcls = xc;
+            q.par = xc ? sx : sy;
+            q.perp = xc ? sy : sx;
+            q.cosd = (float)c;
+            q.sind = (float)s;
+            double kap = xc ? g.dx / g.dy : g.dy / g.dx;
+            q.kappa = (float)kap;
+            double tB = xc ? -1.0 / du : 1.0 / du;
+            int em = nu / 2;
+            double rm = slope(xc, c, s, em);
+            q.tB = (float)tB;
+            q.tA = (float)((double)em - tB * std::atan(kap * rm));
+            double r0 = slope(xc, c, s, 0), r1 = slope(xc, c, s, nu);
+            q.rmin = (float)std::min(r0, r1);
+            q.rmax = (float)std::max(r0, r1);
+            int nl = xc ? g.ny : g.nx;
+            double side = (nl / 2.0 - q.perp) > 0 ? 1.0 : -1.0;
+            q.sigma = (float)((r1 > r0 ? 1.0 : -1.0) * side);
+            q.pad = 0;
+            vcs[v] = make_double2(c, s);
+            vx[v] = xc;
+            if (xc) nxv++;
+            // the source must lie outside the image across the lines
+            if (std::fabs(q.perp - nl / 2.0) <= nl / 2.0 + 1.0)
+                return set_error(RN_ERR_ARG, "fan geometry: source inside the image footprint");
+        }
+        gs.nxv = nxv;
+        int a = 0, b = nxv;
+        for (int k = 0; k < gs.nview; k++) {
+            int v = gs.view_off + k;
+            if (vx[v]) perm[gs.view_off + a++] = k;
+            else perm[gs.view_off + b++] = k;
+        }
+    }
+    if (std::fabs(nu * du / 2.0) >= M_PI / 4)
+        return set_error(RN_ERR_ARG, "fan geometry: fan half-angle must be below 45 degrees");
+
+    RN_CUDA_TRY(cudaMalloc(&p->d_views, sizeof(ViewGeo) * V));
+    RN_CUDA_TRY(cudaMalloc(&p->d_edges, sizeof(double) * V * (nu + 1)));
+    RN_CUDA_TRY(cudaMalloc(&p->d_cell, sizeof(float2) * nu));
+    RN_CUDA_TRY(cudaMalloc(&p->d_perm, sizeof(int) * V));
+    RN_CUDA_TRY(cudaMalloc(&p->d_sets, sizeof(GeoSet) * p->h_sets.size()));
+    double2* d_vcs = nullptr;
+    int* d_vx = nullptr;
+    double2* d_esc = nullptr;
+    RN_CUDA_TRY(cudaMalloc(&d_vcs, sizeof(double2) * V));
+    RN_CUDA_TRY(cudaMalloc(&d_vx, sizeof(int) * V));
+    RN_CUDA_TRY(cudaMalloc(&d_esc, sizeof(double2) * (nu + 1)));
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_views, vg.data(), sizeof(ViewGeo) * V, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_cell, cell.data(), sizeof(float2) * nu, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_perm, perm.data(), sizeof(int) * V, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_sets, p->h_sets.data(), sizeof(GeoSet) * p->h_sets.size(),
+                                cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(d_vcs, vcs.data(), sizeof(double2) * V, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(d_vx, vx.data(), sizeof(int) * V, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(d_esc, esc.data(), sizeof(double2) * (nu + 1), cudaMemcpyHostToDevice, st));
+    long long n = (long long)V * (nu + 1);
+    edge_slope_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p->d_edges, d_vcs, d_vx, d_esc, (int)V, nu, g.dx,
+                                                                     g.dy);
+    RN_CUDA_TRY(cudaGetLastError());
+    RN_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(d_vcs);
+    cudaFree(d_vx);
+    cudaFree(d_esc);
+    p->h_sets.shrink_to_fit();
+    return RN_OK;
+}
+
+static int fp_lines_for_smem(int nu, int lp) {
+    int R = kFpMaxLines;
+    while (R > 1 && fp_smem_bytes(nu, lp, R) > (size_t)kSmemBudget) R--;
+    return R;
+}
+
+int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st) {
+    const FanDims& d = p->dims;
+    const int nfp = (int)p->h_fp.size();
+    const int R = std::min(fp_lines_for_smem(d.nu, d.lpx), fp_lines_for_smem(d.nu, d.lpy));
+    if (fp_smem_bytes(d.nu, std::max(d.lpx, d.lpy), R) > (size_t)kSmemBudget)
+        return set_error(RN_ERR_ARG, "fan projection: image lines too long for shared memory");
+    const size_t smem = fp_smem_bytes(d.nu, std::max(d.lpx, d.lpy), R);
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // slices are processed in waves of at most `slots` line buffers
+    const long long slot = p->line_slot_elems;
+    const int slots = (int)std::max<long long>(1, std::min<long long>(nfp, p->fp_slots));
+    int wbeg = 0;
+    for (int s0 = 0; s0 < nfp; s0 += slots) {
+        int ns = std::min(slots, nfp - s0);
+        long long warps = (long long)ns * (d.nx + d.ny);
+        {
+            LaunchScope ls0(p, st, 0);
+            fan_lines_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(d_img, p->d_fp, s0, ns, d,
+                                                                                    p->d_hl, p->d_la, slot);
+        }
+        RN_CUDA_TRY(cudaGetLastError());
+        int wend = wbeg;
+        while (wend < p->n_fp_work && p->h_fp_work[4 * wend] < s0 + ns) wend++;
+        if (wend > wbeg) {
+            FpParams fp;
+            fp.views = p->d_views;
+            fp.edges = p->d_edges;
+            fp.cell = p->d_cell;
+            fp.perm = p->d_perm;
+            fp.sets = p->d_sets;
+            fp.fps = p->d_fp;
+            fp.work = p->d_fp_work + wbeg;
+            fp.hl = p->d_hl;
+            fp.la = p->d_la;
+            fp.slot_elems = slot;
+            fp.slot_base = s0;
+            fp.prj = d_prj;
+            fp.err = p->d_err;
+            fp.d = d;
+            fp.R = R;
+            LaunchScope ls1(p, st, 1);
+            fan_fp_kernel<<<wend - wbeg, kFpThreads, smem, st>>>(fp);
+            RN_CUDA_TRY(cudaGetLastError());
+        }
+        wbeg = wend;
+    }
+    return RN_OK;
+}
+
+int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st) {
+    const FanDims& d = p->dims;
+    const std::vector<BpSlice>& bps = (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
+    const BpSlice* dbp = (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
+    const int nbp = (int)bps.size();
+    const size_t smem = bp_smem_bytes(p->table_win);
+    if (type == RN_TYPE_MATCHED)
+        RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+        RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int tiles_x = (d.nx + kBpTile - 1) / kBpTile, tiles_y = (d.ny + kBpTile - 1) / kBpTile;
+    int s0 = 0;
+    while (s0 < nbp) {
+        // as many slices as fit in the table scratch
+        int s1 = s0;
+        long long base = bps[s0].table_off;
+        while (s1 < nbp) {
+            const GeoSet& gs = p->h_sets[bps[s1].set];
+            long long end = bps[s1].table_off + (long long)gs.nview * (d.nu + 1);
+            if (end - base > p->tab_elems && s1 > s0) break;
+            s1++;
+        }
+        int ns = s1 - s0;
+        int maxv = 0;
+        for (int s = s0; s < s1; s++) maxv = std::max(maxv, p->h_sets[bps[s].set].nview);
+        dim3 tg((maxv + 7) / 8, ns);
+        {
+            LaunchScope ls2(p, st, 2);
+            fan_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_edges, p->d_cell, d,
+                                             type, p->d_tab, base);
+        }
+        RN_CUDA_TRY(cudaGetLastError());
+        BpParams bp;
+        bp.views = p->d_views;
+        bp.sets = p->d_sets;
+        bp.bps = dbp;
+        bp.tab = p->d_tab;
+        bp.tab_base = base;
+        bp.s_begin = s0;
+        bp.img = d_img;
+        bp.err = p->d_err;
+        bp.d = d;
+        bp.accumulate = accumulate;
+        bp.type = type;
+        bp.tiles_x = tiles_x;
+        bp.tiles_y = tiles_y;
+        bp.win = p->table_win;
+        unsigned grid = (unsigned)(ns * tiles_x * tiles_y);
+        LaunchScope ls3(p, st, 3);
+        if (type == RN_TYPE_MATCHED) fan_bp_kernel<true><<<grid, kBpThreads, smem, st>>>(bp);
+        else fan_bp_kernel<false><<<grid, kBpThreads, smem, st>>>(bp);
+        RN_CUDA_TRY(cudaGetLastError());
+        s0 = s1;
+    }
+    return RN_OK;
+}
+
+}  // namespace rn

@@ -1,0 +1,619 @@
+// Ramp filter, TV surrogate, OS-SQS update and the reference-named host
+// entry points (synchronous, host pointers).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "rn_internal.h"
+
+namespace rn {
+
+// PI as the reference defines it (ReconNet4D/Projector.h:5); the filter
+// constants below use it so the ramp matches the reference's definition.
+static const double kRefPi = 3.141592657;
+
+// ---------------------------------------------------------------------------
+// Ramp filter kernel h[0..2nu-2] (offset k = i - (nu-1)): the spatial-domain
+// result of getRamp (Filter.cu:66-214): RL ramp (equiangular sin^2 or
+// equispaced k^2 form), optionally windowed in the DFT domain
+// (Hamming / Hann / cosine), transformed back, real part.
+// ---------------------------------------------------------------------------
+static std::vector<double> ramp_kernel(int nu, double da, int typeFilter, bool equispace) {
+    const int L = 2 * nu - 1;
+    std::vector<std::complex<double>> r(L);
+    for (int i = 0; i < L; i++) {
+        int k = i - (nu - 1);
+        double v = 0;
+        if (k == 0) v = 1.0 / (4 * da * da);
+        else if (k % 2 != 0) {
+            if (equispace) v = -1.0 / (kRefPi * kRefPi * (double)k * k * da * da);
+            else {
+                double s = std::sin(k * da);
+                v = -1.0 / (kRefPi * kRefPi * s * s);
+            }
+        }
+        r[i] = v;
+    }
+    if (typeFilter >= 1 && typeFilter <= 3) {
+        // DFT with a twiddle table (exact index arithmetic mod L)
+        std::vector<std::complex<double>> tw(L);
+        for (int i = 0; i < L; i++) tw[i] = std::polar(1.0, -2.0 * M_PI * i / L);
+        std::vector<std::complex<double>> F(L);
+        for (int k = 0; k < L; k++) {
+            std::complex<double> acc = 0;
+            long long idx = 0;
+            for (int j = 0; j < L; j++) {
+                acc += r[j] * tw[idx];
+                idx += k;
+                if (idx >= L) idx -= L;
+            }
+            F[k] = acc;
+        }
+        for (int i = 0; i < L; i++) {
+            double w;
+            if (typeFilter == 1) w = 0.54 + 0.46 * std::cos(2 * kRefPi * i / (double)(L - 1));
+            else if (typeFilter == 2) w = 0.5 + 0.5 * std::cos(2 * kRefPi * i / (double)(L - 1));
+            else w = std::fabs(std::cos(kRefPi * i / (double)(L - 1)));
+            F[i] *= w;
+        }
+        for (int j = 0; j < L; j++) {
+            std::complex<double> acc = 0;
+            long long idx = 0;
+            for (int k = 0; k < L; k++) {
+                acc += F[k] * std::conj(tw[idx]);
+                idx += j;
+                if (idx >= L) idx -= L;
+            }
+            r[j] = acc / (double)L;
+        }
+    }
+    std::vector<double> h(L);
+    for (int i = 0; i < L; i++) h[i] = r[i].real();
+    return h;
+}
+
+// Device copy of the filter kernel, cached per (device, nu, da, type, geometry).
+struct FilterKey {
+    int dev, nu, type, fan;
+    float da, off_a;
+    bool operator<(const FilterKey& o) const {
+        return std::tie(dev, nu, type, fan, da, off_a) < std::tie(o.dev, o.nu, o.type, o.fan, o.da, o.off_a);
+    }
+};
+struct FilterVal {
+    float* d_h = nullptr;   // [2nu-1]
+    float* d_pw = nullptr;  // [nu] pre-weights
+};
+static std::mutex g_filter_mu;
+static std::map<FilterKey, FilterVal> g_filters;
+
+static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cudaStream_t st, FilterVal& out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    FilterKey key{dev, nu, typeFilter, fan, da, off_a};
+    std::lock_guard<std::mutex> lk(g_filter_mu);
+    auto it = g_filters.find(key);
+    if (it != g_filters.end()) {
+        out = it->second;
+        return RN_OK;
+    }
+    std::vector<double> h = ramp_kernel(nu, da, typeFilter, !fan);
+    std::vector<float> hf(h.begin(), h.end());
+    std::vector<float> pw(nu, 1.f);
+    if (fan)
+        for (int i = 0; i < nu; i++) pw[i] = (float)std::cos(((i - (nu - 1) / 2.0) - off_a) * (double)da);
+    FilterVal v;
+    RN_CUDA_TRY(cudaMalloc(&v.d_h, sizeof(float) * hf.size()));
+    RN_CUDA_TRY(cudaMalloc(&v.d_pw, sizeof(float) * nu));
+    RN_CUDA_TRY(cudaMemcpyAsync(v.d_h, hf.data(), sizeof(float) * hf.size(), cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(v.d_pw, pw.data(), sizeof(float) * nu, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaStreamSynchronize(st));
+    g_filters[key] = v;
+    out = v;
+    return RN_OK;
+}
+
+// Toeplitz product per sinogram plane: out[view][iu] = scale * sum_j
+// (prj[view][j] * pw[j]) * h[nu-1+iu-j].  CTA tile 64 views x 64 outputs,
+// 4x4 per thread, inputs staged 32 at a time in shared memory.
+__global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, const float* __restrict__ prj,
+                                                     const float* __restrict__ h, const float* __restrict__ pw,
+                                                     int nu, int nview, int nv, int nc, float scale) {
+    __shared__ float Xs[32][64 + 4];
+    __shared__ float Hs[96];
+    const int plane = blockIdx.z;
+    const int b = plane / (nv * nc);
+    const int rem = plane - b * nv * nc;
+    const long long off = (long long)b * nu * nview * nv * nc + rem;   // (iv, c) folded: rem = iv*nc + c
+    const long long su = (long long)nview * nv * nc, sview = (long long)nv * nc;
+    const int v0 = blockIdx.x * 64, i0 = blockIdx.y * 64;
+    const int tid = threadIdx.x;
+    const int tv = tid & 15, to = tid >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[a][c] = 0.f;
+    for (int j0 = 0; j0 < nu; j0 += 32) {
+        for (int e = tid; e < 32 * 64; e += 256) {
+            int jj = e >> 6, vv = e & 63;
+            int j = j0 + jj, v = v0 + vv;
+            float x = 0.f;
+            if (j < nu && v < nview) x = prj[off + (long long)j * su + (long long)v * sview] * pw[j];
+            Xs[jj][vv] = x;
+        }
+        if (tid < 96) {
+            int k = nu - 1 + i0 - j0 + tid - 31;
+            Hs[tid] = (k >= 0 && k <= 2 * nu - 2) ? h[k] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int jj = 0; jj < 32; jj++) {
+            float4 xv = *reinterpret_cast<const float4*>(&Xs[jj][tv * 4]);
+            float hv[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) hv[c] = Hs[to * 4 + c - jj + 31];
+            float xa[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[a][c] = fmaf(xa[a], hv[c], acc[a][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            int v = v0 + tv * 4 + a, i = i0 + to * 4 + c;
+            if (v < nview && i < nu) out[off + (long long)i * su + (long long)v * sview] = acc[a][c] * scale;
+        }
+}
+
+int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int nview, int nv, float da,
+                  float off_a, float dsd, float dso, int typeFilter, int fan, cudaStream_t st) {
+    (void)dsd;
+    if (nb <= 0 || nc <= 0 || nu <= 0 || nview <= 0 || nv <= 0 || !(da > 0))
+        return set_error(RN_ERR_ARG, "filter: sizes and pitch must be positive");
+    if (d_out == d_prj) return set_error(RN_ERR_ARG, "filter: output must not alias input");
+    FilterVal fv;
+    RN_TRY(get_filter(nu, da, off_a, typeFilter, fan, st, fv));
+    // scale of cFilterFan::Filter (Filter.cu:294-302) without the FFT length factor
+    double scale = fan ? kRefPi / nview * da / dso : kRefPi / nview * da;
+    dim3 grid((nview + 63) / 64, (nu + 63) / 64, nb * nv * nc);
+    filter_kernel<<<grid, 256, 0, st>>>(d_out, d_prj, fv.d_h, fv.d_pw, nu, nview, nv, nc, (float)scale);
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// TV surrogate (TVSQSKernel, TotalVariation.cu:9-68) on planes of an image
+// with strides (isx, isy); plane p at img + plane_off(p).  FP64 TV sums.
+// ---------------------------------------------------------------------------
+struct TvTerms {
+    float grad, norm, var;
+};
+
+__device__ __forceinline__ TvTerms tv_terms(const float* __restrict__ img, int ix, int iy, int nx, int ny,
+                                            long long isx, long long isy) {
+    const float* p = img + ix * isx + iy * isy;
+    float x = *p;
+    float dx0 = ix == 0 ? x : x - p[-isx];
+    float dx1 = ix == nx - 1 ? x : x - p[isx];
+    float dy0 = iy == 0 ? x : x - p[-isy];
+    float dy1 = iy == ny - 1 ? x : x - p[isy];
+    const float eps = 1e-6f;
+    float t0 = sqrtf(dx0 * dx0 + eps), t1 = sqrtf(dx1 * dx1 + eps);
+    float t2 = sqrtf(dy0 * dy0 + eps), t3 = sqrtf(dy1 * dy1 + eps);
+    TvTerms r;
+    r.grad = (dx0 / t0 + dx1 / t1 + dy0 / t2 + dy1 / t3) / 2;
+    r.norm = 1 / t0 + 1 / t1 + 1 / t2 + 1 / t3;
+    r.var = (t0 + t1 + t2 + t3) / 2;
+    return r;
+}
+
+__global__ void tv_kernel(float* grad, float* norm, double* tv, const float* __restrict__ img, int nx, int ny) {
+    const int s = blockIdx.y;
+    const long long base = (long long)s * nx * ny;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < nx * ny) {
+        int ix = i / ny, iy = i - (i / ny) * ny;
+        TvTerms t = tv_terms(img + base, ix, iy, nx, ny, ny, 1);
+        if (grad) grad[base + i] = t.grad;
+        if (norm) norm[base + i] = t.norm;
+        v = (double)t.var;
+    }
+    if (tv) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        __shared__ double ws[32];
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) ws[w] = v;
+        __syncthreads();
+        if (w == 0) {
+            v = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) atomicAdd(&tv[s], v);
+        }
+    }
+}
+
+// r = (fp - prj) * w   (Minus2D + Multiply2D of ossqs.cu:106-122)
+__global__ void residual_kernel(float* __restrict__ r, const float* __restrict__ prj, const float* __restrict__ w,
+                                long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) r[i] = (r[i] - prj[i]) * w[i];
+}
+
+// x_out = clamp(x_in - lam * (M*bp + beta*grad)/(norm + beta*norm_tv + 1e-6))
+// (Divide2D / Minus2D / ValueCrop2D of ossqs.cu:135-146 plus the TV terms);
+// image [B][nx][ny][nz][C], TV within each (b, z, c) plane.
+__global__ void sqs_update_kernel(float* __restrict__ xo, const float* __restrict__ xi, const float* __restrict__ bp,
+                                  const float* __restrict__ nimg, int nb, int nx, int ny, int nz, int nc, float lam,
+                                  float beta, float M, float lb, float ub, int clamp) {
+    long long n = (long long)nb * nx * ny * nz * nc;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float num = M * bp[i];
+    float den = nimg[i] + 1e-6f;
+    if (beta != 0.f) {
+        long long isy = (long long)nz * nc, isx = (long long)ny * isy;
+        long long per_b = (long long)nx * ny * nz * nc;
+        long long bb = i / per_b;
+        long long q = i - bb * per_b;
+        int ix = (int)(q / isx);
+        q -= (long long)ix * isx;
+        int iy = (int)(q / isy);
+        long long zc = q - (long long)iy * isy;
+        const float* plane = xi + bb * per_b + zc;
+        TvTerms t = tv_terms(plane, ix, iy, nx, ny, isx, isy);
+        num += beta * t.grad;
+        den += beta * t.norm;
+    }
+    float v = xi[i] - lam * num / den;
+    if (clamp) v = fminf(fmaxf(v, lb), ub);
+    xo[i] = v;
+}
+
+int sqs_update(rn_fan_plan* p, float* x_out, const float* x_in, const float* prj_s, const float* w_s,
+               const float* norm_img, float lam, float beta, int M, float lb, float ub, int type, cudaStream_t st) {
+    if (!p || !x_out || !x_in || !prj_s || !w_s || !norm_img) return set_error(RN_ERR_ARG, "null argument");
+    if (x_out == x_in) return set_error(RN_ERR_ARG, "sqs update: x_out must not alias x_in");
+    if (!p->d_tmp_prj) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_prj, sizeof(float) * p->prj_elems));
+    if (!p->d_tmp_img) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_img, sizeof(float) * p->img_elems));
+    RN_TRY(fan_project(p, p->d_tmp_prj, x_in, st));
+    long long n = p->prj_elems;
+    residual_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p->d_tmp_prj, prj_s,
+                                                                                               w_s, n);
+    RN_CUDA_TRY(cudaGetLastError());
+    RN_TRY(fan_backproject(p, p->d_tmp_img, p->d_tmp_prj, type, 0, st));
+    const RnFanGeom& g = p->g;
+    long long ni = p->img_elems;
+    sqs_update_kernel<<<(unsigned)((ni + 255) / 256), 256, 0, st>>>(
+        x_out, x_in, p->d_tmp_img, norm_img, g.nBatches, g.nx, g.ny, p->ragged ? 1 : g.nz, p->ragged ? 1 : g.nChannels, lam,
+        beta, (float)M, lb, ub, lb < ub ? 1 : 0);
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host-pointer (reference-named) entry points.
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= n) return RN_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaMalloc");
+        n = bytes;
+        return RN_OK;
+    }
+    template <class T>
+    T* as() {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+// One cached plan and a set of grow-only device buffers per device, guarded
+// by a mutex: repeated host calls with the same geometry and angles reuse the
+// geometry tables and scratch instead of rebuilding them.
+struct HostCtx {
+    std::mutex mu;
+    cudaStream_t st = nullptr;
+    rn_fan_plan* plan = nullptr;
+    RnFanGeom key{};
+    std::vector<float> key_deg;
+    DevBuf a, b, c, d, e;
+};
+static std::mutex g_ctx_mu;
+static std::map<int, HostCtx*> g_ctx;
+
+static HostCtx* host_ctx() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    HostCtx*& c = g_ctx[dev];
+    if (!c) {
+        c = new HostCtx();
+        cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    }
+    return c;
+}
+
+static int ctx_plan(HostCtx* c, const RnFanGeom& g, const float* deg, int nview) {
+    if (c->plan && memcmp(&c->key, &g, sizeof(g)) == 0 && (int)c->key_deg.size() == nview &&
+        memcmp(c->key_deg.data(), deg, sizeof(float) * nview) == 0)
+        return RN_OK;
+    if (c->plan) rn_fan_plan_destroy(c->plan);
+    c->plan = nullptr;
+    RN_TRY(rn_fan_plan_create(&c->plan, &g, deg, c->st));
+    c->key = g;
+    c->key_deg.assign(deg, deg + nview);
+    return RN_OK;
+}
+
+static RnFanGeom fan_geom(int nb, int nc, int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview,
+                          int nv, float da, float dv, float off_a, float off_v, float dsd, float dso) {
+    RnFanGeom g;
+    memset(&g, 0, sizeof(g));
+    g.nBatches = nb;
+    g.nChannels = nc;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.dx = dx;
+    g.dy = dy;
+    g.dz = dz;
+    g.nu = nu;
+    g.nview = nview;
+    g.nv = nv;
+    g.du = da;
+    g.dv = dv;
+    g.off_u = off_a;
+    g.off_v = off_v;
+    g.dsd = dsd;
+    g.dso = dso;
+    return g;
+}
+
+static int finish_sync(HostCtx* c, rn_fan_plan* p) {
+    RN_CUDA_TRY(cudaStreamSynchronize(c->st));
+    if (p) RN_TRY(rn_fan_plan_check(p, c->st));
+    return RN_OK;
+}
+
+static int host_fan_fp(float* prj, const float* img, const float* deg, const RnFanGeom& g) {
+    HostCtx* c = host_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    RN_TRY(ctx_plan(c, g, deg, g.nview));
+    size_t ni = (size_t)c->plan->img_elems, np = (size_t)c->plan->prj_elems;
+    RN_TRY(c->a.ensure(ni * 4));
+    RN_TRY(c->b.ensure(np * 4));
+    RN_CUDA_TRY(cudaMemcpyAsync(c->a.p, img, ni * 4, cudaMemcpyHostToDevice, c->st));
+    RN_TRY(fan_project(c->plan, c->b.as<float>(), c->a.as<float>(), c->st));
+    RN_CUDA_TRY(cudaMemcpyAsync(prj, c->b.p, np * 4, cudaMemcpyDeviceToHost, c->st));
+    return finish_sync(c, c->plan);
+}
+
+static int host_fan_bp(float* img, const float* prj, const float* deg, const RnFanGeom& g, int type) {
+    if (type < 0 || type > 2) type = 0;   // the reference treats any non-1 type as iterative
+    HostCtx* c = host_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    RN_TRY(ctx_plan(c, g, deg, g.nview));
+    size_t ni = (size_t)c->plan->img_elems, np = (size_t)c->plan->prj_elems;
+    RN_TRY(c->a.ensure(ni * 4));
+    RN_TRY(c->b.ensure(np * 4));
+    RN_CUDA_TRY(cudaMemcpyAsync(c->b.p, prj, np * 4, cudaMemcpyHostToDevice, c->st));
+    RN_TRY(fan_backproject(c->plan, c->a.as<float>(), c->b.as<float>(), type, 0, c->st));
+    RN_CUDA_TRY(cudaMemcpyAsync(img, c->a.p, ni * 4, cudaMemcpyDeviceToHost, c->st));
+    return finish_sync(c, c->plan);
+}
+
+}  // namespace rn
+
+using namespace rn;
+
+extern "C" {
+
+int SetDevice(int device) { return (int)cudaSetDevice(device); }
+
+void cDistanceDrivenFanProjection(float* prj, const float* img, const float* deg, int nBatches, int nChannels, int nx,
+                                  int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da,
+                                  float dv, float off_a, float off_v, float dsd, float dso, int typeProjector) {
+    (void)typeProjector;
+    clear_error();
+    if (!prj || !img || !deg) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    host_fan_fp(prj, img, deg, fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a,
+                                        off_v, dsd, dso));
+}
+
+void cDistanceDrivenFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels,
+                                      int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
+                                      float da, float dv, float off_a, float off_v, float dsd, float dso,
+                                      int typeProjector) {
+    clear_error();
+    if (!prj || !img || !deg) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    host_fan_bp(img, prj, deg,
+                fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso),
+                typeProjector);
+}
+
+int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int nu, int nview, int nv, float da,
+              float off_a, float dsd, float dso, int typeFilter, int fan, void* stream) {
+    clear_error();
+    if (!d_out || !d_prj) return set_error(RN_ERR_ARG, "null argument");
+    return filter_device(d_out, d_prj, nBatches, nChannels, nu, nview, nv, da, off_a, dsd, dso, typeFilter, fan,
+                         (cudaStream_t)stream);
+}
+
+static void host_filter(float* out, const float* prj, int nb, int nc, int nu, int nview, int nv, float da,
+                        float off_a, float dsd, float dso, int typeFilter, int fan) {
+    clear_error();
+    if (!out || !prj) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    HostCtx* c = host_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    size_t n = (size_t)nb * nu * nview * nv * nc;
+    if (c->c.ensure(n * 4) != RN_OK || c->d.ensure(n * 4) != RN_OK) return;
+    if (cudaMemcpyAsync(c->c.p, prj, n * 4, cudaMemcpyHostToDevice, c->st) != cudaSuccess) {
+        set_error(RN_ERR_CUDA, "filter: host to device copy failed");
+        return;
+    }
+    if (filter_device(c->d.as<float>(), c->c.as<float>(), nb, nc, nu, nview, nv, da, off_a, dsd, dso, typeFilter,
+                      fan, c->st) != RN_OK)
+        return;
+    if (cudaMemcpyAsync(out, c->d.p, n * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess) {
+        set_error(RN_ERR_CUDA, "filter: device to host copy failed");
+        return;
+    }
+    finish_sync(c, nullptr);
+}
+
+void cFilterFanFilter(float* pFPrj, const float* pPrj, int nBatches, int nChannels, int nu, int nview, int nv,
+                      float da, float dv, float off_a, float off_v, float dsd, float dso, int typeFilter,
+                      int typeProjector) {
+    (void)dv;
+    (void)off_v;
+    (void)typeProjector;
+    host_filter(pFPrj, pPrj, nBatches, nChannels, nu, nview, nv, da, off_a, dsd, dso, typeFilter, 1);
+}
+
+void cFilterParallelFilter(float* pFPrj, const float* pPrj, int nBatches, int nChannels, int nu, int nview, int nv,
+                           float da, float dv, float off_a, float off_v, float dsd, float dso, int typeFilter,
+                           int typeProjector) {
+    (void)dv;
+    (void)off_v;
+    (void)typeProjector;
+    host_filter(pFPrj, pPrj, nBatches, nChannels, nu, nview, nv, da, off_a, dsd, dso, typeFilter, 0);
+}
+
+int rn_tv_sqs(float* d_grad, float* d_norm, double* d_tv, const float* d_img, int nslices, int nx, int ny,
+              void* stream) {
+    clear_error();
+    if (!d_img || nslices <= 0 || nx <= 0 || ny <= 0) return set_error(RN_ERR_ARG, "tv: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (d_tv) RN_CUDA_TRY(cudaMemsetAsync(d_tv, 0, sizeof(double) * nslices, st));
+    dim3 grid((unsigned)((nx * ny + 255) / 256), nslices);
+    tv_kernel<<<grid, 256, 0, st>>>(d_grad, d_norm, d_tv, d_img, nx, ny);
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+float cTVSQS2D(float* grad, float* norm, const float* img, int nx, int ny) {
+    clear_error();
+    if (!grad || !norm || !img || nx <= 0 || ny <= 0) {
+        set_error(RN_ERR_ARG, "cTVSQS2D: bad argument");
+        return 0.f;
+    }
+    HostCtx* c = host_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    size_t n = (size_t)nx * ny;
+    // scratch d: grad [n] | norm [n] | tv (8-byte aligned double)
+    size_t tv_off = (n * 8 + 7) & ~size_t(7);
+    if (c->c.ensure(n * 4) != RN_OK || c->d.ensure(tv_off + 8) != RN_OK) return 0.f;
+    float* dimg = c->c.as<float>();
+    float* dgrad = c->d.as<float>();
+    float* dnorm = dgrad + n;
+    double* dtv = reinterpret_cast<double*>(reinterpret_cast<char*>(c->d.p) + tv_off);
+    if (cudaMemcpyAsync(dimg, img, n * 4, cudaMemcpyHostToDevice, c->st) != cudaSuccess) {
+        set_error(RN_ERR_CUDA, "cTVSQS2D: copy failed");
+        return 0.f;
+    }
+    if (rn_tv_sqs(dgrad, dnorm, dtv, dimg, 1, nx, ny, c->st) != RN_OK) return 0.f;
+    double tv = 0;
+    cudaMemcpyAsync(grad, dgrad, n * 4, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(norm, dnorm, n * 4, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(&tv, dtv, 8, cudaMemcpyDeviceToHost, c->st);
+    if (finish_sync(c, nullptr) != RN_OK) return 0.f;
+    return (float)tv;
+}
+
+int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x_in, const float* d_prj_s,
+                      const float* d_w_s, const float* d_norm_img, float lambda, float beta, int nSubsets, float lb,
+                      float ub, int typeProjector, void* stream) {
+    clear_error();
+    if (typeProjector < 0 || typeProjector > 2) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1 or 2");
+    return sqs_update(subset_plan, d_x_out, d_x_in, d_prj_s, d_w_s, d_norm_img, lambda, beta, nSubsets, lb, ub,
+                      typeProjector, (cudaStream_t)stream);
+}
+
+void cOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
+            const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels,
+            int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
+            float off_a, float off_v, float dsd, float dso, int typeProjector, float lambda) {
+    clear_error();
+    if (!res || !img || !prj || !normImg || !wprj || !degs || nviewPerSubset <= 0 || nSubsets <= 0) {
+        set_error(RN_ERR_ARG, "cOSSQS: bad argument");
+        return;
+    }
+    if (typeProjector < 0 || typeProjector > 2) typeProjector = 0;
+    HostCtx* c = host_ctx();
+    std::lock_guard<std::mutex> lk(c->mu);
+    const size_t ni = (size_t)nBatches * nx * ny * nz * nChannels;
+    const size_t rowC = (size_t)nv * nChannels;   // floats per (u, view)
+    if (c->a.ensure(ni * 4 * 3) != RN_OK) return;
+    float* x0 = c->a.as<float>();
+    float* x1 = x0 + ni;
+    float* dn = x1 + ni;
+    cudaMemcpyAsync(x0, img, ni * 4, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(dn, normImg, ni * 4, cudaMemcpyHostToDevice, c->st);
+    std::vector<float> hs, hw;
+    int start = 0;
+    for (int k = 0; k < nSubsets && start < nview; k++) {
+        int cnt = std::min(nviewPerSubset, nview - start);
+        RnFanGeom g = fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, cnt, nv, da, dv, off_a, off_v, dsd,
+                               dso);
+        rn_fan_plan* sp = nullptr;
+        if (rn_fan_plan_create(&sp, &g, degs + start, c->st) != RN_OK) return;
+        size_t ns = (size_t)nBatches * nu * cnt * rowC;
+        hs.resize(ns);
+        hw.resize(ns);
+        for (int b = 0; b < nBatches; b++)
+            for (int u = 0; u < nu; u++) {
+                size_t src = (((size_t)b * nu + u) * nview + start) * rowC;
+                size_t dst = ((size_t)b * nu + u) * cnt * rowC;
+                memcpy(&hs[dst], prj + src, sizeof(float) * cnt * rowC);
+                memcpy(&hw[dst], wprj + src, sizeof(float) * cnt * rowC);
+            }
+        if (c->b.ensure(ns * 8) != RN_OK) {
+            rn_fan_plan_destroy(sp);
+            return;
+        }
+        float* dps = c->b.as<float>();
+        float* dws = dps + ns;
+        cudaMemcpyAsync(dps, hs.data(), ns * 4, cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(dws, hw.data(), ns * 4, cudaMemcpyHostToDevice, c->st);
+        int s = sqs_update(sp, x1, x0, dps, dws, dn, lambda, 0.f, nSubsets, lb, ub, typeProjector, c->st);
+        if (s == RN_OK) s = finish_sync(c, sp);
+        rn_fan_plan_destroy(sp);
+        if (s != RN_OK) return;
+        std::swap(x0, x1);
+        start += cnt;
+    }
+    cudaMemcpyAsync(res, x0, ni * 4, cudaMemcpyDeviceToHost, c->st);
+    finish_sync(c, nullptr);
+}
+
+}  // extern "C"

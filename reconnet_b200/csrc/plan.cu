@@ -1,0 +1,410 @@
+// Plan construction for the fan projector and the native device API.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "rn_internal.h"
+
+namespace rn {
+
+// ---------------------------------------------------------------------------
+// Error state.
+// ---------------------------------------------------------------------------
+static thread_local std::string t_err;
+static thread_local int t_status = RN_OK;
+
+int set_error(int code, const std::string& msg) {
+    t_status = code;
+    t_err = msg;
+    return code;
+}
+
+int set_cuda_error(cudaError_t e, const char* what) {
+    int code = (e == cudaErrorMemoryAllocation) ? RN_ERR_ALLOC : RN_ERR_CUDA;
+    return set_error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void clear_error() {
+    t_status = RN_OK;
+    t_err.clear();
+}
+
+// Scratch budgets (bytes) for line buffers and edge tables; slices beyond the
+// budget are processed in waves.
+static const long long kLineBudget = 4ll << 30;
+static const long long kTableBudget = 4ll << 30;
+
+static int validate(const RnFanGeom* g) {
+    if (!g) return set_error(RN_ERR_ARG, "null geometry");
+    if (g->nBatches <= 0 || g->nChannels <= 0 || g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->nu <= 0 ||
+        g->nview <= 0 || g->nv <= 0)
+        return set_error(RN_ERR_ARG, "geometry sizes must be positive");
+    if (!(g->dx > 0 && g->dy > 0 && g->dz > 0 && g->du > 0 && g->dv > 0 && g->dsd > 0 && g->dso > 0))
+        return set_error(RN_ERR_ARG, "pixel sizes, detector pitch and distances must be positive");
+    if (g->nx >= (1 << 20) || g->ny >= (1 << 20))
+        return set_error(RN_ERR_ARG, "image too large");
+    return RN_OK;
+}
+
+static void set_dims(rn_fan_plan* p, long long isx, long long isy) {
+    const RnFanGeom& g = p->g;
+    FanDims& d = p->dims;
+    d.nx = g.nx;
+    d.ny = g.ny;
+    d.nu = g.nu;
+    d.dx = g.dx;
+    d.dy = g.dy;
+    d.du = g.du;
+    d.off_u = g.off_u;
+    d.dsd = g.dsd;
+    d.dso = g.dso;
+    d.lpx = (int)((g.nx + 1 + 3) & ~3);
+    d.lpy = (int)((g.ny + 1 + 3) & ~3);
+    d.isx = isx;
+    d.isy = isy;
+}
+
+static void build_fp_work(rn_fan_plan* p) {
+    const int VT = 4;  // kFpViews in fan.cu
+    p->h_fp_work.clear();
+    for (size_t s = 0; s < p->h_fp.size(); s++) {
+        const GeoSet& gs = p->h_sets[p->h_fp[s].set];
+        for (int k = 0; k < gs.nxv; k += VT) {
+            int w[4] = {(int)s, 1, k, std::min(VT, gs.nxv - k)};
+            p->h_fp_work.insert(p->h_fp_work.end(), w, w + 4);
+        }
+        int ny_ = gs.nview - gs.nxv;
+        for (int k = 0; k < ny_; k += VT) {
+            int w[4] = {(int)s, 0, gs.nxv + k, std::min(VT, ny_ - k)};
+            p->h_fp_work.insert(p->h_fp_work.end(), w, w + 4);
+        }
+    }
+    p->n_fp_work = (int)(p->h_fp_work.size() / 4);
+}
+
+// Table window (entries per view staged by the BP kernels): the detector
+// extent, in cells, of a 64x64-pixel tile at the point closest to the source.
+static int table_window(const RnFanGeom& g) {
+    const double tile = 64.0;
+    double diag = tile * std::sqrt((double)g.dx * g.dx + (double)g.dy * g.dy);
+    double hx = g.nx * g.dx / 2.0 + std::fabs(g.cx), hy = g.ny * g.dy / 2.0 + std::fabs(g.cy);
+    double dmin = g.dso - std::sqrt(hx * hx + hy * hy);
+    if (dmin <= 0) return -1;
+    double w = diag / (dmin * g.du) + 8;
+    int win = (int)std::ceil(w);
+    win = (win + 7) & ~7;
+    return std::min(win, g.nu + 1);
+}
+
+static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
+    const RnFanGeom& g = p->g;
+    int win = table_window(g);
+    if (win < 0) return set_error(RN_ERR_ARG, "fan geometry: the image reaches the source");
+    if (win > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
+    p->table_win = win;
+    RN_TRY(fan_build_geometry(p, host_deg, st));
+    build_fp_work(p);
+
+    RN_CUDA_TRY(cudaMalloc(&p->d_fp, sizeof(FpSlice) * p->h_fp.size()));
+    RN_CUDA_TRY(cudaMalloc(&p->d_bp, sizeof(BpSlice) * p->h_bp.size()));
+    RN_CUDA_TRY(cudaMalloc(&p->d_bpr, sizeof(BpSlice) * p->h_bpr.size()));
+    RN_CUDA_TRY(cudaMalloc(&p->d_fp_work, sizeof(int4) * std::max(1, p->n_fp_work)));
+    RN_CUDA_TRY(cudaMalloc(&p->d_err, sizeof(int)));
+    RN_CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_fp, p->h_fp.data(), sizeof(FpSlice) * p->h_fp.size(), cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_bp, p->h_bp.data(), sizeof(BpSlice) * p->h_bp.size(), cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(
+        cudaMemcpyAsync(p->d_bpr, p->h_bpr.data(), sizeof(BpSlice) * p->h_bpr.size(), cudaMemcpyHostToDevice, st));
+    if (p->n_fp_work > 0)
+        RN_CUDA_TRY(cudaMemcpyAsync(p->d_fp_work, p->h_fp_work.data(), sizeof(int4) * p->n_fp_work,
+                                    cudaMemcpyHostToDevice, st));
+
+    // line scratch
+    const FanDims& d = p->dims;
+    p->line_slot_elems = (long long)d.ny * d.lpx + (long long)d.nx * d.lpy;
+    long long slot_bytes = p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float));
+    p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(), kLineBudget / slot_bytes));
+    RN_CUDA_TRY(cudaMalloc(&p->d_hl, sizeof(float2) * p->fp_slots * p->line_slot_elems));
+    RN_CUDA_TRY(cudaMalloc(&p->d_la, sizeof(float) * p->fp_slots * p->line_slot_elems));
+
+    // table scratch: all slices if within budget, else at least the largest slice
+    long long need = 0, largest = 0;
+    for (const BpSlice& b : p->h_bp) {
+        long long n = (long long)p->h_sets[b.set].nview * (g.nu + 1);
+        need = std::max(need, b.table_off + n);
+        largest = std::max(largest, n);
+    }
+    p->tab_elems = std::max(largest, std::min(need, kTableBudget / (long long)sizeof(float4)));
+    RN_CUDA_TRY(cudaMalloc(&p->d_tab, sizeof(float4) * p->tab_elems));
+    RN_CUDA_TRY(cudaStreamSynchronize(st));
+    return RN_OK;
+}
+
+}  // namespace rn
+
+using namespace rn;
+
+extern "C" {
+
+const char* rn_last_error(void) { return rn::t_err.c_str(); }
+int rn_last_status(void) { return rn::t_status; }
+int rn_version(void) { return 1; }
+
+int rn_fan_plan_destroy(rn_fan_plan* p) {
+    if (!p) return RN_OK;
+    cudaFree(p->d_views);
+    cudaFree(p->d_edges);
+    cudaFree(p->d_cell);
+    cudaFree(p->d_perm);
+    cudaFree(p->d_sets);
+    cudaFree(p->d_fp);
+    cudaFree(p->d_bp);
+    cudaFree(p->d_bpr);
+    cudaFree(p->d_fp_work);
+    cudaFree(p->d_err);
+    cudaFree(p->d_hl);
+    cudaFree(p->d_la);
+    cudaFree(p->d_tab);
+    cudaFree(p->d_tmp_img);
+    cudaFree(p->d_tmp_prj);
+    for (auto& t : p->timed) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    delete p;
+    return RN_OK;
+}
+
+int rn_fan_plan_create(rn_fan_plan** out, const RnFanGeom* g, const float* host_deg, void* stream) {
+    clear_error();
+    if (!out || !host_deg) return set_error(RN_ERR_ARG, "null argument");
+    *out = nullptr;
+    RN_TRY(validate(g));
+    cudaStream_t st = (cudaStream_t)stream;
+    rn_fan_plan* p = new rn_fan_plan();
+    p->g = *g;
+    p->ragged = false;
+    cudaGetDevice(&p->device);
+    const int B = g->nBatches, C = g->nChannels, nx = g->nx, ny = g->ny, nz = g->nz, nu = g->nu, nview = g->nview,
+              nv = g->nv;
+    set_dims(p, (long long)ny * nz * C, (long long)nz * C);
+    p->total_views = nview;
+    p->h_sets.push_back(GeoSet{0, nview, 0});
+    const long long img_b = (long long)nx * ny * nz * C, prj_b = (long long)nu * nview * nv * C;
+    p->img_elems = img_b * B;
+    p->prj_elems = prj_b * B;
+
+    // FP slices (b, iv, c): image planes mixed at the z texture coordinate of
+    // detector row iv (DistanceDriven.cu:86,99; texel-centre convention, border).
+    std::vector<std::vector<std::pair<int, float>>> zmix(nv);
+    for (int iv = 0; iv < nv; iv++) {
+        double z = (iv - (nv - 1) / 2.0 + g->off_v) * g->dv;
+        double zc = (z - g->cz) / g->dz + nz / 2.0;
+        double zb = zc - 0.5;
+        double z0 = std::floor(zb);
+        double wz = zb - z0;
+        for (int k = 0; k < 2; k++) {
+            int zi = (int)z0 + k;
+            float w = (float)(k ? wz : 1.0 - wz);
+            if (zi >= 0 && zi < nz && w != 0.f) zmix[iv].push_back({zi, w});
+        }
+    }
+    for (int b = 0; b < B; b++)
+        for (int iv = 0; iv < nv; iv++)
+            for (int c = 0; c < C; c++) {
+                FpSlice f;
+                memset(&f, 0, sizeof(f));
+                for (size_t k = 0; k < zmix[iv].size(); k++) {
+                    f.img_off[k] = b * img_b + (long long)zmix[iv][k].first * C + c;
+                    f.img_w[k] = zmix[iv][k].second;
+                }
+                f.prj_off = b * prj_b + (long long)iv * C + c;
+                f.su = nview * nv * C;
+                f.sview = nv * C;
+                f.set = 0;
+                f.line_slot = 0;
+                p->h_fp.push_back(f);
+            }
+    // matched BP slices (b, z, c): transpose of the z mixing above
+    std::vector<std::vector<std::pair<int, float>>> zin(nz);
+    for (int iv = 0; iv < nv; iv++)
+        for (auto& t : zmix[iv]) zin[t.first].push_back({iv, t.second});
+    // reference BP slices (b, iz, c): sinogram rows mixed at ivf + 0.5
+    // (DistanceDriven.cu:518,543; border addressing along v)
+    std::vector<std::vector<std::pair<int, float>>> vmix(nz);
+    for (int iz = 0; iz < nz; iz++) {
+        double ivf = (iz - (nz - 1) / 2.0) * g->dz / g->dv + g->off_v + (nv - 1.0) / 2.0;
+        double v0 = std::floor(ivf);
+        double wv = ivf - v0;
+        for (int k = 0; k < 2; k++) {
+            int vi = (int)v0 + k;
+            float w = (float)(k ? wv : 1.0 - wv);
+            if (vi >= 0 && vi < nv && w != 0.f) vmix[iz].push_back({vi, w});
+        }
+    }
+    for (int iz = 0; iz < nz; iz++)
+        if ((int)zin[iz].size() > kBpMix) {
+            delete p;
+            return set_error(RN_ERR_ARG, "fan geometry: more than 4 detector rows map onto one image slice");
+        }
+    long long toff = 0;
+    for (int b = 0; b < B; b++)
+        for (int z = 0; z < nz; z++)
+            for (int c = 0; c < C; c++) {
+                BpSlice m, r;
+                memset(&m, 0, sizeof(m));
+                memset(&r, 0, sizeof(r));
+                m.img_off = r.img_off = b * img_b + (long long)z * C + c;
+                for (size_t k = 0; k < zin[z].size(); k++) {
+                    m.prj_off[k] = b * prj_b + (long long)zin[z][k].first * C + c;
+                    m.prj_w[k] = zin[z][k].second;
+                }
+                for (size_t k = 0; k < vmix[z].size(); k++) {
+                    r.prj_off[k] = b * prj_b + (long long)vmix[z][k].first * C + c;
+                    r.prj_w[k] = vmix[z][k].second;
+                }
+                m.su = r.su = nview * nv * C;
+                m.sview = r.sview = nv * C;
+                m.set = r.set = 0;
+                m.table_off = r.table_off = toff;
+                toff += (long long)nview * (nu + 1);
+                p->h_bp.push_back(m);
+                p->h_bpr.push_back(r);
+            }
+    int s = finish_plan(p, host_deg, st);
+    if (s != RN_OK) {
+        std::string msg = rn_last_error();
+        rn_fan_plan_destroy(p);
+        return set_error(s, msg);
+    }
+    *out = p;
+    return RN_OK;
+}
+
+int rn_fan_plan_create_ragged(rn_fan_plan** out, const RnFanGeom* g, const int* nview_per_slice,
+                              const float* host_deg, void* stream) {
+    clear_error();
+    if (!out || !host_deg || !nview_per_slice) return set_error(RN_ERR_ARG, "null argument");
+    *out = nullptr;
+    RnFanGeom gg = *g;
+    gg.nz = gg.nv = gg.nChannels = 1;
+    if (g->nz != 1 || g->nv != 1 || g->nChannels != 1)
+        return set_error(RN_ERR_ARG, "ragged plans hold 2D slices: nz, nv and nChannels must be 1");
+    long long total = 0;
+    for (int s = 0; s < g->nBatches; s++) {
+        if (nview_per_slice[s] <= 0) return set_error(RN_ERR_ARG, "every slice needs at least one view");
+        total += nview_per_slice[s];
+    }
+    gg.nview = (int)std::min<long long>(total, 1 << 30);
+    RN_TRY(validate(&gg));
+    cudaStream_t st = (cudaStream_t)stream;
+    rn_fan_plan* p = new rn_fan_plan();
+    p->g = gg;
+    p->ragged = true;
+    cudaGetDevice(&p->device);
+    const int S = g->nBatches, nx = g->nx, ny = g->ny, nu = g->nu;
+    set_dims(p, ny, 1);
+    p->total_views = total;
+    p->img_elems = (long long)S * nx * ny;
+    p->prj_elems = total * nu;
+    int voff = 0;
+    for (int s = 0; s < S; s++) {
+        int nvs = nview_per_slice[s];
+        p->h_sets.push_back(GeoSet{voff, nvs, 0});
+        FpSlice f;
+        memset(&f, 0, sizeof(f));
+        f.img_off[0] = (long long)s * nx * ny;
+        f.img_w[0] = 1.f;
+        f.prj_off = (long long)nu * voff;
+        f.su = nvs;
+        f.sview = 1;
+        f.set = s;
+        p->h_fp.push_back(f);
+        BpSlice b;
+        memset(&b, 0, sizeof(b));
+        b.img_off = (long long)s * nx * ny;
+        b.prj_off[0] = (long long)nu * voff;
+        b.prj_w[0] = 1.f;
+        b.su = nvs;
+        b.sview = 1;
+        b.set = s;
+        b.table_off = (long long)voff * (nu + 1);
+        p->h_bp.push_back(b);
+        p->h_bpr.push_back(b);
+        voff += nvs;
+    }
+    int st2 = finish_plan(p, host_deg, st);
+    if (st2 != RN_OK) {
+        std::string msg = rn_last_error();
+        rn_fan_plan_destroy(p);
+        return set_error(st2, msg);
+    }
+    *out = p;
+    return RN_OK;
+}
+
+int64_t rn_fan_plan_total_views(const rn_fan_plan* p) { return p ? p->total_views : 0; }
+
+int rn_fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, void* stream) {
+    clear_error();
+    if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
+    return rn::fan_project(p, d_prj, d_img, (cudaStream_t)stream);
+}
+
+int rn_fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, void* stream) {
+    clear_error();
+    if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
+    if (type < 0 || type > 2) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1 or 2");
+    return rn::fan_backproject(p, d_img, d_prj, type, accumulate ? 1 : 0, (cudaStream_t)stream);
+}
+
+int rn_fan_plan_set_timing(rn_fan_plan* p, int enable) {
+    clear_error();
+    if (!p) return set_error(RN_ERR_ARG, "null plan");
+    p->timing = enable != 0;
+    return RN_OK;
+}
+
+int rn_fan_plan_read_timing(rn_fan_plan* p, float* ms, int* counts, int nkinds, long long* launches) {
+    clear_error();
+    if (!p) return set_error(RN_ERR_ARG, "null plan");
+    for (int k = 0; k < nkinds; k++) {
+        if (ms) ms[k] = 0.f;
+        if (counts) counts[k] = 0;
+    }
+    if (launches) *launches = p->launches;
+    if (nkinds <= 0) return RN_OK;   // launch count only; keep pending timings
+    for (auto& t : p->timed) {
+        float e = 0.f;
+        if (cudaEventSynchronize(t.stop) == cudaSuccess && cudaEventElapsedTime(&e, t.start, t.stop) == cudaSuccess &&
+            t.kind >= 0 && t.kind < nkinds) {
+            if (ms) ms[t.kind] += e;
+            if (counts) counts[t.kind] += 1;
+        }
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    p->timed.clear();
+    return RN_OK;
+}
+
+int rn_fan_plan_check(rn_fan_plan* p, void* stream) {
+    clear_error();
+    if (!p) return set_error(RN_ERR_ARG, "null plan");
+    int h = 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    RN_CUDA_TRY(cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h != 0) {
+        RN_CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+        return set_error(RN_ERR_TIMEOUT, "a device-side wait exceeded its spin limit");
+    }
+    return RN_OK;
+}
+
+}  // extern "C"

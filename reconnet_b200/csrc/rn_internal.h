@@ -1,0 +1,175 @@
+// Internal definitions shared by the reconnet_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/reconnet_b200.h"
+
+namespace rn {
+
+// ---------------------------------------------------------------------------
+// Error reporting (thread-local last error, int status codes).
+// ---------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);
+int set_cuda_error(cudaError_t e, const char* what);
+void clear_error();
+
+#define RN_CUDA_TRY(call)                                         \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) return ::rn::set_cuda_error(_e, #call); \
+    } while (0)
+
+#define RN_TRY(call)                       \
+    do {                                   \
+        int _s = (call);                   \
+        if (_s != RN_OK) return _s;        \
+    } while (0)
+
+// Spin limit of every device-side wait (mbarrier parity waits).  A wait that
+// exceeds it records RN_ERR_TIMEOUT in the plan's error word and the kernel
+// returns early instead of hanging the GPU.
+constexpr long long kSpinLimit = 1ll << 22;
+
+// ---------------------------------------------------------------------------
+// Geometry tables (device).
+// ---------------------------------------------------------------------------
+
+// Per view, image coordinates with the origin at the corner of pixel 0
+// (PhysicsToImg, ReconNet4D/DistanceDriven.cu:14-20).  "Lines" are image rows
+// for X-class views (|cos| > |sin|, DistanceDriven.cu:299-312) and image
+// columns for Y-class views; positions along a line are x (X) or y (Y).
+struct ViewGeo {
+    double par, perp;   // source coordinate along / across the lines
+    float cosd, sind;   // cos/sin of the view angle
+    float tA, tB;       // edge index of a slope r: t = tA + tB * atan(kappa * r)
+    float kappa;        // physical / image slope factor
+    float rmin, rmax;   // slope range covered by the detector
+    float sigma;        // +-1: do edge indices increase along the line?
+    int xcls;           // 1 = X-class
+    int pad;
+};
+
+// A 2D forward problem: sinogram plane at prj_off (strides su, sview)
+// projected from a mix of up to 2 image planes (z interpolation).
+struct FpSlice {
+    long long img_off[2];
+    float img_w[2];
+    long long prj_off;
+    int su, sview;
+    int set;            // geometry set (angle list)
+    int line_slot;      // index of this slice's line buffers
+};
+
+// A 2D backward problem: image plane at img_off from a mix of up to 4
+// sinogram planes.
+constexpr int kBpMix = 4;
+struct BpSlice {
+    long long img_off;
+    long long prj_off[kBpMix];
+    float prj_w[kBpMix];
+    int su, sview;
+    int set;
+    long long table_off;  // first float4 of this slice's edge tables
+};
+
+struct GeoSet {
+    int view_off;   // first view in the view tables
+    int nview;
+    int nxv;        // number of X-class views; class-sorted order in perm
+};
+
+// Kernel launch parameters shared by the fan kernels.
+struct FanDims {
+    int nx, ny, nu;
+    float dx, dy;
+    float du, off_u, dsd, dso;
+    int lpx, lpy;   // padded line lengths (>= nx+1 / ny+1, multiple of 4)
+    long long isx, isy;   // image strides (elements) along x and y
+};
+
+}  // namespace rn
+
+// Plan object (opaque in the C API).
+struct rn_fan_plan {
+    RnFanGeom g;
+    bool ragged;
+    int device;
+    rn::FanDims dims;
+
+    // host copies
+    std::vector<rn::GeoSet> h_sets;
+    std::vector<rn::FpSlice> h_fp;
+    std::vector<rn::BpSlice> h_bp;     // matched backprojection slices
+    std::vector<rn::BpSlice> h_bpr;    // reference-mode backprojection slices
+    std::vector<int> h_fp_work;    // packed FP work items
+    int n_fp_work = 0;
+    int64_t total_views = 0;
+    long long prj_elems = 0, img_elems = 0;
+
+    // device tables
+    rn::ViewGeo* d_views = nullptr;
+    double* d_edges = nullptr;      // [total_views][nu+1] slopes
+    float2* d_cell = nullptr;       // [nu] (cos a_u, sin a_u)
+    int* d_perm = nullptr;          // [total_views] class-sorted view order per set
+    rn::GeoSet* d_sets = nullptr;
+    rn::FpSlice* d_fp = nullptr;
+    rn::BpSlice* d_bp = nullptr;
+    rn::BpSlice* d_bpr = nullptr;
+    int4* d_fp_work = nullptr;      // {slice, class, vbegin, vcount}
+    int* d_err = nullptr;           // device error word
+
+    // scratch
+    float2* d_hl = nullptr;         // line prefixes (hi, lo)
+    float* d_la = nullptr;          // line values
+    long long line_slot_elems = 0;  // per FP slice: ny*lpx + nx*lpy
+    long long fp_slots = 0;         // FP slices whose lines fit in the scratch
+    int table_win = 0;              // staged table entries per view (BP)
+    float4* d_tab = nullptr;        // BP edge tables
+    long long tab_elems = 0;
+    float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, lazily allocated)
+    float* d_tmp_prj = nullptr;     // sinogram-sized scratch (SQS update, lazily allocated)
+
+    // instrumentation: kernel launch count and optional per-kernel CUDA-event
+    // timing (kinds: 0 line prologue, 1 forward projection, 2 edge tables,
+    // 3 backprojection, 4 other)
+    long long launches = 0;
+    bool timing = false;
+    struct TimedLaunch {
+        int kind;
+        cudaEvent_t start, stop;
+    };
+    std::vector<TimedLaunch> timed;
+};
+
+namespace rn {
+constexpr int kTimedKinds = 5;
+// Brackets one kernel launch of `plan` on stream `st`: counts it and, when
+// timing is enabled, records a start/stop event pair around it.
+struct LaunchScope {
+    rn_fan_plan* p;
+    cudaStream_t st;
+    int idx = -1;
+    LaunchScope(rn_fan_plan* plan, cudaStream_t s, int kind) : p(plan), st(s) {
+        p->launches++;
+        if (p->timing) {
+            rn_fan_plan::TimedLaunch t{kind, nullptr, nullptr};
+            cudaEventCreate(&t.start);
+            cudaEventCreate(&t.stop);
+            cudaEventRecord(t.start, st);
+            p->timed.push_back(t);
+            idx = (int)p->timed.size() - 1;
+        }
+    }
+    ~LaunchScope() {
+        if (idx >= 0) cudaEventRecord(p->timed[idx].stop, st);
+    }
+};
+int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st);
+int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st);
+int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st);
+}  // namespace rn

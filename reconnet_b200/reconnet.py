@@ -1,0 +1,294 @@
+"""Host (numpy) API mirroring the reference's ``ReconNet`` class.
+
+Same attribute names, defaults and method signatures as
+python/ReconNet_no_tf.py:26-632 for the distance-driven path; every method
+calls the reference-named C entry points of ``libreconnet_b200.so`` and raises
+``ReconNetError`` on failure (the reference printed to stderr and threw).
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+
+import numpy as np
+
+from . import _native as N
+
+_c = ctypes
+
+
+def _fptr(a):
+    return a.ctypes.data_as(_c.POINTER(_c.c_float))
+
+
+class ReconNet:
+    """Geometry holder + DD projector calls (python/ReconNet_no_tf.py:26)."""
+
+    def __init__(self):
+        # defaults of python/ReconNet_no_tf.py:27-47
+        self.rotview = 720
+        self.nu = 736
+        self.nv = 1
+        self.nx = 512
+        self.ny = 512
+        self.nz = 1
+        self.dx = 1
+        self.dy = 1
+        self.dz = 2
+        self.cx = 0
+        self.cy = 0
+        self.cz = 0
+        self.dsd = 1085.6
+        self.dso = 595
+        self.du = 1.2858
+        self.dv = 2
+        self.da = self.du / self.dsd
+        self.off_a = 0
+        self.off_u = 0
+        self.off_v = 0
+        self.UpdateAngularSampling()
+
+    def FromFile(self, filename):
+        """Whitespace-separated ``name value`` lines (ReconNet_no_tf.py:49-73)."""
+        params = {}
+        with open(filename, "r") as f:
+            for line in f:
+                parts = [p for p in re.split(r"[ \t\n]", line) if p != ""]
+                if len(parts) < 2:
+                    continue
+                params[parts[0].lower()] = np.float32(parts[1])
+        for k, v in params.items():
+            setattr(self, k, v)
+        for k in ("rotview", "nu", "nv", "nx", "ny", "nz"):
+            setattr(self, k, int(getattr(self, k)))
+        self.off_a = -self.off_a
+        self.da = self.du / self.dsd
+        self.UpdateAngularSampling()
+
+    def UpdateAngularSampling(self):
+        self.angles = (np.arange(0, self.rotview, dtype=np.float32) * 2 * np.pi / self.rotview).tolist()
+
+    def get_det_sz(self, type_projector=0):
+        return [self.da, self.dv]
+
+    def get_det_off(self, type_projector=0):
+        return [self.off_a, self.off_v]
+
+    def get_img_shape(self):
+        return [self.nx, self.ny, self.nz]
+
+    def get_sino_shape(self):
+        return [self.nu, self.rotview, self.nv]
+
+    def cSetDevice(self, device):
+        return N.lib.SetDevice(int(device))
+
+    # ---- ramp filter (Filter.cu:432 / :476) ----
+    def cFilter4d(self, sino, type_filter=0, type_projector=0):
+        sino = np.ascontiguousarray(sino, np.float32)
+        fsino = np.zeros(sino.shape, np.float32)
+        N.lib.cFilterFanFilter(_fptr(fsino), _fptr(sino), sino.shape[0], sino.shape[4], sino.shape[1],
+                               sino.shape[2], sino.shape[3], self.da, self.dv, self.off_a, self.off_v,
+                               self.dsd, self.dso, int(type_filter), int(type_projector))
+        N.check_last()
+        return fsino
+
+    def cFilter3d(self, sino, type_filter=0, type_projector=0):
+        return self.cFilter4d(sino[..., np.newaxis, :], type_filter, type_projector)[..., 0, :]
+
+    def cFilterParallel4d(self, sino, type_filter=0):
+        sino = np.ascontiguousarray(sino, np.float32)
+        fsino = np.zeros(sino.shape, np.float32)
+        N.lib.cFilterParallelFilter(_fptr(fsino), _fptr(sino), sino.shape[0], sino.shape[4], sino.shape[1],
+                                    sino.shape[2], sino.shape[3], self.da, self.dv, self.off_a, self.off_v,
+                                    self.dsd, self.dso, int(type_filter), 0)
+        N.check_last()
+        return fsino
+
+    # ---- DD fan projector (DistanceDriven.cu:386 / :793) ----
+    def _angles(self, angles):
+        if angles is None:
+            return np.array(self.angles, np.float32)
+        return np.ascontiguousarray(angles, np.float32)
+
+    def _fan_args(self, img_shape5, sino_shape5, type_projector):
+        B, nx, ny, nz, C = img_shape5
+        _, nu, nview, nv, _ = sino_shape5
+        return (B, C, nx, ny, nz, self.dx, self.dy, self.dz, nu, nview, nv, self.da, self.dv, self.off_a,
+                self.off_v, self.dsd, self.dso, int(type_projector))
+
+    def cDDFanProjection4d(self, img, angles=None, sino_shape=None, type_projector=0):
+        img = np.ascontiguousarray(img, np.float32)
+        angles = self._angles(angles)
+        if sino_shape is None:
+            sino_shape = [self.nu, len(angles), self.nv]
+        sino = np.zeros([img.shape[0], sino_shape[0], sino_shape[1], sino_shape[2], img.shape[4]], np.float32)
+        N.lib.cDistanceDrivenFanProjection(_fptr(sino), _fptr(img), _fptr(angles),
+                                           *self._fan_args(img.shape, sino.shape, type_projector))
+        N.check_last()
+        return sino
+
+    def cDDFanProjection3d(self, img, angles=None, sino_shape=None, type_projector=0):
+        angles = self._angles(angles)
+        if sino_shape is None:
+            sino_shape = [self.nu, len(angles), 1]
+        sino = self.cDDFanProjection4d(img[..., np.newaxis, :], angles, sino_shape, type_projector)
+        return np.squeeze(sino, -2)
+
+    def cDDFanBackprojection4d(self, sino, angles=None, img_shape=None, type_projector=0):
+        sino = np.ascontiguousarray(sino, np.float32)
+        angles = self._angles(angles)
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, self.nz]
+        img = np.zeros([sino.shape[0], img_shape[0], img_shape[1], img_shape[2], sino.shape[4]], np.float32)
+        N.lib.cDistanceDrivenFanBackprojection(_fptr(img), _fptr(sino), _fptr(angles),
+                                               *self._fan_args(img.shape, sino.shape, type_projector))
+        N.check_last()
+        return img
+
+    def cDDFanBackprojection3d(self, sino, angles=None, img_shape=None, type_projector=0):
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, 1]
+        img = self.cDDFanBackprojection4d(sino[..., np.newaxis, :], angles, img_shape, type_projector)
+        return img[..., 0, :]
+
+    def cDDFanNormImg4d(self, sino, wsino=None, angles=None, img_shape=None, type_projector=0):
+        """normImg = BP(W * FP(1)) (ReconNet_no_tf.py:202-223)."""
+        angles = self._angles(angles)
+        wsino = np.ones(sino.shape, np.float32) if wsino is None else np.asarray(wsino, np.float32)
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, self.nz]
+        ones = np.ones([sino.shape[0], img_shape[0], img_shape[1], img_shape[2], sino.shape[4]], np.float32)
+        fp = self.cDDFanProjection4d(ones, angles, sino.shape[1:4], type_projector)
+        return self.cDDFanBackprojection4d(fp * wsino, angles, img_shape, type_projector)
+
+    def cDDFanNormImg3d(self, sino, wsino=None, angles=None, img_shape=None, type_projector=0):
+        wsino = np.ones(sino.shape, np.float32) if wsino is None else np.asarray(wsino, np.float32)
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, 1]
+        n = self.cDDFanNormImg4d(sino[..., np.newaxis, :], wsino[..., np.newaxis, :], angles, img_shape,
+                                 type_projector)
+        return n[..., 0, :]
+
+    # ---- OS-SQS with the DD projector (ossqs.cu:12 semantics) ----
+    def cDDFanOSSQS4d(self, nSubsets, img, sino, normImg, wsino=None, angles=None, order=None, lb=None, ub=None,
+                      type_projector=0, lam=1):
+        """Same arguments as cSiddonFanOSSQS4d (ReconNet_no_tf.py:396-440) with the DD pair."""
+        img = np.ascontiguousarray(img, np.float32)
+        sino = np.asarray(sino, np.float32)
+        normImg = np.ascontiguousarray(normImg, np.float32)
+        lb = np.finfo(np.float32).min if lb is None else lb
+        ub = np.finfo(np.float32).max if ub is None else ub
+        wsino = np.ones(sino.shape, np.float32) if wsino is None else np.asarray(wsino, np.float32)
+        angles = self._angles(angles)
+        nviewPerSubset = int(np.ceil(sino.shape[2] / float(nSubsets)))
+        if order is not None:
+            angles = np.ascontiguousarray(angles[order])
+            sino = sino[..., order, :, :]
+            wsino = wsino[..., order, :, :]
+        sino = np.ascontiguousarray(sino, np.float32)
+        wsino = np.ascontiguousarray(wsino, np.float32)
+        res = np.zeros(img.shape, np.float32)
+        B, nx, ny, nz, C = img.shape
+        N.lib.cOSSQS(_fptr(res), _fptr(img), _fptr(sino), _fptr(normImg), _fptr(wsino), _fptr(angles),
+                     float(lb), float(ub), nviewPerSubset, int(nSubsets), B, C, nx, ny, nz, self.dx, self.dy,
+                     self.dz, sino.shape[1], sino.shape[2], sino.shape[3], self.da, self.dv, self.off_a, self.off_v,
+                     self.dsd, self.dso, int(type_projector), float(lam))
+        N.check_last()
+        return res
+
+    def cDDFanOSSQS3d(self, nSubsets, img, sino, normImg, wsino=None, angles=None, order=None, lb=None, ub=None,
+                      type_projector=0, lam=1):
+        wsino = np.ones(sino.shape, np.float32) if wsino is None else np.asarray(wsino, np.float32)
+        res = self.cDDFanOSSQS4d(nSubsets, img[..., np.newaxis, :], sino[..., np.newaxis, :],
+                                 normImg[..., np.newaxis, :], wsino[..., np.newaxis, :], angles, order, lb, ub,
+                                 type_projector, lam)
+        return res[..., 0, :]
+
+    # ---- tomosynthesis DD (DistanceDriven3D.cu:346 / :666) ----
+    def _tomo_args(self, img_shape5, prj_shape5):
+        B, nx, ny, nz, C = img_shape5
+        _, nu, nview, nv, _ = prj_shape5
+        return (B, C, nx, ny, nz, self.dx, self.dy, self.dz, self.cx, self.cy, self.cz, nu, nview, nv, self.du,
+                self.dv, self.off_u, self.off_v)
+
+    def cDDTomoProjection4d(self, img, detCenter, src):
+        img = np.ascontiguousarray(img, np.float32)
+        detCenter = np.ascontiguousarray(detCenter, np.float32)
+        src = np.ascontiguousarray(src, np.float32)
+        prj = np.zeros([img.shape[0], self.nu, detCenter.shape[0], self.nv, img.shape[-1]], np.float32)
+        N.lib.cDistanceDrivenTomoProjection(_fptr(prj), _fptr(img), _fptr(detCenter), _fptr(src),
+                                            *self._tomo_args(img.shape, prj.shape))
+        N.check_last()
+        return prj
+
+    def cDDTomoBackprojection4d(self, prj, detCenter, src):
+        prj = np.ascontiguousarray(prj, np.float32)
+        detCenter = np.ascontiguousarray(detCenter, np.float32)
+        src = np.ascontiguousarray(src, np.float32)
+        img = np.zeros([prj.shape[0], self.nx, self.ny, self.nz, prj.shape[-1]], np.float32)
+        N.lib.cDistanceDrivenTomoBackprojection(_fptr(img), _fptr(prj), _fptr(detCenter), _fptr(src),
+                                                *self._tomo_args(img.shape, prj.shape))
+        N.check_last()
+        return img
+
+    def cDDTomoNormImg4d(self, prj, detCenter, src, mask=None):
+        img = np.ones([prj.shape[0], self.nx, self.ny, self.nz, prj.shape[-1]], np.float32)
+        if mask is None:
+            mask = np.ones_like(img)
+        fp = self.cDDTomoProjection4d(img * mask, detCenter, src)
+        return self.cDDTomoBackprojection4d(fp, detCenter, src) * mask
+
+    # ---- TV surrogate (TotalVariation.cu:70) ----
+    def cTVSQS2d(self, img):
+        img = np.ascontiguousarray(img, np.float32)
+        if img.ndim != 4 or img.shape[0] != 1 or img.shape[-1] != 1:
+            raise ValueError("img.shape must be [1, _, _, 1]")
+        grad = np.zeros(img.shape, np.float32)
+        norm = np.zeros(img.shape, np.float32)
+        tv = N.lib.cTVSQS2D(_fptr(grad), _fptr(norm), _fptr(img), img.shape[1], img.shape[2])
+        N.check_last()
+        return grad, norm, tv
+
+
+def ParkerWeighting(reconNet):
+    """Parker short-scan weights (python/ReconNet_no_tf.py:640-659), shape [1, nu, nview, 1]."""
+    gamma = (reconNet.angles[-1] - np.pi) / 2
+    alphas = ((np.arange(reconNet.nu) - (reconNet.nu - 1) / 2) - reconNet.off_a) * reconNet.da
+    weights = []
+    for beta in reconNet.angles:
+        res1 = (np.sin(np.pi / 4 * beta / (gamma - alphas))) ** 2
+        res2 = (np.sin(np.pi / 4 * (np.pi + 2 * gamma - beta) / (gamma + alphas))) ** 2
+        i1 = np.where(beta < 2 * gamma - 2 * alphas)[0]
+        i2 = np.where(beta <= np.pi - 2 * alphas)[0]
+        w = res2
+        w[i2] = 1
+        w[i1] = res1[i1]
+        weights.append(w)
+    return np.transpose(np.array(weights))[np.newaxis, ..., np.newaxis]
+
+
+def RiessWeighting(reconNet, sigma=30, theta=10 * np.pi / 180):
+    """Riess short-scan weights (python/ReconNet_no_tf.py:665-693), shape [1, nu, nview, 1]."""
+    import scipy.ndimage
+
+    gamma = (reconNet.angles[-1] - np.pi) / 2
+    alphas = ((np.arange(reconNet.nu) - (reconNet.nu - 1) / 2) - reconNet.off_a) * reconNet.da
+    weights = []
+    for beta in reconNet.angles:
+        w = np.ones([reconNet.nu], np.float32)
+        res1 = (np.sin(np.pi / 4 * beta / (gamma - alphas))) ** 2
+        res2 = (np.sin(np.pi / 4 * (np.pi + 2 * gamma - beta) / (gamma + alphas))) ** 2
+        i1 = np.where(beta < 2 * gamma - 2 * alphas)[0]
+        i2 = np.where(beta < -2 * gamma + 2 * alphas)[0]
+        i3 = np.where(beta > np.pi - 2 * alphas)[0]
+        i4 = np.where(beta > np.pi + 2 * gamma + 2 * alphas)[0]
+        w[i4] = 2 - res2[i4]
+        w[i3] = res2[i3]
+        w[i2] = 2 - res1[i2]
+        w[i1] = res1[i1]
+        ws = scipy.ndimage.gaussian_filter1d(w, sigma, mode="nearest")
+        ind = np.where(np.all((beta > theta, beta < np.pi + 2 * gamma - theta)))
+        ws[ind] = w[ind]
+        weights.append(ws)
+    return np.transpose(np.array(weights))[np.newaxis, ..., np.newaxis]

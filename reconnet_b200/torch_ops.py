@@ -1,0 +1,240 @@
+"""PyTorch-facing device API: plans over CUDA tensors and autograd.
+
+``FanPlan`` owns a native ``rn_fan_plan`` (geometry tables + scratch) and runs
+the sm_100a kernels on the caller's current CUDA stream with the tensors'
+device pointers.  ``FanProjectFn`` mirrors the reference's TF op + registered
+gradient pair (ReconNet4D/zOpsReconNet.cc:26-82, python/ReconNet.py:773-800):
+forward = DD forward projection, backward = the matched (exact-transpose)
+backprojection.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+@dataclass
+class FanGeometry:
+    """Fan-beam geometry; field meaning follows Projector (Projector.h:10-37).
+
+    ``da`` is the angular detector pitch in radians (du_mm / dsd)."""
+    nx: int = 512
+    ny: int = 512
+    nz: int = 1
+    dx: float = 1.0
+    dy: float = 1.0
+    dz: float = 1.0
+    nu: int = 736
+    nv: int = 1
+    da: float = 1.2858 / 1085.6
+    dv: float = 1.0
+    off_a: float = 0.0
+    off_v: float = 0.0
+    dsd: float = 1085.6
+    dso: float = 595.0
+    cx: float = 0.0
+    cy: float = 0.0
+    cz: float = 0.0
+
+    def native(self, nbatches: int, nchannels: int, nview: int) -> N.RnFanGeom:
+        g = N.RnFanGeom()
+        g.nBatches, g.nChannels = int(nbatches), int(nchannels)
+        g.nx, g.ny, g.nz = int(self.nx), int(self.ny), int(self.nz)
+        g.dx, g.dy, g.dz = float(self.dx), float(self.dy), float(self.dz)
+        g.cx, g.cy, g.cz = float(self.cx), float(self.cy), float(self.cz)
+        g.nu, g.nview, g.nv = int(self.nu), int(nview), int(self.nv)
+        g.du, g.dv = float(self.da), float(self.dv)
+        g.off_u, g.off_v = float(self.off_a), float(self.off_v)
+        g.dsd, g.dso = float(self.dsd), float(self.dso)
+        return g
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _dev_ptr(t: torch.Tensor) -> int:
+    if not t.is_cuda:
+        raise ValueError("reconnet_b200 device API needs CUDA tensors")
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise ValueError("tensors must be contiguous float32")
+    return t.data_ptr()
+
+
+class FanPlan:
+    """Native plan for a batch of fan-beam problems.
+
+    Reference layout (``nview_per_slice`` is None): image ``[B, nx, ny, nz, C]``,
+    sinogram ``[B, nu, nview, nv, C]``, one angle list.
+
+    Ragged layout: ``nbatches`` independent ``[nx, ny]`` slices; slice ``s`` has
+    ``nview_per_slice[s]`` views; the sinogram is packed as the concatenation
+    of per-slice ``[nu, nview_s]`` blocks (a flat tensor)."""
+
+    def __init__(self, geom: FanGeometry, angles, nbatches: int = 1, nchannels: int = 1,
+                 nview_per_slice: Optional[Sequence[int]] = None, device=None):
+        self.geom = geom
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.angles = np.ascontiguousarray(np.asarray(angles, np.float32).ravel())
+        self.nbatches, self.nchannels = int(nbatches), int(nchannels)
+        self.ragged = nview_per_slice is not None
+        self._plan = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = _stream_ptr(self.device)
+            aptr = self.angles.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+            if self.ragged:
+                nvs = np.ascontiguousarray(np.asarray(nview_per_slice, np.int32))
+                if nvs.sum() != self.angles.size:
+                    raise ValueError("angles must hold sum(nview_per_slice) entries")
+                self.nview_per_slice = nvs
+                g = geom.native(self.nbatches, 1, int(nvs.sum()))
+                g.nz = g.nv = 1
+                N.check(N.lib.rn_fan_plan_create_ragged(ctypes.byref(self._plan), ctypes.byref(g),
+                                                        nvs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), aptr, st))
+                self.img_shape = (self.nbatches, geom.nx, geom.ny)
+                self.sino_shape = (int(nvs.sum()) * geom.nu,)
+            else:
+                self.nview = self.angles.size
+                g = geom.native(self.nbatches, self.nchannels, self.nview)
+                N.check(N.lib.rn_fan_plan_create(ctypes.byref(self._plan), ctypes.byref(g), aptr, st))
+                self.img_shape = (self.nbatches, geom.nx, geom.ny, geom.nz, self.nchannels)
+                self.sino_shape = (self.nbatches, geom.nu, self.nview, geom.nv, self.nchannels)
+        self.total_views = int(N.lib.rn_fan_plan_total_views(self._plan))
+
+    def __del__(self):
+        p = getattr(self, "_plan", None)
+        if p is not None and p.value:
+            try:
+                N.lib.rn_fan_plan_destroy(p)
+            except Exception:
+                pass
+            self._plan = ctypes.c_void_p()
+
+    # updates per call, the unit of the Gray/s metric: ray-line (FP) and
+    # pixel-view (BP) footprint integrations
+    def fp_updates(self) -> int:
+        g = self.geom
+        if self.ragged:
+            return int(self.total_views) * g.nu * g.ny
+        return self.nbatches * self.nchannels * g.nv * self.nview * g.nu * g.ny
+
+    def bp_updates(self) -> int:
+        g = self.geom
+        if self.ragged:
+            return int(self.total_views) * g.nx * g.ny
+        return self.nbatches * self.nchannels * g.nz * self.nview * g.nx * g.ny
+
+    def project(self, img: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if tuple(img.shape) != self.img_shape:
+            raise ValueError(f"image shape {tuple(img.shape)} != {self.img_shape}")
+        if out is None:
+            out = torch.empty(self.sino_shape, dtype=torch.float32, device=img.device)
+        N.check(N.lib.rn_fan_project(self._plan, _dev_ptr(out), _dev_ptr(img), _stream_ptr(img.device)))
+        return out
+
+    def backproject(self, sino: torch.Tensor, type_projector: int = N.RN_TYPE_MATCHED,
+                    out: Optional[torch.Tensor] = None, accumulate: bool = False) -> torch.Tensor:
+        if tuple(sino.shape) != self.sino_shape:
+            raise ValueError(f"sinogram shape {tuple(sino.shape)} != {self.sino_shape}")
+        if out is None:
+            out = torch.empty(self.img_shape, dtype=torch.float32, device=sino.device)
+        N.check(N.lib.rn_fan_backproject(self._plan, _dev_ptr(out), _dev_ptr(sino), int(type_projector),
+                                         int(bool(accumulate)), _stream_ptr(sino.device)))
+        return out
+
+    KERNEL_KINDS = ("lines", "fp", "tables", "bp", "other")
+
+    def set_timing(self, enable: bool) -> None:
+        """Bracket every kernel launch with CUDA events (for per-kernel timing)."""
+        N.check(N.lib.rn_fan_plan_set_timing(self._plan, int(bool(enable))))
+
+    def read_timing(self):
+        """-> ({kind: (total_ms, launches)}, total kernels launched by this plan)."""
+        n = len(self.KERNEL_KINDS)
+        ms = (ctypes.c_float * n)()
+        cnt = (ctypes.c_int * n)()
+        launches = ctypes.c_longlong()
+        N.check(N.lib.rn_fan_plan_read_timing(self._plan, ms, cnt, n, ctypes.byref(launches)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_KINDS)}, int(launches.value)
+
+    def launches(self) -> int:
+        """Total number of kernels this plan has launched."""
+        launches = ctypes.c_longlong()
+        N.check(N.lib.rn_fan_plan_read_timing(self._plan, None, None, 0, ctypes.byref(launches)))
+        return launches.value
+
+    def check(self) -> None:
+        """Synchronise and raise if a device-side bounded wait gave up."""
+        N.check(N.lib.rn_fan_plan_check(self._plan, _stream_ptr(self.device)))
+
+    def sqs_update(self, x_out, x_in, prj_s, w_s, norm_img, lam=1.0, beta=0.0, n_subsets=1,
+                   lb=None, ub=None, type_projector=N.RN_TYPE_MATCHED):
+        """One OS-SQS subset step on every slice (this plan = the subset's views)."""
+        lb = float(np.finfo(np.float32).min) if lb is None else float(lb)
+        ub = float(np.finfo(np.float32).max) if ub is None else float(ub)
+        N.check(N.lib.rn_fan_sqs_update(self._plan, _dev_ptr(x_out), _dev_ptr(x_in), _dev_ptr(prj_s),
+                                        _dev_ptr(w_s), _dev_ptr(norm_img), float(lam), float(beta),
+                                        int(n_subsets), lb, ub, int(type_projector),
+                                        _stream_ptr(x_in.device)))
+        return x_out
+
+
+class FanProjectFn(torch.autograd.Function):
+    """y = A x with dL/dx = A^T dL/dy (A^T = matched backprojection)."""
+
+    @staticmethod
+    def forward(ctx, img, plan: FanPlan):
+        ctx.plan = plan
+        return plan.project(img.contiguous())
+
+    @staticmethod
+    def backward(ctx, gy):
+        return ctx.plan.backproject(gy.contiguous(), N.RN_TYPE_MATCHED), None
+
+
+class FanBackprojectFn(torch.autograd.Function):
+    """x = A^T y (matched) with dL/dy = A dL/dx."""
+
+    @staticmethod
+    def forward(ctx, sino, plan: FanPlan):
+        ctx.plan = plan
+        return plan.backproject(sino.contiguous(), N.RN_TYPE_MATCHED)
+
+    @staticmethod
+    def backward(ctx, gx):
+        return ctx.plan.project(gx.contiguous()), None
+
+
+def fan_project(img: torch.Tensor, plan: FanPlan) -> torch.Tensor:
+    return FanProjectFn.apply(img, plan)
+
+
+def fan_backproject(sino: torch.Tensor, plan: FanPlan) -> torch.Tensor:
+    return FanBackprojectFn.apply(sino, plan)
+
+
+def filter_sino(sino: torch.Tensor, geom: FanGeometry, type_filter: int = 0, fan: bool = True) -> torch.Tensor:
+    """Ramp filter (cFilterFan::Filter, Filter.cu:216) on a [B, nu, nview, nv, C] CUDA tensor."""
+    out = torch.empty_like(sino)
+    B, nu, nview, nv, C = sino.shape
+    N.check(N.lib.rn_filter(_dev_ptr(out), _dev_ptr(sino), B, C, nu, nview, nv, float(geom.da),
+                            float(geom.off_a), float(geom.dsd), float(geom.dso), int(type_filter), int(bool(fan)),
+                            _stream_ptr(sino.device)))
+    return out
+
+
+def tv_sqs(img: torch.Tensor, want_tv: bool = True):
+    """TV surrogate terms of a [S, nx, ny] CUDA tensor -> (grad, norm, tv[S] float64)."""
+    S, nx, ny = img.shape
+    grad = torch.empty_like(img)
+    norm = torch.empty_like(img)
+    tv = torch.empty(S, dtype=torch.float64, device=img.device) if want_tv else None
+    N.check(N.lib.rn_tv_sqs(_dev_ptr(grad), _dev_ptr(norm), tv.data_ptr() if tv is not None else None,
+                            _dev_ptr(img), S, nx, ny, _stream_ptr(img.device)))
+    return grad, norm, tv

@@ -1,0 +1,125 @@
+"""Generate golden vectors from the reference's own CUDA kernels.
+
+Runs on a GPU machine: loads ``oracle/_ref/libreconnet_ref.so`` (the
+reference's ReconNet4D_no_tf sources compiled by ``make -C oracle ref``) and
+calls its C entry points through ctypes exactly as python/ReconNet_no_tf.py
+does, on small seeded inputs.  Writes ``tests/golden/ref_*.npz`` (inputs,
+geometry and reference outputs); the CPU test suite checks the oracle against
+these files.
+
+    python tests/golden/make_golden.py [outdir]
+"""
+import ctypes
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.path.join(ROOT, "oracle", "_ref", "libreconnet_ref.so")
+
+_f = ctypes.c_float
+_i = ctypes.c_int
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def load_ref(path=REF):
+    lib = ctypes.CDLL(path)
+    fan = [_fp, _fp, _fp] + [_i, _i, _i, _i, _i, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i]
+    lib.cDistanceDrivenFanProjection.argtypes = fan
+    lib.cDistanceDrivenFanBackprojection.argtypes = fan
+    filt = [_fp, _fp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i]
+    lib.cFilterFanFilter.argtypes = filt
+    lib.cFilterParallelFilter.argtypes = filt
+    lib.cTVSQS2D.argtypes = [_fp, _fp, _fp, _i, _i]
+    lib.cTVSQS2D.restype = _f
+    tomo = [_fp, _fp, _fp, _fp] + [_i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f]
+    lib.cDistanceDrivenTomoProjection.argtypes = tomo
+    lib.cDistanceDrivenTomoBackprojection.argtypes = tomo
+    return lib
+
+
+def p(a):
+    return a.ctypes.data_as(_fp)
+
+
+FAN_CASES = {
+    # name: geometry, batches, channels, nview
+    "fan2d": (dict(nx=48, ny=40, nz=1, dx=1.0, dy=1.1, dz=1.0, nu=64, nv=1, da=0.0025, dv=1.0, off_a=0.0,
+                   off_v=0.0, dsd=1085.6, dso=595.0), 1, 1, 72),
+    "fan_offsets": (dict(nx=40, ny=52, nz=1, dx=0.9, dy=1.0, dz=1.0, nu=64, nv=1, da=0.0025, dv=1.0, off_a=0.7,
+                         off_v=0.0, dsd=1085.6, dso=595.0), 1, 1, 45),
+    "fan_multislice": (dict(nx=48, ny=40, nz=3, dx=1.0, dy=1.1, dz=1.0, nu=64, nv=3, da=0.0025, dv=1.0, off_a=0.0,
+                            off_v=0.0, dsd=1085.6, dso=595.0), 2, 2, 36),
+    "fan_cfg0": (dict(nx=256, ny=256, nz=1, dx=1.0, dy=1.0, dz=1.0, nu=736, nv=1, da=1.2858 / 1085.6, dv=1.0,
+                      off_a=0.0, off_v=0.0, dsd=1085.6, dso=595.0), 1, 1, 45),
+}
+
+
+def fan_case(lib, name, rng):
+    g, B, C, nview = FAN_CASES[name]
+    ang = (np.arange(nview) * 2 * np.pi / nview).astype(np.float32)
+    img = rng.random((B, g["nx"], g["ny"], g["nz"], C)).astype(np.float32)
+    sino_in = rng.random((B, g["nu"], nview, g["nv"], C)).astype(np.float32)
+    args = lambda t: (B, C, g["nx"], g["ny"], g["nz"], g["dx"], g["dy"], g["dz"], g["nu"], nview, g["nv"], g["da"],
+                      g["dv"], g["off_a"], g["off_v"], g["dsd"], g["dso"], t)
+    fp = np.zeros((B, g["nu"], nview, g["nv"], C), np.float32)
+    lib.cDistanceDrivenFanProjection(p(fp), p(img), p(ang), *args(0))
+    out = dict(img=img, sino_in=sino_in, angles=ang, fp=fp, B=B, C=C, **{k: np.float64(v) for k, v in g.items()})
+    for t in (0, 1):
+        bp = np.zeros(img.shape, np.float32)
+        lib.cDistanceDrivenFanBackprojection(p(bp), p(sino_in), p(ang), *args(t))
+        out[f"bp{t}"] = bp
+    if g["nv"] == 1 and C == 1 and g["nx"] <= 64:
+        for tf in (0, 2):
+            fs = np.zeros(sino_in.shape, np.float32)
+            lib.cFilterFanFilter(p(fs), p(sino_in), B, C, g["nu"], nview, g["nv"], g["da"], g["dv"], g["off_a"],
+                                 g["off_v"], g["dsd"], g["dso"], tf, 1)
+            out[f"filt{tf}"] = fs
+    return out
+
+
+def tv_case(lib, rng):
+    img = (rng.random((1, 37, 29, 1)) * 0.02).astype(np.float32)
+    grad = np.zeros_like(img)
+    norm = np.zeros_like(img)
+    tv = lib.cTVSQS2D(p(grad), p(norm), p(img), 37, 29)
+    return dict(img=img, grad=grad, norm=norm, tv=np.float64(tv))
+
+
+def tomo_case(lib, rng):
+    nview = 5
+    dc = np.zeros((nview, 3), np.float32)
+    src = np.zeros((nview, 3), np.float32)
+    for k in range(nview):
+        a = (k - (nview - 1) / 2) * 0.15
+        src[k] = (600 * math.sin(a), 10.0, 600 * math.cos(a))
+        dc[k] = (0.0, 0.0, -40.0)
+    g = dict(dx=1.0, dy=1.0, dz=2.0, cx=0.0, cy=0.0, cz=0.0, du=1.5, dv=1.5, off_u=0.2, off_v=-0.3)
+    nx, ny, nz, nu, nv = 16, 14, 6, 24, 20
+    img = rng.random((1, nx, ny, nz, 1)).astype(np.float32)
+    prj_in = rng.random((1, nu, nview, nv, 1)).astype(np.float32)
+    targs = (1, 1, nx, ny, nz, g["dx"], g["dy"], g["dz"], g["cx"], g["cy"], g["cz"], nu, nview, nv, g["du"],
+             g["dv"], g["off_u"], g["off_v"])
+    fp = np.zeros((1, nu, nview, nv, 1), np.float32)
+    lib.cDistanceDrivenTomoProjection(p(fp), p(img), p(dc), p(src), *targs)
+    bp = np.zeros(img.shape, np.float32)
+    lib.cDistanceDrivenTomoBackprojection(p(bp), p(prj_in), p(dc), p(src), *targs)
+    return dict(img=img, prj_in=prj_in, det_center=dc, src=src, fp=fp, bp=bp, nu=nu, nv=nv,
+                **{k: np.float64(v) for k, v in g.items()})
+
+
+def main(outdir=HERE):
+    lib = load_ref()
+    rng = np.random.default_rng(20240601)
+    for name in FAN_CASES:
+        np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **fan_case(lib, name, rng))
+    np.savez_compressed(os.path.join(outdir, "ref_tv.npz"), **tv_case(lib, rng))
+    np.savez_compressed(os.path.join(outdir, "ref_tomo.npz"), **tomo_case(lib, rng))
+    print("golden vectors written to", outdir)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE)

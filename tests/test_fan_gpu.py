@@ -1,0 +1,286 @@
+"""GPU parity of the sm_100a DD fan kernels against the FP64 oracle, through the
+C ABI (device API via FanPlan, host API via the reference-named functions).
+
+Tolerance: relative L2 <= 1e-5 for FP32 projections / backprojections against
+the FP64 oracle, and |<Ax,y> - <x,A^T y>| / |<Ax,y>| <= 1e-5 for the matched
+pair (FP64 accumulation of the FP32 results)."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2, small_fan, to_geometry
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+CASES = {
+    "2d": (dict(), 1, 1, 72),
+    "offsets": (dict(off_a=0.7, nx=40, ny=52, dx=0.9, dy=1.0), 1, 1, 45),
+    "multislice": (dict(nz=3, nv=3), 2, 2, 36),
+    "zmix": (dict(nz=3, nv=4, dz=1.5, dv=1.0, off_v=0.3), 1, 2, 30),
+    "few_views": (dict(nu=17, da=0.009), 1, 1, 5),
+}
+
+
+def _setup(name, rng):
+    import torch
+    from reconnet_b200.torch_ops import FanPlan
+    kw, B, C, nview = CASES[name]
+    g = small_fan(**kw)
+    ang = (np.arange(nview) * 2 * np.pi / nview + 0.01 * (name == "few_views")).astype(np.float32)
+    plan = FanPlan(to_geometry(g), ang, nbatches=B, nchannels=C)
+    x = rng.random((B, g.nx, g.ny, g.nz, C)).astype(np.float32)
+    y = rng.random((B, g.nu, nview, g.nv, C)).astype(np.float32)
+    return g, ang, plan, x, y, torch
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fp_matches_oracle(name, rng):
+    from oracle import oracle as O
+    g, ang, plan, x, y, torch = _setup(name, rng)
+    got = plan.project(torch.from_numpy(x).cuda()).cpu().numpy()
+    plan.check()
+    ref = O.fan_fp(x, ang, g, g.nu, g.nv)
+    assert rel_l2(got, ref) <= TOL
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("ptype", [0, 1, 2])
+def test_bp_matches_oracle(name, ptype, rng):
+    from oracle import oracle as O
+    g, ang, plan, x, y, torch = _setup(name, rng)
+    got = plan.backproject(torch.from_numpy(y).cuda(), ptype).cpu().numpy()
+    plan.check()
+    ref = O.fan_bp(y, ang, g, (g.nx, g.ny, g.nz), ptype)
+    assert rel_l2(got, ref) <= TOL
+
+
+def test_host_api_matches_device_api(rng):
+    from reconnet_b200.reconnet import ReconNet
+    g, ang, plan, x, y, torch = _setup("multislice", rng)
+    rn = ReconNet()
+    for k in ("nx", "ny", "nz", "dx", "dy", "dz", "nu", "nv", "da", "dv", "off_a", "off_v", "dsd", "dso"):
+        setattr(rn, k, getattr(g, k))
+    fp_h = rn.cDDFanProjection4d(x, ang)
+    fp_d = plan.project(torch.from_numpy(x).cuda()).cpu().numpy()
+    np.testing.assert_array_equal(fp_h, fp_d)
+    for t in (0, 1, 2):
+        bp_h = rn.cDDFanBackprojection4d(y, ang, type_projector=t)
+        bp_d = plan.backproject(torch.from_numpy(y).cuda(), t).cpu().numpy()
+        np.testing.assert_array_equal(bp_h, bp_d)
+
+
+def test_accumulate_mode(rng):
+    g, ang, plan, x, y, torch = _setup("2d", rng)
+    yd = torch.from_numpy(y).cuda()
+    base = torch.from_numpy(x).cuda()
+    ref = base + plan.backproject(yd, 2)
+    out = base.clone()
+    plan.backproject(yd, 2, out=out, accumulate=True)
+    assert torch.allclose(out, ref, rtol=0, atol=0)
+
+
+def test_ragged_plan_matches_per_slice_plans(rng):
+    import torch
+    from reconnet_b200.torch_ops import FanPlan
+    g = small_fan()
+    counts = [31, 47, 20]
+    angs = [(np.arange(n) * 2 * np.pi / n).astype(np.float32) for n in counts]
+    rag = FanPlan(to_geometry(g), np.concatenate(angs), nbatches=3, nview_per_slice=counts)
+    x = rng.random((3, g.nx, g.ny)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    p = rag.project(xd)
+    y = torch.from_numpy(rng.random(p.shape).astype(np.float32)).cuda()
+    b = {t: rag.backproject(y, t) for t in (0, 1, 2)}
+    off = 0
+    for s, n in enumerate(counts):
+        one = FanPlan(to_geometry(g), angs[s])
+        ps = one.project(xd[s].reshape(1, g.nx, g.ny, 1, 1).contiguous())
+        seg = p[off * g.nu:(off + n) * g.nu].reshape(1, g.nu, n, 1, 1)
+        assert torch.equal(ps, seg)
+        ys = y[off * g.nu:(off + n) * g.nu].reshape(1, g.nu, n, 1, 1).contiguous()
+        for t in (0, 1, 2):
+            assert torch.equal(one.backproject(ys, t)[0, :, :, 0, 0], b[t][s])
+        off += n
+
+
+@pytest.mark.parametrize("cfg", ["cfg0", "cfg1"])
+def test_adjoint_full_size(cfg, rng):
+    """<Ax, y> = <x, A^T y> at the workload sizes (phantom x, random y)."""
+    import torch
+    from reconnet_b200 import phantom as P
+    from reconnet_b200.torch_ops import FanPlan
+    geom = P.geom_cfg0() if cfg == "cfg0" else P.geom_cfg1()
+    nview = 720 if cfg == "cfg0" else 864
+    plan = FanPlan(geom, P.uniform_angles(nview))
+    x = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
+    xd = torch.from_numpy(x).cuda()
+    Ax = plan.project(xd)
+    yd = torch.rand_like(Ax)
+    Aty = plan.backproject(yd, 2)
+    plan.check()
+    lhs = float((Ax.double() * yd.double()).sum())
+    rhs = float((xd.double() * Aty.double()).sum())
+    assert abs(lhs - rhs) / abs(lhs) <= TOL
+
+
+def test_cfg0_full_size_fp_bp_vs_oracle(rng):
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200 import phantom as P
+    from reconnet_b200.torch_ops import FanPlan
+    geom = P.geom_cfg0()
+    ang = P.uniform_angles(720)
+    plan = FanPlan(geom, ang)
+    x = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
+    got = plan.project(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref = O.fan_fp(x, ang, geom, geom.nu, 1)
+    assert rel_l2(got, ref) <= TOL
+    y = ref.astype(np.float32)
+    for t in (0, 2):
+        bp = plan.backproject(torch.from_numpy(y).cuda(), t).cpu().numpy()
+        assert rel_l2(bp, O.fan_bp(y, ang, geom, (geom.nx, geom.ny, 1), t)) <= TOL
+
+
+def test_cfg1_slice_fp_vs_oracle(rng):
+    """One full 512x512, 888-channel slice (the batched workload's slice)."""
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200 import phantom as P
+    from reconnet_b200.torch_ops import FanPlan
+    geom = P.geom_cfg1()
+    ang = P.uniform_angles(600)[::4].copy()
+    plan = FanPlan(geom, ang)
+    x = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
+    got = plan.project(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref = O.fan_fp(x, ang, geom, geom.nu, 1)
+    assert rel_l2(got, ref) <= TOL
+    y = ref.astype(np.float32)
+    bp = plan.backproject(torch.from_numpy(y).cuda(), 2).cpu().numpy()
+    assert rel_l2(bp, O.fan_bp(y, ang, geom, (geom.nx, geom.ny, 1), 2)) <= TOL
+
+
+@pytest.mark.parametrize("tf", [0, 1, 2, 3])
+def test_filter_matches_oracle(tf, rng):
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200.torch_ops import filter_sino
+    g = small_fan(nu=97, da=0.003, off_a=0.4)
+    s = rng.random((2, g.nu, 50, 2, 1)).astype(np.float32)
+    got = filter_sino(torch.from_numpy(s).cuda(), to_geometry(g), tf).cpu().numpy()
+    assert rel_l2(got, O.filter_sino(s, g, tf)) <= TOL
+    got_p = filter_sino(torch.from_numpy(s).cuda(), to_geometry(g), tf, fan=False).cpu().numpy()
+    assert rel_l2(got_p, O.filter_sino(s, g, tf, fan=False)) <= TOL
+
+
+def test_filter_host_api_full_size(rng):
+    from oracle import oracle as O
+    from reconnet_b200 import phantom as P
+    from reconnet_b200.reconnet import ReconNet
+    rn = ReconNet()
+    rn.nu, rn.da = 736, 1.2858 / 1085.6
+    s = rng.random((1, 736, 720, 1)).astype(np.float32)
+    got = rn.cFilter3d(s, 2)
+    ref = O.filter_sino(s[..., None, :], P.geom_cfg0(), 2)[..., 0, :]
+    assert rel_l2(got, ref) <= TOL
+
+
+def test_tv_matches_oracle(rng):
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200.reconnet import ReconNet
+    from reconnet_b200.torch_ops import tv_sqs
+    img = rng.random((3, 33, 41)).astype(np.float32) * 0.02
+    grad, norm, tv = tv_sqs(torch.from_numpy(img).cuda())
+    for s in range(3):
+        g2, n2, t2 = O.tv_sqs(img[s])
+        assert rel_l2(grad[s].cpu().numpy(), g2) <= TOL
+        assert rel_l2(norm[s].cpu().numpy(), n2) <= TOL
+        assert abs(float(tv[s]) - t2) / t2 <= TOL
+    gh, nh, th = ReconNet().cTVSQS2d(img[0][None, :, :, None])
+    g2, n2, t2 = O.tv_sqs(img[0])
+    assert rel_l2(gh[0, :, :, 0], g2) <= TOL and abs(th - t2) / t2 <= TOL
+
+
+@pytest.mark.parametrize("beta,ptype", [(0.0, 2), (0.02, 2), (0.0, 0)])
+def test_sqs_update_matches_oracle(beta, ptype, rng):
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200.torch_ops import FanPlan
+    g = small_fan()
+    nview, M = 48, 4
+    ang = (np.arange(nview) * 2 * np.pi / nview).astype(np.float32)
+    x = (rng.random((g.nx, g.ny)) * 0.02).astype(np.float32)
+    truth = (rng.random((g.nx, g.ny)) * 0.02).astype(np.float32)
+    sino = O.fan_fp(truth[None, :, :, None, None], ang, g, g.nu, 1)[0, :, :, 0, 0].astype(np.float32)
+    w = (0.5 + rng.random(sino.shape)).astype(np.float32)
+    norm = O.fan_bp((O.fan_fp(np.ones((1, g.nx, g.ny, 1, 1), np.float32), ang, g, g.nu, 1)[0, :, :, 0, 0] * w)
+                    .astype(np.float32)[None, :, :, None, None], ang, g, (g.nx, g.ny, 1), ptype)[0, :, :, 0, 0]
+    norm = norm.astype(np.float32)
+    views = np.arange(1, nview, M)
+    ref = O.sqs_subset_update(x, sino, w, norm, ang, views, g, M, lam=0.9, beta=beta, lb=0.0, ub=1.0, bp_type=ptype)
+    sp = FanPlan(to_geometry(g), ang[views])
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    xo = torch.empty((1, g.nx, g.ny, 1, 1), device="cuda")
+    sp.sqs_update(xo, dev(x[None, :, :, None, None]), dev(sino[:, views][None, :, :, None, None]),
+                  dev(w[:, views][None, :, :, None, None]), dev(norm[None, :, :, None, None]), lam=0.9, beta=beta,
+                  n_subsets=M, lb=0.0, ub=1.0, type_projector=ptype)
+    assert rel_l2(xo.cpu().numpy()[0, :, :, 0, 0], ref) <= TOL
+
+
+def test_cossqs_host_matches_oracle_loop(rng):
+    """cOSSQS (ossqs.cu:12) with contiguous subsets and the corrected tail."""
+    from oracle import oracle as O
+    from reconnet_b200.reconnet import ReconNet
+    g = small_fan()
+    nview, M = 50, 4            # 50 = 13+13+13+11: the tail subset has 11 views
+    ang = (np.arange(nview) * 2 * np.pi / nview).astype(np.float32)
+    truth = (rng.random((g.nx, g.ny)) * 0.02).astype(np.float32)
+    sino = O.fan_fp(truth[None, :, :, None, None], ang, g, g.nu, 1)[0, :, :, 0, 0].astype(np.float32)
+    w = np.ones_like(sino)
+    norm = O.fan_bp(O.fan_fp(np.ones((1, g.nx, g.ny, 1, 1), np.float32), ang, g, g.nu, 1).astype(np.float32), ang, g,
+                    (g.nx, g.ny, 1), 2)[0, :, :, 0, 0].astype(np.float32)
+    x = np.zeros((g.nx, g.ny), np.float32)
+    nps = int(np.ceil(nview / M))
+    ref = x.astype(np.float64)
+    for k in range(M):
+        views = np.arange(k * nps, min(nview, (k + 1) * nps))
+        ref = O.sqs_subset_update(ref.astype(np.float32), sino, w, norm, ang, views, g, M, bp_type=2)
+    rn = ReconNet()
+    for k in ("nx", "ny", "nz", "dx", "dy", "dz", "nu", "nv", "da", "dv", "off_a", "off_v", "dsd", "dso"):
+        setattr(rn, k, getattr(g, k))
+    got = rn.cDDFanOSSQS3d(M, x[None, :, :, None], sino[None, :, :, None], norm[None, :, :, None],
+                           w[None, :, :, None], ang, type_projector=2)[0, :, :, 0]
+    assert rel_l2(got, ref) <= 1e-4   # four chained steps
+
+
+def test_tomo_matches_oracle(rng):
+    from oracle import oracle as O
+    from reconnet_b200.reconnet import ReconNet
+    from test_oracle_cpu import _tomo_setup
+    g, dc, src = _tomo_setup(rng)
+    rn = ReconNet()
+    rn.nx, rn.ny, rn.nz, rn.nu, rn.nv = 16, 14, 6, 24, 20
+    for k in ("dx", "dy", "dz", "cx", "cy", "cz", "du", "dv", "off_u", "off_v"):
+        setattr(rn, k, getattr(g, k))
+    img = rng.random((2, 16, 14, 6, 1)).astype(np.float32)
+    got = rn.cDDTomoProjection4d(img, dc, src)
+    assert rel_l2(got, O.tomo_fp(img, dc, src, g, 24, 20)) <= TOL
+    prj = rng.random(got.shape).astype(np.float32)
+    gb = rn.cDDTomoBackprojection4d(prj, dc, src)
+    assert rel_l2(gb, O.tomo_bp(prj, dc, src, g, (16, 14, 6))) <= TOL
+
+
+def test_invalid_arguments_raise():
+    import torch
+    from reconnet_b200 import _native as N
+    from reconnet_b200.torch_ops import FanPlan
+    g = small_fan()
+    plan = FanPlan(to_geometry(g), np.zeros(4, np.float32))
+    y = torch.zeros(plan.sino_shape, device="cuda")
+    with pytest.raises(N.ReconNetError):
+        plan.backproject(y, 7)
+    with pytest.raises(ValueError):
+        plan.project(torch.zeros((1, 3, 3, 1, 1), device="cuda"))
+    with pytest.raises(N.ReconNetError):   # source inside the image
+        FanPlan(to_geometry(small_fan(dso=20.0, dsd=40.0)), np.zeros(4, np.float32))
