@@ -145,38 +145,29 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_sample(geom, counts, angles, target_s=12.0):
-    """FP32 OpenMP port of the oracle on one slice of the workload, with the
-    view subset sized for about `target_s` seconds; returns (Gray/s, threads, desc)."""
+def cpu_baseline_sample(geom, counts, angles, imgs, target_s=12.0):
+    """FP32 OpenMP port of the oracle on whole slices of the workload (all of
+    each slice's views, FP + matched BP), slice after slice until about
+    `target_s` seconds; returns (Gray/s, threads, description)."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
-    n0 = int(counts[0])
-    ang0 = angles[:n0]
-    img = workload_first_image(geom)
-
-    def run(nv):
-        sel = ang0[:: max(1, n0 // nv)][:nv].copy()
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    upd, dt, done = 0, 0.0, 0
+    for s in range(len(counts)):
+        sel = np.ascontiguousarray(angles[offs[s]:offs[s + 1]])
+        img = imgs[s][None, :, :, None, None]
         t0 = time.perf_counter()
         p = O.fan_fp(img, sel, geom, geom.nu, 1, dtype=np.float32)
         O.fan_bp(p, sel, geom, (geom.nx, geom.ny, 1), 2, dtype=np.float32)
-        dt = time.perf_counter() - t0
-        upd = sel.size * (geom.nu * geom.ny + geom.nx * geom.ny)
-        return upd, dt, sel.size
-
-    upd, dt, nv = run(4)
-    per_view = dt / max(nv, 1)
-    nv = int(max(4, min(n0, target_s / max(per_view, 1e-6))))
-    upd, dt, nv = run(nv)
-    desc = (f"1 slice 512x512, 888 ch, {nv} of its {n0} views: FP + matched BP, FP32 OpenMP port of the "
+        dt += time.perf_counter() - t0
+        upd += sel.size * (geom.nu * geom.ny + geom.nx * geom.ny)
+        done += 1
+        if dt >= target_s:
+            break
+    desc = (f"{done} of the {len(counts)} slices (all their views), FP + matched BP, FP32 OpenMP port of the "
             f"oracle, {threads} threads, {dt:.1f} s")
     return upd / dt / 1e9, threads, desc
-
-
-def workload_first_image(geom):
-    from reconnet_b200 import phantom as P
-    rng = np.random.default_rng(100)
-    return P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
 
 
 def run_reference(args):
@@ -373,7 +364,7 @@ def run_b200(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, desc = cpu_baseline_sample(geom, counts, angles)
+        v, cores, desc = cpu_baseline_sample(geom, counts, angles, imgs)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
 
     if rank == 0:

@@ -188,7 +188,10 @@ int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x
 /* Tomosynthesis DD on device pointers (same arguments as the reference-named
  * host functions above plus a caller-provided FP64 scratch d_sat whose size
  * rn_tomo_sat_bytes reports: fp_bytes for projection, bp_bytes for
- * backprojection).  detCenter / src are [nview][3] device arrays. */
+ * backprojection).  detCenter / src are [nview][3] device arrays.
+ * weightAllViews = 0 reproduces cDistanceDrivenTomoBackprojection, whose
+ * length pre-weight reaches view 0 only (its launch grid holds one row of
+ * views, ReconNet4D/DistanceDriven3D.cu:612-621); 1 weights every view. */
 int rn_tomo_sat_bytes(int nx, int ny, int nz, int nu, int nview, int nv, size_t* fp_bytes, size_t* bp_bytes);
 int rn_tomo_project(float* d_prj, const float* d_img, const float* d_detCenter, const float* d_src, double* d_sat,
                     int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, float cx,
@@ -197,7 +200,7 @@ int rn_tomo_project(float* d_prj, const float* d_img, const float* d_detCenter, 
 int rn_tomo_backproject(float* d_img, const float* d_prj, const float* d_detCenter, const float* d_src, double* d_sat,
                         int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, float cx,
                         float cy, float cz, int nu, int nview, int nv, float du, float dv, float off_u, float off_v,
-                        void* stream);
+                        int weightAllViews, void* stream);
 
 #ifdef __cplusplus
 }

@@ -50,10 +50,11 @@ inline int64_t prj_index(const Fan& g, int b, int iu, int iview, int iv, int c) 
 }
 
 // View split of DistanceDriven.cu:299-312 (|cos| > |sin| -> rays run along y,
-// the "X" kernels integrate along x on every image row).
+// the "X" kernels integrate along x on every image row).  Evaluated in float
+// with the host libm, as the reference does: at angles such as float(3pi/4)
+// the two rounded values tie and the view goes to the Y class.
 inline bool x_class(float deg) {
-    double d = (double)deg;
-    return std::fabs(std::cos(d)) > std::fabs(std::sin(d));
+    return std::fabs(std::cos(deg)) > std::fabs(std::sin(deg));
 }
 
 // Channel angle of detector cell iu, DistanceDriven.cu:83.
@@ -594,8 +595,11 @@ void tomo_fp(T* prj, const float* img, const float* detCenter, const float* src,
         }
 }
 
+// weight_mode 0: as the reference, whose pre-weight launch
+// (DistanceDriven3D.cu:612-621) has a single row of views in its grid, so only
+// view 0 receives the length weight; 1: every view is weighted.
 template <typename T>
-void tomo_bp(T* img, const float* prj, const float* detCenter, const float* src, const Tomo& g) {
+void tomo_bp(T* img, const float* prj, const float* detCenter, const float* src, const Tomo& g, int weight_mode) {
     size_t nacc = (size_t)(g.nu + 1) * g.nview * (g.nv + 1);
     for (int b = 0; b < g.nb; b++)
         for (int c = 0; c < g.nc; c++) {
@@ -610,8 +614,9 @@ void tomo_bp(T* img, const float* prj, const float* detCenter, const float* src,
                         double u = (iu - g.off_u - (g.nu - 1) / 2.0) * g.du;
                         double v = (iv - g.off_v - (g.nv - 1) / 2.0) * g.dv;
                         double ddx = sp[0] - (dc[0] + u), ddy = sp[1] - (dc[1] + v), ddz = sp[2] - dc[2];
-                        T w = (T)prj[((((size_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + c] *
-                              (T)(g.dz / std::fabs(ddz) * std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz));
+                        T w = (T)prj[((((size_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + c];
+                        if (weight_mode == 1 || iview == 0)
+                            w *= (T)(g.dz / std::fabs(ddz) * std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz));
                         size_t o = ((size_t)(iu + 1) * g.nview + iview) * (g.nv + 1) + (iv + 1);
                         acc[o] = w + acc[((size_t)iu * g.nview + iview) * (g.nv + 1) + (iv + 1)] +
                                  acc[((size_t)(iu + 1) * g.nview + iview) * (g.nv + 1) + iv] -
@@ -738,8 +743,9 @@ double oracle_tv_sqs_f64(double* grad, double* norm, const float* img, int nx, i
 void oracle_tomo_fp_f64(double* prj, const float* img, const float* detCenter, const float* src, TOMO_ARGS) {
     tomo_fp<double>(prj, img, detCenter, src, make_tomo(TOMO_PASS));
 }
-void oracle_tomo_bp_f64(double* img, const float* prj, const float* detCenter, const float* src, TOMO_ARGS) {
-    tomo_bp<double>(img, prj, detCenter, src, make_tomo(TOMO_PASS));
+void oracle_tomo_bp_f64(double* img, const float* prj, const float* detCenter, const float* src, TOMO_ARGS,
+                        int weight_mode) {
+    tomo_bp<double>(img, prj, detCenter, src, make_tomo(TOMO_PASS), weight_mode);
 }
 
 }  // extern "C"

@@ -57,7 +57,7 @@ def lib():
         L.oracle_tv_sqs_f64.argtypes = [_dp, _dp, _fp, _i, _i]
         L.oracle_tv_sqs_f64.restype = ctypes.c_double
         L.oracle_tomo_fp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
-        L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
+        L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO + [_i]
         _lib = L
     return _lib
 
@@ -169,8 +169,11 @@ def tomo_fp(img, det_center, src, g, nu, nv):
     return out
 
 
-def tomo_bp(prj, det_center, src, g, img_shape):
-    """DistanceDrivenTomo::BackprojectionTomo (DistanceDriven3D.cu:409-663)."""
+def tomo_bp(prj, det_center, src, g, img_shape, weight_mode=0):
+    """DistanceDrivenTomo::BackprojectionTomo (DistanceDriven3D.cu:409-663).
+
+    weight_mode 0 reproduces the reference (length pre-weight on view 0 only,
+    DistanceDriven3D.cu:612-621); 1 weights every view."""
     prj = _f32(prj)
     dc = _f32(det_center)
     sp = _f32(src)
@@ -178,7 +181,7 @@ def tomo_bp(prj, det_center, src, g, img_shape):
     nx, ny, nz = img_shape
     out = np.zeros((B, nx, ny, nz, C), np.float64)
     lib().oracle_tomo_bp_f64(_ptr(out, ctypes.c_double), _ptr(prj, _f), _ptr(dc, _f), _ptr(sp, _f),
-                             *_tomo_args(g, out.shape, prj.shape))
+                             *_tomo_args(g, out.shape, prj.shape), int(weight_mode))
     return out
 
 

@@ -74,7 +74,7 @@ SIGNATURES = {
     "rn_tomo_sat_bytes": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_size_t),
                                ctypes.POINTER(ctypes.c_size_t)]),
     "rn_tomo_project": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),
-    "rn_tomo_backproject": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),
+    "rn_tomo_backproject": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_i, _vp]),
 }
 
 

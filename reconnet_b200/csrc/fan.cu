@@ -658,7 +658,10 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
             int v = gs.view_off + k;
             double th = (double)host_deg[v];
             double c = std::cos(th), s = std::sin(th);
-            int xc = std::fabs(c) > std::fabs(s) ? 1 : 0;
+            // class rule of the reference host code (DistanceDriven.cu:302), in
+            // float: ties of the rounded values go to the Y class
+            const float degf = host_deg[v];
+            int xc = std::fabs(std::cos(degf)) > std::fabs(std::sin(degf)) ? 1 : 0;
             double sx = (g.dso * s - g.cx) / g.dx + g.nx / 2.0;
             double sy = (-g.dso * c - g.cy) / g.dy + g.ny / 2.0;
             ViewGeo& q = vg[v];

@@ -119,9 +119,12 @@ __global__ void tomo_fp_kernel(float* __restrict__ prj, const double* __restrict
 }
 
 // Weighted (u, v) SAT per view, layout [view][u in 0..nu][v in 0..nv].
+// weight_all = 0 applies the length weight to view 0 only, as the reference's
+// pre-weight launch does (its grid has one row of views,
+// DistanceDriven3D.cu:612-621); 1 weights every view.
 __global__ void tomo_bp_sat_u(double* __restrict__ sat, const float* __restrict__ prj,
                               const float* __restrict__ detCenter, const float* __restrict__ src, TomoDims d, int b,
-                              int c) {
+                              int c, int weight_all) {
     // one thread per (view, v): prefix along u of the weighted projections
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.nview * d.nv) return;
@@ -137,7 +140,8 @@ __global__ void tomo_bp_sat_u(double* __restrict__ sat, const float* __restrict_
     for (int iu = 0; iu < d.nu; iu++) {
         float u = (iu - d.off_u - (d.nu - 1) / 2.0f) * d.du;
         double ddx = (double)sp[0] - (dc[0] + u), ddy = (double)sp[1] - (dc[1] + v), ddz = (double)sp[2] - dc[2];
-        double w = (double)d.dz / fabs(ddz) * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+        double w = (weight_all || view == 0) ? (double)d.dz / fabs(ddz) * sqrt(ddx * ddx + ddy * ddy + ddz * ddz)
+                                             : 1.0;
         acc += w * (double)prj[(long long)b * d.nu * d.nview * d.nv * d.nc +
                                ((long long)iu * d.nview + view) * d.nv * d.nc + (long long)iv * d.nc + c];
         base[(long long)(iu + 1) * (d.nv + 1)] = acc;
@@ -210,11 +214,12 @@ int tomo_project(float* d_prj, const float* d_img, const float* d_dc, const floa
 }
 
 int tomo_backproject(float* d_img, const float* d_prj, const float* d_dc, const float* d_src, const TomoDims& d,
-                     double* d_sat, cudaStream_t st) {
+                     double* d_sat, int weight_all, cudaStream_t st) {
     RN_TRY(tomo_validate(d));
     for (int b = 0; b < d.nb; b++)
         for (int c = 0; c < d.nc; c++) {
-            tomo_bp_sat_u<<<(d.nview * d.nv + 127) / 128, 128, 0, st>>>(d_sat, d_prj, d_dc, d_src, d, b, c);
+            tomo_bp_sat_u<<<(d.nview * d.nv + 127) / 128, 128, 0, st>>>(d_sat, d_prj, d_dc, d_src, d, b, c,
+                                                                          weight_all);
             tomo_bp_sat_v<<<(d.nview * (d.nu + 1) + 127) / 128, 128, 0, st>>>(d_sat, d);
             dim3 blk(32, 8);
             dim3 grd((d.nx + 31) / 32, (d.ny + 7) / 8, d.nz);
@@ -276,7 +281,7 @@ static int host_tomo(bool fp, float* out, const float* in, const float* dc, cons
     } else {
         RN_CUDA_TRY(cudaMemcpyAsync(dprj, in, np * 4, cudaMemcpyHostToDevice, st));
         RN_TRY(tomo_backproject(dimg, dprj, (float*)g_tomo.buf[2], (float*)g_tomo.buf[3], d, (double*)g_tomo.buf[4],
-                                st));
+                                0, st));
         RN_CUDA_TRY(cudaMemcpyAsync(out, dimg, ni * 4, cudaMemcpyDeviceToHost, st));
     }
     RN_CUDA_TRY(cudaStreamSynchronize(st));
@@ -310,13 +315,13 @@ int rn_tomo_project(float* d_prj, const float* d_img, const float* d_detCenter, 
 int rn_tomo_backproject(float* d_img, const float* d_prj, const float* d_detCenter, const float* d_src, double* d_sat,
                         int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, float cx,
                         float cy, float cz, int nu, int nview, int nv, float du, float dv, float off_u, float off_v,
-                        void* stream) {
+                        int weightAllViews, void* stream) {
     clear_error();
     if (!d_prj || !d_img || !d_detCenter || !d_src || !d_sat) return set_error(RN_ERR_ARG, "null argument");
     return tomo_backproject(d_img, d_prj, d_detCenter, d_src,
                             tomo_dims(nBatches, nChannels, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nview, nv, du, dv,
                                       off_u, off_v),
-                            d_sat, (cudaStream_t)stream);
+                            d_sat, weightAllViews ? 1 : 0, (cudaStream_t)stream);
 }
 
 void cDistanceDrivenTomoProjection(float* prj, const float* img, const float* detCenter, const float* src,

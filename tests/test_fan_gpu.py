@@ -268,7 +268,23 @@ def test_tomo_matches_oracle(rng):
     assert rel_l2(got, O.tomo_fp(img, dc, src, g, 24, 20)) <= TOL
     prj = rng.random(got.shape).astype(np.float32)
     gb = rn.cDDTomoBackprojection4d(prj, dc, src)
-    assert rel_l2(gb, O.tomo_bp(prj, dc, src, g, (16, 14, 6))) <= TOL
+    assert rel_l2(gb, O.tomo_bp(prj, dc, src, g, (16, 14, 6), 0)) <= TOL
+    # device API, both pre-weight modes
+    import ctypes
+    import torch
+    from reconnet_b200 import _native as N
+    fpb, bpb = ctypes.c_size_t(), ctypes.c_size_t()
+    N.lib.rn_tomo_sat_bytes(16, 14, 6, 24, 5, 20, ctypes.byref(fpb), ctypes.byref(bpb))
+    sat = torch.empty(max(fpb.value, bpb.value) // 8 + 1, dtype=torch.float64, device="cuda")
+    dprj = torch.from_numpy(prj).cuda()
+    ddc, dsrc = torch.from_numpy(dc).cuda(), torch.from_numpy(src).cuda()
+    for mode in (0, 1):
+        out = torch.empty((2, 16, 14, 6, 1), device="cuda")
+        N.check(N.lib.rn_tomo_backproject(out.data_ptr(), dprj.data_ptr(), ddc.data_ptr(), dsrc.data_ptr(),
+                                          sat.data_ptr(), 2, 1, 16, 14, 6, g.dx, g.dy, g.dz, g.cx, g.cy, g.cz, 24,
+                                          5, 20, g.du, g.dv, g.off_u, g.off_v, mode,
+                                          torch.cuda.current_stream().cuda_stream))
+        assert rel_l2(out.cpu().numpy(), O.tomo_bp(prj, dc, src, g, (16, 14, 6), mode)) <= TOL
 
 
 def test_invalid_arguments_raise():

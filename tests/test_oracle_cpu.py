@@ -37,9 +37,9 @@ def _direct_fan_fp(img2d, angles, g):
         return s
 
     for iv, th in enumerate(angles):
+        xcls = O.view_is_x(th)          # float rule of DistanceDriven.cu:302
         th = float(th)
         c, s = math.cos(th), math.sin(th)
-        xcls = abs(c) > abs(s)
         for iu in range(g.nu):
             a = (-(iu - (g.nu - 1) / 2) - g.off_a) * g.da
             src = (g.dso * s / g.dx + nx / 2, -g.dso * c / g.dy + ny / 2)
@@ -82,9 +82,9 @@ def _direct_bp_ref(sino, angles, g, fbp):
     nu, nview = sino.shape
     out = np.zeros((g.nx, g.ny))
     for iv, th in enumerate(angles):
+        xcls = O.view_is_x(th)
         th = float(th)
         c, s = math.cos(th), math.sin(th)
-        xcls = abs(c) > abs(s)
         w = sino[:, iv].astype(np.float64).copy()
         if not fbp:
             for iu in range(nu):
@@ -253,13 +253,22 @@ def test_tomo_pair_consistency(rng):
     p = O.tomo_fp(img, dc, src, g, nu, nv)[0, :, :, :, 0]
     # central ray of the central view crosses nz*dz of material
     assert abs(p[nu // 2, 2, nv // 2] - 0.01 * nz * g.dz) < 0.01 * nz * g.dz * 0.15
-    b = O.tomo_bp(np.ones((1, nu, 5, nv, 1), np.float32), dc, src, g, (nx, ny, nz))
-    assert np.all(b[0, 4:-4, 4:-4, :, 0] > 0)
+    for mode in (0, 1):
+        b = O.tomo_bp(np.ones((1, nu, 5, nv, 1), np.float32), dc, src, g, (nx, ny, nz), mode)
+        assert np.all(b[0, 4:-4, 4:-4, :, 0] > 0)
+    # weight mode 1 weights every view; mode 0 (reference) only view 0
+    y = np.ones((1, nu, 5, nv, 1), np.float32)
+    y[:, :, 0] = 0
+    assert rel_l2(O.tomo_bp(y, dc, src, g, (nx, ny, nz), 0) * 2.0, O.tomo_bp(y, dc, src, g, (nx, ny, nz), 1)) < 0.2
 
 
 def test_view_class_split_ties():
-    """Exactly-45-degree float angles fall in the Y class (cos < sin after
-    rounding of the float angle), as in DistanceDriven.cu:302."""
+    """The class rule is evaluated in float as the reference host code does
+    (DistanceDriven.cu:302): at float(3pi/4) the rounded |cos| and |sin| tie,
+    so the view is Y class although |cos| > |sin| in exact arithmetic."""
     assert not O.view_is_x(np.float32(np.pi / 4))
+    assert not O.view_is_x(np.float32(3 * np.pi / 4))
+    d = float(np.float32(3 * np.pi / 4))
+    assert abs(math.cos(d)) > abs(math.sin(d))
     assert O.view_is_x(np.float32(0.0))
     assert not O.view_is_x(np.float32(np.pi / 2))
