@@ -185,6 +185,28 @@ int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x
                       const float* d_w_s, const float* d_norm_img, float lambda, float beta, int nSubsets, float lb,
                       float ub, int typeProjector, void* stream);
 
+/* Forward projection of one 2D slice that allocates nothing (no counterpart
+ * in the reference).  For callers that may not allocate device memory --
+ * code running inside another framework's memory pool or under a fixed
+ * memory budget, real-time pipelines that forbid cudaMalloc after start-up,
+ * plugins handed only device pointers.  Same kernels and results as
+ * rn_fan_project on a plan with nBatches = nChannels = nz = nv = 1: d_img is
+ * [nx][ny], d_prj [nu][nview] (both device memory, caller-owned), host_deg
+ * holds nview angles on the host.  All scratch (geometry tables, edge slopes,
+ * line prefix arrays) lives in one fixed 16 MiB device array compiled into
+ * the library, which every GPU that loads the library keeps until exit; a
+ * geometry whose scratch exceeds it (bytes ~ 8*nview*(nu+1) +
+ * 12*(ny*(nx+4) + nx*(ny+4)) + small tables, e.g. 512x512 with up to about
+ * 1150 views of 888 channels) is rejected with RN_ERR_ARG and a message
+ * giving the bytes needed.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  Every call shares the one array and
+ * overwrites it (the device error word is cleared by each call), so calls
+ * that overlap on the GPU -- from several host threads or streams -- race;
+ * serialise them.  The call synchronises `stream` before returning. */
+int rn_fan_project_noalloc(float* d_prj, const float* d_img, const float* host_deg, int nx, int ny, float dx,
+                           float dy, int nu, int nview, float da, float off_a, float dsd, float dso, void* stream);
+
 /* Tomosynthesis DD on device pointers (same arguments as the reference-named
  * host functions above plus a caller-provided FP64 scratch d_sat whose size
  * rn_tomo_sat_bytes reports: fp_bytes for projection, bp_bytes for

@@ -71,6 +71,7 @@ SIGNATURES = {
     "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
     "rn_tv_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
     "rn_fan_sqs_update": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _f, _f, _i, _vp]),
+    "rn_fan_project_noalloc": (_i, [_vp, _vp, _fp, _i, _i, _f, _f, _i, _i, _f, _f, _f, _f, _vp]),
     "rn_tomo_sat_bytes": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_size_t),
                                ctypes.POINTER(ctypes.c_size_t)]),
     "rn_tomo_project": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),

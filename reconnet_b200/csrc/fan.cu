@@ -24,9 +24,12 @@
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "rn_device.cuh"
@@ -846,3 +849,213 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
 }
 
 }  // namespace rn
+
+// ===========================================================================
+// Forward projection without any allocation.
+//
+// Some callers cannot allocate device memory: code that runs inside another
+// framework's memory pool or under a strict memory budget, real-time or
+// embedded pipelines that must not call cudaMalloc after start-up, and
+// plugins that are only handed device pointers.  rn_fan_project_noalloc
+// serves them: it is the forward projector above (same kernels, same
+// arithmetic) with every piece of its scratch -- geometry tables, slopes and
+// the line prefix arrays -- placed in the fixed device array below instead of
+// a plan.  The array is kNoAllocScratchBytes (16 MiB) and stays resident on
+// every GPU that loads this library until the process exits.
+// ===========================================================================
+namespace rn {
+
+constexpr size_t kNoAllocScratchBytes = 16u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device.  In host code the symbol is
+// only a host-side stand-in, so the address is looked up once per device
+// (with that device current) and passed to the kernels.
+static std::mutex g_noalloc_mu;
+static std::vector<unsigned char*> g_noalloc_ptr;
+
+static int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    RN_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if ((int)g_noalloc_ptr.size() <= dev) g_noalloc_ptr.resize(dev + 1, nullptr);
+    if (!g_noalloc_ptr[dev]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    *out = g_noalloc_ptr[dev];
+    return RN_OK;
+}
+
+static size_t na_align(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace rn
+
+extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const float* host_deg, int nx, int ny,
+                                      float dx, float dy, int nu, int nview, float da, float off_a, float dsd,
+                                      float dso, void* stream) {
+    using namespace rn;
+    clear_error();
+    if (!d_prj || !d_img || !host_deg) return set_error(RN_ERR_ARG, "null argument");
+    if (nx <= 0 || ny <= 0 || nu <= 0 || nview <= 0 || !(dx > 0 && dy > 0 && da > 0 && dsd > 0 && dso > 0))
+        return set_error(RN_ERR_ARG, "sizes, pitches and distances must be positive");
+    cudaStream_t st = (cudaStream_t)stream;
+    FanDims d;
+    d.nx = nx;
+    d.ny = ny;
+    d.nu = nu;
+    d.dx = dx;
+    d.dy = dy;
+    d.du = da;
+    d.off_u = off_a;
+    d.dsd = dsd;
+    d.dso = dso;
+    d.lpx = (nx + 1 + 3) & ~3;
+    d.lpy = (ny + 1 + 3) & ~3;
+    d.isx = ny;
+    d.isy = 1;
+
+    // scratch layout (offsets in bytes, 256-aligned)
+    const int nwork_max = (nview + kFpViews - 1) / kFpViews + 2;
+    const long long slot = (long long)ny * d.lpx + (long long)nx * d.lpy;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off = na_align(off + bytes);
+        return o;
+    };
+    const size_t o_err = take(sizeof(int));
+    const size_t o_set = take(sizeof(GeoSet));
+    const size_t o_fp = take(sizeof(FpSlice));
+    const size_t o_views = take(sizeof(ViewGeo) * nview);
+    const size_t o_perm = take(sizeof(int) * nview);
+    const size_t o_work = take(sizeof(int4) * nwork_max);
+    const size_t o_cell = take(sizeof(float2) * nu);
+    const size_t o_vcs = take(sizeof(double2) * nview);
+    const size_t o_vx = take(sizeof(int) * nview);
+    const size_t o_esc = take(sizeof(double2) * (nu + 1));
+    const size_t host_bytes = off;   // everything above is staged from the host
+    const size_t o_edges = take(sizeof(double) * (size_t)nview * (nu + 1));
+    const size_t o_hl = take(sizeof(float2) * (size_t)slot);
+    const size_t o_la = take(sizeof(float) * (size_t)slot);
+    if (off > kNoAllocScratchBytes)
+        return set_error(RN_ERR_ARG, "rn_fan_project_noalloc: this geometry needs " + std::to_string(off) +
+                                         " bytes of scratch, more than its fixed " +
+                                         std::to_string(kNoAllocScratchBytes) + " bytes");
+    const int R = std::min(fp_lines_for_smem(nu, d.lpx), fp_lines_for_smem(nu, d.lpy));
+    const size_t smem = fp_smem_bytes(nu, std::max(d.lpx, d.lpy), R);
+    if (smem > (size_t)kSmemBudget) return set_error(RN_ERR_ARG, "image lines too long for shared memory");
+
+    // host-side tables, same quantities as fan_build_geometry
+    std::vector<unsigned char> h(host_bytes, 0);
+    ViewGeo* vg = reinterpret_cast<ViewGeo*>(h.data() + o_views);
+    int* perm = reinterpret_cast<int*>(h.data() + o_perm);
+    int4* work = reinterpret_cast<int4*>(h.data() + o_work);
+    float2* cell = reinterpret_cast<float2*>(h.data() + o_cell);
+    double2* vcs = reinterpret_cast<double2*>(h.data() + o_vcs);
+    int* vx = reinterpret_cast<int*>(h.data() + o_vx);
+    double2* esc = reinterpret_cast<double2*>(h.data() + o_esc);
+    for (int e = 0; e <= nu; e++) {
+        double gam = (-((double)e - 0.5 - (nu - 1) / 2.0) - off_a) * (double)da;
+        esc[e] = make_double2(std::sin(gam), std::cos(gam));
+    }
+    for (int u = 0; u < nu; u++) {
+        double a = (-((double)u - (nu - 1) / 2.0) - off_a) * (double)da;
+        cell[u] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    if (std::fabs(nu * (double)da / 2.0) >= M_PI / 4)
+        return set_error(RN_ERR_ARG, "fan geometry: fan half-angle must be below 45 degrees");
+    int nxv = 0;
+    for (int v = 0; v < nview; v++) {
+        double th = (double)host_deg[v];
+        double c = std::cos(th), s = std::sin(th);
+        const float degf = host_deg[v];
+        int xc = std::fabs(std::cos(degf)) > std::fabs(std::sin(degf)) ? 1 : 0;
+        double sx = dso * s / dx + nx / 2.0;
+        double sy = -dso * c / dy + ny / 2.0;
+        auto slope = [&](int e) {
+            double sn = esc[e].x * c - esc[e].y * s;
+            double cn = esc[e].y * c + esc[e].x * s;
+            return xc ? (sn * dy) / (cn * dx) : (cn * dx) / (sn * dy);
+        };
+        ViewGeo& q = vg[v];
+        q.xcls = xc;
+        q.par = xc ? sx : sy;
+        q.perp = xc ? sy : sx;
+        q.cosd = (float)c;
+        q.sind = (float)s;
+        double kap = xc ? (double)dx / dy : (double)dy / dx;
+        q.kappa = (float)kap;
+        double tB = xc ? -1.0 / da : 1.0 / da;
+        q.tB = (float)tB;
+        q.tA = (float)((double)(nu / 2) - tB * std::atan(kap * slope(nu / 2)));
+        double r0 = slope(0), r1 = slope(nu);
+        q.rmin = (float)std::min(r0, r1);
+        q.rmax = (float)std::max(r0, r1);
+        int nl = xc ? ny : nx;
+        q.sigma = (float)((r1 > r0 ? 1.0 : -1.0) * ((nl / 2.0 - q.perp) > 0 ? 1.0 : -1.0));
+        q.pad = 0;
+        if (std::fabs(q.perp - nl / 2.0) <= nl / 2.0 + 1.0)
+            return set_error(RN_ERR_ARG, "fan geometry: source inside the image footprint");
+        vcs[v] = make_double2(c, s);
+        vx[v] = xc;
+        nxv += xc;
+    }
+    {
+        int a = 0, b = nxv;
+        for (int v = 0; v < nview; v++) perm[vx[v] ? a++ : b++] = v;
+    }
+    int nwork = 0;
+    for (int k = 0; k < nxv; k += kFpViews) work[nwork++] = make_int4(0, 1, k, std::min(kFpViews, nxv - k));
+    for (int k = 0; k < nview - nxv; k += kFpViews)
+        work[nwork++] = make_int4(0, 0, nxv + k, std::min(kFpViews, nview - nxv - k));
+    *reinterpret_cast<GeoSet*>(h.data() + o_set) = GeoSet{0, nview, nxv};
+    FpSlice* fs = reinterpret_cast<FpSlice*>(h.data() + o_fp);
+    memset(fs, 0, sizeof(FpSlice));
+    fs->img_w[0] = 1.f;
+    fs->su = nview;
+    fs->sview = 1;
+    // o_err stays 0: the error word starts cleared on every call
+
+    unsigned char* base = nullptr;
+    RN_TRY(noalloc_scratch(&base));
+    RN_CUDA_TRY(cudaMemcpyAsync(base, h.data(), host_bytes, cudaMemcpyHostToDevice, st));
+    double* edges = reinterpret_cast<double*>(base + o_edges);
+    long long ne = (long long)nview * (nu + 1);
+    edge_slope_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(
+        edges, reinterpret_cast<const double2*>(base + o_vcs), reinterpret_cast<const int*>(base + o_vx),
+        reinterpret_cast<const double2*>(base + o_esc), nview, nu, dx, dy);
+    RN_CUDA_TRY(cudaGetLastError());
+    float2* hl = reinterpret_cast<float2*>(base + o_hl);
+    float* la = reinterpret_cast<float*>(base + o_la);
+    const FpSlice* dfs = reinterpret_cast<const FpSlice*>(base + o_fp);
+    fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, hl,
+                                                                                          la, slot);
+    RN_CUDA_TRY(cudaGetLastError());
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FpParams fp;
+    fp.views = reinterpret_cast<const ViewGeo*>(base + o_views);
+    fp.edges = edges;
+    fp.cell = reinterpret_cast<const float2*>(base + o_cell);
+    fp.perm = reinterpret_cast<const int*>(base + o_perm);
+    fp.sets = reinterpret_cast<const GeoSet*>(base + o_set);
+    fp.fps = dfs;
+    fp.work = reinterpret_cast<const int4*>(base + o_work);
+    fp.hl = hl;
+    fp.la = la;
+    fp.slot_elems = slot;
+    fp.slot_base = 0;
+    fp.prj = d_prj;
+    fp.err = reinterpret_cast<int*>(base + o_err);
+    fp.d = d;
+    fp.R = R;
+    fan_fp_kernel<<<nwork, kFpThreads, smem, st>>>(fp);
+    RN_CUDA_TRY(cudaGetLastError());
+    int herr = 0;
+    RN_CUDA_TRY(cudaMemcpyAsync(&herr, base + o_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr != 0) return set_error(RN_ERR_TIMEOUT, "a device-side wait exceeded its spin limit");
+    return RN_OK;
+}
