@@ -196,9 +196,9 @@ int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x
  * line prefix arrays) lives in one fixed 16 MiB device array compiled into
  * the library, which every GPU that loads the library keeps until exit; a
  * geometry whose scratch exceeds it (bytes ~ 8*nview*(nu+1) +
- * 12*(ny*(nx+4) + nx*(ny+4)) + small tables, e.g. 512x512 with up to about
- * 1150 views of 888 channels) is rejected with RN_ERR_ARG and a message
- * giving the bytes needed.  The first call on a device looks up the array's
+ * 16*(ny*(nx+1+2m) + nx*(ny+1+2m)) + small tables, m ~ 12 line padding
+ * entries, e.g. 512x512 with up to about 1000 views of 888 channels) is
+ * rejected with RN_ERR_ARG and a message giving the bytes needed.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) with that device current; make that
  * first call before any stream capture.  Every call shares the one array and
  * overwrites it (the device error word is cleared by each call), so calls

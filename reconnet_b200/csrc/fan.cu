@@ -41,7 +41,8 @@ namespace rn {
 // Tunables.
 // ---------------------------------------------------------------------------
 constexpr int kFpThreads = 512;
-constexpr int kFpViews = 4;          // views per FP CTA
+constexpr int kFpViews = 4;          // views per FP CTA (at most)
+constexpr int kFpRays = 7;           // ray slots per FP thread
 constexpr int kFpMaxLines = 16;      // lines per staged chunk (upper bound)
 constexpr int kSmemBudget = 227 * 1024;
 
@@ -87,7 +88,7 @@ __device__ __forceinline__ double warp_incl_scan(double v) {
 }
 
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
-                                 FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems) {
+                                 FanDims d, float4* __restrict__ line, long long slot_elems) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     int per_slice = d.ny + d.nx;
@@ -99,9 +100,9 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
     int l = xl ? li : li - d.ny;
     int n = xl ? d.nx : d.ny;
     int lp = xl ? d.lpx : d.lpy;
+    const int M = d.margin;
     long long base = (long long)si * slot_elems + (xl ? (long long)l * d.lpx : (long long)d.ny * d.lpx + (long long)l * d.lpy);
-    float2* ohl = hl + base;
-    float* ola = la + base;
+    float4* out = line + base;   // entry j holds position k = j - M
     double carry = 0.0;
     for (int k0 = 0; k0 < n; k0 += 32) {
         int k = k0 + lane;
@@ -129,21 +130,33 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
         double incl = warp_incl_scan(a);
         double excl = carry + incl - a;
         if (k < n) {
-            ohl[k] = split_double(excl);
-            ola[k] = (float)a;
+            float2 q = split_double(excl);
+            out[k + M] = make_float4(q.x, q.y, (float)a, 0.f);
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    // entry n and padding up to lp: P = total, a = 0
-    for (int k = n + lane; k < lp; k += 32) {
-        ohl[k] = split_double(carry);
-        ola[k] = 0.f;
-    }
+    // margins: P = 0 before the line, P = total from position n on
+    float2 tot = split_double(carry);
+    for (int j = lane; j < M; j += 32) out[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = n + M + lane; j < lp; j += 32) out[j] = make_float4(tot.x, tot.y, 0.f, 0.f);
 }
 
 // ---------------------------------------------------------------------------
 // FP kernel.
+//
+// One CTA = (slice, view class, up to kFpViews views).  Each thread owns up
+// to kFpRays rays for the whole kernel: their accumulators and active line
+// ranges stay in registers.  Lines are staged R at a time into a double
+// buffer by bulk async copies.  Per chunk, a ray's position at the chunk's
+// first line is rebuilt from a per-edge table (X0 hi/lo at line 0, slope
+// hi/lo) so the FP32 position error stays at half an ulp of the position.
+// Only the lines where the ray's footprint overlaps the image are visited
+// (the others add exactly zero); the line arrays carry `margin` padding
+// entries on both sides so the visited lines need no clamping.
 // ---------------------------------------------------------------------------
+constexpr float kFloorBias = 12582912.0f;   // 1.5 * 2^23
+constexpr int kFloorBiasBits = 0x4B400000;
+
 struct FpParams {
     const ViewGeo* views;
     const double* edges;
@@ -152,15 +165,27 @@ struct FpParams {
     const GeoSet* sets;
     const FpSlice* fps;
     const int4* work;
-    const float2* hl;
-    const float* la;
+    const float4* line;
     long long slot_elems;
     int slot_base;     // first FP slice of the current wave
     float* prj;
     int* err;
     FanDims d;
     int R;             // lines per chunk
+    int vt;            // views per CTA (size of the per-edge table)
 };
+
+__device__ __forceinline__ void fp_endpoint(float x, const float4* __restrict__ row, unsigned lpm1, float& hi,
+                                            float& rest) {
+    // x >= 0 (padded coordinate): floor via a round-down add against 1.5*2^23
+    float y = __fadd_rd(x, kFloorBias);
+    unsigned k = (unsigned)(__float_as_int(y) - kFloorBiasBits);
+    float f = x - (y - kFloorBias);
+    k = min(k, lpm1);
+    float4 E = row[k];
+    hi = E.x;
+    rest = fmaf(f, E.z, E.y);
+}
 
 __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -170,12 +195,10 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     const GeoSet gs = p.sets[fs.set];
     const int nu = p.d.nu;
     const int nlines = xcls ? p.d.ny : p.d.nx;
-    const int n = xcls ? p.d.nx : p.d.ny;
     const int lp = xcls ? p.d.lpx : p.d.lpy;
     const int R = p.R;
     const long long slot = (long long)(s - p.slot_base) * p.slot_elems + (xcls ? 0ll : (long long)p.d.ny * p.d.lpx);
-    const float2* ghl = p.hl + slot;
-    const float* gla = p.la + slot;
+    const float4* gline = p.line + slot;
 
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
     int* s_gv = reinterpret_cast<int*>(smem + 16);                  // kFpViews
@@ -183,17 +206,12 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     double* s_par = reinterpret_cast<double*>(smem + 64);           // kFpViews
     double* s_perp = s_par + kFpViews;                              // kFpViews
     float* s_g = reinterpret_cast<float*>(smem + 128);              // kFpViews * kFpMaxLines
-    float* s_acc = s_g + kFpViews * kFpMaxLines;                    // kFpViews * nu
-    size_t off = 128 + sizeof(float) * (kFpViews * kFpMaxLines + align4((long long)kFpViews * nu));
+    float4* s_edge = reinterpret_cast<float4*>(smem + 128 + sizeof(float) * kFpViews * kFpMaxLines);
+    size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)p.vt * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    float2* bhl[2];
-    float* bla[2];
-    const size_t hl_bytes = (size_t)R * lp * sizeof(float2);
-    const size_t la_bytes = (size_t)R * lp * sizeof(float);
-    bhl[0] = reinterpret_cast<float2*>(smem + off);
-    bla[0] = reinterpret_cast<float*>(smem + off + hl_bytes);
-    bhl[1] = reinterpret_cast<float2*>(smem + off + hl_bytes + la_bytes);
-    bla[1] = reinterpret_cast<float*>(smem + off + 2 * hl_bytes + la_bytes);
+    float4* buf[2];
+    buf[0] = reinterpret_cast<float4*>(smem + off);
+    buf[1] = buf[0] + (size_t)R * lp;
 
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -209,8 +227,54 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         s_par[tid] = p.views[gv].par;
         s_perp[tid] = p.views[gv].perp;
     }
+    __syncthreads();
+    // per-edge positions at line 0 (padded) and slopes, as hi/lo floats
+    const double M = (double)p.d.margin;
+    for (int i = tid; i < vcount * (nu + 1); i += kFpThreads) {
+        int v = i / (nu + 1);
+        int e = i - v * (nu + 1);
+        double r = p.edges[(long long)s_gv[v] * (nu + 1) + e];
+        double X0 = s_par[v] - r * s_perp[v] + M;
+        float xh = (float)X0, rh = (float)r;
+        s_edge[i] = make_float4(xh, (float)(X0 - (double)xh), rh, (float)(r - (double)rh));
+    }
+    // ray slots: active line range [lb, le) where the footprint overlaps
+    // [0, n], packed lb << 16 | le
     const int nrays = vcount * nu;
-    for (int i = tid; i < nrays; i += kFpThreads) s_acc[i] = 0.f;
+    const double n_d = (double)(xcls ? p.d.nx : p.d.ny);
+    int rng[kFpRays];
+    float acc[kFpRays];
+#pragma unroll
+    for (int k = 0; k < kFpRays; k++) {
+        acc[k] = 0.f;
+        rng[k] = 0;
+        int ray = tid + k * kFpThreads;
+        if (ray < nrays) {
+            int v = ray / nu, u = ray - (ray / nu) * nu;
+            const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
+            double ra = ed[u], rb = ed[u + 1];
+            double par = s_par[v], perp = s_perp[v];
+            // positions x_e(l) = par + r_e (l - perp); the edges do not cross
+            // inside the image, so hi/lo are fixed per ray
+            double lm = 0.5 * nlines;
+            bool aHi = (par + ra * (lm - perp)) >= (par + rb * (lm - perp));
+            double rh = aHi ? ra : rb, rl = aHi ? rb : ra;
+            double lo_l = -1e30, hi_l = 1e30;
+            // hi(l) > 0
+            if (rh > 0) lo_l = fmax(lo_l, perp - par / rh);
+            else if (rh < 0) hi_l = fmin(hi_l, perp - par / rh);
+            else if (!(par > 0)) hi_l = -1e30;
+            // lo(l) < n
+            if (rl > 0) hi_l = fmin(hi_l, perp + (n_d - par) / rl);
+            else if (rl < 0) lo_l = fmax(lo_l, perp + (n_d - par) / rl);
+            else if (!(par < n_d)) hi_l = -1e30;
+            // first overlapping line is floor(lo_l) + 1, last is ceil(hi_l) - 1;
+            // visit one more line on each side (FP64 rounding) -- the line
+            // padding covers one line's advance beyond the footprint
+            double lb = fmax(0.0, floor(lo_l)), le = fmin((double)nlines, floor(hi_l) + 2.0);
+            if (le > lb) rng[k] = ((int)lb << 16) | (int)le;
+        }
+    }
     __syncthreads();
 
     const int nchunks = (nlines + R - 1) / R;
@@ -218,63 +282,58 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         int b = c & 1;
         int l0 = c * R;
         int rc = min(R, nlines - l0);
-        uint32_t bh = (uint32_t)((size_t)rc * lp * sizeof(float2));
-        uint32_t ba = (uint32_t)((size_t)rc * lp * sizeof(float));
+        uint32_t bytes = (uint32_t)((size_t)rc * lp * sizeof(float4));
         fence_proxy_async();
-        mbar_arrive_expect_tx(&bars[b], bh + ba);
-        bulk_g2s(bhl[b], ghl + (long long)l0 * lp, bh, &bars[b]);
-        bulk_g2s(bla[b], gla + (long long)l0 * lp, ba, &bars[b]);
+        mbar_arrive_expect_tx(&bars[b], bytes);
+        bulk_g2s(buf[b], gline + (long long)l0 * lp, bytes, &bars[b]);
     };
     if (tid == 0) issue(0);
 
-    const float fn = (float)n;
+    const unsigned lpm1 = (unsigned)(lp - 1);
     bool ok = true;
     for (int c = 0; c < nchunks; c++) {
         const int b = c & 1;
         const int l0 = c * R;
         const int rc = min(R, nlines - l0);
         if (tid == 0 && c + 1 < nchunks) issue(c + 1);
-        // per-view 1/(line - perp) for this chunk
         if (tid < vcount * R) {
             int v = tid / R, j = tid - (tid / R) * R;
             s_g[v * kFpMaxLines + j] = (float)(1.0 / ((double)(l0 + j) - s_perp[v]));
         }
-        if (!mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1))) {
-            ok = false;
-        }
-        __syncthreads();
+        if (!mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1))) ok = false;
         if (!__syncthreads_and(ok)) {
             if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
+            ok = false;
             break;
         }
-        const float2* HL = bhl[b];
-        const float* LA = bla[b];
-        for (int ray = tid; ray < nrays; ray += kFpThreads) {
-            const int v = ray / nu;
-            const int u = ray - v * nu;
-            const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
-            const double ra = ed[u], rb = ed[u + 1];
-            const double t0 = (double)l0 - s_perp[v];
-            const double par = s_par[v];
-            const float Xa = (float)(par + ra * t0), Xb = (float)(par + rb * t0);
-            const float fra = (float)ra, frb = (float)rb;
-            const float* g = s_g + v * kFpMaxLines;
-            float acc = 0.f;
-            float jf = 0.f;
-            for (int j = 0; j < rc; j++, jf += 1.f) {
-                float xa = fminf(fmaxf(fmaf(fra, jf, Xa), 0.f), fn);
-                float xb = fminf(fmaxf(fmaf(frb, jf, Xb), 0.f), fn);
-                float fa, fb;
-                int ka = floor_frac(xa, fa);
-                int kb = floor_frac(xb, fb);
-                const float2 ha = HL[j * lp + ka];
-                const float2 hb = HL[j * lp + kb];
-                const float aa = LA[j * lp + ka];
-                const float ab = LA[j * lp + kb];
-                float dP = (hb.x - ha.x) + ((hb.y - ha.y) + (fb * ab - fa * aa));
-                acc = fmaf(dP, g[j], acc);
+        const float4* L = buf[b];
+        const float fl0 = (float)l0;
+#pragma unroll
+        for (int k = 0; k < kFpRays; k++) {
+            const int ray = tid + k * kFpThreads;
+            const int jb = max((rng[k] >> 16) - l0, 0);
+            const int je = min((rng[k] & 0xffff) - l0, rc);
+            if (ray < nrays && jb < je) {
+                const int v = ray / nu;
+                const int u = ray - v * nu;
+                const float4 Ea = s_edge[v * (nu + 1) + u];
+                const float4 Eb = s_edge[v * (nu + 1) + u + 1];
+                const float Xa = fmaf(Ea.z, fl0, Ea.x) + fmaf(Ea.w, fl0, Ea.y);
+                const float Xb = fmaf(Eb.z, fl0, Eb.x) + fmaf(Eb.w, fl0, Eb.y);
+                const float ra = Ea.z, rb = Eb.z;
+                const float* g = s_g + v * kFpMaxLines;
+                const float4* row = L + (size_t)jb * lp;
+                float a = acc[k];
+                float jf = (float)jb;
+                for (int j = jb; j < je; j++, jf += 1.f, row += lp) {
+                    float ha, ra_, hb, rb_;
+                    fp_endpoint(fmaf(ra, jf, Xa), row, lpm1, ha, ra_);
+                    fp_endpoint(fmaf(rb, jf, Xb), row, lpm1, hb, rb_);
+                    float dP = (hb - ha) + (rb_ - ra_);
+                    a = fmaf(dP, g[j], a);
+                }
+                acc[k] = a;
             }
-            s_acc[ray] += acc;
         }
         __syncthreads();
     }
@@ -282,7 +341,10 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
 
     // epilogue: scale by L_u / (r_{u+1} - r_u) and store
     const float lenA = xcls ? p.d.dy : p.d.dx;
-    for (int ray = tid; ray < nrays; ray += kFpThreads) {
+#pragma unroll
+    for (int k = 0; k < kFpRays; k++) {
+        const int ray = tid + k * kFpThreads;
+        if (ray >= nrays) continue;
         const int v = ray / nu;
         const int u = ray - v * nu;
         const int gv = s_gv[v];
@@ -290,9 +352,8 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         const float dr = (float)(ed[u + 1] - ed[u]);
         const ViewGeo& vg = p.views[gv];
         const float2 cs = p.cell[u];   // (cos a, sin a)
-        float L = xcls ? lenA / fabsf(vg.cosd * cs.x + vg.sind * cs.y) : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
-        float val = s_acc[ray] * (L / dr);
-        p.prj[fs.prj_off + (long long)u * fs.su + (long long)s_vl[v] * fs.sview] = val;
+        float Lw = xcls ? lenA / fabsf(vg.cosd * cs.x + vg.sind * cs.y) : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
+        p.prj[fs.prj_off + (long long)u * fs.su + (long long)s_vl[v] * fs.sview] = acc[k] * (Lw / dr);
     }
 }
 
@@ -379,11 +440,6 @@ struct BpParams {
     int win;           // staged table entries per view
 };
 
-// Edge index t of the matched parametrisation at lattice point
-// (line l, position q): slope r = (q - par) / (l - perp).
-__device__ __forceinline__ float matched_t(const ViewGeo& vg, float r) {
-    return vg.tA + vg.tB * atanf(vg.kappa * r);
-}
 
 // Reference detector coordinate of a physical point (GetProjectionOnDetector,
 // DistanceDriven.cu:479-485, and the mapping at :530-533).
@@ -399,6 +455,12 @@ struct BpShared {
     int elo[2][kBpViews];
     int gv[2][kBpViews];
 };
+
+// Edge index t of the matched parametrisation for a slope r
+// (r = (q - par) / (l - perp) at lattice point (line l, position q)).
+__device__ __forceinline__ float matched_t(const ViewGeo& vg, float r) {
+    return vg.tA + vg.tB * atanf(vg.kappa * r);
+}
 
 template <bool kMatched>
 __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
@@ -517,6 +579,21 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                 const int nl = vg.xcls ? ny : nx;
                 const float par = (float)vg.par, perp = (float)vg.perp;
                 const int emax = min(nu - 1, elo + cnt - 1);
+                // edge index t(r) = tA + tB atan(kappa r) as a cubic around the
+                // slope r_t of this thread's block centre: truncation below
+                // 2e-5 cells over the 5x5 lattice (it only selects the
+                // footprint; the fraction inside it is exact)
+                const float rt = ((float)(Q0 + 2) - par) / ((float)(L0 + 2) - perp);
+                const float ut = vg.kappa * rt;
+                const float iw = 1.0f / fmaf(ut, ut, 1.0f);
+                const float k1 = vg.tB * vg.kappa * iw;
+                const float c0 = fmaf(vg.tB, atanf(ut), vg.tA);
+                const float c1 = k1;
+                const float c2 = -k1 * vg.kappa * ut * iw;
+                const float c3 = k1 * vg.kappa * vg.kappa * (fmaf(3.0f * ut, ut, -1.0f) * (1.0f / 3.0f)) * iw * iw;
+                float dq[5];
+#pragma unroll
+                for (int qi = 0; qi < 5; qi++) dq[qi] = (float)(Q0 + qi) - par;
                 float dprev[4];
 #pragma unroll
                 for (int li = 0; li < 5; li++) {
@@ -525,9 +602,11 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                     float fh[5], fl[5];
 #pragma unroll
                     for (int qi = 0; qi < 5; qi++) {
-                        float r = ((float)(Q0 + qi) - par) * g;
-                        float t = matched_t(vg, r);
-                        int e = (int)floorf(t);
+                        float r = dq[qi] * g;
+                        float h = r - rt;
+                        float t = fmaf(h, fmaf(h, fmaf(h, c3, c2), c1), c0);
+                        // floor for |t| < 2^22 via a round-down add
+                        int e = __float_as_int(__fadd_rd(t, 12582912.0f)) - 0x4B400000;
                         e = min(max(e, elo), emax);
                         float rc = fminf(fmaxf(r, vg.rmin), vg.rmax);
                         float4 E = T[e - elo];
@@ -616,14 +695,27 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
+int fan_fp_views(int nu) { return std::min(kFpViews, (kFpThreads * kFpRays) / std::max(nu, 1)); }
+
 static size_t fp_smem_bytes(int nu, int lp, int R) {
-    size_t off = 128 + sizeof(float) * (kFpViews * kFpMaxLines + align4((long long)kFpViews * nu));
+    size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)fan_fp_views(nu) * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    return off + 2 * (size_t)R * lp * (sizeof(float2) + sizeof(float));
+    return off + 2 * (size_t)R * lp * sizeof(float4);
 }
 
 static size_t bp_smem_bytes(int win) {
     return ((sizeof(BpShared) + 127) & ~size_t(127)) + 2 * (size_t)kBpViews * win * sizeof(float4);
+}
+
+// Padding (entries per side) of the FP line arrays needed by one view: the
+// widest footprint along a line anywhere in the image (distance dmax_mm from
+// the source at most, stretched by 1/cos of the steepest ray) plus one line's
+// advance of the steepest ray (visited line ranges are widened by one line)
+// and two entries of slack.  Visited positions then stay inside the array.
+static double fp_margin_view(double rmax_abs, double kappa, double pix_along, double dmax_mm, double du) {
+    double kr = kappa * rmax_abs;
+    double foot = dmax_mm * du * std::sqrt(1.0 + kr * kr) / pix_along;
+    return foot + rmax_abs + 2.0;
 }
 
 int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
@@ -649,6 +741,9 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     std::vector<double2> vcs(V);
     std::vector<int> vx(V);
     std::vector<int> perm(V);
+    const double dmax_mm = g.dso + std::sqrt(std::pow(g.nx * (double)g.dx / 2 + std::fabs(g.cx), 2) +
+                                             std::pow(g.ny * (double)g.dy / 2 + std::fabs(g.cy), 2));
+    double margin = 0.0;
     auto slope = [&](int xc, double c, double s, int e) {
         double sn = esc[e].x * c - esc[e].y * s;
         double cn = esc[e].y * c + esc[e].x * s;
@@ -683,6 +778,8 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
             double r0 = slope(xc, c, s, 0), r1 = slope(xc, c, s, nu);
             q.rmin = (float)std::min(r0, r1);
             q.rmax = (float)std::max(r0, r1);
+            margin = std::max(margin, fp_margin_view(std::max(std::fabs(r0), std::fabs(r1)), kap,
+                                                     xc ? g.dx : g.dy, dmax_mm, du));
             int nl = xc ? g.ny : g.nx;
             double side = (nl / 2.0 - q.perp) > 0 ? 1.0 : -1.0;
             q.sigma = (float)((r1 > r0 ? 1.0 : -1.0) * side);
@@ -704,6 +801,10 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     }
     if (std::fabs(nu * du / 2.0) >= M_PI / 4)
         return set_error(RN_ERR_ARG, "fan geometry: fan half-angle must be below 45 degrees");
+    if (margin > 4096) return set_error(RN_ERR_ARG, "fan geometry: footprints too wide for the line arrays");
+    p->dims.margin = (int)std::ceil(margin);
+    p->dims.lpx = g.nx + 1 + 2 * p->dims.margin;
+    p->dims.lpy = g.ny + 1 + 2 * p->dims.margin;
 
     RN_CUDA_TRY(cudaMalloc(&p->d_views, sizeof(ViewGeo) * V));
     RN_CUDA_TRY(cudaMalloc(&p->d_edges, sizeof(double) * V * (nu + 1)));
@@ -760,7 +861,7 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
         {
             LaunchScope ls0(p, st, 0);
             fan_lines_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(d_img, p->d_fp, s0, ns, d,
-                                                                                    p->d_hl, p->d_la, slot);
+                                                                                    p->d_line, slot);
         }
         RN_CUDA_TRY(cudaGetLastError());
         int wend = wbeg;
@@ -774,14 +875,14 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
             fp.sets = p->d_sets;
             fp.fps = p->d_fp;
             fp.work = p->d_fp_work + wbeg;
-            fp.hl = p->d_hl;
-            fp.la = p->d_la;
+            fp.line = p->d_line;
             fp.slot_elems = slot;
             fp.slot_base = s0;
             fp.prj = d_prj;
             fp.err = p->d_err;
             fp.d = d;
             fp.R = R;
+            fp.vt = fan_fp_views(d.nu);
             LaunchScope ls1(p, st, 1);
             fan_fp_kernel<<<wend - wbeg, kFpThreads, smem, st>>>(fp);
             RN_CUDA_TRY(cudaGetLastError());
@@ -912,13 +1013,35 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     d.off_u = off_a;
     d.dsd = dsd;
     d.dso = dso;
-    d.lpx = (nx + 1 + 3) & ~3;
-    d.lpy = (ny + 1 + 3) & ~3;
     d.isx = ny;
     d.isy = 1;
+    const int VT = fan_fp_views(nu);
+    if (VT < 1) return set_error(RN_ERR_ARG, "too many detector channels for the forward projector");
+    if (nx >= (1 << 15) || ny >= (1 << 15)) return set_error(RN_ERR_ARG, "image too large");
+
+    // line padding: same bound as the plan path (fan_build_geometry)
+    const double dmax_mm = dso + std::sqrt(std::pow(nx * (double)dx / 2, 2) + std::pow(ny * (double)dy / 2, 2));
+    double margin = 0.0;
+    for (int v = 0; v < nview; v++) {
+        const float degf = host_deg[v];
+        double th = (double)degf;
+        int xc = std::fabs(std::cos(degf)) > std::fabs(std::sin(degf)) ? 1 : 0;
+        double kap = xc ? (double)dx / dy : (double)dy / dx;
+        double rmax = 0.0;
+        for (int e : {0, nu}) {
+            double gam = (-((double)e - 0.5 - (nu - 1) / 2.0) - off_a) * (double)da;
+            double sn = std::sin(gam - th), cn = std::cos(gam - th);
+            rmax = std::max(rmax, std::fabs(xc ? (sn * dy) / (cn * dx) : (cn * dx) / (sn * dy)));
+        }
+        margin = std::max(margin, fp_margin_view(rmax, kap, xc ? dx : dy, dmax_mm, da));
+    }
+    if (margin > 4096) return set_error(RN_ERR_ARG, "fan geometry: footprints too wide for the line arrays");
+    d.margin = (int)std::ceil(margin);
+    d.lpx = nx + 1 + 2 * d.margin;
+    d.lpy = ny + 1 + 2 * d.margin;
 
     // scratch layout (offsets in bytes, 256-aligned)
-    const int nwork_max = (nview + kFpViews - 1) / kFpViews + 2;
+    const int nwork_max = (nview + VT - 1) / VT + 2;
     const long long slot = (long long)ny * d.lpx + (long long)nx * d.lpy;
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -938,8 +1061,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     const size_t o_esc = take(sizeof(double2) * (nu + 1));
     const size_t host_bytes = off;   // everything above is staged from the host
     const size_t o_edges = take(sizeof(double) * (size_t)nview * (nu + 1));
-    const size_t o_hl = take(sizeof(float2) * (size_t)slot);
-    const size_t o_la = take(sizeof(float) * (size_t)slot);
+    const size_t o_line = take(sizeof(float4) * (size_t)slot);
     if (off > kNoAllocScratchBytes)
         return set_error(RN_ERR_ARG, "rn_fan_project_noalloc: this geometry needs " + std::to_string(off) +
                                          " bytes of scratch, more than its fixed " +
@@ -1008,9 +1130,8 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
         for (int v = 0; v < nview; v++) perm[vx[v] ? a++ : b++] = v;
     }
     int nwork = 0;
-    for (int k = 0; k < nxv; k += kFpViews) work[nwork++] = make_int4(0, 1, k, std::min(kFpViews, nxv - k));
-    for (int k = 0; k < nview - nxv; k += kFpViews)
-        work[nwork++] = make_int4(0, 0, nxv + k, std::min(kFpViews, nview - nxv - k));
+    for (int k = 0; k < nxv; k += VT) work[nwork++] = make_int4(0, 1, k, std::min(VT, nxv - k));
+    for (int k = 0; k < nview - nxv; k += VT) work[nwork++] = make_int4(0, 0, nxv + k, std::min(VT, nview - nxv - k));
     *reinterpret_cast<GeoSet*>(h.data() + o_set) = GeoSet{0, nview, nxv};
     FpSlice* fs = reinterpret_cast<FpSlice*>(h.data() + o_fp);
     memset(fs, 0, sizeof(FpSlice));
@@ -1028,11 +1149,10 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
         edges, reinterpret_cast<const double2*>(base + o_vcs), reinterpret_cast<const int*>(base + o_vx),
         reinterpret_cast<const double2*>(base + o_esc), nview, nu, dx, dy);
     RN_CUDA_TRY(cudaGetLastError());
-    float2* hl = reinterpret_cast<float2*>(base + o_hl);
-    float* la = reinterpret_cast<float*>(base + o_la);
+    float4* line = reinterpret_cast<float4*>(base + o_line);
     const FpSlice* dfs = reinterpret_cast<const FpSlice*>(base + o_fp);
-    fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, hl,
-                                                                                          la, slot);
+    fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, line,
+                                                                                          slot);
     RN_CUDA_TRY(cudaGetLastError());
     RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     FpParams fp;
@@ -1043,14 +1163,14 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     fp.sets = reinterpret_cast<const GeoSet*>(base + o_set);
     fp.fps = dfs;
     fp.work = reinterpret_cast<const int4*>(base + o_work);
-    fp.hl = hl;
-    fp.la = la;
+    fp.line = line;
     fp.slot_elems = slot;
     fp.slot_base = 0;
     fp.prj = d_prj;
     fp.err = reinterpret_cast<int*>(base + o_err);
     fp.d = d;
     fp.R = R;
+    fp.vt = VT;
     fan_fp_kernel<<<nwork, kFpThreads, smem, st>>>(fp);
     RN_CUDA_TRY(cudaGetLastError());
     int herr = 0;

@@ -46,8 +46,10 @@ static int validate(const RnFanGeom* g) {
         return set_error(RN_ERR_ARG, "geometry sizes must be positive");
     if (!(g->dx > 0 && g->dy > 0 && g->dz > 0 && g->du > 0 && g->dv > 0 && g->dsd > 0 && g->dso > 0))
         return set_error(RN_ERR_ARG, "pixel sizes, detector pitch and distances must be positive");
-    if (g->nx >= (1 << 20) || g->ny >= (1 << 20))
-        return set_error(RN_ERR_ARG, "image too large");
+    if (g->nx >= (1 << 15) || g->ny >= (1 << 15))
+        return set_error(RN_ERR_ARG, "image too large (at most 32767 pixels per side)");
+    if (fan_fp_views(g->nu) < 1)
+        return set_error(RN_ERR_ARG, "too many detector channels for the forward projector");
     return RN_OK;
 }
 
@@ -63,14 +65,15 @@ static void set_dims(rn_fan_plan* p, long long isx, long long isy) {
     d.off_u = g.off_u;
     d.dsd = g.dsd;
     d.dso = g.dso;
-    d.lpx = (int)((g.nx + 1 + 3) & ~3);
-    d.lpy = (int)((g.ny + 1 + 3) & ~3);
+    d.margin = 0;            // set with the geometry tables (fan_build_geometry)
+    d.lpx = g.nx + 1;
+    d.lpy = g.ny + 1;
     d.isx = isx;
     d.isy = isy;
 }
 
 static void build_fp_work(rn_fan_plan* p) {
-    const int VT = 4;  // kFpViews in fan.cu
+    const int VT = fan_fp_views(p->g.nu);
     p->h_fp_work.clear();
     for (size_t s = 0; s < p->h_fp.size(); s++) {
         const GeoSet& gs = p->h_sets[p->h_fp[s].set];
@@ -127,10 +130,9 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     // line scratch
     const FanDims& d = p->dims;
     p->line_slot_elems = (long long)d.ny * d.lpx + (long long)d.nx * d.lpy;
-    long long slot_bytes = p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float));
+    long long slot_bytes = p->line_slot_elems * (long long)sizeof(float4);
     p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(), kLineBudget / slot_bytes));
-    RN_CUDA_TRY(cudaMalloc(&p->d_hl, sizeof(float2) * p->fp_slots * p->line_slot_elems));
-    RN_CUDA_TRY(cudaMalloc(&p->d_la, sizeof(float) * p->fp_slots * p->line_slot_elems));
+    RN_CUDA_TRY(cudaMalloc(&p->d_line, sizeof(float4) * p->fp_slots * p->line_slot_elems));
 
     // table scratch: all slices if within budget, else at least the largest slice
     long long need = 0, largest = 0;
@@ -167,8 +169,7 @@ int rn_fan_plan_destroy(rn_fan_plan* p) {
     cudaFree(p->d_bpr);
     cudaFree(p->d_fp_work);
     cudaFree(p->d_err);
-    cudaFree(p->d_hl);
-    cudaFree(p->d_la);
+    cudaFree(p->d_line);
     cudaFree(p->d_tab);
     cudaFree(p->d_tmp_img);
     cudaFree(p->d_tmp_prj);

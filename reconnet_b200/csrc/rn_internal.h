@@ -88,7 +88,8 @@ struct FanDims {
     int nx, ny, nu;
     float dx, dy;
     float du, off_u, dsd, dso;
-    int lpx, lpy;   // padded line lengths (>= nx+1 / ny+1, multiple of 4)
+    int margin;     // padding entries on each side of an FP line array
+    int lpx, lpy;   // FP line lengths in float4 entries: n + 1 + 2 * margin
     long long isx, isy;   // image strides (elements) along x and y
 };
 
@@ -124,8 +125,7 @@ struct rn_fan_plan {
     int* d_err = nullptr;           // device error word
 
     // scratch
-    float2* d_hl = nullptr;         // line prefixes (hi, lo)
-    float* d_la = nullptr;          // line values
+    float4* d_line = nullptr;       // FP line arrays: {prefix hi, prefix lo, value, 0}
     long long line_slot_elems = 0;  // per FP slice: ny*lpx + nx*lpy
     long long fp_slots = 0;         // FP slices whose lines fit in the scratch
     int table_win = 0;              // staged table entries per view (BP)
@@ -147,6 +147,8 @@ struct rn_fan_plan {
 };
 
 namespace rn {
+// Views per forward-projection CTA for nu channels (0 if nu is too large).
+int fan_fp_views(int nu);
 constexpr int kTimedKinds = 5;
 // Brackets one kernel launch of `plan` on stream `st`: counts it and, when
 // timing is enabled, records a start/stop event pair around it.
