@@ -42,7 +42,7 @@ namespace rn {
 // ---------------------------------------------------------------------------
 constexpr int kFpThreads = 512;
 constexpr int kFpViews = 4;          // views per FP CTA (at most)
-constexpr int kFpRays = 7;           // ray slots per FP thread
+constexpr int kFpGroups = 8;         // groups of 31 rays per FP warp (at most)
 constexpr int kFpMaxLines = 16;      // lines per staged chunk (upper bound)
 constexpr int kSmemBudget = 227 * 1024;
 
@@ -88,7 +88,7 @@ __device__ __forceinline__ double warp_incl_scan(double v) {
 }
 
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
-                                 FanDims d, float4* __restrict__ line, long long slot_elems) {
+                                 FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     int per_slice = d.ny + d.nx;
@@ -102,7 +102,8 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
     int lp = xl ? d.lpx : d.lpy;
     const int M = d.margin;
     long long base = (long long)si * slot_elems + (xl ? (long long)l * d.lpx : (long long)d.ny * d.lpx + (long long)l * d.lpy);
-    float4* out = line + base;   // entry j holds position k = j - M
+    float2* ohl = hl + base;    // entry j holds position k = j - M
+    float* ola = la + base;
     double carry = 0.0;
     for (int k0 = 0; k0 < n; k0 += 32) {
         int k = k0 + lane;
@@ -130,30 +131,41 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
         double incl = warp_incl_scan(a);
         double excl = carry + incl - a;
         if (k < n) {
-            float2 q = split_double(excl);
-            out[k + M] = make_float4(q.x, q.y, (float)a, 0.f);
+            ohl[k + M] = split_double(excl);
+            ola[k + M] = (float)a;
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     // margins: P = 0 before the line, P = total from position n on
     float2 tot = split_double(carry);
-    for (int j = lane; j < M; j += 32) out[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int j = n + M + lane; j < lp; j += 32) out[j] = make_float4(tot.x, tot.y, 0.f, 0.f);
+    for (int j = lane; j < M; j += 32) {
+        ohl[j] = make_float2(0.f, 0.f);
+        ola[j] = 0.f;
+    }
+    for (int j = n + M + lane; j < lp; j += 32) {
+        ohl[j] = tot;
+        ola[j] = 0.f;
+    }
 }
 
 // ---------------------------------------------------------------------------
 // FP kernel.
 //
-// One CTA = (slice, view class, up to kFpViews views).  Each thread owns up
-// to kFpRays rays for the whole kernel: their accumulators and active line
-// ranges stay in registers.  Lines are staged R at a time into a double
-// buffer by bulk async copies.  Per chunk, a ray's position at the chunk's
-// first line is rebuilt from a per-edge table (X0 hi/lo at line 0, slope
-// hi/lo) so the FP32 position error stays at half an ulp of the position.
-// Only the lines where the ray's footprint overlaps the image are visited
-// (the others add exactly zero); the line arrays carry `margin` padding
-// entries on both sides so the visited lines need no clamping.
+// One CTA = (slice, view class, up to kFpViews views), 16 warps.  A warp
+// owns groups of 31 adjacent rays of one view: lane i evaluates the prefix
+// integral at cell edge e0+i and takes edge e0+i+1 from its neighbour with a
+// shuffle, so every edge is evaluated once.  Group accumulators and line
+// ranges stay in registers for the whole kernel.  Lines are staged R at a
+// time into a double buffer by bulk async copies.  Per chunk, an edge's
+// position at the chunk's first line is rebuilt from a per-edge table (X0
+// hi/lo at line 0, slope hi/lo), so the FP32 position error stays at half an
+// ulp.  A group visits only the lines where one of its footprints overlaps
+// the image (the others add exactly zero), and every ray masks the lines
+// outside its own range; the line arrays carry `margin` padding entries on
+// both sides so visited positions need no clamping.
 // ---------------------------------------------------------------------------
+constexpr int kFpWarps = kFpThreads / 32;
+constexpr int kFpGroupRays = 31;
 constexpr float kFloorBias = 12582912.0f;   // 1.5 * 2^23
 constexpr int kFloorBiasBits = 0x4B400000;
 
@@ -165,7 +177,8 @@ struct FpParams {
     const GeoSet* sets;
     const FpSlice* fps;
     const int4* work;
-    const float4* line;
+    const float2* hl;
+    const float* la;
     long long slot_elems;
     int slot_base;     // first FP slice of the current wave
     float* prj;
@@ -175,16 +188,22 @@ struct FpParams {
     int vt;            // views per CTA (size of the per-edge table)
 };
 
-__device__ __forceinline__ void fp_endpoint(float x, const float4* __restrict__ row, unsigned lpm1, float& hi,
-                                            float& rest) {
-    // x >= 0 (padded coordinate): floor via a round-down add against 1.5*2^23
-    float y = __fadd_rd(x, kFloorBias);
-    unsigned k = (unsigned)(__float_as_int(y) - kFloorBiasBits);
-    float f = x - (y - kFloorBias);
-    k = min(k, lpm1);
-    float4 E = row[k];
-    hi = E.x;
-    rest = fmaf(f, E.z, E.y);
+// Active line range [lb, le) of the footprint between edge slopes ra, rb
+// (positions x(l) = par + r (l - perp)) over [0, n], visiting one extra line
+// on each side against FP64 rounding; 0 if empty, else lb << 16 | le.
+__device__ __forceinline__ int fp_ray_range(double ra, double rb, double par, double perp, int nlines, double n) {
+    double lm = 0.5 * nlines;
+    bool aHi = (par + ra * (lm - perp)) >= (par + rb * (lm - perp));   // the edges meet only at the source
+    double rh = aHi ? ra : rb, rl = aHi ? rb : ra;
+    double lo_l = -1e30, hi_l = 1e30;
+    if (rh > 0) lo_l = fmax(lo_l, perp - par / rh);          // hi(l) > 0
+    else if (rh < 0) hi_l = fmin(hi_l, perp - par / rh);
+    else if (!(par > 0)) hi_l = -1e30;
+    if (rl > 0) hi_l = fmin(hi_l, perp + (n - par) / rl);    // lo(l) < n
+    else if (rl < 0) lo_l = fmax(lo_l, perp + (n - par) / rl);
+    else if (!(par < n)) hi_l = -1e30;
+    double lb = fmax(0.0, floor(lo_l)), le = fmin((double)nlines, floor(hi_l) + 2.0);
+    return (le > lb) ? (((int)lb << 16) | (int)le) : 0;
 }
 
 __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
@@ -198,7 +217,8 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     const int lp = xcls ? p.d.lpx : p.d.lpy;
     const int R = p.R;
     const long long slot = (long long)(s - p.slot_base) * p.slot_elems + (xcls ? 0ll : (long long)p.d.ny * p.d.lpx);
-    const float4* gline = p.line + slot;
+    const float2* ghl = p.hl + slot;
+    const float* gla = p.la + slot;
 
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
     int* s_gv = reinterpret_cast<int*>(smem + 16);                  // kFpViews
@@ -209,11 +229,16 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     float4* s_edge = reinterpret_cast<float4*>(smem + 128 + sizeof(float) * kFpViews * kFpMaxLines);
     size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)p.vt * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    float4* buf[2];
-    buf[0] = reinterpret_cast<float4*>(smem + off);
-    buf[1] = buf[0] + (size_t)R * lp;
+    const size_t hl_bytes = (size_t)R * lp * sizeof(float2), la_bytes = (size_t)R * lp * sizeof(float);
+    float2* bhl[2];
+    float* bla[2];
+    bhl[0] = reinterpret_cast<float2*>(smem + off);
+    bla[0] = reinterpret_cast<float*>(smem + off + hl_bytes);
+    bhl[1] = reinterpret_cast<float2*>(smem + off + hl_bytes + la_bytes);
+    bla[1] = reinterpret_cast<float*>(smem + off + 2 * hl_bytes + la_bytes);
 
     const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -238,41 +263,31 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         float xh = (float)X0, rh = (float)r;
         s_edge[i] = make_float4(xh, (float)(X0 - (double)xh), rh, (float)(r - (double)rh));
     }
-    // ray slots: active line range [lb, le) where the footprint overlaps
-    // [0, n], packed lb << 16 | le
-    const int nrays = vcount * nu;
+    // ray groups of this warp: own ray range (per lane) and the group's
+    // union range (warp-uniform)
+    const int ngpv = (nu + kFpGroupRays - 1) / kFpGroupRays;    // groups per view
+    const int ngroups = vcount * ngpv;
     const double n_d = (double)(xcls ? p.d.nx : p.d.ny);
-    int rng[kFpRays];
-    float acc[kFpRays];
+    int rng[kFpGroups], urng[kFpGroups];
+    float acc[kFpGroups];
 #pragma unroll
-    for (int k = 0; k < kFpRays; k++) {
+    for (int k = 0; k < kFpGroups; k++) {
         acc[k] = 0.f;
         rng[k] = 0;
-        int ray = tid + k * kFpThreads;
-        if (ray < nrays) {
-            int v = ray / nu, u = ray - (ray / nu) * nu;
-            const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
-            double ra = ed[u], rb = ed[u + 1];
-            double par = s_par[v], perp = s_perp[v];
-            // positions x_e(l) = par + r_e (l - perp); the edges do not cross
-            // inside the image, so hi/lo are fixed per ray
-            double lm = 0.5 * nlines;
-            bool aHi = (par + ra * (lm - perp)) >= (par + rb * (lm - perp));
-            double rh = aHi ? ra : rb, rl = aHi ? rb : ra;
-            double lo_l = -1e30, hi_l = 1e30;
-            // hi(l) > 0
-            if (rh > 0) lo_l = fmax(lo_l, perp - par / rh);
-            else if (rh < 0) hi_l = fmin(hi_l, perp - par / rh);
-            else if (!(par > 0)) hi_l = -1e30;
-            // lo(l) < n
-            if (rl > 0) hi_l = fmin(hi_l, perp + (n_d - par) / rl);
-            else if (rl < 0) lo_l = fmax(lo_l, perp + (n_d - par) / rl);
-            else if (!(par < n_d)) hi_l = -1e30;
-            // first overlapping line is floor(lo_l) + 1, last is ceil(hi_l) - 1;
-            // visit one more line on each side (FP64 rounding) -- the line
-            // padding covers one line's advance beyond the footprint
-            double lb = fmax(0.0, floor(lo_l)), le = fmin((double)nlines, floor(hi_l) + 2.0);
-            if (le > lb) rng[k] = ((int)lb << 16) | (int)le;
+        urng[k] = 0;
+        const int grp = warp + k * kFpWarps;
+        if (grp < ngroups) {   // warp-uniform
+            const int v = grp / ngpv;
+            const int u = (grp - v * ngpv) * kFpGroupRays + lane;
+            if (lane < kFpGroupRays && u < nu) {
+                const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
+                rng[k] = fp_ray_range(ed[u], ed[u + 1], s_par[v], s_perp[v], nlines, n_d);
+            }
+            int lb = rng[k] ? (rng[k] >> 16) : 0x7fffffff;
+            int le = rng[k] ? (rng[k] & 0xffff) : 0;
+            lb = __reduce_min_sync(0xffffffffu, lb);
+            le = __reduce_max_sync(0xffffffffu, le);
+            urng[k] = (le > lb) ? ((lb << 16) | le) : 0;
         }
     }
     __syncthreads();
@@ -282,10 +297,12 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         int b = c & 1;
         int l0 = c * R;
         int rc = min(R, nlines - l0);
-        uint32_t bytes = (uint32_t)((size_t)rc * lp * sizeof(float4));
+        uint32_t bh = (uint32_t)((size_t)rc * lp * sizeof(float2));
+        uint32_t ba = (uint32_t)((size_t)rc * lp * sizeof(float));
         fence_proxy_async();
-        mbar_arrive_expect_tx(&bars[b], bytes);
-        bulk_g2s(buf[b], gline + (long long)l0 * lp, bytes, &bars[b]);
+        mbar_arrive_expect_tx(&bars[b], bh + ba);
+        bulk_g2s(bhl[b], ghl + (long long)l0 * lp, bh, &bars[b]);
+        bulk_g2s(bla[b], gla + (long long)l0 * lp, ba, &bars[b]);
     };
     if (tid == 0) issue(0);
 
@@ -306,31 +323,36 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             ok = false;
             break;
         }
-        const float4* L = buf[b];
+        const float2* HL = bhl[b];
+        const float* LA = bla[b];
         const float fl0 = (float)l0;
 #pragma unroll
-        for (int k = 0; k < kFpRays; k++) {
-            const int ray = tid + k * kFpThreads;
-            const int jb = max((rng[k] >> 16) - l0, 0);
-            const int je = min((rng[k] & 0xffff) - l0, rc);
-            if (ray < nrays && jb < je) {
-                const int v = ray / nu;
-                const int u = ray - v * nu;
-                const float4 Ea = s_edge[v * (nu + 1) + u];
-                const float4 Eb = s_edge[v * (nu + 1) + u + 1];
-                const float Xa = fmaf(Ea.z, fl0, Ea.x) + fmaf(Ea.w, fl0, Ea.y);
-                const float Xb = fmaf(Eb.z, fl0, Eb.x) + fmaf(Eb.w, fl0, Eb.y);
-                const float ra = Ea.z, rb = Eb.z;
+        for (int k = 0; k < kFpGroups; k++) {
+            const int J0 = max((urng[k] >> 16) - l0, 0);
+            const int J1 = min((urng[k] & 0xffff) - l0, rc);
+            if (J0 < J1) {   // warp-uniform
+                const int grp = warp + k * kFpWarps;
+                const int v = grp / ngpv;
+                const int e = min((grp - v * ngpv) * kFpGroupRays + lane, nu);
+                const float4 E = s_edge[v * (nu + 1) + e];
+                const float X = fmaf(E.z, fl0, E.x) + fmaf(E.w, fl0, E.y);
+                const float r = E.z;
+                const int jb = (rng[k] >> 16) - l0, jn = (rng[k] & 0xffff) - (rng[k] >> 16);
                 const float* g = s_g + v * kFpMaxLines;
-                const float4* row = L + (size_t)jb * lp;
                 float a = acc[k];
-                float jf = (float)jb;
-                for (int j = jb; j < je; j++, jf += 1.f, row += lp) {
-                    float ha, ra_, hb, rb_;
-                    fp_endpoint(fmaf(ra, jf, Xa), row, lpm1, ha, ra_);
-                    fp_endpoint(fmaf(rb, jf, Xb), row, lpm1, hb, rb_);
-                    float dP = (hb - ha) + (rb_ - ra_);
-                    a = fmaf(dP, g[j], a);
+                float jf = (float)J0;
+                for (int j = J0; j < J1; j++, jf += 1.f) {
+                    const float x = fmaf(r, jf, X);
+                    // x >= 0 (padded coordinate): floor via a round-down add against 1.5*2^23
+                    const float y = __fadd_rd(x, kFloorBias);
+                    const unsigned kk = min((unsigned)(__float_as_int(y) - kFloorBiasBits), lpm1);
+                    const float f = x - (y - kFloorBias);
+                    const float2 h = HL[j * lp + kk];
+                    const float hi = h.x, rest = fmaf(f, LA[j * lp + kk], h.y);
+                    const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
+                    const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
+                    const float dP = (nhi - hi) + (nrest - rest);
+                    if ((unsigned)(j - jb) < (unsigned)jn) a = fmaf(dP, g[j], a);
                 }
                 acc[k] = a;
             }
@@ -342,11 +364,12 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     // epilogue: scale by L_u / (r_{u+1} - r_u) and store
     const float lenA = xcls ? p.d.dy : p.d.dx;
 #pragma unroll
-    for (int k = 0; k < kFpRays; k++) {
-        const int ray = tid + k * kFpThreads;
-        if (ray >= nrays) continue;
-        const int v = ray / nu;
-        const int u = ray - v * nu;
+    for (int k = 0; k < kFpGroups; k++) {
+        const int grp = warp + k * kFpWarps;
+        if (grp >= ngroups) continue;
+        const int v = grp / ngpv;
+        const int u = (grp - v * ngpv) * kFpGroupRays + lane;
+        if (lane >= kFpGroupRays || u >= nu) continue;
         const int gv = s_gv[v];
         const double* ed = p.edges + (long long)gv * (nu + 1);
         const float dr = (float)(ed[u + 1] - ed[u]);
@@ -695,12 +718,15 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
-int fan_fp_views(int nu) { return std::min(kFpViews, (kFpThreads * kFpRays) / std::max(nu, 1)); }
+int fan_fp_views(int nu) {
+    const int ngpv = (std::max(nu, 1) + 30) / 31;   // groups of 31 rays per view
+    return std::min(kFpViews, (kFpGroups * (kFpThreads / 32)) / ngpv);
+}
 
 static size_t fp_smem_bytes(int nu, int lp, int R) {
     size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)fan_fp_views(nu) * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    return off + 2 * (size_t)R * lp * sizeof(float4);
+    return off + 2 * (size_t)R * lp * (sizeof(float2) + sizeof(float));
 }
 
 static size_t bp_smem_bytes(int win) {
@@ -803,8 +829,8 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
         return set_error(RN_ERR_ARG, "fan geometry: fan half-angle must be below 45 degrees");
     if (margin > 4096) return set_error(RN_ERR_ARG, "fan geometry: footprints too wide for the line arrays");
     p->dims.margin = (int)std::ceil(margin);
-    p->dims.lpx = g.nx + 1 + 2 * p->dims.margin;
-    p->dims.lpy = g.ny + 1 + 2 * p->dims.margin;
+    p->dims.lpx = (g.nx + 1 + 2 * p->dims.margin + 3) & ~3;
+    p->dims.lpy = (g.ny + 1 + 2 * p->dims.margin + 3) & ~3;
 
     RN_CUDA_TRY(cudaMalloc(&p->d_views, sizeof(ViewGeo) * V));
     RN_CUDA_TRY(cudaMalloc(&p->d_edges, sizeof(double) * V * (nu + 1)));
@@ -861,7 +887,7 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
         {
             LaunchScope ls0(p, st, 0);
             fan_lines_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(d_img, p->d_fp, s0, ns, d,
-                                                                                    p->d_line, slot);
+                                                                                    p->d_hl, p->d_la, slot);
         }
         RN_CUDA_TRY(cudaGetLastError());
         int wend = wbeg;
@@ -875,7 +901,8 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
             fp.sets = p->d_sets;
             fp.fps = p->d_fp;
             fp.work = p->d_fp_work + wbeg;
-            fp.line = p->d_line;
+            fp.hl = p->d_hl;
+            fp.la = p->d_la;
             fp.slot_elems = slot;
             fp.slot_base = s0;
             fp.prj = d_prj;
@@ -1037,8 +1064,8 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     }
     if (margin > 4096) return set_error(RN_ERR_ARG, "fan geometry: footprints too wide for the line arrays");
     d.margin = (int)std::ceil(margin);
-    d.lpx = nx + 1 + 2 * d.margin;
-    d.lpy = ny + 1 + 2 * d.margin;
+    d.lpx = (nx + 1 + 2 * d.margin + 3) & ~3;
+    d.lpy = (ny + 1 + 2 * d.margin + 3) & ~3;
 
     // scratch layout (offsets in bytes, 256-aligned)
     const int nwork_max = (nview + VT - 1) / VT + 2;
@@ -1061,7 +1088,8 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     const size_t o_esc = take(sizeof(double2) * (nu + 1));
     const size_t host_bytes = off;   // everything above is staged from the host
     const size_t o_edges = take(sizeof(double) * (size_t)nview * (nu + 1));
-    const size_t o_line = take(sizeof(float4) * (size_t)slot);
+    const size_t o_hl = take(sizeof(float2) * (size_t)slot);
+    const size_t o_la = take(sizeof(float) * (size_t)slot);
     if (off > kNoAllocScratchBytes)
         return set_error(RN_ERR_ARG, "rn_fan_project_noalloc: this geometry needs " + std::to_string(off) +
                                          " bytes of scratch, more than its fixed " +
@@ -1149,10 +1177,11 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
         edges, reinterpret_cast<const double2*>(base + o_vcs), reinterpret_cast<const int*>(base + o_vx),
         reinterpret_cast<const double2*>(base + o_esc), nview, nu, dx, dy);
     RN_CUDA_TRY(cudaGetLastError());
-    float4* line = reinterpret_cast<float4*>(base + o_line);
+    float2* hl = reinterpret_cast<float2*>(base + o_hl);
+    float* la = reinterpret_cast<float*>(base + o_la);
     const FpSlice* dfs = reinterpret_cast<const FpSlice*>(base + o_fp);
-    fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, line,
-                                                                                          slot);
+    fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, hl,
+                                                                                          la, slot);
     RN_CUDA_TRY(cudaGetLastError());
     RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     FpParams fp;
@@ -1163,7 +1192,8 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     fp.sets = reinterpret_cast<const GeoSet*>(base + o_set);
     fp.fps = dfs;
     fp.work = reinterpret_cast<const int4*>(base + o_work);
-    fp.line = line;
+    fp.hl = hl;
+    fp.la = la;
     fp.slot_elems = slot;
     fp.slot_base = 0;
     fp.prj = d_prj;

@@ -130,9 +130,10 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     // line scratch
     const FanDims& d = p->dims;
     p->line_slot_elems = (long long)d.ny * d.lpx + (long long)d.nx * d.lpy;
-    long long slot_bytes = p->line_slot_elems * (long long)sizeof(float4);
+    long long slot_bytes = p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float));
     p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(), kLineBudget / slot_bytes));
-    RN_CUDA_TRY(cudaMalloc(&p->d_line, sizeof(float4) * p->fp_slots * p->line_slot_elems));
+    RN_CUDA_TRY(cudaMalloc(&p->d_hl, sizeof(float2) * p->fp_slots * p->line_slot_elems));
+    RN_CUDA_TRY(cudaMalloc(&p->d_la, sizeof(float) * p->fp_slots * p->line_slot_elems));
 
     // table scratch: all slices if within budget, else at least the largest slice
     long long need = 0, largest = 0;
@@ -169,7 +170,8 @@ int rn_fan_plan_destroy(rn_fan_plan* p) {
     cudaFree(p->d_bpr);
     cudaFree(p->d_fp_work);
     cudaFree(p->d_err);
-    cudaFree(p->d_line);
+    cudaFree(p->d_hl);
+    cudaFree(p->d_la);
     cudaFree(p->d_tab);
     cudaFree(p->d_tmp_img);
     cudaFree(p->d_tmp_prj);

@@ -89,7 +89,7 @@ struct FanDims {
     float dx, dy;
     float du, off_u, dsd, dso;
     int margin;     // padding entries on each side of an FP line array
-    int lpx, lpy;   // FP line lengths in float4 entries: n + 1 + 2 * margin
+    int lpx, lpy;   // FP line lengths: n + 1 + 2 * margin, rounded up to a multiple of 4
     long long isx, isy;   // image strides (elements) along x and y
 };
 
@@ -125,7 +125,8 @@ struct rn_fan_plan {
     int* d_err = nullptr;           // device error word
 
     // scratch
-    float4* d_line = nullptr;       // FP line arrays: {prefix hi, prefix lo, value, 0}
+    float2* d_hl = nullptr;         // FP line prefixes (hi, lo)
+    float* d_la = nullptr;          // FP line values
     long long line_slot_elems = 0;  // per FP slice: ny*lpx + nx*lpy
     long long fp_slots = 0;         // FP slices whose lines fit in the scratch
     int table_win = 0;              // staged table entries per view (BP)
