@@ -339,10 +339,10 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                 const float r = E.z;
                 const int jb = (rng[k] >> 16) - l0, jn = (rng[k] & 0xffff) - (rng[k] >> 16);
                 const float* g = s_g + v * kFpMaxLines;
-                float a = acc[k];
-                float jf = (float)J0;
-                for (int j = J0; j < J1; j++, jf += 1.f) {
-                    const float x = fmaf(r, jf, X);
+                // prefix integral at this lane's edge on line j, and the
+                // footprint difference with the next lane's edge
+                auto line_dp = [&](int j) -> float {
+                    const float x = fmaf(r, (float)j, X);
                     // x >= 0 (padded coordinate): floor via a round-down add against 1.5*2^23
                     const float y = __fadd_rd(x, kFloorBias);
                     const unsigned kk = min((unsigned)(__float_as_int(y) - kFloorBiasBits), lpm1);
@@ -351,10 +351,20 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                     const float hi = h.x, rest = fmaf(f, LA[j * lp + kk], h.y);
                     const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
                     const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
-                    const float dP = (nhi - hi) + (nrest - rest);
-                    if ((unsigned)(j - jb) < (unsigned)jn) a = fmaf(dP, g[j], a);
+                    return (nhi - hi) + (nrest - rest);
+                };
+                float a0 = acc[k], a1 = 0.f;
+                int j = J0;
+                for (; j + 1 < J1; j += 2) {   // two independent lines per iteration
+                    const float d0 = line_dp(j), d1 = line_dp(j + 1);
+                    if ((unsigned)(j - jb) < (unsigned)jn) a0 = fmaf(d0, g[j], a0);
+                    if ((unsigned)(j + 1 - jb) < (unsigned)jn) a1 = fmaf(d1, g[j + 1], a1);
                 }
-                acc[k] = a;
+                if (j < J1) {
+                    const float d0 = line_dp(j);
+                    if ((unsigned)(j - jb) < (unsigned)jn) a0 = fmaf(d0, g[j], a0);
+                }
+                acc[k] = a0 + a1;
             }
         }
         __syncthreads();
@@ -385,7 +395,7 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
 // so that the u-strided sinogram reads of neighbouring views share sectors.
 //   matched (type 2): W_u = prj * L_u; entry e < nu = {Qhi, Qlo, W_e/(r_{e+1}-r_e), r_e}
 //   reference (0/1):  W_u = prj * (L_u if type 0); entry k <= nu = {Uhi, Ulo, W_k, 0}
-// with Q/U the FP64 prefix over u.
+// with Q/U the FP64 prefix over u; stored at index e+1 after a guard entry.
 // ---------------------------------------------------------------------------
 __global__ void fan_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin,
                                  int ns, const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
@@ -403,7 +413,12 @@ __global__ void fan_table_kernel(const float* __restrict__ prj, const BpSlice* _
     const ViewGeo vg = views[gv];
     const int nu = d.nu;
     const double* ed = edges + (long long)gv * (nu + 1);
-    float4* out = tab + (bs.table_off - tab_base) + (long long)vl * (nu + 1);
+    // per view: index 0 is a guard entry (prefix 0, slope 0), index e+1 holds
+    // edge / cell e, index nu+1 the total with slope 0; indices outside the
+    // detector therefore evaluate to 0 or the total without clamping
+    float4* out = tab + (bs.table_off - tab_base) + (long long)vl * (nu + 2);
+    if (lane == 0) out[0] = make_float4(0.f, 0.f, 0.f, type == RN_TYPE_MATCHED ? (float)ed[0] : 0.f);
+    out += 1;
     const float lenA = vg.xcls ? d.dy : d.dx;
     double carry = 0.0;
     for (int u0 = 0; u0 < nu; u0 += 32) {
@@ -473,10 +488,16 @@ __device__ __forceinline__ float ref_t(float px, float py, float c, float s, con
     return -(a / d.du + d.off_u) + d.nu * 0.5f;
 }
 
+// Per-view parameters the BP inner loop reads, staged in shared memory.
+struct BpView {
+    float par, perp, kappa, tA, tB, sigma, cosd, sind;
+    int xcls, pad0, pad1, pad2;
+};
+
 struct BpShared {
     uint64_t bars[2];
     int elo[2][kBpViews];
-    int gv[2][kBpViews];
+    BpView vw[2][kBpViews];
 };
 
 // Edge index t of the matched parametrisation for a slope r
@@ -506,7 +527,7 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
     const int tid = threadIdx.x;
     const int X0 = txi * kBpTile, Y0 = tyi * kBpTile;            // CTA pixel origin
     const int x0 = X0 + (tid & 15) * 4, y0 = Y0 + (tid >> 4) * 4; // thread pixel origin
-    const int tabn = nu + 1;
+    const int tabn = nu + 2;   // table entries per view (guard + nu + total)
 
     if (tid == 0) {
         mbar_init(&sh->bars[0], 1);
@@ -536,7 +557,7 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                 tmin = fminf(tmin, t);
                 tmax = fmaxf(tmax, t);
             }
-        int lo = (int)floorf(tmin) - 2;
+        int lo = (int)floorf(tmin) + 1 - 2;   // table index = edge/cell index + 1
         lo = max(0, min(lo, tabn - p.win));
         return lo;
     };
@@ -548,7 +569,17 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
             int b = c & 1;
             if (vl < gs.nview) {
                 sh->elo[b][tid] = window(vl);
-                sh->gv[b][tid] = gs.view_off + vl;
+                const ViewGeo& vg = p.views[gs.view_off + vl];
+                BpView& w = sh->vw[b][tid];
+                w.par = (float)vg.par;
+                w.perp = (float)vg.perp;
+                w.kappa = vg.kappa;
+                w.tA = vg.tA;
+                w.tB = vg.tB;
+                w.sigma = vg.sigma;
+                w.cosd = vg.cosd;
+                w.sind = vg.sind;
+                w.xcls = vg.xcls;
             }
         }
     };
@@ -591,17 +622,17 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
         }
         const int vc = min(kBpViews, gs.nview - c * kBpViews);
         for (int v = 0; v < vc; v++) {
-            const ViewGeo vg = p.views[sh->gv[b][v]];
+            const BpView vg = sh->vw[b][v];
             const float4* T = buf[b] + v * p.win;
-            const int elo = sh->elo[b][v];
+            const int ilo = sh->elo[b][v];
             const int cnt = min(p.win, tabn);
+            const int imax = ilo + cnt - 1;   // <= nu + 1
             if (kMatched) {
                 // lattice lines: rows (X) or columns (Y); positions along them
                 const int L0 = vg.xcls ? y0 : x0;
                 const int Q0 = vg.xcls ? x0 : y0;
                 const int nl = vg.xcls ? ny : nx;
-                const float par = (float)vg.par, perp = (float)vg.perp;
-                const int emax = min(nu - 1, elo + cnt - 1);
+                const float par = vg.par, perp = vg.perp;
                 // edge index t(r) = tA + tB atan(kappa r) as a cubic around the
                 // slope r_t of this thread's block centre: truncation below
                 // 2e-5 cells over the 5x5 lattice (it only selects the
@@ -628,13 +659,13 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                         float r = dq[qi] * g;
                         float h = r - rt;
                         float t = fmaf(h, fmaf(h, fmaf(h, c3, c2), c1), c0);
-                        // floor for |t| < 2^22 via a round-down add
-                        int e = __float_as_int(__fadd_rd(t, 12582912.0f)) - 0x4B400000;
-                        e = min(max(e, elo), emax);
-                        float rc = fminf(fmaxf(r, vg.rmin), vg.rmax);
-                        float4 E = T[e - elo];
+                        // table index floor(t) + 1 for |t| < 2^22 via a round-down add;
+                        // beyond the detector it reaches a zero-slope guard entry
+                        int i = __float_as_int(__fadd_rd(t, 12582912.0f)) - (0x4B400000 - 1);
+                        i = min(max(i, ilo), imax);
+                        float4 E = T[i - ilo];
                         fh[qi] = E.x;
-                        fl[qi] = fmaf(E.z, rc - E.w, E.y);
+                        fl[qi] = fmaf(E.z, r - E.w, E.y);
                     }
                     float dcur[4];
 #pragma unroll
@@ -654,7 +685,6 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
             } else {
                 // reference DDBPFanKernelX/Y: pixel edges at the pixel centre line
                 const float cs = vg.cosd, sn = vg.sind;
-                const int kmax = min(nu, elo + cnt - 1);
 #pragma unroll
                 for (int li = 0; li < 4; li++) {
                     float tq[5], uh[5], ul[5];
@@ -671,10 +701,10 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                         float t = ref_t(px, py, cs, sn, p.d);
                         float tc = fminf(fmaxf(t, 0.f), (float)nu);
                         float fr;
-                        int k = floor_frac(tc, fr);
-                        k = min(max(k, elo), kmax);
-                        fr = tc - (float)k;
-                        float4 E = T[k - elo];
+                        int i = floor_frac(tc, fr) + 1;   // table index of cell k
+                        i = min(max(i, ilo), imax);
+                        fr = tc - (float)(i - 1);
+                        float4 E = T[i - ilo];
                         tq[qi] = t;
                         uh[qi] = E.x;
                         ul[qi] = fmaf(fr, E.z, E.y);
@@ -937,7 +967,7 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         long long base = bps[s0].table_off;
         while (s1 < nbp) {
             const GeoSet& gs = p->h_sets[bps[s1].set];
-            long long end = bps[s1].table_off + (long long)gs.nview * (d.nu + 1);
+            long long end = bps[s1].table_off + (long long)gs.nview * (d.nu + 2);
             if (end - base > p->tab_elems && s1 > s0) break;
             s1++;
         }

@@ -101,7 +101,7 @@ static int table_window(const RnFanGeom& g) {
     double w = diag / (dmin * g.du) + 8;
     int win = (int)std::ceil(w);
     win = (win + 7) & ~7;
-    return std::min(win, g.nu + 1);
+    return std::min(win, g.nu + 2);
 }
 
 static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
@@ -138,7 +138,7 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     // table scratch: all slices if within budget, else at least the largest slice
     long long need = 0, largest = 0;
     for (const BpSlice& b : p->h_bp) {
-        long long n = (long long)p->h_sets[b.set].nview * (g.nu + 1);
+        long long n = (long long)p->h_sets[b.set].nview * (g.nu + 2);
         need = std::max(need, b.table_off + n);
         largest = std::max(largest, n);
     }
@@ -275,7 +275,7 @@ int rn_fan_plan_create(rn_fan_plan** out, const RnFanGeom* g, const float* host_
                 m.sview = r.sview = nv * C;
                 m.set = r.set = 0;
                 m.table_off = r.table_off = toff;
-                toff += (long long)nview * (nu + 1);
+                toff += (long long)nview * (nu + 2);
                 p->h_bp.push_back(m);
                 p->h_bpr.push_back(r);
             }
@@ -336,7 +336,7 @@ int rn_fan_plan_create_ragged(rn_fan_plan** out, const RnFanGeom* g, const int* 
         b.su = nvs;
         b.sview = 1;
         b.set = s;
-        b.table_off = (long long)voff * (nu + 1);
+        b.table_off = (long long)voff * (nu + 2);
         p->h_bp.push_back(b);
         p->h_bpr.push_back(b);
         voff += nvs;
