@@ -229,13 +229,10 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     float4* s_edge = reinterpret_cast<float4*>(smem + 128 + sizeof(float) * kFpViews * kFpMaxLines);
     size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)p.vt * (nu + 1);
     off = (off + 127) & ~size_t(127);
+    // double buffer: buffer b holds R lines of (hi, lo) then R lines of values
     const size_t hl_bytes = (size_t)R * lp * sizeof(float2), la_bytes = (size_t)R * lp * sizeof(float);
-    float2* bhl[2];
-    float* bla[2];
-    bhl[0] = reinterpret_cast<float2*>(smem + off);
-    bla[0] = reinterpret_cast<float*>(smem + off + hl_bytes);
-    bhl[1] = reinterpret_cast<float2*>(smem + off + hl_bytes + la_bytes);
-    bla[1] = reinterpret_cast<float*>(smem + off + 2 * hl_bytes + la_bytes);
+    unsigned char* const buf0 = smem + off;
+    const size_t buf_bytes = hl_bytes + la_bytes;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -299,10 +296,11 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         int rc = min(R, nlines - l0);
         uint32_t bh = (uint32_t)((size_t)rc * lp * sizeof(float2));
         uint32_t ba = (uint32_t)((size_t)rc * lp * sizeof(float));
+        unsigned char* dst = buf0 + b * buf_bytes;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bars[b], bh + ba);
-        bulk_g2s(bhl[b], ghl + (long long)l0 * lp, bh, &bars[b]);
-        bulk_g2s(bla[b], gla + (long long)l0 * lp, ba, &bars[b]);
+        bulk_g2s(dst, ghl + (long long)l0 * lp, bh, &bars[b]);
+        bulk_g2s(dst + hl_bytes, gla + (long long)l0 * lp, ba, &bars[b]);
     };
     if (tid == 0) issue(0);
 
@@ -323,8 +321,8 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             ok = false;
             break;
         }
-        const float2* HL = bhl[b];
-        const float* LA = bla[b];
+        const float2* HL = reinterpret_cast<const float2*>(buf0 + b * buf_bytes);
+        const float* LA = reinterpret_cast<const float*>(buf0 + b * buf_bytes + hl_bytes);
         const float fl0 = (float)l0;
 #pragma unroll
         for (int k = 0; k < kFpGroups; k++) {
@@ -339,32 +337,26 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                 const float r = E.z;
                 const int jb = (rng[k] >> 16) - l0, jn = (rng[k] & 0xffff) - (rng[k] >> 16);
                 const float* g = s_g + v * kFpMaxLines;
-                // prefix integral at this lane's edge on line j, and the
-                // footprint difference with the next lane's edge
-                auto line_dp = [&](int j) -> float {
-                    const float x = fmaf(r, (float)j, X);
-                    // x >= 0 (padded coordinate): floor via a round-down add against 1.5*2^23
+                const float2* hrow = HL + J0 * lp;
+                const float* arow = LA + J0 * lp;
+                float a = acc[k];
+                float jf = (float)J0;
+                for (int j = J0; j < J1; j++, jf += 1.f, hrow += lp, arow += lp) {
+                    // prefix integral at this lane's edge on line j; x >= 0 is the
+                    // padded coordinate, floored by a round-down add against 1.5*2^23
+                    const float x = fmaf(r, jf, X);
                     const float y = __fadd_rd(x, kFloorBias);
                     const unsigned kk = min((unsigned)(__float_as_int(y) - kFloorBiasBits), lpm1);
                     const float f = x - (y - kFloorBias);
-                    const float2 h = HL[j * lp + kk];
-                    const float hi = h.x, rest = fmaf(f, LA[j * lp + kk], h.y);
+                    const float2 h = hrow[kk];
+                    const float hi = h.x, rest = fmaf(f, arow[kk], h.y);
+                    // footprint difference with the next lane's edge
                     const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
                     const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
-                    return (nhi - hi) + (nrest - rest);
-                };
-                float a0 = acc[k], a1 = 0.f;
-                int j = J0;
-                for (; j + 1 < J1; j += 2) {   // two independent lines per iteration
-                    const float d0 = line_dp(j), d1 = line_dp(j + 1);
-                    if ((unsigned)(j - jb) < (unsigned)jn) a0 = fmaf(d0, g[j], a0);
-                    if ((unsigned)(j + 1 - jb) < (unsigned)jn) a1 = fmaf(d1, g[j + 1], a1);
+                    const float dP = (nhi - hi) + (nrest - rest);
+                    if ((unsigned)(j - jb) < (unsigned)jn) a = fmaf(dP, g[j], a);
                 }
-                if (j < J1) {
-                    const float d0 = line_dp(j);
-                    if ((unsigned)(j - jb) < (unsigned)jn) a0 = fmaf(d0, g[j], a0);
-                }
-                acc[k] = a0 + a1;
+                acc[k] = a;
             }
         }
         __syncthreads();
@@ -510,10 +502,8 @@ template <bool kMatched>
 __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     BpShared* sh = reinterpret_cast<BpShared*>(smem);
-    float4* buf[2];
     size_t off = (sizeof(BpShared) + 127) & ~size_t(127);
-    buf[0] = reinterpret_cast<float4*>(smem + off);
-    buf[1] = buf[0] + kBpViews * p.win;
+    float4* const buf0 = reinterpret_cast<float4*>(smem + off);   // buffer b at buf0 + b * kBpViews * win
 
     const int tiles_per_slice = p.tiles_x * p.tiles_y;
     const int si = blockIdx.x / tiles_per_slice;
@@ -593,7 +583,7 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
         mbar_arrive_expect_tx(&sh->bars[b], total);
         for (int v = 0; v < vc; v++) {
             int vl = c * kBpViews + v;
-            bulk_g2s(buf[b] + v * p.win, gtab + (long long)vl * tabn + sh->elo[b][v],
+            bulk_g2s(buf0 + (b * kBpViews + v) * p.win, gtab + (long long)vl * tabn + sh->elo[b][v],
                      (uint32_t)(cnt * sizeof(float4)), &sh->bars[b]);
         }
     };
@@ -623,7 +613,7 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
         const int vc = min(kBpViews, gs.nview - c * kBpViews);
         for (int v = 0; v < vc; v++) {
             const BpView vg = sh->vw[b][v];
-            const float4* T = buf[b] + v * p.win;
+            const float4* T = buf0 + (b * kBpViews + v) * p.win;
             const int ilo = sh->elo[b][v];
             const int cnt = min(p.win, tabn);
             const int imax = ilo + cnt - 1;   // <= nu + 1
@@ -774,6 +764,24 @@ static double fp_margin_view(double rmax_abs, double kappa, double pix_along, do
     return foot + rmax_abs + 2.0;
 }
 
+// Opt the large-shared-memory kernels in to the full per-CTA budget once per
+// device (at plan creation), so that projection calls themselves only launch.
+static std::mutex g_attr_mu;
+static std::vector<char> g_attr_done;
+
+int fan_kernel_attributes() {
+    int dev = 0;
+    RN_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if ((int)g_attr_done.size() <= dev) g_attr_done.resize(dev + 1, 0);
+    if (g_attr_done[dev]) return RN_OK;
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    g_attr_done[dev] = 1;
+    return RN_OK;
+}
+
 int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     const RnFanGeom& g = p->g;
     const int nu = g.nu;
@@ -906,7 +914,6 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
     if (fp_smem_bytes(d.nu, std::max(d.lpx, d.lpy), R) > (size_t)kSmemBudget)
         return set_error(RN_ERR_ARG, "fan projection: image lines too long for shared memory");
     const size_t smem = fp_smem_bytes(d.nu, std::max(d.lpx, d.lpy), R);
-    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // slices are processed in waves of at most `slots` line buffers
     const long long slot = p->line_slot_elems;
     const int slots = (int)std::max<long long>(1, std::min<long long>(nfp, p->fp_slots));
@@ -955,10 +962,6 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
     const BpSlice* dbp = (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
     const int nbp = (int)bps.size();
     const size_t smem = bp_smem_bytes(p->table_win);
-    if (type == RN_TYPE_MATCHED)
-        RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    else
-        RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int tiles_x = (d.nx + kBpTile - 1) / kBpTile, tiles_y = (d.ny + kBpTile - 1) / kBpTile;
     int s0 = 0;
     while (s0 < nbp) {
@@ -1213,7 +1216,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, hl,
                                                                                           la, slot);
     RN_CUDA_TRY(cudaGetLastError());
-    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RN_TRY(fan_kernel_attributes());
     FpParams fp;
     fp.views = reinterpret_cast<const ViewGeo*>(base + o_views);
     fp.edges = edges;

@@ -110,6 +110,7 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     if (win < 0) return set_error(RN_ERR_ARG, "fan geometry: the image reaches the source");
     if (win > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
     p->table_win = win;
+    RN_TRY(fan_kernel_attributes());
     RN_TRY(fan_build_geometry(p, host_deg, st));
     build_fp_work(p);
 

@@ -150,6 +150,9 @@ struct rn_fan_plan {
 namespace rn {
 // Views per forward-projection CTA for nu channels (0 if nu is too large).
 int fan_fp_views(int nu);
+// Sets the dynamic shared-memory limits of the fan kernels on the current
+// device (once per device).
+int fan_kernel_attributes();
 constexpr int kTimedKinds = 5;
 // Brackets one kernel launch of `plan` on stream `st`: counts it and, when
 // timing is enabled, records a start/stop event pair around it.
