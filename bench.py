@@ -147,6 +147,19 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def bench_config(nslices, counts, world):
+    """The workload description both arms print (the same config on each)."""
+    nview = int(np.sum(counts))
+    return {"workload": "batched 2D fan-beam DD forward projection + matched backprojection: "
+                        f"{nslices} slices 512x512 @0.7 mm, 888 ch @1.2858 mm, "
+                        "views U[576,1152] per slice over 360 deg",
+            "slices_per_gpu": nslices, "total_views_per_gpu": nview,
+            "fp_updates_per_step": nview * 888 * 512, "bp_updates_per_step": nview * 512 * 512,
+            "l2": "inputs larger than L2 (64 MB image batch, "
+                  f"{nview * 888 * 4 / 1e6:.0f} MB sinogram, ~1.2 GB scratch per step)",
+            "parallelism": f"dp{world} (independent slice batches)"}
+
+
 def cpu_baseline_sample(geom, counts, angles, imgs, target_s=12.0):
     """FP32 OpenMP port of the oracle on whole slices of the workload (all of
     each slice's views, FP + matched BP), slice after slice until about
@@ -210,11 +223,12 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded random-ellipse phantoms",
-            "config": {"workload": "batched 2D fan-beam DD FP + matched BP (bounded CPU sample per step)",
-                       "slices": args.slices, "nx": geom.nx, "ny": geom.ny, "nu": geom.nu},
+            "config": bench_config(args.slices, counts, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    line["reference_gpu"] = reference_gpu(geom, counts, angles, imgs, min(3, args.steps))
+    import torch
+    if torch.cuda.is_available():
+        line["reference_gpu"] = reference_gpu(geom, counts, angles, imgs, min(3, args.steps))
     print(json.dumps(line), flush=True)
 
 
@@ -416,14 +430,7 @@ def run_b200(args):
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic: seeded random-ellipse phantoms (10 ellipses, 5-120 mm, 0-0.04/mm)",
-                "config": {"workload": "batched 2D fan-beam DD forward projection + matched backprojection: "
-                                       f"{args.slices} slices 512x512 @0.7 mm, 888 ch @1.2858 mm, "
-                                       "views U[576,1152] per slice over 360 deg",
-                           "slices_per_gpu": args.slices, "total_views_per_gpu": int(plan.total_views),
-                           "fp_updates_per_step": fp_upd, "bp_updates_per_step": bp_upd,
-                           "l2": "inputs larger than L2 (64 MB image batch, "
-                                 f"{p.numel() * 4 / 1e6:.0f} MB sinogram, ~1.2 GB scratch per step)",
-                           "parallelism": f"dp{world} (independent slice batches)"},
+                "config": bench_config(args.slices, counts, world),
                 "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk.summary()}
         if cpu is not None:

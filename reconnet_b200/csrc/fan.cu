@@ -157,15 +157,21 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
 // shuffle, so every edge is evaluated once.  Group accumulators and line
 // ranges stay in registers for the whole kernel.  Lines are staged R at a
 // time into a double buffer by bulk async copies.  Per chunk, an edge's
-// position at the chunk's first line is rebuilt from a per-edge table (X0
-// hi/lo at line 0, slope hi/lo), so the FP32 position error stays at half an
-// ulp.  A group visits only the lines where one of its footprints overlaps
-// the image (the others add exactly zero), and every ray masks the lines
-// outside its own range; the line arrays carry `margin` padding entries on
-// both sides so visited positions need no clamping.
+// position at the chunk's first line is rebuilt from a per-edge table (the
+// line-0 position as integer cell + offset, the slope as hi/lo floats) and
+// split into an integer cell and a small FP32 offset, so per-line positions
+// carry ~1e-6 cells of rounding.  A group
+// visits only the lines where one of its footprints overlaps the image.  The
+// line arrays carry `margin` zero-valued padding entries on both sides and
+// positions beyond them clamp to the ends, so a footprint that misses a line
+// adds exactly zero and no per-ray masking is needed.
 // ---------------------------------------------------------------------------
 constexpr int kFpWarps = kFpThreads / 32;
 constexpr int kFpGroupRays = 31;
+// shared-memory header: barriers and view data (128 B), then the per-line
+// factors 1 / (l - perp) of two chunks; the per-edge table follows
+constexpr int kFpHeader = 128 + 2 * (int)sizeof(float) * kFpViews * kFpMaxLines;
+static_assert(kFpHeader % 16 == 0, "per-edge table must be 16-byte aligned");
 constexpr float kFloorBias = 12582912.0f;   // 1.5 * 2^23
 constexpr int kFloorBiasBits = 0x4B400000;
 
@@ -225,9 +231,9 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     int* s_vl = s_gv + kFpViews;                                    // set-local view index
     double* s_par = reinterpret_cast<double*>(smem + 64);           // kFpViews
     double* s_perp = s_par + kFpViews;                              // kFpViews
-    float* s_g = reinterpret_cast<float*>(smem + 128);              // kFpViews * kFpMaxLines
-    float4* s_edge = reinterpret_cast<float4*>(smem + 128 + sizeof(float) * kFpViews * kFpMaxLines);
-    size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)p.vt * (nu + 1);
+    float* s_g = reinterpret_cast<float*>(smem + 128);              // 2 x kFpViews x kFpMaxLines
+    float4* s_edge = reinterpret_cast<float4*>(smem + kFpHeader);
+    size_t off = kFpHeader + sizeof(float4) * (size_t)p.vt * (nu + 1);
     off = (off + 127) & ~size_t(127);
     // double buffer: buffer b holds R lines of (hi, lo) then R lines of values
     const size_t hl_bytes = (size_t)R * lp * sizeof(float2), la_bytes = (size_t)R * lp * sizeof(float);
@@ -257,31 +263,32 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         int e = i - v * (nu + 1);
         double r = p.edges[(long long)s_gv[v] * (nu + 1) + e];
         double X0 = s_par[v] - r * s_perp[v] + M;
-        float xh = (float)X0, rh = (float)r;
-        s_edge[i] = make_float4(xh, (float)(X0 - (double)xh), rh, (float)(r - (double)rh));
+        double Xi0 = floor(X0);
+        float rh = (float)r;
+        s_edge[i] = make_float4((float)(X0 - Xi0), __int_as_float((int)Xi0), rh, (float)(r - (double)rh));
     }
     // ray groups of this warp: own ray range (per lane) and the group's
     // union range (warp-uniform)
     const int ngpv = (nu + kFpGroupRays - 1) / kFpGroupRays;    // groups per view
     const int ngroups = vcount * ngpv;
     const double n_d = (double)(xcls ? p.d.nx : p.d.ny);
-    int rng[kFpGroups], urng[kFpGroups];
+    int urng[kFpGroups];
     float acc[kFpGroups];
 #pragma unroll
     for (int k = 0; k < kFpGroups; k++) {
         acc[k] = 0.f;
-        rng[k] = 0;
         urng[k] = 0;
         const int grp = warp + k * kFpWarps;
         if (grp < ngroups) {   // warp-uniform
             const int v = grp / ngpv;
             const int u = (grp - v * ngpv) * kFpGroupRays + lane;
+            int rng = 0;
             if (lane < kFpGroupRays && u < nu) {
                 const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
-                rng[k] = fp_ray_range(ed[u], ed[u + 1], s_par[v], s_perp[v], nlines, n_d);
+                rng = fp_ray_range(ed[u], ed[u + 1], s_par[v], s_perp[v], nlines, n_d);
             }
-            int lb = rng[k] ? (rng[k] >> 16) : 0x7fffffff;
-            int le = rng[k] ? (rng[k] & 0xffff) : 0;
+            int lb = rng ? (rng >> 16) : 0x7fffffff;
+            int le = rng ? (rng & 0xffff) : 0;
             lb = __reduce_min_sync(0xffffffffu, lb);
             le = __reduce_max_sync(0xffffffffu, le);
             urng[k] = (le > lb) ? ((lb << 16) | le) : 0;
@@ -302,25 +309,32 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         bulk_g2s(dst, ghl + (long long)l0 * lp, bh, &bars[b]);
         bulk_g2s(dst + hl_bytes, gla + (long long)l0 * lp, ba, &bars[b]);
     };
+    // per-line factors 1 / (l - perp) of chunk c into slot c & 1
+    auto line_factors = [&](int c) {
+        if (tid < vcount * R) {
+            const int v = tid / R, j = tid - (tid / R) * R;
+            s_g[(c & 1) * kFpViews * kFpMaxLines + v * kFpMaxLines + j] =
+                (float)(1.0 / ((double)(c * R + j) - s_perp[v]));
+        }
+    };
     if (tid == 0) issue(0);
+    line_factors(0);
 
+    // One barrier per chunk: after it every warp has finished chunk c - 1, so
+    // buffer (c + 1) & 1 and factor slot (c + 1) & 1 may be refilled.
     const unsigned lpm1 = (unsigned)(lp - 1);
     bool ok = true;
     for (int c = 0; c < nchunks; c++) {
         const int b = c & 1;
         const int l0 = c * R;
         const int rc = min(R, nlines - l0);
-        if (tid == 0 && c + 1 < nchunks) issue(c + 1);
-        if (tid < vcount * R) {
-            int v = tid / R, j = tid - (tid / R) * R;
-            s_g[v * kFpMaxLines + j] = (float)(1.0 / ((double)(l0 + j) - s_perp[v]));
-        }
         if (!mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1))) ok = false;
         if (!__syncthreads_and(ok)) {
             if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
             ok = false;
             break;
         }
+        if (tid == 0 && c + 1 < nchunks) issue(c + 1);
         const float2* HL = reinterpret_cast<const float2*>(buf0 + b * buf_bytes);
         const float* LA = reinterpret_cast<const float*>(buf0 + b * buf_bytes + hl_bytes);
         const float fl0 = (float)l0;
@@ -333,20 +347,32 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                 const int v = grp / ngpv;
                 const int e = min((grp - v * ngpv) * kFpGroupRays + lane, nu);
                 const float4 E = s_edge[v * (nu + 1) + e];
-                const float X = fmaf(E.z, fl0, E.x) + fmaf(E.w, fl0, E.y);
+                // edge position at the chunk's first line, Xi0 + Xf0 + (rhi + rlo) l0,
+                // split into an integer cell Xi (floor bias folded in) and a small
+                // offset Xf with error-free steps: rhi l0 = pr + pe exactly, pr =
+                // floor(pr) + pf exactly.  Per-line positions then stay below ~50
+                // cells and keep ~1e-6 cells of precision.
+                const float pr = E.z * fl0;
+                const float pe = fmaf(E.z, fl0, -pr);
+                const float py = __fadd_rd(pr, kFloorBias);
+                const float pf = pr - (py - kFloorBias);
+                const int Xi = __float_as_int(E.y) + (__float_as_int(py) - kFloorBiasBits) - kFloorBiasBits;
+                const float Xf = (E.x + pf) + fmaf(E.w, fl0, pe);
                 const float r = E.z;
-                const int jb = (rng[k] >> 16) - l0, jn = (rng[k] & 0xffff) - (rng[k] >> 16);
-                const float* g = s_g + v * kFpMaxLines;
+                const float* g = s_g + b * kFpViews * kFpMaxLines + v * kFpMaxLines;
                 const float2* hrow = HL + J0 * lp;
                 const float* arow = LA + J0 * lp;
                 float a = acc[k];
                 float jf = (float)J0;
                 for (int j = J0; j < J1; j++, jf += 1.f, hrow += lp, arow += lp) {
-                    // prefix integral at this lane's edge on line j; x >= 0 is the
-                    // padded coordinate, floored by a round-down add against 1.5*2^23
-                    const float x = fmaf(r, jf, X);
+                    // prefix integral at this lane's edge on line j: cell kk and
+                    // fraction f of the padded position, floored by a round-down
+                    // add against 1.5*2^23.  Positions beyond the padded line clamp
+                    // to its ends, where the prefix is 0 or the line total and the
+                    // value 0, so a ray that misses line j adds exactly 0.
+                    const float x = fmaf(r, jf, Xf);
                     const float y = __fadd_rd(x, kFloorBias);
-                    const unsigned kk = min((unsigned)(__float_as_int(y) - kFloorBiasBits), lpm1);
+                    const unsigned kk = min((unsigned)max(__float_as_int(y) + Xi, 0), lpm1);
                     const float f = x - (y - kFloorBias);
                     const float2 h = hrow[kk];
                     const float hi = h.x, rest = fmaf(f, arow[kk], h.y);
@@ -354,12 +380,12 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                     const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
                     const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
                     const float dP = (nhi - hi) + (nrest - rest);
-                    if ((unsigned)(j - jb) < (unsigned)jn) a = fmaf(dP, g[j], a);
+                    a = fmaf(dP, g[j], a);
                 }
                 acc[k] = a;
             }
         }
-        __syncthreads();
+        if (c + 1 < nchunks) line_factors(c + 1);
     }
     if (!ok) return;
 
@@ -430,7 +456,8 @@ __global__ void fan_table_kernel(const float* __restrict__ prj, const BpSlice* _
                                   : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
                 s *= L;
             }
-            W = (double)s;
+            // matched tables carry the sign and the 1/2 of the two-line average
+            W = type == RN_TYPE_MATCHED ? (double)(s * (0.5f * vg.sigma)) : (double)s;
         }
         double incl = warp_incl_scan(W);
         double excl = carry + incl - W;
@@ -487,15 +514,120 @@ struct BpView {
 };
 
 struct BpShared {
+    ViewGeo rec[2][kBpViews];   // view records staged for the next chunk
     uint64_t bars[2];
-    int elo[2][kBpViews];
-    BpView vw[2][kBpViews];
+    int elo[3][kBpViews];       // first staged table entry per view
+    BpView vw[3][kBpViews];
 };
 
 // Edge index t of the matched parametrisation for a slope r
 // (r = (q - par) / (l - perp) at lattice point (line l, position q)).
 __device__ __forceinline__ float matched_t(const ViewGeo& vg, float r) {
     return vg.tA + vg.tB * atanf(vg.kappa * r);
+}
+
+// Matched backprojection of one view into a thread's 4x4 pixels at (x0, y0):
+// lattice lines are rows (X-class, kX) or columns, positions q along them.
+// The staged table window T starts at table index ilo; entries carry the
+// prefix (hi, lo), the slope scaled by sigma / 2 and the edge slope r_e.
+__device__ __forceinline__ void bp_matched_view(float (&acc)[4][4], const BpView& vg, const float4* T, int ilo,
+                                                int imax, int x0, int y0, int nl, bool kX) {
+    const int L0 = kX ? y0 : x0;
+    const int Q0 = kX ? x0 : y0;
+    const float par = vg.par, perp = vg.perp;
+    // edge index t(r) = tA + tB atan(kappa r) as a cubic around the slope r_t
+    // of this thread's block centre: truncation below 2e-5 cells over the 5x5
+    // lattice (it only selects the footprint; the fraction inside it is
+    // exact).  Approximate reciprocals: rt is only the expansion point, and a
+    // relative error in g scales all slopes of a line alike.
+    const float rt = __fdividef((float)(Q0 + 2) - par, (float)(L0 + 2) - perp);
+    const float ut = vg.kappa * rt;
+    const float iw = __fdividef(1.0f, fmaf(ut, ut, 1.0f));
+    const float k1 = vg.tB * vg.kappa * iw;
+    const float c0 = fmaf(vg.tB, atanf(ut), vg.tA);
+    const float c1 = k1;
+    const float c2 = -k1 * vg.kappa * ut * iw;
+    const float c3 = k1 * vg.kappa * vg.kappa * (fmaf(3.0f * ut, ut, -1.0f) * (1.0f / 3.0f)) * iw * iw;
+    float dq[5];
+#pragma unroll
+    for (int qi = 0; qi < 5; qi++) dq[qi] = (float)(Q0 + qi) - par;
+    float dprev[4];
+#pragma unroll
+    for (int li = 0; li < 5; li++) {
+        const int l = L0 + li;
+        const float g = __fdividef(1.0f, (float)l - perp);
+        float fh[5], fl[5];
+#pragma unroll
+        for (int qi = 0; qi < 5; qi++) {
+            const float r = dq[qi] * g;
+            const float h = r - rt;
+            const float t = fmaf(h, fmaf(h, fmaf(h, c3, c2), c1), c0);
+            // table index floor(t) + 1 for |t| < 2^22 via a round-down add;
+            // beyond the detector it reaches a zero-slope guard entry
+            int i = __float_as_int(__fadd_rd(t, 12582912.0f)) - (0x4B400000 - 1);
+            i = min(max(i, ilo), imax);
+            const float4 E = T[i - ilo];
+            fh[qi] = E.x;
+            fl[qi] = fmaf(E.z, r - E.w, E.y);
+        }
+        float dcur[4];
+#pragma unroll
+        for (int qi = 0; qi < 4; qi++) dcur[qi] = (fh[qi + 1] - fh[qi]) + (fl[qi + 1] - fl[qi]);
+        if (li > 0) {
+            const float m = (l < nl) ? 1.f : 0.f;   // line l exists?
+#pragma unroll
+            for (int qi = 0; qi < 4; qi++) {
+                const float v2 = fmaf(m, dcur[qi], dprev[qi]);
+                if (kX) acc[qi][li - 1] += v2;
+                else acc[li - 1][qi] += v2;
+            }
+        }
+#pragma unroll
+        for (int qi = 0; qi < 4; qi++) dprev[qi] = dcur[qi];
+    }
+}
+
+// Warp 0 of a backprojection CTA prepares chunk c (views c*kBpViews ...) of
+// its tile at (X0, Y0): lane = view * 4 + tile corner evaluates the edge index
+// at its corner, a 4-lane min gives the first staged table entry, and the
+// view's parameters go to slot c % 3.  Kept out of line: it runs once per
+// chunk in one warp, and inlined its temporaries would raise the register
+// count of the whole accumulation loop.
+template <bool kMatched>
+__device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, int nview, int X0, int Y0,
+                                     int tabn, int win, const FanDims d) {
+    const int lane = threadIdx.x & 31, v = lane >> 2, corner = lane & 3;
+    const bool valid = c * kBpViews + v < nview;
+    const ViewGeo& vg = src[valid ? v : 0];
+    const int cx = corner & 1, cy = corner >> 1;
+    float t;
+    if (kMatched) {
+        const int xcls = vg.xcls;
+        const float X = (float)(X0 + cx * kBpTile), Y = (float)(Y0 + cy * kBpTile);
+        const float l = xcls ? Y : X, q = xcls ? X : Y;
+        t = matched_t(vg, (q - (float)vg.par) / (l - (float)vg.perp));
+    } else {
+        const float px = ((float)(X0 + cx * kBpTile) - 0.5f - (d.nx - 1) * 0.5f) * d.dx;
+        const float py = ((float)(Y0 + cy * kBpTile) - 0.5f - (d.ny - 1) * 0.5f) * d.dy;
+        t = ref_t(px, py, vg.cosd, vg.sind, d);
+    }
+    t = fminf(t, __shfl_xor_sync(0xffffffffu, t, 1));
+    t = fminf(t, __shfl_xor_sync(0xffffffffu, t, 2));
+    if (valid && corner == 0) {
+        const int slot = c % 3;
+        const int lo = (int)floorf(t) + 1 - 2;   // table index = edge/cell index + 1
+        sh->elo[slot][v] = max(0, min(lo, tabn - win));
+        BpView& w = sh->vw[slot][v];
+        w.par = (float)vg.par;
+        w.perp = (float)vg.perp;
+        w.kappa = vg.kappa;
+        w.tA = vg.tA;
+        w.tB = vg.tB;
+        w.sigma = vg.sigma;
+        w.cosd = vg.cosd;
+        w.sind = vg.sind;
+        w.xcls = vg.xcls;
+    }
 }
 
 template <bool kMatched>
@@ -525,70 +657,30 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
         fence_mbar_init();
     }
 
-    // window of table entries touched by the CTA tile for view vl
-    auto window = [&](int vl) -> int {
-        const ViewGeo vg = p.views[gs.view_off + vl];
-        float tmin = 1e30f, tmax = -1e30f;
-#pragma unroll
-        for (int cx = 0; cx < 2; cx++)
-#pragma unroll
-            for (int cy = 0; cy < 2; cy++) {
-                float t;
-                if (kMatched) {
-                    float X = (float)(X0 + cx * kBpTile), Y = (float)(Y0 + cy * kBpTile);
-                    float l = vg.xcls ? Y : X, q = vg.xcls ? X : Y;
-                    float r = (q - (float)vg.par) / (l - (float)vg.perp);
-                    t = matched_t(vg, r);
-                } else {
-                    float px = ((float)(X0 + cx * kBpTile) - 0.5f - (nx - 1) * 0.5f) * p.d.dx;
-                    float py = ((float)(Y0 + cy * kBpTile) - 0.5f - (ny - 1) * 0.5f) * p.d.dy;
-                    t = ref_t(px, py, vg.cosd, vg.sind, p.d);
-                }
-                tmin = fminf(tmin, t);
-                tmax = fmaxf(tmax, t);
-            }
-        int lo = (int)floorf(tmin) + 1 - 2;   // table index = edge/cell index + 1
-        lo = max(0, min(lo, tabn - p.win));
-        return lo;
-    };
-
     const int nchunks = (gs.nview + kBpViews - 1) / kBpViews;
-    auto prep = [&](int c) {   // threads < kBpViews compute windows for chunk c
-        if (tid < kBpViews) {
-            int vl = c * kBpViews + tid;
-            int b = c & 1;
-            if (vl < gs.nview) {
-                sh->elo[b][tid] = window(vl);
-                const ViewGeo& vg = p.views[gs.view_off + vl];
-                BpView& w = sh->vw[b][tid];
-                w.par = (float)vg.par;
-                w.perp = (float)vg.perp;
-                w.kappa = vg.kappa;
-                w.tA = vg.tA;
-                w.tB = vg.tB;
-                w.sigma = vg.sigma;
-                w.cosd = vg.cosd;
-                w.sind = vg.sind;
-                w.xcls = vg.xcls;
-            }
-        }
+    auto prep = [&](int c, const ViewGeo* src) {
+        bp_prep<kMatched>(sh, src, c, gs.nview, X0, Y0, tabn, p.win, p.d);
     };
+    // tid 0: stage chunk c's table windows into buffer c & 1 and the view
+    // records of chunk c + 1 into record slot (c + 1) & 1, on barrier c & 1.
     auto issue = [&](int c) {
-        int b = c & 1;
-        int vc = min(kBpViews, gs.nview - c * kBpViews);
-        uint32_t total = 0;
-        int cnt = min(p.win, tabn);
-        total = (uint32_t)(vc * cnt * sizeof(float4));
+        const int b = c & 1;
+        const int vc = min(kBpViews, gs.nview - c * kBpViews);
+        const int cnt = min(p.win, tabn);
+        const int vn = c + 1 < nchunks ? min(kBpViews, gs.nview - (c + 1) * kBpViews) : 0;
         fence_proxy_async();
-        mbar_arrive_expect_tx(&sh->bars[b], total);
+        mbar_arrive_expect_tx(&sh->bars[b], (uint32_t)(vc * cnt * sizeof(float4) + vn * sizeof(ViewGeo)));
         for (int v = 0; v < vc; v++) {
-            int vl = c * kBpViews + v;
-            bulk_g2s(buf0 + (b * kBpViews + v) * p.win, gtab + (long long)vl * tabn + sh->elo[b][v],
+            const int vl = c * kBpViews + v;
+            bulk_g2s(buf0 + (b * kBpViews + v) * p.win, gtab + (long long)vl * tabn + sh->elo[c % 3][v],
                      (uint32_t)(cnt * sizeof(float4)), &sh->bars[b]);
         }
+        if (vn > 0)
+            bulk_g2s(sh->rec[(c + 1) & 1], p.views + gs.view_off + (c + 1) * kBpViews,
+                     (uint32_t)(vn * sizeof(ViewGeo)), &sh->bars[b]);
     };
 
-    prep(0);
+    if (tid < 32) prep(0, p.views + gs.view_off);
     __syncthreads();
     if (tid == 0) issue(0);
 
@@ -598,80 +690,31 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
 
+    // One barrier per chunk: after it every warp has finished chunk c - 1, so
+    // buffer (c + 1) & 1 and record slot c & 1 may be refilled; window and
+    // parameter slots rotate over three chunks because warp 0 prepares chunk
+    // c + 1 while other warps may still compute chunk c - 1.
     bool ok = true;
     for (int c = 0; c < nchunks; c++) {
         const int b = c & 1;
-        if (c + 1 < nchunks) prep(c + 1);
-        __syncthreads();
-        if (tid == 0 && c + 1 < nchunks) issue(c + 1);
         if (!mbar_wait(&sh->bars[b], (uint32_t)((c >> 1) & 1))) ok = false;
+        if (tid < 32 && c + 1 < nchunks) prep(c + 1, sh->rec[(c + 1) & 1]);
         if (!__syncthreads_and(ok)) {
             if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
             ok = false;
             break;
         }
+        if (tid == 0 && c + 1 < nchunks) issue(c + 1);
+        const int slot = c % 3;
         const int vc = min(kBpViews, gs.nview - c * kBpViews);
         for (int v = 0; v < vc; v++) {
-            const BpView vg = sh->vw[b][v];
+            const BpView vg = sh->vw[slot][v];
             const float4* T = buf0 + (b * kBpViews + v) * p.win;
-            const int ilo = sh->elo[b][v];
+            const int ilo = sh->elo[slot][v];
             const int cnt = min(p.win, tabn);
             const int imax = ilo + cnt - 1;   // <= nu + 1
             if (kMatched) {
-                // lattice lines: rows (X) or columns (Y); positions along them
-                const int L0 = vg.xcls ? y0 : x0;
-                const int Q0 = vg.xcls ? x0 : y0;
-                const int nl = vg.xcls ? ny : nx;
-                const float par = vg.par, perp = vg.perp;
-                // edge index t(r) = tA + tB atan(kappa r) as a cubic around the
-                // slope r_t of this thread's block centre: truncation below
-                // 2e-5 cells over the 5x5 lattice (it only selects the
-                // footprint; the fraction inside it is exact)
-                const float rt = ((float)(Q0 + 2) - par) / ((float)(L0 + 2) - perp);
-                const float ut = vg.kappa * rt;
-                const float iw = 1.0f / fmaf(ut, ut, 1.0f);
-                const float k1 = vg.tB * vg.kappa * iw;
-                const float c0 = fmaf(vg.tB, atanf(ut), vg.tA);
-                const float c1 = k1;
-                const float c2 = -k1 * vg.kappa * ut * iw;
-                const float c3 = k1 * vg.kappa * vg.kappa * (fmaf(3.0f * ut, ut, -1.0f) * (1.0f / 3.0f)) * iw * iw;
-                float dq[5];
-#pragma unroll
-                for (int qi = 0; qi < 5; qi++) dq[qi] = (float)(Q0 + qi) - par;
-                float dprev[4];
-#pragma unroll
-                for (int li = 0; li < 5; li++) {
-                    const int l = L0 + li;
-                    const float g = 1.0f / ((float)l - perp);
-                    float fh[5], fl[5];
-#pragma unroll
-                    for (int qi = 0; qi < 5; qi++) {
-                        float r = dq[qi] * g;
-                        float h = r - rt;
-                        float t = fmaf(h, fmaf(h, fmaf(h, c3, c2), c1), c0);
-                        // table index floor(t) + 1 for |t| < 2^22 via a round-down add;
-                        // beyond the detector it reaches a zero-slope guard entry
-                        int i = __float_as_int(__fadd_rd(t, 12582912.0f)) - (0x4B400000 - 1);
-                        i = min(max(i, ilo), imax);
-                        float4 E = T[i - ilo];
-                        fh[qi] = E.x;
-                        fl[qi] = fmaf(E.z, r - E.w, E.y);
-                    }
-                    float dcur[4];
-#pragma unroll
-                    for (int qi = 0; qi < 4; qi++) dcur[qi] = (fh[qi + 1] - fh[qi]) + (fl[qi + 1] - fl[qi]);
-                    if (li > 0) {
-                        const float m = (l < nl) ? 1.f : 0.f;   // line l exists?
-#pragma unroll
-                        for (int qi = 0; qi < 4; qi++) {
-                            float v2 = vg.sigma * 0.5f * (dprev[qi] + m * dcur[qi]);
-                            if (vg.xcls) acc[qi][li - 1] += v2;
-                            else acc[li - 1][qi] += v2;
-                        }
-                    }
-#pragma unroll
-                    for (int qi = 0; qi < 4; qi++) dprev[qi] = dcur[qi];
-                }
+                bp_matched_view(acc, vg, T, ilo, imax, x0, y0, vg.xcls ? ny : nx, vg.xcls);
             } else {
                 // reference DDBPFanKernelX/Y: pixel edges at the pixel centre line
                 const float cs = vg.cosd, sn = vg.sind;
@@ -718,7 +761,6 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                 }
             }
         }
-        __syncthreads();
     }
     if (!ok) return;
 
@@ -744,7 +786,7 @@ int fan_fp_views(int nu) {
 }
 
 static size_t fp_smem_bytes(int nu, int lp, int R) {
-    size_t off = 128 + sizeof(float) * kFpViews * kFpMaxLines + sizeof(float4) * (size_t)fan_fp_views(nu) * (nu + 1);
+    size_t off = kFpHeader + sizeof(float4) * (size_t)fan_fp_views(nu) * (nu + 1);
     off = (off + 127) & ~size_t(127);
     return off + 2 * (size_t)R * lp * (sizeof(float2) + sizeof(float));
 }
@@ -847,7 +889,7 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
             int nl = xc ? g.ny : g.nx;
             double side = (nl / 2.0 - q.perp) > 0 ? 1.0 : -1.0;
             q.sigma = (float)((r1 > r0 ? 1.0 : -1.0) * side);
-            q.pad = 0;
+            q.pad[0] = q.pad[1] = q.pad[2] = 0;
             vcs[v] = make_double2(c, s);
             vx[v] = xc;
             if (xc) nxv++;
@@ -1179,7 +1221,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
         q.rmax = (float)std::max(r0, r1);
         int nl = xc ? ny : nx;
         q.sigma = (float)((r1 > r0 ? 1.0 : -1.0) * ((nl / 2.0 - q.perp) > 0 ? 1.0 : -1.0));
-        q.pad = 0;
+        q.pad[0] = q.pad[1] = q.pad[2] = 0;
         if (std::fabs(q.perp - nl / 2.0) <= nl / 2.0 + 1.0)
             return set_error(RN_ERR_ARG, "fan geometry: source inside the image footprint");
         vcs[v] = make_double2(c, s);

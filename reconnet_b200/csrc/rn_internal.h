@@ -51,8 +51,9 @@ struct ViewGeo {
     float rmin, rmax;   // slope range covered by the detector
     float sigma;        // +-1: do edge indices increase along the line?
     int xcls;           // 1 = X-class
-    int pad;
+    int pad[3];         // 64-byte records: chunks of them are bulk-copyable
 };
+static_assert(sizeof(ViewGeo) == 64, "ViewGeo is staged by 16-byte bulk copies");
 
 // A 2D forward problem: sinogram plane at prj_off (strides su, sview)
 // projected from a mix of up to 2 image planes (z interpolation).

@@ -107,7 +107,7 @@ def test_unrolled_ossqs_gradients_match_finite_differences(rng):
 
     def loss(step, tvw, x_init=x0, checkpoint=True):
         x = unrolled_ossqs(x_init, plans, bs, ws, norm, step, tvw, checkpoint=checkpoint)
-        return ((x - truth) ** 2).sum()
+        return ((x - truth).double() ** 2).sum()
 
     step = torch.tensor([0.8, 0.9, 1.0], device="cuda", requires_grad=True)
     tvw = torch.tensor([0.02, 0.01, 0.005], device="cuda", requires_grad=True)
@@ -129,7 +129,9 @@ def test_unrolled_ossqs_gradients_match_finite_differences(rng):
     # directional derivative w.r.t. the starting image
     x_init = (0.01 * torch.rand_like(truth)).requires_grad_(True)
     gx, = torch.autograd.grad(loss(step.detach(), tvw.detach(), x_init), (x_init,))
-    v = torch.randn_like(truth) * 1e-5    # well inside the TV smoothing scale sqrt(1e-6)
+    # a step along the gradient (a random direction is nearly orthogonal to it),
+    # 1e-5 at most per pixel: well inside the TV smoothing scale sqrt(1e-6)
+    v = gx / gx.abs().max() * 1e-5
     with torch.no_grad():
         fd = float(loss(step, tvw, x_init + v) - loss(step, tvw, x_init - v)) / 2
     assert abs(fd - float((gx * v).sum())) <= 2e-2 * abs(fd)
