@@ -648,7 +648,12 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
     const int nu = p.d.nu, nx = p.d.nx, ny = p.d.ny;
     const int tid = threadIdx.x;
     const int X0 = txi * kBpTile, Y0 = tyi * kBpTile;            // CTA pixel origin
-    const int x0 = X0 + (tid & 15) * 4, y0 = Y0 + (tid >> 4) * 4; // thread pixel origin
+    // thread pixel origin: a warp covers 8 x 4 threads (32 x 16 pixels), and
+    // each group of 8 lanes that shares one shared-memory wavefront covers
+    // 2 x 4 threads, so its table reads spread over distinct banks more often
+    const int lane = tid & 31, warp = tid >> 5;
+    const int tx = ((warp & 1) << 3) | (lane & 1) | ((lane >> 3) << 1), ty = ((warp >> 1) << 2) | ((lane >> 1) & 3);
+    const int x0 = X0 + tx * 4, y0 = Y0 + ty * 4;
     const int tabn = nu + 2;   // table entries per view (guard + nu + total)
 
     if (tid == 0) {
