@@ -272,16 +272,20 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     const int ngpv = (nu + kFpGroupRays - 1) / kFpGroupRays;    // groups per view
     const int ngroups = vcount * ngpv;
     const double n_d = (double)(xcls ? p.d.nx : p.d.ny);
-    int urng[kFpGroups];
+    // per group: line range (lb << 16 | le) and this lane's edge-table slot
+    // (view << 16 | entry), fixed for the whole kernel
+    int urng[kFpGroups], gslot[kFpGroups];
     float acc[kFpGroups];
 #pragma unroll
     for (int k = 0; k < kFpGroups; k++) {
         acc[k] = 0.f;
         urng[k] = 0;
+        gslot[k] = 0;
         const int grp = warp + k * kFpWarps;
         if (grp < ngroups) {   // warp-uniform
             const int v = grp / ngpv;
             const int u = (grp - v * ngpv) * kFpGroupRays + lane;
+            gslot[k] = (v << 16) | (v * (nu + 1) + min(u, nu));
             int rng = 0;
             if (lane < kFpGroupRays && u < nu) {
                 const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
@@ -338,51 +342,80 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         const float2* HL = reinterpret_cast<const float2*>(buf0 + b * buf_bytes);
         const float* LA = reinterpret_cast<const float*>(buf0 + b * buf_bytes + hl_bytes);
         const float fl0 = (float)l0;
+        // edge position of group k's lane at the chunk's first line, Xi0 + Xf0 +
+        // (rhi + rlo) l0, split into an integer cell Xi (floor bias folded in)
+        // and a small offset Xf with error-free steps: rhi l0 = pr + pe exactly,
+        // pr = floor(pr) + pf exactly.  Per-line positions then stay below ~50
+        // cells and keep ~1e-6 cells of precision.
+        auto setup = [&](int k, int& Xi, float& Xf, float& r, const float*& g) {
+            const float4 E = s_edge[gslot[k] & 0xffff];
+            const float pr = E.z * fl0;
+            const float pe = fmaf(E.z, fl0, -pr);
+            const float py = __fadd_rd(pr, kFloorBias);
+            const float pf = pr - (py - kFloorBias);
+            Xi = __float_as_int(E.y) + (__float_as_int(py) - kFloorBiasBits) - kFloorBiasBits;
+            Xf = (E.x + pf) + fmaf(E.w, fl0, pe);
+            r = E.z;
+            g = s_g + b * kFpViews * kFpMaxLines + (gslot[k] >> 16) * kFpMaxLines;
+        };
+        // prefix integral at this lane's edge on line j and the footprint
+        // difference with the next lane's edge: cell kk and fraction f of the
+        // padded position, floored by a round-down add against 1.5*2^23.
+        // Positions beyond the padded line clamp to its ends, where the prefix
+        // is 0 or the line total and the value 0, so a ray that misses line j
+        // adds exactly 0.
+        auto footprint = [&](float jf, int Xi, float Xf, float r, const float2* hrow, const float* arow) -> float {
+            const float x = fmaf(r, jf, Xf);
+            const float y = __fadd_rd(x, kFloorBias);
+            const unsigned kk = min((unsigned)max(__float_as_int(y) + Xi, 0), lpm1);
+            const float f = x - (y - kFloorBias);
+            const float2 h = hrow[kk];
+            const float hi = h.x, rest = fmaf(f, arow[kk], h.y);
+            const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
+            const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
+            return (nhi - hi) + (nrest - rest);
+        };
+        auto single = [&](int k, int J0, int J1) {
+            int Xi;
+            float Xf, r;
+            const float* g;
+            setup(k, Xi, Xf, r, g);
+            const float2* hrow = HL + J0 * lp;
+            const float* arow = LA + J0 * lp;
+            float a = acc[k];
+            float jf = (float)J0;
+            for (int j = J0; j < J1; j++, jf += 1.f, hrow += lp, arow += lp)
+                a = fmaf(footprint(jf, Xi, Xf, r, hrow, arow), g[j], a);
+            acc[k] = a;
+        };
+        // groups in pairs: where both have lines in this chunk, one loop over
+        // the union of their ranges runs two independent chains (a group adds
+        // exactly 0 on lines outside its range)
 #pragma unroll
-        for (int k = 0; k < kFpGroups; k++) {
-            const int J0 = max((urng[k] >> 16) - l0, 0);
-            const int J1 = min((urng[k] & 0xffff) - l0, rc);
-            if (J0 < J1) {   // warp-uniform
-                const int grp = warp + k * kFpWarps;
-                const int v = grp / ngpv;
-                const int e = min((grp - v * ngpv) * kFpGroupRays + lane, nu);
-                const float4 E = s_edge[v * (nu + 1) + e];
-                // edge position at the chunk's first line, Xi0 + Xf0 + (rhi + rlo) l0,
-                // split into an integer cell Xi (floor bias folded in) and a small
-                // offset Xf with error-free steps: rhi l0 = pr + pe exactly, pr =
-                // floor(pr) + pf exactly.  Per-line positions then stay below ~50
-                // cells and keep ~1e-6 cells of precision.
-                const float pr = E.z * fl0;
-                const float pe = fmaf(E.z, fl0, -pr);
-                const float py = __fadd_rd(pr, kFloorBias);
-                const float pf = pr - (py - kFloorBias);
-                const int Xi = __float_as_int(E.y) + (__float_as_int(py) - kFloorBiasBits) - kFloorBiasBits;
-                const float Xf = (E.x + pf) + fmaf(E.w, fl0, pe);
-                const float r = E.z;
-                const float* g = s_g + b * kFpViews * kFpMaxLines + v * kFpMaxLines;
+        for (int k = 0; k < kFpGroups; k += 2) {
+            const int J0a = max((urng[k] >> 16) - l0, 0), J1a = min((urng[k] & 0xffff) - l0, rc);
+            const int J0b = max((urng[k + 1] >> 16) - l0, 0), J1b = min((urng[k + 1] & 0xffff) - l0, rc);
+            if (J0a < J1a && J0b < J1b) {   // warp-uniform
+                int Xia, Xib;
+                float Xfa, Xfb, ra, rb;
+                const float *ga, *gb;
+                setup(k, Xia, Xfa, ra, ga);
+                setup(k + 1, Xib, Xfb, rb, gb);
+                const int J0 = min(J0a, J0b), J1 = max(J1a, J1b);
                 const float2* hrow = HL + J0 * lp;
                 const float* arow = LA + J0 * lp;
-                float a = acc[k];
+                float aa = acc[k], ab = acc[k + 1];
                 float jf = (float)J0;
                 for (int j = J0; j < J1; j++, jf += 1.f, hrow += lp, arow += lp) {
-                    // prefix integral at this lane's edge on line j: cell kk and
-                    // fraction f of the padded position, floored by a round-down
-                    // add against 1.5*2^23.  Positions beyond the padded line clamp
-                    // to its ends, where the prefix is 0 or the line total and the
-                    // value 0, so a ray that misses line j adds exactly 0.
-                    const float x = fmaf(r, jf, Xf);
-                    const float y = __fadd_rd(x, kFloorBias);
-                    const unsigned kk = min((unsigned)max(__float_as_int(y) + Xi, 0), lpm1);
-                    const float f = x - (y - kFloorBias);
-                    const float2 h = hrow[kk];
-                    const float hi = h.x, rest = fmaf(f, arow[kk], h.y);
-                    // footprint difference with the next lane's edge
-                    const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
-                    const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
-                    const float dP = (nhi - hi) + (nrest - rest);
-                    a = fmaf(dP, g[j], a);
+                    aa = fmaf(footprint(jf, Xia, Xfa, ra, hrow, arow), ga[j], aa);
+                    ab = fmaf(footprint(jf, Xib, Xfb, rb, hrow, arow), gb[j], ab);
                 }
-                acc[k] = a;
+                acc[k] = aa;
+                acc[k + 1] = ab;
+            } else if (J0a < J1a) {
+                single(k, J0a, J1a);
+            } else if (J0b < J1b) {
+                single(k + 1, J0b, J1b);
             }
         }
         if (c + 1 < nchunks) line_factors(c + 1);
