@@ -101,8 +101,8 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
     int n = xl ? d.nx : d.ny;
     int lp = xl ? d.lpx : d.lpy;
     const int M = d.margin;
-    long long base = (long long)si * slot_elems + (xl ? (long long)l * d.lpx : (long long)d.ny * d.lpx + (long long)l * d.lpy);
-    float2* ohl = hl + base;    // entry j holds position k = j - M
+    long long base = (long long)si * slot_elems + (xl ? (long long)l * d.spx : (long long)d.ny * d.spx + (long long)l * d.spy);
+    float2* ohl = hl + base;    // entry j (at line_pos(j)) holds position k = j - M
     float* ola = la + base;
     double carry = 0.0;
     for (int k0 = 0; k0 < n; k0 += 32) {
@@ -131,20 +131,20 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
         double incl = warp_incl_scan(a);
         double excl = carry + incl - a;
         if (k < n) {
-            ohl[k + M] = split_double(excl);
-            ola[k + M] = (float)a;
+            ohl[line_pos(k + M)] = split_double(excl);
+            ola[line_pos(k + M)] = (float)a;
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     // margins: P = 0 before the line, P = total from position n on
     float2 tot = split_double(carry);
     for (int j = lane; j < M; j += 32) {
-        ohl[j] = make_float2(0.f, 0.f);
-        ola[j] = 0.f;
+        ohl[line_pos(j)] = make_float2(0.f, 0.f);
+        ola[line_pos(j)] = 0.f;
     }
     for (int j = n + M + lane; j < lp; j += 32) {
-        ohl[j] = tot;
-        ola[j] = 0.f;
+        ohl[line_pos(j)] = tot;
+        ola[line_pos(j)] = 0.f;
     }
 }
 
@@ -220,9 +220,10 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     const GeoSet gs = p.sets[fs.set];
     const int nu = p.d.nu;
     const int nlines = xcls ? p.d.ny : p.d.nx;
-    const int lp = xcls ? p.d.lpx : p.d.lpy;
+    const int lp = xcls ? p.d.lpx : p.d.lpy;   // entries per line
+    const int sp = xcls ? p.d.spx : p.d.spy;   // line stride (padded)
     const int R = p.R;
-    const long long slot = (long long)(s - p.slot_base) * p.slot_elems + (xcls ? 0ll : (long long)p.d.ny * p.d.lpx);
+    const long long slot = (long long)(s - p.slot_base) * p.slot_elems + (xcls ? 0ll : (long long)p.d.ny * p.d.spx);
     const float2* ghl = p.hl + slot;
     const float* gla = p.la + slot;
 
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     size_t off = kFpHeader + sizeof(float4) * (size_t)p.vt * (nu + 1);
     off = (off + 127) & ~size_t(127);
     // double buffer: buffer b holds R lines of (hi, lo) then R lines of values
-    const size_t hl_bytes = (size_t)R * lp * sizeof(float2), la_bytes = (size_t)R * lp * sizeof(float);
+    const size_t hl_bytes = (size_t)R * sp * sizeof(float2), la_bytes = (size_t)R * sp * sizeof(float);
     unsigned char* const buf0 = smem + off;
     const size_t buf_bytes = hl_bytes + la_bytes;
 
@@ -305,13 +306,13 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         int b = c & 1;
         int l0 = c * R;
         int rc = min(R, nlines - l0);
-        uint32_t bh = (uint32_t)((size_t)rc * lp * sizeof(float2));
-        uint32_t ba = (uint32_t)((size_t)rc * lp * sizeof(float));
+        uint32_t bh = (uint32_t)((size_t)rc * sp * sizeof(float2));
+        uint32_t ba = (uint32_t)((size_t)rc * sp * sizeof(float));
         unsigned char* dst = buf0 + b * buf_bytes;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bars[b], bh + ba);
-        bulk_g2s(dst, ghl + (long long)l0 * lp, bh, &bars[b]);
-        bulk_g2s(dst + hl_bytes, gla + (long long)l0 * lp, ba, &bars[b]);
+        bulk_g2s(dst, ghl + (long long)l0 * sp, bh, &bars[b]);
+        bulk_g2s(dst + hl_bytes, gla + (long long)l0 * sp, ba, &bars[b]);
     };
     // per-line factors 1 / (l - perp) of chunk c into slot c & 1
     auto line_factors = [&](int c) {
@@ -368,9 +369,10 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             const float x = fmaf(r, jf, Xf);
             const float y = __fadd_rd(x, kFloorBias);
             const unsigned kk = min((unsigned)max(__float_as_int(y) + Xi, 0), lpm1);
+            const unsigned pos = kk + (kk >> 4);   // line_pos
             const float f = x - (y - kFloorBias);
-            const float2 h = hrow[kk];
-            const float hi = h.x, rest = fmaf(f, arow[kk], h.y);
+            const float2 h = hrow[pos];
+            const float hi = h.x, rest = fmaf(f, arow[pos], h.y);
             const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
             const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
             return (nhi - hi) + (nrest - rest);
@@ -380,11 +382,11 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             float Xf, r;
             const float* g;
             setup(k, Xi, Xf, r, g);
-            const float2* hrow = HL + J0 * lp;
-            const float* arow = LA + J0 * lp;
+            const float2* hrow = HL + J0 * sp;
+            const float* arow = LA + J0 * sp;
             float a = acc[k];
             float jf = (float)J0;
-            for (int j = J0; j < J1; j++, jf += 1.f, hrow += lp, arow += lp)
+            for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp)
                 a = fmaf(footprint(jf, Xi, Xf, r, hrow, arow), g[j], a);
             acc[k] = a;
         };
@@ -402,11 +404,11 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                 setup(k, Xia, Xfa, ra, ga);
                 setup(k + 1, Xib, Xfb, rb, gb);
                 const int J0 = min(J0a, J0b), J1 = max(J1a, J1b);
-                const float2* hrow = HL + J0 * lp;
-                const float* arow = LA + J0 * lp;
+                const float2* hrow = HL + J0 * sp;
+                const float* arow = LA + J0 * sp;
                 float aa = acc[k], ab = acc[k + 1];
                 float jf = (float)J0;
-                for (int j = J0; j < J1; j++, jf += 1.f, hrow += lp, arow += lp) {
+                for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp) {
                     aa = fmaf(footprint(jf, Xia, Xfa, ra, hrow, arow), ga[j], aa);
                     ab = fmaf(footprint(jf, Xib, Xfb, rb, hrow, arow), gb[j], ab);
                 }
@@ -823,10 +825,10 @@ int fan_fp_views(int nu) {
     return std::min(kFpViews, (kFpGroups * (kFpThreads / 32)) / ngpv);
 }
 
-static size_t fp_smem_bytes(int nu, int lp, int R) {
+static size_t fp_smem_bytes(int nu, int sp, int R) {
     size_t off = kFpHeader + sizeof(float4) * (size_t)fan_fp_views(nu) * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    return off + 2 * (size_t)R * lp * (sizeof(float2) + sizeof(float));
+    return off + 2 * (size_t)R * sp * (sizeof(float2) + sizeof(float));
 }
 
 static size_t bp_smem_bytes(int win) {
@@ -949,6 +951,8 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     p->dims.margin = (int)std::ceil(margin);
     p->dims.lpx = (g.nx + 1 + 2 * p->dims.margin + 3) & ~3;
     p->dims.lpy = (g.ny + 1 + 2 * p->dims.margin + 3) & ~3;
+    p->dims.spx = line_stride(p->dims.lpx);
+    p->dims.spy = line_stride(p->dims.lpy);
 
     RN_CUDA_TRY(cudaMalloc(&p->d_views, sizeof(ViewGeo) * V));
     RN_CUDA_TRY(cudaMalloc(&p->d_edges, sizeof(double) * V * (nu + 1)));
@@ -981,19 +985,19 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     return RN_OK;
 }
 
-static int fp_lines_for_smem(int nu, int lp) {
+static int fp_lines_for_smem(int nu, int sp) {
     int R = kFpMaxLines;
-    while (R > 1 && fp_smem_bytes(nu, lp, R) > (size_t)kSmemBudget) R--;
+    while (R > 1 && fp_smem_bytes(nu, sp, R) > (size_t)kSmemBudget) R--;
     return R;
 }
 
 int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st) {
     const FanDims& d = p->dims;
     const int nfp = (int)p->h_fp.size();
-    const int R = std::min(fp_lines_for_smem(d.nu, d.lpx), fp_lines_for_smem(d.nu, d.lpy));
-    if (fp_smem_bytes(d.nu, std::max(d.lpx, d.lpy), R) > (size_t)kSmemBudget)
+    const int R = std::min(fp_lines_for_smem(d.nu, d.spx), fp_lines_for_smem(d.nu, d.spy));
+    if (fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R) > (size_t)kSmemBudget)
         return set_error(RN_ERR_ARG, "fan projection: image lines too long for shared memory");
-    const size_t smem = fp_smem_bytes(d.nu, std::max(d.lpx, d.lpy), R);
+    const size_t smem = fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R);
     // slices are processed in waves of at most `slots` line buffers
     const long long slot = p->line_slot_elems;
     const int slots = (int)std::max<long long>(1, std::min<long long>(nfp, p->fp_slots));
@@ -1179,10 +1183,12 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     d.margin = (int)std::ceil(margin);
     d.lpx = (nx + 1 + 2 * d.margin + 3) & ~3;
     d.lpy = (ny + 1 + 2 * d.margin + 3) & ~3;
+    d.spx = line_stride(d.lpx);
+    d.spy = line_stride(d.lpy);
 
     // scratch layout (offsets in bytes, 256-aligned)
     const int nwork_max = (nview + VT - 1) / VT + 2;
-    const long long slot = (long long)ny * d.lpx + (long long)nx * d.lpy;
+    const long long slot = (long long)ny * d.spx + (long long)nx * d.spy;
     size_t off = 0;
     auto take = [&](size_t bytes) {
         size_t o = off;
@@ -1207,8 +1213,8 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
         return set_error(RN_ERR_ARG, "rn_fan_project_noalloc: this geometry needs " + std::to_string(off) +
                                          " bytes of scratch, more than its fixed " +
                                          std::to_string(kNoAllocScratchBytes) + " bytes");
-    const int R = std::min(fp_lines_for_smem(nu, d.lpx), fp_lines_for_smem(nu, d.lpy));
-    const size_t smem = fp_smem_bytes(nu, std::max(d.lpx, d.lpy), R);
+    const int R = std::min(fp_lines_for_smem(nu, d.spx), fp_lines_for_smem(nu, d.spy));
+    const size_t smem = fp_smem_bytes(nu, std::max(d.spx, d.spy), R);
     if (smem > (size_t)kSmemBudget) return set_error(RN_ERR_ARG, "image lines too long for shared memory");
 
     // host-side tables, same quantities as fan_build_geometry

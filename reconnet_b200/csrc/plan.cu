@@ -68,6 +68,8 @@ static void set_dims(rn_fan_plan* p, long long isx, long long isy) {
     d.margin = 0;            // set with the geometry tables (fan_build_geometry)
     d.lpx = g.nx + 1;
     d.lpy = g.ny + 1;
+    d.spx = line_stride(d.lpx);
+    d.spy = line_stride(d.lpy);
     d.isx = isx;
     d.isy = isy;
 }
@@ -130,7 +132,7 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
 
     // line scratch
     const FanDims& d = p->dims;
-    p->line_slot_elems = (long long)d.ny * d.lpx + (long long)d.nx * d.lpy;
+    p->line_slot_elems = (long long)d.ny * d.spx + (long long)d.nx * d.spy;
     long long slot_bytes = p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float));
     p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(), kLineBudget / slot_bytes));
     RN_CUDA_TRY(cudaMalloc(&p->d_hl, sizeof(float2) * p->fp_slots * p->line_slot_elems));

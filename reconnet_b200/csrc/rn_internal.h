@@ -85,12 +85,19 @@ struct GeoSet {
 };
 
 // Kernel launch parameters shared by the fan kernels.
+// FP line arrays keep one unused slot after every 16 entries (entry j at
+// j + j / 16), so that the lanes of a warp, whose entries are typically 1-1.4
+// apart, do not meet in the same shared-memory bank 16 or 32 entries apart.
+__host__ __device__ inline int line_pos(int j) { return j + (j >> 4); }
+inline int line_stride(int lp) { return (line_pos(lp - 1) + 1 + 3) & ~3; }
+
 struct FanDims {
     int nx, ny, nu;
     float dx, dy;
     float du, off_u, dsd, dso;
     int margin;     // padding entries on each side of an FP line array
     int lpx, lpy;   // FP line lengths: n + 1 + 2 * margin, rounded up to a multiple of 4
+    int spx, spy;   // FP line strides in memory: entry j sits at line_pos(j)
     long long isx, isy;   // image strides (elements) along x and y
 };
 
