@@ -185,6 +185,78 @@ class FanPlan:
         return x_out
 
 
+class StreamedFanPair:
+    """Forward projection followed by the backprojection of its result for a
+    ragged batch of independent slices held in pinned host memory, with the
+    transfers overlapped.
+
+    The slices run in ``groups`` contiguous groups, each with its own plan and
+    device buffers.  A group's host-to-device copy runs on one copy stream, its
+    FP + BP on the caller's current stream, and its device-to-host copy on a
+    second copy stream, so the copies of one group overlap the computation of
+    the others (and of the neighbouring calls).  Results are identical to one
+    plan over the whole batch: every slice is processed independently."""
+
+    def __init__(self, geom: FanGeometry, angles, nview_per_slice: Sequence[int], groups: int = 4,
+                 type_projector: int = N.RN_TYPE_MATCHED, device=None):
+        from types import SimpleNamespace
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        counts = np.asarray(nview_per_slice, np.int64)
+        angles = np.asarray(angles, np.float32).ravel()
+        if counts.sum() != angles.size:
+            raise ValueError("angles must hold sum(nview_per_slice) entries")
+        nsl = len(counts)
+        ngroups = max(1, min(int(groups), nsl))
+        bounds = np.linspace(0, nsl, ngroups + 1).round().astype(int)
+        offs = np.concatenate([[0], np.cumsum(counts)])
+        self.type_projector = int(type_projector)
+        self.nslices = nsl
+        self.groups = []
+        for g in range(ngroups):
+            s0, s1 = int(bounds[g]), int(bounds[g + 1])
+            plan = FanPlan(geom, angles[offs[s0]:offs[s1]], nbatches=s1 - s0, nview_per_slice=counts[s0:s1],
+                           device=self.device)
+            self.groups.append(SimpleNamespace(
+                s0=s0, s1=s1, plan=plan,
+                x=torch.empty(plan.img_shape, device=self.device),
+                p=torch.empty(plan.sino_shape, device=self.device),
+                b=torch.empty(plan.img_shape, device=self.device),
+                h2d=torch.cuda.Event(), comp=torch.cuda.Event(), d2h=torch.cuda.Event()))
+        self.h2d_stream = torch.cuda.Stream(self.device)
+        self.d2h_stream = torch.cuda.Stream(self.device)
+        self.done = torch.cuda.Event()
+
+    def updates(self) -> int:
+        return sum(g.plan.fp_updates() + g.plan.bp_updates() for g in self.groups)
+
+    def __call__(self, host_img: torch.Tensor, host_out: torch.Tensor) -> torch.cuda.Event:
+        """host_img, host_out: pinned float32 [S, nx, ny] host tensors.  Enqueues
+        the work and returns an event that completes when host_out is written."""
+        if host_img.shape[0] != self.nslices or host_out.shape[0] != self.nslices:
+            raise ValueError("host tensors must hold one [nx, ny] image per slice")
+        comp = torch.cuda.current_stream(self.device)
+        for g in self.groups:
+            self.h2d_stream.wait_event(g.comp)          # the previous call's FP has read g.x
+            with torch.cuda.stream(self.h2d_stream):
+                g.x.copy_(host_img[g.s0:g.s1], non_blocking=True)
+                g.h2d.record(self.h2d_stream)
+            comp.wait_event(g.h2d)
+            comp.wait_event(g.d2h)                      # the previous call's copy of g.b is done
+            g.plan.project(g.x, out=g.p)
+            g.plan.backproject(g.p, self.type_projector, out=g.b)
+            g.comp.record(comp)
+            self.d2h_stream.wait_event(g.comp)
+            with torch.cuda.stream(self.d2h_stream):
+                host_out[g.s0:g.s1].copy_(g.b, non_blocking=True)
+                g.d2h.record(self.d2h_stream)
+        self.done.record(self.d2h_stream)
+        return self.done
+
+    def check(self) -> None:
+        for g in self.groups:
+            g.plan.check()
+
+
 class FanProjectFn(torch.autograd.Function):
     """y = A x with dL/dx = A^T dL/dy (A^T = matched backprojection)."""
 

@@ -300,3 +300,25 @@ def test_invalid_arguments_raise():
         plan.project(torch.zeros((1, 3, 3, 1, 1), device="cuda"))
     with pytest.raises(N.ReconNetError):   # source inside the image
         FanPlan(to_geometry(small_fan(dso=20.0, dsd=40.0)), np.zeros(4, np.float32))
+
+
+def test_streamed_pair_matches_single_plan(rng):
+    """StreamedFanPair (slice groups, overlapped host copies) returns exactly
+    what one ragged plan computes, call after call."""
+    import torch
+    from reconnet_b200.torch_ops import FanPlan, StreamedFanPair
+    g = small_fan()
+    counts = np.array([40, 52, 33, 45, 37], np.int64)
+    angles = np.concatenate([(np.arange(n) * 2 * np.pi / n + 0.1 * s).astype(np.float32)
+                             for s, n in enumerate(counts)])
+    geom = to_geometry(g)
+    plan = FanPlan(geom, angles, nbatches=len(counts), nview_per_slice=counts)
+    pair = StreamedFanPair(geom, angles, counts, groups=3)
+    assert pair.updates() == plan.fp_updates() + plan.bp_updates()
+    out = torch.empty((len(counts), g.nx, g.ny), dtype=torch.float32).pin_memory()
+    for call in range(3):
+        imgs = torch.from_numpy(rng.random((len(counts), g.nx, g.ny)).astype(np.float32)).pin_memory()
+        pair(imgs, out).synchronize()
+        pair.check()
+        ref = plan.backproject(plan.project(imgs.cuda()), 2).cpu()
+        assert torch.equal(out, ref), call
