@@ -190,14 +190,18 @@ class StreamedFanPair:
     ragged batch of independent slices held in pinned host memory, with the
     transfers overlapped.
 
-    The slices run in ``groups`` contiguous groups, each with its own plan and
-    device buffers.  A group's host-to-device copy runs on one copy stream, its
-    FP + BP on the caller's current stream, and its device-to-host copy on a
-    second copy stream, so the copies of one group overlap the computation of
-    the others (and of the neighbouring calls).  Results are identical to one
-    plan over the whole batch: every slice is processed independently."""
+    The slices run in ``groups`` contiguous groups, each with its own plan, and
+    the device buffers are double-buffered across calls.  One group gives the
+    best throughput over a sequence of calls (no extra launch tails); more
+    groups also overlap the copies within a single call.  A group's
+    host-to-device copy runs on one copy stream, its FP + BP on the caller's
+    current stream, and its device-to-host copy on a second copy stream.  So a
+    call's copies overlap the computation of its other groups and of the
+    neighbouring calls (the next call's inputs are copied while this call
+    computes).  Results are identical to one plan over the whole batch: every
+    slice is processed independently."""
 
-    def __init__(self, geom: FanGeometry, angles, nview_per_slice: Sequence[int], groups: int = 4,
+    def __init__(self, geom: FanGeometry, angles, nview_per_slice: Sequence[int], groups: int = 1,
                  type_projector: int = N.RN_TYPE_MATCHED, device=None):
         from types import SimpleNamespace
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -216,39 +220,44 @@ class StreamedFanPair:
             s0, s1 = int(bounds[g]), int(bounds[g + 1])
             plan = FanPlan(geom, angles[offs[s0]:offs[s1]], nbatches=s1 - s0, nview_per_slice=counts[s0:s1],
                            device=self.device)
-            self.groups.append(SimpleNamespace(
-                s0=s0, s1=s1, plan=plan,
-                x=torch.empty(plan.img_shape, device=self.device),
-                p=torch.empty(plan.sino_shape, device=self.device),
-                b=torch.empty(plan.img_shape, device=self.device),
-                h2d=torch.cuda.Event(), comp=torch.cuda.Event(), d2h=torch.cuda.Event()))
+            bufs = [SimpleNamespace(x=torch.empty(plan.img_shape, device=self.device),
+                                    b=torch.empty(plan.img_shape, device=self.device),
+                                    h2d=torch.cuda.Event(), comp=torch.cuda.Event(), d2h=torch.cuda.Event())
+                    for _ in range(2)]
+            self.groups.append(SimpleNamespace(s0=s0, s1=s1, plan=plan, bufs=bufs,
+                                               p=torch.empty(plan.sino_shape, device=self.device)))
         self.h2d_stream = torch.cuda.Stream(self.device)
         self.d2h_stream = torch.cuda.Stream(self.device)
         self.done = torch.cuda.Event()
+        self.calls = 0
 
     def updates(self) -> int:
         return sum(g.plan.fp_updates() + g.plan.bp_updates() for g in self.groups)
 
     def __call__(self, host_img: torch.Tensor, host_out: torch.Tensor) -> torch.cuda.Event:
         """host_img, host_out: pinned float32 [S, nx, ny] host tensors.  Enqueues
-        the work and returns an event that completes when host_out is written."""
+        the work and returns an event that completes when host_out is written;
+        host_img may be reused once the call after next has been enqueued."""
         if host_img.shape[0] != self.nslices or host_out.shape[0] != self.nslices:
             raise ValueError("host tensors must hold one [nx, ny] image per slice")
         comp = torch.cuda.current_stream(self.device)
+        k = self.calls & 1
+        self.calls += 1
         for g in self.groups:
-            self.h2d_stream.wait_event(g.comp)          # the previous call's FP has read g.x
+            bf = g.bufs[k]
+            self.h2d_stream.wait_event(bf.comp)         # the FP two calls ago has read bf.x
             with torch.cuda.stream(self.h2d_stream):
-                g.x.copy_(host_img[g.s0:g.s1], non_blocking=True)
-                g.h2d.record(self.h2d_stream)
-            comp.wait_event(g.h2d)
-            comp.wait_event(g.d2h)                      # the previous call's copy of g.b is done
-            g.plan.project(g.x, out=g.p)
-            g.plan.backproject(g.p, self.type_projector, out=g.b)
-            g.comp.record(comp)
-            self.d2h_stream.wait_event(g.comp)
+                bf.x.copy_(host_img[g.s0:g.s1], non_blocking=True)
+                bf.h2d.record(self.h2d_stream)
+            comp.wait_event(bf.h2d)
+            comp.wait_event(bf.d2h)                     # the copy of bf.b two calls ago is done
+            g.plan.project(bf.x, out=g.p)
+            g.plan.backproject(g.p, self.type_projector, out=bf.b)
+            bf.comp.record(comp)
+            self.d2h_stream.wait_event(bf.comp)
             with torch.cuda.stream(self.d2h_stream):
-                host_out[g.s0:g.s1].copy_(g.b, non_blocking=True)
-                g.d2h.record(self.d2h_stream)
+                host_out[g.s0:g.s1].copy_(bf.b, non_blocking=True)
+                bf.d2h.record(self.d2h_stream)
         self.done.record(self.d2h_stream)
         return self.done
 
