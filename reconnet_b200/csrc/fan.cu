@@ -46,8 +46,7 @@ constexpr int kFpGroups = 8;         // groups of 31 rays per FP warp (at most)
 constexpr int kFpMaxLines = 16;      // lines per staged chunk (upper bound)
 constexpr int kSmemBudget = 227 * 1024;
 
-constexpr int kBpThreads = 256;      // 16 x 16 threads
-constexpr int kBpTile = 64;          // pixels per CTA side (4 x 4 per thread)
+
 constexpr int kBpViews = 8;          // views per staged chunk
 
 __host__ __device__ inline long long align4(long long v) { return (v + 3) & ~3ll; }
@@ -561,64 +560,93 @@ __device__ __forceinline__ float matched_t(const ViewGeo& vg, float r) {
     return vg.tA + vg.tB * atanf(vg.kappa * r);
 }
 
-// Matched backprojection of one view into a thread's 4x4 pixels at (x0, y0):
-// lattice lines are rows (X-class, kX) or columns, positions q along them.
-// The staged table window T starts at table index ilo; entries carry the
-// prefix (hi, lo), the slope scaled by sigma / 2 and the edge slope r_e.
-__device__ __forceinline__ void bp_matched_view(float (&acc)[4][4], const BpView& vg, const float4* T, int ilo,
-                                                int imax, int x0, int y0, int nl, bool kX) {
-    const int L0 = kX ? y0 : x0;
-    const int Q0 = kX ? x0 : y0;
-    const float par = vg.par, perp = vg.perp;
-    // edge index t(r) = tA + tB atan(kappa r) as a cubic around the slope r_t
-    // of this thread's block centre: truncation below 2e-5 cells over the 5x5
-    // lattice (it only selects the footprint; the fraction inside it is
-    // exact).  Approximate reciprocals: rt is only the expansion point, and a
-    // relative error in g scales all slopes of a line alike.
-    const float rt = __fdividef((float)(Q0 + 2) - par, (float)(L0 + 2) - perp);
+// Matched backprojection: lane i of a warp owns pixel column x = X0 + i and
+// kBmRows pixel rows from y0; lane 31 owns no pixel and only supplies the
+// right edge of lane 30's column.  The staged table window T starts at table
+// index ilo; entries carry the prefix (hi, lo), the slope scaled by sigma / 2
+// and the edge slope r_e.
+//
+// Edge index t(r) = tA + tB atan(kappa r) as a cubic around the slope r_t at
+// the lane's middle lattice point: along one lane the lattice points differ
+// in one coordinate only, and the truncation stays below 4e-5 cells over 17
+// points (it only selects the cell; the value inside it is exact).
+struct TCubic {
+    float rt, c0, c1, c2, c3;
+};
+__device__ __forceinline__ TCubic t_cubic(const BpView& vg, float rt) {
     const float ut = vg.kappa * rt;
     const float iw = __fdividef(1.0f, fmaf(ut, ut, 1.0f));
     const float k1 = vg.tB * vg.kappa * iw;
-    const float c0 = fmaf(vg.tB, atanf(ut), vg.tA);
-    const float c1 = k1;
-    const float c2 = -k1 * vg.kappa * ut * iw;
-    const float c3 = k1 * vg.kappa * vg.kappa * (fmaf(3.0f * ut, ut, -1.0f) * (1.0f / 3.0f)) * iw * iw;
-    float dq[5];
+    TCubic c;
+    c.rt = rt;
+    c.c0 = fmaf(vg.tB, atanf(ut), vg.tA);
+    c.c1 = k1;
+    c.c2 = -k1 * vg.kappa * ut * iw;
+    c.c3 = k1 * vg.kappa * vg.kappa * (fmaf(3.0f * ut, ut, -1.0f) * (1.0f / 3.0f)) * iw * iw;
+    return c;
+}
+
+// H at slope r: prefix (hi) and the rest (lo + slope * (r - r_e)) of the
+// table entry of the cell that contains r.
+__device__ __forceinline__ void bp_h(const TCubic& c, float r, const float4* T, int ilo, int imax, float& hi,
+                                     float& rest) {
+    const float h = r - c.rt;
+    const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+    // table index floor(t) + 1 for |t| < 2^22 via a round-down add; beyond
+    // the detector it reaches a zero-slope guard entry
+    int i = __float_as_int(__fadd_rd(t, 12582912.0f)) - (0x4B400000 - 1);
+    i = min(max(i, ilo), imax);
+    const float4 E = T[i - ilo];
+    hi = E.x;
+    rest = fmaf(E.z, r - E.w, E.y);
+}
+
+// X-class view (lattice lines are rows): the lane's lattice column q = x,
+// lines y0 .. y0 + kBmRows.  Pixel (x, y) receives the footprint difference
+// with the next lane's column on line y and, if line y + 1 exists, on line
+// y + 1.
+__device__ __forceinline__ void bp_matched_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                             int imax, int x, int y0, int ny) {
+    const float A = (float)x - vg.par;
+    // (approximate reciprocals: a relative error in 1 / (l - perp) scales all
+    // slopes of a line alike)
+    const TCubic c = t_cubic(vg, A * __fdividef(1.0f, (float)(y0 + kBmRows / 2) - vg.perp));
+    float dprev = 0.f;
 #pragma unroll
-    for (int qi = 0; qi < 5; qi++) dq[qi] = (float)(Q0 + qi) - par;
-    float dprev[4];
+    for (int j = 0; j <= kBmRows; j++) {
+        const float r = A * __fdividef(1.0f, (float)(y0 + j) - vg.perp);
+        float hi, rest;
+        bp_h(c, r, T, ilo, imax, hi, rest);
+        const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
+        const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
+        const float d = (nhi - hi) + (nrest - rest);
+        if (j > 0) acc[j - 1] += fmaf((y0 + j < ny) ? 1.f : 0.f, d, dprev);
+        dprev = d;
+    }
+}
+
+// Y-class view (lattice lines are columns): the lane's line l = x, lattice
+// points q = y0 .. y0 + kBmRows.  Pixel (x, y) receives the difference along
+// line x and, if line x + 1 exists, the next lane's difference along it.
+__device__ __forceinline__ void bp_matched_y(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                             int imax, int x, int y0, int nx) {
+    const float g = __fdividef(1.0f, (float)x - vg.perp);
+    const float r0 = ((float)y0 - vg.par) * g;
+    const TCubic c = t_cubic(vg, fmaf((float)(kBmRows / 2), g, r0));
+    const float m = (x + 1 < nx) ? 1.f : 0.f;
+    float hprev = 0.f, rprev = 0.f;
 #pragma unroll
-    for (int li = 0; li < 5; li++) {
-        const int l = L0 + li;
-        const float g = __fdividef(1.0f, (float)l - perp);
-        float fh[5], fl[5];
-#pragma unroll
-        for (int qi = 0; qi < 5; qi++) {
-            const float r = dq[qi] * g;
-            const float h = r - rt;
-            const float t = fmaf(h, fmaf(h, fmaf(h, c3, c2), c1), c0);
-            // table index floor(t) + 1 for |t| < 2^22 via a round-down add;
-            // beyond the detector it reaches a zero-slope guard entry
-            int i = __float_as_int(__fadd_rd(t, 12582912.0f)) - (0x4B400000 - 1);
-            i = min(max(i, ilo), imax);
-            const float4 E = T[i - ilo];
-            fh[qi] = E.x;
-            fl[qi] = fmaf(E.z, r - E.w, E.y);
+    for (int j = 0; j <= kBmRows; j++) {
+        const float r = fmaf((float)j, g, r0);
+        float hi, rest;
+        bp_h(c, r, T, ilo, imax, hi, rest);
+        if (j > 0) {
+            const float d = (hi - hprev) + (rest - rprev);
+            const float nd = __shfl_down_sync(0xffffffffu, d, 1);
+            acc[j - 1] += fmaf(m, nd, d);
         }
-        float dcur[4];
-#pragma unroll
-        for (int qi = 0; qi < 4; qi++) dcur[qi] = (fh[qi + 1] - fh[qi]) + (fl[qi + 1] - fl[qi]);
-        if (li > 0) {
-            const float m = (l < nl) ? 1.f : 0.f;   // line l exists?
-#pragma unroll
-            for (int qi = 0; qi < 4; qi++) {
-                const float v2 = fmaf(m, dcur[qi], dprev[qi]);
-                if (kX) acc[qi][li - 1] += v2;
-                else acc[li - 1][qi] += v2;
-            }
-        }
-#pragma unroll
-        for (int qi = 0; qi < 4; qi++) dprev[qi] = dcur[qi];
+        hprev = hi;
+        rprev = rest;
     }
 }
 
@@ -638,7 +666,7 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
     float t;
     if (kMatched) {
         const int xcls = vg.xcls;
-        const float X = (float)(X0 + cx * kBpTile), Y = (float)(Y0 + cy * kBpTile);
+        const float X = (float)(X0 + cx * kBmCols), Y = (float)(Y0 + cy * kBmTileY);
         const float l = xcls ? Y : X, q = xcls ? X : Y;
         t = matched_t(vg, (q - (float)vg.par) / (l - (float)vg.perp));
     } else {
@@ -682,13 +710,16 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
     const float4* gtab = p.tab + (bs.table_off - p.tab_base);
     const int nu = p.d.nu, nx = p.d.nx, ny = p.d.ny;
     const int tid = threadIdx.x;
-    const int X0 = txi * kBpTile, Y0 = tyi * kBpTile;            // CTA pixel origin
-    // thread pixel origin: a warp covers 8 x 4 threads (32 x 16 pixels), and
-    // each group of 8 lanes that shares one shared-memory wavefront covers
-    // 2 x 4 threads, so its table reads spread over distinct banks more often
+    // CTA pixel origin and thread pixel origin.  Matched: lane i of warp w
+    // owns column X0 + i, rows Y0 + 16 w ...  Reference mode: 4 x 4 pixels
+    // per thread; a warp covers 8 x 4 threads (32 x 16 pixels), and each
+    // group of 8 lanes that shares one shared-memory wavefront covers 2 x 4
+    // threads, so its table reads spread over distinct banks more often.
+    const int X0 = txi * (kMatched ? kBmCols : kBpTile), Y0 = tyi * (kMatched ? kBmTileY : kBpTile);
     const int lane = tid & 31, warp = tid >> 5;
     const int tx = ((warp & 1) << 3) | (lane & 1) | ((lane >> 3) << 1), ty = ((warp >> 1) << 2) | ((lane >> 1) & 3);
-    const int x0 = X0 + tx * 4, y0 = Y0 + ty * 4;
+    const int x0 = kMatched ? X0 + lane : X0 + tx * 4;
+    const int y0 = kMatched ? Y0 + warp * kBmRows : Y0 + ty * 4;
     const int tabn = nu + 2;   // table entries per view (guard + nu + total)
 
     if (tid == 0) {
@@ -724,11 +755,11 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
     __syncthreads();
     if (tid == 0) issue(0);
 
-    float acc[4][4];
+    // accumulators: matched acc[j] = pixel (x0, y0 + j); reference mode
+    // acc[a * 4 + b] = pixel (x0 + a, y0 + b)
+    float acc[16];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+    for (int a = 0; a < 16; a++) acc[a] = 0.f;
 
     // One barrier per chunk: after it every warp has finished chunk c - 1, so
     // buffer (c + 1) & 1 and record slot c & 1 may be refilled; window and
@@ -754,7 +785,8 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
             const int cnt = min(p.win, tabn);
             const int imax = ilo + cnt - 1;   // <= nu + 1
             if (kMatched) {
-                bp_matched_view(acc, vg, T, ilo, imax, x0, y0, vg.xcls ? ny : nx, vg.xcls);
+                if (vg.xcls) bp_matched_x(acc, vg, T, ilo, imax, x0, y0, ny);
+                else bp_matched_y(acc, vg, T, ilo, imax, x0, y0, nx);
             } else {
                 // reference DDBPFanKernelX/Y: pixel edges at the pixel centre line
                 const float cs = vg.cosd, sn = vg.sind;
@@ -795,8 +827,8 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
                             float dd = p.d.dso + ry;
                             val *= p.d.dso * p.d.dso / (rx * rx + dd * dd);
                         }
-                        if (vg.xcls) acc[qi][li] += val;
-                        else acc[li][qi] += val;
+                        if (vg.xcls) acc[qi * 4 + li] += val;
+                        else acc[li * 4 + qi] += val;
                     }
                 }
             }
@@ -805,16 +837,29 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
     if (!ok) return;
 
     float* out = p.img + bs.img_off;
+    if (kMatched) {
+        if (lane < kBmCols && x0 < nx) {
 #pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int bb = 0; bb < 4; bb++) {
-            int ix = x0 + a, iy = y0 + bb;
-            if (ix < nx && iy < ny) {
-                float* q = out + (long long)ix * p.d.isx + (long long)iy * p.d.isy;
-                *q = p.accumulate ? (*q + acc[a][bb]) : acc[a][bb];
+            for (int j = 0; j < kBmRows; j++) {
+                const int iy = y0 + j;
+                if (iy < ny) {
+                    float* q = out + (long long)x0 * p.d.isx + (long long)iy * p.d.isy;
+                    *q = p.accumulate ? (*q + acc[j]) : acc[j];
+                }
             }
         }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int bb = 0; bb < 4; bb++) {
+                const int ix = x0 + a, iy = y0 + bb;
+                if (ix < nx && iy < ny) {
+                    float* q = out + (long long)ix * p.d.isx + (long long)iy * p.d.isy;
+                    *q = p.accumulate ? (*q + acc[a * 4 + bb]) : acc[a * 4 + bb];
+                }
+            }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1045,8 +1090,11 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
     const std::vector<BpSlice>& bps = (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
     const BpSlice* dbp = (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
     const int nbp = (int)bps.size();
-    const size_t smem = bp_smem_bytes(p->table_win);
-    const int tiles_x = (d.nx + kBpTile - 1) / kBpTile, tiles_y = (d.ny + kBpTile - 1) / kBpTile;
+    const bool matched = type == RN_TYPE_MATCHED;
+    const int win = matched ? p->table_win_m : p->table_win;
+    const size_t smem = bp_smem_bytes(win);
+    const int tw = matched ? kBmCols : kBpTile, th = matched ? kBmTileY : kBpTile;
+    const int tiles_x = (d.nx + tw - 1) / tw, tiles_y = (d.ny + th - 1) / th;
     int s0 = 0;
     while (s0 < nbp) {
         // as many slices as fit in the table scratch
@@ -1082,7 +1130,7 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         bp.type = type;
         bp.tiles_x = tiles_x;
         bp.tiles_y = tiles_y;
-        bp.win = p->table_win;
+        bp.win = win;
         unsigned grid = (unsigned)(ns * tiles_x * tiles_y);
         LaunchScope ls3(p, st, 3);
         if (type == RN_TYPE_MATCHED) fan_bp_kernel<true><<<grid, kBpThreads, smem, st>>>(bp);

@@ -93,10 +93,9 @@ static void build_fp_work(rn_fan_plan* p) {
 }
 
 // Table window (entries per view staged by the BP kernels): the detector
-// extent, in cells, of a 64x64-pixel tile at the point closest to the source.
-static int table_window(const RnFanGeom& g) {
-    const double tile = 64.0;
-    double diag = tile * std::sqrt((double)g.dx * g.dx + (double)g.dy * g.dy);
+// extent, in cells, of a tw x th-pixel tile at the point closest to the source.
+static int table_window(const RnFanGeom& g, int tw, int th) {
+    double diag = std::sqrt((double)tw * tw * g.dx * g.dx + (double)th * th * g.dy * g.dy);
     double hx = g.nx * g.dx / 2.0 + std::fabs(g.cx), hy = g.ny * g.dy / 2.0 + std::fabs(g.cy);
     double dmin = g.dso - std::sqrt(hx * hx + hy * hy);
     if (dmin <= 0) return -1;
@@ -108,10 +107,11 @@ static int table_window(const RnFanGeom& g) {
 
 static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     const RnFanGeom& g = p->g;
-    int win = table_window(g);
-    if (win < 0) return set_error(RN_ERR_ARG, "fan geometry: the image reaches the source");
-    if (win > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
+    int win = table_window(g, kBpTile, kBpTile), win_m = table_window(g, kBmCols, kBmTileY);
+    if (win < 0 || win_m < 0) return set_error(RN_ERR_ARG, "fan geometry: the image reaches the source");
+    if (std::max(win, win_m) > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
     p->table_win = win;
+    p->table_win_m = win_m;
     RN_TRY(fan_kernel_attributes());
     RN_TRY(fan_build_geometry(p, host_deg, st));
     build_fp_work(p);
