@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--slices", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ossqs", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the tomosynthesis and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
     return ap.parse_args()
 
@@ -319,6 +320,118 @@ def ossqs_run(plan, geom, counts, angles, truth, n_iter, dev, n_subsets=24, I0=5
                     "(starved_ray_fraction) carry a clipped, biased line integral, which bounds the noisy RMSE"}
 
 
+def tomo_run(dev, cpu_sample=True):
+    """Tomosynthesis DD pair (DistanceDriven3D) at configs[2]'s volume size:
+    512x512x128 voxels of 0.8x0.8x1.0 mm, a 736x736 flat detector of 0.6 mm
+    cells 80 mm below the isocentre, 25 sources on a +-20 deg arc at 650 mm.
+    Updates: FP = views * nu * nv * nz ray-plane integrals, BP = voxels * views;
+    algorithmic bytes 16 B per update (4 summed-area-table corners)."""
+    import ctypes
+    import math
+
+    import torch
+
+    from reconnet_b200 import _native as N
+    nx, ny, nz, nu, nv, nview = 512, 512, 128, 736, 736, 25
+    dx, dy, dz, du, dv = 0.8, 0.8, 1.0, 0.6, 0.6
+    dc = np.zeros((nview, 3), np.float32)
+    src = np.zeros((nview, 3), np.float32)
+    for k in range(nview):
+        a = (k - (nview - 1) / 2) / ((nview - 1) / 2) * math.radians(20)
+        src[k] = (650 * math.sin(a), 0.0, 650 * math.cos(a))
+        dc[k] = (0.0, 0.0, -80.0)
+    rng = np.random.default_rng(11)
+    from reconnet_b200.phantom import ellipsoid_phantom
+    img = ellipsoid_phantom(nx, ny, nz, dx, dy, dz, rng, device=dev)[None, :, :, :, None].contiguous()
+    prj = torch.empty((1, nu, nview, nv, 1), device=dev)
+    back = torch.empty_like(img)
+    fpb, bpb = ctypes.c_size_t(), ctypes.c_size_t()
+    N.lib.rn_tomo_sat_bytes(nx, ny, nz, nu, nview, nv, ctypes.byref(fpb), ctypes.byref(bpb))
+    sat = torch.empty(max(fpb.value, bpb.value) // 8 + 1, dtype=torch.float64, device=dev)
+    ddc, dsrc = torch.from_numpy(dc).to(dev), torch.from_numpy(src).to(dev)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    geo = (1, 1, nx, ny, nz, dx, dy, dz, 0.0, 0.0, 0.0, nu, nview, nv, du, dv, 0.0, 0.0)
+    st = lambda: ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    fp = lambda: N.check(N.lib.rn_tomo_project(P(prj), P(img), P(ddc), P(dsrc), P(sat), *geo, st()))
+    bp = lambda: N.check(N.lib.rn_tomo_backproject(P(back), P(prj), P(ddc), P(dsrc), P(sat), *geo, 1, st()))
+    peak, kind = measured_peaks()
+    out = {"workload": "tomosynthesis at configs[2] volume size: 512x512x128 @0.8x0.8x1.0 mm, 736x736 flat "
+                       "detector @0.6 mm, 25 views over +-20 deg (configs[2]'s 360-deg cylindrical CT geometry has "
+                       "no reference kernel; DistanceDriven3D is the reference's tomosynthesis pair)",
+           "model": "16 B per update (4 summed-area-table corners)"}
+    for name, f, upd in (("fp", fp, nview * nu * nv * nz), ("bp", bp, nx * ny * nz * nview)):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        ach = 16.0 * upd / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "updates": upd, "gupd_s": upd / ms / 1e6,
+                     "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                  "peak_kind": kind}}
+    if cpu_sample:
+        from oracle import oracle as O
+        from types import SimpleNamespace
+        O.set_threads(os.cpu_count() or 1)
+        g = SimpleNamespace(dx=dx, dy=dy, dz=dz, cx=0.0, cy=0.0, cz=0.0, du=du, dv=dv, off_u=0.0, off_v=0.0)
+        vol = img.cpu().numpy()
+        t0 = time.perf_counter()
+        O.tomo_fp(vol, dc[:1], src[:1], g, nu, nv)
+        t1 = time.perf_counter()
+        O.tomo_bp(np.ones((1, nu, 1, nv, 1), np.float32), dc[:1], src[:1], g, (nx, ny, nz), 1)
+        t2 = time.perf_counter()
+        out["cpu_baseline"] = {"fp_gupd_s": nu * nv * nz / (t1 - t0) / 1e9, "bp_gupd_s": nx * ny * nz / (t2 - t1) / 1e9,
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": "1 of the 25 views, FP64 OpenMP oracle (the reference has no CPU path)"}
+    return out
+
+
+def filter_run(dev, cpu_sample=True):
+    """Ramp filter (Filter.cu): 64 fan sinograms of 888 channels x 1152 views,
+    Ram-Lak window.  The filter is a linear convolution of every view with the
+    (2 nu - 1)-tap kernel: nu^2 multiply-adds per view."""
+    import torch
+
+    from reconnet_b200.phantom import geom_cfg1
+    from reconnet_b200.torch_ops import filter_sino
+    geom = geom_cfg1()
+    B, nu, nview = 64, geom.nu, 1152
+    rng = np.random.default_rng(12)
+    sino = torch.from_numpy(rng.random((B, nu, nview, 1, 1), dtype=np.float32)).to(dev)
+    filter_sino(sino, geom)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        filter_sino(sino, geom)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    flops = 2.0 * nu * nu * nview * B
+    # FP32 SIMT peak from the SM count and the measured-peaks clock (FMA = 2 FLOP)
+    props = torch.cuda.get_device_properties(dev)
+    simt_peak = props.multi_processor_count * 128 * 2 * 1.965e9 / 1e12
+    out = {"workload": f"{B} fan sinograms, {nu} channels x {nview} views, Ram-Lak",
+           "ms": ms, "views_per_s": B * nview / (ms * 1e-3),
+           "roofline": {"bound": "fp32 simt", "achieved": flops / (ms * 1e-3) / 1e12, "peak": simt_peak,
+                        "unit": "TFLOP/s", "frac": flops / (ms * 1e-3) / 1e12 / simt_peak,
+                        "peak_kind": "nominal (148 SMs x 128 FMA/clk x 1965 MHz)"}}
+    if cpu_sample:
+        from oracle import oracle as O
+        O.set_threads(os.cpu_count() or 1)
+        sample = sino[:1, :, :64].cpu().numpy()
+        t0 = time.perf_counter()
+        O.filter_sino(sample, geom, 0, True)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"views_per_s": 64 / dt, "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": "64 views of one sinogram, FP64 OpenMP oracle"}
+    return out
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -449,6 +562,10 @@ def run_b200(args):
            "serial_ms_per_step": ms_serial / e2e_steps}
 
     ossqs = None if args.no_ossqs else ossqs_run(plan, geom, counts, angles, x, args.ossqs_iters, dev)
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras["tomo"] = tomo_run(dev, cpu_sample=world == 1)
+        extras["filter"] = filter_run(dev, cpu_sample=world == 1)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -467,6 +584,7 @@ def run_b200(args):
             line["cpu_baseline"] = cpu
         if ossqs is not None:
             line["ossqs_tv"] = ossqs
+        line.update(extras)
         print(json.dumps(line), flush=True)
     del plan
     if world > 1:

@@ -35,14 +35,23 @@ def ellipse_phantom(nx, ny, dx, dy, rng, n_ellipses=10, axes=(5.0, 120.0), mu=(0
     return img.astype(np.float32)
 
 
-def ellipsoid_phantom(nx, ny, nz, dx, dy, dz, rng, n_ellipsoids=10, axes=(5.0, 120.0), mu=(0.0, 0.04)):
-    """Random 3D ellipsoids on [nx, ny, nz] (axis-aligned in z, rotated in xy)."""
-    xs = (np.arange(nx) - (nx - 1) / 2.0) * dx
-    ys = (np.arange(ny) - (ny - 1) / 2.0) * dy
-    zs = (np.arange(nz) - (nz - 1) / 2.0) * dz
-    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+def ellipsoid_phantom(nx, ny, nz, dx, dy, dz, rng, n_ellipsoids=10, axes=(5.0, 120.0), mu=(0.0, 0.04),
+                      device=None):
+    """Random 3D ellipsoids on [nx, ny, nz] (axis-aligned in z, rotated in xy).
+    With ``device`` (a torch device) the volume is rasterised there and
+    returned as a torch tensor; the seeded parameters are the same."""
+    if device is not None:
+        import torch
+        ar = lambda n, d: (torch.arange(n, device=device, dtype=torch.float64) - (n - 1) / 2.0) * d
+        X, Y, Z = torch.meshgrid(ar(nx, dx), ar(ny, dy), ar(nz, dz), indexing="ij")
+        img = torch.zeros((nx, ny, nz), dtype=torch.float32, device=device)
+    else:
+        xs = (np.arange(nx) - (nx - 1) / 2.0) * dx
+        ys = (np.arange(ny) - (ny - 1) / 2.0) * dy
+        zs = (np.arange(nz) - (nz - 1) / 2.0) * dz
+        X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+        img = np.zeros((nx, ny, nz), np.float32)
     R = 0.8 * min(nx * dx, ny * dy) / 2.0
-    img = np.zeros((nx, ny, nz), np.float32)
     for _ in range(n_ellipsoids):
         rr = R * np.sqrt(rng.uniform())
         th = rng.uniform(0, 2 * np.pi)
