@@ -75,17 +75,6 @@ __global__ void edge_slope_kernel(double* edges, const double2* view_cs, const i
 // rows l-1 and l) and Y lines (columns).  Entry k of a line holds the prefix
 // P[k] = sum_{i<k} a_i as (hi, lo) and the value a_k (a_n = 0).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_incl_scan(double v) {
-    const unsigned full = 0xffffffffu;
-    int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        double t = __shfl_up_sync(full, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
-
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
                                  FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;

@@ -80,4 +80,16 @@ __device__ __forceinline__ float2 split_double(double v) {
     return make_float2(hi, lo);
 }
 
+// Inclusive prefix sum over the 32 lanes of a warp (all lanes participate).
+__device__ __forceinline__ double warp_incl_scan(double v) {
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double t = __shfl_up_sync(full, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
 }  // namespace rn

@@ -20,6 +20,7 @@
 #include <mutex>
 #include <vector>
 
+#include "rn_device.cuh"
 #include "rn_internal.h"
 
 namespace rn {
@@ -31,163 +32,246 @@ struct TomoDims {
     float du, dv, off_u, off_v;
 };
 
-// SAT of one (b, c) volume, layout [z][x][y] with x in [0,nx], y in [0,ny].
-__global__ void tomo_sat_rows(double* __restrict__ sat, const float* __restrict__ img, TomoDims d, int b, int c) {
-    // one thread per (z, x): prefix along y for image column x (into row x+1)
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nz * d.nx) return;
-    int z = i / d.nx, x = i - (i / d.nx) * d.nx;
-    double* row = sat + ((long long)z * (d.nx + 1) + (x + 1)) * (d.ny + 1);
-    const float* src = img + (long long)b * d.nx * d.ny * d.nz * d.nc + (long long)x * d.ny * d.nz * d.nc +
-                       (long long)z * d.nc + c;
+// ---------------------------------------------------------------------------
+// Summed-area tables.  FP: per z plane, layout [z][y][x] (x fastest), x in
+// [0, nx], y in [0, ny].  BP: per view, the length-weighted projections,
+// layout [view][v][u] (u fastest), u in [0, nu], v in [0, nv].  Rows run
+// along the axis that the lanes of the main kernels walk, so their corner
+// lookups are coalesced.  Built in two passes: a tiled pass that reads the
+// source along its contiguous axis, transposes 32 x 32 tiles through shared
+// memory and scans along the row with warp scans (carry across tiles), then
+// a pass along the other axis.
+// ---------------------------------------------------------------------------
+
+// Row prefixes S[z][y + 1][x + 1] = sum_{x' <= x} img[x'][y][z].  Block
+// (32, 8): blockIdx.x = y, blockIdx.y = a tile of 32 planes.
+__global__ void __launch_bounds__(256) tomo_sat_x(double* __restrict__ sat, const float* __restrict__ img, TomoDims d,
+                                                  int b, int c) {
+    __shared__ float tile[32][33];
+    const int y = blockIdx.x, z0 = blockIdx.y * 32;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const long long plane = (long long)(d.nx + 1) * (d.ny + 1), row = d.nx + 1;
+    const long long sx = (long long)d.ny * d.nz * d.nc;   // img stride along x
+    const float* base = img + (long long)b * d.nx * sx + (long long)y * d.nz * d.nc + c;
+    double carry[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int x0 = 0; x0 < d.nx; x0 += 32) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {   // rows x0 + w + 8k, lanes along z (contiguous)
+            const int x = x0 + w + 8 * k, z = z0 + lane;
+            tile[w + 8 * k][lane] = (x < d.nx && z < d.nz) ? base[(long long)x * sx + (long long)z * d.nc] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; k++) {   // plane z0 + w + 8k, lanes along x
+            const int zz = w + 8 * k, z = z0 + zz;
+            const double v = (double)tile[lane][zz];
+            const double incl = warp_incl_scan(v);
+            if (z < d.nz && x0 + lane < d.nx) sat[z * plane + (y + 1) * row + (x0 + lane + 1)] = carry[k] + incl;
+            carry[k] += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncthreads();
+    }
+    // column x = 0 of row y + 1, and row y = 0 of the tile's planes
+    const int z = z0 + lane;
+    if (w == 0 && z < d.nz) sat[z * plane + (y + 1) * row] = 0.0;
+    if (y == 0)
+        for (int zz = w; zz < 32 && z0 + zz < d.nz; zz += 8)
+            for (int x = lane; x <= d.nx; x += 32) sat[(z0 + zz) * plane + x] = 0.0;
+}
+
+// Column prefixes along y: one thread per (z, x), x fastest.
+__global__ void tomo_sat_y(double* __restrict__ sat, TomoDims d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nz * (d.nx + 1)) return;
+    const int z = i / (d.nx + 1), x = i - z * (d.nx + 1);
+    const long long row = d.nx + 1;
+    double* col = sat + (long long)z * (d.nx + 1) * (d.ny + 1) + x;
     double acc = 0.0;
-    row[0] = 0.0;
-    for (int y = 0; y < d.ny; y++) {
-        acc += (double)src[(long long)y * d.nz * d.nc];
-        row[y + 1] = acc;
-    }
-    if (x == 0) {
-        double* r0 = sat + (long long)z * (d.nx + 1) * (d.ny + 1);
-        for (int y = 0; y <= d.ny; y++) r0[y] = 0.0;
+    for (int y = 1; y <= d.ny; y++) {
+        acc += col[y * row];
+        col[y * row] = acc;
     }
 }
 
-__global__ void tomo_sat_cols(double* __restrict__ sat, TomoDims d) {
-    // one thread per (z, y): prefix along x
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nz * (d.ny + 1)) return;
-    int z = i / (d.ny + 1), y = i - (i / (d.ny + 1)) * (d.ny + 1);
-    double* base = sat + (long long)z * (d.nx + 1) * (d.ny + 1) + y;
+// Length weight of detector cell (u, v) of a view (PreweightBPCartKernelXY,
+// DistanceDriven3D.cu:409-431).
+__device__ __forceinline__ double tomo_len_weight(const float* dc, const float* sp, float u, float v, float dz) {
+    const double ddx = (double)sp[0] - (dc[0] + u), ddy = (double)sp[1] - (dc[1] + v), ddz = (double)sp[2] - dc[2];
+    return (double)dz / fabs(ddz) * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+}
+
+// Weighted row prefixes S[view][v + 1][u + 1] = sum_{u' <= u} w p(u', v).
+// weight_all = 0 applies the length weight to view 0 only, as the reference's
+// pre-weight launch does (its grid has one row of views,
+// DistanceDriven3D.cu:612-621); 1 weights every view.  Block (32, 8):
+// blockIdx.x = a tile of 32 detector rows v, blockIdx.y = view.
+__global__ void __launch_bounds__(256) tomo_bp_sat_u(double* __restrict__ sat, const float* __restrict__ prj,
+                                                     const float* __restrict__ detCenter,
+                                                     const float* __restrict__ src, TomoDims d, int b, int c,
+                                                     int weight_all) {
+    __shared__ double tile[32][33];
+    const int v0 = blockIdx.x * 32, view = blockIdx.y;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const float* dc = detCenter + 3 * view;
+    const float* sp = src + 3 * view;
+    const bool weighted = weight_all || view == 0;
+    const long long vplane = (long long)(d.nu + 1) * (d.nv + 1), row = d.nu + 1;
+    double* S = sat + view * vplane;
+    const long long su = (long long)d.nview * d.nv * d.nc;   // prj stride along u
+    const float* base = prj + (long long)b * d.nu * su + (long long)view * d.nv * d.nc + c;
+    double carry[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int u0 = 0; u0 < d.nu; u0 += 32) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {   // cells u0 + w + 8k, lanes along v (contiguous)
+            const int iu = u0 + w + 8 * k, iv = v0 + lane;
+            double val = 0.0;
+            if (iu < d.nu && iv < d.nv) {
+                val = (double)base[(long long)iu * su + (long long)iv * d.nc];
+                if (weighted) {
+                    const float u = (iu - d.off_u - (d.nu - 1) / 2.0f) * d.du;
+                    const float v = (iv - d.off_v - (d.nv - 1) / 2.0f) * d.dv;
+                    val *= tomo_len_weight(dc, sp, u, v, d.dz);
+                }
+            }
+            tile[w + 8 * k][lane] = val;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; k++) {   // row v0 + w + 8k, lanes along u
+            const int vv = w + 8 * k, iv = v0 + vv;
+            const double incl = warp_incl_scan(tile[lane][vv]);
+            if (iv < d.nv && u0 + lane < d.nu) S[(iv + 1) * row + (u0 + lane + 1)] = carry[k] + incl;
+            carry[k] += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncthreads();
+    }
+    const int iv = v0 + lane;
+    if (w == 0 && iv < d.nv) S[(iv + 1) * row] = 0.0;
+    if (blockIdx.x == 0)
+        for (int u = lane + 32 * w; u <= d.nu; u += 256) S[u] = 0.0;
+}
+
+// Column prefixes along v: one thread per (view, u), u fastest.
+__global__ void tomo_bp_sat_v(double* __restrict__ sat, TomoDims d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nview * (d.nu + 1)) return;
+    const int view = i / (d.nu + 1), u = i - view * (d.nu + 1);
+    const long long row = d.nu + 1;
+    double* col = sat + (long long)view * (d.nu + 1) * (d.nv + 1) + u;
     double acc = 0.0;
-    for (int x = 1; x <= d.nx; x++) {
-        acc += base[(long long)x * (d.ny + 1)];
-        base[(long long)x * (d.ny + 1)] = acc;
+    for (int v = 1; v <= d.nv; v++) {
+        acc += col[v * row];
+        col[v * row] = acc;
     }
 }
 
-// Clamp_float + bilinear interpolation of InterpolateXY / InterpolateUV
-// (DistanceDriven3D.cu:75-135, :493-517) on an (n0 x n1) grid, row stride s0.
-__device__ __forceinline__ double sat_bilinear(const double* __restrict__ a, float x, float y, int n0, int n1,
-                                               long long s0) {
-    x = x < 0.f ? 0.f : (x >= (float)n0 ? (float)(n0 - 1) : x);
-    y = y < 0.f ? 0.f : (y >= (float)n1 ? (float)(n1 - 1) : y);
-    int i0 = (int)x, j0 = (int)y;
-    int i1 = min(i0 + 1, n0 - 1), j1 = min(j0 + 1, n1 - 1);
-    double wx = (double)(x - (float)i0), wy = (double)(y - (float)j0);
-    return a[i0 * s0 + j0] * (1 - wx) * (1 - wy) + a[i1 * s0 + j0] * wx * (1 - wy) + a[i0 * s0 + j1] * (1 - wx) * wy +
-           a[i1 * s0 + j1] * wx * wy;
+// Clamp_float + the index / weight of one coordinate of InterpolateXY /
+// InterpolateUV (DistanceDriven3D.cu:75-135, :493-517) on a grid of n points.
+struct Lerp {
+    int i0, i1;
+    double w;
+};
+__device__ __forceinline__ Lerp lerp_at(float x, int n) {
+    x = x < 0.f ? 0.f : (x >= (float)n ? (float)(n - 1) : x);
+    Lerp l;
+    l.i0 = (int)x;
+    l.i1 = min(l.i0 + 1, n - 1);
+    l.w = (double)(x - (float)l.i0);
+    return l;
+}
+// Bilinear value of a table with rows along the second coordinate:
+// a[r * row + col], col from lc, r from lr.
+__device__ __forceinline__ double sat_at(const double* __restrict__ a, const Lerp& lc, const Lerp& lr, long long row) {
+    const double* r0 = a + lr.i0 * row;
+    const double* r1 = a + lr.i1 * row;
+    return (r0[lc.i0] * (1 - lc.w) + r0[lc.i1] * lc.w) * (1 - lr.w) + (r1[lc.i0] * (1 - lc.w) + r1[lc.i1] * lc.w) * lr.w;
 }
 
-__global__ void tomo_fp_kernel(float* __restrict__ prj, const double* __restrict__ sat,
-                               const float* __restrict__ detCenter, const float* __restrict__ src, TomoDims d, int b,
-                               int c) {
-    int iu = blockIdx.x * blockDim.x + threadIdx.x;
-    int iview = blockIdx.y;
-    int iv = blockIdx.z * blockDim.y + threadIdx.y;
-    if (iu >= d.nu || iv >= d.nv) return;
+// FP: lane i of a warp owns detector column iu = 31 blockIdx.x + i and its
+// left cell edge; lane 31 only supplies the right edge of lane 30's cell.  A
+// warp handles one detector row v of one view, and per z plane each lane
+// evaluates D = S(x_e, y2) - S(x_e, y1) at its edge, so the rectangle
+// integral of a cell is D(next lane) - D(this lane): 8 table reads per ray
+// and plane instead of 16.  The rectangle's area is (x_{e+1} - x_e)(y2 - y1) =
+// drx dry (z - sz)^2, exact for the straight edge rays.
+__global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, const double* __restrict__ sat,
+                                                      const float* __restrict__ detCenter,
+                                                      const float* __restrict__ src, TomoDims d, int b, int c) {
+    const int lane = threadIdx.x;
+    const int iu = blockIdx.x * 31 + lane;
+    const int iview = blockIdx.y;
+    const int iv = blockIdx.z * blockDim.y + threadIdx.y;
+    if (iv >= d.nv) return;   // warp-uniform
     const float* dc = detCenter + 3 * iview;
     const float* sp = src + 3 * iview;
-    float u = (iu - d.off_u - (d.nu - 1) / 2.0f) * d.du;
-    float v = (iv - d.off_v - (d.nv - 1) / 2.0f) * d.dv;
+    const float u = (iu - d.off_u - (d.nu - 1) / 2.0f) * d.du;
+    const float v = (iv - d.off_v - (d.nv - 1) / 2.0f) * d.dv;
     auto img_x = [&](float px) { return (px - d.cx) / d.dx + d.nx / 2.0f; };
     auto img_y = [&](float py) { return (py - d.cy) / d.dy + d.ny / 2.0f; };
     auto img_z = [&](float pz) { return (pz - d.cz) / d.dz + d.nz / 2.0f; };
-    float sx = img_x(sp[0]), sy = img_y(sp[1]), sz = img_z(sp[2]);
-    float xa = img_x(dc[0] + u - d.du / 2), xb = img_x(dc[0] + u + d.du / 2);
-    float ya = img_y(dc[1] + v - d.dv / 2), yb = img_y(dc[1] + v + d.dv / 2);
-    float zd = img_z(dc[2]);
-    if (xa > xb) { float t = xa; xa = xb; xb = t; }
-    if (ya > yb) { float t = ya; ya = yb; yb = t; }
-    float rx1 = (xa - sx) / (zd - sz), rx2 = (xb - sx) / (zd - sz);
-    float ry1 = (ya - sy) / (zd - sz), ry2 = (yb - sy) / (zd - sz);
-    const long long plane = (long long)(d.nx + 1) * (d.ny + 1);
-    double val = 0.0;
+    const float sx = img_x(sp[0]), sy = img_y(sp[1]), sz = img_z(sp[2]);
+    const float zd = img_z(dc[2]);
+    const float xe = img_x(dc[0] + u - d.du / 2);
+    const float ya = img_y(dc[1] + v - d.dv / 2), yb = img_y(dc[1] + v + d.dv / 2);
+    const float rxe = (xe - sx) / (zd - sz);
+    const float rya = (ya - sy) / (zd - sz), ryb = (yb - sy) / (zd - sz);
+    const float drx = __shfl_down_sync(0xffffffffu, rxe, 1) - rxe;   // signed, as are D and dry
+    const float k = 1.0f / (drx * (ryb - rya));
+    const long long plane = (long long)(d.nx + 1) * (d.ny + 1), row = d.nx + 1;
+    float val = 0.f;
     for (int iz = 0; iz < d.nz; iz++) {
-        float x1 = sx + rx1 * (iz - sz), x2 = sx + rx2 * (iz - sz);
-        float y1 = sy + ry1 * (iz - sz), y2 = sy + ry2 * (iz - sz);
+        const float t = (float)iz - sz;
+        const Lerp lx = lerp_at(sx + rxe * t, d.nx + 1);
+        const Lerp l1 = lerp_at(sy + rya * t, d.ny + 1), l2 = lerp_at(sy + ryb * t, d.ny + 1);
         const double* a = sat + iz * plane;
-        double q = sat_bilinear(a, x2, y2, d.nx + 1, d.ny + 1, d.ny + 1) +
-                   sat_bilinear(a, x1, y1, d.nx + 1, d.ny + 1, d.ny + 1) -
-                   sat_bilinear(a, x2, y1, d.nx + 1, d.ny + 1, d.ny + 1) -
-                   sat_bilinear(a, x1, y2, d.nx + 1, d.ny + 1, d.ny + 1);
-        val += q / ((double)(x2 - x1) * (double)(y2 - y1));
+        const double D = sat_at(a, lx, l2, row) - sat_at(a, lx, l1, row);
+        const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
+        val = fmaf((float)q, k / (t * t), val);
     }
-    double ddx = (double)sp[0] - (dc[0] + u), ddy = (double)sp[1] - (dc[1] + v), ddz = (double)sp[2] - dc[2];
-    val *= (double)d.dz / fabs(ddz) * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
-    prj[(long long)b * d.nu * d.nview * d.nv * d.nc + ((long long)iu * d.nview + iview) * d.nv * d.nc +
-        (long long)iv * d.nc + c] = (float)val;
-}
-
-// Weighted (u, v) SAT per view, layout [view][u in 0..nu][v in 0..nv].
-// weight_all = 0 applies the length weight to view 0 only, as the reference's
-// pre-weight launch does (its grid has one row of views,
-// DistanceDriven3D.cu:612-621); 1 weights every view.
-__global__ void tomo_bp_sat_u(double* __restrict__ sat, const float* __restrict__ prj,
-                              const float* __restrict__ detCenter, const float* __restrict__ src, TomoDims d, int b,
-                              int c, int weight_all) {
-    // one thread per (view, v): prefix along u of the weighted projections
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nview * d.nv) return;
-    int view = i / d.nv, iv = i - (i / d.nv) * d.nv;
-    const float* dc = detCenter + 3 * view;
-    const float* sp = src + 3 * view;
-    double* base = sat + (long long)view * (d.nu + 1) * (d.nv + 1) + (iv + 1);
-    double acc = 0.0;
-    if (iv == 0)
-        for (int u = 0; u <= d.nu; u++) sat[(long long)view * (d.nu + 1) * (d.nv + 1) + (long long)u * (d.nv + 1)] = 0;
-    base[0] = 0.0;
-    float v = (iv - d.off_v - (d.nv - 1) / 2.0f) * d.dv;
-    for (int iu = 0; iu < d.nu; iu++) {
-        float u = (iu - d.off_u - (d.nu - 1) / 2.0f) * d.du;
-        double ddx = (double)sp[0] - (dc[0] + u), ddy = (double)sp[1] - (dc[1] + v), ddz = (double)sp[2] - dc[2];
-        double w = (weight_all || view == 0) ? (double)d.dz / fabs(ddz) * sqrt(ddx * ddx + ddy * ddy + ddz * ddz)
-                                             : 1.0;
-        acc += w * (double)prj[(long long)b * d.nu * d.nview * d.nv * d.nc +
-                               ((long long)iu * d.nview + view) * d.nv * d.nc + (long long)iv * d.nc + c];
-        base[(long long)(iu + 1) * (d.nv + 1)] = acc;
+    if (lane < 31 && iu < d.nu) {
+        val *= (float)tomo_len_weight(dc, sp, u, v, d.dz);
+        prj[(long long)b * d.nu * d.nview * d.nv * d.nc + ((long long)iu * d.nview + iview) * d.nv * d.nc +
+            (long long)iv * d.nc + c] = val;
     }
 }
 
-__global__ void tomo_bp_sat_v(double* __restrict__ sat, TomoDims d) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nview * (d.nu + 1)) return;
-    double* row = sat + (long long)i * (d.nv + 1);
-    double acc = 0.0;
-    for (int v = 1; v <= d.nv; v++) {
-        acc += row[v];
-        row[v] = acc;
-    }
-}
-
-__global__ void tomo_bp_kernel(float* __restrict__ img, const double* __restrict__ sat,
-                               const float* __restrict__ detCenter, const float* __restrict__ src, TomoDims d, int b,
-                               int c) {
-    int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    int iz = blockIdx.z;
-    if (ix >= d.nx || iy >= d.ny) return;
-    float x = (ix - (d.nx - 1) / 2.0f) * d.dx + d.cx;
-    float y = (iy - (d.ny - 1) / 2.0f) * d.dy + d.cy;
-    float z = (iz - (d.nz - 1) / 2.0f) * d.dz + d.cz;
-    double val = 0.0;
-    const long long vstride = (long long)(d.nu + 1) * (d.nv + 1);
+// BP: lane i of a warp owns voxel column ix = 31 blockIdx.x + i and its left
+// face; lane 31 only supplies the right face of lane 30's voxel.  A warp
+// handles one (y, z) row.  Per view each lane evaluates D = S(u_e, v2) -
+// S(u_e, v1) at its face's detector coordinate (ProjectConeToDetCart,
+// DistanceDriven3D.cu:478-489), and the voxel's rectangle integral is
+// D(next lane) - D(this lane); the rectangle's area is r^2 dx dy / (du dv).
+__global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, const double* __restrict__ sat,
+                                                      const float* __restrict__ detCenter,
+                                                      const float* __restrict__ src, TomoDims d, int b, int c) {
+    const int lane = threadIdx.x;
+    const int ix = blockIdx.x * 31 + lane;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int iz = blockIdx.z;
+    if (iy >= d.ny) return;   // warp-uniform
+    const float xf = (ix - (d.nx - 1) / 2.0f) * d.dx + d.cx - d.dx / 2;
+    const float y = (iy - (d.ny - 1) / 2.0f) * d.dy + d.cy;
+    const float z = (iz - (d.nz - 1) / 2.0f) * d.dz + d.cz;
+    const float cu = d.off_u + (d.nu - 1) / 2.0f, cv = d.off_v + (d.nv - 1) / 2.0f;
+    const float aunit = d.dx * d.dy / (d.du * d.dv);
+    const long long vplane = (long long)(d.nu + 1) * (d.nv + 1), row = d.nu + 1;
+    float val = 0.f;
     for (int view = 0; view < d.nview; view++) {
         const float* dc = detCenter + 3 * view;
         const float* sp = src + 3 * view;
-        // ProjectConeToDetCart (DistanceDriven3D.cu:478-489)
-        float r = (dc[2] - sp[2]) / (z - sp[2]);
-        float u1 = (sp[0] - dc[0] + r * (x - d.dx / 2 - sp[0])) / d.du + d.off_u + (d.nu - 1) / 2.0f;
-        float u2 = (sp[0] - dc[0] + r * (x + d.dx / 2 - sp[0])) / d.du + d.off_u + (d.nu - 1) / 2.0f;
-        float v1 = (sp[1] - dc[1] + r * (y - d.dy / 2 - sp[1])) / d.dv + d.off_v + (d.nv - 1) / 2.0f;
-        float v2 = (sp[1] - dc[1] + r * (y + d.dy / 2 - sp[1])) / d.dv + d.off_v + (d.nv - 1) / 2.0f;
-        const double* a = sat + view * vstride;
-        double q = sat_bilinear(a, u2, v2, d.nu + 1, d.nv + 1, d.nv + 1) -
-                   sat_bilinear(a, u2, v1, d.nu + 1, d.nv + 1, d.nv + 1) +
-                   sat_bilinear(a, u1, v1, d.nu + 1, d.nv + 1, d.nv + 1) -
-                   sat_bilinear(a, u1, v2, d.nu + 1, d.nv + 1, d.nv + 1);
-        val += q / ((double)(u2 - u1) * (double)(v2 - v1));
+        const float r = (dc[2] - sp[2]) / (z - sp[2]);
+        const float ue = (sp[0] - dc[0] + r * (xf - sp[0])) / d.du + cu;
+        const float v1 = (sp[1] - dc[1] + r * (y - d.dy / 2 - sp[1])) / d.dv + cv;
+        const float v2 = (sp[1] - dc[1] + r * (y + d.dy / 2 - sp[1])) / d.dv + cv;
+        const Lerp lu = lerp_at(ue, d.nu + 1);
+        const Lerp l1 = lerp_at(v1, d.nv + 1), l2 = lerp_at(v2, d.nv + 1);
+        const double* a = sat + view * vplane;
+        const double D = sat_at(a, lu, l2, row) - sat_at(a, lu, l1, row);
+        const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
+        val = fmaf((float)q, 1.0f / (r * r * aunit), val);
     }
-    img[(long long)b * d.nx * d.ny * d.nz * d.nc + (((long long)ix * d.ny + iy) * d.nz + iz) * d.nc + c] = (float)val;
+    if (lane < 31 && ix < d.nx)
+        img[(long long)b * d.nx * d.ny * d.nz * d.nc + (((long long)ix * d.ny + iy) * d.nz + iz) * d.nc + c] = val;
 }
 
 static int tomo_validate(const TomoDims& d) {
@@ -203,10 +287,10 @@ int tomo_project(float* d_prj, const float* d_img, const float* d_dc, const floa
     RN_TRY(tomo_validate(d));
     for (int b = 0; b < d.nb; b++)
         for (int c = 0; c < d.nc; c++) {
-            tomo_sat_rows<<<(d.nz * d.nx + 127) / 128, 128, 0, st>>>(d_sat, d_img, d, b, c);
-            tomo_sat_cols<<<(d.nz * (d.ny + 1) + 127) / 128, 128, 0, st>>>(d_sat, d);
+            tomo_sat_x<<<dim3(d.ny, (d.nz + 31) / 32), dim3(32, 8), 0, st>>>(d_sat, d_img, d, b, c);
+            tomo_sat_y<<<(d.nz * (d.nx + 1) + 255) / 256, 256, 0, st>>>(d_sat, d);
             dim3 blk(32, 4);
-            dim3 grd((d.nu + 31) / 32, d.nview, (d.nv + 3) / 4);
+            dim3 grd((d.nu + 30) / 31, d.nview, (d.nv + 3) / 4);
             tomo_fp_kernel<<<grd, blk, 0, st>>>(d_prj, d_sat, d_dc, d_src, d, b, c);
         }
     RN_CUDA_TRY(cudaGetLastError());
@@ -218,11 +302,11 @@ int tomo_backproject(float* d_img, const float* d_prj, const float* d_dc, const 
     RN_TRY(tomo_validate(d));
     for (int b = 0; b < d.nb; b++)
         for (int c = 0; c < d.nc; c++) {
-            tomo_bp_sat_u<<<(d.nview * d.nv + 127) / 128, 128, 0, st>>>(d_sat, d_prj, d_dc, d_src, d, b, c,
-                                                                          weight_all);
-            tomo_bp_sat_v<<<(d.nview * (d.nu + 1) + 127) / 128, 128, 0, st>>>(d_sat, d);
+            tomo_bp_sat_u<<<dim3((d.nv + 31) / 32, d.nview), dim3(32, 8), 0, st>>>(d_sat, d_prj, d_dc, d_src, d, b,
+                                                                                    c, weight_all);
+            tomo_bp_sat_v<<<(d.nview * (d.nu + 1) + 255) / 256, 256, 0, st>>>(d_sat, d);
             dim3 blk(32, 8);
-            dim3 grd((d.nx + 31) / 32, (d.ny + 7) / 8, d.nz);
+            dim3 grd((d.nx + 30) / 31, (d.ny + 7) / 8, d.nz);
             tomo_bp_kernel<<<grd, blk, 0, st>>>(d_img, d_sat, d_dc, d_src, d, b, c);
         }
     RN_CUDA_TRY(cudaGetLastError());
