@@ -3,15 +3,15 @@
 // BackprojectionTomo (ReconNet4D/DistanceDriven3D.cu:37-663):
 //   FP: per ray, for every z plane at integer z, the source-to-detector
 //       rectangle [x1,x2] x [y1,y2] spanned by the cell's edge rays is
-//       integrated with a 2D summed-area table (4 bilinear corner lookups),
-//       normalised by its area, and the sum is scaled by
-//       dz / |dz_src-det| * |src - det|;
-//   BP: the sinogram is pre-weighted by the same length factor, a (u, v)
-//       summed-area table is built per view, and every voxel integrates the
-//       detector rectangle spanned by its projected faces.
-// The summed-area tables are FP64 (as in the reference) so that corner
-// differences keep full precision; each (b, c) volume is processed by one
-// launch sequence on the caller's stream.
+//       integrated over the piecewise-constant plane (the reference reads 4
+//       bilinear corners of a 2D summed-area table), normalised by its area,
+//       and the sum is scaled by dz / |dz_src-det| * |src - det|;
+//   BP: the sinogram is pre-weighted by the same length factor, and every
+//       voxel integrates the detector rectangle spanned by its projected faces.
+// Here the FP integrals come from FP64 row-prefix tables (rows_integral), the
+// same quantity in exact arithmetic as the reference's corner form, and the BP
+// reads an FP64 summed-area table as the reference does; each (b, c) volume
+// is processed by one launch sequence on the caller's stream.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -33,17 +33,19 @@ struct TomoDims {
 };
 
 // ---------------------------------------------------------------------------
-// Summed-area tables.  FP: per z plane, layout [z][y][x] (x fastest), x in
-// [0, nx], y in [0, ny].  BP: per view, the length-weighted projections,
-// layout [view][v][u] (u fastest), u in [0, nu], v in [0, nv].  Rows run
-// along the axis that the lanes of the main kernels walk, so their corner
-// lookups are coalesced.  Built in two passes: a tiled pass that reads the
-// source along its contiguous axis, transposes 32 x 32 tiles through shared
-// memory and scans along the row with warp scans (carry across tiles), then
-// a pass along the other axis.
+// Tables (FP64).  FP: per z plane, row prefixes along x of image row y,
+// layout [z][y + 1][x] (x fastest, x in [0, nx]); a rectangle integral is the
+// sum over the rows it overlaps (rows_integral), which equals the reference's
+// summed-area-table corner form.  BP: per view, the (u, v) summed-area table
+// of the length-weighted projections, layout [view][v][u] (u fastest, u in
+// [0, nu], v in [0, nv]).  Rows run along the axis that the lanes of the main
+// kernels walk, so their reads are coalesced.  Row prefixes are built by a
+// tiled pass that reads the source along its contiguous axis, transposes 32 x
+// 32 tiles through shared memory and scans along the row with warp scans
+// (carry across tiles); the BP table then gets a pass along v.
 // ---------------------------------------------------------------------------
 
-// Row prefixes S[z][y + 1][x + 1] = sum_{x' <= x} img[x'][y][z].  Block
+// Row prefixes R[z][y + 1][x + 1] = sum_{x' <= x} img[x'][y][z].  Block
 // (32, 8): blockIdx.x = y, blockIdx.y = a tile of 32 planes.
 __global__ void __launch_bounds__(256) tomo_sat_x(double* __restrict__ sat, const float* __restrict__ img, TomoDims d,
                                                   int b, int c) {
@@ -79,20 +81,6 @@ __global__ void __launch_bounds__(256) tomo_sat_x(double* __restrict__ sat, cons
             for (int x = lane; x <= d.nx; x += 32) sat[(z0 + zz) * plane + x] = 0.0;
 }
 
-// Column prefixes along y: one thread per (z, x), x fastest.
-__global__ void tomo_sat_y(double* __restrict__ sat, TomoDims d) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nz * (d.nx + 1)) return;
-    const int z = i / (d.nx + 1), x = i - z * (d.nx + 1);
-    const long long row = d.nx + 1;
-    double* col = sat + (long long)z * (d.nx + 1) * (d.ny + 1) + x;
-    double acc = 0.0;
-    for (int y = 1; y <= d.ny; y++) {
-        acc += col[y * row];
-        col[y * row] = acc;
-    }
-}
-
 // Length weight of detector cell (u, v) of a view (PreweightBPCartKernelXY,
 // DistanceDriven3D.cu:409-431).
 __device__ __forceinline__ double tomo_len_weight(const float* dc, const float* sp, float u, float v, float dz) {
@@ -100,7 +88,7 @@ __device__ __forceinline__ double tomo_len_weight(const float* dc, const float* 
     return (double)dz / fabs(ddz) * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
 }
 
-// Weighted row prefixes S[view][v + 1][u + 1] = sum_{u' <= u} w p(u', v).
+// Weighted row prefixes R[view][v + 1][u + 1] = sum_{u' <= u} w p(u', v).
 // weight_all = 0 applies the length weight to view 0 only, as the reference's
 // pre-weight launch does (its grid has one row of views,
 // DistanceDriven3D.cu:612-621); 1 weights every view.  Block (32, 8):
@@ -179,6 +167,27 @@ __device__ __forceinline__ Lerp lerp_at(float x, int n) {
     l.w = (double)(x - (float)l.i0);
     return l;
 }
+// Integral over [y1, y2] (clamped to [0, n]; the result changes sign when
+// y2 < y1) of the row prefixes of a table R[row j + 1][col], interpolated
+// linearly at the column lc: the summed-area-table difference S(c, y2) -
+// S(c, y1) written as the rows that [y1, y2] overlaps, each weighted by its
+// overlap.  Equal to the bilinear corner form of InterpolateXY / UV in exact
+// arithmetic, with one or two rows instead of four corner reads.
+__device__ __forceinline__ double rows_integral(const double* __restrict__ R, const Lerp& lc, float y1, float y2, int n,
+                                                long long row) {
+    float lo = fminf(y1, y2), hi = fmaxf(y1, y2);
+    lo = fminf(fmaxf(lo, 0.f), (float)n);
+    hi = fminf(fmaxf(hi, 0.f), (float)n);
+    double acc = 0.0;
+#pragma unroll 4
+    for (int j = (int)lo; (float)j < hi; j++) {   // rows j < n overlapped by [lo, hi]
+        const float ov = fminf(hi, (float)(j + 1)) - fmaxf(lo, (float)j);
+        const double* r = R + (long long)(j + 1) * row;
+        acc += (r[lc.i0] * (1 - lc.w) + r[lc.i1] * lc.w) * (double)ov;
+    }
+    return y2 >= y1 ? acc : -acc;
+}
+
 // Bilinear value of a table with rows along the second coordinate:
 // a[r * row + col], col from lc, r from lr.
 __device__ __forceinline__ double sat_at(const double* __restrict__ a, const Lerp& lc, const Lerp& lr, long long row) {
@@ -190,10 +199,11 @@ __device__ __forceinline__ double sat_at(const double* __restrict__ a, const Ler
 // FP: lane i of a warp owns detector column iu = 31 blockIdx.x + i and its
 // left cell edge; lane 31 only supplies the right edge of lane 30's cell.  A
 // warp handles one detector row v of one view, and per z plane each lane
-// evaluates D = S(x_e, y2) - S(x_e, y1) at its edge, so the rectangle
-// integral of a cell is D(next lane) - D(this lane): 8 table reads per ray
-// and plane instead of 16.  The rectangle's area is (x_{e+1} - x_e)(y2 - y1) =
-// drx dry (z - sz)^2, exact for the straight edge rays.
+// evaluates D = S(x_e, y2) - S(x_e, y1) at its edge from the rows [y1, y2]
+// overlaps, so the rectangle integral of a cell is D(next lane) - D(this
+// lane): two reads per overlapped row instead of the reference's 16 corner
+// reads.  The rectangle's area is (x_{e+1} - x_e)(y2 - y1) = drx dry
+// (z - sz)^2, exact for the straight edge rays.
 __global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, const double* __restrict__ sat,
                                                       const float* __restrict__ detCenter,
                                                       const float* __restrict__ src, TomoDims d, int b, int c) {
@@ -222,11 +232,9 @@ __global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, c
     for (int iz = 0; iz < d.nz; iz++) {
         const float t = (float)iz - sz;
         const Lerp lx = lerp_at(sx + rxe * t, d.nx + 1);
-        const Lerp l1 = lerp_at(sy + rya * t, d.ny + 1), l2 = lerp_at(sy + ryb * t, d.ny + 1);
-        const double* a = sat + iz * plane;
-        const double D = sat_at(a, lx, l2, row) - sat_at(a, lx, l1, row);
+        const double D = rows_integral(sat + iz * plane, lx, sy + rya * t, sy + ryb * t, d.ny, row);
         const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
-        val = fmaf((float)q, k / (t * t), val);
+        val = fmaf((float)q, __fdividef(k, t * t), val);
     }
     if (lane < 31 && iu < d.nu) {
         val *= (float)tomo_len_weight(dc, sp, u, v, d.dz);
@@ -239,8 +247,10 @@ __global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, c
 // face; lane 31 only supplies the right face of lane 30's voxel.  A warp
 // handles one (y, z) row.  Per view each lane evaluates D = S(u_e, v2) -
 // S(u_e, v1) at its face's detector coordinate (ProjectConeToDetCart,
-// DistanceDriven3D.cu:478-489), and the voxel's rectangle integral is
-// D(next lane) - D(this lane); the rectangle's area is r^2 dx dy / (du dv).
+// DistanceDriven3D.cu:478-489) by bilinear reads of the (u, v) summed-area
+// table, and the voxel's rectangle integral is D(next lane) - D(this lane):
+// 8 table reads instead of the reference's 16.  The rectangle's area is
+// r^2 dx dy / (du dv).
 __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, const double* __restrict__ sat,
                                                       const float* __restrict__ detCenter,
                                                       const float* __restrict__ src, TomoDims d, int b, int c) {
@@ -268,7 +278,7 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
         const double* a = sat + view * vplane;
         const double D = sat_at(a, lu, l2, row) - sat_at(a, lu, l1, row);
         const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
-        val = fmaf((float)q, 1.0f / (r * r * aunit), val);
+        val = fmaf((float)q, __fdividef(1.0f, r * r * aunit), val);
     }
     if (lane < 31 && ix < d.nx)
         img[(long long)b * d.nx * d.ny * d.nz * d.nc + (((long long)ix * d.ny + iy) * d.nz + iz) * d.nc + c] = val;
@@ -288,7 +298,6 @@ int tomo_project(float* d_prj, const float* d_img, const float* d_dc, const floa
     for (int b = 0; b < d.nb; b++)
         for (int c = 0; c < d.nc; c++) {
             tomo_sat_x<<<dim3(d.ny, (d.nz + 31) / 32), dim3(32, 8), 0, st>>>(d_sat, d_img, d, b, c);
-            tomo_sat_y<<<(d.nz * (d.nx + 1) + 255) / 256, 256, 0, st>>>(d_sat, d);
             dim3 blk(32, 4);
             dim3 grd((d.nu + 30) / 31, d.nview, (d.nv + 3) / 4);
             tomo_fp_kernel<<<grd, blk, 0, st>>>(d_prj, d_sat, d_dc, d_src, d, b, c);
