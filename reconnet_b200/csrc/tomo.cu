@@ -264,15 +264,16 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
     const float z = (iz - (d.nz - 1) / 2.0f) * d.dz + d.cz;
     const float cu = d.off_u + (d.nu - 1) / 2.0f, cv = d.off_v + (d.nv - 1) / 2.0f;
     const float aunit = d.dx * d.dy / (d.du * d.dv);
+    const float idu = 1.0f / d.du, idv = 1.0f / d.dv;
     const long long vplane = (long long)(d.nu + 1) * (d.nv + 1), row = d.nu + 1;
     float val = 0.f;
     for (int view = 0; view < d.nview; view++) {
         const float* dc = detCenter + 3 * view;
         const float* sp = src + 3 * view;
         const float r = (dc[2] - sp[2]) / (z - sp[2]);
-        const float ue = (sp[0] - dc[0] + r * (xf - sp[0])) / d.du + cu;
-        const float v1 = (sp[1] - dc[1] + r * (y - d.dy / 2 - sp[1])) / d.dv + cv;
-        const float v2 = (sp[1] - dc[1] + r * (y + d.dy / 2 - sp[1])) / d.dv + cv;
+        const float ue = fmaf(sp[0] - dc[0] + r * (xf - sp[0]), idu, cu);
+        const float v1 = fmaf(sp[1] - dc[1] + r * (y - d.dy / 2 - sp[1]), idv, cv);
+        const float v2 = fmaf(sp[1] - dc[1] + r * (y + d.dy / 2 - sp[1]), idv, cv);
         const Lerp lu = lerp_at(ue, d.nu + 1);
         const Lerp l1 = lerp_at(v1, d.nv + 1), l2 = lerp_at(v2, d.nv + 1);
         const double* a = sat + view * vplane;
