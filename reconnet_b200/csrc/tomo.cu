@@ -254,10 +254,12 @@ __global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, c
 __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, const double* __restrict__ sat,
                                                       const float* __restrict__ detCenter,
                                                       const float* __restrict__ src, TomoDims d, int b, int c) {
+    // z runs fastest over the grid, so the CTAs resident at a time cover few
+    // (x, y) columns and their detector footprints in all views stay in L2
     const int lane = threadIdx.x;
-    const int ix = blockIdx.x * 31 + lane;
-    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    const int iz = blockIdx.z;
+    const int iz = blockIdx.x;
+    const int ix = blockIdx.y * 31 + lane;
+    const int iy = blockIdx.z * blockDim.y + threadIdx.y;
     if (iy >= d.ny) return;   // warp-uniform
     const float xf = (ix - (d.nx - 1) / 2.0f) * d.dx + d.cx - d.dx / 2;
     const float y = (iy - (d.ny - 1) / 2.0f) * d.dy + d.cy;
@@ -316,7 +318,7 @@ int tomo_backproject(float* d_img, const float* d_prj, const float* d_dc, const 
                                                                                     c, weight_all);
             tomo_bp_sat_v<<<(d.nview * (d.nu + 1) + 255) / 256, 256, 0, st>>>(d_sat, d);
             dim3 blk(32, 8);
-            dim3 grd((d.nx + 30) / 31, (d.ny + 7) / 8, d.nz);
+            dim3 grd(d.nz, (d.nx + 30) / 31, (d.ny + 7) / 8);
             tomo_bp_kernel<<<grd, blk, 0, st>>>(d_img, d_sat, d_dc, d_src, d, b, c);
         }
     RN_CUDA_TRY(cudaGetLastError());
