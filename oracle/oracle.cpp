@@ -15,6 +15,9 @@
 // T: T = double is the FP64 oracle used for parity, T = float is the FP32
 // OpenMP port used as the timed CPU baseline.
 //
+// The Siddon pair is restated with exact FP64 crossings rather than the
+// reference's incremental FP32 tracing (see siddon_trace).
+//
 // The matched backprojector (typeProjector == 2) is not a reference kernel:
 // it is the mechanical transpose of the FP restatement below (scatter into
 // adjoint prefix arrays, then suffix sums), so <Ax, y> == <x, A^T y> holds to
@@ -513,6 +516,128 @@ double tv_sqs(T* grad, T* norm, const float* img, int nx, int ny) {
 }
 
 // --------------------------------------------------------------------------
+// Siddon fan projector pair: SiddonFanProjectionKernel /
+// SiddonFanBackprojectionKernel with InitializeSiddon and the tracing loops
+// (Siddon.cu:14-375).  Ray (iu, iview, iv) runs from the source
+// (dso sin t, -dso cos t, z) to the centre of detector cell iu rotated with
+// the view, at the height z = (iv - (nv-1)/2 + off_v) dv of its detector row
+// (Siddon.cu:253-263); image coordinates put the origin at the corner of
+// voxel 0 (:13-20).  Each voxel receives the length (mm) of the ray inside it.
+// Restated with the exact parametric crossings in FP64: every crossing of a
+// grid plane between the entry and exit parameters, sorted, and the voxel at
+// the middle of each segment.  An axis along which the ray moves by at most
+// 1e-6 voxels is parallel, as InboundAlpha treats it (:22-41).
+// --------------------------------------------------------------------------
+template <typename Visit>
+void siddon_trace(const Fan& g, const double src[3], const double dst[3], Visit&& visit) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double d[3] = {g.dx, g.dy, g.dz};
+    double dist = 0;
+    double s[3], e[3], dd[3];
+    for (int k = 0; k < 3; k++) {
+        dist += (src[k] - dst[k]) * (src[k] - dst[k]);
+        s[k] = src[k] / d[k] + n[k] / 2.0;   // centre of the grid at the origin
+        e[k] = dst[k] / d[k] + n[k] / 2.0;
+        dd[k] = e[k] - s[k];
+    }
+    dist = std::sqrt(dist);
+    bool par[3];
+    double amin = 0.0, amax = 1.0;
+    for (int k = 0; k < 3; k++) {
+        par[k] = !(std::fabs(dd[k]) > 1e-6);
+        if (par[k]) {
+            if (s[k] < 0 || s[k] > n[k]) return;
+            continue;
+        }
+        double a0 = (0 - s[k]) / dd[k], a1 = (n[k] - s[k]) / dd[k];
+        amin = std::max(amin, std::min(a0, a1));
+        amax = std::min(amax, std::max(a0, a1));
+    }
+    if (amax <= amin) return;
+    std::vector<double> al;
+    al.reserve(n[0] + n[1] + n[2] + 2);
+    al.push_back(amin);
+    al.push_back(amax);
+    for (int k = 0; k < 3; k++) {
+        if (par[k]) continue;
+        for (int i = 0; i <= n[k]; i++) {
+            double a = (i - s[k]) / dd[k];
+            if (a > amin && a < amax) al.push_back(a);
+        }
+    }
+    std::sort(al.begin(), al.end());
+    for (size_t i = 0; i + 1 < al.size(); i++) {
+        double a = al[i], b = al[i + 1];
+        if (b <= a) continue;
+        double m = 0.5 * (a + b);
+        int idx[3];
+        bool inside = true;
+        for (int k = 0; k < 3; k++) {
+            double p = par[k] ? s[k] : s[k] + m * dd[k];
+            idx[k] = (int)std::floor(p);
+            if (idx[k] < 0 || idx[k] >= n[k]) inside = false;
+        }
+        if (inside) visit(idx[0], idx[1], idx[2], (b - a) * dist);
+    }
+}
+
+inline void siddon_ray(const Fan& g, double deg, int iu, int iv, double src[3], double dst[3]) {
+    double c = std::cos(deg), sn = std::sin(deg);
+    double a = chan_angle(g, iu);
+    double z = (iv - (g.nv - 1) / 2.0 + g.off_v) * g.dv;
+    src[0] = g.dso * sn;
+    src[1] = -g.dso * c;
+    src[2] = z;
+    double rx = g.dsd * std::sin(a), ry = -g.dso + g.dsd * std::cos(a);
+    dst[0] = rx * c - ry * sn;
+    dst[1] = rx * sn + ry * c;
+    dst[2] = z;
+}
+
+template <typename T>
+void siddon_fp(T* prj, const float* img, const float* deg, const Fan& g) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int b = 0; b < g.nb; b++)
+        for (int iview = 0; iview < g.nview; iview++)
+            for (int iu = 0; iu < g.nu; iu++)
+                for (int iv = 0; iv < g.nv; iv++) {
+                    double src[3], dst[3];
+                    siddon_ray(g, deg[iview], iu, iv, src, dst);
+                    for (int c = 0; c < g.nc; c++) {
+                        double val = 0;
+                        siddon_trace(g, src, dst, [&](int ix, int iy, int iz, double len) {
+                            val += len * img[img_index(g, b, ix, iy, iz, c)];
+                        });
+                        prj[prj_index(g, b, iu, iview, iv, c)] = (T)val;
+                    }
+                }
+}
+
+// The exact transpose of siddon_fp (the reference scatters with atomicAdd,
+// Siddon.cu:268-375); accumulated per batch in a local FP64 image.
+template <typename T>
+void siddon_bp(T* img, const float* prj, const float* deg, const Fan& g) {
+    for (int b = 0; b < g.nb; b++)
+        for (int c = 0; c < g.nc; c++) {
+            std::vector<double> acc((size_t)g.nx * g.ny * g.nz, 0.0);
+            for (int iview = 0; iview < g.nview; iview++)
+                for (int iu = 0; iu < g.nu; iu++)
+                    for (int iv = 0; iv < g.nv; iv++) {
+                        double src[3], dst[3];
+                        siddon_ray(g, deg[iview], iu, iv, src, dst);
+                        double w = prj[prj_index(g, b, iu, iview, iv, c)];
+                        siddon_trace(g, src, dst, [&](int ix, int iy, int iz, double len) {
+                            acc[((size_t)ix * g.ny + iy) * g.nz + iz] += w * len;
+                        });
+                    }
+            for (int ix = 0; ix < g.nx; ix++)
+                for (int iy = 0; iy < g.ny; iy++)
+                    for (int iz = 0; iz < g.nz; iz++)
+                        img[img_index(g, b, ix, iy, iz, c)] = (T)acc[((size_t)ix * g.ny + iy) * g.nz + iz];
+        }
+}
+
+// --------------------------------------------------------------------------
 // Tomosynthesis DD: DistanceDrivenTomo::ProjectionTomo / BackprojectionTomo
 // (DistanceDriven3D.cu:37-343, :409-663).  detU = (1,0,0), detV = (0,1,0).
 // --------------------------------------------------------------------------
@@ -728,6 +853,13 @@ void oracle_fan_bp_f32(float* img, const float* prj, const float* deg, FAN_ARGS,
     if (typeProjector == 2) fan_bp_matched<float>(img, prj, deg, g);
     else fan_bp_ref<float>(img, prj, deg, g, typeProjector);
 }
+void oracle_siddon_fp_f64(double* prj, const float* img, const float* deg, FAN_ARGS) {
+    siddon_fp<double>(prj, img, deg, make_fan(FAN_PASS));
+}
+void oracle_siddon_bp_f64(double* img, const float* prj, const float* deg, FAN_ARGS) {
+    siddon_bp<double>(img, prj, deg, make_fan(FAN_PASS));
+}
+
 void oracle_ramp_kernel(double* h, int nu, float da, int typeFilter, int equispace) {
     std::vector<double> k = ramp_kernel(nu, da, typeFilter, equispace != 0);
     std::memcpy(h, k.data(), sizeof(double) * k.size());

@@ -51,6 +51,8 @@ def lib():
         L.oracle_fan_fp_f64.argtypes = [_dp, _fp, _fp] + _FAN
         L.oracle_fan_fp_f32.argtypes = [_fp, _fp, _fp] + _FAN
         L.oracle_fan_bp_f64.argtypes = [_dp, _fp, _fp] + _FAN + [_i]
+        L.oracle_siddon_fp_f64.argtypes = [_dp, _fp, _fp] + _FAN
+        L.oracle_siddon_bp_f64.argtypes = [_dp, _fp, _fp] + _FAN
         L.oracle_fan_bp_f32.argtypes = [_fp, _fp, _fp] + _FAN + [_i]
         L.oracle_ramp_kernel.argtypes = [_dp, _i, _f, _i, _i]
         L.oracle_filter_f64.argtypes = [_dp, _fp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i]
@@ -129,6 +131,31 @@ def ramp_kernel(nu, da, type_filter=0, equispace=False):
     h = np.zeros(2 * nu - 1, np.float64)
     lib().oracle_ramp_kernel(_ptr(h, ctypes.c_double), int(nu), float(da), int(type_filter), int(bool(equispace)))
     return h
+
+
+def siddon_fp(img, angles, g, nu, nv=None):
+    """Siddon fan forward projection (Siddon.cu:14-266): ray lengths in mm
+    through each voxel, exact FP64 crossings."""
+    img = _f32(img)
+    ang = _f32(angles)
+    B, nx, ny, nz, C = img.shape
+    nv = nz if nv is None else nv
+    out = np.zeros((B, nu, ang.size, nv, C), np.float64)
+    lib().oracle_siddon_fp_f64(_ptr(out, ctypes.c_double), _ptr(img, _f), _ptr(ang, _f),
+                               *_fan_args(g, img.shape, out.shape))
+    return out
+
+
+def siddon_bp(sino, angles, g, img_shape):
+    """Transpose of ``siddon_fp`` (Siddon.cu:268-420 scatters with atomics)."""
+    sino = _f32(sino)
+    ang = _f32(angles)
+    B, nu, nview, nv, C = sino.shape
+    nx, ny, nz = img_shape
+    out = np.zeros((B, nx, ny, nz, C), np.float64)
+    lib().oracle_siddon_bp_f64(_ptr(out, ctypes.c_double), _ptr(sino, _f), _ptr(ang, _f),
+                               *_fan_args(g, out.shape, sino.shape))
+    return out
 
 
 def filter_sino(sino, g, type_filter=0, fan=True):

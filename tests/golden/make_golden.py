@@ -8,6 +8,7 @@ geometry and reference outputs); the CPU test suite checks the oracle against
 these files.
 
     python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py --siddon [outdir]   (the Siddon pair only)
 """
 import ctypes
 import math
@@ -38,6 +39,9 @@ def load_ref(path=REF):
     tomo = [_fp, _fp, _fp, _fp] + [_i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f]
     lib.cDistanceDrivenTomoProjection.argtypes = tomo
     lib.cDistanceDrivenTomoBackprojection.argtypes = tomo
+    if hasattr(lib, "cSiddonFanProjection"):
+        lib.cSiddonFanProjection.argtypes = fan
+        lib.cSiddonFanBackprojection.argtypes = fan
     return lib
 
 
@@ -111,7 +115,39 @@ def tomo_case(lib, rng):
                 **{k: np.float64(v) for k, v in g.items()})
 
 
-def main(outdir=HERE):
+SIDDON_CASES = {
+    "siddon2d": (dict(nx=48, ny=40, nz=1, dx=1.0, dy=1.1, dz=1.0, nu=64, nv=1, da=0.0025, dv=1.0, off_a=0.3,
+                      off_v=0.0, dsd=1085.6, dso=595.0), 1, 1, 72),
+    "siddon_multislice": (dict(nx=40, ny=36, nz=3, dx=1.0, dy=1.0, dz=1.0, nu=48, nv=3, da=0.003, dv=1.0,
+                               off_a=0.0, off_v=0.25, dsd=1085.6, dso=595.0), 2, 1, 30),
+}
+
+
+def siddon_case(lib, rng):
+    """cSiddonFanProjection / cSiddonFanBackprojection (Siddon.cu:424-538)."""
+    out = {}
+    for name, (g, B, C, nview) in SIDDON_CASES.items():
+        ang = (np.arange(nview) * 2 * np.pi / nview + 0.013).astype(np.float32)
+        img = rng.random((B, g["nx"], g["ny"], g["nz"], C)).astype(np.float32)
+        sino_in = rng.random((B, g["nu"], nview, g["nv"], C)).astype(np.float32)
+        args = (B, C, g["nx"], g["ny"], g["nz"], g["dx"], g["dy"], g["dz"], g["nu"], nview, g["nv"], g["da"], g["dv"],
+                g["off_a"], g["off_v"], g["dsd"], g["dso"], 0)
+        fp = np.zeros((B, g["nu"], nview, g["nv"], C), np.float32)
+        lib.cSiddonFanProjection(p(fp), p(img), p(ang), *args)
+        bp = np.zeros(img.shape, np.float32)
+        lib.cSiddonFanBackprojection(p(bp), p(sino_in), p(ang), *args)
+        out[name] = dict(img=img, sino_in=sino_in, angles=ang, fp=fp, bp=bp, B=B, C=C,
+                         **{k: np.float64(v) for k, v in g.items()})
+    return out
+
+
+def main(outdir=HERE, only=None):
+    if only == "siddon":
+        lib = load_ref()
+        for name, d in siddon_case(lib, np.random.default_rng(20241203)).items():
+            np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
+        print("siddon golden vectors written to", outdir)
+        return
     lib = load_ref()
     rng = np.random.default_rng(20240601)
     for name in FAN_CASES:
@@ -122,4 +158,5 @@ def main(outdir=HERE):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else HERE, only="siddon" if "--siddon" in sys.argv else None)
