@@ -48,6 +48,7 @@ extern "C" {
 #define RN_TYPE_ITERATIVE 0
 #define RN_TYPE_FBP 1
 #define RN_TYPE_MATCHED 2
+#define RN_TYPE_SIDDON 3     /* Siddon ray lengths (rn_fan_project_siddon / rn_fan_backproject) */
 
 const char* rn_last_error(void);
 int rn_last_status(void);
@@ -72,6 +73,17 @@ void cDistanceDrivenFanBackprojection(float* img, const float* prj, const float*
                                       int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview,
                                       int nv, float da, float dv, float off_a, float off_v, float dsd, float dso,
                                       int typeProjector);
+
+/* replaces ReconNet4D/Siddon.cu:424-479 (prj is overwritten) */
+void cSiddonFanProjection(float* prj, const float* img, const float* deg, int nBatches, int nChannels, int nx, int ny,
+                          int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
+                          float off_a, float off_v, float dsd, float dso, int typeProjector);
+
+/* replaces ReconNet4D/Siddon.cu:481-536 (img is overwritten, as the reference
+ * zeroes its device copy before scattering) */
+void cSiddonFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels, int nx,
+                              int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da,
+                              float dv, float off_a, float off_v, float dsd, float dso, int typeProjector);
 
 /* replaces ReconNet4D/DistanceDriven3D.cu:346-407 */
 void cDistanceDrivenTomoProjection(float* prj, const float* img, const float* detCenter, const float* src,
@@ -147,8 +159,16 @@ int64_t rn_fan_plan_total_views(const rn_fan_plan* plan);
 /* Forward projection, device pointers, stream-ordered; prj is overwritten. */
 int rn_fan_project(rn_fan_plan* plan, float* d_prj, const float* d_img, void* stream);
 
-/* Backprojection; typeProjector as above.  accumulate = 0 overwrites img,
- * 1 adds to it (the reference class-level Backprojection accumulates). */
+/* Siddon forward projection (SiddonFanProjectionKernel,
+ * ReconNet4D/Siddon.cu:240-266): each ray, from the source to the centre of
+ * its detector cell at the height of its detector row, sums the voxels times
+ * the length (mm) of the ray inside them.  prj is overwritten. */
+int rn_fan_project_siddon(rn_fan_plan* plan, float* d_prj, const float* d_img, void* stream);
+
+/* Backprojection; typeProjector as above (RN_TYPE_SIDDON: the exact transpose
+ * of rn_fan_project_siddon, gathered per voxel; the reference scatters with
+ * atomics, Siddon.cu:268-380).  accumulate = 0 overwrites img, 1 adds to it
+ * (the reference class-level Backprojection accumulates). */
 int rn_fan_backproject(rn_fan_plan* plan, float* d_img, const float* d_prj, int typeProjector, int accumulate,
                        void* stream);
 

@@ -19,6 +19,7 @@ RN_ERR_TIMEOUT = 4
 RN_TYPE_ITERATIVE = 0
 RN_TYPE_FBP = 1
 RN_TYPE_MATCHED = 2
+RN_TYPE_SIDDON = 3
 
 _f = ctypes.c_float
 _i = ctypes.c_int
@@ -52,6 +53,8 @@ SIGNATURES = {
     "SetDevice": (_i, [_i]),
     "cDistanceDrivenFanProjection": (None, [_fp, _fp, _fp] + _FAN),
     "cDistanceDrivenFanBackprojection": (None, [_fp, _fp, _fp] + _FAN),
+    "cSiddonFanProjection": (None, [_fp, _fp, _fp] + _FAN),
+    "cSiddonFanBackprojection": (None, [_fp, _fp, _fp] + _FAN),
     "cDistanceDrivenTomoProjection": (None, [_fp, _fp, _fp, _fp] + _TOMO),
     "cDistanceDrivenTomoBackprojection": (None, [_fp, _fp, _fp, _fp] + _TOMO),
     "cFilterFanFilter": (None, [_fp, _fp] + _FILT),
@@ -64,6 +67,7 @@ SIGNATURES = {
     "rn_fan_plan_destroy": (_i, [_vp]),
     "rn_fan_plan_total_views": (ctypes.c_int64, [_vp]),
     "rn_fan_project": (_i, [_vp, _vp, _vp, _vp]),
+    "rn_fan_project_siddon": (_i, [_vp, _vp, _vp, _vp]),
     "rn_fan_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "rn_fan_plan_check": (_i, [_vp, _vp]),
     "rn_fan_plan_set_timing": (_i, [_vp, _i]),

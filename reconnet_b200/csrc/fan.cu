@@ -76,7 +76,8 @@ __global__ void edge_slope_kernel(double* edges, const double2* view_cs, const i
 // P[k] = sum_{i<k} a_i as (hi, lo) and the value a_k (a_n = 0).
 // ---------------------------------------------------------------------------
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
-                                 FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems) {
+                                 FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems,
+                                 int band) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     int per_slice = d.ny + d.nx;
@@ -97,7 +98,8 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
         int k = k0 + lane;
         double a = 0.0;
         if (k < n) {
-            // blended value of rows (l-1, l) [X] or columns (l-1, l) [Y] at position k
+            // blended value of rows (l-1, l) [X] or columns (l-1, l) [Y] at position k;
+            // band mode (Siddon): row / column l itself
             float s = 0.f;
 #pragma unroll
             for (int j = 0; j < 2; j++) {
@@ -112,7 +114,7 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
                     v1 = __ldg(p + (long long)l * d.isx + (long long)k * d.isy);
                     if (l > 0) v0 = __ldg(p + (long long)(l - 1) * d.isx + (long long)k * d.isy);
                 }
-                s += w * (0.5f * v0 + 0.5f * v1);
+                s += w * (band ? v1 : 0.5f * v0 + 0.5f * v1);
             }
             a = (double)s;
         }
@@ -200,6 +202,7 @@ __device__ __forceinline__ int fp_ray_range(double ra, double rb, double par, do
     return (le > lb) ? (((int)lb << 16) | (int)le) : 0;
 }
 
+template <bool kSiddon>
 __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int4 w = p.work[blockIdx.x];
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             int rng = 0;
             if (lane < kFpGroupRays && u < nu) {
                 const double* ed = p.edges + (long long)s_gv[v] * (nu + 1);
-                rng = fp_ray_range(ed[u], ed[u + 1], s_par[v], s_perp[v], nlines, n_d);
+                rng = fp_ray_range(ed[u], ed[kSiddon ? u : u + 1], s_par[v], s_perp[v], nlines, n_d);
             }
             int lb = rng ? (rng >> 16) : 0x7fffffff;
             int le = rng ? (rng & 0xffff) : 0;
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     };
     // per-line factors 1 / (l - perp) of chunk c into slot c & 1
     auto line_factors = [&](int c) {
-        if (tid < vcount * R) {
+        if (!kSiddon && tid < vcount * R) {
             const int v = tid / R, j = tid - (tid / R) * R;
             s_g[(c & 1) * kFpViews * kFpMaxLines + v * kFpMaxLines + j] =
                 (float)(1.0 / ((double)(c * R + j) - s_perp[v]));
@@ -365,6 +368,30 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
             return (nhi - hi) + (nrest - rest);
         };
+        // Siddon (kSiddon): lane = ray.  On band j (image row / column j, not
+        // blended) the ray runs from its position at boundary j to boundary
+        // j + 1; the band adds the integral of the row over that interval
+        // divided by the interval's signed width r, taken from the two
+        // positions' cells.  The second position is formed from the first's
+        // fraction plus r, so the width keeps ~1e-7 cells of precision, and a
+        // ray that stays inside one cell adds that cell's value exactly (also
+        // for r = 0).  The epilogue multiplies by the ray length per band.
+        auto band = [&](float jf, int Xi, float Xf, float r, float ir, const float2* hrow, const float* arow) -> float {
+            const float x = fmaf(r, jf, Xf);
+            const float y = __fadd_rd(x, kFloorBias);
+            const int ka = __float_as_int(y) + Xi;
+            const float fa = x - (y - kFloorBias);
+            const float t = fa + r;
+            const float yt = __fadd_rd(t, kFloorBias);
+            const int kb = ka + (__float_as_int(yt) - kFloorBiasBits);
+            const float fb = t - (yt - kFloorBias);
+            const unsigned ua = min((unsigned)max(ka, 0), lpm1), ub = min((unsigned)max(kb, 0), lpm1);
+            const unsigned pa = ua + (ua >> 4), pb = ub + (ub >> 4);
+            const float2 ha = hrow[pa], hb = hrow[pb];
+            const float aa = arow[pa];
+            const float d = (hb.x - ha.x) + (fmaf(fb, arow[pb], hb.y) - fmaf(fa, aa, ha.y));
+            return ka == kb ? aa : d * ir;
+        };
         auto single = [&](int k, int J0, int J1) {
             int Xi;
             float Xf, r;
@@ -374,8 +401,14 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             const float* arow = LA + J0 * sp;
             float a = acc[k];
             float jf = (float)J0;
-            for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp)
-                a = fmaf(footprint(jf, Xi, Xf, r, hrow, arow), g[j], a);
+            if constexpr (kSiddon) {
+                const float ir = 1.0f / r;
+                for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp)
+                    a += band(jf, Xi, Xf, r, ir, hrow, arow);
+            } else {
+                for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp)
+                    a = fmaf(footprint(jf, Xi, Xf, r, hrow, arow), g[j], a);
+            }
             acc[k] = a;
         };
         // groups in pairs: where both have lines in this chunk, one loop over
@@ -396,9 +429,17 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                 const float* arow = LA + J0 * sp;
                 float aa = acc[k], ab = acc[k + 1];
                 float jf = (float)J0;
-                for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp) {
-                    aa = fmaf(footprint(jf, Xia, Xfa, ra, hrow, arow), ga[j], aa);
-                    ab = fmaf(footprint(jf, Xib, Xfb, rb, hrow, arow), gb[j], ab);
+                if constexpr (kSiddon) {
+                    const float ira = 1.0f / ra, irb = 1.0f / rb;
+                    for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp) {
+                        aa += band(jf, Xia, Xfa, ra, ira, hrow, arow);
+                        ab += band(jf, Xib, Xfb, rb, irb, hrow, arow);
+                    }
+                } else {
+                    for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp) {
+                        aa = fmaf(footprint(jf, Xia, Xfa, ra, hrow, arow), ga[j], aa);
+                        ab = fmaf(footprint(jf, Xib, Xfb, rb, hrow, arow), gb[j], ab);
+                    }
                 }
                 acc[k] = aa;
                 acc[k + 1] = ab;
@@ -423,11 +464,20 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         if (lane >= kFpGroupRays || u >= nu) continue;
         const int gv = s_gv[v];
         const double* ed = p.edges + (long long)gv * (nu + 1);
-        const float dr = (float)(ed[u + 1] - ed[u]);
-        const ViewGeo& vg = p.views[gv];
-        const float2 cs = p.cell[u];   // (cos a, sin a)
-        float Lw = xcls ? lenA / fabsf(vg.cosd * cs.x + vg.sind * cs.y) : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
-        p.prj[fs.prj_off + (long long)u * fs.su + (long long)s_vl[v] * fs.sview] = acc[k] * (Lw / dr);
+        float scale;
+        if constexpr (kSiddon) {
+            // ray length per band: r cells along the band, one band across
+            const double along = xcls ? p.d.dx : p.d.dy, across = xcls ? p.d.dy : p.d.dx;
+            scale = (float)sqrt(ed[u] * ed[u] * along * along + across * across);
+        } else {
+            const float dr = (float)(ed[u + 1] - ed[u]);
+            const ViewGeo& vg = p.views[gv];
+            const float2 cs = p.cell[u];   // (cos a, sin a)
+            const float Lw = xcls ? lenA / fabsf(vg.cosd * cs.x + vg.sind * cs.y)
+                                  : lenA / fabsf(vg.sind * cs.x - vg.cosd * cs.y);
+            scale = Lw / dr;
+        }
+        p.prj[fs.prj_off + (long long)u * fs.su + (long long)s_vl[v] * fs.sview] = acc[k] * scale;
     }
 }
 
@@ -531,9 +581,46 @@ __device__ __forceinline__ float ref_t(float px, float py, float c, float s, con
 }
 
 // Per-view parameters the BP inner loop reads, staged in shared memory.
+// Siddon BP table: per view, entry u + 1 holds the slope of ray u (a double
+// in x, y) and c_u = w_u * (ray length per band), w_u the sinogram value mixed
+// over the slice's detector rows.
+__global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin,
+                                    int ns, const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
+                                    const double* __restrict__ cslopes, FanDims d, float4* __restrict__ tab,
+                                    long long tab_base) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int si = blockIdx.y;
+    if (si >= ns) return;
+    const BpSlice bs = bps[s_begin + si];
+    const GeoSet gs = sets[bs.set];
+    const int vl = blockIdx.x * 8 + warp;
+    if (vl >= gs.nview) return;
+    const int gv = gs.view_off + vl;
+    const int nu = d.nu;
+    const double along = views[gv].xcls ? d.dx : d.dy, across = views[gv].xcls ? d.dy : d.dx;
+    float4* out = tab + (bs.table_off - tab_base) + (long long)vl * (nu + 2);
+    for (int u = lane; u < nu; u += 32) {
+        float w = 0.f;
+#pragma unroll
+        for (int k = 0; k < kBpMix; k++) {
+            const float wk = bs.prj_w[k];
+            if (wk == 0.f) continue;
+            w += wk * __ldg(prj + bs.prj_off[k] + (long long)u * bs.su + (long long)vl * bs.sview);
+        }
+        const double r = cslopes[(long long)gv * (nu + 1) + u];
+        const float c = w * (float)sqrt(r * r * along * along + across * across);
+        out[u + 1] = make_float4(__int_as_float(__double2loint(r)), __int_as_float(__double2hiint(r)), c, 0.f);
+    }
+    if (lane == 0) {
+        out[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        out[nu + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
 struct BpView {
+    double pard, perpd;   // source coordinates (Siddon band positions)
     float par, perp, kappa, tA, tB, sigma, cosd, sind;
-    int xcls, pad0, pad1, pad2;
+    int xcls, pad0;
 };
 
 struct BpShared {
@@ -639,13 +726,86 @@ __device__ __forceinline__ void bp_matched_y(float (&acc)[kBmRows], const BpView
     }
 }
 
+// Siddon backprojection (kMode 2), the exact transpose of the Siddon forward
+// projection: pixel column q-range [q, q + 1] on the band between lattice
+// lines l and l + 1 receives, from every ray u that crosses it, c_u (its
+// sinogram value times its length per band) times the fraction of the ray's
+// band interval [pos_u(l), pos_u(l + 1)] inside [q, q + 1], where pos_u(l) =
+// par + r_u (l - perp).  The candidate rays are those whose centre index
+// u + 1/2 lies between the edge indices t at the pixel's four lattice corners
+// (widened by 1e-3 against the cubic's truncation; a ray that misses the
+// pixel adds a zero fraction).  Table entry u + 1 holds r_u as a double and
+// c_u.  X-class: lane column q = x on lines y0 + j; Y-class: line l = x and
+// positions q = y0 + j; the corners on the neighbour column / line come from
+// the next lane.
+__device__ __forceinline__ float siddon_fraction(double r, double A, double D) {
+    // ray position relative to the pixel at line l (A = par - q, D = l - perp)
+    const float xa = (float)fma(r, D, A);
+    const float xb = xa + (float)r;
+    const float lo = fminf(xa, xb), hi = fmaxf(xa, xb);
+    const float ov = fmaxf(0.f, fminf(hi, 1.f) - fmaxf(lo, 0.f));
+    const float w = hi - lo;
+    return w > 1e-7f ? __fdividef(ov, w) : ((xa >= 0.f && xa < 1.f) ? 1.f : 0.f);
+}
+
+__device__ __forceinline__ float siddon_pixel(const float4* T, int ilo, int imax, int nu, float t00, float t01,
+                                              float t10, float t11, double A, double D) {
+    const float tmin = fminf(fminf(t00, t01), fminf(t10, t11)), tmax = fmaxf(fmaxf(t00, t01), fmaxf(t10, t11));
+    const int u0 = max(max((int)ceilf(tmin - 0.5f - 1e-3f), 0), ilo - 1);
+    const int u1 = min(min((int)floorf(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
+    float v = 0.f;
+    for (int u = u0; u <= u1; u++) {
+        const float4 E = T[u + 1 - ilo];
+        const double r = __hiloint2double(__float_as_int(E.y), __float_as_int(E.x));
+        v = fmaf(E.z, siddon_fraction(r, A, D), v);
+    }
+    return v;
+}
+
+__device__ __forceinline__ void bp_siddon_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                            int imax, int x, int y0, int nu) {
+    const float A = (float)x - vg.par;
+    const TCubic c = t_cubic(vg, A * __fdividef(1.0f, (float)(y0 + kBmRows / 2) - vg.perp));
+    const double Ad = vg.pard - (double)x;
+    float tp = 0.f, tnp = 0.f;
+#pragma unroll
+    for (int j = 0; j <= kBmRows; j++) {
+        const float h = A * __fdividef(1.0f, (float)(y0 + j) - vg.perp) - c.rt;
+        const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+        const float tn = __shfl_down_sync(0xffffffffu, t, 1);
+        if (j > 0)
+            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ad, (double)(y0 + j - 1) - vg.perpd);
+        tp = t;
+        tnp = tn;
+    }
+}
+
+__device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                            int imax, int x, int y0, int nu) {
+    const float g = __fdividef(1.0f, (float)x - vg.perp);
+    const float r0 = ((float)y0 - vg.par) * g;
+    const TCubic c = t_cubic(vg, fmaf((float)(kBmRows / 2), g, r0));
+    const double D = (double)x - vg.perpd;
+    float tp = 0.f, tnp = 0.f;
+#pragma unroll
+    for (int j = 0; j <= kBmRows; j++) {
+        const float h = fmaf((float)j, g, r0) - c.rt;
+        const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+        const float tn = __shfl_down_sync(0xffffffffu, t, 1);
+        if (j > 0)
+            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, vg.pard - (double)(y0 + j - 1), D);
+        tp = t;
+        tnp = tn;
+    }
+}
+
 // Warp 0 of a backprojection CTA prepares chunk c (views c*kBpViews ...) of
 // its tile at (X0, Y0): lane = view * 4 + tile corner evaluates the edge index
 // at its corner, a 4-lane min gives the first staged table entry, and the
 // view's parameters go to slot c % 3.  Kept out of line: it runs once per
 // chunk in one warp, and inlined its temporaries would raise the register
 // count of the whole accumulation loop.
-template <bool kMatched>
+template <int kMode>
 __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, int nview, int X0, int Y0,
                                      int tabn, int win, const FanDims d) {
     const int lane = threadIdx.x & 31, v = lane >> 2, corner = lane & 3;
@@ -653,7 +813,7 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
     const ViewGeo& vg = src[valid ? v : 0];
     const int cx = corner & 1, cy = corner >> 1;
     float t;
-    if (kMatched) {
+    if (kMode != 0) {
         const int xcls = vg.xcls;
         const float X = (float)(X0 + cx * kBmCols), Y = (float)(Y0 + cy * kBmTileY);
         const float l = xcls ? Y : X, q = xcls ? X : Y;
@@ -670,6 +830,8 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
         const int lo = (int)floorf(t) + 1 - 2;   // table index = edge/cell index + 1
         sh->elo[slot][v] = max(0, min(lo, tabn - win));
         BpView& w = sh->vw[slot][v];
+        w.pard = vg.par;
+        w.perpd = vg.perp;
         w.par = (float)vg.par;
         w.perp = (float)vg.perp;
         w.kappa = vg.kappa;
@@ -682,8 +844,10 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
     }
 }
 
-template <bool kMatched>
+// kMode: 0 reference-mode (typeProjector 0 / 1), 1 matched, 2 Siddon.
+template <int kMode>
 __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
+    constexpr bool kMatched = kMode != 0;   // column-warp tiles and the matched edge index
     extern __shared__ __align__(128) unsigned char smem[];
     BpShared* sh = reinterpret_cast<BpShared*>(smem);
     size_t off = (sizeof(BpShared) + 127) & ~size_t(127);
@@ -719,7 +883,7 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
 
     const int nchunks = (gs.nview + kBpViews - 1) / kBpViews;
     auto prep = [&](int c, const ViewGeo* src) {
-        bp_prep<kMatched>(sh, src, c, gs.nview, X0, Y0, tabn, p.win, p.d);
+        bp_prep<kMode>(sh, src, c, gs.nview, X0, Y0, tabn, p.win, p.d);
     };
     // tid 0: stage chunk c's table windows into buffer c & 1 and the view
     // records of chunk c + 1 into record slot (c + 1) & 1, on barrier c & 1.
@@ -773,7 +937,10 @@ __global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
             const int ilo = sh->elo[slot][v];
             const int cnt = min(p.win, tabn);
             const int imax = ilo + cnt - 1;   // <= nu + 1
-            if (kMatched) {
+            if (kMode == 2) {
+                if (vg.xcls) bp_siddon_x(acc, vg, T, ilo, imax, x0, y0, nu);
+                else bp_siddon_y(acc, vg, T, ilo, imax, x0, y0, nu);
+            } else if (kMode == 1) {
                 if (vg.xcls) bp_matched_x(acc, vg, T, ilo, imax, x0, y0, ny);
                 else bp_matched_y(acc, vg, T, ilo, imax, x0, y0, nx);
             } else {
@@ -891,9 +1058,11 @@ int fan_kernel_attributes() {
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if ((int)g_attr_done.size() <= dev) g_attr_done.resize(dev + 1, 0);
     if (g_attr_done[dev]) return RN_OK;
-    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
-    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
-    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_fp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
     g_attr_done[dev] = 1;
     return RN_OK;
 }
@@ -1011,6 +1180,21 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     edge_slope_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p->d_edges, d_vcs, d_vx, d_esc, (int)V, nu, g.dx,
                                                                      g.dy);
     RN_CUDA_TRY(cudaGetLastError());
+    // slopes of the rays through the cell centres (the Siddon pair): the same
+    // table with the fan angle of cell u itself (entry nu repeats a spacing on)
+    {
+        std::vector<double2> csc(nu + 1);
+        for (int e = 0; e <= nu; e++) {
+            double gam = (-((double)e - (nu - 1) / 2.0) - off_u) * du;
+            csc[e] = make_double2(std::sin(gam), std::cos(gam));
+        }
+        RN_CUDA_TRY(cudaMalloc(&p->d_cslopes, sizeof(double) * V * (nu + 1)));
+        RN_CUDA_TRY(cudaMemcpyAsync(d_esc, csc.data(), sizeof(double2) * (nu + 1), cudaMemcpyHostToDevice, st));
+        edge_slope_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p->d_cslopes, d_vcs, d_vx, d_esc, (int)V, nu,
+                                                                         g.dx, g.dy);
+        RN_CUDA_TRY(cudaGetLastError());
+        RN_CUDA_TRY(cudaStreamSynchronize(st));   // csc goes out of scope
+    }
     RN_CUDA_TRY(cudaStreamSynchronize(st));
     cudaFree(d_vcs);
     cudaFree(d_vx);
@@ -1025,7 +1209,7 @@ static int fp_lines_for_smem(int nu, int sp) {
     return R;
 }
 
-int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st) {
+int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st, bool siddon) {
     const FanDims& d = p->dims;
     const int nfp = (int)p->h_fp.size();
     const int R = std::min(fp_lines_for_smem(d.nu, d.spx), fp_lines_for_smem(d.nu, d.spy));
@@ -1041,8 +1225,8 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
         long long warps = (long long)ns * (d.nx + d.ny);
         {
             LaunchScope ls0(p, st, 0);
-            fan_lines_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(d_img, p->d_fp, s0, ns, d,
-                                                                                    p->d_hl, p->d_la, slot);
+            fan_lines_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(
+                d_img, siddon ? p->d_fps : p->d_fp, s0, ns, d, p->d_hl, p->d_la, slot, siddon ? 1 : 0);
         }
         RN_CUDA_TRY(cudaGetLastError());
         int wend = wbeg;
@@ -1050,11 +1234,11 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
         if (wend > wbeg) {
             FpParams fp;
             fp.views = p->d_views;
-            fp.edges = p->d_edges;
+            fp.edges = siddon ? p->d_cslopes : p->d_edges;
             fp.cell = p->d_cell;
             fp.perm = p->d_perm;
             fp.sets = p->d_sets;
-            fp.fps = p->d_fp;
+            fp.fps = siddon ? p->d_fps : p->d_fp;
             fp.work = p->d_fp_work + wbeg;
             fp.hl = p->d_hl;
             fp.la = p->d_la;
@@ -1066,7 +1250,8 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
             fp.R = R;
             fp.vt = fan_fp_views(d.nu);
             LaunchScope ls1(p, st, 1);
-            fan_fp_kernel<<<wend - wbeg, kFpThreads, smem, st>>>(fp);
+            if (siddon) fan_fp_kernel<true><<<wend - wbeg, kFpThreads, smem, st>>>(fp);
+            else fan_fp_kernel<false><<<wend - wbeg, kFpThreads, smem, st>>>(fp);
             RN_CUDA_TRY(cudaGetLastError());
         }
         wbeg = wend;
@@ -1076,10 +1261,11 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
 
 int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st) {
     const FanDims& d = p->dims;
-    const std::vector<BpSlice>& bps = (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
-    const BpSlice* dbp = (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
+    const bool siddon = type == RN_TYPE_SIDDON;
+    const std::vector<BpSlice>& bps = siddon ? p->h_bps : (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
+    const BpSlice* dbp = siddon ? p->d_bps : (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
     const int nbp = (int)bps.size();
-    const bool matched = type == RN_TYPE_MATCHED;
+    const bool matched = type == RN_TYPE_MATCHED || siddon;   // column-warp tiles
     const int win = matched ? p->table_win_m : p->table_win;
     const size_t smem = bp_smem_bytes(win);
     const int tw = matched ? kBmCols : kBpTile, th = matched ? kBmTileY : kBpTile;
@@ -1101,8 +1287,12 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         dim3 tg((maxv + 7) / 8, ns);
         {
             LaunchScope ls2(p, st, 2);
-            fan_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_edges, p->d_cell, d,
-                                             type, p->d_tab, base);
+            if (siddon)
+                siddon_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_cslopes, d,
+                                                        p->d_tab, base);
+            else
+                fan_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_edges, p->d_cell,
+                                                     d, type, p->d_tab, base);
         }
         RN_CUDA_TRY(cudaGetLastError());
         BpParams bp;
@@ -1122,8 +1312,9 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         bp.win = win;
         unsigned grid = (unsigned)(ns * tiles_x * tiles_y);
         LaunchScope ls3(p, st, 3);
-        if (type == RN_TYPE_MATCHED) fan_bp_kernel<true><<<grid, kBpThreads, smem, st>>>(bp);
-        else fan_bp_kernel<false><<<grid, kBpThreads, smem, st>>>(bp);
+        if (siddon) fan_bp_kernel<2><<<grid, kBpThreads, smem, st>>>(bp);
+        else if (type == RN_TYPE_MATCHED) fan_bp_kernel<1><<<grid, kBpThreads, smem, st>>>(bp);
+        else fan_bp_kernel<0><<<grid, kBpThreads, smem, st>>>(bp);
         RN_CUDA_TRY(cudaGetLastError());
         s0 = s1;
     }
@@ -1337,7 +1528,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     float* la = reinterpret_cast<float*>(base + o_la);
     const FpSlice* dfs = reinterpret_cast<const FpSlice*>(base + o_fp);
     fan_lines_kernel<<<(unsigned)(((long long)(nx + ny) * 32 + 255) / 256), 256, 0, st>>>(d_img, dfs, 0, 1, d, hl,
-                                                                                          la, slot);
+                                                                                          la, slot, 0);
     RN_CUDA_TRY(cudaGetLastError());
     RN_TRY(fan_kernel_attributes());
     FpParams fp;
@@ -1357,7 +1548,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     fp.d = d;
     fp.R = R;
     fp.vt = VT;
-    fan_fp_kernel<<<nwork, kFpThreads, smem, st>>>(fp);
+    fan_fp_kernel<false><<<nwork, kFpThreads, smem, st>>>(fp);
     RN_CUDA_TRY(cudaGetLastError());
     int herr = 0;
     RN_CUDA_TRY(cudaMemcpyAsync(&herr, base + o_err, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -396,7 +396,7 @@ static int finish_sync(HostCtx* c, rn_fan_plan* p) {
     return RN_OK;
 }
 
-static int host_fan_fp(float* prj, const float* img, const float* deg, const RnFanGeom& g) {
+static int host_fan_fp(float* prj, const float* img, const float* deg, const RnFanGeom& g, bool siddon = false) {
     HostCtx* c = host_ctx();
     std::lock_guard<std::mutex> lk(c->mu);
     RN_TRY(ctx_plan(c, g, deg, g.nview));
@@ -404,13 +404,13 @@ static int host_fan_fp(float* prj, const float* img, const float* deg, const RnF
     RN_TRY(c->a.ensure(ni * 4));
     RN_TRY(c->b.ensure(np * 4));
     RN_CUDA_TRY(cudaMemcpyAsync(c->a.p, img, ni * 4, cudaMemcpyHostToDevice, c->st));
-    RN_TRY(fan_project(c->plan, c->b.as<float>(), c->a.as<float>(), c->st));
+    RN_TRY(fan_project(c->plan, c->b.as<float>(), c->a.as<float>(), c->st, siddon));
     RN_CUDA_TRY(cudaMemcpyAsync(prj, c->b.p, np * 4, cudaMemcpyDeviceToHost, c->st));
     return finish_sync(c, c->plan);
 }
 
 static int host_fan_bp(float* img, const float* prj, const float* deg, const RnFanGeom& g, int type) {
-    if (type < 0 || type > 2) type = 0;   // the reference treats any non-1 type as iterative
+    if (type < 0 || type > 3) type = 0;   // the reference treats any non-1 type as iterative
     HostCtx* c = host_ctx();
     std::lock_guard<std::mutex> lk(c->mu);
     RN_TRY(ctx_plan(c, g, deg, g.nview));
@@ -442,6 +442,34 @@ void cDistanceDrivenFanProjection(float* prj, const float* img, const float* deg
     }
     host_fan_fp(prj, img, deg, fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a,
                                         off_v, dsd, dso));
+}
+
+void cSiddonFanProjection(float* prj, const float* img, const float* deg, int nBatches, int nChannels, int nx, int ny,
+                          int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
+                          float off_a, float off_v, float dsd, float dso, int typeProjector) {
+    (void)typeProjector;
+    clear_error();
+    if (!prj || !img || !deg) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    host_fan_fp(prj, img, deg,
+                fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso),
+                true);
+}
+
+void cSiddonFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels, int nx,
+                              int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da,
+                              float dv, float off_a, float off_v, float dsd, float dso, int typeProjector) {
+    (void)typeProjector;
+    clear_error();
+    if (!prj || !img || !deg) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    host_fan_bp(img, prj, deg,
+                fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso),
+                RN_TYPE_SIDDON);
 }
 
 void cDistanceDrivenFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels,

@@ -119,6 +119,8 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     RN_CUDA_TRY(cudaMalloc(&p->d_fp, sizeof(FpSlice) * p->h_fp.size()));
     RN_CUDA_TRY(cudaMalloc(&p->d_bp, sizeof(BpSlice) * p->h_bp.size()));
     RN_CUDA_TRY(cudaMalloc(&p->d_bpr, sizeof(BpSlice) * p->h_bpr.size()));
+    RN_CUDA_TRY(cudaMalloc(&p->d_fps, sizeof(FpSlice) * p->h_fps.size()));
+    RN_CUDA_TRY(cudaMalloc(&p->d_bps, sizeof(BpSlice) * p->h_bps.size()));
     RN_CUDA_TRY(cudaMalloc(&p->d_fp_work, sizeof(int4) * std::max(1, p->n_fp_work)));
     RN_CUDA_TRY(cudaMalloc(&p->d_err, sizeof(int)));
     RN_CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
@@ -126,6 +128,10 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     RN_CUDA_TRY(cudaMemcpyAsync(p->d_bp, p->h_bp.data(), sizeof(BpSlice) * p->h_bp.size(), cudaMemcpyHostToDevice, st));
     RN_CUDA_TRY(
         cudaMemcpyAsync(p->d_bpr, p->h_bpr.data(), sizeof(BpSlice) * p->h_bpr.size(), cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(
+        cudaMemcpyAsync(p->d_fps, p->h_fps.data(), sizeof(FpSlice) * p->h_fps.size(), cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(
+        cudaMemcpyAsync(p->d_bps, p->h_bps.data(), sizeof(BpSlice) * p->h_bps.size(), cudaMemcpyHostToDevice, st));
     if (p->n_fp_work > 0)
         RN_CUDA_TRY(cudaMemcpyAsync(p->d_fp_work, p->h_fp_work.data(), sizeof(int4) * p->n_fp_work,
                                     cudaMemcpyHostToDevice, st));
@@ -171,6 +177,9 @@ int rn_fan_plan_destroy(rn_fan_plan* p) {
     cudaFree(p->d_fp);
     cudaFree(p->d_bp);
     cudaFree(p->d_bpr);
+    cudaFree(p->d_fps);
+    cudaFree(p->d_bps);
+    cudaFree(p->d_cslopes);
     cudaFree(p->d_fp_work);
     cudaFree(p->d_err);
     cudaFree(p->d_hl);
@@ -282,6 +291,48 @@ int rn_fan_plan_create(rn_fan_plan** out, const RnFanGeom* g, const float* host_
                 p->h_bp.push_back(m);
                 p->h_bpr.push_back(r);
             }
+    // Siddon slices: a ray at the height of detector row iv stays in image
+    // slice floor(z) (it is parallel to the slices, Siddon.cu:22-60), none if
+    // z falls outside [0, nz)
+    std::vector<int> siz(nv, -1);
+    std::vector<std::vector<int>> srows(nz);
+    for (int iv = 0; iv < nv; iv++) {
+        double z = (iv - (nv - 1) / 2.0 + g->off_v) * g->dv;
+        double zc = (z - g->cz) / g->dz + nz / 2.0;
+        if (zc >= 0 && zc < nz) {
+            siz[iv] = std::min((int)std::floor(zc), nz - 1);
+            srows[siz[iv]].push_back(iv);
+        }
+    }
+    for (int iz = 0; iz < nz; iz++)
+        if ((int)srows[iz].size() > kBpMix) {
+            delete p;
+            return set_error(RN_ERR_ARG, "fan geometry: more than 4 detector rows fall in one image slice (Siddon)");
+        }
+    for (int b = 0; b < B; b++)
+        for (int iv = 0; iv < nv; iv++)
+            for (int c = 0; c < C; c++) {
+                FpSlice f = p->h_fp[((size_t)b * nv + iv) * C + c];
+                memset(f.img_off, 0, sizeof(f.img_off));
+                memset(f.img_w, 0, sizeof(f.img_w));
+                if (siz[iv] >= 0) {
+                    f.img_off[0] = b * img_b + (long long)siz[iv] * C + c;
+                    f.img_w[0] = 1.f;
+                }
+                p->h_fps.push_back(f);
+            }
+    for (int b = 0; b < B; b++)
+        for (int z = 0; z < nz; z++)
+            for (int c = 0; c < C; c++) {
+                BpSlice m = p->h_bp[((size_t)b * nz + z) * C + c];
+                memset(m.prj_off, 0, sizeof(m.prj_off));
+                memset(m.prj_w, 0, sizeof(m.prj_w));
+                for (size_t k = 0; k < srows[z].size(); k++) {
+                    m.prj_off[k] = b * prj_b + (long long)srows[z][k] * C + c;
+                    m.prj_w[k] = 1.f;
+                }
+                p->h_bps.push_back(m);
+            }
     int s = finish_plan(p, host_deg, st);
     if (s != RN_OK) {
         std::string msg = rn_last_error();
@@ -342,6 +393,8 @@ int rn_fan_plan_create_ragged(rn_fan_plan** out, const RnFanGeom* g, const int* 
         b.table_off = (long long)voff * (nu + 2);
         p->h_bp.push_back(b);
         p->h_bpr.push_back(b);
+        p->h_fps.push_back(f);
+        p->h_bps.push_back(b);
         voff += nvs;
     }
     int st2 = finish_plan(p, host_deg, st);
@@ -362,10 +415,16 @@ int rn_fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, void* strea
     return rn::fan_project(p, d_prj, d_img, (cudaStream_t)stream);
 }
 
+int rn_fan_project_siddon(rn_fan_plan* p, float* d_prj, const float* d_img, void* stream) {
+    clear_error();
+    if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
+    return rn::fan_project(p, d_prj, d_img, (cudaStream_t)stream, true);
+}
+
 int rn_fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, void* stream) {
     clear_error();
     if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
-    if (type < 0 || type > 2) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1 or 2");
+    if (type < 0 || type > 3) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1, 2 or 3");
     return rn::fan_backproject(p, d_img, d_prj, type, accumulate ? 1 : 0, (cudaStream_t)stream);
 }
 

@@ -139,6 +139,13 @@ struct rn_fan_plan {
     rn::BpSlice* d_bp = nullptr;
     rn::BpSlice* d_bpr = nullptr;
     int4* d_fp_work = nullptr;      // {slice, class, vbegin, vcount}
+    // Siddon pair: FP slices (one image slice per detector row), BP slices
+    // (the detector rows of each image slice) and ray slopes at cell centres
+    std::vector<rn::FpSlice> h_fps;
+    std::vector<rn::BpSlice> h_bps;
+    rn::FpSlice* d_fps = nullptr;
+    rn::BpSlice* d_bps = nullptr;
+    double* d_cslopes = nullptr;    // [views][nu + 1], entry u = slope of the ray through cell u
     int* d_err = nullptr;           // device error word
 
     // scratch
@@ -194,6 +201,6 @@ struct LaunchScope {
     }
 };
 int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st);
-int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st);
+int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st, bool siddon = false);
 int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st);
 }  // namespace rn

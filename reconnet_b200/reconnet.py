@@ -152,6 +152,59 @@ class ReconNet:
         img = self.cDDFanBackprojection4d(sino[..., np.newaxis, :], angles, img_shape, type_projector)
         return img[..., 0, :]
 
+    # ---- Siddon fan pair (python/ReconNet_no_tf.py:290-394) ----
+    def cSiddonFanProjection4d(self, img, angles=None, sino_shape=None, type_projector=0):
+        img = np.ascontiguousarray(img, np.float32)
+        angles = self._angles(angles)
+        if sino_shape is None:
+            sino_shape = [self.nu, len(angles), self.nv]
+        sino = np.zeros([img.shape[0], sino_shape[0], sino_shape[1], sino_shape[2], img.shape[4]], np.float32)
+        N.lib.cSiddonFanProjection(_fptr(sino), _fptr(img), _fptr(angles),
+                                   *self._fan_args(img.shape, sino.shape, type_projector))
+        N.check_last()
+        return sino
+
+    def cSiddonFanProjection3d(self, img, angles=None, sino_shape=None, type_projector=0):
+        angles = self._angles(angles)
+        if sino_shape is None:
+            sino_shape = [self.nu, len(angles), 1]
+        sino = self.cSiddonFanProjection4d(img[..., np.newaxis, :], angles, sino_shape, type_projector)
+        return np.squeeze(sino, -2)
+
+    def cSiddonFanBackprojection4d(self, sino, angles=None, img_shape=None, type_projector=0):
+        sino = np.ascontiguousarray(sino, np.float32)
+        angles = self._angles(angles)
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, self.nz]
+        img = np.zeros([sino.shape[0], img_shape[0], img_shape[1], img_shape[2], sino.shape[4]], np.float32)
+        N.lib.cSiddonFanBackprojection(_fptr(img), _fptr(sino), _fptr(angles),
+                                       *self._fan_args(img.shape, sino.shape, type_projector))
+        N.check_last()
+        return img
+
+    def cSiddonFanBackprojection3d(self, sino, angles=None, img_shape=None, type_projector=0):
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, 1]
+        img = self.cSiddonFanBackprojection4d(sino[..., np.newaxis, :], angles, img_shape, type_projector)
+        return img[..., 0, :]
+
+    def cSiddonFanNormImg4d(self, sino, wsino=None, angles=None, img_shape=None, type_projector=0):
+        """normImg = BP(W * FP(1)) with the Siddon pair (ReconNet_no_tf.py:359-380)."""
+        angles = self._angles(angles)
+        wsino = np.ones(sino.shape, np.float32) if wsino is None else np.asarray(wsino, np.float32)
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, self.nz]
+        ones = np.ones([sino.shape[0], img_shape[0], img_shape[1], img_shape[2], sino.shape[4]], np.float32)
+        fp = self.cSiddonFanProjection4d(ones, angles, list(sino.shape[1:4]), type_projector)
+        return self.cSiddonFanBackprojection4d(fp * wsino, angles, img_shape, type_projector)
+
+    def cSiddonFanNormImg3d(self, sino, wsino=None, angles=None, img_shape=None, type_projector=0):
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, 1]
+        w = None if wsino is None else np.asarray(wsino)[..., np.newaxis, :]
+        norm = self.cSiddonFanNormImg4d(np.asarray(sino)[..., np.newaxis, :], w, angles, img_shape, type_projector)
+        return norm[..., 0, :]
+
     def cDDFanNormImg4d(self, sino, wsino=None, angles=None, img_shape=None, type_projector=0):
         """normImg = BP(W * FP(1)) (ReconNet_no_tf.py:202-223)."""
         angles = self._angles(angles)

@@ -130,12 +130,16 @@ class FanPlan:
             return int(self.total_views) * g.nx * g.ny
         return self.nbatches * self.nchannels * g.nz * self.nview * g.nx * g.ny
 
-    def project(self, img: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    def project(self, img: torch.Tensor, out: Optional[torch.Tensor] = None, siddon: bool = False) -> torch.Tensor:
+        """Distance-driven forward projection, or the Siddon ray-length
+        projection with ``siddon=True`` (its transpose: ``backproject(...,
+        N.RN_TYPE_SIDDON)``)."""
         if tuple(img.shape) != self.img_shape:
             raise ValueError(f"image shape {tuple(img.shape)} != {self.img_shape}")
         if out is None:
             out = torch.empty(self.sino_shape, dtype=torch.float32, device=img.device)
-        N.check(N.lib.rn_fan_project(self._plan, _dev_ptr(out), _dev_ptr(img), _stream_ptr(img.device)))
+        fn = N.lib.rn_fan_project_siddon if siddon else N.lib.rn_fan_project
+        N.check(fn(self._plan, _dev_ptr(out), _dev_ptr(img), _stream_ptr(img.device)))
         return out
 
     def backproject(self, sino: torch.Tensor, type_projector: int = N.RN_TYPE_MATCHED,

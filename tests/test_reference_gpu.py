@@ -93,3 +93,19 @@ def test_reference_host_call_timing(ref, rng):
     print(f"\nFP+BP host call, 512x512 736x720: reference {ts['reference']*1e3:.2f} ms, "
           f"b200 {ts['b200']*1e3:.2f} ms")
     assert ts["b200"] < ts["reference"]
+
+
+def test_siddon_vs_reference_kernels(ref, rng):
+    """The reference's Siddon kernels (incremental FP32 tracing, __sinf/__cosf
+    ray directions, float atomics in the backprojector) against the Siddon
+    pair here: measured ~4e-5 (FP) / ~1e-4 (BP) apart."""
+    from reconnet_b200.reconnet import ReconNet
+    lib = ref.load_ref()
+    if not hasattr(lib, "cSiddonFanProjection"):
+        pytest.skip("reference library built without Siddon.cu")
+    for name, out in ref.siddon_case(lib, rng).items():
+        rn = ReconNet()
+        for k in ("nx", "ny", "nz", "dx", "dy", "dz", "nu", "nv", "da", "dv", "off_a", "off_v", "dsd", "dso"):
+            setattr(rn, k, out[k].item() if k not in ("nx", "ny", "nz", "nu", "nv") else int(out[k]))
+        assert rel_l2(rn.cSiddonFanProjection4d(out["img"], out["angles"]), out["fp"]) <= 2e-4, name
+        assert rel_l2(rn.cSiddonFanBackprojection4d(out["sino_in"], out["angles"]), out["bp"]) <= 4e-4, name
