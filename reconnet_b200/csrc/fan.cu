@@ -581,8 +581,8 @@ __device__ __forceinline__ float ref_t(float px, float py, float c, float s, con
 }
 
 // Per-view parameters the BP inner loop reads, staged in shared memory.
-// Siddon BP table: per view, entry u + 1 holds the slope of ray u (a double
-// in x, y) and c_u = w_u * (ray length per band), w_u the sinogram value mixed
+// Siddon BP table: per view, entry u + 1 holds the slope of ray u as hi / lo
+// floats and c_u = w_u * (ray length per band), w_u the sinogram value mixed
 // over the slice's detector rows.
 __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin,
                                     int ns, const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
@@ -609,7 +609,8 @@ __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice
         }
         const double r = cslopes[(long long)gv * (nu + 1) + u];
         const float c = w * (float)sqrt(r * r * along * along + across * across);
-        out[u + 1] = make_float4(__int_as_float(__double2loint(r)), __int_as_float(__double2hiint(r)), c, 0.f);
+        const float rh = (float)r;
+        out[u + 1] = make_float4(rh, (float)(r - (double)rh), c, 0.f);
     }
     if (lane == 0) {
         out[0] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -738,43 +739,54 @@ __device__ __forceinline__ void bp_matched_y(float (&acc)[kBmRows], const BpView
 // c_u.  X-class: lane column q = x on lines y0 + j; Y-class: line l = x and
 // positions q = y0 + j; the corners on the neighbour column / line come from
 // the next lane.
-__device__ __forceinline__ float siddon_fraction(double r, double A, double D) {
-    // ray position relative to the pixel at line l (A = par - q, D = l - perp)
-    const float xa = (float)fma(r, D, A);
-    const float xb = xa + (float)r;
+// Contribution of one candidate ray: its position at line l relative to the
+// pixel, x = (par - q) + r (l - perp), from hi / lo parts (A = par - q and D =
+// l - perp as hi / lo floats, r from the table), to ~1e-7 cells.
+__device__ __forceinline__ float siddon_candidate(const float4 E, float Ah, float Al, float Dh, float Dl) {
+    const float xa = fmaf(E.x, Dh, Ah) + fmaf(E.y, Dh, fmaf(E.x, Dl, Al));
+    const float xb = xa + E.x;
     const float lo = fminf(xa, xb), hi = fmaxf(xa, xb);
     const float ov = fmaxf(0.f, fminf(hi, 1.f) - fmaxf(lo, 0.f));
     const float w = hi - lo;
-    return w > 1e-7f ? __fdividef(ov, w) : ((xa >= 0.f && xa < 1.f) ? 1.f : 0.f);
+    return E.z * (w > 1e-7f ? __fdividef(ov, w) : ((xa >= 0.f && xa < 1.f) ? 1.f : 0.f));
 }
 
+// Sum over the candidate rays of a pixel: the first two unrolled (most pixels
+// have at most two), the rest in a loop.
 __device__ __forceinline__ float siddon_pixel(const float4* T, int ilo, int imax, int nu, float t00, float t01,
-                                              float t10, float t11, double A, double D) {
+                                              float t10, float t11, float Ah, float Al, float Dh, float Dl) {
     const float tmin = fminf(fminf(t00, t01), fminf(t10, t11)), tmax = fmaxf(fmaxf(t00, t01), fmaxf(t10, t11));
     const int u0 = max(max((int)ceilf(tmin - 0.5f - 1e-3f), 0), ilo - 1);
     const int u1 = min(min((int)floorf(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
     float v = 0.f;
-    for (int u = u0; u <= u1; u++) {
-        const float4 E = T[u + 1 - ilo];
-        const double r = __hiloint2double(__float_as_int(E.y), __float_as_int(E.x));
-        v = fmaf(E.z, siddon_fraction(r, A, D), v);
-    }
+    if (u0 <= u1) v = siddon_candidate(T[u0 + 1 - ilo], Ah, Al, Dh, Dl);
+    if (u0 + 1 <= u1) v += siddon_candidate(T[u0 + 2 - ilo], Ah, Al, Dh, Dl);
+    for (int u = u0 + 2; u <= u1; u++) v += siddon_candidate(T[u + 1 - ilo], Ah, Al, Dh, Dl);
     return v;
+}
+
+__device__ __forceinline__ void split_hilo(double v, float& h, float& l) {
+    h = (float)v;
+    l = (float)(v - (double)h);
 }
 
 __device__ __forceinline__ void bp_siddon_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
                                             int imax, int x, int y0, int nu) {
     const float A = (float)x - vg.par;
     const TCubic c = t_cubic(vg, A * __fdividef(1.0f, (float)(y0 + kBmRows / 2) - vg.perp));
-    const double Ad = vg.pard - (double)x;
+    float Ah, Al;
+    split_hilo(vg.pard - (double)x, Ah, Al);
     float tp = 0.f, tnp = 0.f;
 #pragma unroll
     for (int j = 0; j <= kBmRows; j++) {
         const float h = A * __fdividef(1.0f, (float)(y0 + j) - vg.perp) - c.rt;
         const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
         const float tn = __shfl_down_sync(0xffffffffu, t, 1);
-        if (j > 0)
-            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ad, (double)(y0 + j - 1) - vg.perpd);
+        if (j > 0) {
+            float Dh, Dl;
+            split_hilo((double)(y0 + j - 1) - vg.perpd, Dh, Dl);
+            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al, Dh, Dl);
+        }
         tp = t;
         tnp = tn;
     }
@@ -785,15 +797,19 @@ __device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView&
     const float g = __fdividef(1.0f, (float)x - vg.perp);
     const float r0 = ((float)y0 - vg.par) * g;
     const TCubic c = t_cubic(vg, fmaf((float)(kBmRows / 2), g, r0));
-    const double D = (double)x - vg.perpd;
+    float Dh, Dl;
+    split_hilo((double)x - vg.perpd, Dh, Dl);
     float tp = 0.f, tnp = 0.f;
 #pragma unroll
     for (int j = 0; j <= kBmRows; j++) {
         const float h = fmaf((float)j, g, r0) - c.rt;
         const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
         const float tn = __shfl_down_sync(0xffffffffu, t, 1);
-        if (j > 0)
-            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, vg.pard - (double)(y0 + j - 1), D);
+        if (j > 0) {
+            float Ah, Al;
+            split_hilo(vg.pard - (double)(y0 + j - 1), Ah, Al);
+            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al, Dh, Dl);
+        }
         tp = t;
         tnp = tn;
     }
@@ -845,8 +861,10 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
 }
 
 // kMode: 0 reference-mode (typeProjector 0 / 1), 1 matched, 2 Siddon.
+// Siddon tiles run three CTAs per SM (80 registers, 180 vs 174 Gupd/s at two
+// CTAs); the DD modes keep the compiler's register choice (71 / 80).
 template <int kMode>
-__global__ void __launch_bounds__(kBpThreads) fan_bp_kernel(BpParams p) {
+__global__ void __launch_bounds__(kBpThreads, kMode == 2 ? 3 : 0) fan_bp_kernel(BpParams p) {
     constexpr bool kMatched = kMode != 0;   // column-warp tiles and the matched edge index
     extern __shared__ __align__(128) unsigned char smem[];
     BpShared* sh = reinterpret_cast<BpShared*>(smem);
