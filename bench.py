@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--slices", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ossqs", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the tomosynthesis and filter measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
     return ap.parse_args()
 
@@ -390,6 +390,52 @@ def tomo_run(dev, cpu_sample=True):
     return out
 
 
+def siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=True):
+    """Siddon fan pair (Siddon.cu, the reference OS-SQS projector) on the
+    bench's slice batch: FP of every view of every slice, then the Siddon
+    transpose BP.  Updates are counted as for DD: FP = views * nu * ny
+    ray-band integrals, BP = views * nx * ny pixel-view gathers; the byte
+    model is the same 8 B per update (two prefix samples per band)."""
+    import torch
+
+    from reconnet_b200 import _native as N
+    peak, kind = measured_peaks()
+    out = {"workload": "the fan batch above, Siddon ray-length pair (FP, then its exact transpose)",
+           "model": f"{BYTES_PER_UPDATE} B per update"}
+    for name, f, upd in (("fp", lambda: plan.project(x, out=p, siddon=True), plan.fp_updates()),
+                         ("bp", lambda: plan.backproject(p, N.RN_TYPE_SIDDON, out=b), plan.bp_updates())):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        ach = BYTES_PER_UPDATE * upd / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "updates": upd, "gupd_s": upd / ms / 1e6,
+                     "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                  "peak_kind": kind}}
+    plan.check()
+    if cpu_sample:
+        from oracle import oracle as O
+        O.set_threads(os.cpu_count() or 1)
+        nvw = 128
+        sel = np.ascontiguousarray(angles[:nvw])
+        img = x[0].cpu().numpy()[None, :, :, None, None]
+        t0 = time.perf_counter()
+        s = O.siddon_fp(img, sel, geom, geom.nu, 1)
+        t1 = time.perf_counter()
+        O.siddon_bp(s.astype(np.float32), sel, geom, (geom.nx, geom.ny, 1))
+        t2 = time.perf_counter()
+        out["cpu_baseline"] = {"fp_gupd_s": nvw * geom.nu * geom.ny / (t1 - t0) / 1e9,
+                               "bp_gupd_s": nvw * geom.nx * geom.ny / (t2 - t1) / 1e9,
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"{nvw} views of slice 0, FP64 OpenMP oracle (exact crossings)"}
+    return out
+
+
 def filter_run(dev, cpu_sample=True):
     """Ramp filter (Filter.cu): 64 fan sinograms of 888 channels x 1152 views,
     Ram-Lak window.  The filter is a linear convolution of every view with the
@@ -564,6 +610,7 @@ def run_b200(args):
     ossqs = None if args.no_ossqs else ossqs_run(plan, geom, counts, angles, x, args.ossqs_iters, dev)
     extras = {}
     if rank == 0 and not args.no_extras:
+        extras["siddon"] = siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=world == 1)
         extras["tomo"] = tomo_run(dev, cpu_sample=world == 1)
         extras["filter"] = filter_run(dev, cpu_sample=world == 1)
 

@@ -107,14 +107,23 @@ void cFilterParallelFilter(float* pFPrj, const float* pPrj, int nBatches, int nC
                            float da, float dv, float off_a, float off_v, float dsd, float dso, int typeFilter,
                            int typeProjector);
 
-/* replaces ReconNet4D/ossqs.cu:12-161.  Same arguments; the projector is the
- * DD fan pair (forward + the backprojector selected by typeProjector), and the
- * last subset holds views [startView, nview) instead of the reference's
- * nview - nviewPerSubset. */
+/* replaces ReconNet4D/ossqs.cu:12-161.  Same arguments and the same projector:
+ * the Siddon fan pair (cSiddonFanProjection and its transpose), typeProjector
+ * ignored as the reference's SiddonFan ignores it.  The last subset holds
+ * views [startView, nview) instead of the reference's nview - nviewPerSubset. */
 void cOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
             const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels,
             int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
             float off_a, float off_v, float dsd, float dso, int typeProjector, float lambda);
+
+/* cOSSQS with the DD fan pair: cDistanceDrivenFanProjection and the
+ * backprojector selected by typeProjector (0 / 1 reference modes, 2 matched
+ * transpose).  No reference counterpart. */
+void cDDFanOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
+                 const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches,
+                 int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
+                 float da, float dv, float off_a, float off_v, float dsd, float dso, int typeProjector,
+                 float lambda);
 
 /* replaces ReconNet4D/TotalVariation.cu:70-142; the TV value is summed in FP64 */
 float cTVSQS2D(float* grad, float* norm, const float* img, int nx, int ny);
@@ -200,7 +209,8 @@ int rn_tv_sqs(float* d_grad, float* d_norm, double* d_tv, const float* d_img, in
  *                  / (normImg + beta * norm_tv(x_in) + 1e-6), lb, ub)
  * `subset_plan` is a plan holding only the subset's views (same slice
  * layout); d_prj_s / d_w_s are the subset's measured and weight sinograms in
- * that plan's layout.  x_out must not alias x_in. */
+ * that plan's layout.  typeProjector 0 / 1 / 2 run the DD forward projector
+ * with that backprojector, 3 the Siddon pair.  x_out must not alias x_in. */
 int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x_in, const float* d_prj_s,
                       const float* d_w_s, const float* d_norm_img, float lambda, float beta, int nSubsets, float lb,
                       float ub, int typeProjector, void* stream);

@@ -217,21 +217,31 @@ def tomo_bp(prj, det_center, src, g, img_shape, weight_mode=0):
 # term from TotalVariation.cu, explicit subset view lists).
 # ---------------------------------------------------------------------------
 def sqs_subset_update(x, sino, wsino, norm_img, angles, views, g, n_subsets, lam=1.0, beta=0.0,
-                      lb=-np.inf, ub=np.inf, bp_type=2):
-    """One ordered-subset SQS step on a [nx, ny] slice (2D, B = C = 1).
+                      lb=-np.inf, ub=np.inf, bp_type=2, projector="dd"):
+    """One ordered-subset SQS step on a [nx, ny] slice (2D, B = C = 1),
+    ossqs.cu:91-149 with the TV terms of the TV-regularised variant.
 
     x_new = clamp(x - lam * (M * A_s^T W_s (A_s x - b_s) + beta * grad_tv(x))
                         / (norm_img + beta * norm_tv(x) + 1e-6), lb, ub)
-    ``sino``/``wsino`` are [nu, nview]; ``views`` lists the subset's view indices.
+    ``sino``/``wsino`` are [nu, nview]; ``views`` lists the subset's view
+    indices.  projector "dd": DD forward and the ``bp_type`` backprojector;
+    "siddon": the Siddon pair (the reference cOSSQS projector, ossqs.cu:81).
     """
     x = np.asarray(x, np.float32)
     nx, ny = x.shape
     nu = sino.shape[0]
     views = np.asarray(views)
     ang = np.asarray(angles, np.float32)[views]
-    fp = fan_fp(x[None, :, :, None, None], ang, g, nu, 1)[0, :, :, 0, 0]
+    if projector == "siddon":
+        fp = siddon_fp(x[None, :, :, None, None], ang, g, nu, 1)[0, :, :, 0, 0]
+    else:
+        fp = fan_fp(x[None, :, :, None, None], ang, g, nu, 1)[0, :, :, 0, 0]
     r = (fp - sino[:, views].astype(np.float64)) * wsino[:, views].astype(np.float64)
-    bp = fan_bp(r.astype(np.float32)[None, :, :, None, None], ang, g, (nx, ny, 1), bp_type)[0, :, :, 0, 0]
+    r = r.astype(np.float32)[None, :, :, None, None]
+    if projector == "siddon":
+        bp = siddon_bp(r, ang, g, (nx, ny, 1))[0, :, :, 0, 0]
+    else:
+        bp = fan_bp(r, ang, g, (nx, ny, 1), bp_type)[0, :, :, 0, 0]
     num = n_subsets * bp
     den = np.asarray(norm_img, np.float64) + 1e-6
     if beta > 0:

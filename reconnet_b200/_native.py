@@ -60,6 +60,7 @@ SIGNATURES = {
     "cFilterFanFilter": (None, [_fp, _fp] + _FILT),
     "cFilterParallelFilter": (None, [_fp, _fp] + _FILT),
     "cOSSQS": (None, [_fp, _fp, _fp, _fp, _fp, _fp, _f, _f, _i, _i] + _FAN[:-1] + [_i, _f]),
+    "cDDFanOSSQS": (None, [_fp, _fp, _fp, _fp, _fp, _fp, _f, _f, _i, _i] + _FAN[:-1] + [_i, _f]),
     "cTVSQS2D": (_f, [_fp, _fp, _fp, _i, _i]),
     "rn_fan_plan_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnFanGeom), _fp, _vp]),
     "rn_fan_plan_create_ragged": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnFanGeom),

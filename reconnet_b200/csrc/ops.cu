@@ -291,7 +291,7 @@ int sqs_update(rn_fan_plan* p, float* x_out, const float* x_in, const float* prj
     if (x_out == x_in) return set_error(RN_ERR_ARG, "sqs update: x_out must not alias x_in");
     if (!p->d_tmp_prj) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_prj, sizeof(float) * p->prj_elems));
     if (!p->d_tmp_img) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_img, sizeof(float) * p->img_elems));
-    RN_TRY(fan_project(p, p->d_tmp_prj, x_in, st));
+    RN_TRY(fan_project(p, p->d_tmp_prj, x_in, st, type == RN_TYPE_SIDDON));
     long long n = p->prj_elems;
     residual_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p->d_tmp_prj, prj_s,
                                                                                                w_s, n);
@@ -582,21 +582,26 @@ int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x
                       const float* d_w_s, const float* d_norm_img, float lambda, float beta, int nSubsets, float lb,
                       float ub, int typeProjector, void* stream) {
     clear_error();
-    if (typeProjector < 0 || typeProjector > 2) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1 or 2");
+    if (typeProjector < 0 || typeProjector > 3) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1, 2 or 3");
     return sqs_update(subset_plan, d_x_out, d_x_in, d_prj_s, d_w_s, d_norm_img, lambda, beta, nSubsets, lb, ub,
                       typeProjector, (cudaStream_t)stream);
 }
 
-void cOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
-            const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels,
-            int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
-            float off_a, float off_v, float dsd, float dso, int typeProjector, float lambda) {
+}  // extern "C"
+
+// Host OS-SQS loop shared by cOSSQS (Siddon pair) and cDDFanOSSQS (DD pair,
+// type = typeProjector): contiguous subsets of nviewPerSubset views, the
+// last one holding the remaining views.
+static void host_ossqs(const char* name, float* res, const float* img, const float* prj, const float* normImg,
+                       const float* wprj, const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets,
+                       int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, int nu,
+                       int nview, int nv, float da, float dv, float off_a, float off_v, float dsd, float dso,
+                       int typeProjector, float lambda) {
     clear_error();
     if (!res || !img || !prj || !normImg || !wprj || !degs || nviewPerSubset <= 0 || nSubsets <= 0) {
-        set_error(RN_ERR_ARG, "cOSSQS: bad argument");
+        set_error(RN_ERR_ARG, std::string(name) + ": bad argument");
         return;
     }
-    if (typeProjector < 0 || typeProjector > 2) typeProjector = 0;
     HostCtx* c = host_ctx();
     std::lock_guard<std::mutex> lk(c->mu);
     const size_t ni = (size_t)nBatches * nx * ny * nz * nChannels;
@@ -642,6 +647,30 @@ void cOSSQS(float* res, const float* img, const float* prj, const float* normImg
     }
     cudaMemcpyAsync(res, x0, ni * 4, cudaMemcpyDeviceToHost, c->st);
     finish_sync(c, nullptr);
+}
+
+extern "C" {
+
+// ossqs.cu:12-161: the reference runs its Siddon pair whatever typeProjector
+// says (SiddonFan ignores it).
+void cOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
+            const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels,
+            int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da, float dv,
+            float off_a, float off_v, float dsd, float dso, int typeProjector, float lambda) {
+    (void)typeProjector;
+    host_ossqs("cOSSQS", res, img, prj, normImg, wprj, degs, lb, ub, nviewPerSubset, nSubsets, nBatches, nChannels,
+               nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso, RN_TYPE_SIDDON, lambda);
+}
+
+void cDDFanOSSQS(float* res, const float* img, const float* prj, const float* normImg, const float* wprj,
+                 const float* degs, float lb, float ub, int nviewPerSubset, int nSubsets, int nBatches,
+                 int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
+                 float da, float dv, float off_a, float off_v, float dsd, float dso, int typeProjector,
+                 float lambda) {
+    if (typeProjector < 0 || typeProjector > 2) typeProjector = 0;
+    host_ossqs("cDDFanOSSQS", res, img, prj, normImg, wprj, degs, lb, ub, nviewPerSubset, nSubsets, nBatches,
+               nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso, typeProjector,
+               lambda);
 }
 
 }  // extern "C"

@@ -37,9 +37,14 @@ class BatchedOSSQS:
     def __init__(self, geom: FanGeometry, counts: Sequence[int], angles, sino: torch.Tensor,
                  weights: torch.Tensor, n_subsets: int, beta: float = 0.0, lam: float = 1.0,
                  lb: Optional[float] = 0.0, ub: Optional[float] = None, use_graph: bool = True,
-                 device=None):
+                 device=None, projector: str = "dd"):
         """counts[s] views per slice, angles concatenated per slice, sino /
-        weights packed per slice as [nu, counts[s]] blocks (flat CUDA tensors)."""
+        weights packed per slice as [nu, counts[s]] blocks (flat CUDA tensors).
+        projector "dd": DD forward + matched backprojection; "siddon": the
+        Siddon pair, the projector of the reference's cOSSQS (ossqs.cu:81)."""
+        if projector not in ("dd", "siddon"):
+            raise ValueError("projector must be 'dd' or 'siddon'")
+        self.type = N.RN_TYPE_SIDDON if projector == "siddon" else N.RN_TYPE_MATCHED
         self.geom = geom
         self.device = torch.device(device) if device is not None else sino.device
         self.counts = np.asarray(counts, np.int64)
@@ -69,9 +74,10 @@ class BatchedOSSQS:
             self.plans.append(plan)
             self.sub_b.append(sino.reshape(-1)[gidx].contiguous())
             self.sub_w.append(weights.reshape(-1)[gidx].contiguous())
-        # normImg = A^T W A 1 over all views (matched pair)
+        # normImg = A^T W A 1 over all views (the same pair)
         ones = torch.ones(self.full.img_shape, device=self.device)
-        self.norm_img = self.full.backproject(self.full.project(ones) * weights.reshape(-1), N.RN_TYPE_MATCHED)
+        a1 = self.full.project(ones, siddon=self.type == N.RN_TYPE_SIDDON)
+        self.norm_img = self.full.backproject(a1 * weights.reshape(-1), self.type)
         self.use_graph = use_graph
         self._graph = None
         self._xa = torch.zeros(self.full.img_shape, device=self.device)
@@ -82,7 +88,7 @@ class BatchedOSSQS:
         for m in range(self.M):
             self.plans[m].sqs_update(dst, src, self.sub_b[m], self.sub_w[m], self.norm_img, lam=self.lam,
                                      beta=self.beta, n_subsets=self.M, lb=self.lb, ub=self.ub,
-                                     type_projector=N.RN_TYPE_MATCHED)
+                                     type_projector=self.type)
             src, dst = dst, src
         if src is not self._xa:      # odd number of subsets: bring the result home
             self._xa.copy_(src)

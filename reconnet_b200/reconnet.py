@@ -223,10 +223,28 @@ class ReconNet:
                                  type_projector)
         return n[..., 0, :]
 
-    # ---- OS-SQS with the DD projector (ossqs.cu:12 semantics) ----
+    # ---- OS-SQS (ossqs.cu:12 semantics) ----
+    def cSiddonFanOSSQS4d(self, nSubsets, img, sino, normImg, wsino=None, angles=None, order=None, lb=None,
+                          ub=None, type_projector=0, lam=1):
+        """cOSSQS with the Siddon pair, as ReconNet_no_tf.py:396-440."""
+        return self._ossqs(N.lib.cOSSQS, nSubsets, img, sino, normImg, wsino, angles, order, lb, ub,
+                           type_projector, lam)
+
+    def cSiddonFanOSSQS3d(self, nSubsets, img, sino, normImg, wsino=None, angles=None, order=None, lb=None,
+                          ub=None, type_projector=0, lam=1):
+        wsino = np.ones(sino.shape, np.float32) if wsino is None else np.asarray(wsino, np.float32)
+        res = self.cSiddonFanOSSQS4d(nSubsets, img[..., np.newaxis, :], sino[..., np.newaxis, :],
+                                     normImg[..., np.newaxis, :], wsino[..., np.newaxis, :], angles, order, lb, ub,
+                                     type_projector, lam)
+        return res[..., 0, :]
+
     def cDDFanOSSQS4d(self, nSubsets, img, sino, normImg, wsino=None, angles=None, order=None, lb=None, ub=None,
                       type_projector=0, lam=1):
-        """Same arguments as cSiddonFanOSSQS4d (ReconNet_no_tf.py:396-440) with the DD pair."""
+        """Same arguments as cSiddonFanOSSQS4d with the DD pair (cDDFanOSSQS)."""
+        return self._ossqs(N.lib.cDDFanOSSQS, nSubsets, img, sino, normImg, wsino, angles, order, lb, ub,
+                           type_projector, lam)
+
+    def _ossqs(self, fn, nSubsets, img, sino, normImg, wsino, angles, order, lb, ub, type_projector, lam):
         img = np.ascontiguousarray(img, np.float32)
         sino = np.asarray(sino, np.float32)
         normImg = np.ascontiguousarray(normImg, np.float32)
@@ -243,10 +261,10 @@ class ReconNet:
         wsino = np.ascontiguousarray(wsino, np.float32)
         res = np.zeros(img.shape, np.float32)
         B, nx, ny, nz, C = img.shape
-        N.lib.cOSSQS(_fptr(res), _fptr(img), _fptr(sino), _fptr(normImg), _fptr(wsino), _fptr(angles),
-                     float(lb), float(ub), nviewPerSubset, int(nSubsets), B, C, nx, ny, nz, self.dx, self.dy,
-                     self.dz, sino.shape[1], sino.shape[2], sino.shape[3], self.da, self.dv, self.off_a, self.off_v,
-                     self.dsd, self.dso, int(type_projector), float(lam))
+        fn(_fptr(res), _fptr(img), _fptr(sino), _fptr(normImg), _fptr(wsino), _fptr(angles), float(lb), float(ub),
+           nviewPerSubset, int(nSubsets), B, C, nx, ny, nz, self.dx, self.dy, self.dz, sino.shape[1],
+           sino.shape[2], sino.shape[3], self.da, self.dv, self.off_a, self.off_v, self.dsd, self.dso,
+           int(type_projector), float(lam))
         N.check_last()
         return res
 

@@ -9,6 +9,7 @@ these files.
 
     python tests/golden/make_golden.py [outdir]
     python tests/golden/make_golden.py --siddon [outdir]   (the Siddon pair only)
+    python tests/golden/make_golden.py --ossqs [outdir]    (cOSSQS only)
 """
 import ctypes
 import math
@@ -42,6 +43,8 @@ def load_ref(path=REF):
     if hasattr(lib, "cSiddonFanProjection"):
         lib.cSiddonFanProjection.argtypes = fan
         lib.cSiddonFanBackprojection.argtypes = fan
+    if hasattr(lib, "cOSSQS"):
+        lib.cOSSQS.argtypes = [_fp] * 6 + [_f, _f, _i, _i] + fan[3:-1] + [_i, _f]
     return lib
 
 
@@ -141,12 +144,45 @@ def siddon_case(lib, rng):
     return out
 
 
+def ossqs_case(lib, rng):
+    """cOSSQS (ossqs.cu:12-161, the Siddon pair): a 2D slice, 60 views in 4
+    contiguous subsets of 15 (nview a multiple of nviewPerSubset, so the
+    reference's tail-subset rule does not come into play), weights in
+    [0.5, 1.5), a clamp to [0, 1], lambda 0.8, one pass."""
+    g = dict(SIDDON_CASES["siddon2d"][0])
+    nview, M = 60, 4
+    ang = (np.arange(nview) * 2 * np.pi / nview + 0.013).astype(np.float32)
+    truth = (rng.random((1, g["nx"], g["ny"], 1, 1)) * 0.02).astype(np.float32)
+    args = (1, 1, g["nx"], g["ny"], g["nz"], g["dx"], g["dy"], g["dz"], g["nu"], nview, g["nv"], g["da"], g["dv"],
+            g["off_a"], g["off_v"], g["dsd"], g["dso"])
+    sino = np.zeros((1, g["nu"], nview, 1, 1), np.float32)
+    lib.cSiddonFanProjection(p(sino), p(truth), p(ang), *args, 0)
+    w = (0.5 + rng.random(sino.shape)).astype(np.float32)
+    ones = np.ones(truth.shape, np.float32)
+    a1 = np.zeros(sino.shape, np.float32)
+    lib.cSiddonFanProjection(p(a1), p(ones), p(ang), *args, 0)
+    a1 = np.ascontiguousarray(a1 * w)
+    norm = np.zeros(truth.shape, np.float32)
+    lib.cSiddonFanBackprojection(p(norm), p(a1), p(ang), *args, 0)
+    x0 = (rng.random(truth.shape) * 0.02).astype(np.float32)
+    res = np.zeros(truth.shape, np.float32)
+    lib.cOSSQS(p(res), p(x0), p(sino), p(norm), p(w), p(ang), 0.0, 1.0, nview // M, M, *args, 0, 0.8)
+    return dict(x0=x0, sino=sino, w=w, norm=norm, angles=ang, res=res, n_subsets=M, lam=0.8, lb=0.0, ub=1.0,
+                **{k: np.float64(v) for k, v in g.items()})
+
+
 def main(outdir=HERE, only=None):
     if only == "siddon":
         lib = load_ref()
         for name, d in siddon_case(lib, np.random.default_rng(20241203)).items():
             np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
         print("siddon golden vectors written to", outdir)
+        return
+    if only == "ossqs":
+        lib = load_ref()
+        np.savez_compressed(os.path.join(outdir, "ref_ossqs_siddon.npz"),
+                            **ossqs_case(lib, np.random.default_rng(20241204)))
+        print("cOSSQS golden vectors written to", outdir)
         return
     lib = load_ref()
     rng = np.random.default_rng(20240601)
@@ -159,4 +195,5 @@ def main(outdir=HERE, only=None):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    main(args[0] if args else HERE, only="siddon" if "--siddon" in sys.argv else None)
+    only = "siddon" if "--siddon" in sys.argv else "ossqs" if "--ossqs" in sys.argv else None
+    main(args[0] if args else HERE, only=only)

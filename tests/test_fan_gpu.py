@@ -202,8 +202,9 @@ def test_tv_matches_oracle(rng):
     assert rel_l2(gh[0, :, :, 0], g2) <= TOL and abs(th - t2) / t2 <= TOL
 
 
-@pytest.mark.parametrize("beta,ptype", [(0.0, 2), (0.02, 2), (0.0, 0)])
+@pytest.mark.parametrize("beta,ptype", [(0.0, 2), (0.02, 2), (0.0, 0), (0.02, 3)])
 def test_sqs_update_matches_oracle(beta, ptype, rng):
+    """rn_fan_sqs_update: DD forward with backprojector 0 / 2, or the Siddon pair (3)."""
     import torch
     from oracle import oracle as O
     from reconnet_b200.torch_ops import FanPlan
@@ -215,10 +216,11 @@ def test_sqs_update_matches_oracle(beta, ptype, rng):
     sino = O.fan_fp(truth[None, :, :, None, None], ang, g, g.nu, 1)[0, :, :, 0, 0].astype(np.float32)
     w = (0.5 + rng.random(sino.shape)).astype(np.float32)
     norm = O.fan_bp((O.fan_fp(np.ones((1, g.nx, g.ny, 1, 1), np.float32), ang, g, g.nu, 1)[0, :, :, 0, 0] * w)
-                    .astype(np.float32)[None, :, :, None, None], ang, g, (g.nx, g.ny, 1), ptype)[0, :, :, 0, 0]
+                    .astype(np.float32)[None, :, :, None, None], ang, g, (g.nx, g.ny, 1), min(ptype, 2))[0, :, :, 0, 0]
     norm = norm.astype(np.float32)
     views = np.arange(1, nview, M)
-    ref = O.sqs_subset_update(x, sino, w, norm, ang, views, g, M, lam=0.9, beta=beta, lb=0.0, ub=1.0, bp_type=ptype)
+    ref = O.sqs_subset_update(x, sino, w, norm, ang, views, g, M, lam=0.9, beta=beta, lb=0.0, ub=1.0,
+                              bp_type=min(ptype, 2), projector="siddon" if ptype == 3 else "dd")
     sp = FanPlan(to_geometry(g), ang[views])
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
     xo = torch.empty((1, g.nx, g.ny, 1, 1), device="cuda")
@@ -228,8 +230,10 @@ def test_sqs_update_matches_oracle(beta, ptype, rng):
     assert rel_l2(xo.cpu().numpy()[0, :, :, 0, 0], ref) <= TOL
 
 
-def test_cossqs_host_matches_oracle_loop(rng):
-    """cOSSQS (ossqs.cu:12) with contiguous subsets and the corrected tail."""
+@pytest.mark.parametrize("projector", ["siddon", "dd"])
+def test_cossqs_host_matches_oracle_loop(projector, rng):
+    """cOSSQS (ossqs.cu:12: the Siddon pair) and cDDFanOSSQS (the DD pair,
+    matched backprojector) with contiguous subsets and the corrected tail."""
     from oracle import oracle as O
     from reconnet_b200.reconnet import ReconNet
     g = small_fan()
@@ -245,12 +249,14 @@ def test_cossqs_host_matches_oracle_loop(rng):
     ref = x.astype(np.float64)
     for k in range(M):
         views = np.arange(k * nps, min(nview, (k + 1) * nps))
-        ref = O.sqs_subset_update(ref.astype(np.float32), sino, w, norm, ang, views, g, M, bp_type=2)
+        ref = O.sqs_subset_update(ref.astype(np.float32), sino, w, norm, ang, views, g, M, bp_type=2,
+                                  projector=projector)
     rn = ReconNet()
     for k in ("nx", "ny", "nz", "dx", "dy", "dz", "nu", "nv", "da", "dv", "off_a", "off_v", "dsd", "dso"):
         setattr(rn, k, getattr(g, k))
-    got = rn.cDDFanOSSQS3d(M, x[None, :, :, None], sino[None, :, :, None], norm[None, :, :, None],
-                           w[None, :, :, None], ang, type_projector=2)[0, :, :, 0]
+    fn = rn.cSiddonFanOSSQS3d if projector == "siddon" else rn.cDDFanOSSQS3d
+    got = fn(M, x[None, :, :, None], sino[None, :, :, None], norm[None, :, :, None], w[None, :, :, None], ang,
+             type_projector=2)[0, :, :, 0]
     assert rel_l2(got, ref) <= 1e-4   # four chained steps
 
 

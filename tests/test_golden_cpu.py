@@ -113,3 +113,28 @@ def test_siddon_vs_reference(path):
     assert rel_l2(fp, d["fp"]) < 1e-4      # measured 3.9e-5 / 4.3e-5
     bp = O.siddon_bp(d["sino_in"], d["angles"], g, (n["nx"], n["ny"], n["nz"]))
     assert rel_l2(bp, d["bp"]) < 2e-4      # measured 6.6e-5 / 1.1e-4
+
+
+OSSQS = os.path.join(GOLDEN, "ref_ossqs_siddon.npz")
+
+
+def ossqs_oracle_loop(d, g):
+    """The oracle's OS-SQS pass with contiguous subsets and the Siddon pair,
+    on a cOSSQS golden case (tests/golden/make_golden.py ossqs_case)."""
+    M = int(d["n_subsets"])
+    nview = d["angles"].size
+    nps = nview // M
+    x = d["x0"][0, :, :, 0, 0]
+    sino, w, norm = d["sino"][0, :, :, 0, 0], d["w"][0, :, :, 0, 0], d["norm"][0, :, :, 0, 0]
+    for k in range(M):
+        x = O.sqs_subset_update(x.astype(np.float32), sino, w, norm, d["angles"], np.arange(k * nps, (k + 1) * nps),
+                                g, M, lam=float(d["lam"]), lb=float(d["lb"]), ub=float(d["ub"]), projector="siddon")
+    return x
+
+
+def test_ossqs_siddon_vs_reference():
+    """The oracle's OS-SQS loop against the reference's cOSSQS
+    (ossqs.cu:12-161: Siddon pair, Minus2D / Multiply2D / Divide2D /
+    ValueCrop2D) on the same inputs."""
+    d, g, _ = _fan(OSSQS)
+    assert rel_l2(ossqs_oracle_loop(d, g), d["res"][0, :, :, 0, 0]) < 1e-4   # measured 2.8e-5

@@ -39,26 +39,33 @@ def test_batched_ossqs_graph_matches_eager(rng):
     assert torch.equal(runs[0], runs[1])
 
 
-def test_batched_ossqs_iteration_matches_oracle(rng):
+@pytest.mark.parametrize("projector", ["dd", "siddon"])
+def test_batched_ossqs_iteration_matches_oracle(projector, rng):
     import torch
     from oracle import oracle as O
     from reconnet_b200.ossqs import BatchedOSSQS, interleaved_subsets
     g, angs, truth, b, w, sinos, ws = _ragged_problem(rng)
     counts = [a.size for a in angs]
     M, beta = 3, 0.02
-    os_ = BatchedOSSQS(to_geometry(g), counts, np.concatenate(angs), b, w, n_subsets=M, beta=beta, lb=0.0, ub=1.0)
+    os_ = BatchedOSSQS(to_geometry(g), counts, np.concatenate(angs), b, w, n_subsets=M, beta=beta, lb=0.0, ub=1.0,
+                       projector=projector)
     x0 = (rng.random((3, g.nx, g.ny)) * 0.01).astype(np.float32)
     got = os_.run(torch.from_numpy(x0).cuda(), 1).cpu().numpy()
     for s, n in enumerate(counts):
         sino = sinos[s].reshape(g.nu, n)
         wsn = ws[s].reshape(g.nu, n)
         ones = np.ones((1, g.nx, g.ny, 1, 1), np.float32)
-        norm = O.fan_bp((O.fan_fp(ones, angs[s], g, g.nu, 1)[0, :, :, 0, 0] * wsn).astype(np.float32)
-                        [None, :, :, None, None], angs[s], g, (g.nx, g.ny, 1), 2)[0, :, :, 0, 0].astype(np.float32)
+        if projector == "siddon":
+            a1 = (O.siddon_fp(ones, angs[s], g, g.nu, 1)[0, :, :, 0, 0] * wsn).astype(np.float32)
+            norm = O.siddon_bp(a1[None, :, :, None, None], angs[s], g, (g.nx, g.ny, 1))[0, :, :, 0, 0]
+        else:
+            a1 = (O.fan_fp(ones, angs[s], g, g.nu, 1)[0, :, :, 0, 0] * wsn).astype(np.float32)
+            norm = O.fan_bp(a1[None, :, :, None, None], angs[s], g, (g.nx, g.ny, 1), 2)[0, :, :, 0, 0]
+        norm = norm.astype(np.float32)
         x = x0[s]
         for views in interleaved_subsets(n, M):
             x = O.sqs_subset_update(x, sino, wsn, norm, angs[s], views, g, M, beta=beta, lb=0.0,
-                                    ub=1.0).astype(np.float32)
+                                    ub=1.0, projector=projector).astype(np.float32)
         assert rel_l2(got[s], x) <= 1e-4
 
 

@@ -109,3 +109,21 @@ def test_siddon_vs_reference_kernels(ref, rng):
             setattr(rn, k, out[k].item() if k not in ("nx", "ny", "nz", "nu", "nv") else int(out[k]))
         assert rel_l2(rn.cSiddonFanProjection4d(out["img"], out["angles"]), out["fp"]) <= 2e-4, name
         assert rel_l2(rn.cSiddonFanBackprojection4d(out["sino_in"], out["angles"]), out["bp"]) <= 4e-4, name
+
+
+def test_cossqs_vs_reference(ref, rng):
+    """cOSSQS here (Siddon pair, like ossqs.cu:81) against the reference's
+    cOSSQS on the same inputs, nview a multiple of nviewPerSubset."""
+    from reconnet_b200.reconnet import ReconNet
+    lib = ref.load_ref()
+    if not hasattr(lib, "cOSSQS"):
+        pytest.skip("reference library built without ossqs.cu")
+    d = ref.ossqs_case(lib, rng)
+    rn = ReconNet()
+    for k in ("nx", "ny", "nz", "dx", "dy", "dz", "nu", "nv", "da", "dv", "off_a", "off_v", "dsd", "dso"):
+        setattr(rn, k, d[k].item() if k not in ("nx", "ny", "nz", "nu", "nv") else int(d[k]))
+    got = rn.cSiddonFanOSSQS4d(int(d["n_subsets"]), d["x0"], d["sino"], d["norm"], d["w"], d["angles"],
+                               lb=float(d["lb"]), ub=float(d["ub"]), lam=float(d["lam"]))
+    err = rel_l2(got, d["res"])
+    print(f"cOSSQS vs reference: {err:.3g}")
+    assert err <= 1e-4   # measured 2.8e-5

@@ -98,3 +98,21 @@ def test_siddon_full_size_slice(rng):
     bp = plan.backproject(fp, N.RN_TYPE_SIDDON).cpu().numpy()
     assert rel_l2(bp, O.siddon_bp(fp.cpu().numpy(), ang, g, (g.nx, g.ny, 1))) <= TOL
     plan.check()
+
+
+def test_cossqs_matches_oracle_on_reference_case():
+    """cOSSQS on the committed cOSSQS golden case (inputs from the reference's
+    own Siddon kernels) against the oracle's OS-SQS loop with the Siddon pair."""
+    import os
+    from conftest import ROOT
+    from test_golden_cpu import _fan, ossqs_oracle_loop
+    from reconnet_b200.reconnet import ReconNet
+    d, g, n = _fan(os.path.join(ROOT, "tests", "golden", "ref_ossqs_siddon.npz"))
+    rn = ReconNet()
+    for k in ("dx", "dy", "dz", "da", "dv", "off_a", "off_v", "dsd", "dso"):
+        setattr(rn, k, getattr(g, k))
+    for k, v in n.items():
+        setattr(rn, k, v)
+    got = rn.cSiddonFanOSSQS4d(int(d["n_subsets"]), d["x0"], d["sino"], d["norm"], d["w"], d["angles"],
+                               lb=float(d["lb"]), ub=float(d["ub"]), lam=float(d["lam"]))
+    assert rel_l2(got[0, :, :, 0, 0], ossqs_oracle_loop(d, g)) <= 1e-4   # four chained steps
