@@ -49,6 +49,7 @@ extern "C" {
 #define RN_TYPE_FBP 1
 #define RN_TYPE_MATCHED 2
 #define RN_TYPE_SIDDON 3     /* Siddon ray lengths (rn_fan_project_siddon / rn_fan_backproject) */
+#define RN_TYPE_PIXEL 4      /* pixel-driven FBP backprojection (rn_fan_backproject) */
 
 const char* rn_last_error(void);
 int rn_last_status(void);
@@ -106,6 +107,16 @@ void cFilterFanFilter(float* pFPrj, const float* pPrj, int nBatches, int nChanne
 void cFilterParallelFilter(float* pFPrj, const float* pPrj, int nBatches, int nChannels, int nu, int nview, int nv,
                            float da, float dv, float off_a, float off_v, float dsd, float dso, int typeFilter,
                            int typeProjector);
+
+/* replaces ReconNet4D/PixelDriven.cu:100-141 (pixel-driven backprojection
+ * with the FBP weight dso^2 / L^2, bilinear in (u, v), zero beyond the
+ * detector).  Same signature; typeProjector is ignored as in the reference;
+ * img is overwritten.  Channels are read with their stride (the reference's
+ * texture copy is only right for nChannels = 1). */
+void cPixelDrivenFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels,
+                                   int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
+                                   float da, float dv, float off_a, float off_v, float dsd, float dso,
+                                   int typeProjector);
 
 /* replaces ReconNet4D/ossqs.cu:12-161.  Same arguments and the same projector:
  * the Siddon fan pair (cSiddonFanProjection and its transpose), typeProjector
@@ -176,8 +187,9 @@ int rn_fan_project_siddon(rn_fan_plan* plan, float* d_prj, const float* d_img, v
 
 /* Backprojection; typeProjector as above (RN_TYPE_SIDDON: the exact transpose
  * of rn_fan_project_siddon, gathered per voxel; the reference scatters with
- * atomics, Siddon.cu:268-380).  accumulate = 0 overwrites img, 1 adds to it
- * (the reference class-level Backprojection accumulates). */
+ * atomics, Siddon.cu:268-380; RN_TYPE_PIXEL: the pixel-driven FBP
+ * backprojection of PixelDriven.cu:11-62).  accumulate = 0 overwrites img, 1
+ * adds to it (the reference class-level Backprojection accumulates). */
 int rn_fan_backproject(rn_fan_plan* plan, float* d_img, const float* d_prj, int typeProjector, int accumulate,
                        void* stream);
 

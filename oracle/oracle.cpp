@@ -638,6 +638,57 @@ void siddon_bp(T* img, const float* prj, const float* deg, const Fan& g) {
 }
 
 // --------------------------------------------------------------------------
+// Pixel-driven fan backprojection with the FBP weight: bpFanKernel3D as
+// cPixelDrivenFan::Backprojection launches it (PixelDriven.cu:11-97, isFBP =
+// true).  Pixel centre (x, y) = ((ix - (nx-1)/2) dx, (iy - (ny-1)/2) dy),
+// rotated into the view frame (source at (0, -dso)); the ray angle a =
+// atan(rx / (ry + dso)) gives the detector coordinate pu = -(a/da + off_a) +
+// (nu-1)/2, and slice iz the row coordinate pv = (iz - (nz-1)/2) dz/dv +
+// off_v + (nv-1)/2.  The sample is the bilinear interpolation of the view's
+// (u, v) plane at (pu, pv) with zeros outside (border addressing, texel
+// centres at integers), weighted dso^2 / (rx^2 + (dso + ry)^2).  The output is
+// overwritten.  Channel c reads channel c (the reference's texture copy reads
+// nv contiguous floats from the channel's offset, which is the channel's data
+// only for nChannels = 1).
+// --------------------------------------------------------------------------
+template <typename T>
+void pixel_bp(T* img, const float* prj, const float* deg, const Fan& g) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int b = 0; b < g.nb; b++)
+        for (int ix = 0; ix < g.nx; ix++)
+            for (int iy = 0; iy < g.ny; iy++)
+                for (int iz = 0; iz < g.nz; iz++)
+                    for (int c = 0; c < g.nc; c++) {
+                        const double x = (ix - (g.nx - 1) / 2.0) * g.dx, y = (iy - (g.ny - 1) / 2.0) * g.dy;
+                        const double pv = (iz - (g.nz - 1) / 2.0) * g.dz / g.dv + g.off_v + (g.nv - 1) / 2.0;
+                        int v0;
+                        double wv;
+                        tex_split(pv + 0.5, v0, wv);
+                        double val = 0;
+                        for (int iview = 0; iview < g.nview; iview++) {
+                            const double cs = std::cos((double)deg[iview]), sn = std::sin((double)deg[iview]);
+                            const double rx = x * cs + y * sn, ry = -x * sn + y * cs;
+                            const double a = std::atan(rx / (ry + g.dso));
+                            const double dist = g.dso * g.dso / (rx * rx + (g.dso + ry) * (g.dso + ry));
+                            const double pu = -(a / g.du + g.off_u) + (g.nu - 1) / 2.0;
+                            int u0;
+                            double wu;
+                            tex_split(pu + 0.5, u0, wu);
+                            double s = 0;
+                            for (int du = 0; du < 2; du++)
+                                for (int dv = 0; dv < 2; dv++) {
+                                    const int iu = u0 + du, iv = v0 + dv;
+                                    if (iu < 0 || iu >= g.nu || iv < 0 || iv >= g.nv) continue;
+                                    s += (du ? wu : 1 - wu) * (dv ? wv : 1 - wv) *
+                                         prj[prj_index(g, b, iu, iview, iv, c)];
+                                }
+                            val += s * dist;
+                        }
+                        img[img_index(g, b, ix, iy, iz, c)] = (T)val;
+                    }
+}
+
+// --------------------------------------------------------------------------
 // Tomosynthesis DD: DistanceDrivenTomo::ProjectionTomo / BackprojectionTomo
 // (DistanceDriven3D.cu:37-343, :409-663).  detU = (1,0,0), detV = (0,1,0).
 // --------------------------------------------------------------------------
@@ -858,6 +909,12 @@ void oracle_siddon_fp_f64(double* prj, const float* img, const float* deg, FAN_A
 }
 void oracle_siddon_bp_f64(double* img, const float* prj, const float* deg, FAN_ARGS) {
     siddon_bp<double>(img, prj, deg, make_fan(FAN_PASS));
+}
+void oracle_pixel_bp_f64(double* img, const float* prj, const float* deg, FAN_ARGS) {
+    pixel_bp<double>(img, prj, deg, make_fan(FAN_PASS));
+}
+void oracle_pixel_bp_f32(float* img, const float* prj, const float* deg, FAN_ARGS) {
+    pixel_bp<float>(img, prj, deg, make_fan(FAN_PASS));
 }
 
 void oracle_ramp_kernel(double* h, int nu, float da, int typeFilter, int equispace) {

@@ -53,6 +53,8 @@ def lib():
         L.oracle_fan_bp_f64.argtypes = [_dp, _fp, _fp] + _FAN + [_i]
         L.oracle_siddon_fp_f64.argtypes = [_dp, _fp, _fp] + _FAN
         L.oracle_siddon_bp_f64.argtypes = [_dp, _fp, _fp] + _FAN
+        L.oracle_pixel_bp_f64.argtypes = [_dp, _fp, _fp] + _FAN
+        L.oracle_pixel_bp_f32.argtypes = [_fp, _fp, _fp] + _FAN
         L.oracle_fan_bp_f32.argtypes = [_fp, _fp, _fp] + _FAN + [_i]
         L.oracle_ramp_kernel.argtypes = [_dp, _i, _f, _i, _i]
         L.oracle_filter_f64.argtypes = [_dp, _fp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i]
@@ -155,6 +157,22 @@ def siddon_bp(sino, angles, g, img_shape):
     out = np.zeros((B, nx, ny, nz, C), np.float64)
     lib().oracle_siddon_bp_f64(_ptr(out, ctypes.c_double), _ptr(sino, _f), _ptr(ang, _f),
                                *_fan_args(g, out.shape, sino.shape))
+    return out
+
+
+def pixel_bp(sino, angles, g, img_shape, dtype=np.float64):
+    """Pixel-driven fan backprojection with the FBP weight
+    (PixelDriven.cu:11-97); the output is overwritten."""
+    sino = _f32(sino)
+    ang = _f32(angles)
+    B, nu, nview, nv, C = sino.shape
+    nx, ny, nz = img_shape
+    out = np.zeros((B, nx, ny, nz, C), dtype=dtype)
+    args = _fan_args(g, out.shape, sino.shape)
+    if dtype == np.float64:
+        lib().oracle_pixel_bp_f64(_ptr(out, ctypes.c_double), _ptr(sino, _f), _ptr(ang, _f), *args)
+    else:
+        lib().oracle_pixel_bp_f32(_ptr(out, _f), _ptr(sino, _f), _ptr(ang, _f), *args)
     return out
 
 

@@ -20,6 +20,7 @@ RN_TYPE_ITERATIVE = 0
 RN_TYPE_FBP = 1
 RN_TYPE_MATCHED = 2
 RN_TYPE_SIDDON = 3
+RN_TYPE_PIXEL = 4
 
 _f = ctypes.c_float
 _i = ctypes.c_int
@@ -55,6 +56,7 @@ SIGNATURES = {
     "cDistanceDrivenFanBackprojection": (None, [_fp, _fp, _fp] + _FAN),
     "cSiddonFanProjection": (None, [_fp, _fp, _fp] + _FAN),
     "cSiddonFanBackprojection": (None, [_fp, _fp, _fp] + _FAN),
+    "cPixelDrivenFanBackprojection": (None, [_fp, _fp, _fp] + _FAN),
     "cDistanceDrivenTomoProjection": (None, [_fp, _fp, _fp, _fp] + _TOMO),
     "cDistanceDrivenTomoBackprojection": (None, [_fp, _fp, _fp, _fp] + _TOMO),
     "cFilterFanFilter": (None, [_fp, _fp] + _FILT),

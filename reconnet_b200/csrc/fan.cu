@@ -618,6 +618,56 @@ __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice
     }
 }
 
+// Pixel-driven BP table: per view, entry k = u + 1 (u = -1 .. nu) holds the
+// slope r_u of the ray through the centre of cell u as hi / lo floats, dso^2
+// P_u and dso^2 (P_{u+1} - P_u), P_u the sinogram value mixed over the slice's
+// detector rows (P_{-1} = P_{nu} = 0: border addressing).  r_u for u = 0 .. nu
+// comes from the cell-centre slope table; r_{-1} is r_0 turned by one cell
+// pitch: with rho = kappa r = tan(psi), psi moving by +du (X class) or -du
+// (Y class) per cell towards negative u.
+__global__ void pd_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin, int ns,
+                                const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
+                                const double* __restrict__ cslopes, FanDims d, float4* __restrict__ tab,
+                                long long tab_base) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int si = blockIdx.y;
+    if (si >= ns) return;
+    const BpSlice bs = bps[s_begin + si];
+    const GeoSet gs = sets[bs.set];
+    const int vl = blockIdx.x * 8 + warp;
+    if (vl >= gs.nview) return;
+    const int gv = gs.view_off + vl;
+    const int nu = d.nu;
+    const int xcls = views[gv].xcls;
+    const double dso2 = (double)d.dso * d.dso;
+    float4* out = tab + (bs.table_off - tab_base) + (long long)vl * (nu + 2);
+    auto value = [&](int u) -> float {
+        if (u < 0 || u >= nu) return 0.f;
+        float w = 0.f;
+#pragma unroll
+        for (int k = 0; k < kBpMix; k++) {
+            const float wk = bs.prj_w[k];
+            if (wk == 0.f) continue;
+            w += wk * __ldg(prj + bs.prj_off[k] + (long long)u * bs.su + (long long)vl * bs.sview);
+        }
+        return w;
+    };
+    for (int k = lane; k < nu + 2; k += 32) {
+        const int u = k - 1;
+        double r;
+        if (u >= 0) {
+            r = cslopes[(long long)gv * (nu + 1) + u];
+        } else {
+            const double kap = xcls ? (double)d.dx / d.dy : (double)d.dy / d.dx;
+            const double rho = kap * cslopes[(long long)gv * (nu + 1)], tn = tan((double)d.du);
+            r = (xcls ? (rho + tn) / (1.0 - rho * tn) : (rho - tn) / (1.0 + rho * tn)) / kap;
+        }
+        const float p0 = value(u), p1 = value(u + 1);
+        const float rh = (float)r;
+        out[k] = make_float4(rh, (float)(r - (double)rh), (float)(dso2 * p0), (float)(dso2 * ((double)p1 - p0)));
+    }
+}
+
 struct BpView {
     double pard, perpd;   // source coordinates (Siddon band positions)
     float par, perp, kappa, tA, tB, sigma, cosd, sind;
@@ -815,6 +865,82 @@ __device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView&
     }
 }
 
+// Pixel-driven backprojection (kMode 3; bpFanKernel3D with the FBP weight,
+// PixelDriven.cu:11-62): pixel (x, y) receives, per view, the sinogram value
+// at the detector coordinate pu of the ray through its centre, interpolated
+// linearly between cell centres (zero beyond the detector), times dso^2 / L^2,
+// L the source-to-centre distance.  The edge-index cubic picks a cell u0 near
+// pu; the rest is exact: with A = par - q_c and D = l_c - perp the centre's
+// offsets from the source along / across the lines, x_u = A + r_u D is the
+// offset of ray u0 from the centre along its line, r - r_u = -x_u / D, and
+//   pu - u0 = tB atan(kappa (r - r_u) / (1 + kappa^2 r r_u))
+//           = -tB dq dl x_u D / L^2 (1 + dq^2 A x_u / L^2)
+// to second order in (r - r_u) (dq, dl the pixel pitches along / across the
+// lines; L^2 = (A dq)^2 + (D dl)^2).  A, D and x_u are carried as hi / lo
+// floats, so pu is good to ~1e-6 cells.  A pixel whose cell estimate is a
+// hair off lands at a fraction just outside [0, 1] of the neighbouring
+// interval, which is its exact linear extension.
+__device__ __forceinline__ float pd_sample(const float4* T, int ilo, int imax, float t, float Ah, float Al, float Dh,
+                                           float Dl, float cfrac, float dq, float dl) {
+    // table index floor(pu) + 1 = floor(t - 1/2) + 1 (round-down add, |t| < 2^22)
+    int k = __float_as_int(__fadd_rd(t - 0.5f, 12582912.0f)) - (0x4B400000 - 1);
+    k = min(max(k, ilo), imax);
+    const float4 E = T[k - ilo];
+    const float xu = fmaf(E.x, Dh, Ah) + fmaf(E.y, Dh, fmaf(E.x, Dl, Al));
+    const float a = Ah * dq, b = Dh * dl;
+    const float il2 = __fdividef(1.0f, fmaf(a, a, b * b));
+    const float xl = xu * il2;
+    const float frac = cfrac * Dh * xl * fmaf(dq * a, xl, 1.0f);
+    const float val = (k == 0 && frac < 0.f) ? 0.f : fmaf(frac, E.w, E.z);
+    return val * il2;
+}
+
+// s + e = a + b exactly (TwoSum).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// X-class view: lane column q = x, pixel rows y0 + j (centres l = y0 + j + 1/2).
+__device__ __forceinline__ void bp_pixel_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                           int imax, int x, int y0, float dq, float dl) {
+    const float A = (float)x + 0.5f - vg.par;
+    const TCubic c = t_cubic(vg, A * __fdividef(1.0f, (float)(y0 + kBmRows / 2) - vg.perp));
+    float Ah, Al, Dh0, Dl0;
+    split_hilo(vg.pard - ((double)x + 0.5), Ah, Al);
+    split_hilo(((double)y0 + 0.5) - vg.perpd, Dh0, Dl0);
+    const float cfrac = -vg.tB * dq * dl;
+#pragma unroll
+    for (int j = 0; j < kBmRows; j++) {
+        const float h = A * __fdividef(1.0f, (float)(y0 + j) + 0.5f - vg.perp) - c.rt;
+        const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+        float Dh, e;
+        two_sum(Dh0, (float)j, Dh, e);
+        acc[j] += pd_sample(T, ilo, imax, t, Ah, Al, Dh, Dl0 + e, cfrac, dq, dl);
+    }
+}
+
+// Y-class view: lane line l = x (centre x + 1/2), positions q = y0 + j + 1/2.
+__device__ __forceinline__ void bp_pixel_y(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                           int imax, int x, int y0, float dq, float dl) {
+    const float g = __fdividef(1.0f, (float)x + 0.5f - vg.perp);
+    const float r0 = ((float)y0 + 0.5f - vg.par) * g;
+    const TCubic c = t_cubic(vg, fmaf((float)(kBmRows / 2) - 0.5f, g, r0));
+    float Ah0, Al0, Dh, Dl;
+    split_hilo(vg.pard - ((double)y0 + 0.5), Ah0, Al0);
+    split_hilo(((double)x + 0.5) - vg.perpd, Dh, Dl);
+    const float cfrac = -vg.tB * dq * dl;
+#pragma unroll
+    for (int j = 0; j < kBmRows; j++) {
+        const float h = fmaf((float)j, g, r0) - c.rt;
+        const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+        float Ah, e;
+        two_sum(Ah0, -(float)j, Ah, e);
+        acc[j] += pd_sample(T, ilo, imax, t, Ah, Al0 + e, Dh, Dl, cfrac, dq, dl);
+    }
+}
+
 // Warp 0 of a backprojection CTA prepares chunk c (views c*kBpViews ...) of
 // its tile at (X0, Y0): lane = view * 4 + tile corner evaluates the edge index
 // at its corner, a 4-lane min gives the first staged table entry, and the
@@ -860,7 +986,7 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
     }
 }
 
-// kMode: 0 reference-mode (typeProjector 0 / 1), 1 matched, 2 Siddon.
+// kMode: 0 reference-mode (typeProjector 0 / 1), 1 matched, 2 Siddon, 3 pixel-driven.
 // Siddon tiles run three CTAs per SM (80 registers, 180 vs 174 Gupd/s at two
 // CTAs); the DD modes keep the compiler's register choice (71 / 80).
 template <int kMode>
@@ -955,7 +1081,10 @@ __global__ void __launch_bounds__(kBpThreads, kMode == 2 ? 3 : 0) fan_bp_kernel(
             const int ilo = sh->elo[slot][v];
             const int cnt = min(p.win, tabn);
             const int imax = ilo + cnt - 1;   // <= nu + 1
-            if (kMode == 2) {
+            if (kMode == 3) {
+                if (vg.xcls) bp_pixel_x(acc, vg, T, ilo, imax, x0, y0, p.d.dx, p.d.dy);
+                else bp_pixel_y(acc, vg, T, ilo, imax, x0, y0, p.d.dy, p.d.dx);
+            } else if (kMode == 2) {
                 if (vg.xcls) bp_siddon_x(acc, vg, T, ilo, imax, x0, y0, nu);
                 else bp_siddon_y(acc, vg, T, ilo, imax, x0, y0, nu);
             } else if (kMode == 1) {
@@ -1081,6 +1210,7 @@ int fan_kernel_attributes() {
     RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
     RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
     RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
+    RN_CUDA_TRY(cudaFuncSetAttribute(fan_bp_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget));
     g_attr_done[dev] = 1;
     return RN_OK;
 }
@@ -1279,11 +1409,13 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
 
 int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st) {
     const FanDims& d = p->dims;
-    const bool siddon = type == RN_TYPE_SIDDON;
+    const bool siddon = type == RN_TYPE_SIDDON, pixel = type == RN_TYPE_PIXEL;
+    // slices: Siddon rows per image slice; matched: the transpose of the FP z
+    // mixing; reference modes and pixel-driven: rows mixed at the slice's v
     const std::vector<BpSlice>& bps = siddon ? p->h_bps : (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
     const BpSlice* dbp = siddon ? p->d_bps : (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
     const int nbp = (int)bps.size();
-    const bool matched = type == RN_TYPE_MATCHED || siddon;   // column-warp tiles
+    const bool matched = type == RN_TYPE_MATCHED || siddon || pixel;   // column-warp tiles
     const int win = matched ? p->table_win_m : p->table_win;
     const size_t smem = bp_smem_bytes(win);
     const int tw = matched ? kBmCols : kBpTile, th = matched ? kBmTileY : kBpTile;
@@ -1308,6 +1440,9 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
             if (siddon)
                 siddon_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_cslopes, d,
                                                         p->d_tab, base);
+            else if (pixel)
+                pd_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_cslopes, d,
+                                                    p->d_tab, base);
             else
                 fan_table_kernel<<<tg, 256, 0, st>>>(d_prj, dbp, s0, ns, p->d_sets, p->d_views, p->d_edges, p->d_cell,
                                                      d, type, p->d_tab, base);
@@ -1330,7 +1465,8 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         bp.win = win;
         unsigned grid = (unsigned)(ns * tiles_x * tiles_y);
         LaunchScope ls3(p, st, 3);
-        if (siddon) fan_bp_kernel<2><<<grid, kBpThreads, smem, st>>>(bp);
+        if (pixel) fan_bp_kernel<3><<<grid, kBpThreads, smem, st>>>(bp);
+        else if (siddon) fan_bp_kernel<2><<<grid, kBpThreads, smem, st>>>(bp);
         else if (type == RN_TYPE_MATCHED) fan_bp_kernel<1><<<grid, kBpThreads, smem, st>>>(bp);
         else fan_bp_kernel<0><<<grid, kBpThreads, smem, st>>>(bp);
         RN_CUDA_TRY(cudaGetLastError());

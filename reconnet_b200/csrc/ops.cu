@@ -410,7 +410,6 @@ static int host_fan_fp(float* prj, const float* img, const float* deg, const RnF
 }
 
 static int host_fan_bp(float* img, const float* prj, const float* deg, const RnFanGeom& g, int type) {
-    if (type < 0 || type > 3) type = 0;   // the reference treats any non-1 type as iterative
     HostCtx* c = host_ctx();
     std::lock_guard<std::mutex> lk(c->mu);
     RN_TRY(ctx_plan(c, g, deg, g.nview));
@@ -472,11 +471,29 @@ void cSiddonFanBackprojection(float* img, const float* prj, const float* deg, in
                 RN_TYPE_SIDDON);
 }
 
+// PixelDriven.cu:73-141: pixel-driven FBP backprojection (typeProjector is
+// ignored there: cPixelDrivenFan always runs the FBP weight); the output is
+// overwritten.
+void cPixelDrivenFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels, int nx,
+                                   int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv, float da,
+                                   float dv, float off_a, float off_v, float dsd, float dso, int typeProjector) {
+    (void)typeProjector;
+    clear_error();
+    if (!prj || !img || !deg) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    host_fan_bp(img, prj, deg,
+                fan_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, nu, nview, nv, da, dv, off_a, off_v, dsd, dso),
+                RN_TYPE_PIXEL);
+}
+
 void cDistanceDrivenFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, int nChannels,
                                       int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
                                       float da, float dv, float off_a, float off_v, float dsd, float dso,
                                       int typeProjector) {
     clear_error();
+    if (typeProjector < 0 || typeProjector > 3) typeProjector = 0;   // the reference treats any non-1 type as iterative
     if (!prj || !img || !deg) {
         set_error(RN_ERR_ARG, "null argument");
         return;

@@ -424,7 +424,7 @@ int rn_fan_project_siddon(rn_fan_plan* p, float* d_prj, const float* d_img, void
 int rn_fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, void* stream) {
     clear_error();
     if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
-    if (type < 0 || type > 3) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1, 2 or 3");
+    if (type < 0 || type > 4) return set_error(RN_ERR_ARG, "typeProjector must be 0, 1, 2, 3 or 4");
     return rn::fan_backproject(p, d_img, d_prj, type, accumulate ? 1 : 0, (cudaStream_t)stream);
 }
 

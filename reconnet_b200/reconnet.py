@@ -152,6 +152,24 @@ class ReconNet:
         img = self.cDDFanBackprojection4d(sino[..., np.newaxis, :], angles, img_shape, type_projector)
         return img[..., 0, :]
 
+    # ---- pixel-driven FBP backprojection (python/ReconNet_no_tf.py:101-131) ----
+    def cPixelBackprojection4d(self, sino, angles=None, img_shape=None, type_projector=0):
+        sino = np.ascontiguousarray(sino, np.float32)
+        angles = self._angles(angles)
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, self.nz]
+        img = np.zeros([sino.shape[0], img_shape[0], img_shape[1], img_shape[2], sino.shape[4]], np.float32)
+        N.lib.cPixelDrivenFanBackprojection(_fptr(img), _fptr(sino), _fptr(angles),
+                                            *self._fan_args(img.shape, sino.shape, type_projector))
+        N.check_last()
+        return img
+
+    def cPixelBackprojection3d(self, sino, angles=None, img_shape=None, type_projector=0):
+        if img_shape is None:
+            img_shape = [self.nx, self.ny, 1]
+        img = self.cPixelBackprojection4d(sino[..., np.newaxis, :], angles, img_shape, type_projector)
+        return img[..., 0, :]
+
     # ---- Siddon fan pair (python/ReconNet_no_tf.py:290-394) ----
     def cSiddonFanProjection4d(self, img, angles=None, sino_shape=None, type_projector=0):
         img = np.ascontiguousarray(img, np.float32)

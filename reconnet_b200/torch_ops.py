@@ -314,6 +314,18 @@ def filter_sino(sino: torch.Tensor, geom: FanGeometry, type_filter: int = 0, fan
     return out
 
 
+def fbp(sino: torch.Tensor, plan: "FanPlan", geom: FanGeometry, type_filter: int = 0,
+        weights: Optional[torch.Tensor] = None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Fan-beam FBP on the device: optional short-scan weights (Parker /
+    Riess, multiplied into the sinogram), the ramp filter (cFilterFan), then
+    the pixel-driven backprojection with the dso^2 / L^2 weight
+    (cPixelDrivenFan) -- the reference's FBP chain (ReconNet_no_tf.py:84-131,
+    640-693).  sino is [B, nu, nview, nv, C] in the plan's layout."""
+    if weights is not None:
+        sino = sino * weights
+    return plan.backproject(filter_sino(sino, geom, type_filter), N.RN_TYPE_PIXEL, out=out)
+
+
 def tv_sqs(img: torch.Tensor, want_tv: bool = True):
     """TV surrogate terms of a [S, nx, ny] CUDA tensor -> (grad, norm, tv[S] float64)."""
     S, nx, ny = img.shape

@@ -10,6 +10,7 @@ these files.
     python tests/golden/make_golden.py [outdir]
     python tests/golden/make_golden.py --siddon [outdir]   (the Siddon pair only)
     python tests/golden/make_golden.py --ossqs [outdir]    (cOSSQS only)
+    python tests/golden/make_golden.py --pixel [outdir]    (pixel-driven backprojection only)
 """
 import ctypes
 import math
@@ -43,6 +44,8 @@ def load_ref(path=REF):
     if hasattr(lib, "cSiddonFanProjection"):
         lib.cSiddonFanProjection.argtypes = fan
         lib.cSiddonFanBackprojection.argtypes = fan
+    if hasattr(lib, "cPixelDrivenFanBackprojection"):
+        lib.cPixelDrivenFanBackprojection.argtypes = fan
     if hasattr(lib, "cOSSQS"):
         lib.cOSSQS.argtypes = [_fp] * 6 + [_f, _f, _i, _i] + fan[3:-1] + [_i, _f]
     return lib
@@ -144,6 +147,29 @@ def siddon_case(lib, rng):
     return out
 
 
+PIXEL_CASES = {
+    "pixel2d": (dict(nx=48, ny=40, nz=1, dx=1.0, dy=1.1, dz=1.0, nu=64, nv=1, da=0.0025, dv=1.0, off_a=0.3,
+                     off_v=0.0, dsd=1085.6, dso=595.0), 2, 72),
+    # slices between detector rows (v interpolation) and rows beyond the volume
+    "pixel_multislice": (dict(nx=40, ny=36, nz=3, dx=1.0, dy=1.0, dz=1.3, nu=48, nv=4, da=0.003, dv=1.0,
+                              off_a=-0.4, off_v=0.35, dsd=1085.6, dso=595.0), 1, 30),
+}
+
+
+def pixel_case(lib, rng):
+    """cPixelDrivenFanBackprojection (PixelDriven.cu:100-141), nChannels = 1."""
+    out = {}
+    for name, (g, B, nview) in PIXEL_CASES.items():
+        ang = (np.arange(nview) * 2 * np.pi / nview + 0.021).astype(np.float32)
+        sino_in = rng.random((B, g["nu"], nview, g["nv"], 1)).astype(np.float32)
+        args = (B, 1, g["nx"], g["ny"], g["nz"], g["dx"], g["dy"], g["dz"], g["nu"], nview, g["nv"], g["da"], g["dv"],
+                g["off_a"], g["off_v"], g["dsd"], g["dso"], 0)
+        bp = np.zeros((B, g["nx"], g["ny"], g["nz"], 1), np.float32)
+        lib.cPixelDrivenFanBackprojection(p(bp), p(sino_in), p(ang), *args)
+        out[name] = dict(sino_in=sino_in, angles=ang, bp=bp, B=B, **{k: np.float64(v) for k, v in g.items()})
+    return out
+
+
 def ossqs_case(lib, rng):
     """cOSSQS (ossqs.cu:12-161, the Siddon pair): a 2D slice, 60 views in 4
     contiguous subsets of 15 (nview a multiple of nviewPerSubset, so the
@@ -178,6 +204,12 @@ def main(outdir=HERE, only=None):
             np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
         print("siddon golden vectors written to", outdir)
         return
+    if only == "pixel":
+        lib = load_ref()
+        for name, d in pixel_case(lib, np.random.default_rng(20241205)).items():
+            np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
+        print("pixel-driven golden vectors written to", outdir)
+        return
     if only == "ossqs":
         lib = load_ref()
         np.savez_compressed(os.path.join(outdir, "ref_ossqs_siddon.npz"),
@@ -195,5 +227,5 @@ def main(outdir=HERE, only=None):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    only = "siddon" if "--siddon" in sys.argv else "ossqs" if "--ossqs" in sys.argv else None
+    only = next((k for k in ("siddon", "ossqs", "pixel") if f"--{k}" in sys.argv), None)
     main(args[0] if args else HERE, only=only)

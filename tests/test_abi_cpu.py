@@ -44,7 +44,7 @@ def test_reference_signatures_match_reference_python_calls():
     counts = {"cDistanceDrivenFanProjection": 21, "cDistanceDrivenFanBackprojection": 21,
               "cDistanceDrivenTomoProjection": 22, "cDistanceDrivenTomoBackprojection": 22,
               "cFilterFanFilter": 15, "cFilterParallelFilter": 15, "cOSSQS": 29, "cTVSQS2D": 5, "SetDevice": 1,
-              "cSiddonFanProjection": 21, "cSiddonFanBackprojection": 21}
+              "cSiddonFanProjection": 21, "cSiddonFanBackprojection": 21, "cPixelDrivenFanBackprojection": 21}
     for k, n in counts.items():
         assert len(N.SIGNATURES[k][1]) == n, k
 

@@ -138,3 +138,21 @@ def test_ossqs_siddon_vs_reference():
     ValueCrop2D) on the same inputs."""
     d, g, _ = _fan(OSSQS)
     assert rel_l2(ossqs_oracle_loop(d, g), d["res"][0, :, :, 0, 0]) < 1e-4   # measured 2.8e-5
+
+
+PIXEL = sorted(glob.glob(os.path.join(GOLDEN, "ref_pixel*.npz")))
+
+
+@pytest.mark.parametrize("path", PIXEL, ids=[os.path.basename(p)[4:-4] for p in PIXEL])
+def test_pixel_bp_vs_reference(path):
+    """The pixel-driven backprojection (PixelDriven.cu:11-62) reads its
+    sinogram through a linear-filtering texture with 8-bit weights and uses
+    __sinf/__cosf; the oracle is checked with exact weights and with the
+    weights rounded to 1/256."""
+    d, g, n = _fan(path)
+    exact = O.pixel_bp(d["sino_in"], d["angles"], g, (n["nx"], n["ny"], n["nz"]))
+    O.set_tex_quant(1)
+    rounded = O.pixel_bp(d["sino_in"], d["angles"], g, (n["nx"], n["ny"], n["nz"]))
+    print(f"{os.path.basename(path)}: exact {rel_l2(exact, d['bp']):.3g}, rounded {rel_l2(rounded, d['bp']):.3g}")
+    assert rel_l2(exact, d["bp"]) < 2e-3      # measured 1.1e-4 / 9.7e-4
+    assert rel_l2(rounded, d["bp"]) < 5e-4    # measured 8.6e-6 / 2.3e-4

@@ -127,3 +127,19 @@ def test_cossqs_vs_reference(ref, rng):
     err = rel_l2(got, d["res"])
     print(f"cOSSQS vs reference: {err:.3g}")
     assert err <= 1e-4   # measured 2.8e-5
+
+
+def test_pixel_bp_vs_reference_kernels(ref, rng):
+    """The reference's bpFanKernel3D (texture reads with 8-bit weights) against
+    the pixel-driven backprojection here."""
+    from reconnet_b200.reconnet import ReconNet
+    lib = ref.load_ref()
+    if not hasattr(lib, "cPixelDrivenFanBackprojection"):
+        pytest.skip("reference library built without PixelDriven.cu")
+    for name, out in ref.pixel_case(lib, rng).items():
+        rn = ReconNet()
+        for k in ("nx", "ny", "nz", "dx", "dy", "dz", "nu", "nv", "da", "dv", "off_a", "off_v", "dsd", "dso"):
+            setattr(rn, k, out[k].item() if k not in ("nx", "ny", "nz", "nu", "nv") else int(out[k]))
+        err = rel_l2(rn.cPixelBackprojection4d(out["sino_in"], out["angles"]), out["bp"])
+        print(f"pixel-driven BP vs reference ({name}): {err:.3g}")
+        assert err <= REF_TOL, name
