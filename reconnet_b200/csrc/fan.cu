@@ -571,15 +571,6 @@ struct BpParams {
 };
 
 
-// Reference detector coordinate of a physical point (GetProjectionOnDetector,
-// DistanceDriven.cu:479-485, and the mapping at :530-533).
-__device__ __forceinline__ float ref_t(float px, float py, float c, float s, const FanDims& d) {
-    float rx = px * c + py * s;
-    float ry = -px * s + py * c;
-    float a = atanf(rx / (ry + d.dso));
-    return -(a / d.du + d.off_u) + d.nu * 0.5f;
-}
-
 // Per-view parameters the BP inner loop reads, staged in shared memory.
 // Siddon BP table: per view, entry u + 1 holds the slope of ray u as hi / lo
 // floats and c_u = w_u * (ray length per band), w_u the sinogram value mixed
@@ -670,8 +661,8 @@ __global__ void pd_table_kernel(const float* __restrict__ prj, const BpSlice* __
 
 struct BpView {
     double pard, perpd;   // source coordinates (Siddon band positions)
-    float par, perp, kappa, tA, tB, sigma, cosd, sind;
-    int xcls, pad0;
+    float par, perp, kappa, tA, tB;
+    int xcls;
 };
 
 struct BpShared {
@@ -865,6 +856,82 @@ __device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView&
     }
 }
 
+// Reference-mode backprojection (kMode 0; DDBPFanKernelX/Y,
+// DistanceDriven.cu:500-614): pixel (x, y) receives, per view, the mean of the
+// pre-weighted detector prefix U over the interval between the detector
+// coordinates t of its two edges taken on its centre line,
+// (U(t2) - U(t1)) / (t2 - t1), U clamped to [0, nu] and the interval not
+// (typeProjector 1 also weights it dso^2 / L^2 at the pixel centre).  On the
+// column-warp tiles the edge coordinates come from the per-lane cubic: X
+// class, lane column x evaluates its left edge (lattice column x) on the 16
+// centre rows and takes the right edge from the next lane; Y class, lane
+// column x (centre line x + 1/2) evaluates the 17 lattice points along it.
+// A rounding of t moves both the prefix difference and the interval, so the
+// ratio is insensitive to it (exactly so when both edges fall in one cell).
+// Table entry e + 1 holds U at edge e as (hi, lo) and the value of cell e.
+__device__ __forceinline__ void ref_u(float t, const float4* T, int ilo, int imax, int nu, float& hi, float& rest) {
+    const float tc = fminf(fmaxf(t, 0.f), (float)nu);
+    float fr;
+    int i = floor_frac(tc, fr) + 1;
+    i = min(max(i, ilo), imax);
+    fr = tc - (float)(i - 1);
+    const float4 E = T[i - ilo];
+    hi = E.x;
+    rest = fmaf(fr, E.z, E.y);
+}
+
+__device__ __forceinline__ void bp_ref_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                         int imax, int x, int y0, int nu, bool fbp, float dq, float dl, float dso2) {
+    const float A = (float)x - vg.par;
+    const TCubic c = t_cubic(vg, A * __fdividef(1.0f, (float)(y0 + kBmRows / 2) - vg.perp));
+    const float aq = (A + 0.5f) * dq;
+#pragma unroll
+    for (int j = 0; j < kBmRows; j++) {
+        const float D = (float)(y0 + j) + 0.5f - vg.perp;
+        const float h = A * __fdividef(1.0f, D) - c.rt;
+        const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+        float hi, rest;
+        ref_u(t, T, ilo, imax, nu, hi, rest);
+        const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
+        const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
+        const float nt = __shfl_down_sync(0xffffffffu, t, 1);
+        float v = __fdividef((nhi - hi) + (nrest - rest), nt - t);
+        if (fbp) {
+            const float b = D * dl;
+            v *= __fdividef(dso2, fmaf(aq, aq, b * b));
+        }
+        acc[j] += v;
+    }
+}
+
+__device__ __forceinline__ void bp_ref_y(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
+                                         int imax, int x, int y0, int nu, bool fbp, float dq, float dl, float dso2) {
+    const float D = (float)x + 0.5f - vg.perp;
+    const float g = __fdividef(1.0f, D);
+    const float r0 = ((float)y0 - vg.par) * g;
+    const TCubic c = t_cubic(vg, fmaf((float)(kBmRows / 2), g, r0));
+    const float b = D * dl;
+    float hprev = 0.f, rprev = 0.f, tprev = 0.f;
+#pragma unroll
+    for (int j = 0; j <= kBmRows; j++) {
+        const float h = fmaf((float)j, g, r0) - c.rt;
+        const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
+        float hi, rest;
+        ref_u(t, T, ilo, imax, nu, hi, rest);
+        if (j > 0) {
+            float v = __fdividef((hi - hprev) + (rest - rprev), t - tprev);
+            if (fbp) {
+                const float a = ((float)(y0 + j) - 0.5f - vg.par) * dq;
+                v *= __fdividef(dso2, fmaf(a, a, b * b));
+            }
+            acc[j - 1] += v;
+        }
+        hprev = hi;
+        rprev = rest;
+        tprev = t;
+    }
+}
+
 // Pixel-driven backprojection (kMode 3; bpFanKernel3D with the FBP weight,
 // PixelDriven.cu:11-62): pixel (x, y) receives, per view, the sinogram value
 // at the detector coordinate pu of the ray through its centre, interpolated
@@ -954,17 +1021,10 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
     const bool valid = c * kBpViews + v < nview;
     const ViewGeo& vg = src[valid ? v : 0];
     const int cx = corner & 1, cy = corner >> 1;
-    float t;
-    if (kMode != 0) {
-        const int xcls = vg.xcls;
-        const float X = (float)(X0 + cx * kBmCols), Y = (float)(Y0 + cy * kBmTileY);
-        const float l = xcls ? Y : X, q = xcls ? X : Y;
-        t = matched_t(vg, (q - (float)vg.par) / (l - (float)vg.perp));
-    } else {
-        const float px = ((float)(X0 + cx * kBpTile) - 0.5f - (d.nx - 1) * 0.5f) * d.dx;
-        const float py = ((float)(Y0 + cy * kBpTile) - 0.5f - (d.ny - 1) * 0.5f) * d.dy;
-        t = ref_t(px, py, vg.cosd, vg.sind, d);
-    }
+    const int xcls = vg.xcls;
+    const float X = (float)(X0 + cx * kBmCols), Y = (float)(Y0 + cy * kBmTileY);
+    const float l = xcls ? Y : X, q = xcls ? X : Y;
+    float t = matched_t(vg, (q - (float)vg.par) / (l - (float)vg.perp));
     t = fminf(t, __shfl_xor_sync(0xffffffffu, t, 1));
     t = fminf(t, __shfl_xor_sync(0xffffffffu, t, 2));
     if (valid && corner == 0) {
@@ -979,9 +1039,6 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
         w.kappa = vg.kappa;
         w.tA = vg.tA;
         w.tB = vg.tB;
-        w.sigma = vg.sigma;
-        w.cosd = vg.cosd;
-        w.sind = vg.sind;
         w.xcls = vg.xcls;
     }
 }
@@ -990,8 +1047,7 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
 // Siddon tiles run three CTAs per SM (80 registers, 180 vs 174 Gupd/s at two
 // CTAs); the DD modes keep the compiler's register choice (71 / 80).
 template <int kMode>
-__global__ void __launch_bounds__(kBpThreads, kMode == 2 ? 3 : 0) fan_bp_kernel(BpParams p) {
-    constexpr bool kMatched = kMode != 0;   // column-warp tiles and the matched edge index
+__global__ void __launch_bounds__(kBpThreads, (kMode == 2 || kMode == 0) ? 3 : 0) fan_bp_kernel(BpParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     BpShared* sh = reinterpret_cast<BpShared*>(smem);
     size_t off = (sizeof(BpShared) + 127) & ~size_t(127);
@@ -1007,16 +1063,13 @@ __global__ void __launch_bounds__(kBpThreads, kMode == 2 ? 3 : 0) fan_bp_kernel(
     const float4* gtab = p.tab + (bs.table_off - p.tab_base);
     const int nu = p.d.nu, nx = p.d.nx, ny = p.d.ny;
     const int tid = threadIdx.x;
-    // CTA pixel origin and thread pixel origin.  Matched: lane i of warp w
-    // owns column X0 + i, rows Y0 + 16 w ...  Reference mode: 4 x 4 pixels
-    // per thread; a warp covers 8 x 4 threads (32 x 16 pixels), and each
-    // group of 8 lanes that shares one shared-memory wavefront covers 2 x 4
-    // threads, so its table reads spread over distinct banks more often.
-    const int X0 = txi * (kMatched ? kBmCols : kBpTile), Y0 = tyi * (kMatched ? kBmTileY : kBpTile);
+    // Column-warp tiles: lane i of warp w owns pixel column X0 + i and rows
+    // Y0 + 16 w .. + 15 (lane 31's column belongs to the next tile: it only
+    // supplies edges).
+    const int X0 = txi * kBmCols, Y0 = tyi * kBmTileY;
     const int lane = tid & 31, warp = tid >> 5;
-    const int tx = ((warp & 1) << 3) | (lane & 1) | ((lane >> 3) << 1), ty = ((warp >> 1) << 2) | ((lane >> 1) & 3);
-    const int x0 = kMatched ? X0 + lane : X0 + tx * 4;
-    const int y0 = kMatched ? Y0 + warp * kBmRows : Y0 + ty * 4;
+    const int x0 = X0 + lane;
+    const int y0 = Y0 + warp * kBmRows;
     const int tabn = nu + 2;   // table entries per view (guard + nu + total)
 
     if (tid == 0) {
@@ -1052,11 +1105,10 @@ __global__ void __launch_bounds__(kBpThreads, kMode == 2 ? 3 : 0) fan_bp_kernel(
     __syncthreads();
     if (tid == 0) issue(0);
 
-    // accumulators: matched acc[j] = pixel (x0, y0 + j); reference mode
-    // acc[a * 4 + b] = pixel (x0 + a, y0 + b)
-    float acc[16];
+    // accumulators: acc[j] = pixel (x0, y0 + j)
+    float acc[kBmRows];
 #pragma unroll
-    for (int a = 0; a < 16; a++) acc[a] = 0.f;
+    for (int a = 0; a < kBmRows; a++) acc[a] = 0.f;
 
     // One barrier per chunk: after it every warp has finished chunk c - 1, so
     // buffer (c + 1) & 1 and record slot c & 1 may be refilled; window and
@@ -1091,77 +1143,25 @@ __global__ void __launch_bounds__(kBpThreads, kMode == 2 ? 3 : 0) fan_bp_kernel(
                 if (vg.xcls) bp_matched_x(acc, vg, T, ilo, imax, x0, y0, ny);
                 else bp_matched_y(acc, vg, T, ilo, imax, x0, y0, nx);
             } else {
-                // reference DDBPFanKernelX/Y: pixel edges at the pixel centre line
-                const float cs = vg.cosd, sn = vg.sind;
-#pragma unroll
-                for (int li = 0; li < 4; li++) {
-                    float tq[5], uh[5], ul[5];
-#pragma unroll
-                    for (int qi = 0; qi < 5; qi++) {
-                        float px, py;
-                        if (vg.xcls) {
-                            px = ((float)(x0 + qi) - 0.5f - (nx - 1) * 0.5f) * p.d.dx;
-                            py = ((float)(y0 + li) - (ny - 1) * 0.5f) * p.d.dy;
-                        } else {
-                            px = ((float)(x0 + li) - (nx - 1) * 0.5f) * p.d.dx;
-                            py = ((float)(y0 + qi) - 0.5f - (ny - 1) * 0.5f) * p.d.dy;
-                        }
-                        float t = ref_t(px, py, cs, sn, p.d);
-                        float tc = fminf(fmaxf(t, 0.f), (float)nu);
-                        float fr;
-                        int i = floor_frac(tc, fr) + 1;   // table index of cell k
-                        i = min(max(i, ilo), imax);
-                        fr = tc - (float)(i - 1);
-                        float4 E = T[i - ilo];
-                        tq[qi] = t;
-                        uh[qi] = E.x;
-                        ul[qi] = fmaf(fr, E.z, E.y);
-                    }
-#pragma unroll
-                    for (int qi = 0; qi < 4; qi++) {
-                        float dU = (uh[qi + 1] - uh[qi]) + (ul[qi + 1] - ul[qi]);
-                        float val = dU / (tq[qi + 1] - tq[qi]);
-                        int ax = vg.xcls ? qi : li, ay = vg.xcls ? li : qi;
-                        if (p.type == RN_TYPE_FBP) {
-                            float px = ((float)(x0 + ax) - (nx - 1) * 0.5f) * p.d.dx;
-                            float py = ((float)(y0 + ay) - (ny - 1) * 0.5f) * p.d.dy;
-                            float rx = px * cs + py * sn;
-                            float ry = -px * sn + py * cs;
-                            float dd = p.d.dso + ry;
-                            val *= p.d.dso * p.d.dso / (rx * rx + dd * dd);
-                        }
-                        if (vg.xcls) acc[qi * 4 + li] += val;
-                        else acc[li * 4 + qi] += val;
-                    }
-                }
+                const bool fbp = p.type == RN_TYPE_FBP;
+                const float dso2 = p.d.dso * p.d.dso;
+                if (vg.xcls) bp_ref_x(acc, vg, T, ilo, imax, x0, y0, nu, fbp, p.d.dx, p.d.dy, dso2);
+                else bp_ref_y(acc, vg, T, ilo, imax, x0, y0, nu, fbp, p.d.dy, p.d.dx, dso2);
             }
         }
     }
     if (!ok) return;
 
     float* out = p.img + bs.img_off;
-    if (kMatched) {
-        if (lane < kBmCols && x0 < nx) {
+    if (lane < kBmCols && x0 < nx) {
 #pragma unroll
-            for (int j = 0; j < kBmRows; j++) {
-                const int iy = y0 + j;
-                if (iy < ny) {
-                    float* q = out + (long long)x0 * p.d.isx + (long long)iy * p.d.isy;
-                    *q = p.accumulate ? (*q + acc[j]) : acc[j];
-                }
+        for (int j = 0; j < kBmRows; j++) {
+            const int iy = y0 + j;
+            if (iy < ny) {
+                float* q = out + (long long)x0 * p.d.isx + (long long)iy * p.d.isy;
+                *q = p.accumulate ? (*q + acc[j]) : acc[j];
             }
         }
-    } else {
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-            for (int bb = 0; bb < 4; bb++) {
-                const int ix = x0 + a, iy = y0 + bb;
-                if (ix < nx && iy < ny) {
-                    float* q = out + (long long)ix * p.d.isx + (long long)iy * p.d.isy;
-                    *q = p.accumulate ? (*q + acc[a * 4 + bb]) : acc[a * 4 + bb];
-                }
-            }
     }
 }
 
@@ -1415,11 +1415,9 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
     const std::vector<BpSlice>& bps = siddon ? p->h_bps : (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
     const BpSlice* dbp = siddon ? p->d_bps : (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
     const int nbp = (int)bps.size();
-    const bool matched = type == RN_TYPE_MATCHED || siddon || pixel;   // column-warp tiles
-    const int win = matched ? p->table_win_m : p->table_win;
+    const int win = p->table_win_m;
     const size_t smem = bp_smem_bytes(win);
-    const int tw = matched ? kBmCols : kBpTile, th = matched ? kBmTileY : kBpTile;
-    const int tiles_x = (d.nx + tw - 1) / tw, tiles_y = (d.ny + th - 1) / th;
+    const int tiles_x = (d.nx + kBmCols - 1) / kBmCols, tiles_y = (d.ny + kBmTileY - 1) / kBmTileY;
     int s0 = 0;
     while (s0 < nbp) {
         // as many slices as fit in the table scratch

@@ -107,10 +107,9 @@ static int table_window(const RnFanGeom& g, int tw, int th) {
 
 static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     const RnFanGeom& g = p->g;
-    int win = table_window(g, kBpTile, kBpTile), win_m = table_window(g, kBmCols, kBmTileY);
-    if (win < 0 || win_m < 0) return set_error(RN_ERR_ARG, "fan geometry: the image reaches the source");
-    if (std::max(win, win_m) > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
-    p->table_win = win;
+    const int win_m = table_window(g, kBmCols, kBmTileY);
+    if (win_m < 0) return set_error(RN_ERR_ARG, "fan geometry: the image reaches the source");
+    if (win_m > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
     p->table_win_m = win_m;
     RN_TRY(fan_kernel_attributes());
     RN_TRY(fan_build_geometry(p, host_deg, st));

@@ -69,11 +69,9 @@ struct FpSlice {
 // A 2D backward problem: image plane at img_off from a mix of up to 4
 // sinogram planes.
 constexpr int kBpMix = 4;
-// Backprojection tiles (CTA of 256 threads).  Reference mode: 64 x 64
-// pixels, 4 x 4 per thread.  Matched: 31 pixel columns (one per lane; lane
-// 31 only supplies an edge) by 8 warps x kBmRows rows.
+// Backprojection tiles (CTA of 256 threads, every mode): 31 pixel columns
+// (one per lane; lane 31 only supplies an edge) by 8 warps x kBmRows rows.
 constexpr int kBpThreads = 256;
-constexpr int kBpTile = 64;
 constexpr int kBmCols = 31;
 constexpr int kBmRows = 16;
 constexpr int kBmTileY = kBmRows * (kBpThreads / 32);
@@ -153,8 +151,7 @@ struct rn_fan_plan {
     float* d_la = nullptr;          // FP line values
     long long line_slot_elems = 0;  // per FP slice: ny*lpx + nx*lpy
     long long fp_slots = 0;         // FP slices whose lines fit in the scratch
-    int table_win = 0;              // staged table entries per view (reference-mode BP, 64 x 64 tiles)
-    int table_win_m = 0;            // staged table entries per view (matched BP, 31 x 128 tiles)
+    int table_win_m = 0;            // staged table entries per view (BP tiles of 31 x 128 pixels)
     float4* d_tab = nullptr;        // BP edge tables
     long long tab_elems = 0;
     float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, lazily allocated)
