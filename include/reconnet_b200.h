@@ -216,6 +216,21 @@ int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int
 int rn_tv_sqs(float* d_grad, float* d_norm, double* d_tv, const float* d_img, int nslices, int nx, int ny,
               void* stream);
 
+/* Isotropic TV surrogate of the prior solver (PriorFunctionSolver/TVSQS.cu:8-93
+ * 2D, :160-265 3D) on device pointers, one pass: with backward differences d_k
+ * and forward differences f_k (0 on the borders),
+ *   var = sqrt(sum_k d_k^2 + eps),
+ *   s1  = sum_k d_k / var + sum_k f_k / var(p + e_k),
+ *   s2  = ndim / var + sum_k 1 / var(p + e_k)   (var(p + e_k) = var on the high border).
+ * Arrays [nb][nx][ny][nz][nc]; ndim 2 requires nz = 1; d_var may be NULL. */
+int rn_tv_iso_sqs(float* d_s1, float* d_s2, float* d_var, const float* d_img, int nb, int nx, int ny, int nz, int nc,
+                  float eps, int ndim, void* stream);
+
+/* The same on host pointers (synchronous; the prior-solver shim's cTVSQS2D /
+ * cTVSQS3D forward here). */
+int rn_tv_iso_sqs_host(float* s1, float* s2, float* var, const float* img, int nb, int nx, int ny, int nz, int nc,
+                       float eps, int ndim);
+
 /* One OS-SQS subset update on all slices of a plan (device pointers):
  *   x_out = clamp(x_in - lambda * (nSubsets * A_s^T W_s (A_s x_in - b_s) + beta * grad_tv(x_in))
  *                  / (normImg + beta * norm_tv(x_in) + 1e-6), lb, ub)

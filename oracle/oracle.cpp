@@ -516,6 +516,59 @@ double tv_sqs(T* grad, T* norm, const float* img, int nx, int ny) {
 }
 
 // --------------------------------------------------------------------------
+// Isotropic TV surrogate of the prior solver: Variation2DKernel +
+// TVSQS2DKernel (PriorFunctionSolver/TVSQS.cu:8-93) and Variation3DKernel +
+// TVSQS3DKernel (:160-265), on [nb][nx][ny][nz][nc] (nz = 1 in 2D).  var is
+// the root of eps plus the squared backward differences (none on the low
+// border); s1 / s2 add, per axis, the backward term over var and the forward
+// term over the neighbour's var, which the high border replaces by the
+// voxel's own var.
+// --------------------------------------------------------------------------
+void tv_iso_sqs(double* s1, double* s2, double* var, const float* img, int nb, int nx, int ny, int nz, int nc,
+                double eps, int ndim) {
+    const int64_t sz = nc, sy = (int64_t)nz * nc, sx = (int64_t)ny * sy;
+    const int64_t n = (int64_t)nb * nx * sx;
+    auto idx = [&](int64_t i, int& x, int& y, int& z) {
+        int64_t q = i / nc;
+        z = (int)(q % nz);
+        q /= nz;
+        y = (int)(q % ny);
+        q /= ny;
+        x = (int)(q % nx);
+    };
+    for (int64_t i = 0; i < n; i++) {
+        int x, y, z;
+        idx(i, x, y, z);
+        double s = eps, v0 = img[i];
+        if (x > 0) s += (v0 - img[i - sx]) * (v0 - img[i - sx]);
+        if (y > 0) s += (v0 - img[i - sy]) * (v0 - img[i - sy]);
+        if (ndim == 3 && z > 0) s += (v0 - img[i - sz]) * (v0 - img[i - sz]);
+        var[i] = std::sqrt(s);
+    }
+    for (int64_t i = 0; i < n; i++) {
+        int x, y, z;
+        idx(i, x, y, z);
+        const double v0 = img[i], v = var[i];
+        double a = 0, b = ndim / v;
+        if (x > 0) a += (v0 - img[i - sx]) / v;
+        if (y > 0) a += (v0 - img[i - sy]) / v;
+        if (ndim == 3 && z > 0) a += (v0 - img[i - sz]) / v;
+        const int64_t st[3] = {sx, sy, sz};
+        const int pos[3] = {x, y, z}, lim[3] = {nx, ny, nz};
+        for (int k = 0; k < ndim; k++) {
+            if (pos[k] < lim[k] - 1) {
+                a += (v0 - img[i + st[k]]) / var[i + st[k]];
+                b += 1.0 / var[i + st[k]];
+            } else {
+                b += 1.0 / v;
+            }
+        }
+        s1[i] = a;
+        s2[i] = b;
+    }
+}
+
+// --------------------------------------------------------------------------
 // Siddon fan projector pair: SiddonFanProjectionKernel /
 // SiddonFanBackprojectionKernel with InitializeSiddon and the tracing loops
 // (Siddon.cu:14-375).  Ray (iu, iview, iv) runs from the source
@@ -925,6 +978,10 @@ void oracle_filter_f64(double* out, const float* prj, int nb, int nc, int nu, in
                        float off_a, float off_v, float dsd, float dso, int typeFilter, int fan) {
     (void)dv; (void)off_v;
     filter_sino<double>(out, prj, nb, nc, nu, nview, nv, da, off_a, dsd, dso, typeFilter, fan != 0);
+}
+void oracle_tv_iso_sqs_f64(double* s1, double* s2, double* var, const float* img, int nb, int nx, int ny, int nz,
+                           int nc, double eps, int ndim) {
+    tv_iso_sqs(s1, s2, var, img, nb, nx, ny, nz, nc, eps, ndim);
 }
 double oracle_tv_sqs_f64(double* grad, double* norm, const float* img, int nx, int ny) {
     return tv_sqs<double>(grad, norm, img, nx, ny);

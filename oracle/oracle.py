@@ -60,6 +60,7 @@ def lib():
         L.oracle_filter_f64.argtypes = [_dp, _fp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i]
         L.oracle_tv_sqs_f64.argtypes = [_dp, _dp, _fp, _i, _i]
         L.oracle_tv_sqs_f64.restype = ctypes.c_double
+        L.oracle_tv_iso_sqs_f64.argtypes = [_dp, _dp, _dp, _fp, _i, _i, _i, _i, _i, ctypes.c_double, _i]
         L.oracle_tomo_fp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO + [_i]
         _lib = L
@@ -194,6 +195,23 @@ def tv_sqs(img2d):
     norm = np.zeros((nx, ny), np.float64)
     tv = lib().oracle_tv_sqs_f64(_ptr(grad, ctypes.c_double), _ptr(norm, ctypes.c_double), _ptr(img, _f), nx, ny)
     return grad, norm, float(tv)
+
+
+def tv_iso_sqs(img, ndim, eps=1e-8):
+    """Isotropic TV surrogate (PriorFunctionSolver/TVSQS.cu:8-93, 160-265):
+    img is [nb, nx, ny, nc] (ndim 2) or [nb, nx, ny, nz, nc] (ndim 3);
+    returns (s1, s2, var) in FP64."""
+    img = _f32(img)
+    if ndim == 2:
+        nb, nx, ny, nc = img.shape
+        nz = 1
+    else:
+        nb, nx, ny, nz, nc = img.shape
+    s1, s2, var = (np.zeros(img.shape, np.float64) for _ in range(3))
+    d = ctypes.c_double
+    lib().oracle_tv_iso_sqs_f64(_ptr(s1, d), _ptr(s2, d), _ptr(var, d), _ptr(img, _f), nb, nx, ny, nz, nc,
+                                float(eps), int(ndim))
+    return s1, s2, var
 
 
 def _tomo_args(g, img_shape, prj_shape):

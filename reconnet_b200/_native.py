@@ -10,6 +10,7 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libreconnet_b200.so")
+PRIOR_LIB_PATH = os.path.join(_HERE, "_lib", "libreconnet_b200_prior.so")
 
 RN_OK = 0
 RN_ERR_ARG = 1
@@ -77,6 +78,8 @@ SIGNATURES = {
     "rn_fan_plan_read_timing": (_i, [_vp, _fp, ctypes.POINTER(_i), _i, ctypes.POINTER(ctypes.c_longlong)]),
     "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
     "rn_tv_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
+    "rn_tv_iso_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _vp]),
+    "rn_tv_iso_sqs_host": (_i, [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _i, _f, _i]),
     "rn_fan_sqs_update": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _i, _f, _f, _i, _vp]),
     "rn_fan_project_noalloc": (_i, [_vp, _vp, _fp, _i, _i, _f, _f, _i, _i, _f, _f, _f, _f, _vp]),
     "rn_tomo_sat_bytes": (_i, [_i, _i, _i, _i, _i, _i, ctypes.POINTER(ctypes.c_size_t),
@@ -99,6 +102,27 @@ def _load():
 
 
 lib = _load()
+
+# the prior-solver shim (include/reconnet_b200_prior.h), loaded on first use
+PRIOR_SIGNATURES = {
+    "cTVSQS2D": (None, [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _f]),
+    "cTVSQS3D": (None, [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _i, _f]),
+}
+_prior = None
+
+
+def prior_lib():
+    global _prior
+    if _prior is None:
+        if not os.path.exists(PRIOR_LIB_PATH):
+            raise ImportError(f"prior-solver shim not built ({PRIOR_LIB_PATH}); run `python -m reconnet_b200.build`")
+        p = ctypes.CDLL(PRIOR_LIB_PATH)
+        for name, (res, args) in PRIOR_SIGNATURES.items():
+            fn = getattr(p, name)
+            fn.restype = res
+            fn.argtypes = args
+        _prior = p
+    return _prior
 
 
 def last_error() -> str:

@@ -3,7 +3,9 @@
 Each ``csrc/*.cu`` is compiled with nvcc for ``sm_100a`` (objects under
 ``reconnet_b200/_lib/obj``, rebuilt when a source or header is newer), then
 linked into one shared library exporting the C ABI of
-``include/reconnet_b200.h``.  Run ``python -m reconnet_b200.build``.
+``include/reconnet_b200.h``; ``libreconnet_b200_prior.so`` (the prior-solver
+names of ``include/reconnet_b200_prior.h``) forwards to it.  Run
+``python -m reconnet_b200.build``.
 """
 from __future__ import annotations
 
@@ -20,6 +22,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 OBJDIR = os.path.join(LIBDIR, "obj")
 LIB = os.path.join(LIBDIR, "libreconnet_b200.so")
+PRIOR_LIB = os.path.join(LIBDIR, "libreconnet_b200_prior.so")
+PRIOR_SRC = os.path.join(CSRC, "prior_abi.cpp")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -68,6 +72,14 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    # the prior-solver shim: the reference prior library's names, forwarded
+    if (force or not os.path.exists(PRIOR_LIB) or os.path.getmtime(PRIOR_LIB) < os.path.getmtime(LIB)
+            or os.path.getmtime(PRIOR_LIB) < os.path.getmtime(PRIOR_SRC)):
+        cmd = ["g++", "-O2", "-shared", "-fPIC", "-std=c++17", "-o", PRIOR_LIB, PRIOR_SRC, "-L" + LIBDIR,
+               "-lreconnet_b200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"prior shim link failed:\n{r.stderr}")
     return LIB
 
 

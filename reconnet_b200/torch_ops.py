@@ -326,6 +326,22 @@ def fbp(sino: torch.Tensor, plan: "FanPlan", geom: FanGeometry, type_filter: int
     return plan.backproject(filter_sino(sino, geom, type_filter), N.RN_TYPE_PIXEL, out=out)
 
 
+def tv_iso_sqs(img: torch.Tensor, ndim: int, eps: float = 1e-8, want_var: bool = True):
+    """Isotropic TV surrogate (PriorFunctionSolver/TVSQS.cu) of a CUDA tensor
+    [nb, nx, ny, nc] (ndim 2) or [nb, nx, ny, nz, nc] (ndim 3) -> (s1, s2, var)."""
+    if ndim == 2:
+        nb, nx, ny, nc = img.shape
+        nz = 1
+    else:
+        nb, nx, ny, nz, nc = img.shape
+    img = img.contiguous()
+    s1, s2 = torch.empty_like(img), torch.empty_like(img)
+    var = torch.empty_like(img) if want_var else None
+    N.check(N.lib.rn_tv_iso_sqs(_dev_ptr(s1), _dev_ptr(s2), _dev_ptr(var) if var is not None else None,
+                                _dev_ptr(img), nb, nx, ny, nz, nc, float(eps), int(ndim), _stream_ptr(img.device)))
+    return s1, s2, var
+
+
 def tv_sqs(img: torch.Tensor, want_tv: bool = True):
     """TV surrogate terms of a [S, nx, ny] CUDA tensor -> (grad, norm, tv[S] float64)."""
     S, nx, ny = img.shape

@@ -11,6 +11,7 @@ these files.
     python tests/golden/make_golden.py --siddon [outdir]   (the Siddon pair only)
     python tests/golden/make_golden.py --ossqs [outdir]    (cOSSQS only)
     python tests/golden/make_golden.py --pixel [outdir]    (pixel-driven backprojection only)
+    python tests/golden/make_golden.py --prior [outdir]    (the prior solver's TV, oracle/_ref/libprior_ref.so)
 """
 import ctypes
 import math
@@ -170,6 +171,33 @@ def pixel_case(lib, rng):
     return out
 
 
+PRIOR_REF = os.path.join(ROOT, "oracle", "_ref", "libprior_ref.so")
+
+
+def load_prior_ref(path=PRIOR_REF):
+    lib = ctypes.CDLL(path)
+    lib.cTVSQS2D.argtypes = [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _f]
+    lib.cTVSQS3D.argtypes = [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _i, _f]
+    return lib
+
+
+def prior_case(lib, rng):
+    """cTVSQS2D / cTVSQS3D of the prior solver (PriorFunctionSolver/TVSQS.cu):
+    smooth-plus-noise images with flat patches (zero differences, where eps
+    matters), two batches and two channels."""
+    out = {}
+    for ndim, shape in ((2, (2, 23, 17, 2)), (3, (2, 11, 9, 7, 2))):
+        x = rng.random(shape).astype(np.float32)
+        x[0, 2:6, 3:8] = 0.5
+        s1, s2, var = (np.zeros(shape, np.float32) for _ in range(3))
+        if ndim == 2:
+            lib.cTVSQS2D(p(s1), p(s2), p(var), p(x), *shape, 1e-8)
+        else:
+            lib.cTVSQS3D(p(s1), p(s2), p(var), p(x), *shape, 1e-8)
+        out[f"tviso{ndim}d"] = dict(img=x, s1=s1, s2=s2, var=var, ndim=ndim, eps=1e-8)
+    return out
+
+
 def ossqs_case(lib, rng):
     """cOSSQS (ossqs.cu:12-161, the Siddon pair): a 2D slice, 60 views in 4
     contiguous subsets of 15 (nview a multiple of nviewPerSubset, so the
@@ -210,6 +238,12 @@ def main(outdir=HERE, only=None):
             np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
         print("pixel-driven golden vectors written to", outdir)
         return
+    if only == "prior":
+        lib = load_prior_ref()
+        for name, d in prior_case(lib, np.random.default_rng(20241206)).items():
+            np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
+        print("prior-solver golden vectors written to", outdir)
+        return
     if only == "ossqs":
         lib = load_ref()
         np.savez_compressed(os.path.join(outdir, "ref_ossqs_siddon.npz"),
@@ -227,5 +261,5 @@ def main(outdir=HERE, only=None):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    only = next((k for k in ("siddon", "ossqs", "pixel") if f"--{k}" in sys.argv), None)
+    only = next((k for k in ("siddon", "ossqs", "pixel", "prior") if f"--{k}" in sys.argv), None)
     main(args[0] if args else HERE, only=only)

@@ -73,3 +73,17 @@ def test_reference_named_void_calls_report_errors():
     assert N.lib.rn_last_status() == N.RN_ERR_ARG
     with pytest.raises(N.ReconNetError):
         N.check_last()
+
+
+def test_prior_shim_exports_reference_names():
+    """libreconnet_b200_prior.so exports the prior solver's cTVSQS2D /
+    cTVSQS3D (include/reconnet_b200_prior.h) and resolves its forwarder."""
+    import re
+    from conftest import ROOT
+    from reconnet_b200 import _native as N
+    hdr = open(os.path.join(ROOT, "include", "reconnet_b200_prior.h")).read()
+    names = set(re.findall(r"^void (\w+)\(", hdr, re.M))
+    assert names == set(N.PRIOR_SIGNATURES)
+    lib = N.prior_lib()
+    for n in names:
+        assert hasattr(lib, n)

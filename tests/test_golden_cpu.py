@@ -156,3 +156,17 @@ def test_pixel_bp_vs_reference(path):
     print(f"{os.path.basename(path)}: exact {rel_l2(exact, d['bp']):.3g}, rounded {rel_l2(rounded, d['bp']):.3g}")
     assert rel_l2(exact, d["bp"]) < 2e-3      # measured 1.1e-4 / 9.7e-4
     assert rel_l2(rounded, d["bp"]) < 5e-4    # measured 8.6e-6 / 2.3e-4
+
+
+TVISO = sorted(glob.glob(os.path.join(GOLDEN, "ref_tviso*.npz")))
+
+
+@pytest.mark.parametrize("path", TVISO, ids=[os.path.basename(p)[4:-4] for p in TVISO])
+def test_tv_iso_vs_reference(path):
+    """The prior solver's isotropic TV surrogate (PriorFunctionSolver/TVSQS.cu),
+    FP32 in the reference, against the FP64 restatement."""
+    d = dict(np.load(path))
+    s1, s2, var = O.tv_iso_sqs(d["img"], int(d["ndim"]), float(d["eps"]))
+    assert rel_l2(var, d["var"]) < 1e-6     # measured 3.5e-8 / 3.6e-8
+    assert rel_l2(s2, d["s2"]) < 1e-6      # measured 1.7e-8 / 1.9e-8
+    assert rel_l2(s1, d["s1"]) < 1e-6      # measured 4.7e-8 / 4.8e-8
