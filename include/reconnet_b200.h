@@ -216,6 +216,60 @@ int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int
 int rn_tv_sqs(float* d_grad, float* d_norm, double* d_tv, const float* d_img, int nslices, int nx, int ny,
               void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Siddon cone-beam pair with arbitrary per-view geometry (SiddonCone.cu).
+ * Ray (iu, iview, iv) runs from src[iview] to detCenter[iview] + u detU[iview]
+ * + v detV[iview], u = (iu - off_u - (nu-1)/2) du, v = (iv - off_v -
+ * (nv-1)/2) dv; the grid of nx x ny x nz voxels (dx, dy, dz mm) is centred at
+ * (cx, cy, cz).  Geometry arrays are [nview][3] floats (mm), images
+ * [nBatches][nx][ny][nz][nChannels], projections [nBatches][nu][nview][nv]
+ * [nChannels].  Every view needs a main axis along which all its rays advance,
+ * with lateral slopes of at most 4 (RN_ERR_ARG otherwise).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int nBatches, nChannels, nx, ny, nz;
+    float dx, dy, dz, cx, cy, cz;
+    int nu, nview, nv;
+    float du, dv, off_u, off_v;
+} RnConeGeom;
+
+typedef struct rn_cone_plan rn_cone_plan;
+
+/* Plan: per-view geometry and the per-ray table (32 B per ray) on the device.
+ * The geometry arrays are host pointers. */
+int rn_cone_plan_create(rn_cone_plan** plan, const RnConeGeom* g, const float* detCenter, const float* detU,
+                        const float* detV, const float* src, void* stream);
+int rn_cone_plan_destroy(rn_cone_plan* plan);
+/* Forward projection (prj overwritten) and its exact transpose (accumulate =
+ * 0 overwrites img, 1 adds to it), device pointers, on `stream`. */
+int rn_cone_project(rn_cone_plan* plan, float* d_prj, const float* d_img, void* stream);
+int rn_cone_backproject(rn_cone_plan* plan, float* d_img, const float* d_prj, int accumulate, void* stream);
+long long rn_cone_plan_launches(const rn_cone_plan* plan);
+
+/* replaces ReconNet4D/SiddonCone.cu:126-201 (host pointers; prj overwritten) */
+void cSiddonConeProjectionAbitrary(float* prj, const float* img, const float* detCenter, const float* detU,
+                                   const float* detV, const float* src, int nBatches, int nChannels, int nx, int ny,
+                                   int nz, float dx, float dy, float dz, float cx, float cy, float cz, int nu,
+                                   int nview, int nv, float du, float dv, float off_u, float off_v);
+
+/* replaces ReconNet4D/SiddonCone.cu:203-278 (host pointers; img overwritten;
+ * the exact transpose, gathered per voxel: the reference scatters with
+ * atomics) */
+void cSiddonConeBackprojectionAbitrary(float* img, const float* prj, const float* detCenter, const float* detU,
+                                       const float* detV, const float* src, int nBatches, int nChannels, int nx,
+                                       int ny, int nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                                       int nu, int nview, int nv, float du, float dv, float off_u, float off_v);
+
+/* replaces ReconNet4D/ossqs.cu:163-333: OS-SQS with the cone pair,
+ *   x = clamp(mask * (x - lambda nSubsets A_s^T (A_s x - b_s) / (normImg + 1e-6)), lb, ub)
+ * over contiguous subsets of nviewPerSubset views (the last one holds the
+ * remaining views); typeProjector is ignored as in the reference. */
+void cOSSQSConeAbitrary(float* res, const float* img, const float* prj, const float* normImg, const float* mask,
+                        const float* detCenter, const float* detU, const float* detV, const float* src, float lb,
+                        float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels, int nx, int ny,
+                        int nz, float dx, float dy, float dz, float cx, float cy, float cz, int nu, int nview, int nv,
+                        float du, float dv, float off_u, float off_v, int typeProjector, float lambda);
+
 /* Isotropic TV surrogate of the prior solver (PriorFunctionSolver/TVSQS.cu:8-93
  * 2D, :160-265 3D) on device pointers, one pass: with backward differences d_k
  * and forward differences f_k (0 on the borders),

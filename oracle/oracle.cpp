@@ -581,16 +581,16 @@ void tv_iso_sqs(double* s1, double* s2, double* var, const float* img, int nb, i
 // the middle of each segment.  An axis along which the ray moves by at most
 // 1e-6 voxels is parallel, as InboundAlpha treats it (:22-41).
 // --------------------------------------------------------------------------
+// Grid with voxel counts n, sizes d and centre c (PhysicsToImg, Siddon.cu:14-21).
 template <typename Visit>
-void siddon_trace(const Fan& g, const double src[3], const double dst[3], Visit&& visit) {
-    const int n[3] = {g.nx, g.ny, g.nz};
-    const double d[3] = {g.dx, g.dy, g.dz};
+void siddon_trace_grid(const int n[3], const double d[3], const double c[3], const double src[3],
+                       const double dst[3], Visit&& visit) {
     double dist = 0;
     double s[3], e[3], dd[3];
     for (int k = 0; k < 3; k++) {
         dist += (src[k] - dst[k]) * (src[k] - dst[k]);
-        s[k] = src[k] / d[k] + n[k] / 2.0;   // centre of the grid at the origin
-        e[k] = dst[k] / d[k] + n[k] / 2.0;
+        s[k] = (src[k] - c[k]) / d[k] + n[k] / 2.0;
+        e[k] = (dst[k] - c[k]) / d[k] + n[k] / 2.0;
         dd[k] = e[k] - s[k];
     }
     dist = std::sqrt(dist);
@@ -632,6 +632,14 @@ void siddon_trace(const Fan& g, const double src[3], const double dst[3], Visit&
         }
         if (inside) visit(idx[0], idx[1], idx[2], (b - a) * dist);
     }
+}
+
+// The fan grid: centred at the origin.
+template <typename Visit>
+void siddon_trace(const Fan& g, const double src[3], const double dst[3], Visit&& visit) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double d[3] = {g.dx, g.dy, g.dz}, c[3] = {0, 0, 0};
+    siddon_trace_grid(n, d, c, src, dst, visit);
 }
 
 inline void siddon_ray(const Fan& g, double deg, int iu, int iv, double src[3], double dst[3]) {
@@ -887,6 +895,70 @@ void tomo_bp(T* img, const float* prj, const float* detCenter, const float* src,
         }
 }
 
+// --------------------------------------------------------------------------
+// Siddon cone pair with arbitrary per-view geometry:
+// SiddonConeProjectionAbitraryKernel / SiddonConeBackprojectionAbitraryKernel
+// (SiddonCone.cu:20-67).  Ray (iu, iview, iv) runs from src[iview] to
+// detCenter + u detU + v detV, u = (iu - off_u - (nu-1)/2) du,
+// v = (iv - off_v - (nv-1)/2) dv; each voxel receives the ray's length inside
+// it (mm), on the grid centred at (cx, cy, cz).  Moving the end points towards
+// the grid (MoveSourceDstNearGrid, SiddonParallel.cu:35-55) keeps the part of
+// the ray inside the grid, so it does not appear here.  The backprojection is
+// the exact transpose (the reference scatters with atomics).
+// --------------------------------------------------------------------------
+inline void cone_ray(const Tomo& g, const float* detCenter, const float* detU, const float* detV, const float* src,
+                     int iview, int iu, int iv, double s[3], double e[3]) {
+    const double u = (iu - g.off_u - (g.nu - 1) / 2.0) * g.du, v = (iv - g.off_v - (g.nv - 1) / 2.0) * g.dv;
+    for (int k = 0; k < 3; k++) {
+        s[k] = src[3 * iview + k];
+        e[k] = (double)detCenter[3 * iview + k] + (double)detU[3 * iview + k] * u + (double)detV[3 * iview + k] * v;
+    }
+}
+
+template <typename T>
+void cone_fp(T* prj, const float* img, const float* detCenter, const float* detU, const float* detV, const float* src,
+             const Tomo& g) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double d[3] = {g.dx, g.dy, g.dz}, c[3] = {g.cx, g.cy, g.cz};
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int b = 0; b < g.nb; b++)
+        for (int iu = 0; iu < g.nu; iu++)
+            for (int iview = 0; iview < g.nview; iview++)
+                for (int iv = 0; iv < g.nv; iv++) {
+                    double s[3], e[3];
+                    cone_ray(g, detCenter, detU, detV, src, iview, iu, iv, s, e);
+                    for (int ch = 0; ch < g.nc; ch++) {
+                        double val = 0;
+                        siddon_trace_grid(n, d, c, s, e, [&](int ix, int iy, int iz, double len) {
+                            val += len * img[((((size_t)b * g.nx + ix) * g.ny + iy) * g.nz + iz) * g.nc + ch];
+                        });
+                        prj[((((size_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + ch] = (T)val;
+                    }
+                }
+}
+
+template <typename T>
+void cone_bp(T* img, const float* prj, const float* detCenter, const float* detU, const float* detV, const float* src,
+             const Tomo& g) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double d[3] = {g.dx, g.dy, g.dz}, c[3] = {g.cx, g.cy, g.cz};
+    for (int b = 0; b < g.nb; b++)
+        for (int ch = 0; ch < g.nc; ch++) {
+            std::vector<double> acc((size_t)g.nx * g.ny * g.nz, 0.0);
+            for (int iu = 0; iu < g.nu; iu++)
+                for (int iview = 0; iview < g.nview; iview++)
+                    for (int iv = 0; iv < g.nv; iv++) {
+                        double s[3], e[3];
+                        cone_ray(g, detCenter, detU, detV, src, iview, iu, iv, s, e);
+                        const double w = prj[((((size_t)b * g.nu + iu) * g.nview + iview) * g.nv + iv) * g.nc + ch];
+                        siddon_trace_grid(n, d, c, s, e, [&](int ix, int iy, int iz, double len) {
+                            acc[((size_t)ix * g.ny + iy) * g.nz + iz] += w * len;
+                        });
+                    }
+            for (size_t i = 0; i < acc.size(); i++) img[(((size_t)b * g.nx * g.ny * g.nz) + i) * g.nc + ch] = (T)acc[i];
+        }
+}
+
 inline Fan make_fan(int nb, int nc, int nx, int ny, int nz, float dx, float dy, float dz, int nu, int nview, int nv,
                     float da, float dv, float off_a, float off_v, float dsd, float dso) {
     Fan g;
@@ -985,6 +1057,14 @@ void oracle_tv_iso_sqs_f64(double* s1, double* s2, double* var, const float* img
 }
 double oracle_tv_sqs_f64(double* grad, double* norm, const float* img, int nx, int ny) {
     return tv_sqs<double>(grad, norm, img, nx, ny);
+}
+void oracle_cone_fp_f64(double* prj, const float* img, const float* detCenter, const float* detU, const float* detV,
+                        const float* src, TOMO_ARGS) {
+    cone_fp<double>(prj, img, detCenter, detU, detV, src, make_tomo(TOMO_PASS));
+}
+void oracle_cone_bp_f64(double* img, const float* prj, const float* detCenter, const float* detU, const float* detV,
+                        const float* src, TOMO_ARGS) {
+    cone_bp<double>(img, prj, detCenter, detU, detV, src, make_tomo(TOMO_PASS));
 }
 void oracle_tomo_fp_f64(double* prj, const float* img, const float* detCenter, const float* src, TOMO_ARGS) {
     tomo_fp<double>(prj, img, detCenter, src, make_tomo(TOMO_PASS));

@@ -61,6 +61,8 @@ def lib():
         L.oracle_tv_sqs_f64.argtypes = [_dp, _dp, _fp, _i, _i]
         L.oracle_tv_sqs_f64.restype = ctypes.c_double
         L.oracle_tv_iso_sqs_f64.argtypes = [_dp, _dp, _dp, _fp, _i, _i, _i, _i, _i, ctypes.c_double, _i]
+        L.oracle_cone_fp_f64.argtypes = [_dp, _fp, _fp, _fp, _fp, _fp] + _TOMO
+        L.oracle_cone_bp_f64.argtypes = [_dp, _fp, _fp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_fp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO + [_i]
         _lib = L
@@ -212,6 +214,29 @@ def tv_iso_sqs(img, ndim, eps=1e-8):
     lib().oracle_tv_iso_sqs_f64(_ptr(s1, d), _ptr(s2, d), _ptr(var, d), _ptr(img, _f), nb, nx, ny, nz, nc,
                                 float(eps), int(ndim))
     return s1, s2, var
+
+
+def cone_fp(img, det_center, det_u, det_v, src, g, nu, nv):
+    """Siddon cone projection, arbitrary geometry (SiddonCone.cu:20-42)."""
+    img = _f32(img)
+    B, nx, ny, nz, C = img.shape
+    geo = [_f32(a).reshape(-1, 3) for a in (det_center, det_u, det_v, src)]
+    out = np.zeros((B, nu, geo[0].shape[0], nv, C), np.float64)
+    lib().oracle_cone_fp_f64(_ptr(out, ctypes.c_double), _ptr(img, _f), *[_ptr(a, _f) for a in geo],
+                             *_tomo_args(g, img.shape, out.shape))
+    return out
+
+
+def cone_bp(prj, det_center, det_u, det_v, src, g, img_shape):
+    """Transpose of ``cone_fp`` (SiddonCone.cu:44-67 scatters with atomics)."""
+    prj = _f32(prj)
+    B, nu, nview, nv, C = prj.shape
+    nx, ny, nz = img_shape
+    geo = [_f32(a).reshape(-1, 3) for a in (det_center, det_u, det_v, src)]
+    out = np.zeros((B, nx, ny, nz, C), np.float64)
+    lib().oracle_cone_bp_f64(_ptr(out, ctypes.c_double), _ptr(prj, _f), *[_ptr(a, _f) for a in geo],
+                             *_tomo_args(g, out.shape, prj.shape))
+    return out
 
 
 def _tomo_args(g, img_shape, prj_shape):

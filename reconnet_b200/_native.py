@@ -37,6 +37,14 @@ class RnFanGeom(ctypes.Structure):
                 ("du", _f), ("dv", _f), ("off_u", _f), ("off_v", _f), ("dsd", _f), ("dso", _f)]
 
 
+class RnConeGeom(ctypes.Structure):
+    """Mirror of ``RnConeGeom`` (the SiddonCone setup, ReconNet4D/SiddonCone.cu:126-201)."""
+    _fields_ = [("nBatches", _i), ("nChannels", _i), ("nx", _i), ("ny", _i), ("nz", _i),
+                ("dx", _f), ("dy", _f), ("dz", _f), ("cx", _f), ("cy", _f), ("cz", _f),
+                ("nu", _i), ("nview", _i), ("nv", _i),
+                ("du", _f), ("dv", _f), ("off_u", _f), ("off_v", _f)]
+
+
 class ReconNetError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"reconnet_b200 error {code}: {msg}")
@@ -69,6 +77,14 @@ SIGNATURES = {
     "rn_fan_plan_create_ragged": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnFanGeom),
                                        ctypes.POINTER(_i), _fp, _vp]),
     "rn_fan_plan_destroy": (_i, [_vp]),
+    "rn_cone_plan_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnConeGeom), _fp, _fp, _fp, _fp, _vp]),
+    "rn_cone_plan_destroy": (_i, [_vp]),
+    "rn_cone_project": (_i, [_vp, _vp, _vp, _vp]),
+    "rn_cone_backproject": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "rn_cone_plan_launches": (ctypes.c_longlong, [_vp]),
+    "cSiddonConeProjectionAbitrary": (None, [_fp] * 6 + _TOMO),
+    "cSiddonConeBackprojectionAbitrary": (None, [_fp] * 6 + _TOMO),
+    "cOSSQSConeAbitrary": (None, [_fp] * 9 + [_f, _f, _i, _i] + _TOMO + [_i, _f]),
     "rn_fan_plan_total_views": (ctypes.c_int64, [_vp]),
     "rn_fan_project": (_i, [_vp, _vp, _vp, _vp]),
     "rn_fan_project_siddon": (_i, [_vp, _vp, _vp, _vp]),

@@ -1,0 +1,640 @@
+// Siddon cone-beam projector pair with arbitrary per-view geometry
+// (SiddonCone.cu): ray (iu, iview, iv) runs from src[iview] to
+// detCenter + u detU + v detV, u = (iu - off_u - (nu-1)/2) du,
+// v = (iv - off_v - (nv-1)/2) dv, and each voxel of the grid centred at
+// (cx, cy, cz) receives the length (mm) of the ray inside it.
+//
+// Voxel coordinates put the origin at the corner of voxel 0
+// (PhysicsToImg, Siddon.cu:14-21).  Every view has a main axis m (the axis
+// along which its central ray advances most, in voxels) and lateral axes a,
+// b; a ray's lateral positions are affine in its main coordinate:
+// a(k) = S_a + (k - S_m) r_a, r_a = D_a / D_m.
+//
+// Forward projection: one thread per ray steps through the unit slabs
+// [k, k + 1] along m.  Inside a slab the ray crosses at most ceil|r_a| +
+// ceil|r_b| lateral grid lines (the host rejects views with |r| > 4), so the
+// slab splits into a few pieces of known voxel; each piece adds
+// (its share of the slab) x seg x the voxel value, seg being the ray's length
+// per slab.  Lateral positions are 64-bit fixed point (32 fractional bits,
+// stepped by an integer add), so the split points are exact to ~1e-7 slabs
+// however far the source is.
+//
+// Backprojection, the exact transpose as a gather (the reference scatters
+// with atomics): per voxel and view, the candidate rays are the detector
+// cells inside the voxel's shadow (its 8 corners projected through the
+// source, bounded by interval arithmetic); each candidate adds seg x its
+// sinogram value x the part of the voxel's main-axis extent over which it
+// lies inside the voxel laterally.  The ray's lateral offsets from the voxel
+// at the voxel's low main-axis face, x_a = (S_a - a_v) + (m_v - S_m) r_a, come
+// from hi / lo float parts with exact products, as in the fan Siddon
+// backprojection, to ~1e-7 voxels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "rn_internal.h"
+
+namespace rn {
+
+struct ConeView {
+    double S[3];              // source, voxel coordinates
+    double C[3];              // end point of ray (iu, iv) = (0, 0), voxel coordinates
+    double Eu[3], Ev[3];      // end-point step per detector index along u / v
+    float Sh[3], Sl[3];       // source as hi / lo floats
+    float au[4], av[4], ad[4];   // shadow: iu = (au . P + au[3]) / (ad . P + ad[3]), iv likewise
+    float ulo, uhi, vlo, vhi, dlo, dhi;   // sums of min(0, a_k) / max(0, a_k) over the three axes
+    int m, a, b, pad;
+};
+
+struct ConeDims {
+    int n[3];
+    float d[3];
+    long long st[3];          // image strides (elements) along x, y, z
+    int nc, nu, nv, nview, nb;
+    long long img_b, prj_b;   // batch strides
+};
+
+// Per ray (view, iv, iu) geometry for the backprojection:
+// {r_a hi, r_a lo, r_b hi, r_b lo}, {1 / r_a, 1 / r_b, seg, E_m}.
+__global__ void cone_ray_kernel(float4* __restrict__ rays, const ConeView* __restrict__ views, ConeDims cd) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)cd.nview * cd.nv * cd.nu;
+    if (i >= n) return;
+    const int iu = (int)(i % cd.nu);
+    const int iv = (int)((i / cd.nu) % cd.nv);
+    const int view = (int)(i / ((long long)cd.nu * cd.nv));
+    const ConeView& V = views[view];
+    double D[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) D[k] = V.C[k] + iu * V.Eu[k] + iv * V.Ev[k] - V.S[k];
+    const double Dm = D[V.m], ra = D[V.a] / Dm, rb = D[V.b] / Dm;
+    const double dm = cd.d[V.m], da = cd.d[V.a], db = cd.d[V.b];
+    const double seg = sqrt(dm * dm + ra * ra * da * da + rb * rb * db * db);
+    const float rah = (float)ra, rbh = (float)rb;
+    rays[2 * i] = make_float4(rah, (float)(ra - rah), rbh, (float)(rb - rbh));
+    rays[2 * i + 1] = make_float4(fabs(ra) > 1e-30 ? (float)(1.0 / ra) : 1e30f,
+                                  fabs(rb) > 1e-30 ? (float)(1.0 / rb) : 1e30f, (float)seg,
+                                  (float)(V.S[V.m] + Dm));
+}
+
+__device__ __forceinline__ long long to_fixed(double v) { return llrint(v * 4294967296.0); }
+
+// First crossing of a lateral axis inside the slab, in slab units, or 2 if
+// none: fixed-point position p at the slab start, nx crossings, slope sign,
+// |1 / r|.
+__device__ __forceinline__ float first_crossing(long long p, int nx, bool pos, float ir) {
+    if (nx == 0) return 2.f;
+    const float f = __uint2float_rn((unsigned)p) * 2.3283064365386963e-10f;   // fractional part
+    return (pos ? 1.f - f : f) * ir;
+}
+
+__global__ void __launch_bounds__(256) cone_fp_kernel(float* __restrict__ prj, const float* __restrict__ img,
+                                                       const ConeView* __restrict__ views, ConeDims cd) {
+    const int iu = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (iu >= cd.nu || iv >= cd.nv) return;
+    int zi = blockIdx.z;
+    const int c = zi % cd.nc;
+    zi /= cd.nc;
+    const int view = zi % cd.nview;
+    const int bt = zi / cd.nview;
+    const ConeView& V = views[view];
+    const int m = V.m, a = V.a, b = V.b;
+    double D[3], S[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        S[k] = V.S[k];
+        D[k] = V.C[k] + iu * V.Eu[k] + iv * V.Ev[k] - S[k];
+    }
+    float* out = prj + bt * cd.prj_b + (((long long)iu * cd.nview + view) * cd.nv + iv) * cd.nc + c;
+    // parameter range of the segment inside the grid
+    double t0 = 0.0, t1 = 1.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (fabs(D[k]) > 1e-12) {
+            const double ta = -S[k] / D[k], tb = (cd.n[k] - S[k]) / D[k];
+            t0 = fmax(t0, fmin(ta, tb));
+            t1 = fmin(t1, fmax(ta, tb));
+        } else if (S[k] < 0.0 || S[k] > cd.n[k]) {
+            t1 = -1.0;
+        }
+    }
+    if (t1 <= t0) {
+        *out = 0.f;
+        return;
+    }
+    const double Dm = D[m], ra = D[a] / Dm, rb = D[b] / Dm;
+    const double mlo = S[m] + fmin(t0 * Dm, t1 * Dm), mhi = S[m] + fmax(t0 * Dm, t1 * Dm);
+    const int k0 = max(0, (int)floor(mlo)), k1 = min(cd.n[m] - 1, (int)ceil(mhi) - 1);
+    const double dm = cd.d[m], da = cd.d[a], db = cd.d[b];
+    const float seg = (float)sqrt(dm * dm + ra * ra * da * da + rb * rb * db * db);
+    // the segment's own ends along m (the grid faces are handled by the
+    // voxel bounds), relative to slab k0
+    const double sm_lo = fmin(S[m], S[m] + Dm), sm_hi = fmax(S[m], S[m] + Dm);
+    const float slo = (float)fmax(sm_lo - k0, -1.0), shi = (float)fmin(sm_hi - k0, (double)(k1 - k0) + 2.0);
+    long long A = to_fixed(S[a] + (k0 - S[m]) * ra), B = to_fixed(S[b] + (k0 - S[m]) * rb);
+    const long long RA = to_fixed(ra), RB = to_fixed(rb);
+    const bool pa = ra > 0, pb = rb > 0;
+    const float ira = fabs(ra) > 1e-30 ? (float)(1.0 / fabs(ra)) : 1e30f;
+    const float irb = fabs(rb) > 1e-30 ? (float)(1.0 / fabs(rb)) : 1e30f;
+    const int sa = pa ? 1 : -1, sb = pb ? 1 : -1;
+    const int na_ = cd.n[a], nb_ = cd.n[b];
+    const long long sta = cd.st[a], stb = cd.st[b], stm = cd.st[m];
+    const float* base = img + bt * cd.img_b + c;
+    float acc = 0.f;
+    for (int k = k0; k <= k1; k++) {
+        const int j = k - k0;
+        const float tlo = fmaxf(0.f, slo - (float)j), thi = fminf(1.f, shi - (float)j);
+        const long long An = A + RA, Bn = B + RB;
+        int ca = (int)(A >> 32), cb = (int)(B >> 32);
+        int nxa = abs((int)(An >> 32) - ca), nxb = abs((int)(Bn >> 32) - cb);
+        float ta = first_crossing(A, nxa, pa, ira), tb = first_crossing(B, nxb, pb, irb);
+        const float* sl = base + (long long)k * stm;
+        float tcur = 0.f;
+        for (;;) {
+            const float tn = fminf(fminf(ta, tb), thi);
+            const float len = tn - fmaxf(tcur, tlo);
+            if (len > 0.f && (unsigned)ca < (unsigned)na_ && (unsigned)cb < (unsigned)nb_)
+                acc = fmaf(len, __ldg(sl + ca * sta + cb * stb), acc);
+            if (tn >= thi) break;
+            tcur = tn;
+            if (ta <= tb) {
+                ca += sa;
+                ta = (--nxa > 0) ? ta + ira : 2.f;
+            } else {
+                cb += sb;
+                tb = (--nxb > 0) ? tb + irb : 2.f;
+            }
+        }
+        A = An;
+        B = Bn;
+    }
+    *out = acc * seg;
+}
+
+__device__ __forceinline__ void two_sum_f(float a, float b, float& s, float& e) {
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// One thread per voxel (z fastest) of slice `bc` = b * nc + c.
+__global__ void __launch_bounds__(256) cone_bp_kernel(float* __restrict__ img, const float* __restrict__ prj,
+                                                       const float4* __restrict__ rays,
+                                                       const ConeView* __restrict__ views, ConeDims cd,
+                                                       int accumulate) {
+    const long long nvox = (long long)cd.n[0] * cd.n[1] * cd.n[2];
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nvox) return;
+    const int bc = blockIdx.y;
+    const int c = bc % cd.nc, bt = bc / cd.nc;
+    const int z = (int)(q % cd.n[2]);
+    const int y = (int)((q / cd.n[2]) % cd.n[1]);
+    const int x = (int)(q / ((long long)cd.n[2] * cd.n[1]));
+    const float P[3] = {(float)x, (float)y, (float)z};
+    const int pi[3] = {x, y, z};
+    const float* pb = prj + bt * cd.prj_b + c;
+    float acc = 0.f;
+    for (int view = 0; view < cd.nview; view++) {
+        const ConeView& V = views[view];
+        // shadow of the voxel [P, P + 1]^3 on the detector, in cell indices
+        const float nu0 = fmaf(V.au[0], P[0], fmaf(V.au[1], P[1], fmaf(V.au[2], P[2], V.au[3])));
+        const float nv0 = fmaf(V.av[0], P[0], fmaf(V.av[1], P[1], fmaf(V.av[2], P[2], V.av[3])));
+        const float nd0 = fmaf(V.ad[0], P[0], fmaf(V.ad[1], P[1], fmaf(V.ad[2], P[2], V.ad[3])));
+        const float dmin = nd0 + V.dlo, dmax = nd0 + V.dhi;
+        if (!(dmin > 0.f)) continue;
+        const float id0 = 1.f / dmin, id1 = 1.f / dmax;
+        const float ulo = nu0 + V.ulo, uhi = nu0 + V.uhi, vlo = nv0 + V.vlo, vhi = nv0 + V.vhi;
+        const int u0 = max(0, (int)ceilf(fminf(ulo * id0, ulo * id1) - 1e-3f));
+        const int u1 = min(cd.nu - 1, (int)floorf(fmaxf(uhi * id0, uhi * id1) + 1e-3f));
+        const int v0 = max(0, (int)ceilf(fminf(vlo * id0, vlo * id1) - 1e-3f));
+        const int v1 = min(cd.nv - 1, (int)floorf(fmaxf(vhi * id0, vhi * id1) + 1e-3f));
+        if (u0 > u1 || v0 > v1) continue;
+        // voxel offsets from the source as hi / lo: A = S - lateral index,
+        // M = main index - S_m
+        const int m = V.m, a = V.a, b = V.b;
+        float Ah, Al, Bh, Bl, Mh, Ml, e;
+        two_sum_f(V.Sh[a], -(float)pi[a], Ah, e);
+        Al = e + V.Sl[a];
+        two_sum_f(V.Sh[b], -(float)pi[b], Bh, e);
+        Bl = e + V.Sl[b];
+        two_sum_f((float)pi[m], -V.Sh[m], Mh, e);
+        Ml = e - V.Sl[m];
+        const float sm = (float)pi[m] - V.Sh[m] - V.Sl[m];   // main index - S_m (segment clipping only)
+        for (int iv = v0; iv <= v1; iv++) {
+            const long long rrow = ((long long)view * cd.nv + iv) * cd.nu;
+            const float* prow = pb + ((long long)view * cd.nv + iv) * cd.nc;
+            for (int iu = u0; iu <= u1; iu++) {
+                const float4 g0 = __ldg(rays + 2 * (rrow + iu));
+                const float4 g1 = __ldg(rays + 2 * (rrow + iu) + 1);
+                const float xa = fmaf(g0.x, Mh, Ah) + fmaf(g0.y, Mh, fmaf(g0.x, Ml, Al));
+                const float xb = fmaf(g0.z, Mh, Bh) + fmaf(g0.w, Mh, fmaf(g0.z, Ml, Bl));
+                const float ta0 = -xa * g1.x, ta1 = (1.f - xa) * g1.x;
+                const float tb0 = -xb * g1.y, tb1 = (1.f - xb) * g1.y;
+                // the segment's ends along m: source (at -sm from the voxel's
+                // low face) and end point E_m
+                const float e0 = -sm, e1 = g1.w - (float)pi[m];
+                const float tl = fmaxf(fmaxf(fmaxf(0.f, fminf(ta0, ta1)), fminf(tb0, tb1)), fminf(e0, e1));
+                const float th = fminf(fminf(fminf(1.f, fmaxf(ta0, ta1)), fmaxf(tb0, tb1)), fmaxf(e0, e1));
+                if (th > tl) acc = fmaf((th - tl) * g1.z, __ldg(prow + (long long)iu * cd.nview * cd.nv * cd.nc), acc);
+            }
+        }
+    }
+    float* o = img + bt * cd.img_b + ((long long)x * cd.st[0] + (long long)y * cd.st[1] + (long long)z * cd.st[2]) + c;
+    *o = accumulate ? *o + acc : acc;
+}
+
+}  // namespace rn
+
+using namespace rn;
+
+struct rn_cone_plan {
+    ConeDims cd;
+    int device = 0;
+    ConeView* d_views = nullptr;
+    float4* d_rays = nullptr;
+    long long launches = 0;
+};
+
+namespace {
+
+int cone_views(rn_cone_plan* p, const RnConeGeom& g, const float* dc, const float* du_, const float* dv_,
+               const float* src, std::vector<ConeView>& out) {
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double d[3] = {g.dx, g.dy, g.dz}, cen[3] = {g.cx, g.cy, g.cz};
+    const double u0 = g.off_u + (g.nu - 1) / 2.0, v0 = g.off_v + (g.nv - 1) / 2.0;
+    out.resize(g.nview);
+    for (int iv = 0; iv < g.nview; iv++) {
+        ConeView V;
+        memset(&V, 0, sizeof(V));
+        for (int k = 0; k < 3; k++) {
+            V.S[k] = ((double)src[3 * iv + k] - cen[k]) / d[k] + n[k] / 2.0;
+            V.Eu[k] = (double)du_[3 * iv + k] * g.du / d[k];
+            V.Ev[k] = (double)dv_[3 * iv + k] * g.dv / d[k];
+            V.C[k] = ((double)dc[3 * iv + k] - u0 * g.du * du_[3 * iv + k] - v0 * g.dv * dv_[3 * iv + k] - cen[k]) / d[k] +
+                     n[k] / 2.0;
+            V.Sh[k] = (float)V.S[k];
+            V.Sl[k] = (float)(V.S[k] - (double)V.Sh[k]);
+        }
+        // main axis: the largest advance of the central ray, in voxels
+        double Dc[3];
+        for (int k = 0; k < 3; k++) Dc[k] = V.C[k] + (g.nu - 1) / 2.0 * V.Eu[k] + (g.nv - 1) / 2.0 * V.Ev[k] - V.S[k];
+        int m = 0;
+        for (int k = 1; k < 3; k++)
+            if (std::fabs(Dc[k]) > std::fabs(Dc[m])) m = k;
+        V.m = m;
+        V.a = (m + 1) % 3;
+        V.b = (m + 2) % 3;
+        if (V.a > V.b) std::swap(V.a, V.b);
+        // every ray must advance along m, with lateral slopes of at most 4
+        for (int corner = 0; corner < 4; corner++) {
+            const double iu = (corner & 1) ? g.nu - 1 : 0, ivv = (corner & 2) ? g.nv - 1 : 0;
+            double D[3];
+            for (int k = 0; k < 3; k++) D[k] = V.C[k] + iu * V.Eu[k] + ivv * V.Ev[k] - V.S[k];
+            if (D[m] * Dc[m] <= 0.0 || std::fabs(D[V.a]) > 4.0 * std::fabs(D[m]) ||
+                std::fabs(D[V.b]) > 4.0 * std::fabs(D[m]))
+                return set_error(RN_ERR_ARG, "cone geometry: rays of one view too oblique to a common main axis");
+        }
+        // shadow: the ray from S through P meets the detector plane at
+        // index (iu, iv); with W = P - S and the plane normal nrm (oriented
+        // so that K = nrm . (C - S) > 0), iu = (alpha_u . W) / (nrm . W)
+        double nrm[3] = {V.Eu[1] * V.Ev[2] - V.Eu[2] * V.Ev[1], V.Eu[2] * V.Ev[0] - V.Eu[0] * V.Ev[2],
+                         V.Eu[0] * V.Ev[1] - V.Eu[1] * V.Ev[0]};
+        double K = 0;
+        for (int k = 0; k < 3; k++) K += nrm[k] * (V.C[k] - V.S[k]);
+        if (std::fabs(K) < 1e-12) return set_error(RN_ERR_ARG, "cone geometry: source in the detector plane");
+        if (K < 0) {
+            for (int k = 0; k < 3; k++) nrm[k] = -nrm[k];
+            K = -K;
+        }
+        auto cross = [](const double* x, const double* y, double* r) {
+            r[0] = x[1] * y[2] - x[2] * y[1];
+            r[1] = x[2] * y[0] - x[0] * y[2];
+            r[2] = x[0] * y[1] - x[1] * y[0];
+        };
+        double gu[3], gv[3];
+        cross(V.Ev, nrm, gu);
+        double su = 0;
+        for (int k = 0; k < 3; k++) su += V.Eu[k] * gu[k];
+        for (int k = 0; k < 3; k++) gu[k] /= su;
+        cross(nrm, V.Eu, gv);
+        double sv = 0;
+        for (int k = 0; k < 3; k++) sv += V.Ev[k] * gv[k];
+        for (int k = 0; k < 3; k++) gv[k] /= sv;
+        double scu = 0, scv = 0;   // (S - C) . g
+        for (int k = 0; k < 3; k++) {
+            scu += (V.S[k] - V.C[k]) * gu[k];
+            scv += (V.S[k] - V.C[k]) * gv[k];
+        }
+        double au[3], av[3], bu = 0, bv = 0, bd = 0;
+        for (int k = 0; k < 3; k++) {
+            au[k] = scu * nrm[k] + K * gu[k];
+            av[k] = scv * nrm[k] + K * gv[k];
+            bu -= au[k] * V.S[k];
+            bv -= av[k] * V.S[k];
+            bd -= nrm[k] * V.S[k];
+        }
+        for (int k = 0; k < 3; k++) {
+            V.au[k] = (float)au[k];
+            V.av[k] = (float)av[k];
+            V.ad[k] = (float)nrm[k];
+            V.ulo += (float)std::min(0.0, au[k]);
+            V.uhi += (float)std::max(0.0, au[k]);
+            V.vlo += (float)std::min(0.0, av[k]);
+            V.vhi += (float)std::max(0.0, av[k]);
+            V.dlo += (float)std::min(0.0, nrm[k]);
+            V.dhi += (float)std::max(0.0, nrm[k]);
+        }
+        V.au[3] = (float)bu;
+        V.av[3] = (float)bv;
+        V.ad[3] = (float)bd;
+        out[iv] = V;
+    }
+    (void)p;
+    return RN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rn_cone_plan_create(rn_cone_plan** out, const RnConeGeom* g, const float* host_detCenter, const float* host_detU,
+                        const float* host_detV, const float* host_src, void* stream) {
+    clear_error();
+    if (!out || !g || !host_detCenter || !host_detU || !host_detV || !host_src)
+        return set_error(RN_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (g->nBatches <= 0 || g->nChannels <= 0 || g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->nu <= 0 ||
+        g->nview <= 0 || g->nv <= 0)
+        return set_error(RN_ERR_ARG, "cone geometry: sizes must be positive");
+    if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0) || !(g->du > 0) || !(g->dv > 0))
+        return set_error(RN_ERR_ARG, "cone geometry: pixel sizes must be positive");
+    if (g->nx > (1 << 20) || g->ny > (1 << 20) || g->nz > (1 << 20))
+        return set_error(RN_ERR_ARG, "cone geometry: grid too large");
+    rn_cone_plan* p = new rn_cone_plan();
+    cudaGetDevice(&p->device);
+    ConeDims& cd = p->cd;
+    cd.n[0] = g->nx;
+    cd.n[1] = g->ny;
+    cd.n[2] = g->nz;
+    cd.d[0] = g->dx;
+    cd.d[1] = g->dy;
+    cd.d[2] = g->dz;
+    cd.nc = g->nChannels;
+    cd.st[2] = cd.nc;
+    cd.st[1] = (long long)g->nz * cd.nc;
+    cd.st[0] = (long long)g->ny * cd.st[1];
+    cd.nu = g->nu;
+    cd.nv = g->nv;
+    cd.nview = g->nview;
+    cd.nb = g->nBatches;
+    cd.img_b = (long long)g->nx * cd.st[0];
+    cd.prj_b = (long long)g->nu * g->nview * g->nv * cd.nc;
+    std::vector<ConeView> views;
+    int s = cone_views(p, *g, host_detCenter, host_detU, host_detV, host_src, views);
+    if (s != RN_OK) {
+        delete p;
+        return s;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long nrays = (long long)g->nview * g->nv * g->nu;
+    cudaError_t e = cudaMalloc(&p->d_views, sizeof(ConeView) * views.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_rays, sizeof(float4) * 2 * nrays);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p->d_views, views.data(), sizeof(ConeView) * views.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        cone_ray_kernel<<<(unsigned)((nrays + 255) / 256), 256, 0, st>>>(p->d_rays, p->d_views, cd);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // `views` goes out of scope
+    if (e != cudaSuccess) {
+        rn_cone_plan_destroy(p);
+        return set_cuda_error(e, "rn_cone_plan_create");
+    }
+    *out = p;
+    return RN_OK;
+}
+
+int rn_cone_plan_destroy(rn_cone_plan* p) {
+    if (!p) return RN_OK;
+    cudaFree(p->d_views);
+    cudaFree(p->d_rays);
+    delete p;
+    return RN_OK;
+}
+
+int rn_cone_project(rn_cone_plan* p, float* d_prj, const float* d_img, void* stream) {
+    clear_error();
+    if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
+    const ConeDims& cd = p->cd;
+    const long long nz = (long long)cd.nb * cd.nview * cd.nc;
+    if (nz > 65535) return set_error(RN_ERR_ARG, "cone projection: more than 65535 views x batches x channels");
+    dim3 grid((cd.nu + 31) / 32, (cd.nv + 7) / 8, (unsigned)nz);
+    cone_fp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd);
+    p->launches++;
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+int rn_cone_backproject(rn_cone_plan* p, float* d_img, const float* d_prj, int accumulate, void* stream) {
+    clear_error();
+    if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
+    const ConeDims& cd = p->cd;
+    const long long nvox = (long long)cd.n[0] * cd.n[1] * cd.n[2];
+    const int slices = cd.nb * cd.nc;
+    if (slices > 65535) return set_error(RN_ERR_ARG, "cone backprojection: too many batches x channels");
+    dim3 grid((unsigned)((nvox + 255) / 256), slices);
+    cone_bp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_rays, p->d_views, cd, accumulate);
+    p->launches++;
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+long long rn_cone_plan_launches(const rn_cone_plan* p) { return p ? p->launches : 0; }
+
+}  // extern "C"
+
+namespace rn {
+
+// r = a - b (cone OS-SQS residual, no weights: ossqs.cu:281-287).
+__global__ void cone_residual_kernel(float* __restrict__ r, const float* __restrict__ b, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        r[i] -= b[i];
+}
+
+// x = clamp(mask (x - lm bp / (norm + 1e-6)), lb, ub): Divide2D, Minus2D,
+// Multiply2D and ValueCrop2D of ossqs.cu:299-316 in one pass.
+__global__ void cone_sqs_kernel(float* __restrict__ x, const float* __restrict__ bp, const float* __restrict__ norm,
+                                const float* __restrict__ mask, float lm, float lb, float ub, int clamp, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float v = (x[i] - lm * (bp[i] / (norm[i] + 1e-6f))) * mask[i];
+        if (clamp) v = fminf(fmaxf(v, lb), ub);
+        x[i] = v;
+    }
+}
+
+static RnConeGeom cone_geom(int nBatches, int nChannels, int nx, int ny, int nz, float dx, float dy, float dz, float cx,
+                            float cy, float cz, int nu, int nview, int nv, float du, float dv, float off_u,
+                            float off_v) {
+    RnConeGeom g;
+    g.nBatches = nBatches;
+    g.nChannels = nChannels;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.dx = dx;
+    g.dy = dy;
+    g.dz = dz;
+    g.cx = cx;
+    g.cy = cy;
+    g.cz = cz;
+    g.nu = nu;
+    g.nview = nview;
+    g.nv = nv;
+    g.du = du;
+    g.dv = dv;
+    g.off_u = off_u;
+    g.off_v = off_v;
+    return g;
+}
+
+// Device buffers of one host call, freed on every path.
+struct HostBufs {
+    std::vector<void*> ptrs;
+    template <class T>
+    int get(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaMalloc");
+        ptrs.push_back(q);
+        *p = reinterpret_cast<T*>(q);
+        return RN_OK;
+    }
+    ~HostBufs() {
+        for (void* q : ptrs) cudaFree(q);
+    }
+};
+
+static int cone_host(bool forward, float* out, const float* in, const float* dc, const float* du_, const float* dv_,
+                     const float* src, const RnConeGeom& g) {
+    const size_t ni = (size_t)g.nBatches * g.nx * g.ny * g.nz * g.nChannels;
+    const size_t np = (size_t)g.nBatches * g.nu * g.nview * g.nv * g.nChannels;
+    rn_cone_plan* p = nullptr;
+    RN_TRY(rn_cone_plan_create(&p, &g, dc, du_, dv_, src, nullptr));
+    HostBufs hb;
+    float *dimg = nullptr, *dprj = nullptr;
+    int s = hb.get(&dimg, ni);
+    if (s == RN_OK) s = hb.get(&dprj, np);
+    if (s == RN_OK) {
+        cudaError_t e = forward ? cudaMemcpy(dimg, in, ni * 4, cudaMemcpyHostToDevice)
+                                : cudaMemcpy(dprj, in, np * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) s = set_cuda_error(e, "copy to device");
+    }
+    if (s == RN_OK) s = forward ? rn_cone_project(p, dprj, dimg, nullptr) : rn_cone_backproject(p, dimg, dprj, 0, nullptr);
+    if (s == RN_OK) {
+        cudaError_t e = forward ? cudaMemcpy(out, dprj, np * 4, cudaMemcpyDeviceToHost)
+                                : cudaMemcpy(out, dimg, ni * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) s = set_cuda_error(e, "copy to host");
+    }
+    rn_cone_plan_destroy(p);
+    return s;
+}
+
+}  // namespace rn
+
+extern "C" {
+
+void cSiddonConeProjectionAbitrary(float* prj, const float* img, const float* detCenter, const float* detU,
+                                   const float* detV, const float* src, int nBatches, int nChannels, int nx, int ny,
+                                   int nz, float dx, float dy, float dz, float cx, float cy, float cz, int nu,
+                                   int nview, int nv, float du, float dv, float off_u, float off_v) {
+    clear_error();
+    if (!prj || !img) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    cone_host(true, prj, img, detCenter, detU, detV, src,
+              cone_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nview, nv, du, dv, off_u, off_v));
+}
+
+void cSiddonConeBackprojectionAbitrary(float* img, const float* prj, const float* detCenter, const float* detU,
+                                       const float* detV, const float* src, int nBatches, int nChannels, int nx,
+                                       int ny, int nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                                       int nu, int nview, int nv, float du, float dv, float off_u, float off_v) {
+    clear_error();
+    if (!prj || !img) {
+        set_error(RN_ERR_ARG, "null argument");
+        return;
+    }
+    cone_host(false, img, prj, detCenter, detU, detV, src,
+              cone_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nview, nv, du, dv, off_u, off_v));
+}
+
+void cOSSQSConeAbitrary(float* res, const float* img, const float* prj, const float* normImg, const float* mask,
+                        const float* detCenter, const float* detU, const float* detV, const float* src, float lb,
+                        float ub, int nviewPerSubset, int nSubsets, int nBatches, int nChannels, int nx, int ny,
+                        int nz, float dx, float dy, float dz, float cx, float cy, float cz, int nu, int nview, int nv,
+                        float du, float dv, float off_u, float off_v, int typeProjector, float lambda) {
+    (void)typeProjector;
+    clear_error();
+    if (!res || !img || !prj || !normImg || !mask || !detCenter || !detU || !detV || !src || nviewPerSubset <= 0 ||
+        nSubsets <= 0) {
+        set_error(RN_ERR_ARG, "cOSSQSConeAbitrary: bad argument");
+        return;
+    }
+    const size_t ni = (size_t)nBatches * nx * ny * nz * nChannels;
+    const size_t rowC = (size_t)nv * nChannels;
+    HostBufs hb;
+    float *x = nullptr, *dn = nullptr, *dm = nullptr, *bp = nullptr, *fp = nullptr, *ps = nullptr;
+    const size_t nsmax = (size_t)nBatches * nu * nviewPerSubset * rowC;
+    if (hb.get(&x, ni) || hb.get(&dn, ni) || hb.get(&dm, ni) || hb.get(&bp, ni) || hb.get(&fp, nsmax) ||
+        hb.get(&ps, nsmax))
+        return;
+    if (cudaMemcpy(x, img, ni * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dn, normImg, ni * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dm, mask, ni * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_error(RN_ERR_CUDA, "cOSSQSConeAbitrary: copy failed");
+        return;
+    }
+    std::vector<float> hs;
+    int start = 0;
+    for (int k = 0; k < nSubsets && start < nview; k++) {
+        const int cnt = std::min(nviewPerSubset, nview - start);
+        RnConeGeom g = cone_geom(nBatches, nChannels, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, cnt, nv, du, dv, off_u,
+                                 off_v);
+        rn_cone_plan* p = nullptr;
+        if (rn_cone_plan_create(&p, &g, detCenter + 3 * start, detU + 3 * start, detV + 3 * start, src + 3 * start,
+                                nullptr) != RN_OK)
+            return;
+        const size_t ns = (size_t)nBatches * nu * cnt * rowC;
+        hs.resize(ns);
+        for (int b = 0; b < nBatches; b++)
+            for (int u = 0; u < nu; u++)
+                memcpy(&hs[((size_t)b * nu + u) * cnt * rowC], prj + (((size_t)b * nu + u) * nview + start) * rowC,
+                       sizeof(float) * cnt * rowC);
+        int s = RN_OK;
+        if (cudaMemcpy(ps, hs.data(), ns * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+            s = set_error(RN_ERR_CUDA, "cOSSQSConeAbitrary: copy failed");
+        if (s == RN_OK) s = rn_cone_project(p, fp, x, nullptr);
+        if (s == RN_OK) {
+            cone_residual_kernel<<<(unsigned)std::min<size_t>((ns + 255) / 256, 148 * 16), 256>>>(fp, ps, (long long)ns);
+            s = rn_cone_backproject(p, bp, fp, 0, nullptr);
+        }
+        if (s == RN_OK) {
+            cone_sqs_kernel<<<(unsigned)std::min<size_t>((ni + 255) / 256, 148 * 16), 256>>>(
+                x, bp, dn, dm, lambda * nSubsets, lb, ub, lb < ub ? 1 : 0, (long long)ni);
+            cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) s = set_cuda_error(e, "cOSSQSConeAbitrary");
+        }
+        rn_cone_plan_destroy(p);
+        if (s != RN_OK) return;
+        start += cnt;
+    }
+    if (cudaMemcpy(res, x, ni * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        set_error(RN_ERR_CUDA, "cOSSQSConeAbitrary: copy failed");
+}
+
+}  // extern "C"

@@ -328,6 +328,55 @@ class ReconNet:
         fp = self.cDDTomoProjection4d(img * mask, detCenter, src)
         return self.cDDTomoBackprojection4d(fp, detCenter, src) * mask
 
+    # ---- Siddon cone pair, arbitrary geometry (python/ReconNet_no_tf.py:503-610) ----
+    def cSiddonConeProjectionAbitrary4d(self, img, detCenter, detU, detV, src):
+        img = np.ascontiguousarray(img, np.float32)
+        geo = [np.ascontiguousarray(a, np.float32) for a in (detCenter, detU, detV, src)]
+        prj = np.zeros([img.shape[0], self.nu, geo[0].shape[0], self.nv, img.shape[-1]], np.float32)
+        N.lib.cSiddonConeProjectionAbitrary(_fptr(prj), _fptr(img), *[_fptr(a) for a in geo],
+                                            *self._tomo_args(img.shape, prj.shape))
+        N.check_last()
+        return prj
+
+    def cSiddonConeBackprojectionAbitrary4d(self, prj, detCenter, detU, detV, src):
+        prj = np.ascontiguousarray(prj, np.float32)
+        geo = [np.ascontiguousarray(a, np.float32) for a in (detCenter, detU, detV, src)]
+        img = np.zeros([prj.shape[0], self.nx, self.ny, self.nz, prj.shape[-1]], np.float32)
+        N.lib.cSiddonConeBackprojectionAbitrary(_fptr(img), _fptr(prj), *[_fptr(a) for a in geo],
+                                                *self._tomo_args(img.shape, prj.shape))
+        N.check_last()
+        return img
+
+    def cSiddonConeNormImgAbitrary4d(self, prj, detCenter, detU, detV, src, mask=None):
+        img = np.ones([prj.shape[0], self.nx, self.ny, self.nz, prj.shape[-1]], np.float32)
+        if mask is None:
+            mask = np.ones_like(img)
+        fp = self.cSiddonConeProjectionAbitrary4d(img * mask, detCenter, detU, detV, src)
+        return self.cSiddonConeBackprojectionAbitrary4d(fp, detCenter, detU, detV, src) * mask
+
+    def cSiddonConeAbitraryOSSQS4d(self, nSubsets, img, prj, normImg, detCenter, detU, detV, src, mask=None,
+                                   order=None, lb=None, ub=None, lam=1):
+        img = np.ascontiguousarray(img, np.float32)
+        prj = np.asarray(prj, np.float32)
+        normImg = np.ascontiguousarray(normImg, np.float32)
+        geo = [np.asarray(a, np.float32) for a in (detCenter, detU, detV, src)]
+        mask = np.ones(img.shape, np.float32) if mask is None else np.ascontiguousarray(mask, np.float32)
+        nviewPerSubset = int(np.ceil(prj.shape[2] / float(nSubsets)))
+        lb = np.finfo(np.float32).min if lb is None else lb
+        ub = np.finfo(np.float32).max if ub is None else ub
+        if order is not None:
+            prj = prj[:, :, order, :, :]
+            geo = [a[order, ...] for a in geo]
+        prj = np.ascontiguousarray(prj, np.float32)
+        geo = [np.ascontiguousarray(a, np.float32) for a in geo]
+        res = np.zeros(img.shape, np.float32)
+        B, nx, ny, nz, C = img.shape
+        N.lib.cOSSQSConeAbitrary(_fptr(res), _fptr(img), _fptr(prj), _fptr(normImg), _fptr(mask),
+                                 *[_fptr(a) for a in geo], float(lb), float(ub), nviewPerSubset, int(nSubsets),
+                                 *self._tomo_args(img.shape, prj.shape), 2, float(lam))
+        N.check_last()
+        return res
+
     # ---- TV surrogate (TotalVariation.cu:70) ----
     def cTVSQS2d(self, img):
         img = np.ascontiguousarray(img, np.float32)

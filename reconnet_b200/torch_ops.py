@@ -314,6 +314,87 @@ def filter_sino(sino: torch.Tensor, geom: FanGeometry, type_filter: int = 0, fan
     return out
 
 
+@dataclass
+class ConeGeometry:
+    """Cone-beam grid and detector (the SiddonCone setup, SiddonCone.cu:126-201):
+    grid of nx x ny x nz voxels (dx, dy, dz mm) centred at (cx, cy, cz);
+    detector of nu x nv cells (du, dv mm) with offsets off_u, off_v in cells."""
+    nx: int = 512
+    ny: int = 512
+    nz: int = 128
+    dx: float = 0.8
+    dy: float = 0.8
+    dz: float = 1.0
+    cx: float = 0.0
+    cy: float = 0.0
+    cz: float = 0.0
+    nu: int = 736
+    nv: int = 736
+    du: float = 0.6
+    dv: float = 0.6
+    off_u: float = 0.0
+    off_v: float = 0.0
+
+    def native(self, nbatches: int, nchannels: int, nview: int) -> N.RnConeGeom:
+        g = N.RnConeGeom()
+        g.nBatches, g.nChannels = nbatches, nchannels
+        g.nx, g.ny, g.nz = self.nx, self.ny, self.nz
+        g.dx, g.dy, g.dz, g.cx, g.cy, g.cz = self.dx, self.dy, self.dz, self.cx, self.cy, self.cz
+        g.nu, g.nview, g.nv = self.nu, nview, self.nv
+        g.du, g.dv, g.off_u, g.off_v = self.du, self.dv, self.off_u, self.off_v
+        return g
+
+
+class ConePlan:
+    """Siddon cone-beam pair with arbitrary per-view geometry on CUDA tensors:
+    image ``[B, nx, ny, nz, C]``, projections ``[B, nu, nview, nv, C]``;
+    ``det_center``, ``det_u``, ``det_v``, ``src`` are ``[nview, 3]`` (mm).
+    ``project`` traces ray lengths (SiddonCone.cu:20-42), ``backproject`` is
+    its exact transpose."""
+
+    def __init__(self, geom: ConeGeometry, det_center, det_u, det_v, src, nbatches: int = 1, nchannels: int = 1,
+                 device=None):
+        self.geom = geom
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        geo = [np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1, 3)) for a in (det_center, det_u, det_v, src)]
+        self.nview = geo[0].shape[0]
+        self.nbatches, self.nchannels = int(nbatches), int(nchannels)
+        self._plan = ctypes.c_void_p()
+        g = geom.native(self.nbatches, self.nchannels, self.nview)
+        fp = ctypes.POINTER(ctypes.c_float)
+        with torch.cuda.device(self.device):
+            N.check(N.lib.rn_cone_plan_create(ctypes.byref(self._plan), ctypes.byref(g),
+                                              *[a.ctypes.data_as(fp) for a in geo], _stream_ptr(self.device)))
+        self.img_shape = (self.nbatches, geom.nx, geom.ny, geom.nz, self.nchannels)
+        self.prj_shape = (self.nbatches, geom.nu, self.nview, geom.nv, self.nchannels)
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            N.lib.rn_cone_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def project(self, img: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if tuple(img.shape) != self.img_shape:
+            raise ValueError(f"image shape {tuple(img.shape)} != {self.img_shape}")
+        if out is None:
+            out = torch.empty(self.prj_shape, dtype=torch.float32, device=img.device)
+        N.check(N.lib.rn_cone_project(self._plan, _dev_ptr(out), _dev_ptr(img), _stream_ptr(img.device)))
+        return out
+
+    def backproject(self, prj: torch.Tensor, out: Optional[torch.Tensor] = None,
+                    accumulate: bool = False) -> torch.Tensor:
+        if tuple(prj.shape) != self.prj_shape:
+            raise ValueError(f"projection shape {tuple(prj.shape)} != {self.prj_shape}")
+        if out is None:
+            out = torch.empty(self.img_shape, dtype=torch.float32, device=prj.device)
+        N.check(N.lib.rn_cone_backproject(self._plan, _dev_ptr(out), _dev_ptr(prj), int(bool(accumulate)),
+                                          _stream_ptr(prj.device)))
+        return out
+
+    def launches(self) -> int:
+        return int(N.lib.rn_cone_plan_launches(self._plan))
+
+
 def fbp(sino: torch.Tensor, plan: "FanPlan", geom: FanGeometry, type_filter: int = 0,
         weights: Optional[torch.Tensor] = None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Fan-beam FBP on the device: optional short-scan weights (Parker /

@@ -12,6 +12,7 @@ these files.
     python tests/golden/make_golden.py --ossqs [outdir]    (cOSSQS only)
     python tests/golden/make_golden.py --pixel [outdir]    (pixel-driven backprojection only)
     python tests/golden/make_golden.py --prior [outdir]    (the prior solver's TV, oracle/_ref/libprior_ref.so)
+    python tests/golden/make_golden.py --cone [outdir]     (the Siddon cone pair and cone OS-SQS)
 """
 import ctypes
 import math
@@ -47,6 +48,11 @@ def load_ref(path=REF):
         lib.cSiddonFanBackprojection.argtypes = fan
     if hasattr(lib, "cPixelDrivenFanBackprojection"):
         lib.cPixelDrivenFanBackprojection.argtypes = fan
+    if hasattr(lib, "cSiddonConeProjectionAbitrary"):
+        lib.cSiddonConeProjectionAbitrary.argtypes = [_fp] * 6 + tomo[4:]
+        lib.cSiddonConeBackprojectionAbitrary.argtypes = [_fp] * 6 + tomo[4:]
+    if hasattr(lib, "cOSSQSConeAbitrary"):
+        lib.cOSSQSConeAbitrary.argtypes = [_fp] * 9 + [_f, _f, _i, _i] + tomo[4:] + [_i, _f]
     if hasattr(lib, "cOSSQS"):
         lib.cOSSQS.argtypes = [_fp] * 6 + [_f, _f, _i, _i] + fan[3:-1] + [_i, _f]
     return lib
@@ -171,6 +177,90 @@ def pixel_case(lib, rng):
     return out
 
 
+def cone_geometry(name):
+    """Grid, detector and per-view geometry ([nview, 3] arrays, mm) of the
+    cone test cases: a tomosynthesis arc (rays mostly along z), a circular
+    cone-beam scan whose views cross 45 degrees (the main axis switches
+    between x and y), and a tilted, off-centre detector."""
+    if name == "cone_tomo":
+        g = dict(nx=14, ny=12, nz=6, dx=1.0, dy=0.9, dz=1.5, cx=0.4, cy=-0.3, cz=0.2, nu=20, nv=18, du=1.2,
+                 dv=1.1, off_u=0.3, off_v=-0.4)
+        nview = 7
+        src = np.zeros((nview, 3), np.float32)
+        dc = np.zeros((nview, 3), np.float32)
+        for k in range(nview):
+            a = (k - (nview - 1) / 2) * 0.12
+            src[k] = (400 * math.sin(a), 6.0, 400 * math.cos(a))
+            dc[k] = (1.0, -0.5, -30.0)
+        du = np.tile(np.float32([1, 0, 0]), (nview, 1))
+        dv = np.tile(np.float32([0, 1, 0]), (nview, 1))
+    elif name == "cone_circular":
+        g = dict(nx=12, ny=13, nz=5, dx=1.0, dy=1.0, dz=1.2, cx=0.0, cy=0.5, cz=-0.3, nu=24, nv=8, du=1.5,
+                 dv=1.4, off_u=0.2, off_v=0.1)
+        nview = 9
+        ang = np.arange(nview) * (2 * np.pi / nview) + np.pi / 4 - 0.01
+        src = np.stack([300 * np.cos(ang), 300 * np.sin(ang), np.full(nview, 1.0)], 1).astype(np.float32)
+        dc = np.stack([-250 * np.cos(ang), -250 * np.sin(ang), np.full(nview, 1.0)], 1).astype(np.float32)
+        du = np.stack([-np.sin(ang), np.cos(ang), np.zeros(nview)], 1).astype(np.float32)
+        dv = np.tile(np.float32([0, 0, 1]), (nview, 1))
+    else:   # cone_tilted
+        g = dict(nx=10, ny=11, nz=9, dx=1.1, dy=1.0, dz=0.9, cx=0.0, cy=0.0, cz=0.0, nu=16, nv=15, du=1.4,
+                 dv=1.3, off_u=-0.6, off_v=0.25)
+        nview = 5
+        src = np.zeros((nview, 3), np.float32)
+        dc = np.zeros((nview, 3), np.float32)
+        du = np.zeros((nview, 3), np.float32)
+        dv = np.zeros((nview, 3), np.float32)
+        for k in range(nview):
+            t = 0.3 * (k - 2)
+            src[k] = (50 * math.sin(t), 320 * math.cos(0.2 * k), 20.0)
+            dc[k] = (-3.0, -150.0, -10.0)
+            # u mostly along x, v mostly along z: the plane faces the source (y)
+            u = np.array([math.cos(0.15), 0.05, math.sin(0.15)])
+            u /= np.linalg.norm(u)
+            v = np.cross(u, np.array([0.1, 1.0, 0.05]))
+            du[k] = u
+            dv[k] = v / np.linalg.norm(v)
+    return g, dc, du, dv, src
+
+
+CONE_CASES = ("cone_tomo", "cone_circular", "cone_tilted")
+
+
+def cone_case(lib, rng):
+    """cSiddonConeProjectionAbitrary / ...BackprojectionAbitrary
+    (SiddonCone.cu:126-278) and cOSSQSConeAbitrary (ossqs.cu:163-333)."""
+    out = {}
+    for name in CONE_CASES:
+        g, dc, du, dv, src = cone_geometry(name)
+        nview = dc.shape[0]
+        img = rng.random((1, g["nx"], g["ny"], g["nz"], 1)).astype(np.float32)
+        prj_in = rng.random((1, g["nu"], nview, g["nv"], 1)).astype(np.float32)
+        args = (1, 1, g["nx"], g["ny"], g["nz"], g["dx"], g["dy"], g["dz"], g["cx"], g["cy"], g["cz"], g["nu"], nview,
+                g["nv"], g["du"], g["dv"], g["off_u"], g["off_v"])
+        fp = np.zeros((1, g["nu"], nview, g["nv"], 1), np.float32)
+        lib.cSiddonConeProjectionAbitrary(p(fp), p(img), p(dc), p(du), p(dv), p(src), *args)
+        bp = np.zeros(img.shape, np.float32)
+        lib.cSiddonConeBackprojectionAbitrary(p(bp), p(prj_in), p(dc), p(du), p(dv), p(src), *args)
+        d = dict(img=img, prj_in=prj_in, det_center=dc, det_u=du, det_v=dv, src=src, fp=fp, bp=bp,
+                 **{k: np.float64(v) for k, v in g.items()})
+        if name == "cone_tomo" and hasattr(lib, "cOSSQSConeAbitrary"):
+            # one OS-SQS pass: 7 subsets of one view, a mask and a clamp
+            norm = np.zeros(img.shape, np.float32)
+            ones = np.ones(img.shape, np.float32)
+            a1 = np.zeros(fp.shape, np.float32)
+            lib.cSiddonConeProjectionAbitrary(p(a1), p(ones), p(dc), p(du), p(dv), p(src), *args)
+            lib.cSiddonConeBackprojectionAbitrary(p(norm), p(a1), p(dc), p(du), p(dv), p(src), *args)
+            mask = (rng.random(img.shape) > 0.1).astype(np.float32)
+            x0 = (rng.random(img.shape) * 0.5).astype(np.float32)
+            res = np.zeros(img.shape, np.float32)
+            lib.cOSSQSConeAbitrary(p(res), p(x0), p(fp), p(norm), p(mask), p(dc), p(du), p(dv), p(src), 0.0, 1.0,
+                                   1, nview, *args, 2, 0.7)
+            d.update(ossqs_x0=x0, ossqs_norm=norm, ossqs_mask=mask, ossqs_res=res, ossqs_lam=0.7)
+        out[name] = d
+    return out
+
+
 PRIOR_REF = os.path.join(ROOT, "oracle", "_ref", "libprior_ref.so")
 
 
@@ -238,6 +328,12 @@ def main(outdir=HERE, only=None):
             np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
         print("pixel-driven golden vectors written to", outdir)
         return
+    if only == "cone":
+        lib = load_ref()
+        for name, d in cone_case(lib, np.random.default_rng(20241207)).items():
+            np.savez_compressed(os.path.join(outdir, f"ref_{name}.npz"), **d)
+        print("cone golden vectors written to", outdir)
+        return
     if only == "prior":
         lib = load_prior_ref()
         for name, d in prior_case(lib, np.random.default_rng(20241206)).items():
@@ -261,5 +357,5 @@ def main(outdir=HERE, only=None):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    only = next((k for k in ("siddon", "ossqs", "pixel", "prior") if f"--{k}" in sys.argv), None)
+    only = next((k for k in ("siddon", "ossqs", "pixel", "prior", "cone") if f"--{k}" in sys.argv), None)
     main(args[0] if args else HERE, only=only)

@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "reconnet_b200.h")
 def _declared():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:int|void|float|char|int64_t)\s*\**\s*(\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:int|void|float|char|int64_t|long long)\s*\**\s*(\w+)\s*\(", src, re.M)))
 
 
 def test_library_builds_and_loads():
@@ -44,7 +44,9 @@ def test_reference_signatures_match_reference_python_calls():
     counts = {"cDistanceDrivenFanProjection": 21, "cDistanceDrivenFanBackprojection": 21,
               "cDistanceDrivenTomoProjection": 22, "cDistanceDrivenTomoBackprojection": 22,
               "cFilterFanFilter": 15, "cFilterParallelFilter": 15, "cOSSQS": 29, "cTVSQS2D": 5, "SetDevice": 1,
-              "cSiddonFanProjection": 21, "cSiddonFanBackprojection": 21, "cPixelDrivenFanBackprojection": 21}
+              "cSiddonFanProjection": 21, "cSiddonFanBackprojection": 21, "cPixelDrivenFanBackprojection": 21,
+              "cSiddonConeProjectionAbitrary": 24, "cSiddonConeBackprojectionAbitrary": 24,
+              "cOSSQSConeAbitrary": 33}
     for k, n in counts.items():
         assert len(N.SIGNATURES[k][1]) == n, k
 

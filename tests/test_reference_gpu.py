@@ -143,3 +143,30 @@ def test_pixel_bp_vs_reference_kernels(ref, rng):
         err = rel_l2(rn.cPixelBackprojection4d(out["sino_in"], out["angles"]), out["bp"])
         print(f"pixel-driven BP vs reference ({name}): {err:.3g}")
         assert err <= REF_TOL, name
+
+
+def test_cone_vs_reference_kernels(ref, rng):
+    """The reference's Siddon cone kernels (SiddonCone.cu) and its cone
+    OS-SQS (ossqs.cu:163-333) against this library on the same inputs."""
+    from reconnet_b200.reconnet import ReconNet
+    lib = ref.load_ref()
+    if not hasattr(lib, "cSiddonConeProjectionAbitrary"):
+        pytest.skip("reference library built without SiddonCone.cu")
+    for name, d in ref.cone_case(lib, rng).items():
+        rn = ReconNet()
+        for k in ("nx", "ny", "nz", "nu", "nv"):
+            setattr(rn, k, int(d[k]))
+        for k in ("dx", "dy", "dz", "cx", "cy", "cz", "du", "dv", "off_u", "off_v"):
+            setattr(rn, k, d[k].item())
+        geo = [d[k] for k in ("det_center", "det_u", "det_v", "src")]
+        efp = rel_l2(rn.cSiddonConeProjectionAbitrary4d(d["img"], *geo), d["fp"])
+        ebp = rel_l2(rn.cSiddonConeBackprojectionAbitrary4d(d["prj_in"], *geo), d["bp"])
+        print(f"{name}: fp {efp:.3g} bp {ebp:.3g}")
+        assert efp <= 1e-5 and ebp <= 1e-5, name      # measured ~1e-6 / ~3e-6
+        if "ossqs_res" in d:
+            nview = d["det_center"].shape[0]
+            got = rn.cSiddonConeAbitraryOSSQS4d(nview, d["ossqs_x0"], d["fp"], d["ossqs_norm"], *geo,
+                                                mask=d["ossqs_mask"], lb=0.0, ub=1.0, lam=float(d["ossqs_lam"]))
+            eos = rel_l2(got, d["ossqs_res"])
+            print(f"{name}: cone OS-SQS {eos:.3g}")
+            assert eos <= 1e-4      # measured 7e-6
