@@ -46,7 +46,13 @@ struct ConeView {
     float Sh[3], Sl[3];       // source as hi / lo floats
     float au[4], av[4], ad[4];   // shadow: iu = (au . P + au[3]) / (ad . P + ad[3]), iv likewise
     float ulo, uhi, vlo, vhi, dlo, dhi;   // sums of min(0, a_k) / max(0, a_k) over the three axes
-    int m, a, b, pad;
+    // separable views (affine = 1 or 2): every ray advances by the same Dm0
+    // along m, and r_a = rho[0] + iu rho[1] + iv rho[2], r_b = rho[3] +
+    // iu rho[4] + iv rho[5] with rho[2] = rho[4] = 0 (affine = 1: a follows
+    // iu, b follows iv) or rho[1] = rho[5] = 0 (affine = 2)
+    double rho[6];
+    double Dm0;
+    int m, a, b, affine;
 };
 
 struct ConeDims {
@@ -82,34 +88,33 @@ __global__ void cone_ray_kernel(float4* __restrict__ rays, const ConeView* __res
 
 __device__ __forceinline__ long long to_fixed(double v) { return llrint(v * 4294967296.0); }
 
-// First crossing of a lateral axis inside the slab, in slab units, or 2 if
-// none: fixed-point position p at the slab start, nx crossings, slope sign,
-// |1 / r|.
-__device__ __forceinline__ float first_crossing(long long p, int nx, bool pos, float ir) {
-    if (nx == 0) return 2.f;
-    const float f = __uint2float_rn((unsigned)p) * 2.3283064365386963e-10f;   // fractional part
-    return (pos ? 1.f - f : f) * ir;
+// Fractional part of a fixed-point position as a float in [0, 1) (its top 23
+// bits: exact to 1.2e-7).
+__device__ __forceinline__ float fixed_frac(long long p) {
+    return __uint_as_float(0x3f800000u | ((unsigned)p >> 9)) - 1.0f;
 }
 
-__global__ void __launch_bounds__(256) cone_fp_kernel(float* __restrict__ prj, const float* __restrict__ img,
-                                                       const ConeView* __restrict__ views, ConeDims cd) {
-    const int iu = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
-    if (iu >= cd.nu || iv >= cd.nv) return;
-    int zi = blockIdx.z;
-    const int c = zi % cd.nc;
-    zi /= cd.nc;
-    const int view = zi % cd.nview;
-    const int bt = zi / cd.nview;
-    const ConeView& V = views[view];
-    const int m = V.m, a = V.a, b = V.b;
+// Per-ray stepping state: lateral positions at the start of slab k0 and
+// their step per slab (fixed point, 32 fractional bits), slope signs and
+// |1 / r|, the ray's length per slab, the segment's own ends along m relative
+// to slab k0, and the slabs [k0, k0 + ns).
+struct RayStep {
+    long long A, RA, B, RB;
+    float seg, ira, irb, slo, shi;
+    int k0, ns;
+    bool pa, pb;
+};
+
+__device__ __forceinline__ RayStep cone_ray_step(const ConeView& V, int iu, int iv, const ConeDims& cd, int m, int a,
+                                                 int b) {
+    RayStep R;
+    R.ns = 0;
     double D[3], S[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         S[k] = V.S[k];
         D[k] = V.C[k] + iu * V.Eu[k] + iv * V.Ev[k] - S[k];
     }
-    float* out = prj + bt * cd.prj_b + (((long long)iu * cd.nview + view) * cd.nv + iv) * cd.nc + c;
     // parameter range of the segment inside the grid
     double t0 = 0.0, t1 = 1.0;
 #pragma unroll
@@ -122,63 +127,216 @@ __global__ void __launch_bounds__(256) cone_fp_kernel(float* __restrict__ prj, c
             t1 = -1.0;
         }
     }
-    if (t1 <= t0) {
-        *out = 0.f;
-        return;
-    }
-    const double Dm = D[m], ra = D[a] / Dm, rb = D[b] / Dm;
-    const double mlo = S[m] + fmin(t0 * Dm, t1 * Dm), mhi = S[m] + fmax(t0 * Dm, t1 * Dm);
-    const int k0 = max(0, (int)floor(mlo)), k1 = min(cd.n[m] - 1, (int)ceil(mhi) - 1);
-    const double dm = cd.d[m], da = cd.d[a], db = cd.d[b];
-    const float seg = (float)sqrt(dm * dm + ra * ra * da * da + rb * rb * db * db);
+    if (t1 <= t0) return R;
+    const double Dm = m == 0 ? D[0] : m == 1 ? D[1] : D[2];
+    const double Da = a == 0 ? D[0] : a == 1 ? D[1] : D[2];
+    const double Db = b == 0 ? D[0] : b == 1 ? D[1] : D[2];
+    const double Sm = m == 0 ? S[0] : m == 1 ? S[1] : S[2];
+    const double Sa = a == 0 ? S[0] : a == 1 ? S[1] : S[2];
+    const double Sb = b == 0 ? S[0] : b == 1 ? S[1] : S[2];
+    const int nm = m == 0 ? cd.n[0] : m == 1 ? cd.n[1] : cd.n[2];
+    const double ra = Da / Dm, rb = Db / Dm;
+    const double mlo = Sm + fmin(t0 * Dm, t1 * Dm), mhi = Sm + fmax(t0 * Dm, t1 * Dm);
+    const int k0 = max(0, (int)floor(mlo)), k1 = min(nm - 1, (int)ceil(mhi) - 1);
+    if (k1 < k0) return R;
+    const double dm = m == 0 ? cd.d[0] : m == 1 ? cd.d[1] : cd.d[2];
+    const double da = a == 0 ? cd.d[0] : a == 1 ? cd.d[1] : cd.d[2];
+    const double db = b == 0 ? cd.d[0] : b == 1 ? cd.d[1] : cd.d[2];
+    R.seg = (float)sqrt(dm * dm + ra * ra * da * da + rb * rb * db * db);
     // the segment's own ends along m (the grid faces are handled by the
     // voxel bounds), relative to slab k0
-    const double sm_lo = fmin(S[m], S[m] + Dm), sm_hi = fmax(S[m], S[m] + Dm);
-    const float slo = (float)fmax(sm_lo - k0, -1.0), shi = (float)fmin(sm_hi - k0, (double)(k1 - k0) + 2.0);
-    long long A = to_fixed(S[a] + (k0 - S[m]) * ra), B = to_fixed(S[b] + (k0 - S[m]) * rb);
-    const long long RA = to_fixed(ra), RB = to_fixed(rb);
-    const bool pa = ra > 0, pb = rb > 0;
-    const float ira = fabs(ra) > 1e-30 ? (float)(1.0 / fabs(ra)) : 1e30f;
-    const float irb = fabs(rb) > 1e-30 ? (float)(1.0 / fabs(rb)) : 1e30f;
-    const int sa = pa ? 1 : -1, sb = pb ? 1 : -1;
-    const int na_ = cd.n[a], nb_ = cd.n[b];
-    const long long sta = cd.st[a], stb = cd.st[b], stm = cd.st[m];
-    const float* base = img + bt * cd.img_b + c;
-    float acc = 0.f;
-    for (int k = k0; k <= k1; k++) {
-        const int j = k - k0;
-        const float tlo = fmaxf(0.f, slo - (float)j), thi = fminf(1.f, shi - (float)j);
-        const long long An = A + RA, Bn = B + RB;
-        int ca = (int)(A >> 32), cb = (int)(B >> 32);
-        int nxa = abs((int)(An >> 32) - ca), nxb = abs((int)(Bn >> 32) - cb);
-        float ta = first_crossing(A, nxa, pa, ira), tb = first_crossing(B, nxb, pb, irb);
-        const float* sl = base + (long long)k * stm;
-        float tcur = 0.f;
+    R.slo = (float)fmax(fmin(Sm, Sm + Dm) - k0, -1.0);
+    R.shi = (float)fmin(fmax(Sm, Sm + Dm) - k0, (double)(k1 - k0) + 2.0);
+    R.A = to_fixed(Sa + (k0 - Sm) * ra);
+    R.B = to_fixed(Sb + (k0 - Sm) * rb);
+    R.RA = to_fixed(ra);
+    R.RB = to_fixed(rb);
+    R.pa = ra > 0;
+    R.pb = rb > 0;
+    R.ira = fabs(ra) > 1e-30 ? (float)(1.0 / fabs(ra)) : 1e30f;
+    R.irb = fabs(rb) > 1e-30 ? (float)(1.0 / fabs(rb)) : 1e30f;
+    R.k0 = k0;
+    R.ns = k1 - k0 + 1;
+    return R;
+}
+
+// The voxel values along one slab of a ray times the share of the slab
+// spent in each voxel, for slab entry positions A, B (fixed point), steps
+// RA, RB, and the segment clip [tlo, thi] in slab units; sl points at the
+// slab's voxel (0, 0) and sta, stb are the lateral strides (32-bit: the plan
+// keeps a batch below 2^31 elements).  kUnit: |r| <= 1, so at most one
+// crossing per lateral axis and three pieces, without branches; otherwise
+// the pieces are walked.
+template <bool kUnit>
+__device__ __forceinline__ float slab_sum(long long A, long long RA, long long B, long long RB, bool pa, bool pb,
+                                          float ira, float irb, float tlo, float thi, const float* sl, int sta,
+                                          int stb, int na, int nb) {
+    const long long An = A + RA, Bn = B + RB;
+    const int ca0 = (int)(A >> 32), cb0 = (int)(B >> 32);
+    const int ca1 = (int)(An >> 32), cb1 = (int)(Bn >> 32);
+    if (kUnit) {
+        const float fa = fixed_frac(A), fb = fixed_frac(B);
+        const float ta = ca1 != ca0 ? (pa ? 1.f - fa : fa) * ira : 2.f;
+        const float tb = cb1 != cb0 ? (pb ? 1.f - fb : fb) * irb : 2.f;
+        const float t1 = fminf(ta, tb), t2 = fmaxf(ta, tb);
+        const bool afirst = ta < tb;
+        const int cam = afirst ? ca1 : ca0, cbm = afirst ? cb0 : cb1;
+        const float l0 = fminf(t1, thi) - tlo, lm = fminf(t2, thi) - fmaxf(t1, tlo), l1 = thi - fmaxf(t2, tlo);
+        float s = 0.f;
+        if (l0 > 0.f && (unsigned)ca0 < (unsigned)na && (unsigned)cb0 < (unsigned)nb)
+            s = l0 * __ldg(sl + (ca0 * sta + cb0 * stb));
+        if (lm > 0.f && (unsigned)cam < (unsigned)na && (unsigned)cbm < (unsigned)nb)
+            s = fmaf(lm, __ldg(sl + (cam * sta + cbm * stb)), s);
+        if (l1 > 0.f && (unsigned)ca1 < (unsigned)na && (unsigned)cb1 < (unsigned)nb)
+            s = fmaf(l1, __ldg(sl + (ca1 * sta + cb1 * stb)), s);
+        return s;
+    } else {
+        int ca = ca0, cb = cb0;
+        int nxa = abs(ca1 - ca0), nxb = abs(cb1 - cb0);
+        float ta = nxa ? (pa ? 1.f - fixed_frac(A) : fixed_frac(A)) * ira : 2.f;
+        float tb = nxb ? (pb ? 1.f - fixed_frac(B) : fixed_frac(B)) * irb : 2.f;
+        float tcur = 0.f, s = 0.f;
         for (;;) {
             const float tn = fminf(fminf(ta, tb), thi);
             const float len = tn - fmaxf(tcur, tlo);
-            if (len > 0.f && (unsigned)ca < (unsigned)na_ && (unsigned)cb < (unsigned)nb_)
-                acc = fmaf(len, __ldg(sl + ca * sta + cb * stb), acc);
+            if (len > 0.f && (unsigned)ca < (unsigned)na && (unsigned)cb < (unsigned)nb)
+                s = fmaf(len, __ldg(sl + (ca * sta + cb * stb)), s);
             if (tn >= thi) break;
             tcur = tn;
             if (ta <= tb) {
-                ca += sa;
+                ca += pa ? 1 : -1;
                 ta = (--nxa > 0) ? ta + ira : 2.f;
             } else {
-                cb += sb;
+                cb += pb ? 1 : -1;
                 tb = (--nxb > 0) ? tb + irb : 2.f;
             }
         }
-        A = An;
-        B = Bn;
+        return s;
     }
-    *out = acc * seg;
+}
+
+// Forward projection, one thread per ray: a block holds 32 rays along iu x
+// 8 along iv, or 32 along iv x 8 along iu when `lanes_v` (the detector's v
+// running along z, the image's contiguous axis, so that a warp's loads of
+// one slab lie close together).
+template <bool kUnit>
+__global__ void __launch_bounds__(256) cone_fp_kernel(float* __restrict__ prj, const float* __restrict__ img,
+                                                       const ConeView* __restrict__ views, ConeDims cd,
+                                                       int lanes_v) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int iu = lanes_v ? blockIdx.x * 8 + warp : blockIdx.x * 32 + lane;
+    const int iv = lanes_v ? blockIdx.y * 32 + lane : blockIdx.y * 8 + warp;
+    if (iu >= cd.nu || iv >= cd.nv) return;
+    int zi = blockIdx.z;
+    const int c = zi % cd.nc;
+    zi /= cd.nc;
+    const int view = zi % cd.nview;
+    const int bt = zi / cd.nview;
+    const ConeView& V = views[view];
+    const int m = V.m, a = V.a, b = V.b;
+    const RayStep R = cone_ray_step(V, iu, iv, cd, m, a, b);
+    float acc = 0.f;
+    if (R.ns > 0) {
+        const int sta = (int)(a == 0 ? cd.st[0] : a == 1 ? cd.st[1] : cd.st[2]);
+        const int stb = (int)(b == 0 ? cd.st[0] : b == 1 ? cd.st[1] : cd.st[2]);
+        const int stm = (int)(m == 0 ? cd.st[0] : m == 1 ? cd.st[1] : cd.st[2]);
+        const int na = a == 0 ? cd.n[0] : a == 1 ? cd.n[1] : cd.n[2];
+        const int nb = b == 0 ? cd.n[0] : b == 1 ? cd.n[1] : cd.n[2];
+        const float* sl = img + bt * cd.img_b + c + R.k0 * stm;
+        long long A = R.A, B = R.B;
+        for (int j = 0; j < R.ns; j++) {
+            acc += slab_sum<kUnit>(A, R.RA, B, R.RB, R.pa, R.pb, R.ira, R.irb, fmaxf(0.f, R.slo - (float)j),
+                                   fminf(1.f, R.shi - (float)j), sl, sta, stb, na, nb);
+            A += R.RA;
+            B += R.RB;
+            sl += stm;
+        }
+        acc *= R.seg;
+    }
+    prj[bt * cd.prj_b + (((long long)iu * cd.nview + view) * cd.nv + iv) * cd.nc + c] = acc;
 }
 
 __device__ __forceinline__ void two_sum_f(float a, float b, float& s, float& e) {
     s = a + b;
     const float bb = s - a;
     e = (a - (s - bb)) + (b - bb);
+}
+
+// Separable views: the lateral offsets of ray (iu, iv) from voxel (x, y, z)
+// at its low main-axis face are x_a = A + M r_a(i) and x_b = B + M r_b(j),
+// with (i, j) = (iu, iv) (affine = 1) or (iv, iu) (affine = 2), A = S_a -
+// a_v, B = S_b - b_v, M = m_v - S_m.  The cells whose ray can meet the voxel
+// along a satisfy x_a in (-max(r_a, 0), 1 - min(r_a, 0)): an index range
+// (widened by 0.02), found in FP64; likewise along b.  Each pair (i, j) then
+// adds seg x prj x |[0, 1] n T_a(i) n T_b(j)|, T being the parameter
+// interval over which the ray lies inside the voxel along that axis.
+// Returns false (adding nothing) when a range holds more than kSepMax cells.
+constexpr int kSepMax = 6;
+
+__device__ __forceinline__ bool bp_separable(float& acc, const ConeView& V, int x, int y, int z, const ConeDims& cd,
+                                             const float* pb, int view) {
+    const int m = V.m, a = V.a, b = V.b;
+    const int pm = m == 0 ? x : m == 1 ? y : z, pa = a == 0 ? x : a == 1 ? y : z, pbv = b == 0 ? x : b == 1 ? y : z;
+    const double Sm = m == 0 ? V.S[0] : m == 1 ? V.S[1] : V.S[2];
+    const double Sa = a == 0 ? V.S[0] : a == 1 ? V.S[1] : V.S[2];
+    const double Sb = b == 0 ? V.S[0] : b == 1 ? V.S[1] : V.S[2];
+    const double M = (double)pm - Sm, A = Sa - pa, B = Sb - pbv;
+    const bool swap = V.affine == 2;
+    // r_a = ra0 + i ra1, r_b = rb0 + j rb1
+    const double ra0 = V.rho[0], ra1 = swap ? V.rho[2] : V.rho[1];
+    const double rb0 = V.rho[3], rb1 = swap ? V.rho[4] : V.rho[5];
+    const int ni = swap ? cd.nv : cd.nu, nj = swap ? cd.nu : cd.nv;
+    // index range from x(i) = A + M (r0 + i r1) in (lo, hi), with r ~ -A / M
+    // (the slope of the ray through the voxel's corner)
+    auto range = [&](double A_, double r0, double r1, int n, int& i0, int& i1) {
+        const double rs = -A_ / M;
+        const double lo = -fmax(rs, 0.0) - 0.02, hi = 1.0 - fmin(rs, 0.0) + 0.02;
+        const double k = M * r1;
+        const double q0 = (lo - A_ - M * r0) / k, q1 = (hi - A_ - M * r0) / k;
+        i0 = max(0, (int)ceil(fmax(fmin(q0, q1), -1e9)));
+        i1 = min(n - 1, (int)floor(fmin(fmax(q0, q1), 1e9)));
+    };
+    int i0, i1, j0, j1;
+    range(A, ra0, ra1, ni, i0, i1);
+    range(B, rb0, rb1, nj, j0, j1);
+    if (i1 < i0 || j1 < j0) return true;
+    if (i1 - i0 >= kSepMax || j1 - j0 >= kSepMax) return false;
+    // the first candidate's offsets in FP64, then steps in FP32
+    const double rai = ra0 + i0 * ra1, rbj = rb0 + j0 * rb1;
+    const float xa0 = (float)(A + M * rai), xb0 = (float)(B + M * rbj);
+    const float ga = (float)(M * ra1), gb = (float)(M * rb1);
+    const float rai_f = (float)rai, rbj_f = (float)rbj, ra1f = (float)ra1, rb1f = (float)rb1;
+    // the segment's ends along m, relative to the voxel's low face
+    const float e0 = (float)(-M), e1 = (float)(-M + V.Dm0);
+    const float clo = fmaxf(0.f, fminf(e0, e1)), chi = fminf(1.f, fmaxf(e0, e1));
+    const float dm = m == 0 ? cd.d[0] : m == 1 ? cd.d[1] : cd.d[2];
+    const float da = a == 0 ? cd.d[0] : a == 1 ? cd.d[1] : cd.d[2];
+    const float db = b == 0 ? cd.d[0] : b == 1 ? cd.d[1] : cd.d[2];
+    const float dm2 = dm * dm, da2 = da * da, db2 = db * db;
+    const int su = cd.nview * cd.nv * cd.nc, sv = cd.nc;
+    const float* pview = pb + (long long)view * cd.nv * cd.nc;
+    for (int j = j0; j <= j1; j++) {
+        const float kj = (float)(j - j0);
+        const float xb = fmaf(kj, gb, xb0), rb = fmaf(kj, rb1f, rbj_f);
+        const float ib = fabsf(rb) > 1e-30f ? __fdividef(1.f, rb) : 1e30f;
+        const float tb0 = -xb * ib, tb1 = (1.f - xb) * ib;
+        const float lb = fmaxf(clo, fminf(tb0, tb1)), hb = fminf(chi, fmaxf(tb0, tb1));
+        if (!(hb > lb)) continue;
+        const float qb = fmaf(rb * rb, db2, dm2);
+        for (int i = i0; i <= i1; i++) {
+            const float ki = (float)(i - i0);
+            const float xa = fmaf(ki, ga, xa0), ra = fmaf(ki, ra1f, rai_f);
+            const float ia = fabsf(ra) > 1e-30f ? __fdividef(1.f, ra) : 1e30f;
+            const float ta0 = -xa * ia, ta1 = (1.f - xa) * ia;
+            const float tl = fmaxf(lb, fminf(ta0, ta1)), th = fminf(hb, fmaxf(ta0, ta1));
+            if (th > tl) {
+                const float q = fmaf(ra * ra, da2, qb);
+                const int iu = swap ? j : i, iv = swap ? i : j;
+                acc = fmaf((th - tl) * (q * rsqrtf(q)), __ldg(pview + ((long long)iu * su + iv * sv)), acc);
+            }
+        }
+    }
+    return true;
 }
 
 // One thread per voxel (z fastest) of slice `bc` = b * nc + c.
@@ -195,18 +353,18 @@ __global__ void __launch_bounds__(256) cone_bp_kernel(float* __restrict__ img, c
     const int y = (int)((q / cd.n[2]) % cd.n[1]);
     const int x = (int)(q / ((long long)cd.n[2] * cd.n[1]));
     const float P[3] = {(float)x, (float)y, (float)z};
-    const int pi[3] = {x, y, z};
     const float* pb = prj + bt * cd.prj_b + c;
     float acc = 0.f;
     for (int view = 0; view < cd.nview; view++) {
         const ConeView& V = views[view];
+        if (V.affine && bp_separable(acc, V, x, y, z, cd, pb, view)) continue;
         // shadow of the voxel [P, P + 1]^3 on the detector, in cell indices
         const float nu0 = fmaf(V.au[0], P[0], fmaf(V.au[1], P[1], fmaf(V.au[2], P[2], V.au[3])));
         const float nv0 = fmaf(V.av[0], P[0], fmaf(V.av[1], P[1], fmaf(V.av[2], P[2], V.av[3])));
         const float nd0 = fmaf(V.ad[0], P[0], fmaf(V.ad[1], P[1], fmaf(V.ad[2], P[2], V.ad[3])));
         const float dmin = nd0 + V.dlo, dmax = nd0 + V.dhi;
         if (!(dmin > 0.f)) continue;
-        const float id0 = 1.f / dmin, id1 = 1.f / dmax;
+        const float id0 = __fdividef(1.f, dmin), id1 = __fdividef(1.f, dmax);
         const float ulo = nu0 + V.ulo, uhi = nu0 + V.uhi, vlo = nv0 + V.vlo, vhi = nv0 + V.vhi;
         const int u0 = max(0, (int)ceilf(fminf(ulo * id0, ulo * id1) - 1e-3f));
         const int u1 = min(cd.nu - 1, (int)floorf(fmaxf(uhi * id0, uhi * id1) + 1e-3f));
@@ -216,14 +374,22 @@ __global__ void __launch_bounds__(256) cone_bp_kernel(float* __restrict__ img, c
         // voxel offsets from the source as hi / lo: A = S - lateral index,
         // M = main index - S_m
         const int m = V.m, a = V.a, b = V.b;
+        const int pm = m == 0 ? x : m == 1 ? y : z, pa_ = a == 0 ? x : a == 1 ? y : z, pb_ = b == 0 ? x : b == 1 ? y : z;
+        const float Shm = m == 0 ? V.Sh[0] : m == 1 ? V.Sh[1] : V.Sh[2];
+        const float Sha = a == 0 ? V.Sh[0] : a == 1 ? V.Sh[1] : V.Sh[2];
+        const float Shb = b == 0 ? V.Sh[0] : b == 1 ? V.Sh[1] : V.Sh[2];
+        const float Slm = m == 0 ? V.Sl[0] : m == 1 ? V.Sl[1] : V.Sl[2];
+        const float Sla = a == 0 ? V.Sl[0] : a == 1 ? V.Sl[1] : V.Sl[2];
+        const float Slb = b == 0 ? V.Sl[0] : b == 1 ? V.Sl[1] : V.Sl[2];
         float Ah, Al, Bh, Bl, Mh, Ml, e;
-        two_sum_f(V.Sh[a], -(float)pi[a], Ah, e);
-        Al = e + V.Sl[a];
-        two_sum_f(V.Sh[b], -(float)pi[b], Bh, e);
-        Bl = e + V.Sl[b];
-        two_sum_f((float)pi[m], -V.Sh[m], Mh, e);
-        Ml = e - V.Sl[m];
-        const float sm = (float)pi[m] - V.Sh[m] - V.Sl[m];   // main index - S_m (segment clipping only)
+        two_sum_f(Sha, -(float)pa_, Ah, e);
+        Al = e + Sla;
+        two_sum_f(Shb, -(float)pb_, Bh, e);
+        Bl = e + Slb;
+        two_sum_f((float)pm, -Shm, Mh, e);
+        Ml = e - Slm;
+        const float sm = (float)pm - Shm - Slm;   // main index - S_m (segment clipping only)
+        const long long su = (long long)cd.nview * cd.nv * cd.nc;
         for (int iv = v0; iv <= v1; iv++) {
             const long long rrow = ((long long)view * cd.nv + iv) * cd.nu;
             const float* prow = pb + ((long long)view * cd.nv + iv) * cd.nc;
@@ -236,10 +402,10 @@ __global__ void __launch_bounds__(256) cone_bp_kernel(float* __restrict__ img, c
                 const float tb0 = -xb * g1.y, tb1 = (1.f - xb) * g1.y;
                 // the segment's ends along m: source (at -sm from the voxel's
                 // low face) and end point E_m
-                const float e0 = -sm, e1 = g1.w - (float)pi[m];
+                const float e0 = -sm, e1 = g1.w - (float)pm;
                 const float tl = fmaxf(fmaxf(fmaxf(0.f, fminf(ta0, ta1)), fminf(tb0, tb1)), fminf(e0, e1));
                 const float th = fminf(fminf(fminf(1.f, fmaxf(ta0, ta1)), fmaxf(tb0, tb1)), fmaxf(e0, e1));
-                if (th > tl) acc = fmaf((th - tl) * g1.z, __ldg(prow + (long long)iu * cd.nview * cd.nv * cd.nc), acc);
+                if (th > tl) acc = fmaf((th - tl) * g1.z, __ldg(prow + (long long)iu * su), acc);
             }
         }
     }
@@ -256,13 +422,16 @@ struct rn_cone_plan {
     int device = 0;
     ConeView* d_views = nullptr;
     float4* d_rays = nullptr;
+    int lanes_v = 0;           // forward projection: warps along the detector's v
+    bool unit = true;          // every ray's lateral slopes are at most 1
     long long launches = 0;
 };
 
 namespace {
 
 int cone_views(rn_cone_plan* p, const RnConeGeom& g, const float* dc, const float* du_, const float* dv_,
-               const float* src, std::vector<ConeView>& out) {
+               const float* src, std::vector<ConeView>& out, double& max_slope) {
+    max_slope = 0.0;
     const int n[3] = {g.nx, g.ny, g.nz};
     const double d[3] = {g.dx, g.dy, g.dz}, cen[3] = {g.cx, g.cy, g.cz};
     const double u0 = g.off_u + (g.nu - 1) / 2.0, v0 = g.off_v + (g.nv - 1) / 2.0;
@@ -297,6 +466,7 @@ int cone_views(rn_cone_plan* p, const RnConeGeom& g, const float* dc, const floa
             if (D[m] * Dc[m] <= 0.0 || std::fabs(D[V.a]) > 4.0 * std::fabs(D[m]) ||
                 std::fabs(D[V.b]) > 4.0 * std::fabs(D[m]))
                 return set_error(RN_ERR_ARG, "cone geometry: rays of one view too oblique to a common main axis");
+            max_slope = std::max(max_slope, std::max(std::fabs(D[V.a]), std::fabs(D[V.b])) / std::fabs(D[m]));
         }
         // shadow: the ray from S through P meets the detector plane at
         // index (iu, iv); with W = P - S and the plane normal nrm (oriented
@@ -351,6 +521,23 @@ int cone_views(rn_cone_plan* p, const RnConeGeom& g, const float* dc, const floa
         V.au[3] = (float)bu;
         V.av[3] = (float)bv;
         V.ad[3] = (float)bd;
+        // separable views: the detector is perpendicular to the main axis and
+        // its u / v steps each move along one lateral axis only
+        const double tiny = 1e-9 * std::fabs(Dc[m]);
+        const bool perp = std::fabs(V.Eu[m]) * g.nu + std::fabs(V.Ev[m]) * g.nv <= tiny;
+        const bool a_u = std::fabs(V.Ev[V.a]) * g.nv <= tiny && std::fabs(V.Eu[V.b]) * g.nu <= tiny;
+        const bool a_v = std::fabs(V.Eu[V.a]) * g.nu <= tiny && std::fabs(V.Ev[V.b]) * g.nv <= tiny;
+        if (perp && (a_u || a_v)) {
+            const double Dm0 = V.C[m] - V.S[m];
+            V.affine = a_u ? 1 : 2;
+            V.Dm0 = Dm0;
+            V.rho[0] = (V.C[V.a] - V.S[V.a]) / Dm0;
+            V.rho[1] = V.Eu[V.a] / Dm0;
+            V.rho[2] = V.Ev[V.a] / Dm0;
+            V.rho[3] = (V.C[V.b] - V.S[V.b]) / Dm0;
+            V.rho[4] = V.Eu[V.b] / Dm0;
+            V.rho[5] = V.Ev[V.b] / Dm0;
+        }
         out[iv] = V;
     }
     (void)p;
@@ -372,8 +559,8 @@ int rn_cone_plan_create(rn_cone_plan** out, const RnConeGeom* g, const float* ho
         return set_error(RN_ERR_ARG, "cone geometry: sizes must be positive");
     if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0) || !(g->du > 0) || !(g->dv > 0))
         return set_error(RN_ERR_ARG, "cone geometry: pixel sizes must be positive");
-    if (g->nx > (1 << 20) || g->ny > (1 << 20) || g->nz > (1 << 20))
-        return set_error(RN_ERR_ARG, "cone geometry: grid too large");
+    if ((long long)g->nx * g->ny * g->nz * g->nChannels >= (1LL << 31))
+        return set_error(RN_ERR_ARG, "cone geometry: more than 2^31 voxels x channels per batch");
     rn_cone_plan* p = new rn_cone_plan();
     cudaGetDevice(&p->device);
     ConeDims& cd = p->cd;
@@ -394,10 +581,18 @@ int rn_cone_plan_create(rn_cone_plan** out, const RnConeGeom* g, const float* ho
     cd.img_b = (long long)g->nx * cd.st[0];
     cd.prj_b = (long long)g->nu * g->nview * g->nv * cd.nc;
     std::vector<ConeView> views;
-    int s = cone_views(p, *g, host_detCenter, host_detU, host_detV, host_src, views);
+    double max_slope = 0.0;
+    int s = cone_views(p, *g, host_detCenter, host_detU, host_detV, host_src, views, max_slope);
     if (s != RN_OK) {
         delete p;
         return s;
+    }
+    p->unit = max_slope <= 1.0;
+    // warps along iv when the detector's v step of view 0 runs mostly along z
+    // and z is not the main axis
+    {
+        const double* e = views[0].Ev;
+        p->lanes_v = (views[0].m != 2 && std::fabs(e[2]) >= std::max(std::fabs(e[0]), std::fabs(e[1]))) ? 1 : 0;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const long long nrays = (long long)g->nview * g->nv * g->nu;
@@ -432,8 +627,11 @@ int rn_cone_project(rn_cone_plan* p, float* d_prj, const float* d_img, void* str
     const ConeDims& cd = p->cd;
     const long long nz = (long long)cd.nb * cd.nview * cd.nc;
     if (nz > 65535) return set_error(RN_ERR_ARG, "cone projection: more than 65535 views x batches x channels");
-    dim3 grid((cd.nu + 31) / 32, (cd.nv + 7) / 8, (unsigned)nz);
-    cone_fp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd);
+    const int gx = p->lanes_v ? (cd.nu + 7) / 8 : (cd.nu + 31) / 32;
+    const int gy = p->lanes_v ? (cd.nv + 31) / 32 : (cd.nv + 7) / 8;
+    dim3 grid(gx, gy, (unsigned)nz);
+    if (p->unit) cone_fp_kernel<true><<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd, p->lanes_v);
+    else cone_fp_kernel<false><<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd, p->lanes_v);
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;

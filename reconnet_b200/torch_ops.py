@@ -369,8 +369,12 @@ class ConePlan:
         self.prj_shape = (self.nbatches, geom.nu, self.nview, geom.nv, self.nchannels)
 
     def __del__(self):
-        if getattr(self, "_plan", None) and self._plan.value:
-            N.lib.rn_cone_plan_destroy(self._plan)
+        p = getattr(self, "_plan", None)
+        if p is not None and p.value:
+            try:
+                N.lib.rn_cone_plan_destroy(p)
+            except Exception:
+                pass
             self._plan = ctypes.c_void_p()
 
     def project(self, img: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
