@@ -286,26 +286,28 @@ __device__ __forceinline__ bool bp_separable(float& acc, const ConeView& V, int 
     const double ra0 = V.rho[0], ra1 = swap ? V.rho[2] : V.rho[1];
     const double rb0 = V.rho[3], rb1 = swap ? V.rho[4] : V.rho[5];
     const int ni = swap ? cd.nv : cd.nu, nj = swap ? cd.nu : cd.nv;
-    // index range from x(i) = A + M (r0 + i r1) in (lo, hi), with r ~ -A / M
-    // (the slope of the ray through the voxel's corner)
-    auto range = [&](double A_, double r0, double r1, int n, int& i0, int& i1) {
-        const double rs = -A_ / M;
-        const double lo = -fmax(rs, 0.0) - 0.02, hi = 1.0 - fmin(rs, 0.0) + 0.02;
-        const double k = M * r1;
-        const double q0 = (lo - A_ - M * r0) / k, q1 = (hi - A_ - M * r0) / k;
-        i0 = max(0, (int)ceil(fmax(fmin(q0, q1), -1e9)));
-        i1 = min(n - 1, (int)floor(fmin(fmax(q0, q1), 1e9)));
+    // x(i) = X0 + i G with X0 = A + M r0 and G = M r1 (FP64); the index
+    // range where x(i) in (lo, hi) needs no more than FP32 (it is widened by
+    // 0.02), with r ~ -A / M, the slope of the ray through the voxel corner
+    const double XA0 = A + M * ra0, XB0 = B + M * rb0, GA = M * ra1, GB = M * rb1;
+    const float rs_a = (float)(-A) / (float)M, rs_b = (float)(-B) / (float)M;
+    auto range = [&](double X0, double G, float rs, int n, int& i0, int& i1) {
+        const float lo = -fmaxf(rs, 0.f) - 0.02f, hi = 1.f - fminf(rs, 0.f) + 0.02f;
+        const float x0 = (float)X0, ig = __fdividef(1.f, (float)G);
+        const float q0 = (lo - x0) * ig, q1 = (hi - x0) * ig;
+        i0 = max(0, (int)ceilf(fmaxf(fminf(q0, q1), -1e9f)));
+        i1 = min(n - 1, (int)floorf(fminf(fmaxf(q0, q1), 1e9f)));
     };
     int i0, i1, j0, j1;
-    range(A, ra0, ra1, ni, i0, i1);
-    range(B, rb0, rb1, nj, j0, j1);
+    range(XA0, GA, rs_a, ni, i0, i1);
+    range(XB0, GB, rs_b, nj, j0, j1);
     if (i1 < i0 || j1 < j0) return true;
     if (i1 - i0 >= kSepMax || j1 - j0 >= kSepMax) return false;
     // the first candidate's offsets in FP64, then steps in FP32
-    const double rai = ra0 + i0 * ra1, rbj = rb0 + j0 * rb1;
-    const float xa0 = (float)(A + M * rai), xb0 = (float)(B + M * rbj);
-    const float ga = (float)(M * ra1), gb = (float)(M * rb1);
-    const float rai_f = (float)rai, rbj_f = (float)rbj, ra1f = (float)ra1, rb1f = (float)rb1;
+    const float xa0 = (float)fma((double)i0, GA, XA0), xb0 = (float)fma((double)j0, GB, XB0);
+    const float ga = (float)GA, gb = (float)GB;
+    const float ra1f = (float)ra1, rb1f = (float)rb1;
+    const float rai_f = (float)(ra0 + i0 * ra1), rbj_f = (float)(rb0 + j0 * rb1);
     // the segment's ends along m, relative to the voxel's low face
     const float e0 = (float)(-M), e1 = (float)(-M + V.Dm0);
     const float clo = fmaxf(0.f, fminf(e0, e1)), chi = fminf(1.f, fmaxf(e0, e1));
@@ -340,18 +342,30 @@ __device__ __forceinline__ bool bp_separable(float& acc, const ConeView& V, int 
 }
 
 // One thread per voxel (z fastest) of slice `bc` = b * nc + c.
+// `fast` is the grid axis that runs along the lanes of a warp: z (the
+// image's contiguous axis) by default, or the lateral axis that follows the
+// detector's v (the projections' contiguous axis) for separable views, so
+// that a warp's candidate rays are neighbours in memory.
 __global__ void __launch_bounds__(256) cone_bp_kernel(float* __restrict__ img, const float* __restrict__ prj,
                                                        const float4* __restrict__ rays,
                                                        const ConeView* __restrict__ views, ConeDims cd,
-                                                       int accumulate) {
+                                                       int accumulate, int fast) {
     const long long nvox = (long long)cd.n[0] * cd.n[1] * cd.n[2];
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nvox) return;
     const int bc = blockIdx.y;
     const int c = bc % cd.nc, bt = bc / cd.nc;
-    const int z = (int)(q % cd.n[2]);
-    const int y = (int)((q / cd.n[2]) % cd.n[1]);
-    const int x = (int)(q / ((long long)cd.n[2] * cd.n[1]));
+    // q -> (fast axis, then the other two in x, y, z order, the last slowest)
+    const int s1 = fast == 0 ? 1 : 0, s2 = fast == 2 ? 1 : 2;
+    const int nf = fast == 0 ? cd.n[0] : fast == 1 ? cd.n[1] : cd.n[2];
+    const int n1 = s1 == 0 ? cd.n[0] : cd.n[1];
+    const int i_f = (int)(q % nf);
+    const long long r = q / nf;
+    const int i_1 = (int)(r % n1), i_2 = (int)(r / n1);
+    const int x = fast == 0 ? i_f : i_1;
+    const int y = fast == 1 ? i_f : (s1 == 1 ? i_1 : i_2);
+    const int z = fast == 2 ? i_f : i_2;
+    (void)s2;
     const float P[3] = {(float)x, (float)y, (float)z};
     const float* pb = prj + bt * cd.prj_b + c;
     float acc = 0.f;
@@ -423,6 +437,7 @@ struct rn_cone_plan {
     ConeView* d_views = nullptr;
     float4* d_rays = nullptr;
     int lanes_v = 0;           // forward projection: warps along the detector's v
+    int bp_fast = 2;           // backprojection: grid axis along the lanes
     bool unit = true;          // every ray's lateral slopes are at most 1
     long long launches = 0;
 };
@@ -593,6 +608,12 @@ int rn_cone_plan_create(rn_cone_plan** out, const RnConeGeom* g, const float* ho
     {
         const double* e = views[0].Ev;
         p->lanes_v = (views[0].m != 2 && std::fabs(e[2]) >= std::max(std::fabs(e[0]), std::fabs(e[1]))) ? 1 : 0;
+        // backprojection lanes along the lateral axis that follows the
+        // detector's v when every view is separable the same way
+        bool same = true;
+        for (const ConeView& v : views)
+            same = same && v.affine != 0 && v.affine == views[0].affine && v.a == views[0].a && v.b == views[0].b;
+        if (same) p->bp_fast = views[0].affine == 1 ? views[0].b : views[0].a;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const long long nrays = (long long)g->nview * g->nv * g->nu;
@@ -645,7 +666,8 @@ int rn_cone_backproject(rn_cone_plan* p, float* d_img, const float* d_prj, int a
     const int slices = cd.nb * cd.nc;
     if (slices > 65535) return set_error(RN_ERR_ARG, "cone backprojection: too many batches x channels");
     dim3 grid((unsigned)((nvox + 255) / 256), slices);
-    cone_bp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_rays, p->d_views, cd, accumulate);
+    cone_bp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_rays, p->d_views, cd, accumulate,
+                                                            p->bp_fast);
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
