@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--slices", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ossqs", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis and filter measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis, cone and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
     return ap.parse_args()
 
@@ -230,7 +230,98 @@ def run_reference(args):
     import torch
     if torch.cuda.is_available():
         line["reference_gpu"] = reference_gpu(geom, counts, angles, imgs, min(3, args.steps))
+        if not args.no_extras:
+            line["reference_gpu_extras"] = reference_gpu_extras(geom, counts, angles, imgs)
     print(json.dumps(line), flush=True)
+
+
+def tomo_geometry(nview=25):
+    """The tomosynthesis workload of `tomo_run` / `cone_run`: 25 sources on a
+    +-20 deg arc at 650 mm, the detector centre 80 mm below the isocentre,
+    detector axes along x and y."""
+    import math
+    src = np.zeros((nview, 3), np.float32)
+    dc = np.zeros((nview, 3), np.float32)
+    for k in range(nview):
+        a = (k - (nview - 1) / 2) / ((nview - 1) / 2) * math.radians(20)
+        src[k] = (650 * math.sin(a), 0.0, 650 * math.cos(a))
+        dc[k] = (0.0, 0.0, -80.0)
+    du = np.tile(np.float32([1, 0, 0]), (nview, 1))
+    dv = np.tile(np.float32([0, 1, 0]), (nview, 1))
+    return dc, du, dv, src
+
+
+def reference_gpu_extras(geom, counts, angles, imgs):
+    """The reference library's other paths on the workloads of the extras in
+    this arm's counterpart, through its C entry points with host arrays (so
+    including its per-call allocations and copies; the kernel-only times come
+    from an ncu launch list of this command): the Siddon fan pair and the
+    pixel-driven backprojection on two slices of the fan batch, the
+    tomosynthesis DD pair and the Siddon cone pair on the tomosynthesis
+    workload."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libreconnet_ref.so")
+    if not os.path.exists(path):
+        return {"unavailable": "reference library not built (make -C oracle ref)"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    lib = make_golden.load_ref(path)
+    p = make_golden.p
+    out = {}
+    offs = np.concatenate([[0], np.cumsum(counts)])
+
+    def timed(fn):
+        fn()
+        t0 = time.perf_counter()
+        fn()
+        return (time.perf_counter() - t0) * 1e3
+
+    # fan batch, 2 slices
+    fan_upd = {"fp": 0, "bp": 0}
+    calls = []
+    for s in range(2):
+        n = int(counts[s])
+        img = np.ascontiguousarray(imgs[s][None, :, :, None, None])
+        ang = np.ascontiguousarray(angles[offs[s]:offs[s + 1]])
+        sino = np.zeros((1, geom.nu, n, 1, 1), np.float32)
+        bp = np.zeros_like(img)
+        a = (1, 1, geom.nx, geom.ny, 1, geom.dx, geom.dy, geom.dz, geom.nu, n, 1, geom.da, geom.dv, 0.0, 0.0,
+             geom.dsd, geom.dso, 0)
+        calls.append((img, ang, sino, bp, a))
+        fan_upd["fp"] += n * geom.nu * geom.ny
+        fan_upd["bp"] += n * geom.nx * geom.ny
+    for name, sym, fn in (
+            ("siddon_fp", "cSiddonFanProjection", lambda c: lib.cSiddonFanProjection(p(c[2]), p(c[0]), p(c[1]), *c[4])),
+            ("siddon_bp", "cSiddonFanBackprojection",
+             lambda c: lib.cSiddonFanBackprojection(p(c[3]), p(c[2]), p(c[1]), *c[4])),
+            ("pixel_bp", "cPixelDrivenFanBackprojection",
+             lambda c: lib.cPixelDrivenFanBackprojection(p(c[3]), p(c[2]), p(c[1]), *c[4]))):
+        if not hasattr(lib, sym):
+            continue
+        ms = timed(lambda: [fn(c) for c in calls])
+        upd = fan_upd["fp"] if name.endswith("fp") else fan_upd["bp"]
+        out[name] = {"ms": ms, "gupd_s_host_call": upd / ms / 1e6, "workload": "2 slices of the fan batch"}
+    # tomosynthesis workload
+    nx, ny, nz, nu, nv, nview = 512, 512, 128, 736, 736, 25
+    dc, du, dv, src = tomo_geometry(nview)
+    vol = np.random.default_rng(11).random((1, nx, ny, nz, 1)).astype(np.float32)
+    prj = np.zeros((1, nu, nview, nv, 1), np.float32)
+    back = np.zeros_like(vol)
+    targs = (1, 1, nx, ny, nz, 0.8, 0.8, 1.0, 0.0, 0.0, 0.0, nu, nview, nv, 0.6, 0.6, 0.0, 0.0)
+    pairs = [("tomo_fp", lambda: lib.cDistanceDrivenTomoProjection(p(prj), p(vol), p(dc), p(src), *targs),
+              nview * nu * nv * nz),
+             ("tomo_bp", lambda: lib.cDistanceDrivenTomoBackprojection(p(back), p(prj), p(dc), p(src), *targs),
+              nx * ny * nz * nview)]
+    if hasattr(lib, "cSiddonConeProjectionAbitrary"):
+        pairs += [("cone_fp", lambda: lib.cSiddonConeProjectionAbitrary(p(prj), p(vol), p(dc), p(du), p(dv), p(src),
+                                                                         *targs), nview * nu * nv * nz),
+                  ("cone_bp", lambda: lib.cSiddonConeBackprojectionAbitrary(p(back), p(prj), p(dc), p(du), p(dv),
+                                                                             p(src), *targs), nx * ny * nz * nview)]
+    for name, fn, upd in pairs:
+        ms = timed(fn)
+        out[name] = {"ms": ms, "gupd_s_host_call": upd / ms / 1e6, "workload": "the tomosynthesis workload"}
+    out["note"] = ("reference CUDA library (oracle/_ref) through its C entry points with host arrays: wall time "
+                   "of the second of two calls, including its allocations and copies")
+    return out
 
 
 def reference_gpu(geom, counts, angles, imgs, steps):
@@ -436,6 +527,63 @@ def siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=True):
     return out
 
 
+def cone_run(dev, cpu_sample=True):
+    """Siddon cone pair with per-view geometry (SiddonCone.cu) on the
+    tomosynthesis workload of `tomo_run`: 512x512x128 voxels of 0.8x0.8x1.0 mm,
+    a 736x736 flat detector of 0.6 mm cells 80 mm below the isocentre, 25
+    sources on a +-20 deg arc at 650 mm.  Updates as for the DD pair: FP =
+    views * nu * nv * nz ray-slab steps, BP = voxels * views; the byte model
+    is one 4-byte voxel (FP) or sinogram (BP) read per piece, about 1.3 pieces
+    per update (5.2 B)."""
+    import torch
+
+    from reconnet_b200.phantom import ellipsoid_phantom
+    from reconnet_b200.torch_ops import ConeGeometry, ConePlan
+    nx, ny, nz, nu, nv, nview = 512, 512, 128, 736, 736, 25
+    g = ConeGeometry(nx=nx, ny=ny, nz=nz, dx=0.8, dy=0.8, dz=1.0, nu=nu, nv=nv, du=0.6, dv=0.6)
+    dc, du, dv, src = tomo_geometry(nview)
+    plan = ConePlan(g, dc, du, dv, src, device=dev)
+    img = ellipsoid_phantom(nx, ny, nz, 0.8, 0.8, 1.0, np.random.default_rng(11), device=dev)[None, :, :, :, None]
+    img = img.contiguous()
+    prj = plan.project(img)
+    back = torch.empty_like(img)
+    peak, kind = measured_peaks()
+    out = {"workload": "the tomosynthesis workload above (512x512x128 @0.8x0.8x1.0 mm, 736x736 @0.6 mm, 25 views "
+                       "over +-20 deg), Siddon ray lengths: FP, then its exact transpose",
+           "model": "5.2 B per update (one 4-byte read per piece, ~1.3 pieces)"}
+    for name, f, upd in (("fp", lambda: plan.project(img, out=prj), nview * nu * nv * nz),
+                         ("bp", lambda: plan.backproject(prj, out=back), nx * ny * nz * nview)):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        ach = 5.2 * upd / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "updates": upd, "gupd_s": upd / ms / 1e6,
+                     "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                  "peak_kind": kind}}
+    if cpu_sample:
+        from oracle import oracle as O
+        from types import SimpleNamespace
+        O.set_threads(os.cpu_count() or 1)
+        gg = SimpleNamespace(dx=0.8, dy=0.8, dz=1.0, cx=0.0, cy=0.0, cz=0.0, du=0.6, dv=0.6, off_u=0.0, off_v=0.0)
+        vol = img.cpu().numpy()
+        # one view, the central 128 detector rows (the sample's rows are
+        # centred on the detector centre like the full detector's)
+        t0 = time.perf_counter()
+        O.cone_fp(vol, dc[:1], du[:1], dv[:1], src[:1], gg, nu, 128)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"fp_gupd_s": nu * 128 * nz / dt / 1e9, "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": "the central 128 detector rows of one view, FP64 OpenMP oracle "
+                                         "(exact crossings)"}
+    del plan
+    return out
+
+
 def filter_run(dev, cpu_sample=True):
     """Ramp filter (Filter.cu): 64 fan sinograms of 888 channels x 1152 views,
     Ram-Lak window.  The filter is a linear convolution of every view with the
@@ -612,6 +760,7 @@ def run_b200(args):
     if rank == 0 and not args.no_extras:
         extras["siddon"] = siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=world == 1)
         extras["tomo"] = tomo_run(dev, cpu_sample=world == 1)
+        extras["siddon_cone"] = cone_run(dev, cpu_sample=world == 1)
         extras["filter"] = filter_run(dev, cpu_sample=world == 1)
 
     cpu = None
