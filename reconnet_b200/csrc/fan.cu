@@ -811,12 +811,20 @@ __device__ __forceinline__ void split_hilo(double v, float& h, float& l) {
     l = (float)(v - (double)h);
 }
 
+// s + e = a + b exactly (TwoSum).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
 __device__ __forceinline__ void bp_siddon_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
                                             int imax, int x, int y0, int nu) {
     const float A = (float)x - vg.par;
     const TCubic c = t_cubic(vg, A * __fdividef(1.0f, (float)(y0 + kBmRows / 2) - vg.perp));
-    float Ah, Al;
+    float Ah, Al, Dh0, Dl0;
     split_hilo(vg.pard - (double)x, Ah, Al);
+    split_hilo((double)y0 - vg.perpd, Dh0, Dl0);
     float tp = 0.f, tnp = 0.f;
 #pragma unroll
     for (int j = 0; j <= kBmRows; j++) {
@@ -824,9 +832,10 @@ __device__ __forceinline__ void bp_siddon_x(float (&acc)[kBmRows], const BpView&
         const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
         const float tn = __shfl_down_sync(0xffffffffu, t, 1);
         if (j > 0) {
-            float Dh, Dl;
-            split_hilo((double)(y0 + j - 1) - vg.perpd, Dh, Dl);
-            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al, Dh, Dl);
+            // line y0 + j - 1 minus perp, stepped exactly from the first line
+            float Dh, e;
+            two_sum(Dh0, (float)(j - 1), Dh, e);
+            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al, Dh, Dl0 + e);
         }
         tp = t;
         tnp = tn;
@@ -838,8 +847,9 @@ __device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView&
     const float g = __fdividef(1.0f, (float)x - vg.perp);
     const float r0 = ((float)y0 - vg.par) * g;
     const TCubic c = t_cubic(vg, fmaf((float)(kBmRows / 2), g, r0));
-    float Dh, Dl;
+    float Dh, Dl, Ah0, Al0;
     split_hilo((double)x - vg.perpd, Dh, Dl);
+    split_hilo(vg.pard - (double)y0, Ah0, Al0);
     float tp = 0.f, tnp = 0.f;
 #pragma unroll
     for (int j = 0; j <= kBmRows; j++) {
@@ -847,9 +857,10 @@ __device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView&
         const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
         const float tn = __shfl_down_sync(0xffffffffu, t, 1);
         if (j > 0) {
-            float Ah, Al;
-            split_hilo(vg.pard - (double)(y0 + j - 1), Ah, Al);
-            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al, Dh, Dl);
+            // par minus position y0 + j - 1, stepped exactly from the first
+            float Ah, e;
+            two_sum(Ah0, -(float)(j - 1), Ah, e);
+            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al0 + e, Dh, Dl);
         }
         tp = t;
         tnp = tn;
@@ -962,12 +973,6 @@ __device__ __forceinline__ float pd_sample(const float4* T, int ilo, int imax, f
     return val * il2;
 }
 
-// s + e = a + b exactly (TwoSum).
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-    s = a + b;
-    const float bb = s - a;
-    e = (a - (s - bb)) + (b - bb);
-}
 
 // X-class view: lane column q = x, pixel rows y0 + j (centres l = y0 + j + 1/2).
 __device__ __forceinline__ void bp_pixel_x(float (&acc)[kBmRows], const BpView& vg, const float4* T, int ilo,
