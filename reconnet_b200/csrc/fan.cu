@@ -573,8 +573,9 @@ struct BpParams {
 
 // Per-view parameters the BP inner loop reads, staged in shared memory.
 // Siddon BP table: per view, entry u + 1 holds the slope of ray u as hi / lo
-// floats and c_u = w_u * (ray length per band), w_u the sinogram value mixed
-// over the slice's detector rows.
+// floats, c_u = w_u * (ray length per band), w_u the sinogram value mixed
+// over the slice's detector rows, and 1 / |r_u| (0 for rays within 1e-6 of
+// the line normal).
 __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin,
                                     int ns, const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
                                     const double* __restrict__ cslopes, FanDims d, float4* __restrict__ tab,
@@ -601,7 +602,7 @@ __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice
         const double r = cslopes[(long long)gv * (nu + 1) + u];
         const float c = w * (float)sqrt(r * r * along * along + across * across);
         const float rh = (float)r;
-        out[u + 1] = make_float4(rh, (float)(r - (double)rh), c, 0.f);
+        out[u + 1] = make_float4(rh, (float)(r - (double)rh), c, fabs(r) > 1e-6 ? (float)(1.0 / fabs(r)) : 0.f);
     }
     if (lane == 0) {
         out[0] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -783,13 +784,21 @@ __device__ __forceinline__ void bp_matched_y(float (&acc)[kBmRows], const BpView
 // Contribution of one candidate ray: its position at line l relative to the
 // pixel, x = (par - q) + r (l - perp), from hi / lo parts (A = par - q and D =
 // l - perp as hi / lo floats, r from the table), to ~1e-7 cells.
+// The fraction of the band interval inside [0, 1] is 1 exactly when the
+// interval lies inside, and its overlap times 1 / |r| (E.w) otherwise; rays
+// within 1e-6 of the line normal (E.w = 0) take the point test.
 __device__ __forceinline__ float siddon_candidate(const float4 E, float Ah, float Al, float Dh, float Dl) {
     const float xa = fmaf(E.x, Dh, Ah) + fmaf(E.y, Dh, fmaf(E.x, Dl, Al));
     const float xb = xa + E.x;
     const float lo = fminf(xa, xb), hi = fmaxf(xa, xb);
     const float ov = fmaxf(0.f, fminf(hi, 1.f) - fmaxf(lo, 0.f));
-    const float w = hi - lo;
-    return E.z * (w > 1e-7f ? __fdividef(ov, w) : ((xa >= 0.f && xa < 1.f) ? 1.f : 0.f));
+    const float fr = (lo >= 0.f && hi <= 1.f) ? 1.f : ov * E.w;
+    return E.z * (E.w != 0.f ? fr : ((xa >= 0.f && xa < 1.f) ? 1.f : 0.f));
+}
+
+// floor(x) for |x| < 2^22 on the FMA / ALU pipes (round-down add of 1.5 * 2^23).
+__device__ __forceinline__ int floor_small(float x) {
+    return __float_as_int(__fadd_rd(x, 12582912.0f)) - 0x4B400000;
 }
 
 // Sum over the candidate rays of a pixel: the first two unrolled (most pixels
@@ -797,8 +806,8 @@ __device__ __forceinline__ float siddon_candidate(const float4 E, float Ah, floa
 __device__ __forceinline__ float siddon_pixel(const float4* T, int ilo, int imax, int nu, float t00, float t01,
                                               float t10, float t11, float Ah, float Al, float Dh, float Dl) {
     const float tmin = fminf(fminf(t00, t01), fminf(t10, t11)), tmax = fmaxf(fmaxf(t00, t01), fmaxf(t10, t11));
-    const int u0 = max(max((int)ceilf(tmin - 0.5f - 1e-3f), 0), ilo - 1);
-    const int u1 = min(min((int)floorf(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
+    const int u0 = max(max(-floor_small(0.5f + 1e-3f - tmin), 0), ilo - 1);
+    const int u1 = min(min(floor_small(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
     float v = 0.f;
     if (u0 <= u1) v = siddon_candidate(T[u0 + 1 - ilo], Ah, Al, Dh, Dl);
     if (u0 + 1 <= u1) v += siddon_candidate(T[u0 + 2 - ilo], Ah, Al, Dh, Dl);
