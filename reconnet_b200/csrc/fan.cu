@@ -568,7 +568,25 @@ struct BpParams {
     int type;
     int tiles_x, tiles_y;
     int win;           // staged table entries per view
+    // view split for small batches: CTA part k of a tile takes the k-th
+    // share of the views and writes its partial image to parts + k *
+    // part_stride (summed afterwards by bp_parts_sum_kernel)
+    int nparts;
+    long long part_stride;
+    float* parts;
 };
+
+// out[i] = (accumulate ? out[i] : 0) + sum over k of parts[k * stride + i],
+// the parts summed first, in a fixed order (deterministic; accumulating adds
+// exactly the value a non-accumulating call writes).
+__global__ void bp_parts_sum_kernel(float* __restrict__ out, const float* __restrict__ parts, int nparts,
+                                    long long stride, long long n, int accumulate) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float v = 0.f;
+        for (int k = 0; k < nparts; k++) v += parts[k * stride + i];
+        out[i] = accumulate ? out[i] + v : v;
+    }
+}
 
 
 // Per-view parameters the BP inner loop reads, staged in shared memory.
@@ -1068,14 +1086,25 @@ __global__ void __launch_bounds__(kBpThreads, (kMode == 2 || kMode == 0) ? 3 : 0
     float4* const buf0 = reinterpret_cast<float4*>(smem + off);   // buffer b at buf0 + b * kBpViews * win
 
     const int tiles_per_slice = p.tiles_x * p.tiles_y;
-    const int si = blockIdx.x / tiles_per_slice;
-    const int ti = blockIdx.x - si * tiles_per_slice;
+    const int part = blockIdx.x % p.nparts;
+    const int bid = blockIdx.x / p.nparts;
+    const int si = bid / tiles_per_slice;
+    const int ti = bid - si * tiles_per_slice;
     const int tyi = ti / p.tiles_x;
     const int txi = ti - tyi * p.tiles_x;
     const BpSlice bs = p.bps[p.s_begin + si];
-    const GeoSet gs = p.sets[bs.set];
-    const float4* gtab = p.tab + (bs.table_off - p.tab_base);
+    GeoSet gs = p.sets[bs.set];
     const int nu = p.d.nu, nx = p.d.nx, ny = p.d.ny;
+    const float4* gtab = p.tab + (bs.table_off - p.tab_base);
+    if (p.nparts > 1) {
+        // this part's share of the views, in whole chunks
+        const int nch = (gs.nview + kBpViews - 1) / kBpViews;
+        const int cpp = (nch + p.nparts - 1) / p.nparts;
+        const int vb = min(gs.nview, part * cpp * kBpViews), ve = min(gs.nview, (part + 1) * cpp * kBpViews);
+        gs.view_off += vb;
+        gs.nview = ve - vb;
+        gtab += (long long)vb * (nu + 2);
+    }
     const int tid = threadIdx.x;
     // Column-warp tiles: lane i of warp w owns pixel column X0 + i and rows
     // Y0 + 16 w .. + 15 (lane 31's column belongs to the next tile: it only
@@ -1166,14 +1195,15 @@ __global__ void __launch_bounds__(kBpThreads, (kMode == 2 || kMode == 0) ? 3 : 0
     }
     if (!ok) return;
 
-    float* out = p.img + bs.img_off;
+    float* out = (p.nparts > 1 ? p.parts + part * p.part_stride : p.img) + bs.img_off;
+    const bool add = p.nparts == 1 && p.accumulate;
     if (lane < kBmCols && x0 < nx) {
 #pragma unroll
         for (int j = 0; j < kBmRows; j++) {
             const int iy = y0 + j;
             if (iy < ny) {
                 float* q = out + (long long)x0 * p.d.isx + (long long)iy * p.d.isy;
-                *q = p.accumulate ? (*q + acc[j]) : acc[j];
+                *q = add ? (*q + acc[j]) : acc[j];
             }
         }
     }
@@ -1475,13 +1505,44 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         bp.tiles_x = tiles_x;
         bp.tiles_y = tiles_y;
         bp.win = win;
-        unsigned grid = (unsigned)(ns * tiles_x * tiles_y);
+        // a batch too small to fill the GPU (one wave, fewer than two CTAs
+        // per resident slot) splits every tile's views over several CTAs
+        bp.nparts = 1;
+        bp.part_stride = 0;
+        bp.parts = nullptr;
+        const long long ctas = (long long)ns * tiles_x * tiles_y;
+        const long long target = 2LL * 148 * 3;
+        if (s0 == 0 && s1 == nbp && ctas < target) {
+            const int nch = (maxv + kBpViews - 1) / kBpViews;
+            const int want = (int)std::min<long long>(std::min<long long>(kBpMaxParts, (target + ctas - 1) / ctas), nch);
+            if (want > 1) {
+                const long long need = (long long)want * p->img_elems;
+                if (need > p->bp_parts_cap) {
+                    cudaFree(p->d_bp_parts);
+                    p->d_bp_parts = nullptr;
+                    p->bp_parts_cap = 0;
+                    RN_CUDA_TRY(cudaMalloc(&p->d_bp_parts, sizeof(float) * need));
+                    p->bp_parts_cap = need;
+                }
+                bp.nparts = want;
+                bp.part_stride = p->img_elems;
+                bp.parts = p->d_bp_parts;
+            }
+        }
+        unsigned grid = (unsigned)(ns * tiles_x * tiles_y * bp.nparts);
         LaunchScope ls3(p, st, 3);
         if (pixel) fan_bp_kernel<3><<<grid, kBpThreads, smem, st>>>(bp);
         else if (siddon) fan_bp_kernel<2><<<grid, kBpThreads, smem, st>>>(bp);
         else if (type == RN_TYPE_MATCHED) fan_bp_kernel<1><<<grid, kBpThreads, smem, st>>>(bp);
         else fan_bp_kernel<0><<<grid, kBpThreads, smem, st>>>(bp);
         RN_CUDA_TRY(cudaGetLastError());
+        if (bp.nparts > 1) {
+            LaunchScope ls4(p, st, 4);
+            const long long n = p->img_elems;
+            bp_parts_sum_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 8), 256, 0, st>>>(
+                d_img, bp.parts, bp.nparts, bp.part_stride, n, accumulate);
+            RN_CUDA_TRY(cudaGetLastError());
+        }
         s0 = s1;
     }
     return RN_OK;

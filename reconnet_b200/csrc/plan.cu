@@ -75,7 +75,19 @@ static void set_dims(rn_fan_plan* p, long long isx, long long isy) {
 }
 
 static void build_fp_work(rn_fan_plan* p) {
-    const int VT = fan_fp_views(p->g.nu);
+    // views per work item: at most the kernel's table capacity, fewer when a
+    // small batch would leave SMs idle (one CTA per SM; aim for two waves).
+    // A ray's sum does not depend on which views share its CTA.
+    int VT = fan_fp_views(p->g.nu);
+    auto items = [&](int vt) {
+        long long n = 0;
+        for (size_t s = 0; s < p->h_fp.size(); s++) {
+            const GeoSet& gs = p->h_sets[p->h_fp[s].set];
+            n += (gs.nxv + vt - 1) / vt + (gs.nview - gs.nxv + vt - 1) / vt;
+        }
+        return n;
+    };
+    while (VT > 1 && items(VT) < 2LL * 148) VT--;
     p->h_fp_work.clear();
     for (size_t s = 0; s < p->h_fp.size(); s++) {
         const GeoSet& gs = p->h_sets[p->h_fp[s].set];
@@ -168,6 +180,7 @@ int rn_version(void) { return 1; }
 
 int rn_fan_plan_destroy(rn_fan_plan* p) {
     if (!p) return RN_OK;
+    cudaFree(p->d_bp_parts);
     cudaFree(p->d_views);
     cudaFree(p->d_edges);
     cudaFree(p->d_cell);

@@ -75,6 +75,7 @@ constexpr int kBpThreads = 256;
 constexpr int kBmCols = 31;
 constexpr int kBmRows = 16;
 constexpr int kBmTileY = kBmRows * (kBpThreads / 32);
+constexpr int kBpMaxParts = 16;   // most view parts of a split backprojection
 
 struct BpSlice {
     long long img_off;
@@ -155,6 +156,8 @@ struct rn_fan_plan {
     float4* d_tab = nullptr;        // BP edge tables
     long long tab_elems = 0;
     float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, lazily allocated)
+    float* d_bp_parts = nullptr;    // partial images of a view-split backprojection (lazily allocated)
+    long long bp_parts_cap = 0;     // elements
     float* d_tmp_prj = nullptr;     // sinogram-sized scratch (SQS update, lazily allocated)
 
     // instrumentation: kernel launch count and optional per-kernel CUDA-event

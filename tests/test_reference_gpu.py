@@ -82,9 +82,16 @@ def test_reference_host_call_timing(ref, rng):
     p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     args = (1, 1, 512, 512, 1, 1.0, 1.0, 2.0, rn.nu, ang.size, 1, rn.da, rn.dv, 0.0, 0.0, rn.dsd, rn.dso)
     ts = {}
-    for name, fn in (("reference", lambda: (lib.cDistanceDrivenFanProjection(p(sino), p(img), p(ang), *args, 0),
-                                            lib.cDistanceDrivenFanBackprojection(p(bp), p(sino), p(ang), *args, 0))),
-                     ("b200", lambda: (rn.cDDFanProjection4d(img, ang), rn.cDDFanBackprojection4d(sino, ang)))):
+    calls = [("reference", lambda: (lib.cDistanceDrivenFanProjection(p(sino), p(img), p(ang), *args, 0),
+                                    lib.cDistanceDrivenFanBackprojection(p(bp), p(sino), p(ang), *args, 0))),
+             ("b200", lambda: (rn.cDDFanProjection4d(img, ang), rn.cDDFanBackprojection4d(sino, ang)))]
+    if hasattr(lib, "cSiddonFanProjection"):
+        # the Siddon pair, the other path with a published host-call time
+        calls += [("reference_siddon", lambda: (lib.cSiddonFanProjection(p(sino), p(img), p(ang), *args, 0),
+                                                lib.cSiddonFanBackprojection(p(bp), p(sino), p(ang), *args, 0))),
+                  ("b200_siddon", lambda: (rn.cSiddonFanProjection4d(img, ang),
+                                           rn.cSiddonFanBackprojection4d(sino, ang)))]
+    for name, fn in calls:
         fn()
         t0 = time.perf_counter()
         for _ in range(5):
@@ -93,6 +100,10 @@ def test_reference_host_call_timing(ref, rng):
     print(f"\nFP+BP host call, 512x512 736x720: reference {ts['reference']*1e3:.2f} ms, "
           f"b200 {ts['b200']*1e3:.2f} ms")
     assert ts["b200"] < ts["reference"]
+    if "b200_siddon" in ts:
+        print(f"Siddon FP+BP host call: reference {ts['reference_siddon']*1e3:.2f} ms, "
+              f"b200 {ts['b200_siddon']*1e3:.2f} ms")
+        assert ts["b200_siddon"] < ts["reference_siddon"]
 
 
 def test_siddon_vs_reference_kernels(ref, rng):
