@@ -584,6 +584,36 @@ def cone_run(dev, cpu_sample=True):
     return out
 
 
+def host_calls_run(geom, counts, angles, imgs):
+    """The drop-in path: every slice of the batch through the reference-named
+    host entry points cDistanceDrivenFanProjection + ...Backprojection
+    (typeProjector 0, as the reference arm's `reference_gpu` calls the
+    reference's library), host arrays in and out, one call pair per slice
+    (each slice has its own angles, so each call builds its plan)."""
+    from reconnet_b200.reconnet import ReconNet
+    rn = ReconNet()
+    for k in ("nx", "ny", "dx", "dy", "nu", "da", "dsd", "dso"):
+        setattr(rn, k, getattr(geom, k))
+    rn.nz, rn.nv, rn.dz, rn.dv, rn.off_a, rn.off_v = 1, 1, geom.dz, geom.dv, geom.off_a, geom.off_v
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    imgs5 = [np.ascontiguousarray(im[None, :, :, None, None]) for im in imgs]
+    angs = [np.ascontiguousarray(angles[offs[s]:offs[s + 1]]) for s in range(len(counts))]
+
+    def one_step():
+        for s in range(len(counts)):
+            sino = rn.cDDFanProjection4d(imgs5[s], angs[s])
+            rn.cDDFanBackprojection4d(sino, angs[s], type_projector=0)
+
+    one_step()
+    t0 = time.perf_counter()
+    one_step()
+    dt = time.perf_counter() - t0
+    upd = int(np.sum(counts)) * (geom.nu * geom.ny + geom.nx * geom.ny)
+    return {"value": upd / dt / 1e9, "unit": UNIT, "ms_per_step": dt * 1e3,
+            "api": "reference-named host entry points, per slice, host arrays (numpy) in and out, "
+                   "typeProjector 0; wall time of one step after one warm-up step"}
+
+
 def filter_run(dev, cpu_sample=True):
     """Ramp filter (Filter.cu): 64 fan sinograms of 888 channels x 1152 views,
     Ram-Lak window.  The filter is a linear convolution of every view with the
@@ -755,6 +785,7 @@ def run_b200(args):
                   "H2D and D2H on two copy streams overlapping the FP + BP of the neighbouring steps",
            "serial_ms_per_step": ms_serial / e2e_steps}
 
+    host_calls = host_calls_run(geom, counts, angles, imgs) if rank == 0 and not args.no_extras else None
     ossqs = None if args.no_ossqs else ossqs_run(plan, geom, counts, angles, x, args.ossqs_iters, dev)
     extras = {}
     if rank == 0 and not args.no_extras:
@@ -778,6 +809,8 @@ def run_b200(args):
                 "clocks": clk.summary()}
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if host_calls is not None:
+            line["e2e_host_calls"] = host_calls
         if ossqs is not None:
             line["ossqs_tv"] = ossqs
         line.update(extras)
