@@ -1259,7 +1259,7 @@ int fan_kernel_attributes() {
     return RN_OK;
 }
 
-int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
+int fan_build_geometry(rn_fan_plan* p, const float* host_deg, FanGeoHost& gh) {
     const RnFanGeom& g = p->g;
     const int nu = g.nu;
     const int64_t V = p->total_views;
@@ -1267,21 +1267,27 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
 
     // per-edge (sin, cos) of the fan angle gamma_e; edge e sits at
     // a_e + du/2 of cell e (DistanceDriven.cu:83,90)
-    std::vector<double2> esc(nu + 1);
+    std::vector<double2>& esc = gh.esc;
+    esc.resize(nu + 1);
     for (int e = 0; e <= nu; e++) {
         double gam = (-((double)e - 0.5 - (nu - 1) / 2.0) - off_u) * du;
         esc[e] = make_double2(std::sin(gam), std::cos(gam));
     }
-    std::vector<float2> cell(nu);
+    std::vector<float2>& cell = gh.cell;
+    cell.resize(nu);
     for (int u = 0; u < nu; u++) {
         double a = (-((double)u - (nu - 1) / 2.0) - off_u) * du;
         cell[u] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
 
-    std::vector<ViewGeo> vg(V);
-    std::vector<double2> vcs(V);
-    std::vector<int> vx(V);
-    std::vector<int> perm(V);
+    std::vector<ViewGeo>& vg = gh.views;
+    std::vector<double2>& vcs = gh.vcs;
+    std::vector<int>& vx = gh.vx;
+    std::vector<int>& perm = gh.perm;
+    vg.resize(V);
+    vcs.resize(V);
+    vx.resize(V);
+    perm.resize(V);
     const double dmax_mm = g.dso + std::sqrt(std::pow(g.nx * (double)g.dx / 2 + std::fabs(g.cx), 2) +
                                              std::pow(g.ny * (double)g.dy / 2 + std::fabs(g.cy), 2));
     double margin = 0.0;
@@ -1349,49 +1355,27 @@ int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     p->dims.spx = line_stride(p->dims.lpx);
     p->dims.spy = line_stride(p->dims.lpy);
 
-    RN_CUDA_TRY(cudaMalloc(&p->d_views, sizeof(ViewGeo) * V));
-    RN_CUDA_TRY(cudaMalloc(&p->d_edges, sizeof(double) * V * (nu + 1)));
-    RN_CUDA_TRY(cudaMalloc(&p->d_cell, sizeof(float2) * nu));
-    RN_CUDA_TRY(cudaMalloc(&p->d_perm, sizeof(int) * V));
-    RN_CUDA_TRY(cudaMalloc(&p->d_sets, sizeof(GeoSet) * p->h_sets.size()));
-    double2* d_vcs = nullptr;
-    int* d_vx = nullptr;
-    double2* d_esc = nullptr;
-    RN_CUDA_TRY(cudaMalloc(&d_vcs, sizeof(double2) * V));
-    RN_CUDA_TRY(cudaMalloc(&d_vx, sizeof(int) * V));
-    RN_CUDA_TRY(cudaMalloc(&d_esc, sizeof(double2) * (nu + 1)));
-    RN_CUDA_TRY(cudaMemcpyAsync(p->d_views, vg.data(), sizeof(ViewGeo) * V, cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(p->d_cell, cell.data(), sizeof(float2) * nu, cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(p->d_perm, perm.data(), sizeof(int) * V, cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(p->d_sets, p->h_sets.data(), sizeof(GeoSet) * p->h_sets.size(),
-                                cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(d_vcs, vcs.data(), sizeof(double2) * V, cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(d_vx, vx.data(), sizeof(int) * V, cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(d_esc, esc.data(), sizeof(double2) * (nu + 1), cudaMemcpyHostToDevice, st));
-    long long n = (long long)V * (nu + 1);
-    edge_slope_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p->d_edges, d_vcs, d_vx, d_esc, (int)V, nu, g.dx,
-                                                                     g.dy);
-    RN_CUDA_TRY(cudaGetLastError());
     // slopes of the rays through the cell centres (the Siddon pair): the same
     // table with the fan angle of cell u itself (entry nu repeats a spacing on)
-    {
-        std::vector<double2> csc(nu + 1);
-        for (int e = 0; e <= nu; e++) {
-            double gam = (-((double)e - (nu - 1) / 2.0) - off_u) * du;
-            csc[e] = make_double2(std::sin(gam), std::cos(gam));
-        }
-        RN_CUDA_TRY(cudaMalloc(&p->d_cslopes, sizeof(double) * V * (nu + 1)));
-        RN_CUDA_TRY(cudaMemcpyAsync(d_esc, csc.data(), sizeof(double2) * (nu + 1), cudaMemcpyHostToDevice, st));
-        edge_slope_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p->d_cslopes, d_vcs, d_vx, d_esc, (int)V, nu,
-                                                                         g.dx, g.dy);
-        RN_CUDA_TRY(cudaGetLastError());
-        RN_CUDA_TRY(cudaStreamSynchronize(st));   // csc goes out of scope
+    gh.csc.resize(nu + 1);
+    for (int e = 0; e <= nu; e++) {
+        double gam = (-((double)e - (nu - 1) / 2.0) - off_u) * du;
+        gh.csc[e] = make_double2(std::sin(gam), std::cos(gam));
     }
-    RN_CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFree(d_vcs);
-    cudaFree(d_vx);
-    cudaFree(d_esc);
     p->h_sets.shrink_to_fit();
+    return RN_OK;
+}
+
+int fan_slope_tables(rn_fan_plan* p, const double2* d_vcs, const int* d_vx, const double2* d_esc,
+                     const double2* d_csc, cudaStream_t st) {
+    const RnFanGeom& g = p->g;
+    const long long n = (long long)p->total_views * (g.nu + 1);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    edge_slope_kernel<<<blocks, 256, 0, st>>>(p->d_edges, d_vcs, d_vx, d_esc, (int)p->total_views, g.nu, g.dx, g.dy);
+    RN_CUDA_TRY(cudaGetLastError());
+    edge_slope_kernel<<<blocks, 256, 0, st>>>(p->d_cslopes, d_vcs, d_vx, d_csc, (int)p->total_views, g.nu, g.dx,
+                                              g.dy);
+    RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
 
@@ -1451,12 +1435,63 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
     return RN_OK;
 }
 
+// Backprojection slices of `type`: Siddon rows per image slice; matched: the
+// transpose of the FP z mixing; reference modes and pixel-driven: rows mixed
+// at the slice's v.
+static const std::vector<BpSlice>& bp_slices(const rn_fan_plan* p, int type) {
+    return type == RN_TYPE_SIDDON ? p->h_bps : (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
+}
+
+// End of the launch that starts at slice s0: as many slices as fit in the
+// table scratch (at least one).
+static int bp_wave_end(const rn_fan_plan* p, const std::vector<BpSlice>& bps, int s0) {
+    const int nbp = (int)bps.size();
+    const long long base = bps[s0].table_off;
+    int s1 = s0;
+    while (s1 < nbp) {
+        const GeoSet& gs = p->h_sets[bps[s1].set];
+        long long end = bps[s1].table_off + (long long)gs.nview * (p->dims.nu + 2);
+        if (end - base > p->tab_elems && s1 > s0) break;
+        s1++;
+    }
+    return s1;
+}
+
+static int bp_max_views(const rn_fan_plan* p, const std::vector<BpSlice>& bps, int s0, int s1) {
+    int maxv = 0;
+    for (int s = s0; s < s1; s++) maxv = std::max(maxv, p->h_sets[bps[s].set].nview);
+    return maxv;
+}
+
+// A batch too small to fill the GPU (one launch, fewer than two CTAs per
+// resident slot) splits every tile's views over several CTAs.
+static int bp_parts(const rn_fan_plan* p, const std::vector<BpSlice>& bps, int s0, int s1) {
+    if (s0 != 0 || s1 != (int)bps.size()) return 1;
+    const FanDims& d = p->dims;
+    const long long tiles = (long long)((d.nx + kBmCols - 1) / kBmCols) * ((d.ny + kBmTileY - 1) / kBmTileY);
+    const long long ctas = (long long)(s1 - s0) * tiles;
+    const long long target = 2LL * 148 * 3;
+    if (ctas >= target) return 1;
+    const int nch = (bp_max_views(p, bps, s0, s1) + kBpViews - 1) / kBpViews;
+    const int want = (int)std::min<long long>(std::min<long long>(kBpMaxParts, (target + ctas - 1) / ctas), nch);
+    return std::max(1, want);
+}
+
+int fan_bp_split(const rn_fan_plan* p, int type, int* first_wave_slices) {
+    const std::vector<BpSlice>& bps = bp_slices(p, type);
+    if (bps.empty()) {
+        if (first_wave_slices) *first_wave_slices = 0;
+        return 1;
+    }
+    const int s1 = bp_wave_end(p, bps, 0);
+    if (first_wave_slices) *first_wave_slices = s1;
+    return bp_parts(p, bps, 0, s1);
+}
+
 int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st) {
     const FanDims& d = p->dims;
     const bool siddon = type == RN_TYPE_SIDDON, pixel = type == RN_TYPE_PIXEL;
-    // slices: Siddon rows per image slice; matched: the transpose of the FP z
-    // mixing; reference modes and pixel-driven: rows mixed at the slice's v
-    const std::vector<BpSlice>& bps = siddon ? p->h_bps : (type == RN_TYPE_MATCHED) ? p->h_bp : p->h_bpr;
+    const std::vector<BpSlice>& bps = bp_slices(p, type);
     const BpSlice* dbp = siddon ? p->d_bps : (type == RN_TYPE_MATCHED) ? p->d_bp : p->d_bpr;
     const int nbp = (int)bps.size();
     const int win = p->table_win_m;
@@ -1464,18 +1499,10 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
     const int tiles_x = (d.nx + kBmCols - 1) / kBmCols, tiles_y = (d.ny + kBmTileY - 1) / kBmTileY;
     int s0 = 0;
     while (s0 < nbp) {
-        // as many slices as fit in the table scratch
-        int s1 = s0;
-        long long base = bps[s0].table_off;
-        while (s1 < nbp) {
-            const GeoSet& gs = p->h_sets[bps[s1].set];
-            long long end = bps[s1].table_off + (long long)gs.nview * (d.nu + 2);
-            if (end - base > p->tab_elems && s1 > s0) break;
-            s1++;
-        }
-        int ns = s1 - s0;
-        int maxv = 0;
-        for (int s = s0; s < s1; s++) maxv = std::max(maxv, p->h_sets[bps[s].set].nview);
+        const int s1 = bp_wave_end(p, bps, s0);
+        const long long base = bps[s0].table_off;
+        const int ns = s1 - s0;
+        const int maxv = bp_max_views(p, bps, s0, s1);
         dim3 tg((maxv + 7) / 8, ns);
         {
             LaunchScope ls2(p, st, 2);
@@ -1505,29 +1532,15 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         bp.tiles_x = tiles_x;
         bp.tiles_y = tiles_y;
         bp.win = win;
-        // a batch too small to fill the GPU (one wave, fewer than two CTAs
-        // per resident slot) splits every tile's views over several CTAs
+        // the plan sized d_bp_parts for the split of every type
         bp.nparts = 1;
         bp.part_stride = 0;
         bp.parts = nullptr;
-        const long long ctas = (long long)ns * tiles_x * tiles_y;
-        const long long target = 2LL * 148 * 3;
-        if (s0 == 0 && s1 == nbp && ctas < target) {
-            const int nch = (maxv + kBpViews - 1) / kBpViews;
-            const int want = (int)std::min<long long>(std::min<long long>(kBpMaxParts, (target + ctas - 1) / ctas), nch);
-            if (want > 1) {
-                const long long need = (long long)want * p->img_elems;
-                if (need > p->bp_parts_cap) {
-                    cudaFree(p->d_bp_parts);
-                    p->d_bp_parts = nullptr;
-                    p->bp_parts_cap = 0;
-                    RN_CUDA_TRY(cudaMalloc(&p->d_bp_parts, sizeof(float) * need));
-                    p->bp_parts_cap = need;
-                }
-                bp.nparts = want;
-                bp.part_stride = p->img_elems;
-                bp.parts = p->d_bp_parts;
-            }
+        const int want = bp_parts(p, bps, s0, s1);
+        if (want > 1 && (long long)want * p->img_elems <= p->bp_parts_cap) {
+            bp.nparts = want;
+            bp.part_stride = p->img_elems;
+            bp.parts = p->d_bp_parts;
         }
         unsigned grid = (unsigned)(ns * tiles_x * tiles_y * bp.nparts);
         LaunchScope ls3(p, st, 3);

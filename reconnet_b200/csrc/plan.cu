@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -117,6 +118,68 @@ static int table_window(const RnFanGeom& g, int tw, int th) {
     return std::min(win, g.nu + 2);
 }
 
+// ---------------------------------------------------------------------------
+// Plan memory.  All tables and scratch of a plan share one device allocation,
+// filled by one upload.  A destroyed plan's allocation is kept for the next
+// plan on that device (one per device, at most kArenaKeepBytes), so a plan
+// rebuilt for new angles (the host entry points do this whenever the angles
+// change) calls neither cudaMalloc nor cudaFree.
+// ---------------------------------------------------------------------------
+static const size_t kArenaKeepBytes = 256ull << 20;
+struct KeptArena {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+static std::mutex g_arena_mu;
+static std::vector<KeptArena> g_kept;   // indexed by device
+
+static int arena_acquire(int dev, size_t bytes, void** out, size_t* got) {
+    void* stale = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        if ((int)g_kept.size() > dev && g_kept[dev].ptr) {
+            if (g_kept[dev].bytes >= bytes) {
+                *out = g_kept[dev].ptr;
+                *got = g_kept[dev].bytes;
+                g_kept[dev] = KeptArena();
+                return RN_OK;
+            }
+            stale = g_kept[dev].ptr;   // too small for this plan
+            g_kept[dev] = KeptArena();
+        }
+    }
+    if (stale) cudaFree(stale);
+    RN_CUDA_TRY(cudaMalloc(out, bytes));
+    *got = bytes;
+    return RN_OK;
+}
+
+// The caller has synchronised the device: no launch still reads `ptr`.
+static void arena_release(int dev, void* ptr, size_t bytes) {
+    if (!ptr) return;
+    if (bytes > kArenaKeepBytes || dev < 0) {
+        cudaFree(ptr);
+        return;
+    }
+    void* old = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        if ((int)g_kept.size() <= dev) g_kept.resize(dev + 1);
+        old = g_kept[dev].ptr;
+        g_kept[dev].ptr = ptr;
+        g_kept[dev].bytes = bytes;
+    }
+    if (old) cudaFree(old);
+}
+
+// One region of the plan allocation; `src` (when set) is uploaded into it.
+struct ArenaPart {
+    void** dst;
+    size_t bytes;
+    const void* src;
+    size_t src_bytes;
+};
+
 static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     const RnFanGeom& g = p->g;
     const int win_m = table_window(g, kBmCols, kBmTileY);
@@ -124,37 +187,15 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     if (win_m > 800) return set_error(RN_ERR_ARG, "fan geometry: backprojection tile window too large");
     p->table_win_m = win_m;
     RN_TRY(fan_kernel_attributes());
-    RN_TRY(fan_build_geometry(p, host_deg, st));
+    FanGeoHost gh;
+    RN_TRY(fan_build_geometry(p, host_deg, gh));
     build_fp_work(p);
-
-    RN_CUDA_TRY(cudaMalloc(&p->d_fp, sizeof(FpSlice) * p->h_fp.size()));
-    RN_CUDA_TRY(cudaMalloc(&p->d_bp, sizeof(BpSlice) * p->h_bp.size()));
-    RN_CUDA_TRY(cudaMalloc(&p->d_bpr, sizeof(BpSlice) * p->h_bpr.size()));
-    RN_CUDA_TRY(cudaMalloc(&p->d_fps, sizeof(FpSlice) * p->h_fps.size()));
-    RN_CUDA_TRY(cudaMalloc(&p->d_bps, sizeof(BpSlice) * p->h_bps.size()));
-    RN_CUDA_TRY(cudaMalloc(&p->d_fp_work, sizeof(int4) * std::max(1, p->n_fp_work)));
-    RN_CUDA_TRY(cudaMalloc(&p->d_err, sizeof(int)));
-    RN_CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
-    RN_CUDA_TRY(cudaMemcpyAsync(p->d_fp, p->h_fp.data(), sizeof(FpSlice) * p->h_fp.size(), cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(cudaMemcpyAsync(p->d_bp, p->h_bp.data(), sizeof(BpSlice) * p->h_bp.size(), cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(
-        cudaMemcpyAsync(p->d_bpr, p->h_bpr.data(), sizeof(BpSlice) * p->h_bpr.size(), cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(
-        cudaMemcpyAsync(p->d_fps, p->h_fps.data(), sizeof(FpSlice) * p->h_fps.size(), cudaMemcpyHostToDevice, st));
-    RN_CUDA_TRY(
-        cudaMemcpyAsync(p->d_bps, p->h_bps.data(), sizeof(BpSlice) * p->h_bps.size(), cudaMemcpyHostToDevice, st));
-    if (p->n_fp_work > 0)
-        RN_CUDA_TRY(cudaMemcpyAsync(p->d_fp_work, p->h_fp_work.data(), sizeof(int4) * p->n_fp_work,
-                                    cudaMemcpyHostToDevice, st));
 
     // line scratch
     const FanDims& d = p->dims;
     p->line_slot_elems = (long long)d.ny * d.spx + (long long)d.nx * d.spy;
     long long slot_bytes = p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float));
     p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(), kLineBudget / slot_bytes));
-    RN_CUDA_TRY(cudaMalloc(&p->d_hl, sizeof(float2) * p->fp_slots * p->line_slot_elems));
-    RN_CUDA_TRY(cudaMalloc(&p->d_la, sizeof(float) * p->fp_slots * p->line_slot_elems));
-
     // table scratch: all slices if within budget, else at least the largest slice
     long long need = 0, largest = 0;
     for (const BpSlice& b : p->h_bp) {
@@ -163,8 +204,66 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
         largest = std::max(largest, n);
     }
     p->tab_elems = std::max(largest, std::min(need, kTableBudget / (long long)sizeof(float4)));
-    RN_CUDA_TRY(cudaMalloc(&p->d_tab, sizeof(float4) * p->tab_elems));
-    RN_CUDA_TRY(cudaStreamSynchronize(st));
+    // partial images of a split backprojection: the most any type asks for
+    long long parts = 1;
+    for (int type : {RN_TYPE_ITERATIVE, RN_TYPE_MATCHED, RN_TYPE_SIDDON})
+        parts = std::max<long long>(parts, fan_bp_split(p, type, nullptr));
+    p->bp_parts_cap = parts > 1 ? parts * p->img_elems : 0;
+
+    const long long V = p->total_views, nu = g.nu;
+    double2 *d_vcs = nullptr, *d_esc = nullptr, *d_csc = nullptr;
+    int* d_vx = nullptr;
+    std::vector<ArenaPart> up, dev;
+    auto upload = [&](auto** dst, const auto& vec) {
+        const size_t n = vec.size() * sizeof(vec[0]);
+        up.push_back(ArenaPart{reinterpret_cast<void**>(dst), std::max<size_t>(n, 16), vec.data(), n});
+    };
+    auto device = [&](auto** dst, size_t bytes) {
+        dev.push_back(ArenaPart{reinterpret_cast<void**>(dst), std::max<size_t>(bytes, 16), nullptr, 0});
+    };
+    upload(&p->d_views, gh.views);
+    upload(&p->d_cell, gh.cell);
+    upload(&p->d_perm, gh.perm);
+    upload(&p->d_sets, p->h_sets);
+    upload(&p->d_fp, p->h_fp);
+    upload(&p->d_bp, p->h_bp);
+    upload(&p->d_bpr, p->h_bpr);
+    upload(&p->d_fps, p->h_fps);
+    upload(&p->d_bps, p->h_bps);
+    upload(&p->d_fp_work, p->h_fp_work);
+    upload(&d_vcs, gh.vcs);
+    upload(&d_vx, gh.vx);
+    upload(&d_esc, gh.esc);
+    upload(&d_csc, gh.csc);
+    device(&p->d_err, sizeof(int));
+    device(&p->d_edges, sizeof(double) * V * (nu + 1));
+    device(&p->d_cslopes, sizeof(double) * V * (nu + 1));
+    device(&p->d_hl, sizeof(float2) * p->fp_slots * p->line_slot_elems);
+    device(&p->d_la, sizeof(float) * p->fp_slots * p->line_slot_elems);
+    device(&p->d_tab, sizeof(float4) * p->tab_elems);
+    if (p->bp_parts_cap > 0) device(&p->d_bp_parts, sizeof(float) * p->bp_parts_cap);
+
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t upload_bytes = 0;
+    for (const ArenaPart& a : up) upload_bytes = align(upload_bytes + a.bytes);
+    size_t total = upload_bytes;
+    for (const ArenaPart& a : dev) total = align(total + a.bytes);
+    RN_TRY(arena_acquire(p->device, total, &p->d_arena, &p->arena_bytes));
+    std::vector<unsigned char> blob(upload_bytes, 0);
+    size_t off = 0;
+    for (const ArenaPart& a : up) {
+        *a.dst = static_cast<unsigned char*>(p->d_arena) + off;
+        if (a.src_bytes) memcpy(blob.data() + off, a.src, a.src_bytes);
+        off = align(off + a.bytes);
+    }
+    for (const ArenaPart& a : dev) {
+        *a.dst = static_cast<unsigned char*>(p->d_arena) + off;
+        off = align(off + a.bytes);
+    }
+    RN_CUDA_TRY(cudaMemcpyAsync(p->d_arena, blob.data(), upload_bytes, cudaMemcpyHostToDevice, st));
+    RN_CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+    RN_TRY(fan_slope_tables(p, d_vcs, d_vx, d_esc, d_csc, st));
+    RN_CUDA_TRY(cudaStreamSynchronize(st));   // blob and gh go out of scope
     return RN_OK;
 }
 
@@ -180,23 +279,16 @@ int rn_version(void) { return 1; }
 
 int rn_fan_plan_destroy(rn_fan_plan* p) {
     if (!p) return RN_OK;
-    cudaFree(p->d_bp_parts);
-    cudaFree(p->d_views);
-    cudaFree(p->d_edges);
-    cudaFree(p->d_cell);
-    cudaFree(p->d_perm);
-    cudaFree(p->d_sets);
-    cudaFree(p->d_fp);
-    cudaFree(p->d_bp);
-    cudaFree(p->d_bpr);
-    cudaFree(p->d_fps);
-    cudaFree(p->d_bps);
-    cudaFree(p->d_cslopes);
-    cudaFree(p->d_fp_work);
-    cudaFree(p->d_err);
-    cudaFree(p->d_hl);
-    cudaFree(p->d_la);
-    cudaFree(p->d_tab);
+    if (p->d_arena) {
+        // as cudaFree would, wait until no launch on the device still reads
+        // the plan; after an error keep nothing
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != p->device) cudaSetDevice(p->device);
+        if (cudaDeviceSynchronize() == cudaSuccess) arena_release(p->device, p->d_arena, p->arena_bytes);
+        else cudaFree(p->d_arena);
+        if (cur >= 0 && cur != p->device) cudaSetDevice(cur);
+    }
     cudaFree(p->d_tmp_img);
     cudaFree(p->d_tmp_prj);
     for (auto& t : p->timed) {

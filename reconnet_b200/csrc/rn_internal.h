@@ -156,9 +156,13 @@ struct rn_fan_plan {
     float4* d_tab = nullptr;        // BP edge tables
     long long tab_elems = 0;
     float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, lazily allocated)
-    float* d_bp_parts = nullptr;    // partial images of a view-split backprojection (lazily allocated)
+    float* d_bp_parts = nullptr;    // partial images of a view-split backprojection
     long long bp_parts_cap = 0;     // elements
     float* d_tmp_prj = nullptr;     // sinogram-sized scratch (SQS update, lazily allocated)
+    // every device table and scratch above except the two lazily allocated
+    // ones lives in this one allocation
+    void* d_arena = nullptr;
+    size_t arena_bytes = 0;
 
     // instrumentation: kernel launch count and optional per-kernel CUDA-event
     // timing (kinds: 0 line prologue, 1 forward projection, 2 edge tables,
@@ -200,7 +204,26 @@ struct LaunchScope {
         if (idx >= 0) cudaEventRecord(p->timed[idx].stop, st);
     }
 };
-int fan_build_geometry(rn_fan_plan* p, const float* host_deg, cudaStream_t st);
+// Host-side geometry tables of a fan plan, built by fan_build_geometry and
+// uploaded with the rest of the plan.
+struct FanGeoHost {
+    std::vector<ViewGeo> views;
+    std::vector<double2> vcs;       // per view (cos theta, sin theta)
+    std::vector<int> vx;            // per view: 1 for the X class
+    std::vector<int> perm;          // class-sorted view order per set
+    std::vector<double2> esc;       // per detector edge (sin, cos) of its fan angle
+    std::vector<double2> csc;       // per cell centre (sin, cos); entry nu one spacing on
+    std::vector<float2> cell;       // per cell (cos a_u, sin a_u)
+};
+// Fills the host tables and the line padding of p->dims (no device work).
+int fan_build_geometry(rn_fan_plan* p, const float* host_deg, FanGeoHost& gh);
+// Device slope tables d_edges / d_cslopes from the uploaded per-view and
+// per-edge terms.
+int fan_slope_tables(rn_fan_plan* p, const double2* d_vcs, const int* d_vx, const double2* d_esc,
+                     const double2* d_csc, cudaStream_t st);
+// Parts over which fan_backproject splits a backprojection of `type` (1 when
+// it does not split), and the number of slices in its first launch.
+int fan_bp_split(const rn_fan_plan* p, int type, int* first_wave_slices);
 int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st, bool siddon = false);
 int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st);
 }  // namespace rn
