@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-ossqs", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis, cone and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
+    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter"],
+                    help="run only this extra measurement (one GPU) and print its JSON object")
     return ap.parse_args()
 
 
@@ -820,9 +822,34 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_extra(args):
+    """One extra measurement alone (for profiling a single kernel family)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cpu = not args.no_cpu_baseline
+    if args.extra == "siddon":
+        from reconnet_b200.torch_ops import FanPlan
+        geom, counts, angles, imgs = workload(0, args.slices)
+        plan = FanPlan(geom, angles, nbatches=args.slices, nview_per_slice=counts, device=dev)
+        x = torch.from_numpy(imgs).to(dev)
+        p = torch.empty(plan.sino_shape, device=dev)
+        b = torch.empty(plan.img_shape, device=dev)
+        out = siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=cpu)
+    elif args.extra == "tomo":
+        out = tomo_run(dev, cpu_sample=cpu)
+    elif args.extra == "cone":
+        out = cone_run(dev, cpu_sample=cpu)
+    else:
+        out = filter_run(dev, cpu_sample=cpu)
+    print(json.dumps({args.extra: out}), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.extra and args.impl == "b200":
+        run_extra(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

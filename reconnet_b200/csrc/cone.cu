@@ -341,6 +341,115 @@ __device__ __forceinline__ bool bp_separable(float& acc, const ConeView& V, int 
     return true;
 }
 
+// Backprojection for plans whose views are all separable the same way.  Call
+// U the lateral axis that follows the detector's u and V the one that follows
+// v; the slopes are r_U(iu) = rU0 + iu rU1 and r_V(iv) = rV0 + iv rV1.  A
+// warp holds the voxels along V (lanes) at one U index pu and one main-axis
+// index pm.  For a view, the rays that can meet those voxels along U and
+// their parameter intervals inside [pu, pu + 1] are the same for every lane:
+// lane k computes candidate k's interval, clipped to the slab [0, 1] and to
+// the segment's ends along m, into shared memory.  Each lane then walks its
+// own V candidates and, for each, the warp's U intervals: pair (iu, iv) adds
+// seg x prj x |T_U(iu) n T_V(iv)|, the same sum as bp_separable with each
+// interval computed once instead of once per pair.
+constexpr int kSepWarps = 8;
+
+__device__ __forceinline__ void sep_range(double X0, double G, float rs, int n, int& i0, int& i1) {
+    const float lo = -fmaxf(rs, 0.f) - 0.02f, hi = 1.f - fminf(rs, 0.f) + 0.02f;
+    const float x0 = (float)X0, ig = __fdividef(1.f, (float)G);
+    const float q0 = (lo - x0) * ig, q1 = (hi - x0) * ig;
+    i0 = max(0, (int)ceilf(fmaxf(fminf(q0, q1), -1e9f)));
+    i1 = min(n - 1, (int)floorf(fminf(fmaxf(q0, q1), 1e9f)));
+}
+
+__global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ img, const float* __restrict__ prj,
+                                                           const ConeView* __restrict__ views, ConeDims cd,
+                                                           int accumulate) {
+    __shared__ float4 s_u[kSepWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m = views[0].m;
+    const bool a_is_u = views[0].affine == 1;
+    const int ax_u = a_is_u ? views[0].a : views[0].b, ax_v = a_is_u ? views[0].b : views[0].a;
+    const int nU = ax_u == 0 ? cd.n[0] : ax_u == 1 ? cd.n[1] : cd.n[2];
+    const int nV = ax_v == 0 ? cd.n[0] : ax_v == 1 ? cd.n[1] : cd.n[2];
+    const int nM = m == 0 ? cd.n[0] : m == 1 ? cd.n[1] : cd.n[2];
+    const long long w = (long long)blockIdx.x * kSepWarps + warp;
+    if (w >= (long long)nU * nM) return;   // the whole warp
+    const int pu = (int)(w % nU), pm = (int)(w / nU);
+    const int pv = blockIdx.y * 32 + lane;
+    const bool live = pv < nV;
+    const int bc = blockIdx.z;
+    const int c = bc % cd.nc, bt = bc / cd.nc;
+    const float dU = ax_u == 0 ? cd.d[0] : ax_u == 1 ? cd.d[1] : cd.d[2];
+    const float dV = ax_v == 0 ? cd.d[0] : ax_v == 1 ? cd.d[1] : cd.d[2];
+    const float dM = m == 0 ? cd.d[0] : m == 1 ? cd.d[1] : cd.d[2];
+    const float dU2 = dU * dU, dV2 = dV * dV, dM2 = dM * dM;
+    const long long su = (long long)cd.nview * cd.nv * cd.nc;
+    const int sv = cd.nc;
+    const float* pb = prj + bt * cd.prj_b + c;
+    float acc = 0.f;
+    for (int view = 0; view < cd.nview; view++) {
+        const ConeView& V = views[view];
+        const double M = (double)pm - V.S[m];
+        // the segment's ends along m, relative to the voxel's low face
+        const float e0 = (float)(-M), e1 = (float)(-M + V.Dm0);
+        const float clo = fmaxf(0.f, fminf(e0, e1)), chi = fminf(1.f, fmaxf(e0, e1));
+        if (!(chi > clo)) continue;
+        const double rU0 = a_is_u ? V.rho[0] : V.rho[3], rU1 = a_is_u ? V.rho[1] : V.rho[4];
+        const double rV0 = a_is_u ? V.rho[3] : V.rho[0], rV1 = a_is_u ? V.rho[5] : V.rho[2];
+        const double AU = V.S[ax_u] - (double)pu, AV = V.S[ax_v] - (double)pv;
+        const float iM = __fdividef(1.f, (float)M);
+        const double XU0 = AU + M * rU0, GU = M * rU1, XV0 = AV + M * rV0, GV = M * rV1;
+        int i0, i1, j0, j1;
+        sep_range(XU0, GU, (float)(-AU) * iM, cd.nu, i0, i1);
+        sep_range(XV0, GV, (float)(-AV) * iM, cd.nv, j0, j1);
+        if (!live) j1 = j0 - 1;
+        // this lane's V candidates: offsets from FP64 for the first, then
+        // FP32 steps
+        const float xv0 = (float)fma((double)j0, GV, XV0), gv = (float)GV;
+        const float rvj = (float)(rV0 + j0 * rV1), rv1f = (float)rV1;
+        const float* pview = pb + (long long)view * cd.nv * cd.nc;
+        for (int base = i0; base <= i1; base += 32) {
+            const int nk = min(32, i1 - base + 1);
+            __syncwarp();
+            if (lane < nk) {
+                const int i = base + lane;
+                const float xu = (float)fma((double)i, GU, XU0);
+                const float ru = (float)fma((double)i, rU1, rU0);
+                const float iru = fabsf(ru) > 1e-30f ? __fdividef(1.f, ru) : 1e30f;
+                const float t0 = -xu * iru, t1 = (1.f - xu) * iru;
+                s_u[warp][lane] = make_float4(fmaxf(clo, fminf(t0, t1)), fminf(chi, fmaxf(t0, t1)), ru * ru * dU2,
+                                              __int_as_float(i));
+            }
+            __syncwarp();
+            for (int j = j0; j <= j1; j++) {
+                const float kj = (float)(j - j0);
+                const float xv = fmaf(kj, gv, xv0), rv = fmaf(kj, rv1f, rvj);
+                const float irv = fabsf(rv) > 1e-30f ? __fdividef(1.f, rv) : 1e30f;
+                const float tv0 = -xv * irv, tv1 = (1.f - xv) * irv;
+                const float lv = fminf(tv0, tv1), hv = fmaxf(tv0, tv1);
+                const float qv = fmaf(rv * rv, dV2, dM2);
+                const float* pcol = pview + j * sv;
+                for (int k = 0; k < nk; k++) {
+                    const float4 E = s_u[warp][k];
+                    const float tl = fmaxf(lv, E.x), th = fminf(hv, E.y);
+                    if (th > tl) {
+                        const float q = E.z + qv;
+                        acc = fmaf((th - tl) * (q * rsqrtf(q)), __ldg(pcol + (long long)__float_as_int(E.w) * su),
+                                   acc);
+                    }
+                }
+            }
+        }
+    }
+    if (!live) return;
+    const int x = ax_u == 0 ? pu : ax_v == 0 ? pv : pm;
+    const int y = ax_u == 1 ? pu : ax_v == 1 ? pv : pm;
+    const int z = ax_u == 2 ? pu : ax_v == 2 ? pv : pm;
+    float* o = img + bt * cd.img_b + ((long long)x * cd.st[0] + (long long)y * cd.st[1] + (long long)z * cd.st[2]) + c;
+    *o = accumulate ? *o + acc : acc;
+}
+
 // One thread per voxel (z fastest) of slice `bc` = b * nc + c.
 // `fast` is the grid axis that runs along the lanes of a warp: z (the
 // image's contiguous axis) by default, or the lateral axis that follows the
@@ -438,6 +547,7 @@ struct rn_cone_plan {
     float4* d_rays = nullptr;
     int lanes_v = 0;           // forward projection: warps along the detector's v
     int bp_fast = 2;           // backprojection: grid axis along the lanes
+    bool bp_sep = false;       // every view separable the same way (cone_bp_sep_kernel)
     bool unit = true;          // every ray's lateral slopes are at most 1
     long long launches = 0;
 };
@@ -614,6 +724,7 @@ int rn_cone_plan_create(rn_cone_plan** out, const RnConeGeom* g, const float* ho
         for (const ConeView& v : views)
             same = same && v.affine != 0 && v.affine == views[0].affine && v.a == views[0].a && v.b == views[0].b;
         if (same) p->bp_fast = views[0].affine == 1 ? views[0].b : views[0].a;
+        p->bp_sep = same;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const long long nrays = (long long)g->nview * g->nv * g->nu;
@@ -665,9 +776,18 @@ int rn_cone_backproject(rn_cone_plan* p, float* d_img, const float* d_prj, int a
     const long long nvox = (long long)cd.n[0] * cd.n[1] * cd.n[2];
     const int slices = cd.nb * cd.nc;
     if (slices > 65535) return set_error(RN_ERR_ARG, "cone backprojection: too many batches x channels");
-    dim3 grid((unsigned)((nvox + 255) / 256), slices);
-    cone_bp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_rays, p->d_views, cd, accumulate,
-                                                            p->bp_fast);
+    if (p->bp_sep) {
+        // one warp per (U, m) voxel line segment of 32 along V
+        const int nv_axis = cd.n[p->bp_fast];
+        const long long lines = nvox / nv_axis;
+        dim3 grid((unsigned)((lines + kSepWarps - 1) / kSepWarps), (unsigned)((nv_axis + 31) / 32), slices);
+        cone_bp_sep_kernel<<<grid, 32 * kSepWarps, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_views, cd,
+                                                                             accumulate);
+    } else {
+        dim3 grid((unsigned)((nvox + 255) / 256), slices);
+        cone_bp_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_rays, p->d_views, cd, accumulate,
+                                                                p->bp_fast);
+    }
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
