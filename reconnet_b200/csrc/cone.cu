@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -253,6 +254,215 @@ __global__ void __launch_bounds__(256) cone_fp_kernel(float* __restrict__ prj, c
         }
         acc *= R.seg;
     }
+    prj[bt * cd.prj_b + (((long long)iu * cd.nview + view) * cd.nv + iv) * cd.nc + c] = acc;
+}
+
+// Forward projection with the voxels staged in shared memory (|r| <= 1).
+// The block's rays advance through chunks of kFpZ slabs along m.  For each
+// chunk the block reduces the lateral voxel index range its rays touch (a
+// ray's positions are monotone along m, so its range is spanned by its
+// entry into the chunk and its exit), copies that brick into shared memory
+// as one plane per slab (voxels outside the grid as 0), and the rays take
+// their pieces from there with the arithmetic of slab_sum<true>, so the sums
+// are the same to the bit.  A warp's gathers then hit shared memory instead
+// of ~15 sectors of L1 per load.  A chunk whose brick is larger than a plane
+// falls back to loads from global memory.  `vec`: the main axis is the
+// image's contiguous axis and every group of 4 voxels along it starts
+// 16-byte aligned, so the copy loads float4.
+constexpr int kFpZ = 16;         // slabs per chunk
+constexpr int kFpPlane = 640;    // floats per staged slab plane
+
+// Fractional part of a fixed-point position plus 1, in [1, 2).
+__device__ __forceinline__ float fixed_frac1(long long p) { return __uint_as_float(0x3f800000u | ((unsigned)p >> 9)); }
+
+// Slabs [0, n) of one ray through a staged chunk: A, B are the ray's
+// fixed-point positions at its first slab and advance past the last; `pl` is
+// the plane of the first slab; jf = that slab's index from the ray's first.
+// kClip: some slab of the chunk holds an end of the segment (otherwise every
+// slab is whole: tlo = 0, thi = 1).
+template <bool kClip>
+__device__ __forceinline__ void staged_run(float& acc, long long& A, long long& B, const RayStep& R, int n, float jf,
+                                           const float* pl, int P, int Na, int alo, int blo) {
+    const long long oa = (long long)alo << 32, ob = (long long)blo << 32;
+    long long Ar = A - oa, Br = B - ob;
+    // (pa ? 1 - f : f) * ira as one FMA on f + 1 (the same rounding)
+    const float sA = R.pa ? -R.ira : R.ira, oA = R.pa ? 2.f * R.ira : -R.ira;
+    const float sB = R.pb ? -R.irb : R.irb, oB = R.pb ? 2.f * R.irb : -R.irb;
+    int ca = (int)(Ar >> 32), cb = (int)(Br >> 32);
+    int i0 = cb * Na + ca;
+    for (int j = 0; j < n; j++) {
+        const float fa1 = fixed_frac1(Ar), fb1 = fixed_frac1(Br);
+        Ar += R.RA;
+        Br += R.RB;
+        const int ca1 = (int)(Ar >> 32), cb1 = (int)(Br >> 32);
+        const float ta = ca1 != ca ? fmaf(sA, fa1, oA) : 2.f;
+        const float tb = cb1 != cb ? fmaf(sB, fb1, oB) : 2.f;
+        const float t1 = fminf(ta, tb), t2 = fmaxf(ta, tb);
+        const bool afirst = ta < tb;
+        const int i1 = cb1 * Na + ca1;
+        const int im = afirst ? cb * Na + ca1 : cb1 * Na + ca;
+        float l0, lm, l1;
+        if (kClip) {
+            const float tlo = fmaxf(0.f, R.slo - jf), thi = fminf(1.f, R.shi - jf);
+            l0 = fminf(t1, thi) - tlo;
+            lm = fminf(t2, thi) - fmaxf(t1, tlo);
+            l1 = thi - fmaxf(t2, tlo);
+            jf += 1.f;
+        } else {
+            l0 = fminf(t1, 1.f);
+            lm = fminf(t2, 1.f) - t1;
+            l1 = 1.f - t2;
+        }
+        float s = 0.f;
+        if (l0 > 0.f) s = l0 * pl[i0];
+        if (lm > 0.f) s = fmaf(lm, pl[im], s);
+        if (l1 > 0.f) s = fmaf(l1, pl[i1], s);
+        acc += s;
+        ca = ca1;
+        cb = cb1;
+        i0 = i1;
+        pl += P;
+    }
+    A = Ar + oa;
+    B = Br + ob;
+}
+
+__global__ void __launch_bounds__(256) cone_fp_staged_kernel(float* __restrict__ prj, const float* __restrict__ img,
+                                                              const ConeView* __restrict__ views, ConeDims cd,
+                                                              int lanes_v, int vec) {
+    extern __shared__ float brick[];   // kFpZ planes of stride P
+    __shared__ int4 s_part[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int iu = lanes_v ? blockIdx.x * 8 + warp : blockIdx.x * 32 + lane;
+    const int iv = lanes_v ? blockIdx.y * 32 + lane : blockIdx.y * 8 + warp;
+    const bool valid = iu < cd.nu && iv < cd.nv;
+    int zi = blockIdx.z;
+    const int c = zi % cd.nc;
+    zi /= cd.nc;
+    const int view = zi % cd.nview;
+    const int bt = zi / cd.nview;
+    const ConeView& V = views[view];
+    const int m = V.m, a = V.a, b = V.b;
+    RayStep R = cone_ray_step(V, min(iu, cd.nu - 1), min(iv, cd.nv - 1), cd, m, a, b);
+    if (!valid) R.ns = 0;
+    const int sta = (int)(a == 0 ? cd.st[0] : a == 1 ? cd.st[1] : cd.st[2]);
+    const int stb = (int)(b == 0 ? cd.st[0] : b == 1 ? cd.st[1] : cd.st[2]);
+    const int stm = (int)(m == 0 ? cd.st[0] : m == 1 ? cd.st[1] : cd.st[2]);
+    const int na = a == 0 ? cd.n[0] : a == 1 ? cd.n[1] : cd.n[2];
+    const int nb = b == 0 ? cd.n[0] : b == 1 ? cd.n[1] : cd.n[2];
+    const int nm = m == 0 ? cd.n[0] : m == 1 ? cd.n[1] : cd.n[2];
+    const bool vec4 = vec && m == 2;
+    const float* vol = img + bt * cd.img_b + c;
+    // the block's slabs
+    int klo = R.ns > 0 ? R.k0 : INT_MAX, khi = R.ns > 0 ? R.k0 + R.ns : INT_MIN;
+    klo = __reduce_min_sync(0xffffffffu, klo);
+    khi = __reduce_max_sync(0xffffffffu, khi);
+    if (lane == 0) s_part[warp] = make_int4(klo, khi, 0, 0);
+    __syncthreads();
+    {
+        const int4 q = s_part[lane & 7];
+        klo = __reduce_min_sync(0xffffffffu, q.x);
+        khi = __reduce_max_sync(0xffffffffu, q.y);
+    }
+    __syncthreads();
+    long long A = R.A, B = R.B;
+    int kk = R.k0;                       // this ray's next slab
+    const int kend = R.k0 + R.ns;
+    float acc = 0.f;
+    for (int K = klo >= khi ? khi : (klo / kFpZ) * kFpZ; K < khi; K += kFpZ) {
+        const int js = max(K, kk), je = min(K + kFpZ, kend);
+        const bool act = js < je;
+        int alo = INT_MAX, ahi = INT_MIN, blo = INT_MAX, bhi = INT_MIN;
+        if (act) {
+            const long long Ae = A + (long long)(je - js) * R.RA, Be = B + (long long)(je - js) * R.RB;
+            const int a0 = (int)(A >> 32), a1 = (int)(Ae >> 32), b0 = (int)(B >> 32), b1 = (int)(Be >> 32);
+            alo = min(a0, a1);
+            ahi = max(a0, a1);
+            blo = min(b0, b1);
+            bhi = max(b0, b1);
+        }
+        alo = __reduce_min_sync(0xffffffffu, alo);
+        ahi = __reduce_max_sync(0xffffffffu, ahi);
+        blo = __reduce_min_sync(0xffffffffu, blo);
+        bhi = __reduce_max_sync(0xffffffffu, bhi);
+        if (lane == 0) s_part[warp] = make_int4(alo, ahi, blo, bhi);
+        __syncthreads();
+        {
+            const int4 q = s_part[lane & 7];
+            alo = __reduce_min_sync(0xffffffffu, q.x);
+            ahi = __reduce_max_sync(0xffffffffu, q.y);
+            blo = __reduce_min_sync(0xffffffffu, q.z);
+            bhi = __reduce_max_sync(0xffffffffu, q.w);
+        }
+        // brick planes of stride P = 2 (mod 32): the copy's stores are free
+        // of bank conflicts
+        const long long Na_l = (long long)ahi - alo + 1, Nb_l = (long long)bhi - blo + 1;
+        const bool any = ahi >= alo && bhi >= blo;
+        const long long cols = any ? Na_l * Nb_l : 0;
+        const long long P_l = cols <= 2 ? 2 : ((cols - 2 + 31) / 32) * 32 + 2;
+        const bool staged = any && P_l <= kFpPlane;
+        const float jf = (float)(js - R.k0);
+        if (staged) {
+            const int Na = (int)Na_l, Nb = (int)Nb_l, P = (int)P_l;
+            if (vec4 && K + kFpZ <= nm) {
+                // 4 lanes per column, one float4 each
+                const int q = lane & 3;
+                for (int ib = warp; ib < Nb; ib += 8) {
+                    const int bb = blo + ib;
+                    const bool inb = (unsigned)bb < (unsigned)nb;
+                    for (int ia = lane >> 2; ia < Na; ia += 8) {
+                        const int aa = alo + ia;
+                        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (inb && (unsigned)aa < (unsigned)na)
+                            v = __ldg(reinterpret_cast<const float4*>(vol + (aa * sta + bb * stb + K + 4 * q)));
+                        float* d = brick + 4 * q * P + ib * Na + ia;
+                        d[0] = v.x;
+                        d[P] = v.y;
+                        d[2 * P] = v.z;
+                        d[3 * P] = v.w;
+                    }
+                }
+            } else {
+                // 16 lanes per column, one slab each
+                const int zc = lane & 15, k = K + zc;
+                for (int ib = warp; ib < Nb; ib += 8) {
+                    const int bb = blo + ib;
+                    const bool inb = (unsigned)bb < (unsigned)nb && k < nm;
+                    for (int ia = lane >> 4; ia < Na; ia += 2) {
+                        const int aa = alo + ia;
+                        float v = 0.f;
+                        if (inb && (unsigned)aa < (unsigned)na) v = __ldg(vol + (aa * sta + bb * stb + k * stm));
+                        brick[zc * P + ib * Na + ia] = v;
+                    }
+                }
+            }
+            __syncthreads();
+            if (act) {
+                const float* pl = brick + (js - K) * P;
+                if (R.slo <= jf && R.shi >= jf + (float)(je - js))
+                    staged_run<false>(acc, A, B, R, je - js, jf, pl, P, Na, alo, blo);
+                else
+                    staged_run<true>(acc, A, B, R, je - js, jf, pl, P, Na, alo, blo);
+            }
+        } else {
+            __syncthreads();   // every lane has read s_part before the next chunk writes it
+            if (act) {
+                const float* sl = vol + js * stm;
+                float jg = jf;
+                for (int k = js; k < je; k++) {
+                    acc += slab_sum<true>(A, R.RA, B, R.RB, R.pa, R.pb, R.ira, R.irb, fmaxf(0.f, R.slo - jg),
+                                          fminf(1.f, R.shi - jg), sl, sta, stb, na, nb);
+                    A += R.RA;
+                    B += R.RB;
+                    sl += stm;
+                    jg += 1.f;
+                }
+            }
+        }
+        if (act) kk = je;
+    }
+    if (!valid) return;
+    if (R.ns > 0) acc *= R.seg;
     prj[bt * cd.prj_b + (((long long)iu * cd.nview + view) * cd.nv + iv) * cd.nc + c] = acc;
 }
 
@@ -762,8 +972,14 @@ int rn_cone_project(rn_cone_plan* p, float* d_prj, const float* d_img, void* str
     const int gx = p->lanes_v ? (cd.nu + 7) / 8 : (cd.nu + 31) / 32;
     const int gy = p->lanes_v ? (cd.nv + 31) / 32 : (cd.nv + 7) / 8;
     dim3 grid(gx, gy, (unsigned)nz);
-    if (p->unit) cone_fp_kernel<true><<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd, p->lanes_v);
-    else cone_fp_kernel<false><<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd, p->lanes_v);
+    if (p->unit) {
+        // float4 copies when the voxels along z come in aligned groups of 4
+        const int vec = cd.nc == 1 && cd.n[2] % 4 == 0 && ((uintptr_t)d_img & 15) == 0;
+        cone_fp_staged_kernel<<<grid, 256, kFpZ * kFpPlane * sizeof(float), (cudaStream_t)stream>>>(
+            d_prj, d_img, p->d_views, cd, p->lanes_v, vec);
+    } else {
+        cone_fp_kernel<false><<<grid, 256, 0, (cudaStream_t)stream>>>(d_prj, d_img, p->d_views, cd, p->lanes_v);
+    }
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;

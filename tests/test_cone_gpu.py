@@ -136,7 +136,8 @@ def _sep_case(kind, B=1, C=1):
     along x with more than 32 voxels along v's axis ("swap"); main axis x
     with v along z, the image's contiguous axis ("xmain"); and detector cells
     so fine along u that a voxel's shadow covers more than 32 of them
-    ("fine")."""
+    ("fine"); and cells so coarse that a block's rays spread over more voxels
+    than the forward projector stages in shared memory ("coarse")."""
     import torch
     from reconnet_b200.torch_ops import ConeGeometry, ConePlan
     if kind == "swap":
@@ -157,6 +158,15 @@ def _sep_case(kind, B=1, C=1):
         dc = np.tile([-30.0, 0.5, -0.2], (n, 1))
         du = np.tile([0.0, 1.0, 0.0], (n, 1))
         dv = np.tile([0.0, 0.0, 1.0], (n, 1))
+    elif kind == "coarse":
+        g = dict(nx=150, ny=61, nz=16, dx=1.0, dy=1.0, dz=1.0, cx=0.3, cy=-0.2, cz=0.0, nu=40, nv=17, du=4.0,
+                 dv=3.5, off_u=0.2, off_v=-0.1)
+        n = 2
+        a = (np.arange(n) - 0.5) * 0.02
+        src = np.stack([1000 * np.sin(a), np.full(n, 1.0), 1000 * np.cos(a)], 1)
+        dc = np.tile([0.5, 0.0, -20.0], (n, 1))
+        du = np.tile([1.0, 0.0, 0.0], (n, 1))
+        dv = np.tile([0.0, 1.0, 0.0], (n, 1))
     else:   # fine
         g = dict(nx=6, ny=5, nz=4, dx=1.0, dy=1.0, dz=1.0, cx=0.1, cy=0.0, cz=0.0, nu=330, nv=12, du=0.025,
                  dv=0.6, off_u=0.4, off_v=0.0)
@@ -171,7 +181,7 @@ def _sep_case(kind, B=1, C=1):
     return NS(**g), geo, plan, torch
 
 
-SEP_CASES = ("swap", "xmain", "fine")
+SEP_CASES = ("swap", "xmain", "fine", "coarse")
 
 
 @pytest.mark.parametrize("kind", SEP_CASES)
