@@ -554,18 +554,19 @@ __device__ __forceinline__ bool bp_separable(float& acc, const ConeView& V, int 
 // Backprojection for plans whose views are all separable the same way.  Call
 // U the lateral axis that follows the detector's u and V the one that follows
 // v; the slopes are r_U(iu) = rU0 + iu rU1 and r_V(iv) = rV0 + iv rV1.  A
-// warp holds the voxels along V (lanes) at one U index pu and one main-axis
-// index pm.  For a view, the rays that can meet those voxels along U and
-// their parameter intervals inside [pu, pu + 1] are the same for every lane:
-// lane k computes candidate k's interval, clipped to the slab [0, 1] and to
-// the segment's ends along m, into shared memory.  Each lane then walks its
-// own V candidates and, for each, the warp's U intervals: pair (iu, iv) adds
-// seg x prj x |T_U(iu) n T_V(iv)|, the same sum as bp_separable with each
+// warp holds two neighbouring voxels along U (pu, pu + 1) for each of 32
+// voxels along V (lanes), at one main-axis index pm.  For a view, the rays
+// that can meet those voxels along U and their parameter intervals inside
+// [pu, pu + 1] and [pu + 1, pu + 2] are the same for every lane: lane k
+// computes candidate k's two intervals, clipped to the slab [0, 1] and to the
+// segment's ends along m, into shared memory.  Each lane then walks its own V
+// candidates and, for each, the warp's U candidates: pair (iu, iv) adds
+// seg x prj x |T_U(iu) n T_V(iv)| to each of its two voxels, with one load of
+// prj and one seg for both.  This is the sum of bp_separable with every
 // interval computed once instead of once per pair.
 constexpr int kSepWarps = 8;
 
-__device__ __forceinline__ void sep_range(double X0, double G, float rs, int n, int& i0, int& i1) {
-    const float lo = -fmaxf(rs, 0.f) - 0.02f, hi = 1.f - fminf(rs, 0.f) + 0.02f;
+__device__ __forceinline__ void sep_range(double X0, double G, float lo, float hi, int n, int& i0, int& i1) {
     const float x0 = (float)X0, ig = __fdividef(1.f, (float)G);
     const float q0 = (lo - x0) * ig, q1 = (hi - x0) * ig;
     i0 = max(0, (int)ceilf(fmaxf(fminf(q0, q1), -1e9f)));
@@ -575,7 +576,8 @@ __device__ __forceinline__ void sep_range(double X0, double G, float rs, int n, 
 __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ img, const float* __restrict__ prj,
                                                            const ConeView* __restrict__ views, ConeDims cd,
                                                            int accumulate) {
-    __shared__ float4 s_u[kSepWarps][32];
+    __shared__ float4 s_t[kSepWarps][32];   // {T lo, T hi} for voxel pu, then for pu + 1
+    __shared__ float2 s_q[kSepWarps][32];   // {r_U^2 dU^2, iu}
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int m = views[0].m;
     const bool a_is_u = views[0].affine == 1;
@@ -583,11 +585,12 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
     const int nU = ax_u == 0 ? cd.n[0] : ax_u == 1 ? cd.n[1] : cd.n[2];
     const int nV = ax_v == 0 ? cd.n[0] : ax_v == 1 ? cd.n[1] : cd.n[2];
     const int nM = m == 0 ? cd.n[0] : m == 1 ? cd.n[1] : cd.n[2];
+    const int nU2 = (nU + 1) / 2;
     const long long w = (long long)blockIdx.x * kSepWarps + warp;
-    if (w >= (long long)nU * nM) return;   // the whole warp
-    const int pu = (int)(w % nU), pm = (int)(w / nU);
+    if (w >= (long long)nU2 * nM) return;   // the whole warp
+    const int pu = 2 * (int)(w % nU2), pm = (int)(w / nU2);
     const int pv = blockIdx.y * 32 + lane;
-    const bool live = pv < nV;
+    const bool live = pv < nV, live1 = live && pu + 1 < nU;
     const int bc = blockIdx.z;
     const int c = bc % cd.nc, bt = bc / cd.nc;
     const float dU = ax_u == 0 ? cd.d[0] : ax_u == 1 ? cd.d[1] : cd.d[2];
@@ -597,7 +600,7 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
     const long long su = (long long)cd.nview * cd.nv * cd.nc;
     const int sv = cd.nc;
     const float* pb = prj + bt * cd.prj_b + c;
-    float acc = 0.f;
+    float acc0 = 0.f, acc1 = 0.f;
     for (int view = 0; view < cd.nview; view++) {
         const ConeView& V = views[view];
         const double M = (double)pm - V.S[m];
@@ -610,9 +613,14 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
         const double AU = V.S[ax_u] - (double)pu, AV = V.S[ax_v] - (double)pv;
         const float iM = __fdividef(1.f, (float)M);
         const double XU0 = AU + M * rU0, GU = M * rU1, XV0 = AV + M * rV0, GV = M * rV1;
+        // candidates: x in (-max(r, 0), 1 - min(r, 0)) from voxel pu (and
+        // x - 1 likewise from pu + 1), with r ~ the slope through the voxel
+        // corner, widened by 0.02
+        const float rs = (float)(-AU) * iM, rs1 = rs + iM, rv_s = (float)(-AV) * iM;
         int i0, i1, j0, j1;
-        sep_range(XU0, GU, (float)(-AU) * iM, cd.nu, i0, i1);
-        sep_range(XV0, GV, (float)(-AV) * iM, cd.nv, j0, j1);
+        sep_range(XU0, GU, -fmaxf(fmaxf(rs, rs1), 0.f) - 0.02f, 2.f - fminf(fminf(rs, rs1), 0.f) + 0.02f, cd.nu, i0,
+                  i1);
+        sep_range(XV0, GV, -fmaxf(rv_s, 0.f) - 0.02f, 1.f - fminf(rv_s, 0.f) + 0.02f, cd.nv, j0, j1);
         if (!live) j1 = j0 - 1;
         // this lane's V candidates: offsets from FP64 for the first, then
         // FP32 steps
@@ -627,13 +635,14 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
                 const float xu = (float)fma((double)i, GU, XU0);
                 const float ru = (float)fma((double)i, rU1, rU0);
                 const float iru = fabsf(ru) > 1e-30f ? __fdividef(1.f, ru) : 1e30f;
-                const float t0 = -xu * iru, t1 = (1.f - xu) * iru;
-                s_u[warp][lane] = make_float4(fmaxf(clo, fminf(t0, t1)), fminf(chi, fmaxf(t0, t1)), ru * ru * dU2,
-                                              __int_as_float(i));
+                const float t0 = -xu * iru, t1 = (1.f - xu) * iru, t2 = (2.f - xu) * iru;
+                s_t[warp][lane] = make_float4(fmaxf(clo, fminf(t0, t1)), fminf(chi, fmaxf(t0, t1)),
+                                              fmaxf(clo, fminf(t1, t2)), fminf(chi, fmaxf(t1, t2)));
+                s_q[warp][lane] = make_float2(ru * ru * dU2, __int_as_float(i));
             }
             __syncwarp();
-            for (int j = j0; j <= j1; j++) {
-                const float kj = (float)(j - j0);
+            float kj = 0.f;
+            for (int j = j0; j <= j1; j++, kj += 1.f) {
                 const float xv = fmaf(kj, gv, xv0), rv = fmaf(kj, rv1f, rvj);
                 const float irv = fabsf(rv) > 1e-30f ? __fdividef(1.f, rv) : 1e30f;
                 const float tv0 = -xv * irv, tv1 = (1.f - xv) * irv;
@@ -641,23 +650,29 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
                 const float qv = fmaf(rv * rv, dV2, dM2);
                 const float* pcol = pview + j * sv;
                 for (int k = 0; k < nk; k++) {
-                    const float4 E = s_u[warp][k];
-                    const float tl = fmaxf(lv, E.x), th = fminf(hv, E.y);
-                    if (th > tl) {
-                        const float q = E.z + qv;
-                        acc = fmaf((th - tl) * (q * rsqrtf(q)), __ldg(pcol + (long long)__float_as_int(E.w) * su),
-                                   acc);
+                    const float4 E = s_t[warp][k];
+                    const float l0 = fminf(hv, E.y) - fmaxf(lv, E.x), l1 = fminf(hv, E.w) - fmaxf(lv, E.z);
+                    if (l0 > 0.f || l1 > 0.f) {
+                        const float2 Q = s_q[warp][k];
+                        const float q = Q.x + qv;
+                        const float p = (q * rsqrtf(q)) * __ldg(pcol + (long long)__float_as_int(Q.y) * su);
+                        if (l0 > 0.f) acc0 = fmaf(l0, p, acc0);
+                        if (l1 > 0.f) acc1 = fmaf(l1, p, acc1);
                     }
                 }
             }
         }
     }
     if (!live) return;
-    const int x = ax_u == 0 ? pu : ax_v == 0 ? pv : pm;
-    const int y = ax_u == 1 ? pu : ax_v == 1 ? pv : pm;
-    const int z = ax_u == 2 ? pu : ax_v == 2 ? pv : pm;
-    float* o = img + bt * cd.img_b + ((long long)x * cd.st[0] + (long long)y * cd.st[1] + (long long)z * cd.st[2]) + c;
-    *o = accumulate ? *o + acc : acc;
+    auto out = [&](int qu, float v) {
+        const int x = ax_u == 0 ? qu : ax_v == 0 ? pv : pm;
+        const int y = ax_u == 1 ? qu : ax_v == 1 ? pv : pm;
+        const int z = ax_u == 2 ? qu : ax_v == 2 ? pv : pm;
+        float* o = img + bt * cd.img_b + ((long long)x * cd.st[0] + (long long)y * cd.st[1] + (long long)z * cd.st[2]) + c;
+        *o = accumulate ? *o + v : v;
+    };
+    out(pu, acc0);
+    if (live1) out(pu + 1, acc1);
 }
 
 // One thread per voxel (z fastest) of slice `bc` = b * nc + c.
@@ -758,6 +773,7 @@ struct rn_cone_plan {
     int lanes_v = 0;           // forward projection: warps along the detector's v
     int bp_fast = 2;           // backprojection: grid axis along the lanes
     bool bp_sep = false;       // every view separable the same way (cone_bp_sep_kernel)
+    ConeView h_view0;          // host copy of view 0 (axes of a separable plan)
     bool unit = true;          // every ray's lateral slopes are at most 1
     long long launches = 0;
 };
@@ -935,6 +951,7 @@ int rn_cone_plan_create(rn_cone_plan** out, const RnConeGeom* g, const float* ho
             same = same && v.affine != 0 && v.affine == views[0].affine && v.a == views[0].a && v.b == views[0].b;
         if (same) p->bp_fast = views[0].affine == 1 ? views[0].b : views[0].a;
         p->bp_sep = same;
+        p->h_view0 = views[0];
     }
     cudaStream_t st = (cudaStream_t)stream;
     const long long nrays = (long long)g->nview * g->nv * g->nu;
@@ -993,10 +1010,12 @@ int rn_cone_backproject(rn_cone_plan* p, float* d_img, const float* d_prj, int a
     const int slices = cd.nb * cd.nc;
     if (slices > 65535) return set_error(RN_ERR_ARG, "cone backprojection: too many batches x channels");
     if (p->bp_sep) {
-        // one warp per (U, m) voxel line segment of 32 along V
+        // one warp per 2 (U) x 32 (V) voxels at one m
+        const ConeView& v0 = p->h_view0;
+        const int ax_u = v0.affine == 1 ? v0.a : v0.b;
         const int nv_axis = cd.n[p->bp_fast];
-        const long long lines = nvox / nv_axis;
-        dim3 grid((unsigned)((lines + kSepWarps - 1) / kSepWarps), (unsigned)((nv_axis + 31) / 32), slices);
+        const long long warps = (long long)((cd.n[ax_u] + 1) / 2) * cd.n[v0.m];
+        dim3 grid((unsigned)((warps + kSepWarps - 1) / kSepWarps), (unsigned)((nv_axis + 31) / 32), slices);
         cone_bp_sep_kernel<<<grid, 32 * kSepWarps, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_views, cd,
                                                                              accumulate);
     } else {
