@@ -418,7 +418,8 @@ def tomo_run(dev, cpu_sample=True):
     512x512x128 voxels of 0.8x0.8x1.0 mm, a 736x736 flat detector of 0.6 mm
     cells 80 mm below the isocentre, 25 sources on a +-20 deg arc at 650 mm.
     Updates: FP = views * nu * nv * nz ray-plane integrals, BP = voxels * views;
-    algorithmic bytes 16 B per update (4 summed-area-table corners)."""
+    algorithmic bytes 16 B per update (the reference's 4 summed-area-table
+    corners, 4 B each)."""
     import ctypes
     import math
 
@@ -451,7 +452,7 @@ def tomo_run(dev, cpu_sample=True):
     out = {"workload": "tomosynthesis at configs[2] volume size: 512x512x128 @0.8x0.8x1.0 mm, 736x736 flat "
                        "detector @0.6 mm, 25 views over +-20 deg (configs[2]'s 360-deg cylindrical CT geometry has "
                        "no reference kernel; DistanceDriven3D is the reference's tomosynthesis pair)",
-           "model": "16 B per update (4 summed-area-table corners)"}
+           "model": "16 B per update (the reference's 4 summed-area-table corners)"}
     for name, f, upd in (("fp", fp, nview * nu * nv * nz), ("bp", bp, nx * ny * nz * nview)):
         f()
         torch.cuda.synchronize()

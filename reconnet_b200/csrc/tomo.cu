@@ -8,10 +8,10 @@
 //       and the sum is scaled by dz / |dz_src-det| * |src - det|;
 //   BP: the sinogram is pre-weighted by the same length factor, and every
 //       voxel integrates the detector rectangle spanned by its projected faces.
-// Here the FP integrals come from FP64 row-prefix tables (rows_integral), the
-// same quantity in exact arithmetic as the reference's corner form, and the BP
-// reads an FP64 summed-area table as the reference does; each (b, c) volume
-// is processed by one launch sequence on the caller's stream.
+// Here both integrals come from FP64 row-prefix tables (rows_integral): the
+// rows a rectangle overlaps, each weighted by its overlap, the same quantity
+// in exact arithmetic as the reference's summed-area-table corner form.  Each
+// (b, c) volume is processed by one launch sequence on the caller's stream.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -36,13 +36,13 @@ struct TomoDims {
 // Tables (FP64).  FP: per z plane, row prefixes along x of image row y,
 // layout [z][y + 1][x] (x fastest, x in [0, nx]); a rectangle integral is the
 // sum over the rows it overlaps (rows_integral), which equals the reference's
-// summed-area-table corner form.  BP: per view, the (u, v) summed-area table
-// of the length-weighted projections, layout [view][v][u] (u fastest, u in
-// [0, nu], v in [0, nv]).  Rows run along the axis that the lanes of the main
-// kernels walk, so their reads are coalesced.  Row prefixes are built by a
-// tiled pass that reads the source along its contiguous axis, transposes 32 x
-// 32 tiles through shared memory and scans along the row with warp scans
-// (carry across tiles); the BP table then gets a pass along v.
+// summed-area-table corner form.  BP: per view, row prefixes along u of the
+// length-weighted projections, layout [view][v + 1][u] (u fastest, u in
+// [0, nu]), integrated the same way over detector rows.  Rows run along the
+// axis that the lanes of the main kernels walk, so their reads are coalesced.
+// Row prefixes are built by a tiled pass that reads the source along its
+// contiguous axis, transposes 32 x 32 tiles through shared memory and scans
+// along the row with warp scans (carry across tiles).
 // ---------------------------------------------------------------------------
 
 // Row prefixes R[z][y + 1][x + 1] = sum_{x' <= x} img[x'][y][z].  Block
@@ -139,20 +139,6 @@ __global__ void __launch_bounds__(256) tomo_bp_sat_u(double* __restrict__ sat, c
         for (int u = lane + 32 * w; u <= d.nu; u += 256) S[u] = 0.0;
 }
 
-// Column prefixes along v: one thread per (view, u), u fastest.
-__global__ void tomo_bp_sat_v(double* __restrict__ sat, TomoDims d) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.nview * (d.nu + 1)) return;
-    const int view = i / (d.nu + 1), u = i - view * (d.nu + 1);
-    const long long row = d.nu + 1;
-    double* col = sat + (long long)view * (d.nu + 1) * (d.nv + 1) + u;
-    double acc = 0.0;
-    for (int v = 1; v <= d.nv; v++) {
-        acc += col[v * row];
-        col[v * row] = acc;
-    }
-}
-
 // Clamp_float + the index / weight of one coordinate of InterpolateXY /
 // InterpolateUV (DistanceDriven3D.cu:75-135, :493-517) on a grid of n points.
 struct Lerp {
@@ -186,14 +172,6 @@ __device__ __forceinline__ double rows_integral(const double* __restrict__ R, co
         acc += (r[lc.i0] * (1 - lc.w) + r[lc.i1] * lc.w) * (double)ov;
     }
     return y2 >= y1 ? acc : -acc;
-}
-
-// Bilinear value of a table with rows along the second coordinate:
-// a[r * row + col], col from lc, r from lr.
-__device__ __forceinline__ double sat_at(const double* __restrict__ a, const Lerp& lc, const Lerp& lr, long long row) {
-    const double* r0 = a + lr.i0 * row;
-    const double* r1 = a + lr.i1 * row;
-    return (r0[lc.i0] * (1 - lc.w) + r0[lc.i1] * lc.w) * (1 - lr.w) + (r1[lc.i0] * (1 - lc.w) + r1[lc.i1] * lc.w) * lr.w;
 }
 
 // FP: lane i of a warp owns detector column iu = 31 blockIdx.x + i and its
@@ -247,10 +225,11 @@ __global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, c
 // face; lane 31 only supplies the right face of lane 30's voxel.  A warp
 // handles one (y, z) row.  Per view each lane evaluates D = S(u_e, v2) -
 // S(u_e, v1) at its face's detector coordinate (ProjectConeToDetCart,
-// DistanceDriven3D.cu:478-489) by bilinear reads of the (u, v) summed-area
-// table, and the voxel's rectangle integral is D(next lane) - D(this lane):
-// 8 table reads instead of the reference's 16.  The rectangle's area is
-// r^2 dx dy / (du dv).
+// DistanceDriven3D.cu:478-489), S being the (u, v) summed-area table of the
+// reference, from the detector rows that [v1, v2] overlaps (the same for
+// every lane of the warp): two row-prefix reads per row, two or three rows,
+// instead of the reference's 16 corner reads.  The voxel's rectangle integral
+// is D(next lane) - D(this lane); its area is r^2 dx dy / (du dv).
 __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, const double* __restrict__ sat,
                                                       const float* __restrict__ detCenter,
                                                       const float* __restrict__ src, TomoDims d, int b, int c) {
@@ -277,9 +256,7 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
         const float v1 = fmaf(sp[1] - dc[1] + r * (y - d.dy / 2 - sp[1]), idv, cv);
         const float v2 = fmaf(sp[1] - dc[1] + r * (y + d.dy / 2 - sp[1]), idv, cv);
         const Lerp lu = lerp_at(ue, d.nu + 1);
-        const Lerp l1 = lerp_at(v1, d.nv + 1), l2 = lerp_at(v2, d.nv + 1);
-        const double* a = sat + view * vplane;
-        const double D = sat_at(a, lu, l2, row) - sat_at(a, lu, l1, row);
+        const double D = rows_integral(sat + view * vplane, lu, v1, v2, d.nv, row);
         const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
         val = fmaf((float)q, __fdividef(1.0f, r * r * aunit), val);
     }
@@ -316,7 +293,6 @@ int tomo_backproject(float* d_img, const float* d_prj, const float* d_dc, const 
         for (int c = 0; c < d.nc; c++) {
             tomo_bp_sat_u<<<dim3((d.nv + 31) / 32, d.nview), dim3(32, 8), 0, st>>>(d_sat, d_prj, d_dc, d_src, d, b,
                                                                                     c, weight_all);
-            tomo_bp_sat_v<<<(d.nview * (d.nu + 1) + 255) / 256, 256, 0, st>>>(d_sat, d);
             dim3 blk(32, 8);
             dim3 grd(d.nz, (d.nx + 30) / 31, (d.ny + 7) / 8);
             tomo_bp_kernel<<<grd, blk, 0, st>>>(d_img, d_sat, d_dc, d_src, d, b, c);
