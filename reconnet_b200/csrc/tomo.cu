@@ -145,12 +145,16 @@ struct Lerp {
     int i0, i1;
     double w;
 };
+// The index and the fraction come from a round-down add against 1.5 * 2^23
+// (exact for 0 <= x < 2^22) instead of conversions on the XU pipe; a NaN
+// coordinate clamps to 0.
 __device__ __forceinline__ Lerp lerp_at(float x, int n) {
-    x = x < 0.f ? 0.f : (x >= (float)n ? (float)(n - 1) : x);
+    x = fminf(fmaxf(x, 0.f), (float)(n - 1));
+    const float y = __fadd_rd(x, 12582912.0f);
     Lerp l;
-    l.i0 = (int)x;
+    l.i0 = __float_as_int(y) - 0x4B400000;
     l.i1 = min(l.i0 + 1, n - 1);
-    l.w = (double)(x - (float)l.i0);
+    l.w = (double)(x - (y - 12582912.0f));
     return l;
 }
 // Integral over [y1, y2] (clamped to [0, n]; the result changes sign when
@@ -165,10 +169,14 @@ __device__ __forceinline__ double rows_integral(const double* __restrict__ R, co
     lo = fminf(fmaxf(lo, 0.f), (float)n);
     hi = fminf(fmaxf(hi, 0.f), (float)n);
     double acc = 0.0;
+    // rows j < n overlapped by [lo, hi]; j and its float value fj from a
+    // round-down add, as in lerp_at
+    const float y = __fadd_rd(lo, 12582912.0f);
+    float fj = y - 12582912.0f;
+    const double* r = R + (long long)(__float_as_int(y) - 0x4B400000 + 1) * row;
 #pragma unroll 4
-    for (int j = (int)lo; (float)j < hi; j++) {   // rows j < n overlapped by [lo, hi]
-        const float ov = fminf(hi, (float)(j + 1)) - fmaxf(lo, (float)j);
-        const double* r = R + (long long)(j + 1) * row;
+    for (; fj < hi; fj += 1.f, r += row) {
+        const float ov = fminf(hi, fj + 1.f) - fmaxf(lo, fj);
         acc += (r[lc.i0] * (1 - lc.w) + r[lc.i1] * lc.w) * (double)ov;
     }
     return y2 >= y1 ? acc : -acc;
