@@ -256,6 +256,8 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
     const float idu = 1.0f / d.du, idv = 1.0f / d.dv;
     const long long vplane = (long long)(d.nu + 1) * (d.nv + 1), row = d.nu + 1;
     float val = 0.f;
+    // two views per iteration: their table reads are in flight together
+#pragma unroll 2
     for (int view = 0; view < d.nview; view++) {
         const float* dc = detCenter + 3 * view;
         const float* sp = src + 3 * view;
