@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-ossqs", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis, cone and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
-    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter"],
+    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs"],
                     help="run only this extra measurement (one GPU) and print its JSON object")
     return ap.parse_args()
 
@@ -829,14 +829,17 @@ def run_extra(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     cpu = not args.no_cpu_baseline
-    if args.extra == "siddon":
+    if args.extra in ("siddon", "ossqs"):
         from reconnet_b200.torch_ops import FanPlan
         geom, counts, angles, imgs = workload(0, args.slices)
         plan = FanPlan(geom, angles, nbatches=args.slices, nview_per_slice=counts, device=dev)
         x = torch.from_numpy(imgs).to(dev)
-        p = torch.empty(plan.sino_shape, device=dev)
-        b = torch.empty(plan.img_shape, device=dev)
-        out = siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=cpu)
+        if args.extra == "ossqs":
+            out = ossqs_run(plan, geom, counts, angles, x, args.ossqs_iters, dev)
+        else:
+            p = torch.empty(plan.sino_shape, device=dev)
+            b = torch.empty(plan.img_shape, device=dev)
+            out = siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=cpu)
     elif args.extra == "tomo":
         out = tomo_run(dev, cpu_sample=cpu)
     elif args.extra == "cone":

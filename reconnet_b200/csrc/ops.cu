@@ -214,9 +214,11 @@ __device__ __forceinline__ TvTerms tv_terms(const float* __restrict__ img, int i
     const float eps = 1e-6f;
     float t0 = sqrtf(dx0 * dx0 + eps), t1 = sqrtf(dx1 * dx1 + eps);
     float t2 = sqrtf(dy0 * dy0 + eps), t3 = sqrtf(dy1 * dy1 + eps);
+    // one correctly rounded reciprocal per difference instead of two divides
+    const float r0 = __frcp_rn(t0), r1 = __frcp_rn(t1), r2 = __frcp_rn(t2), r3 = __frcp_rn(t3);
     TvTerms r;
-    r.grad = (dx0 / t0 + dx1 / t1 + dy0 / t2 + dy1 / t3) / 2;
-    r.norm = 1 / t0 + 1 / t1 + 1 / t2 + 1 / t3;
+    r.grad = (dx0 * r0 + dx1 * r1 + dy0 * r2 + dy1 * r3) / 2;
+    r.norm = r0 + r1 + r2 + r3;
     r.var = (t0 + t1 + t2 + t3) / 2;
     return r;
 }
@@ -257,26 +259,24 @@ __global__ void residual_kernel(float* __restrict__ r, const float* __restrict__
 
 // x_out = clamp(x_in - lam * (M*bp + beta*grad)/(norm + beta*norm_tv + 1e-6))
 // (Divide2D / Minus2D / ValueCrop2D of ossqs.cu:135-146 plus the TV terms);
-// image [B][nx][ny][nz][C], TV within each (b, z, c) plane.
+// image [B][nx][ny][nz][C], TV within each (b, z, c) plane.  Grid: x over the
+// ny * nz * nc run of one image row, y = ix, z = b, so no thread divides a
+// 64-bit index.
 __global__ void sqs_update_kernel(float* __restrict__ xo, const float* __restrict__ xi, const float* __restrict__ bp,
-                                  const float* __restrict__ nimg, int nb, int nx, int ny, int nz, int nc, float lam,
-                                  float beta, float M, float lb, float ub, int clamp) {
-    long long n = (long long)nb * nx * ny * nz * nc;
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+                                  const float* __restrict__ nimg, int nx, int ny, int nzc, float lam, float beta,
+                                  float M, float lb, float ub, int clamp) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ny * nzc) return;
+    const int ix = blockIdx.y, bb = blockIdx.z;
+    const long long isx = (long long)ny * nzc;
+    const long long i = ((long long)bb * nx + ix) * isx + j;
     float num = M * bp[i];
     float den = nimg[i] + 1e-6f;
     if (beta != 0.f) {
-        long long isy = (long long)nz * nc, isx = (long long)ny * isy;
-        long long per_b = (long long)nx * ny * nz * nc;
-        long long bb = i / per_b;
-        long long q = i - bb * per_b;
-        int ix = (int)(q / isx);
-        q -= (long long)ix * isx;
-        int iy = (int)(q / isy);
-        long long zc = q - (long long)iy * isy;
-        const float* plane = xi + bb * per_b + zc;
-        TvTerms t = tv_terms(plane, ix, iy, nx, ny, isx, isy);
+        const int iy = nzc == 1 ? j : j / nzc;
+        const int zc = j - iy * nzc;
+        const float* plane = xi + (long long)bb * nx * isx + zc;
+        TvTerms t = tv_terms(plane, ix, iy, nx, ny, isx, nzc);
         num += beta * t.grad;
         den += beta * t.norm;
     }
@@ -289,6 +289,12 @@ int sqs_update(rn_fan_plan* p, float* x_out, const float* x_in, const float* prj
                const float* norm_img, float lam, float beta, int M, float lb, float ub, int type, cudaStream_t st) {
     if (!p || !x_out || !x_in || !prj_s || !w_s || !norm_img) return set_error(RN_ERR_ARG, "null argument");
     if (x_out == x_in) return set_error(RN_ERR_ARG, "sqs update: x_out must not alias x_in");
+    {
+        const RnFanGeom& g = p->g;
+        const long long nzc = p->ragged ? 1 : (long long)g.nz * g.nChannels;
+        if (g.nBatches > 65535 || (long long)g.ny * nzc >= (1LL << 31))
+            return set_error(RN_ERR_ARG, "sqs update: more than 65535 batches, or an image row above 2^31 elements");
+    }
     if (!p->d_tmp_prj) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_prj, sizeof(float) * p->prj_elems));
     if (!p->d_tmp_img) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_img, sizeof(float) * p->img_elems));
     RN_TRY(fan_project(p, p->d_tmp_prj, x_in, st, type == RN_TYPE_SIDDON));
@@ -298,10 +304,10 @@ int sqs_update(rn_fan_plan* p, float* x_out, const float* x_in, const float* prj
     RN_CUDA_TRY(cudaGetLastError());
     RN_TRY(fan_backproject(p, p->d_tmp_img, p->d_tmp_prj, type, 0, st));
     const RnFanGeom& g = p->g;
-    long long ni = p->img_elems;
-    sqs_update_kernel<<<(unsigned)((ni + 255) / 256), 256, 0, st>>>(
-        x_out, x_in, p->d_tmp_img, norm_img, g.nBatches, g.nx, g.ny, p->ragged ? 1 : g.nz, p->ragged ? 1 : g.nChannels, lam,
-        beta, (float)M, lb, ub, lb < ub ? 1 : 0);
+    const int nzc = p->ragged ? 1 : g.nz * g.nChannels;
+    const dim3 grid((unsigned)(((long long)g.ny * nzc + 255) / 256), (unsigned)g.nx, (unsigned)g.nBatches);
+    sqs_update_kernel<<<grid, 256, 0, st>>>(x_out, x_in, p->d_tmp_img, norm_img, g.nx, g.ny, nzc, lam, beta, (float)M,
+                                            lb, ub, lb < ub ? 1 : 0);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
