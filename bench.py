@@ -406,6 +406,7 @@ def ossqs_run(plan, geom, counts, angles, truth, n_iter, dev, n_subsets=24, I0=5
         solver_nf.check()
     return {"iterations": n_iter, "subsets": n_subsets, "I0": I0, "beta": solver.beta,
             "ms_per_iteration": ms / n_iter, "ms_total": ms, "setup_s": setup_s,
+            "tuning": dict(zip(("fp_views", "fp_lines", "bp_parts"), solver.tuning)),
             "rmse_hu_initial": rmse(x0), "rmse_hu_final": rmse(x),
             "starved_ray_fraction": starved, "rmse_hu_final_noise_free_unweighted": rmse(x_nf),
             "note": "graph replay of one full iteration (24 subset updates: FP, residual, matched BP, "

@@ -206,6 +206,32 @@ int rn_fan_plan_check(rn_fan_plan* plan, void* stream);
 int rn_fan_plan_set_timing(rn_fan_plan* plan, int enable);
 int rn_fan_plan_read_timing(rn_fan_plan* plan, float* ms, int* counts, int nkinds, long long* launches);
 
+/* Launch-parameter tuning (no counterpart in the reference, whose kernels
+ * have fixed launch shapes).  Three parameters shape a plan's launches:
+ *   fp_views  views per forward-projection CTA (1 .. 4 for up to ~990
+ *             channels; fewer views give more, smaller CTAs),
+ *   fp_lines  image lines per chunk staged into shared memory (1 .. the most
+ *             that fit),
+ *   bp_parts  CTAs over which each backprojection tile's views are split
+ *             when the whole batch runs in one launch (1 .. 16, and at most
+ *             what the plan's scratch holds; used only for batches too small
+ *             to fill the GPU).
+ * 0 selects the built-in choice; rn_fan_plan_set_tuning clamps fp_views and
+ * fp_lines to their maxima.  Results do not depend on them beyond
+ * FP32 rounding of the chunked positions.
+ * rn_fan_plan_autotune times the candidates on the caller's buffers (prj is
+ * overwritten; for typeProjector's backprojection the plan allocates an
+ * image-sized scratch once) and keeps the fastest; choices are cached for the
+ * process by geometry, per-slice view counts and type, so a second plan of
+ * the same shape takes them without timing.  rn_fan_plan_set_tuning sets
+ * them directly (a solver can tune one subset plan and apply its choice to
+ * the others); rn_fan_plan_get_tuning returns the values in use (bp_parts 0 =
+ * built-in).  Both re-upload the plan's work list on `stream`: the plan must
+ * not be running on another stream meanwhile. */
+int rn_fan_plan_autotune(rn_fan_plan* plan, float* d_prj, const float* d_img, int typeProjector, void* stream);
+int rn_fan_plan_set_tuning(rn_fan_plan* plan, int fp_views, int fp_lines, int bp_parts, void* stream);
+int rn_fan_plan_get_tuning(const rn_fan_plan* plan, int* fp_views, int* fp_lines, int* bp_parts);
+
 /* Ramp filter on device pointers (fan = 1 equiangular / 0 parallel); same
  * parameters as cFilterFanFilter. */
 int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int nu, int nview, int nv, float da,

@@ -91,6 +91,9 @@ SIGNATURES = {
     "rn_fan_backproject": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "rn_fan_plan_check": (_i, [_vp, _vp]),
     "rn_fan_plan_set_timing": (_i, [_vp, _i]),
+    "rn_fan_plan_autotune": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "rn_fan_plan_set_tuning": (_i, [_vp, _i, _i, _i, _vp]),
+    "rn_fan_plan_get_tuning": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "rn_fan_plan_read_timing": (_i, [_vp, _fp, ctypes.POINTER(_i), _i, ctypes.POINTER(ctypes.c_longlong)]),
     "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
     "rn_tv_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp]),

@@ -1385,10 +1385,15 @@ static int fp_lines_for_smem(int nu, int sp) {
     return R;
 }
 
+int fan_fp_lines_max(const rn_fan_plan* p) {
+    return std::min(fp_lines_for_smem(p->dims.nu, p->dims.spx), fp_lines_for_smem(p->dims.nu, p->dims.spy));
+}
+
 int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st, bool siddon) {
     const FanDims& d = p->dims;
     const int nfp = (int)p->h_fp.size();
-    const int R = std::min(fp_lines_for_smem(d.nu, d.spx), fp_lines_for_smem(d.nu, d.spy));
+    const int Rmax = fan_fp_lines_max(p);
+    const int R = p->fp_R > 0 ? std::min(p->fp_R, Rmax) : Rmax;
     if (fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R) > (size_t)kSmemBudget)
         return set_error(RN_ERR_ARG, "fan projection: image lines too long for shared memory");
     const size_t smem = fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R);
@@ -1467,6 +1472,10 @@ static int bp_max_views(const rn_fan_plan* p, const std::vector<BpSlice>& bps, i
 // resident slot) splits every tile's views over several CTAs.
 static int bp_parts(const rn_fan_plan* p, const std::vector<BpSlice>& bps, int s0, int s1) {
     if (s0 != 0 || s1 != (int)bps.size()) return 1;
+    if (p->bp_nparts > 0) {   // tuned
+        const int nch = (bp_max_views(p, bps, s0, s1) + kBpViews - 1) / kBpViews;
+        return std::max(1, std::min(std::min(p->bp_nparts, kBpMaxParts), nch));
+    }
     const FanDims& d = p->dims;
     const long long tiles = (long long)((d.nx + kBmCols - 1) / kBmCols) * ((d.ny + kBmTileY - 1) / kBmTileY);
     const long long ctas = (long long)(s1 - s0) * tiles;

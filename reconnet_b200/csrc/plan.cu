@@ -7,6 +7,7 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "rn_internal.h"
@@ -77,9 +78,11 @@ static void set_dims(rn_fan_plan* p, long long isx, long long isy) {
 
 static void build_fp_work(rn_fan_plan* p) {
     // views per work item: at most the kernel's table capacity, fewer when a
-    // small batch would leave SMs idle (one CTA per SM; aim for two waves).
-    // A ray's sum does not depend on which views share its CTA.
-    int VT = fan_fp_views(p->g.nu);
+    // small batch would leave SMs idle (one CTA per SM; aim for two waves),
+    // or the tuned count.  A ray's sum does not depend on which views share
+    // its CTA.
+    const int vmax = fan_fp_views(p->g.nu);
+    int VT = vmax;
     auto items = [&](int vt) {
         long long n = 0;
         for (size_t s = 0; s < p->h_fp.size(); s++) {
@@ -88,7 +91,10 @@ static void build_fp_work(rn_fan_plan* p) {
         }
         return n;
     };
-    while (VT > 1 && items(VT) < 2LL * 148) VT--;
+    if (p->fp_vt > 0) VT = std::min(p->fp_vt, vmax);
+    else
+        while (VT > 1 && items(VT) < 2LL * 148) VT--;
+    p->fp_vt_used = VT;
     p->h_fp_work.clear();
     for (size_t s = 0; s < p->h_fp.size(); s++) {
         const GeoSet& gs = p->h_sets[p->h_fp[s].set];
@@ -190,6 +196,11 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     FanGeoHost gh;
     RN_TRY(fan_build_geometry(p, host_deg, gh));
     build_fp_work(p);
+    {
+        long long cap = 0;   // one view per item: room for any tuning
+        for (size_t s = 0; s < p->h_fp.size(); s++) cap += p->h_sets[p->h_fp[s].set].nview;
+        p->fp_work_cap = (int)std::max<long long>(cap, p->n_fp_work);
+    }
 
     // line scratch
     const FanDims& d = p->dims;
@@ -230,7 +241,8 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     upload(&p->d_bpr, p->h_bpr);
     upload(&p->d_fps, p->h_fps);
     upload(&p->d_bps, p->h_bps);
-    upload(&p->d_fp_work, p->h_fp_work);
+    up.push_back(ArenaPart{reinterpret_cast<void**>(&p->d_fp_work), sizeof(int4) * (size_t)std::max(1, p->fp_work_cap),
+                           p->h_fp_work.data(), sizeof(int) * p->h_fp_work.size()});
     upload(&d_vcs, gh.vcs);
     upload(&d_vx, gh.vx);
     upload(&d_esc, gh.esc);
@@ -264,6 +276,48 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     RN_CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
     RN_TRY(fan_slope_tables(p, d_vcs, d_vx, d_esc, d_csc, st));
     RN_CUDA_TRY(cudaStreamSynchronize(st));   // blob and gh go out of scope
+    return RN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch-parameter tuning: views per forward-projection work item, lines per
+// staged chunk, and the view split of a single-launch backprojection.  Tuned
+// choices are cached by a hash of the geometry, the per-slice view counts and
+// classes, and the projector type.
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::unordered_map<uint64_t, std::vector<int>> g_tuned;
+
+static uint64_t tune_key(const rn_fan_plan* p, int type) {
+    uint64_t h = 1469598103934665603ull;   // FNV-1a
+    auto mix = [&](const void* d, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(d);
+        for (size_t i = 0; i < n; i++) {
+            h ^= c[i];
+            h *= 1099511628211ull;
+        }
+    };
+    const int ragged = p->ragged ? 1 : 0;
+    mix(&p->g, sizeof(p->g));
+    mix(&ragged, sizeof(ragged));
+    mix(&type, sizeof(type));
+    for (const GeoSet& gs : p->h_sets) {
+        mix(&gs.nview, sizeof(gs.nview));
+        mix(&gs.nxv, sizeof(gs.nxv));
+    }
+    return h;
+}
+
+// Sets the overrides and uploads the rebuilt work list (stream-ordered).
+static int apply_tuning(rn_fan_plan* p, int fp_vt, int fp_R, int bp_nparts, cudaStream_t st) {
+    p->fp_vt = fp_vt;
+    p->fp_R = fp_R;
+    p->bp_nparts = bp_nparts;
+    build_fp_work(p);
+    if (p->n_fp_work > p->fp_work_cap) return set_error(RN_ERR_ARG, "tuning: work list exceeds its capacity");
+    if (p->n_fp_work > 0)
+        RN_CUDA_TRY(cudaMemcpyAsync(p->d_fp_work, p->h_fp_work.data(), sizeof(int4) * p->n_fp_work,
+                                    cudaMemcpyHostToDevice, st));
     return RN_OK;
 }
 
@@ -560,6 +614,109 @@ int rn_fan_plan_read_timing(rn_fan_plan* p, float* ms, int* counts, int nkinds, 
     }
     p->timed.clear();
     return RN_OK;
+}
+
+int rn_fan_plan_set_tuning(rn_fan_plan* p, int fp_views, int fp_lines, int bp_parts, void* stream) {
+    clear_error();
+    if (!p) return set_error(RN_ERR_ARG, "null plan");
+    if (fp_views < 0 || fp_lines < 0 || bp_parts < 0 || bp_parts > kBpMaxParts)
+        return set_error(RN_ERR_ARG, "tuning: negative value, or bp_parts above 16");
+    // above their maxima the first two clamp (plans of one solver can differ
+    // a little in how many lines fit)
+    return apply_tuning(p, std::min(fp_views, fan_fp_views(p->g.nu)), std::min(fp_lines, fan_fp_lines_max(p)),
+                        bp_parts, (cudaStream_t)stream);
+}
+
+int rn_fan_plan_get_tuning(const rn_fan_plan* p, int* fp_views, int* fp_lines, int* bp_parts) {
+    clear_error();
+    if (!p) return set_error(RN_ERR_ARG, "null plan");
+    const int Rmax = fan_fp_lines_max(p);
+    if (fp_views) *fp_views = p->fp_vt_used;
+    if (fp_lines) *fp_lines = p->fp_R > 0 ? std::min(p->fp_R, Rmax) : Rmax;
+    if (bp_parts) *bp_parts = p->bp_nparts;
+    return RN_OK;
+}
+
+int rn_fan_plan_autotune(rn_fan_plan* p, float* d_prj, const float* d_img, int typeProjector, void* stream) {
+    clear_error();
+    if (!p || !d_prj || !d_img) return set_error(RN_ERR_ARG, "null argument");
+    if (typeProjector < RN_TYPE_ITERATIVE || typeProjector > RN_TYPE_PIXEL)
+        return set_error(RN_ERR_ARG, "autotune: unknown typeProjector");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t key = tune_key(p, typeProjector);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return apply_tuning(p, it->second[0], it->second[1], it->second[2], st);
+    }
+    const bool siddon = typeProjector == RN_TYPE_SIDDON;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RN_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_error(RN_ERR_CUDA, "autotune: cudaEventCreate");
+    }
+    // mean of two runs after one untimed run
+    auto timed = [&](auto&& run, float& ms) -> int {
+        RN_TRY(run());
+        RN_CUDA_TRY(cudaEventRecord(e0, st));
+        RN_TRY(run());
+        RN_TRY(run());
+        RN_CUDA_TRY(cudaEventRecord(e1, st));
+        RN_CUDA_TRY(cudaEventSynchronize(e1));
+        RN_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        ms *= 0.5f;
+        return RN_OK;
+    };
+    int s = RN_OK;
+    int best_vt = 0, best_R = 0, best_parts = 0;
+    float best = 1e30f;
+    const int vmax = fan_fp_views(p->g.nu), Rmax = fan_fp_lines_max(p);
+    for (int vt = vmax; vt >= 1 && s == RN_OK; vt--) {
+        for (int R : {Rmax, Rmax / 2}) {
+            if (R < 1) continue;
+            float ms = 0.f;
+            s = apply_tuning(p, vt, R, 0, st);
+            if (s == RN_OK) s = timed([&] { return fan_project(p, d_prj, d_img, st, siddon); }, ms);
+            if (s != RN_OK) break;
+            if (ms < best) {
+                best = ms;
+                best_vt = vt;
+                best_R = R;
+            }
+        }
+    }
+    // the view split of the backprojection, where the plan can split it
+    if (s == RN_OK && p->bp_parts_cap > 0) {
+        if (!p->d_tmp_img) {
+            cudaError_t e = cudaMalloc(&p->d_tmp_img, sizeof(float) * p->img_elems);
+            if (e != cudaSuccess) s = set_cuda_error(e, "autotune: cudaMalloc");
+        }
+        best = 1e30f;
+        for (int parts = 1; parts <= kBpMaxParts && s == RN_OK; parts *= 2) {
+            if ((long long)parts * p->img_elems > p->bp_parts_cap && parts > 1) break;
+            float ms = 0.f;
+            s = apply_tuning(p, best_vt, best_R, parts, st);
+            if (s == RN_OK)
+                s = timed([&] { return fan_backproject(p, p->d_tmp_img, d_prj, typeProjector, 0, st); }, ms);
+            if (s == RN_OK && ms < best) {
+                best = ms;
+                best_parts = parts;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != RN_OK) {
+        const std::string msg = rn_last_error();
+        apply_tuning(p, 0, 0, 0, st);
+        return set_error(s, msg);
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[key] = {best_vt, best_R, best_parts};
+    }
+    return apply_tuning(p, best_vt, best_R, best_parts, st);
 }
 
 int rn_fan_plan_check(rn_fan_plan* p, void* stream) {

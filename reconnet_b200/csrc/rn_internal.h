@@ -158,6 +158,13 @@ struct rn_fan_plan {
     float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, lazily allocated)
     float* d_bp_parts = nullptr;    // partial images of a view-split backprojection
     long long bp_parts_cap = 0;     // elements
+    // launch parameters (0 = the built-in choice); set by rn_fan_plan_set_tuning
+    // or rn_fan_plan_autotune
+    int fp_vt = 0;                  // views per forward-projection work item
+    int fp_R = 0;                   // lines per staged chunk of the forward projection
+    int bp_nparts = 0;              // view parts of a split backprojection (single-launch batches)
+    int fp_vt_used = 0;             // views per work item of the current work list
+    int fp_work_cap = 0;            // work items the device list holds (one view each)
     float* d_tmp_prj = nullptr;     // sinogram-sized scratch (SQS update, lazily allocated)
     // every device table and scratch above except the two lazily allocated
     // ones lives in this one allocation
@@ -224,6 +231,8 @@ int fan_slope_tables(rn_fan_plan* p, const double2* d_vcs, const int* d_vx, cons
 // Parts over which fan_backproject splits a backprojection of `type` (1 when
 // it does not split), and the number of slices in its first launch.
 int fan_bp_split(const rn_fan_plan* p, int type, int* first_wave_slices);
+// Most lines per staged forward-projection chunk that shared memory holds.
+int fan_fp_lines_max(const rn_fan_plan* p);
 int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st, bool siddon = false);
 int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, int accumulate, cudaStream_t st);
 }  // namespace rn

@@ -37,11 +37,14 @@ class BatchedOSSQS:
     def __init__(self, geom: FanGeometry, counts: Sequence[int], angles, sino: torch.Tensor,
                  weights: torch.Tensor, n_subsets: int, beta: float = 0.0, lam: float = 1.0,
                  lb: Optional[float] = 0.0, ub: Optional[float] = None, use_graph: bool = True,
-                 device=None, projector: str = "dd"):
+                 device=None, projector: str = "dd", autotune: bool = True):
         """counts[s] views per slice, angles concatenated per slice, sino /
         weights packed per slice as [nu, counts[s]] blocks (flat CUDA tensors).
         projector "dd": DD forward + matched backprojection; "siddon": the
-        Siddon pair, the projector of the reference's cOSSQS (ossqs.cu:81)."""
+        Siddon pair, the projector of the reference's cOSSQS (ossqs.cu:81).
+        autotune: time the launch parameters of the first subset's plan and
+        use its choice for every subset (subsets hold ~1/n_subsets of the
+        views, so their launches are much smaller than a full pass)."""
         if projector not in ("dd", "siddon"):
             raise ValueError("projector must be 'dd' or 'siddon'")
         self.type = N.RN_TYPE_SIDDON if projector == "siddon" else N.RN_TYPE_MATCHED
@@ -74,6 +77,14 @@ class BatchedOSSQS:
             self.plans.append(plan)
             self.sub_b.append(sino.reshape(-1)[gidx].contiguous())
             self.sub_w.append(weights.reshape(-1)[gidx].contiguous())
+        if autotune:
+            scratch = torch.ones(self.plans[0].img_shape, device=self.device)
+            choice = self.plans[0].autotune(scratch, self.type)
+            for plan in self.plans[1:]:
+                plan.set_tuning(*choice)
+            self.tuning = choice
+        else:
+            self.tuning = self.plans[0].tuning()
         # normImg = A^T W A 1 over all views (the same pair)
         ones = torch.ones(self.full.img_shape, device=self.device)
         a1 = self.full.project(ones, siddon=self.type == N.RN_TYPE_SIDDON)

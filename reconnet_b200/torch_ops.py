@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass, field
-from typing import Optional, Sequence
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -176,6 +176,32 @@ class FanPlan:
     def check(self) -> None:
         """Synchronise and raise if a device-side bounded wait gave up."""
         N.check(N.lib.rn_fan_plan_check(self._plan, _stream_ptr(self.device)))
+
+    def autotune(self, img: torch.Tensor, type_projector: int = N.RN_TYPE_MATCHED,
+                 sino: Optional[torch.Tensor] = None) -> Tuple[int, int, int]:
+        """Time the launch-parameter candidates of this plan's forward
+        projection (Siddon for ``N.RN_TYPE_SIDDON``) and backprojection of
+        ``type_projector`` on ``img`` and keep the fastest (cached per
+        geometry for the process).  ``sino`` (overwritten) is scratch.
+        Returns (fp_views, fp_lines, bp_parts)."""
+        if tuple(img.shape) != self.img_shape:
+            raise ValueError(f"image shape {tuple(img.shape)} != {self.img_shape}")
+        if sino is None:
+            sino = torch.empty(self.sino_shape, dtype=torch.float32, device=img.device)
+        N.check(N.lib.rn_fan_plan_autotune(self._plan, _dev_ptr(sino), _dev_ptr(img), int(type_projector),
+                                           _stream_ptr(img.device)))
+        return self.tuning()
+
+    def tuning(self) -> Tuple[int, int, int]:
+        """(fp_views, fp_lines, bp_parts) in use; bp_parts 0 = built-in."""
+        v, r, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.check(N.lib.rn_fan_plan_get_tuning(self._plan, ctypes.byref(v), ctypes.byref(r), ctypes.byref(b)))
+        return v.value, r.value, b.value
+
+    def set_tuning(self, fp_views: int = 0, fp_lines: int = 0, bp_parts: int = 0) -> None:
+        """Set the launch parameters (0 = built-in choice) on the current stream."""
+        N.check(N.lib.rn_fan_plan_set_tuning(self._plan, int(fp_views), int(fp_lines), int(bp_parts),
+                                             _stream_ptr(self.device)))
 
     def sqs_update(self, x_out, x_in, prj_s, w_s, norm_img, lam=1.0, beta=0.0, n_subsets=1,
                    lb=None, ub=None, type_projector=N.RN_TYPE_MATCHED):
