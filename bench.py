@@ -63,8 +63,8 @@ def dist_env():
 
 def workload(rank, nslices):
     from reconnet_b200 import phantom as P
-    geom = P.geom_cfg1()
-    counts = P.cfg1_view_counts(nslices, seed=1 + rank)
+    geom = P.geom_fan512()
+    counts = P.batch_view_counts(nslices, seed=1 + rank)
     angles = np.concatenate([P.uniform_angles(int(n)) for n in counts])
     rng = np.random.default_rng(100 + rank)
     imgs = np.stack([P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng) for _ in range(nslices)])
@@ -415,7 +415,7 @@ def ossqs_run(plan, geom, counts, angles, truth, n_iter, dev, n_subsets=24, I0=5
 
 
 def tomo_run(dev, cpu_sample=True):
-    """Tomosynthesis DD pair (DistanceDriven3D) at configs[2]'s volume size:
+    """Tomosynthesis DD pair (DistanceDriven3D) on a 512x512x128 volume:
     512x512x128 voxels of 0.8x0.8x1.0 mm, a 736x736 flat detector of 0.6 mm
     cells 80 mm below the isocentre, 25 sources on a +-20 deg arc at 650 mm.
     Updates: FP = views * nu * nv * nz ray-plane integrals, BP = voxels * views;
@@ -450,9 +450,9 @@ def tomo_run(dev, cpu_sample=True):
     fp = lambda: N.check(N.lib.rn_tomo_project(P(prj), P(img), P(ddc), P(dsrc), P(sat), *geo, st()))
     bp = lambda: N.check(N.lib.rn_tomo_backproject(P(back), P(prj), P(ddc), P(dsrc), P(sat), *geo, 1, st()))
     peak, kind = measured_peaks()
-    out = {"workload": "tomosynthesis at configs[2] volume size: 512x512x128 @0.8x0.8x1.0 mm, 736x736 flat "
-                       "detector @0.6 mm, 25 views over +-20 deg (configs[2]'s 360-deg cylindrical CT geometry has "
-                       "no reference kernel; DistanceDriven3D is the reference's tomosynthesis pair)",
+    out = {"workload": "tomosynthesis: 512x512x128 @0.8x0.8x1.0 mm, 736x736 flat detector @0.6 mm, 25 views "
+                       "over +-20 deg (the reference's 3D DD pair is this flat-detector, z-main geometry; a 360-deg "
+                       "cylindrical-detector scan has no reference kernel)",
            "model": "16 B per update (the reference's 4 summed-area-table corners)"}
     for name, f, upd in (("fp", fp, nview * nu * nv * nz), ("bp", bp, nx * ny * nz * nview)):
         f()
@@ -624,9 +624,9 @@ def filter_run(dev, cpu_sample=True):
     (2 nu - 1)-tap kernel: nu^2 multiply-adds per view."""
     import torch
 
-    from reconnet_b200.phantom import geom_cfg1
+    from reconnet_b200.phantom import geom_fan512
     from reconnet_b200.torch_ops import filter_sino
-    geom = geom_cfg1()
+    geom = geom_fan512()
     B, nu, nview = 64, geom.nu, 1152
     rng = np.random.default_rng(12)
     sino = torch.from_numpy(rng.random((B, nu, nview, 1, 1), dtype=np.float32)).to(dev)

@@ -82,19 +82,19 @@ def uniform_angles(nview):
 
 
 # ---- workload geometries ----
-def geom_cfg0() -> FanGeometry:
+def geom_fan256() -> FanGeometry:
     """256x256 1.0 mm image, 736-channel arc detector at 1.2858 mm, 720 views."""
     return FanGeometry(nx=256, ny=256, nz=1, dx=1.0, dy=1.0, dz=1.0, nu=736, nv=1, da=1.2858 / 1085.6, dv=1.0,
                        dsd=1085.6, dso=595.0)
 
 
-def geom_cfg1() -> FanGeometry:
+def geom_fan512() -> FanGeometry:
     """512x512 0.7 mm slices, 888 channels (1.2858 mm pitch assumed)."""
     return FanGeometry(nx=512, ny=512, nz=1, dx=0.7, dy=0.7, dz=1.0, nu=888, nv=1, da=1.2858 / 1085.6, dv=1.0,
                        dsd=1085.6, dso=595.0)
 
 
-def cfg1_view_counts(nslices=64, seed=1):
+def batch_view_counts(nslices=64, seed=1):
     """Seeded uneven view counts in [576, 1152] per slice."""
     rng = np.random.default_rng(seed)
     return rng.integers(576, 1153, size=nslices).astype(np.int32)

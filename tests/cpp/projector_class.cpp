@@ -69,16 +69,16 @@ int main() {
         cudaStream_t st;
         cudaStreamCreate(&st);
         fan.SetCudaStream(st);
-        for (int round = 0; round < 2; round++) {   // round 1: other angles, tables rebuilt
-            const float* dd = round ? d_deg2 : d_deg;
+        for (int pass = 0; pass < 2; pass++) {   // pass 1: other angles, tables rebuilt
+            const float* dd = pass ? d_deg2 : d_deg;
             rn_fan_plan* plan = nullptr;
-            throw_if(rn_fan_plan_create(&plan, &g, round ? deg2.data() : deg.data(), st));
+            throw_if(rn_fan_plan_create(&plan, &g, pass ? deg2.data() : deg.data(), st));
             fan.Projection(d_img, d_out, dd);
             throw_if(rn_fan_project(plan, d_ref, d_img, st));
             cudaStreamSynchronize(st);
             double e = maxdiff(host(d_out, np), host(d_ref, np));
             if (e != 0) {
-                std::printf("fan type %d round %d: Projection differs by %g\n", type, round, e);
+                std::printf("fan type %d pass %d: Projection differs by %g\n", type, pass, e);
                 fails++;
             }
             cudaMemsetAsync(d_out, 0, sizeof(float) * ni, st);
@@ -88,7 +88,7 @@ int main() {
             cudaStreamSynchronize(st);
             e = maxdiff(host(d_out, ni), host(d_ref, ni), 2.f);
             if (e > 1e-5) {
-                std::printf("fan type %d round %d: two Backprojections differ from 2x by %g\n", type, round, e);
+                std::printf("fan type %d pass %d: two Backprojections differ from 2x by %g\n", type, pass, e);
                 fails++;
             }
             rn_fan_plan_destroy(plan);

@@ -70,7 +70,7 @@ FAN_CASES = {
                          off_v=0.0, dsd=1085.6, dso=595.0), 1, 1, 45),
     "fan_multislice": (dict(nx=48, ny=40, nz=3, dx=1.0, dy=1.1, dz=1.0, nu=64, nv=3, da=0.0025, dv=1.0, off_a=0.0,
                             off_v=0.0, dsd=1085.6, dso=595.0), 2, 2, 36),
-    "fan_cfg0": (dict(nx=256, ny=256, nz=1, dx=1.0, dy=1.0, dz=1.0, nu=736, nv=1, da=1.2858 / 1085.6, dv=1.0,
+    "fan256": (dict(nx=256, ny=256, nz=1, dx=1.0, dy=1.0, dz=1.0, nu=736, nv=1, da=1.2858 / 1085.6, dv=1.0,
                       off_a=0.0, off_v=0.0, dsd=1085.6, dso=595.0), 1, 1, 45),
 }
 

@@ -104,14 +104,14 @@ def test_ragged_plan_matches_per_slice_plans(rng):
         off += n
 
 
-@pytest.mark.parametrize("cfg", ["cfg0", "cfg1"])
+@pytest.mark.parametrize("cfg", ["fan256", "fan512"])
 def test_adjoint_full_size(cfg, rng):
     """<Ax, y> = <x, A^T y> at the workload sizes (phantom x, random y)."""
     import torch
     from reconnet_b200 import phantom as P
     from reconnet_b200.torch_ops import FanPlan
-    geom = P.geom_cfg0() if cfg == "cfg0" else P.geom_cfg1()
-    nview = 720 if cfg == "cfg0" else 864
+    geom = P.geom_fan256() if cfg == "fan256" else P.geom_fan512()
+    nview = 720 if cfg == "fan256" else 864
     plan = FanPlan(geom, P.uniform_angles(nview))
     x = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
     xd = torch.from_numpy(x).cuda()
@@ -124,12 +124,12 @@ def test_adjoint_full_size(cfg, rng):
     assert abs(lhs - rhs) / abs(lhs) <= TOL
 
 
-def test_cfg0_full_size_fp_bp_vs_oracle(rng):
+def test_fan256_full_size_fp_bp_vs_oracle(rng):
     import torch
     from oracle import oracle as O
     from reconnet_b200 import phantom as P
     from reconnet_b200.torch_ops import FanPlan
-    geom = P.geom_cfg0()
+    geom = P.geom_fan256()
     ang = P.uniform_angles(720)
     plan = FanPlan(geom, ang)
     x = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
@@ -142,13 +142,13 @@ def test_cfg0_full_size_fp_bp_vs_oracle(rng):
         assert rel_l2(bp, O.fan_bp(y, ang, geom, (geom.nx, geom.ny, 1), t)) <= TOL
 
 
-def test_cfg1_slice_fp_vs_oracle(rng):
+def test_fan512_slice_fp_vs_oracle(rng):
     """One full 512x512, 888-channel slice (the batched workload's slice)."""
     import torch
     from oracle import oracle as O
     from reconnet_b200 import phantom as P
     from reconnet_b200.torch_ops import FanPlan
-    geom = P.geom_cfg1()
+    geom = P.geom_fan512()
     ang = P.uniform_angles(600)[::4].copy()
     plan = FanPlan(geom, ang)
     x = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)[None, :, :, None, None]
@@ -181,7 +181,7 @@ def test_filter_host_api_full_size(rng):
     rn.nu, rn.da = 736, 1.2858 / 1085.6
     s = rng.random((1, 736, 720, 1)).astype(np.float32)
     got = rn.cFilter3d(s, 2)
-    ref = O.filter_sino(s[..., None, :], P.geom_cfg0(), 2)[..., 0, :]
+    ref = O.filter_sino(s[..., None, :], P.geom_fan256(), 2)[..., 0, :]
     assert rel_l2(got, ref) <= TOL
 
 

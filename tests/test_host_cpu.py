@@ -64,7 +64,7 @@ def test_phantom_is_seeded_and_in_range():
     b = P.ellipse_phantom(64, 64, 1.0, 1.0, np.random.default_rng(3))
     assert np.array_equal(a, b) and a.dtype == np.float32
     assert a.min() >= 0 and a.max() <= 0.4
-    c = P.cfg1_view_counts(64, seed=1)
+    c = P.batch_view_counts(64, seed=1)
     assert c.min() >= 576 and c.max() <= 1152 and len(c) == 64
     s, w = P.poisson_sinogram(np.full((4, 5), 2.0), 1e4, np.random.default_rng(0))
     assert s.shape == (4, 5) and np.all(w >= 1)

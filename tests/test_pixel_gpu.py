@@ -81,9 +81,9 @@ def test_pixel_full_size_slice(rng):
     import torch
     from oracle import oracle as O
     from reconnet_b200 import _native as N
-    from reconnet_b200.phantom import geom_cfg1
+    from reconnet_b200.phantom import geom_fan512
     from reconnet_b200.torch_ops import FanPlan
-    geom = geom_cfg1()
+    geom = geom_fan512()
     ang = (np.arange(720) * 2 * np.pi / 720).astype(np.float32)
     y = rng.random((1, geom.nu, 720, 1, 1)).astype(np.float32)
     plan = FanPlan(geom, ang)

@@ -31,7 +31,7 @@ def ref():
     return make_golden
 
 
-@pytest.mark.parametrize("name", ["fan2d", "fan_offsets", "fan_multislice", "fan_cfg0"])
+@pytest.mark.parametrize("name", ["fan2d", "fan_offsets", "fan_multislice", "fan256"])
 def test_fan_vs_reference_kernels(ref, name, rng):
     from reconnet_b200.reconnet import ReconNet
     lib = ref.load_ref()

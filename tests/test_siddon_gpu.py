@@ -83,13 +83,13 @@ def test_siddon_host_api_matches_device(rng):
 
 
 def test_siddon_full_size_slice(rng):
-    """A configs[1] slice (512 x 512 at 0.7 mm, 888 channels) with 96 views."""
+    """A slice of the 64-slice batch workload (512 x 512 at 0.7 mm, 888 channels) with 96 views."""
     import torch
     from oracle import oracle as O
     from reconnet_b200 import _native as N
     from reconnet_b200 import phantom as P
     from reconnet_b200.torch_ops import FanPlan
-    g = P.geom_cfg1()
+    g = P.geom_fan512()
     ang = P.uniform_angles(96)
     img = P.ellipse_phantom(g.nx, g.ny, g.dx, g.dy, rng)[None, :, :, None, None]
     plan = FanPlan(g, ang)

@@ -34,7 +34,7 @@ def test_noalloc_projection_matches_plan_projection_twice(rng):
     from reconnet_b200 import _native as N
     from reconnet_b200 import phantom as P
     from reconnet_b200.torch_ops import FanPlan
-    g = P.geom_cfg1()
+    g = P.geom_fan512()
     for nview in (864, 601):
         ang = P.uniform_angles(nview) + np.float32(0.003 * nview)
         img = torch.from_numpy(P.ellipse_phantom(g.nx, g.ny, g.dx, g.dy, rng)).cuda()
@@ -49,7 +49,7 @@ def test_noalloc_rejects_geometry_beyond_its_scratch():
     import torch
     from reconnet_b200 import _native as N
     from reconnet_b200 import phantom as P
-    g = P.geom_cfg1()
+    g = P.geom_fan512()
     img = torch.zeros((g.nx, g.ny), device="cuda")
     st, _ = _noalloc(N, torch, img, P.uniform_angles(4000), g)
     assert st == N.RN_ERR_ARG
