@@ -561,10 +561,36 @@ __device__ __forceinline__ bool bp_separable(float& acc, const ConeView& V, int 
 // computes candidate k's two intervals, clipped to the slab [0, 1] and to the
 // segment's ends along m, into shared memory.  Each lane then walks its own V
 // candidates and, for each, the warp's U candidates: pair (iu, iv) adds
-// seg x prj x |T_U(iu) n T_V(iv)| to each of its two voxels, with one load of
-// prj and one seg for both.  This is the sum of bp_separable with every
-// interval computed once instead of once per pair.
+// prjw x |T_U(iu) n T_V(iv)| to each of its two voxels, with one load for
+// both; prjw = seg x prj comes from cone_prj_seg_kernel.  This is the sum of
+// bp_separable with every interval and segment length computed once instead
+// of once per pair.
 constexpr int kSepWarps = 8;
+
+// prjw = prj x seg for a separable plan: seg = sqrt(dM^2 + (r_U dU)^2 +
+// (r_V dV)^2), the length per unit slab of ray (iu, iv), so that the
+// backprojector's pairs need no square root.  Grid: x over the (iv, c) run,
+// y = view, z = iu; batches in a loop.
+__global__ void cone_prj_seg_kernel(float* __restrict__ prjw, const float* __restrict__ prj,
+                                    const ConeView* __restrict__ views, ConeDims cd) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= cd.nv * cd.nc) return;
+    const int view = blockIdx.y, iu = blockIdx.z;
+    const int iv = j / cd.nc;
+    const ConeView& V = views[view];
+    const bool a_is_u = views[0].affine == 1;
+    const int m = views[0].m;
+    const int ax_u = a_is_u ? views[0].a : views[0].b, ax_v = a_is_u ? views[0].b : views[0].a;
+    const float dU = ax_u == 0 ? cd.d[0] : ax_u == 1 ? cd.d[1] : cd.d[2];
+    const float dV = ax_v == 0 ? cd.d[0] : ax_v == 1 ? cd.d[1] : cd.d[2];
+    const float dM = m == 0 ? cd.d[0] : m == 1 ? cd.d[1] : cd.d[2];
+    const double rU0 = a_is_u ? V.rho[0] : V.rho[3], rU1 = a_is_u ? V.rho[1] : V.rho[4];
+    const double rV0 = a_is_u ? V.rho[3] : V.rho[0], rV1 = a_is_u ? V.rho[5] : V.rho[2];
+    const float ru = (float)fma((double)iu, rU1, rU0), rv = (float)fma((double)iv, rV1, rV0);
+    const float seg = sqrtf(fmaf(ru * ru, dU * dU, fmaf(rv * rv, dV * dV, dM * dM)));
+    const long long e = ((long long)iu * cd.nview + view) * cd.nv * cd.nc + j;
+    for (int b = 0; b < cd.nb; b++) prjw[b * cd.prj_b + e] = prj[b * cd.prj_b + e] * seg;
+}
 
 __device__ __forceinline__ void sep_range(double X0, double G, float lo, float hi, int n, int& i0, int& i1) {
     const float x0 = (float)X0, ig = __fdividef(1.f, (float)G);
@@ -577,7 +603,7 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
                                                            const ConeView* __restrict__ views, ConeDims cd,
                                                            int accumulate) {
     __shared__ float4 s_t[kSepWarps][32];   // {T lo, T hi} for voxel pu, then for pu + 1
-    __shared__ float2 s_q[kSepWarps][32];   // {r_U^2 dU^2, iu}
+    __shared__ int s_i[kSepWarps][32];      // iu
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int m = views[0].m;
     const bool a_is_u = views[0].affine == 1;
@@ -593,10 +619,6 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
     const bool live = pv < nV, live1 = live && pu + 1 < nU;
     const int bc = blockIdx.z;
     const int c = bc % cd.nc, bt = bc / cd.nc;
-    const float dU = ax_u == 0 ? cd.d[0] : ax_u == 1 ? cd.d[1] : cd.d[2];
-    const float dV = ax_v == 0 ? cd.d[0] : ax_v == 1 ? cd.d[1] : cd.d[2];
-    const float dM = m == 0 ? cd.d[0] : m == 1 ? cd.d[1] : cd.d[2];
-    const float dU2 = dU * dU, dV2 = dV * dV, dM2 = dM * dM;
     const long long su = (long long)cd.nview * cd.nv * cd.nc;
     const int sv = cd.nc;
     const float* pb = prj + bt * cd.prj_b + c;
@@ -638,7 +660,7 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
                 const float t0 = -xu * iru, t1 = (1.f - xu) * iru, t2 = (2.f - xu) * iru;
                 s_t[warp][lane] = make_float4(fmaxf(clo, fminf(t0, t1)), fminf(chi, fmaxf(t0, t1)),
                                               fmaxf(clo, fminf(t1, t2)), fminf(chi, fmaxf(t1, t2)));
-                s_q[warp][lane] = make_float2(ru * ru * dU2, __int_as_float(i));
+                s_i[warp][lane] = i;
             }
             __syncwarp();
             float kj = 0.f;
@@ -647,15 +669,12 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
                 const float irv = fabsf(rv) > 1e-30f ? __fdividef(1.f, rv) : 1e30f;
                 const float tv0 = -xv * irv, tv1 = (1.f - xv) * irv;
                 const float lv = fminf(tv0, tv1), hv = fmaxf(tv0, tv1);
-                const float qv = fmaf(rv * rv, dV2, dM2);
                 const float* pcol = pview + j * sv;
                 for (int k = 0; k < nk; k++) {
                     const float4 E = s_t[warp][k];
                     const float l0 = fminf(hv, E.y) - fmaxf(lv, E.x), l1 = fminf(hv, E.w) - fmaxf(lv, E.z);
                     if (l0 > 0.f || l1 > 0.f) {
-                        const float2 Q = s_q[warp][k];
-                        const float q = Q.x + qv;
-                        const float p = (q * rsqrtf(q)) * __ldg(pcol + (long long)__float_as_int(Q.y) * su);
+                        const float p = __ldg(pcol + (long long)s_i[warp][k] * su);
                         if (l0 > 0.f) acc0 = fmaf(l0, p, acc0);
                         if (l1 > 0.f) acc1 = fmaf(l1, p, acc1);
                     }
@@ -775,6 +794,7 @@ struct rn_cone_plan {
     bool bp_sep = false;       // every view separable the same way (cone_bp_sep_kernel)
     ConeView h_view0;          // host copy of view 0 (axes of a separable plan)
     bool unit = true;          // every ray's lateral slopes are at most 1
+    float* d_prjw = nullptr;   // separable backprojection: projections times segment lengths (lazily allocated)
     long long launches = 0;
 };
 
@@ -976,6 +996,7 @@ int rn_cone_plan_destroy(rn_cone_plan* p) {
     if (!p) return RN_OK;
     cudaFree(p->d_views);
     cudaFree(p->d_rays);
+    cudaFree(p->d_prjw);
     delete p;
     return RN_OK;
 }
@@ -1015,8 +1036,15 @@ int rn_cone_backproject(rn_cone_plan* p, float* d_img, const float* d_prj, int a
         const int ax_u = v0.affine == 1 ? v0.a : v0.b;
         const int nv_axis = cd.n[p->bp_fast];
         const long long warps = (long long)((cd.n[ax_u] + 1) / 2) * cd.n[v0.m];
+        if (!p->d_prjw) RN_CUDA_TRY(cudaMalloc(&p->d_prjw, sizeof(float) * cd.nb * cd.prj_b));
+        if (cd.nu > 65535 || cd.nview > 65535)
+            return set_error(RN_ERR_ARG, "cone backprojection: more than 65535 detector columns or views");
+        cone_prj_seg_kernel<<<dim3((unsigned)((cd.nv * cd.nc + 255) / 256), (unsigned)cd.nview, (unsigned)cd.nu), 256,
+                              0, (cudaStream_t)stream>>>(p->d_prjw, d_prj, p->d_views, cd);
+        RN_CUDA_TRY(cudaGetLastError());
+        p->launches++;
         dim3 grid((unsigned)((warps + kSepWarps - 1) / kSepWarps), (unsigned)((nv_axis + 31) / 32), slices);
-        cone_bp_sep_kernel<<<grid, 32 * kSepWarps, 0, (cudaStream_t)stream>>>(d_img, d_prj, p->d_views, cd,
+        cone_bp_sep_kernel<<<grid, 32 * kSepWarps, 0, (cudaStream_t)stream>>>(d_img, p->d_prjw, p->d_views, cd,
                                                                              accumulate);
     } else {
         dim3 grid((unsigned)((nvox + 255) / 256), slices);
