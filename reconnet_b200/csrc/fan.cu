@@ -78,6 +78,8 @@ __global__ void edge_slope_kernel(double* edges, const double2* view_cs, const i
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
                                  FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems,
                                  int band) {
+    __shared__ __align__(16) float s_lines_a[8][128];
+    __shared__ __align__(16) double s_lines_p[8][128];
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     int per_slice = d.ny + d.nx;
@@ -93,38 +95,61 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
     long long base = (long long)si * slot_elems + (xl ? (long long)l * d.spx : (long long)d.ny * d.spx + (long long)l * d.spy);
     float2* ohl = hl + base;    // entry j (at line_pos(j)) holds position k = j - M
     float* ola = la + base;
-    double carry = 0.0;
-    for (int k0 = 0; k0 < n; k0 += 32) {
-        int k = k0 + lane;
-        double a = 0.0;
-        if (k < n) {
-            // blended value of rows (l-1, l) [X] or columns (l-1, l) [Y] at position k;
-            // band mode (Siddon): row / column l itself
-            float s = 0.f;
+    // blended value of rows (l-1, l) [X] or columns (l-1, l) [Y] at position k;
+    // band mode (Siddon): row / column l itself
+    auto value = [&](int k) -> float {
+        float s = 0.f;
 #pragma unroll
-            for (int j = 0; j < 2; j++) {
-                float w = fs.img_w[j];
-                if (w == 0.f) continue;
-                const float* p = img + fs.img_off[j];
-                float v1, v0 = 0.f;
-                if (xl) {
-                    v1 = __ldg(p + (long long)k * d.isx + (long long)l * d.isy);
-                    if (l > 0) v0 = __ldg(p + (long long)k * d.isx + (long long)(l - 1) * d.isy);
-                } else {
-                    v1 = __ldg(p + (long long)l * d.isx + (long long)k * d.isy);
-                    if (l > 0) v0 = __ldg(p + (long long)(l - 1) * d.isx + (long long)k * d.isy);
-                }
-                s += w * (band ? v1 : 0.5f * v0 + 0.5f * v1);
+        for (int j = 0; j < 2; j++) {
+            float w = fs.img_w[j];
+            if (w == 0.f) continue;
+            const float* p = img + fs.img_off[j];
+            float v1, v0 = 0.f;
+            if (xl) {
+                v1 = __ldg(p + (long long)k * d.isx + (long long)l * d.isy);
+                if (l > 0) v0 = __ldg(p + (long long)k * d.isx + (long long)(l - 1) * d.isy);
+            } else {
+                v1 = __ldg(p + (long long)l * d.isx + (long long)k * d.isy);
+                if (l > 0) v0 = __ldg(p + (long long)(l - 1) * d.isx + (long long)k * d.isy);
             }
-            a = (double)s;
+            s += w * (band ? v1 : 0.5f * v0 + 0.5f * v1);
         }
-        double incl = warp_incl_scan(a);
-        double excl = carry + incl - a;
-        if (k < n) {
-            ohl[line_pos(k + M)] = split_double(excl);
-            ola[line_pos(k + M)] = (float)a;
+        return s;
+    };
+    // Blocks of 128 positions: loaded and stored coalesced (position 32c +
+    // lane), scanned with each lane owning 4 consecutive positions (4 lane,
+    // .., 4 lane + 3, exchanged through shared memory), so one warp scan
+    // serves 128 positions.
+    const int wib = (threadIdx.x >> 5) & 7;
+    float* sa = s_lines_a[wib];
+    double* sp = s_lines_p[wib];
+    double carry = 0.0;
+    for (int k0 = 0; k0 < n; k0 += 128) {
+        float v[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int k = k0 + 32 * c + lane;
+            v[c] = k < n ? value(k) : 0.f;
+            sa[32 * c + lane] = v[c];
+        }
+        __syncwarp();
+        const float4 q = reinterpret_cast<const float4*>(sa)[lane];
+        const double p1 = (double)q.x, p2 = p1 + (double)q.y, p3 = p2 + (double)q.z, p4 = p3 + (double)q.w;
+        const double incl = warp_incl_scan(p4);
+        const double pre = carry + (incl - p4);   // exclusive prefix at position 4 lane
+        reinterpret_cast<double2*>(sp)[2 * lane] = make_double2(pre, pre + p1);
+        reinterpret_cast<double2*>(sp)[2 * lane + 1] = make_double2(pre + p2, pre + p3);
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int k = k0 + 32 * c + lane;
+            if (k < n) {
+                ohl[line_pos(k + M)] = split_double(sp[32 * c + lane]);
+                ola[line_pos(k + M)] = v[c];
+            }
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();   // the next block overwrites sa and sp
     }
     // margins: P = 0 before the line, P = total from position n on
     float2 tot = split_double(carry);
