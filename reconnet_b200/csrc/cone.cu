@@ -313,10 +313,11 @@ __device__ __forceinline__ void staged_run(float& acc, long long& A, long long& 
             lm = fminf(t2, 1.f) - t1;
             l1 = 1.f - t2;
         }
-        float s = 0.f;
-        if (l0 > 0.f) s = l0 * pl[i0];
-        if (lm > 0.f) s = fmaf(lm, pl[im], s);
-        if (l1 > 0.f) s = fmaf(l1, pl[i1], s);
+        // branch-free (every index lies in the brick): a piece of length <= 0
+        // adds exactly 0
+        float s = fmaxf(l0, 0.f) * pl[i0];
+        s = fmaf(fmaxf(lm, 0.f), pl[im], s);
+        s = fmaf(fmaxf(l1, 0.f), pl[i1], s);
         acc += s;
         ca = ca1;
         cb = cb1;
@@ -670,14 +671,14 @@ __global__ void __launch_bounds__(256) cone_bp_sep_kernel(float* __restrict__ im
                 const float tv0 = -xv * irv, tv1 = (1.f - xv) * irv;
                 const float lv = fminf(tv0, tv1), hv = fmaxf(tv0, tv1);
                 const float* pcol = pview + j * sv;
+                // branch-free: a pair that misses both voxels adds exactly 0
+#pragma unroll 2
                 for (int k = 0; k < nk; k++) {
                     const float4 E = s_t[warp][k];
                     const float l0 = fminf(hv, E.y) - fmaxf(lv, E.x), l1 = fminf(hv, E.w) - fmaxf(lv, E.z);
-                    if (l0 > 0.f || l1 > 0.f) {
-                        const float p = __ldg(pcol + (long long)s_i[warp][k] * su);
-                        if (l0 > 0.f) acc0 = fmaf(l0, p, acc0);
-                        if (l1 > 0.f) acc1 = fmaf(l1, p, acc1);
-                    }
+                    const float p = __ldg(pcol + (long long)s_i[warp][k] * su);
+                    acc0 = fmaf(fmaxf(l0, 0.f), p, acc0);
+                    acc1 = fmaf(fmaxf(l1, 0.f), p, acc1);
                 }
             }
         }
