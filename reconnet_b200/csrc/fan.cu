@@ -851,9 +851,11 @@ __device__ __forceinline__ float siddon_pixel(const float4* T, int ilo, int imax
     const float tmin = fminf(fminf(t00, t01), fminf(t10, t11)), tmax = fmaxf(fmaxf(t00, t01), fmaxf(t10, t11));
     const int u0 = max(max(-floor_small(0.5f + 1e-3f - tmin), 0), ilo - 1);
     const int u1 = min(min(floor_small(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
-    float v = 0.f;
-    if (u0 <= u1) v = siddon_candidate(T[u0 + 1 - ilo], Ah, Al, Dh, Dl);
-    if (u0 + 1 <= u1) v += siddon_candidate(T[u0 + 2 - ilo], Ah, Al, Dh, Dl);
+    // the first two without branches: evaluated at indices clamped into the
+    // staged window [ilo, imax] and kept only when they are candidates
+    const float va = siddon_candidate(T[min(u0 + 1, imax) - ilo], Ah, Al, Dh, Dl);
+    const float vb = siddon_candidate(T[min(u0 + 2, imax) - ilo], Ah, Al, Dh, Dl);
+    float v = (u0 <= u1 ? va : 0.f) + (u0 + 1 <= u1 ? vb : 0.f);
     for (int u = u0 + 2; u <= u1; u++) v += siddon_candidate(T[u + 1 - ilo], Ah, Al, Dh, Dl);
     return v;
 }
