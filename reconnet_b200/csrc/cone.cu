@@ -773,7 +773,8 @@ __global__ void __launch_bounds__(256) cone_bp_kernel(float* __restrict__ img, c
                 const float e0 = -sm, e1 = g1.w - (float)pm;
                 const float tl = fmaxf(fmaxf(fmaxf(0.f, fminf(ta0, ta1)), fminf(tb0, tb1)), fminf(e0, e1));
                 const float th = fminf(fminf(fminf(1.f, fmaxf(ta0, ta1)), fmaxf(tb0, tb1)), fmaxf(e0, e1));
-                if (th > tl) acc = fmaf((th - tl) * g1.z, __ldg(prow + (long long)iu * su), acc);
+                // branch-free: a candidate that misses the voxel adds exactly 0
+                acc = fmaf(fmaxf(th - tl, 0.f) * g1.z, __ldg(prow + (long long)iu * su), acc);
             }
         }
     }
