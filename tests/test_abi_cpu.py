@@ -68,6 +68,15 @@ def test_bad_geometry_rejected_without_gpu():
     assert N.lib.rn_fan_sqs_update(None, None, None, None, None, None, 1.0, 0.0, 1, 0.0, 1.0, 9, None) == N.RN_ERR_ARG
 
 
+def test_tuning_calls_reject_null_plans_without_gpu():
+    from reconnet_b200 import _native as N
+    v = ctypes.c_int()
+    assert N.lib.rn_fan_plan_autotune(None, None, None, 2, None) == N.RN_ERR_ARG
+    assert N.lib.rn_fan_plan_set_tuning(None, 0, 0, 0, None) == N.RN_ERR_ARG
+    assert N.lib.rn_fan_plan_get_tuning(None, ctypes.byref(v), ctypes.byref(v), ctypes.byref(v)) == N.RN_ERR_ARG
+    assert "null" in N.last_error()
+
+
 def test_reference_named_void_calls_report_errors():
     from reconnet_b200 import _native as N
     fp = ctypes.POINTER(ctypes.c_float)()
