@@ -89,3 +89,23 @@ def test_batched_ossqs_with_and_without_autotune(rng):
     b = BatchedOSSQS(geom, counts, plan.angles, sino, w, n_subsets=4, autotune=False)
     x0 = torch.zeros_like(x)
     assert rel_l2(a.run(x0, 2).cpu().numpy(), b.run(x0, 2).cpu().numpy()) <= 1e-5
+
+
+def test_settings_on_a_plan_with_rows_and_channels(rng):
+    """A reference-layout plan (2 batches, 3 image slices, 3 detector rows, 2
+    channels): the work list spans every (batch, row, channel) slice."""
+    import torch
+    from reconnet_b200 import _native as N
+    from reconnet_b200.torch_ops import FanPlan
+    g = small_fan(nz=3, nv=3)
+    ang = (np.arange(40) * 2 * np.pi / 40).astype(np.float32)
+    plan = FanPlan(to_geometry(g), ang, nbatches=2, nchannels=2)
+    x = torch.from_numpy(rng.random(plan.img_shape).astype(np.float32)).cuda()
+    p0 = plan.project(x)
+    y = torch.from_numpy(rng.random(p0.shape).astype(np.float32)).cuda()
+    b0 = plan.backproject(y, N.RN_TYPE_MATCHED)
+    for views, lines in [(1, 1), (2, 3), (4, 10 ** 6)]:
+        plan.set_tuning(views, lines, 0)
+        assert rel_l2(plan.project(x).cpu().numpy(), p0.cpu().numpy()) <= TOL
+        assert rel_l2(plan.backproject(y, N.RN_TYPE_MATCHED).cpu().numpy(), b0.cpu().numpy()) <= TOL
+    plan.check()
