@@ -17,7 +17,9 @@
 // (its share of the slab) x seg x the voxel value, seg being the ray's length
 // per slab.  Lateral positions are 64-bit fixed point (32 fractional bits,
 // stepped by an integer add), so the split points are exact to ~1e-7 slabs
-// however far the source is.
+// however far the source is.  With every slope at most 1 the block's voxels
+// are staged in shared memory chunk by chunk (cone_fp_staged_kernel);
+// otherwise the pieces are read from global memory (cone_fp_kernel).
 //
 // Backprojection, the exact transpose as a gather (the reference scatters
 // with atomics): per voxel and view, the candidate rays are the detector
@@ -27,7 +29,10 @@
 // lies inside the voxel laterally.  The ray's lateral offsets from the voxel
 // at the voxel's low main-axis face, x_a = (S_a - a_v) + (m_v - S_m) r_a, come
 // from hi / lo float parts with exact products, as in the fan Siddon
-// backprojection, to ~1e-7 voxels.
+// backprojection, to ~1e-7 voxels (cone_bp_kernel).  When every view is
+// separable the same way (detector perpendicular to the main axis, u and v
+// along the two lateral axes: tomosynthesis) cone_bp_sep_kernel runs
+// instead, on projections pre-multiplied by seg (cone_prj_seg_kernel).
 #include <cuda_runtime.h>
 
 #include <algorithm>
