@@ -92,7 +92,34 @@ struct FilterKey {
 struct FilterVal {
     float* d_h = nullptr;   // [2nu-1]
     float* d_pw = nullptr;  // [nu] pre-weights
+    // FFT form (0 = direct convolution only): transform length N = 2^logN >=
+    // 2nu - 1, the kernel's spectrum (scaled by 1/N) and the twiddles
+    int logN = 0;
+    float2* d_H = nullptr;  // [N]
+    float2* d_tw = nullptr; // [N/2] exp(-2 pi i q / N)
 };
+
+// In-place radix-2 FFT in FP64 (host; the filter spectrum).
+static void fft64(std::vector<std::complex<double>>& a) {
+    const size_t n = a.size();
+    for (size_t i = 1, j = 0; i < n; i++) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (size_t len = 2; len <= n; len <<= 1)
+        for (size_t i = 0; i < n; i += len)
+            for (size_t j = 0; j < len / 2; j++) {
+                const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * (double)j / (double)len);
+                const std::complex<double> u = a[i + j], v = a[i + j + len / 2] * w;
+                a[i + j] = u + v;
+                a[i + j + len / 2] = u - v;
+            }
+}
+
+// Largest transform the FFT filter stages in shared memory (one signal).
+constexpr int kFilterMaxLogN = 14;
 static std::mutex g_filter_mu;
 static std::map<FilterKey, FilterVal> g_filters;
 
@@ -116,6 +143,30 @@ static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cu
     RN_CUDA_TRY(cudaMalloc(&v.d_pw, sizeof(float) * nu));
     RN_CUDA_TRY(cudaMemcpyAsync(v.d_h, hf.data(), sizeof(float) * hf.size(), cudaMemcpyHostToDevice, st));
     RN_CUDA_TRY(cudaMemcpyAsync(v.d_pw, pw.data(), sizeof(float) * nu, cudaMemcpyHostToDevice, st));
+    // FFT form: the kernel placed circularly (offset k = i - (nu-1) at index
+    // k mod N), transformed in FP64; the circular convolution of length N >=
+    // 2nu - 1 equals the linear one on outputs 0 .. nu-1
+    int logN = 1;
+    while ((1 << logN) < 2 * nu - 1) logN++;
+    std::vector<float2> Hf, twf;
+    if (logN <= kFilterMaxLogN) {
+        const int N = 1 << logN;
+        std::vector<std::complex<double>> hc(N, 0.0);
+        for (int i = 0; i < 2 * nu - 1; i++) hc[((i - (nu - 1)) % N + N) % N] += h[i];
+        fft64(hc);
+        Hf.resize(N);
+        for (int f = 0; f < N; f++) Hf[f] = make_float2((float)(hc[f].real() / N), (float)(hc[f].imag() / N));
+        twf.resize(N / 2);
+        for (int q = 0; q < N / 2; q++) {
+            const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * (double)q / (double)N);
+            twf[q] = make_float2((float)w.real(), (float)w.imag());
+        }
+        v.logN = logN;
+        RN_CUDA_TRY(cudaMalloc(&v.d_H, sizeof(float2) * N));
+        RN_CUDA_TRY(cudaMalloc(&v.d_tw, sizeof(float2) * (N / 2)));
+        RN_CUDA_TRY(cudaMemcpyAsync(v.d_H, Hf.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
+        RN_CUDA_TRY(cudaMemcpyAsync(v.d_tw, twf.data(), sizeof(float2) * (N / 2), cudaMemcpyHostToDevice, st));
+    }
     RN_CUDA_TRY(cudaStreamSynchronize(st));
     g_filters[key] = v;
     out = v;
@@ -179,6 +230,136 @@ __global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, co
         }
 }
 
+// FFT filter: the same product as filter_kernel as a circular convolution of
+// length N = 2^logN >= 2nu - 1.  A CTA holds S complex signals in shared
+// memory, each carrying two views (real and imaginary parts: the kernel is
+// real, so their convolutions separate again); views run along the threads
+// for the loads and stores.  Pre-weighted samples go to bit-reversed
+// positions, a radix-2 decimation-in-time pass gives the spectrum in natural
+// order, the product with the kernel's spectrum (which carries 1/N) follows,
+// and a decimation-in-frequency pass with conjugate twiddles returns the
+// outputs in bit-reversed order, scaled on the way out.  N / 2 log2(N) butterflies per
+// view pair instead of nu^2 multiply-adds per view.
+constexpr int kFftThreads = 512;
+
+__global__ void __launch_bounds__(kFftThreads) filter_fft_kernel(float* __restrict__ out, const float* __restrict__ prj,
+                                                         const float2* __restrict__ H, const float2* __restrict__ tw,
+                                                         const float* __restrict__ pw, int nu, int nview, int nv,
+                                                         int nc, int logN, int S, float scale) {
+    extern __shared__ float2 zs[];   // S signals, stride N + 1 (one pad entry against bank conflicts), then the twiddles
+    const int N = 1 << logN, Np = N + 1, halfN = N >> 1;
+    float2* tws = zs + S * Np;
+    for (int q = threadIdx.x; q < halfN; q += blockDim.x) tws[q] = __ldg(tw + q);
+    const int plane = blockIdx.y;
+    const int b = plane / (nv * nc);
+    const int rem = plane - b * nv * nc;
+    const long long off = (long long)b * nu * nview * nv * nc + rem;
+    const long long su = (long long)nview * nv * nc, sview = (long long)nv * nc;
+    const int v0 = blockIdx.x * 2 * S;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < S * N; e += blockDim.x) {
+        const int p = e % S, n = e / S;
+        float a = 0.f, c = 0.f;
+        if (n < nu) {
+            const int va = v0 + 2 * p;
+            const float w = pw[n];
+            const float* src = prj + off + (long long)n * su;
+            if (va < nview) a = src[(long long)va * sview] * w;
+            if (va + 1 < nview) c = src[(long long)(va + 1) * sview] * w;
+        }
+        zs[p * Np + (int)(__brev((unsigned)n) >> (32 - logN))] = make_float2(a, c);
+    }
+    __syncthreads();
+    // decimation in time: pairs of radix-2 levels (s, s + 1) fused into one
+    // pass over quads in registers, then the last level if logN is odd
+    auto cmul = [](float2 a, float2 w) { return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); };
+    auto cmulc = [](float2 a, float2 w) { return make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y); };
+    auto add = [](float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); };
+    auto sub = [](float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); };
+    const int quarterN = N >> 2;
+    int s = 0;
+    for (; s + 1 < logN; s += 2) {
+        const int h = 1 << s;
+        for (int qb = tid; qb < S * quarterN; qb += blockDim.x) {
+            const int p = qb >> (logN - 2), qi = qb & (quarterN - 1);
+            const int j = qi & (h - 1), k = ((qi >> s) << (s + 2)) + j;
+            float2* z = zs + p * Np;
+            const float2 a0 = z[k], a1 = z[k + h], a2 = z[k + 2 * h], a3 = z[k + 3 * h];
+            const float2 w1 = tws[j << (logN - 1 - s)];
+            float2 t = cmul(a1, w1);
+            const float2 b0 = add(a0, t), b1 = sub(a0, t);
+            t = cmul(a3, w1);
+            const float2 b2 = add(a2, t), b3 = sub(a2, t);
+            const float2 w2 = tws[j << (logN - 2 - s)], w3 = tws[(j + h) << (logN - 2 - s)];
+            t = cmul(b2, w2);
+            z[k] = add(b0, t);
+            z[k + 2 * h] = sub(b0, t);
+            t = cmul(b3, w3);
+            z[k + h] = add(b1, t);
+            z[k + 3 * h] = sub(b1, t);
+        }
+        __syncthreads();
+    }
+    if (s < logN) {
+        const int half = 1 << s;
+        for (int bb = tid; bb < S * halfN; bb += blockDim.x) {
+            const int p = bb >> (logN - 1), bi = bb & (halfN - 1);
+            const int j = bi & (half - 1), k = ((bi >> s) << (s + 1)) + j;
+            const float2 w = tws[j << (logN - 1 - s)];
+            float2* z = zs + p * Np;
+            const float2 u = z[k], t = cmul(z[k + half], w);
+            z[k] = add(u, t);
+            z[k + half] = sub(u, t);
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < S * N; e += blockDim.x) {
+        const int p = e >> logN, n = e & (N - 1);
+        float2* z = zs + p * Np;
+        const float2 hh = __ldg(H + n), v = z[n];
+        z[n] = make_float2(v.x * hh.x - v.y * hh.y, v.x * hh.y + v.y * hh.x);
+    }
+    __syncthreads();
+    // decimation in frequency with conjugate twiddles (the inverse): pairs
+    // of levels (s + 1, s) fused, from the top, then level 0 if logN is odd
+    for (s = logN - 2; s >= 0; s -= 2) {
+        const int h = 1 << s;
+        for (int qb = tid; qb < S * quarterN; qb += blockDim.x) {
+            const int p = qb >> (logN - 2), qi = qb & (quarterN - 1);
+            const int j = qi & (h - 1), k = ((qi >> s) << (s + 2)) + j;
+            float2* z = zs + p * Np;
+            const float2 a0 = z[k], a1 = z[k + h], a2 = z[k + 2 * h], a3 = z[k + 3 * h];
+            const float2 w2 = tws[j << (logN - 2 - s)], w3 = tws[(j + h) << (logN - 2 - s)];
+            const float2 b0 = add(a0, a2), b2 = cmulc(sub(a0, a2), w2);
+            const float2 b1 = add(a1, a3), b3 = cmulc(sub(a1, a3), w3);
+            const float2 w1 = tws[j << (logN - 1 - s)];
+            z[k] = add(b0, b1);
+            z[k + h] = cmulc(sub(b0, b1), w1);
+            z[k + 2 * h] = add(b2, b3);
+            z[k + 3 * h] = cmulc(sub(b2, b3), w1);
+        }
+        __syncthreads();
+    }
+    if (s == -1) {
+        for (int bb = tid; bb < S * halfN; bb += blockDim.x) {
+            const int p = bb >> (logN - 1), k = 2 * (bb & (halfN - 1));
+            float2* z = zs + p * Np;
+            const float2 u = z[k], v = z[k + 1];
+            z[k] = add(u, v);
+            z[k + 1] = sub(u, v);   // times conj(tw[0]) = 1
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < S * nu; e += blockDim.x) {
+        const int p = e % S, n = e / S;
+        const float2 r = zs[p * Np + (int)(__brev((unsigned)n) >> (32 - logN))];
+        const int va = v0 + 2 * p;
+        float* dst = out + off + (long long)n * su;
+        if (va < nview) dst[(long long)va * sview] = r.x * scale;
+        if (va + 1 < nview) dst[(long long)(va + 1) * sview] = r.y * scale;
+    }
+}
+
 int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int nview, int nv, float da,
                   float off_a, float dsd, float dso, int typeFilter, int fan, cudaStream_t st) {
     (void)dsd;
@@ -189,6 +370,18 @@ int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int 
     RN_TRY(get_filter(nu, da, off_a, typeFilter, fan, st, fv));
     // scale of cFilterFan::Filter (Filter.cu:294-302) without the FFT length factor
     double scale = fan ? kRefPi / nview * da / dso : kRefPi / nview * da;
+    if (fv.logN > 0 && (long long)nb * nv * nc <= 65535) {
+        // S signals (2S views) per CTA: ~64 KB of shared memory at N = 2048
+        const int N = 1 << fv.logN;
+        const int S = std::max(1, std::min(16, 8192 / N));
+        const size_t smem = sizeof(float2) * ((size_t)S * (N + 1) + N / 2);
+        RN_CUDA_TRY(cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 grid((unsigned)((nview + 2 * S - 1) / (2 * S)), (unsigned)(nb * nv * nc));
+        filter_fft_kernel<<<grid, kFftThreads, smem, st>>>(d_out, d_prj, fv.d_H, fv.d_tw, fv.d_pw, nu, nview, nv, nc, fv.logN,
+                                                   S, (float)scale);
+        RN_CUDA_TRY(cudaGetLastError());
+        return RN_OK;
+    }
     dim3 grid((nview + 63) / 64, (nu + 63) / 64, nb * nv * nc);
     filter_kernel<<<grid, 256, 0, st>>>(d_out, d_prj, fv.d_h, fv.d_pw, nu, nview, nv, nc, (float)scale);
     RN_CUDA_TRY(cudaGetLastError());
