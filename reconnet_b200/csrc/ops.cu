@@ -242,6 +242,54 @@ __global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, co
 // view pair instead of nu^2 multiply-adds per view.
 constexpr int kFftThreads = 512;
 
+__device__ __forceinline__ float2 c_mul(float2 a, float2 w) {
+    return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+__device__ __forceinline__ float2 c_mulc(float2 a, float2 w) {   // a * conj(w)
+    return make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// Radix-2 levels s .. s + T - 1 of every signal in one pass over groups of
+// 2^T elements held in registers: decimation in time (levels ascending) or,
+// kInv, decimation in frequency with conjugate twiddles (levels descending).
+// The arithmetic is that of T separate radix-2 passes.
+template <int T, bool kInv>
+__device__ __forceinline__ void fft_pass(float2* zs, const float2* tws, int Np, int S, int logN, int s) {
+    constexpr int R = 1 << T;
+    const int h = 1 << s, groups = (1 << logN) >> T;
+    for (int gb = threadIdx.x; gb < S * groups; gb += blockDim.x) {
+        const int p = gb >> (logN - T), gi = gb & (groups - 1);
+        const int j = gi & (h - 1), k = ((gi >> s) << (s + T)) + j;
+        float2* z = zs + p * Np + k;
+        float2 a[R];
+#pragma unroll
+        for (int m = 0; m < R; m++) a[m] = z[m * h];
+#pragma unroll
+        for (int tt = 0; tt < T; tt++) {
+            const int t = kInv ? T - 1 - tt : tt;
+            const int st = 1 << t;
+#pragma unroll
+            for (int m = 0; m < R; m++) {
+                if (m & st) continue;
+                const float2 w = tws[(j + (m & (st - 1)) * h) << (logN - 1 - s - t)];
+                if (!kInv) {
+                    const float2 x = c_mul(a[m + st], w);
+                    a[m + st] = c_sub(a[m], x);
+                    a[m] = c_add(a[m], x);
+                } else {
+                    const float2 u = a[m], v = a[m + st];
+                    a[m] = c_add(u, v);
+                    a[m + st] = c_mulc(c_sub(u, v), w);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; m++) z[m * h] = a[m];
+    }
+}
+
 __global__ void __launch_bounds__(kFftThreads) filter_fft_kernel(float* __restrict__ out, const float* __restrict__ prj,
                                                          const float2* __restrict__ H, const float2* __restrict__ tw,
                                                          const float* __restrict__ pw, int nu, int nview, int nv,
@@ -270,47 +318,20 @@ __global__ void __launch_bounds__(kFftThreads) filter_fft_kernel(float* __restri
         zs[p * Np + (int)(__brev((unsigned)n) >> (32 - logN))] = make_float2(a, c);
     }
     __syncthreads();
-    // decimation in time: pairs of radix-2 levels (s, s + 1) fused into one
-    // pass over quads in registers, then the last level if logN is odd
-    auto cmul = [](float2 a, float2 w) { return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); };
-    auto cmulc = [](float2 a, float2 w) { return make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y); };
-    auto add = [](float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); };
-    auto sub = [](float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); };
-    const int quarterN = N >> 2;
+    // decimation in time: radix-2 levels fused three at a time (then two or
+    // one for the remainder), ascending
     int s = 0;
-    for (; s + 1 < logN; s += 2) {
-        const int h = 1 << s;
-        for (int qb = tid; qb < S * quarterN; qb += blockDim.x) {
-            const int p = qb >> (logN - 2), qi = qb & (quarterN - 1);
-            const int j = qi & (h - 1), k = ((qi >> s) << (s + 2)) + j;
-            float2* z = zs + p * Np;
-            const float2 a0 = z[k], a1 = z[k + h], a2 = z[k + 2 * h], a3 = z[k + 3 * h];
-            const float2 w1 = tws[j << (logN - 1 - s)];
-            float2 t = cmul(a1, w1);
-            const float2 b0 = add(a0, t), b1 = sub(a0, t);
-            t = cmul(a3, w1);
-            const float2 b2 = add(a2, t), b3 = sub(a2, t);
-            const float2 w2 = tws[j << (logN - 2 - s)], w3 = tws[(j + h) << (logN - 2 - s)];
-            t = cmul(b2, w2);
-            z[k] = add(b0, t);
-            z[k + 2 * h] = sub(b0, t);
-            t = cmul(b3, w3);
-            z[k + h] = add(b1, t);
-            z[k + 3 * h] = sub(b1, t);
-        }
+    for (; s + 2 < logN; s += 3) {
+        fft_pass<3, false>(zs, tws, Np, S, logN, s);
         __syncthreads();
     }
+    if (s + 1 < logN) {
+        fft_pass<2, false>(zs, tws, Np, S, logN, s);
+        __syncthreads();
+        s += 2;
+    }
     if (s < logN) {
-        const int half = 1 << s;
-        for (int bb = tid; bb < S * halfN; bb += blockDim.x) {
-            const int p = bb >> (logN - 1), bi = bb & (halfN - 1);
-            const int j = bi & (half - 1), k = ((bi >> s) << (s + 1)) + j;
-            const float2 w = tws[j << (logN - 1 - s)];
-            float2* z = zs + p * Np;
-            const float2 u = z[k], t = cmul(z[k + half], w);
-            z[k] = add(u, t);
-            z[k + half] = sub(u, t);
-        }
+        fft_pass<1, false>(zs, tws, Np, S, logN, s);
         __syncthreads();
     }
     for (int e = tid; e < S * N; e += blockDim.x) {
@@ -320,34 +341,17 @@ __global__ void __launch_bounds__(kFftThreads) filter_fft_kernel(float* __restri
         z[n] = make_float2(v.x * hh.x - v.y * hh.y, v.x * hh.y + v.y * hh.x);
     }
     __syncthreads();
-    // decimation in frequency with conjugate twiddles (the inverse): pairs
-    // of levels (s + 1, s) fused, from the top, then level 0 if logN is odd
-    for (s = logN - 2; s >= 0; s -= 2) {
-        const int h = 1 << s;
-        for (int qb = tid; qb < S * quarterN; qb += blockDim.x) {
-            const int p = qb >> (logN - 2), qi = qb & (quarterN - 1);
-            const int j = qi & (h - 1), k = ((qi >> s) << (s + 2)) + j;
-            float2* z = zs + p * Np;
-            const float2 a0 = z[k], a1 = z[k + h], a2 = z[k + 2 * h], a3 = z[k + 3 * h];
-            const float2 w2 = tws[j << (logN - 2 - s)], w3 = tws[(j + h) << (logN - 2 - s)];
-            const float2 b0 = add(a0, a2), b2 = cmulc(sub(a0, a2), w2);
-            const float2 b1 = add(a1, a3), b3 = cmulc(sub(a1, a3), w3);
-            const float2 w1 = tws[j << (logN - 1 - s)];
-            z[k] = add(b0, b1);
-            z[k + h] = cmulc(sub(b0, b1), w1);
-            z[k + 2 * h] = add(b2, b3);
-            z[k + 3 * h] = cmulc(sub(b2, b3), w1);
-        }
+    // decimation in frequency with conjugate twiddles (the inverse): three
+    // levels per pass from the top, then the remaining two or one
+    for (s = logN - 3; s >= 0; s -= 3) {
+        fft_pass<3, true>(zs, tws, Np, S, logN, s);
         __syncthreads();
     }
-    if (s == -1) {
-        for (int bb = tid; bb < S * halfN; bb += blockDim.x) {
-            const int p = bb >> (logN - 1), k = 2 * (bb & (halfN - 1));
-            float2* z = zs + p * Np;
-            const float2 u = z[k], v = z[k + 1];
-            z[k] = add(u, v);
-            z[k + 1] = sub(u, v);   // times conj(tw[0]) = 1
-        }
+    if (s + 3 == 2) {
+        fft_pass<2, true>(zs, tws, Np, S, logN, 0);
+        __syncthreads();
+    } else if (s + 3 == 1) {
+        fft_pass<1, true>(zs, tws, Np, S, logN, 0);
         __syncthreads();
     }
     for (int e = tid; e < S * nu; e += blockDim.x) {
