@@ -236,9 +236,9 @@ __global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, co
 // real, so their convolutions separate again); views run along the threads
 // for the loads and stores.  Pre-weighted samples go to bit-reversed
 // positions, a radix-2 decimation-in-time pass gives the spectrum in natural
-// order, the product with the kernel's spectrum (which carries 1/N) follows,
-// and a decimation-in-frequency pass with conjugate twiddles returns the
-// outputs in bit-reversed order, scaled on the way out.  N / 2 log2(N) butterflies per
+// order, the product with the kernel's spectrum (which carries 1/N) is taken
+// in its last pass, and a decimation-in-frequency pass with conjugate
+// twiddles returns the outputs in bit-reversed order, scaled on the way out.  N / 2 log2(N) butterflies per
 // view pair instead of nu^2 multiply-adds per view.
 constexpr int kFftThreads = 512;
 
@@ -254,9 +254,12 @@ __device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2
 // Radix-2 levels s .. s + T - 1 of every signal in one pass over groups of
 // 2^T elements held in registers: decimation in time (levels ascending) or,
 // kInv, decimation in frequency with conjugate twiddles (levels descending).
-// The arithmetic is that of T separate radix-2 passes.
-template <int T, bool kInv>
-__device__ __forceinline__ void fft_pass(float2* zs, const float2* tws, int Np, int S, int logN, int s) {
+// The arithmetic is that of T separate radix-2 passes.  kMul (the last
+// forward pass, whose outputs are in natural order): multiply by H on the
+// way out.
+template <int T, bool kInv, bool kMul = false>
+__device__ __forceinline__ void fft_pass(float2* zs, const float2* tws, int Np, int S, int logN, int s,
+                                         const float2* __restrict__ H = nullptr) {
     constexpr int R = 1 << T;
     const int h = 1 << s, groups = (1 << logN) >> T;
     for (int gb = threadIdx.x; gb < S * groups; gb += blockDim.x) {
@@ -286,11 +289,11 @@ __device__ __forceinline__ void fft_pass(float2* zs, const float2* tws, int Np, 
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; m++) z[m * h] = a[m];
+        for (int m = 0; m < R; m++) z[m * h] = kMul ? c_mul(a[m], __ldg(H + k + m * h)) : a[m];
     }
 }
 
-__global__ void __launch_bounds__(kFftThreads) filter_fft_kernel(float* __restrict__ out, const float* __restrict__ prj,
+__global__ void __launch_bounds__(kFftThreads, 2) filter_fft_kernel(float* __restrict__ out, const float* __restrict__ prj,
                                                          const float2* __restrict__ H, const float2* __restrict__ tw,
                                                          const float* __restrict__ pw, int nu, int nview, int nv,
                                                          int nc, int logN, int S, float scale) {
@@ -320,27 +323,23 @@ __global__ void __launch_bounds__(kFftThreads) filter_fft_kernel(float* __restri
     __syncthreads();
     // decimation in time: radix-2 levels fused three at a time (then two or
     // one for the remainder), ascending
+    // (the last pass also multiplies by the kernel's spectrum)
     int s = 0;
     for (; s + 2 < logN; s += 3) {
-        fft_pass<3, false>(zs, tws, Np, S, logN, s);
+        if (s + 3 == logN) fft_pass<3, false, true>(zs, tws, Np, S, logN, s, H);
+        else fft_pass<3, false>(zs, tws, Np, S, logN, s);
         __syncthreads();
     }
     if (s + 1 < logN) {
-        fft_pass<2, false>(zs, tws, Np, S, logN, s);
+        if (s + 2 == logN) fft_pass<2, false, true>(zs, tws, Np, S, logN, s, H);
+        else fft_pass<2, false>(zs, tws, Np, S, logN, s);
         __syncthreads();
         s += 2;
     }
     if (s < logN) {
-        fft_pass<1, false>(zs, tws, Np, S, logN, s);
+        fft_pass<1, false, true>(zs, tws, Np, S, logN, s, H);
         __syncthreads();
     }
-    for (int e = tid; e < S * N; e += blockDim.x) {
-        const int p = e >> logN, n = e & (N - 1);
-        float2* z = zs + p * Np;
-        const float2 hh = __ldg(H + n), v = z[n];
-        z[n] = make_float2(v.x * hh.x - v.y * hh.y, v.x * hh.y + v.y * hh.x);
-    }
-    __syncthreads();
     // decimation in frequency with conjugate twiddles (the inverse): three
     // levels per pass from the top, then the remaining two or one
     for (s = logN - 3; s >= 0; s -= 3) {
