@@ -80,17 +80,18 @@ def measured_peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes per launch of `kernel` on this workload from the committed
-    ncu summary (profiles/ncu_dram_bytes.txt: `<kernel> <bytes_per_launch>`)."""
-    p = os.path.join(ROOT, "profiles", "ncu_dram_bytes.txt")
+def ncu_counts(kernel):
+    """Per-launch ncu counters of `kernel` at the bench size from the committed
+    summary (profiles/ncu_counts_bench.txt: `<kernel> <dram_bytes> <warp_inst>`);
+    None where the file or the kernel's line is missing."""
+    p = os.path.join(ROOT, "profiles", "ncu_counts_bench.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
         parts = line.split()
-        if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+        if len(parts) >= 3 and parts[0] == kernel and not line.startswith("#"):
             try:
-                return float(parts[1])
+                return {"dram_bytes": float(parts[1]), "warp_inst": float(parts[2])}
             except ValueError:
                 return None
     return None
@@ -191,7 +192,9 @@ def cpu_baseline_sample(geom, counts, angles, imgs, target_s=12.0):
 def run_reference(args):
     """Reference arm: the CPU port of the reference DD loop on the host cores
     (rank 0 only), plus the reference's own CUDA library (built from its
-    sources into oracle/_ref) on the same GPU for context."""
+    sources into oracle/_ref) on the same GPU for context.  Nothing here loads
+    this repository's sm_100a library: the workload comes from
+    reconnet_b200.phantom / .geometry, which import no native code."""
     rank, local, world = dist_env()
     if rank != 0:
         return
@@ -206,7 +209,7 @@ def run_reference(args):
     def step(nv):
         sel = angles[:n0][:: max(1, n0 // nv)][:nv].copy()
         p = O.fan_fp(img, sel, geom, geom.nu, 1, dtype=np.float32)
-        O.fan_bp(p, sel, geom, (geom.nx, geom.ny, 1), 2, dtype=np.float32)
+        O.fan_bp(p, sel, geom, (geom.nx, geom.ny, 1), 0, dtype=np.float32)
         return sel.size * (geom.nu * geom.ny + geom.nx * geom.ny)
 
     t0 = time.perf_counter()
@@ -220,8 +223,9 @@ def run_reference(args):
         upd += step(nv)
     dt = time.perf_counter() - t0
     value = upd / dt / 1e9
-    sample = (f"per step: 1 slice 512x512, 888 ch, {nv} of its {n0} views, FP + matched BP; FP32 OpenMP port of "
-              f"the reference DD loop (the reference has no CPU path), {threads} threads")
+    sample = (f"per step: 1 slice 512x512, 888 ch, {nv} of its {n0} views: the reference's DD forward projection "
+              f"(DDFPFanKernelX/Y) and its iterative backprojection (DDBPFanKernelX/Y, typeProjector 0), as the "
+              f"oracle's FP32 OpenMP port (the reference has no CPU DD path), {threads} threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -664,6 +668,46 @@ def filter_run(dev, cpu_sample=True):
     return out
 
 
+def fan_roofline(kernel, dur_ms, updates, io_bytes, clocks, dev):
+    """Roofline of the dominant fan kernel against its real bound.
+
+    The DD kernels are not HBM-bound: they read their prefix samples from
+    shared memory and move ~1 GB of DRAM per launch (under 1% of peak).  They
+    are bound by instruction issue (and the L1/shared pipe behind it).  So the
+    headline fraction is issue-rate: the kernel's warp instructions per launch
+    (ncu, profiles/ncu_counts_bench.txt) over its CUDA-event launch time,
+    against one warp instruction per clock on each of the 4 schedulers of
+    every SM at the SM clock sampled during the timed region.  Beside it:
+    `hbm`, the measured DRAM bytes over the same time against the measured
+    HBM peak, and `effective_onchip`, the 8 B-per-footprint model (two FP32
+    prefix samples per update) that these kernels serve from shared memory."""
+    import torch
+    counts = ncu_counts(kernel)
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_hbm, peak_kind = measured_peaks()
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+    t = dur_ms * 1e-3
+    onchip = BYTES_PER_UPDATE * updates + io_bytes
+    out = {"bound": "issue", "kernel": kernel, "launch_ms": dur_ms, "unit": "Gwarp-inst/s",
+           "achieved": None, "peak": None, "frac": None, "traffic": None,
+           "peak_source": f"{n_sm} SMs x 4 schedulers x 1 warp instruction per clock at the sampled SM clock",
+           "hbm": {"achieved": None, "peak": peak_hbm, "unit": "GB/s", "frac": None, "peak_kind": peak_kind},
+           "effective_onchip": {"bytes_per_launch": onchip, "gbs": onchip / t / 1e9,
+                                "model": f"{BYTES_PER_UPDATE} B per footprint update (two FP32 prefix samples, "
+                                         "read from shared memory) + 4 B per image/sinogram element"}}
+    if counts is not None:
+        out["traffic"] = counts["dram_bytes"]
+        out["hbm"]["achieved"] = counts["dram_bytes"] / t / 1e9
+        out["hbm"]["frac"] = out["hbm"]["achieved"] / peak_hbm
+        if mhz:
+            peak_inst = n_sm * 4 * mhz * 1e6
+            out["achieved"] = counts["warp_inst"] / t / 1e9
+            out["peak"] = peak_inst / 1e9
+            out["frac"] = counts["warp_inst"] / t / peak_inst
+            out["sm_mhz"] = mhz
+    return out
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -730,18 +774,10 @@ def run_b200(args):
     fp_ms = kt["fp"][0] / max(kt["fp"][1], 1)
     bp_ms = kt["bp"][0] / max(kt["bp"][1], 1)
     dominant = "fan_fp_kernel" if kt["fp"][0] >= kt["bp"][0] else "fan_bp_kernel"
-    io_bytes = 4 * (x.numel() + p.numel())
-    if dominant == "fan_fp_kernel":
-        alg_bytes, dur_ms = BYTES_PER_UPDATE * fp_upd + io_bytes, fp_ms
-    else:
-        alg_bytes, dur_ms = BYTES_PER_UPDATE * bp_upd + io_bytes, bp_ms
-    peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / (dur_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": ncu_traffic(dominant), "kernel": dominant, "peak_kind": peak_kind,
-                "alg_bytes_per_launch": alg_bytes, "launch_ms": dur_ms,
-                "kernels_ms": {k: (v[0] / max(v[1], 1)) for k, v in kt.items() if v[1]},
-                "model": f"{BYTES_PER_UPDATE} B per footprint update + 4 B per image/sinogram element"}
+    roofline = fan_roofline(dominant, fp_ms if dominant == "fan_fp_kernel" else bp_ms,
+                            fp_upd if dominant == "fan_fp_kernel" else bp_upd, 4 * (x.numel() + p.numel()),
+                            clk.summary(), dev)
+    roofline["kernels_ms"] = {k: (v[0] / max(v[1], 1)) for k, v in kt.items() if v[1]}
 
     # ---- end to end through the public API with host buffers ----
     # StreamedFanPair: pinned host images in, pinned host backprojections out,

@@ -237,6 +237,32 @@ int rn_fan_plan_get_tuning(const rn_fan_plan* plan, int* fp_views, int* fp_lines
 int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int nu, int nview, int nv, float da,
               float off_a, float dsd, float dso, int typeFilter, int fan, void* stream);
 
+/* The same filter with short-scan weights d_w [nu][nview] (broadcast over
+ * batches, detector rows and channels) multiplied into the sinogram as it is
+ * loaded: the reference's FBP chain multiplies its Parker / Riess weights
+ * into the projections before cFilterFanFilter (python/ReconNet_no_tf.py:
+ * 640-693 with :396-440).  d_w comes from rn_fan_shortscan_weights. */
+int rn_filter_weighted(float* d_out, const float* d_prj, const float* d_w, int nBatches, int nChannels, int nu,
+                       int nview, int nv, float da, float off_a, float dsd, float dso, int typeFilter, int fan,
+                       void* stream);
+
+/* Short-scan redundancy weights [nu][nview] for fan-beam FBP over
+ * [0, angles[nview-1]] (gamma = (angles[nview-1] - pi) / 2).  Replaces the
+ * reference's Python ParkerWeighting / RiessWeighting
+ * (python/ReconNet_no_tf.py:640-659 / 665-693), with the same channel angle
+ * alpha = ((u - (nu-1)/2) - off_a) * da.  kind RN_WEIGHT_PARKER, or
+ * RN_WEIGHT_RIESS with its Gaussian smoothing (sigma channels, reach
+ * int(4 sigma + 0.5)) outside theta < beta < pi + 2 gamma - theta.  riessMask
+ * 0 keeps only channel 0 of those middle views unsmoothed, as the reference's
+ * np.where(np.all(...)) does; 1 keeps the whole view unsmoothed.  d_angles is
+ * a device array; the _host variant takes and returns host arrays. */
+#define RN_WEIGHT_PARKER 0
+#define RN_WEIGHT_RIESS 1
+int rn_fan_shortscan_weights(float* d_w, const float* d_angles, int nu, int nview, float da, float off_a, int kind,
+                             float sigma, float theta, int riessMask, void* stream);
+int rn_fan_shortscan_weights_host(float* w, const float* angles, int nu, int nview, float da, float off_a, int kind,
+                                  float sigma, float theta, int riessMask);
+
 /* TV surrogate on a batch of S slices [S][nx][ny]; grad/norm may be NULL;
  * d_tv (may be NULL) receives S FP64 TV values. */
 int rn_tv_sqs(float* d_grad, float* d_norm, double* d_tv, const float* d_img, int nslices, int nx, int ny,

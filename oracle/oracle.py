@@ -311,3 +311,48 @@ def sqs_subset_update(x, sino, wsino, norm_img, angles, views, g, n_subsets, lam
         den = den + beta * norm
     xn = x.astype(np.float64) - lam * num / den
     return np.clip(xn, lb, ub)
+
+
+def shortscan_weights(angles, nu, da, off_a, kind="parker", sigma=30.0, theta=10 * np.pi / 180, mask_all=False):
+    """Short-scan redundancy weights [nu, nview] in FP64 with the reference's
+    conventions (python/ReconNet_no_tf.py:640-693): channel angle
+    alpha = ((u - (nu-1)/2) - off_a) * da, half over-scan
+    gamma = (angles[-1] - pi) / 2.
+
+    Parker (Med. Phys. 9(2), 1982): sin^2 ramps over the doubly measured
+    wedges beta < 2(gamma - alpha) and beta > pi - 2 alpha, 1 between.
+    Riess: the ramps continued past those wedges as 2 - ramp (reference
+    precedence :681-684: first wedge, its continuation, second wedge, its
+    continuation), rounded to FP32 as the reference stores them, then smoothed
+    along the channels by a normalised Gaussian of `sigma` channels reaching
+    int(4 sigma + 0.5) channels with edge values repeated -- except, in views
+    with theta < beta < pi + 2 gamma - theta, channel 0 (the reference's
+    np.where over the 0-d result of np.all, :687-688) or, with mask_all, the
+    whole view."""
+    ang = np.asarray(angles, np.float32).astype(np.float64)
+    beta = ang[None, :]
+    gamma = (ang[-1] - np.pi) / 2
+    alpha = ((np.arange(nu) - (nu - 1) / 2.0) - off_a)[:, None] * float(da)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ramp_in = np.sin(np.pi / 4 * beta / (gamma - alpha)) ** 2
+        ramp_out = np.sin(np.pi / 4 * (np.pi + 2 * gamma - beta) / (gamma + alpha)) ** 2
+    first_wedge = beta < 2 * gamma - 2 * alpha
+    if kind == "parker":
+        return np.where(first_wedge, ramp_in, np.where(beta <= np.pi - 2 * alpha, 1.0, ramp_out))
+    conds = [first_wedge, beta < -2 * gamma + 2 * alpha, beta > np.pi - 2 * alpha, beta > np.pi + 2 * gamma + 2 * alpha]
+    vals = [ramp_in, 2 - ramp_in, ramp_out, 2 - ramp_out]
+    full = np.broadcast_shapes(alpha.shape, beta.shape)
+    w = np.select([np.broadcast_to(c, full) for c in conds], [np.broadcast_to(v, full) for v in vals], default=1.0)
+    w = w.astype(np.float32).astype(np.float64)
+    r = int(4.0 * sigma + 0.5)
+    taps = np.exp(-0.5 * (np.arange(-r, r + 1) / sigma) ** 2)
+    taps /= taps.sum()
+    padded = np.pad(w, ((r, r), (0, 0)), mode="edge")
+    smooth = np.zeros_like(w)
+    for k in range(2 * r + 1):
+        smooth += taps[k] * padded[k:k + nu]
+    keep_view = (beta > theta) & (beta < np.pi + 2 * gamma - theta)        # [1, nview]
+    keep = np.broadcast_to(keep_view, full).copy()
+    if not mask_all:
+        keep[1:, :] = False
+    return np.where(keep, w, smooth)

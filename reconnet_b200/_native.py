@@ -22,6 +22,8 @@ RN_TYPE_FBP = 1
 RN_TYPE_MATCHED = 2
 RN_TYPE_SIDDON = 3
 RN_TYPE_PIXEL = 4
+RN_WEIGHT_PARKER = 0
+RN_WEIGHT_RIESS = 1
 
 _f = ctypes.c_float
 _i = ctypes.c_int
@@ -96,6 +98,9 @@ SIGNATURES = {
     "rn_fan_plan_get_tuning": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "rn_fan_plan_read_timing": (_i, [_vp, _fp, ctypes.POINTER(_i), _i, ctypes.POINTER(ctypes.c_longlong)]),
     "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
+    "rn_filter_weighted": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
+    "rn_fan_shortscan_weights": (_i, [_vp, _vp, _i, _i, _f, _f, _i, _f, _f, _i, _vp]),
+    "rn_fan_shortscan_weights_host": (_i, [_fp, _fp, _i, _i, _f, _f, _i, _f, _f, _i]),
     "rn_tv_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
     "rn_tv_iso_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _vp]),
     "rn_tv_iso_sqs_host": (_i, [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _i, _f, _i]),

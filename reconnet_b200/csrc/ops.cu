@@ -1,6 +1,7 @@
 // Ramp filter, TV surrogate, OS-SQS update and the reference-named host
 // entry points (synchronous, host pointers).
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <stdint.h>
 #include <string.h>
 
@@ -178,10 +179,12 @@ static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cu
 // 4x4 per thread, inputs staged 32 at a time in shared memory.
 __global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, const float* __restrict__ prj,
                                                      const float* __restrict__ h, const float* __restrict__ pw,
-                                                     int nu, int nview, int nv, int nc, float scale) {
+                                                     const float* __restrict__ sw, int nu, int nview, int nv,
+                                                     int nc, int nplane_total, float scale) {
     __shared__ float Xs[32][64 + 4];
     __shared__ float Hs[96];
-    const int plane = blockIdx.z;
+    const int nplanes = nplane_total;
+    for (int plane = blockIdx.z; plane < nplanes; plane += gridDim.z) {
     const int b = plane / (nv * nc);
     const int rem = plane - b * nv * nc;
     const long long off = (long long)b * nu * nview * nv * nc + rem;   // (iv, c) folded: rem = iv*nc + c
@@ -199,7 +202,10 @@ __global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, co
             int jj = e >> 6, vv = e & 63;
             int j = j0 + jj, v = v0 + vv;
             float x = 0.f;
-            if (j < nu && v < nview) x = prj[off + (long long)j * su + (long long)v * sview] * pw[j];
+            if (j < nu && v < nview) {
+                x = prj[off + (long long)j * su + (long long)v * sview] * pw[j];
+                if (sw) x *= sw[(long long)j * nview + v];
+            }
             Xs[jj][vv] = x;
         }
         if (tid < 96) {
@@ -228,6 +234,8 @@ __global__ void __launch_bounds__(256) filter_kernel(float* __restrict__ out, co
             int v = v0 + tv * 4 + a, i = i0 + to * 4 + c;
             if (v < nview && i < nu) out[off + (long long)i * su + (long long)v * sview] = acc[a][c] * scale;
         }
+    __syncthreads();   // the next plane refills Xs / Hs
+    }
 }
 
 // FFT filter: the same product as filter_kernel as a circular convolution of
@@ -295,13 +303,15 @@ __device__ __forceinline__ void fft_pass(float2* zs, const float2* tws, int Np, 
 
 __global__ void __launch_bounds__(kFftThreads, 2) filter_fft_kernel(float* __restrict__ out, const float* __restrict__ prj,
                                                          const float2* __restrict__ H, const float2* __restrict__ tw,
-                                                         const float* __restrict__ pw, int nu, int nview, int nv,
-                                                         int nc, int logN, int S, float scale) {
+                                                         const float* __restrict__ pw, const float* __restrict__ sw,
+                                                         int nu, int nview, int nv, int nc, int nplane_total, int logN,
+                                                         int S, float scale) {
     extern __shared__ float2 zs[];   // S signals, stride N + 1 (one pad entry against bank conflicts), then the twiddles
     const int N = 1 << logN, Np = N + 1, halfN = N >> 1;
     float2* tws = zs + S * Np;
     for (int q = threadIdx.x; q < halfN; q += blockDim.x) tws[q] = __ldg(tw + q);
-    const int plane = blockIdx.y;
+    const int nplanes = nplane_total;
+    for (int plane = blockIdx.y; plane < nplanes; plane += gridDim.y) {
     const int b = plane / (nv * nc);
     const int rem = plane - b * nv * nc;
     const long long off = (long long)b * nu * nview * nv * nc + rem;
@@ -317,6 +327,11 @@ __global__ void __launch_bounds__(kFftThreads, 2) filter_fft_kernel(float* __res
             const float* src = prj + off + (long long)n * su;
             if (va < nview) a = src[(long long)va * sview] * w;
             if (va + 1 < nview) c = src[(long long)(va + 1) * sview] * w;
+            if (sw) {   // short-scan weights [nu][nview]
+                const float* wr = sw + (long long)n * nview;
+                if (va < nview) a *= wr[va];
+                if (va + 1 < nview) c *= wr[va + 1];
+            }
         }
         zs[p * Np + (int)(__brev((unsigned)n) >> (32 - logN))] = make_float2(a, c);
     }
@@ -361,10 +376,13 @@ __global__ void __launch_bounds__(kFftThreads, 2) filter_fft_kernel(float* __res
         if (va < nview) dst[(long long)va * sview] = r.x * scale;
         if (va + 1 < nview) dst[(long long)(va + 1) * sview] = r.y * scale;
     }
+    __syncthreads();   // the next plane reuses the signal buffers
+    }
 }
 
 int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int nview, int nv, float da,
-                  float off_a, float dsd, float dso, int typeFilter, int fan, cudaStream_t st) {
+                  float off_a, float dsd, float dso, int typeFilter, int fan, cudaStream_t st,
+                  const float* d_sw = nullptr) {
     (void)dsd;
     if (nb <= 0 || nc <= 0 || nu <= 0 || nview <= 0 || nv <= 0 || !(da > 0))
         return set_error(RN_ERR_ARG, "filter: sizes and pitch must be positive");
@@ -373,20 +391,26 @@ int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int 
     RN_TRY(get_filter(nu, da, off_a, typeFilter, fan, st, fv));
     // scale of cFilterFan::Filter (Filter.cu:294-302) without the FFT length factor
     double scale = fan ? kRefPi / nview * da / dso : kRefPi / nview * da;
-    if (fv.logN > 0 && (long long)nb * nv * nc <= 65535) {
+    // planes (batch, detector row, channel) beyond the 65,535 grid rows are
+    // taken by the kernels' plane loops
+    const long long nplanes = (long long)nb * nv * nc;
+    if (nplanes > INT_MAX) return set_error(RN_ERR_ARG, "filter: too many sinogram planes");
+    const unsigned grid_planes = (unsigned)std::min<long long>(nplanes, 65535);
+    if (fv.logN > 0) {
         // S signals (2S views) per CTA: ~64 KB of shared memory at N = 2048
         const int N = 1 << fv.logN;
         const int S = std::max(1, std::min(16, 8192 / N));
         const size_t smem = sizeof(float2) * ((size_t)S * (N + 1) + N / 2);
         RN_CUDA_TRY(cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        dim3 grid((unsigned)((nview + 2 * S - 1) / (2 * S)), (unsigned)(nb * nv * nc));
-        filter_fft_kernel<<<grid, kFftThreads, smem, st>>>(d_out, d_prj, fv.d_H, fv.d_tw, fv.d_pw, nu, nview, nv, nc, fv.logN,
-                                                   S, (float)scale);
+        dim3 grid((unsigned)((nview + 2 * S - 1) / (2 * S)), grid_planes);
+        filter_fft_kernel<<<grid, kFftThreads, smem, st>>>(d_out, d_prj, fv.d_H, fv.d_tw, fv.d_pw, d_sw, nu, nview, nv,
+                                                           nc, (int)nplanes, fv.logN, S, (float)scale);
         RN_CUDA_TRY(cudaGetLastError());
         return RN_OK;
     }
-    dim3 grid((nview + 63) / 64, (nu + 63) / 64, nb * nv * nc);
-    filter_kernel<<<grid, 256, 0, st>>>(d_out, d_prj, fv.d_h, fv.d_pw, nu, nview, nv, nc, (float)scale);
+    dim3 grid((nview + 63) / 64, (nu + 63) / 64, grid_planes);
+    filter_kernel<<<grid, 256, 0, st>>>(d_out, d_prj, fv.d_h, fv.d_pw, d_sw, nu, nview, nv, nc, (int)nplanes,
+                                        (float)scale);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
@@ -711,6 +735,15 @@ int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int
     if (!d_out || !d_prj) return set_error(RN_ERR_ARG, "null argument");
     return filter_device(d_out, d_prj, nBatches, nChannels, nu, nview, nv, da, off_a, dsd, dso, typeFilter, fan,
                          (cudaStream_t)stream);
+}
+
+int rn_filter_weighted(float* d_out, const float* d_prj, const float* d_w, int nBatches, int nChannels, int nu,
+                       int nview, int nv, float da, float off_a, float dsd, float dso, int typeFilter, int fan,
+                       void* stream) {
+    clear_error();
+    if (!d_out || !d_prj || !d_w) return set_error(RN_ERR_ARG, "null argument");
+    return filter_device(d_out, d_prj, nBatches, nChannels, nu, nview, nv, da, off_a, dsd, dso, typeFilter, fan,
+                         (cudaStream_t)stream, d_w);
 }
 
 static void host_filter(float* out, const float* prj, int nb, int nc, int nu, int nview, int nv, float da,

@@ -6,7 +6,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .torch_ops import FanGeometry
+from .geometry import FanGeometry
 
 MU_WATER = 0.019          # 1/mm
 HU = MU_WATER / 1000.0    # one Hounsfield unit in 1/mm

@@ -389,44 +389,28 @@ class ReconNet:
         return grad, norm, tv
 
 
+def _shortscan(reconNet, kind, sigma=30.0, theta=10 * np.pi / 180, riess_mask=0):
+    ang = np.ascontiguousarray(np.asarray(reconNet.angles, np.float32).ravel())
+    nu, nview = int(reconNet.nu), int(ang.size)
+    w = np.zeros((nu, nview), np.float32)
+    N.check(N.lib.rn_fan_shortscan_weights_host(_fptr(w), _fptr(ang), nu, nview, float(reconNet.da),
+                                                float(reconNet.off_a), int(kind), float(sigma), float(theta),
+                                                int(riess_mask)))
+    return w[None, :, :, None]
+
+
 def ParkerWeighting(reconNet):
-    """Parker short-scan weights (python/ReconNet_no_tf.py:640-659), shape [1, nu, nview, 1]."""
-    gamma = (reconNet.angles[-1] - np.pi) / 2
-    alphas = ((np.arange(reconNet.nu) - (reconNet.nu - 1) / 2) - reconNet.off_a) * reconNet.da
-    weights = []
-    for beta in reconNet.angles:
-        res1 = (np.sin(np.pi / 4 * beta / (gamma - alphas))) ** 2
-        res2 = (np.sin(np.pi / 4 * (np.pi + 2 * gamma - beta) / (gamma + alphas))) ** 2
-        i1 = np.where(beta < 2 * gamma - 2 * alphas)[0]
-        i2 = np.where(beta <= np.pi - 2 * alphas)[0]
-        w = res2
-        w[i2] = 1
-        w[i1] = res1[i1]
-        weights.append(w)
-    return np.transpose(np.array(weights))[np.newaxis, ..., np.newaxis]
+    """Parker short-scan weights for reconNet.angles over [0, pi + 2 gamma],
+    shape [1, nu, nview, 1] -- the reference's ParkerWeighting
+    (python/ReconNet_no_tf.py:640-659), computed on the GPU by
+    rn_fan_shortscan_weights_host (kernel in csrc/shortscan.cu)."""
+    return _shortscan(reconNet, N.RN_WEIGHT_PARKER)
 
 
-def RiessWeighting(reconNet, sigma=30, theta=10 * np.pi / 180):
-    """Riess short-scan weights (python/ReconNet_no_tf.py:665-693), shape [1, nu, nview, 1]."""
-    import scipy.ndimage
-
-    gamma = (reconNet.angles[-1] - np.pi) / 2
-    alphas = ((np.arange(reconNet.nu) - (reconNet.nu - 1) / 2) - reconNet.off_a) * reconNet.da
-    weights = []
-    for beta in reconNet.angles:
-        w = np.ones([reconNet.nu], np.float32)
-        res1 = (np.sin(np.pi / 4 * beta / (gamma - alphas))) ** 2
-        res2 = (np.sin(np.pi / 4 * (np.pi + 2 * gamma - beta) / (gamma + alphas))) ** 2
-        i1 = np.where(beta < 2 * gamma - 2 * alphas)[0]
-        i2 = np.where(beta < -2 * gamma + 2 * alphas)[0]
-        i3 = np.where(beta > np.pi - 2 * alphas)[0]
-        i4 = np.where(beta > np.pi + 2 * gamma + 2 * alphas)[0]
-        w[i4] = 2 - res2[i4]
-        w[i3] = res2[i3]
-        w[i2] = 2 - res1[i2]
-        w[i1] = res1[i1]
-        ws = scipy.ndimage.gaussian_filter1d(w, sigma, mode="nearest")
-        ind = np.where(np.all((beta > theta, beta < np.pi + 2 * gamma - theta)))
-        ws[ind] = w[ind]
-        weights.append(ws)
-    return np.transpose(np.array(weights))[np.newaxis, ..., np.newaxis]
+def RiessWeighting(reconNet, sigma=30, theta=10 * np.pi / 180, whole_view_exception=False):
+    """Riess short-scan weights, shape [1, nu, nview, 1] -- the reference's
+    RiessWeighting (python/ReconNet_no_tf.py:665-693) on the GPU.  By default
+    the views with theta < beta < pi + 2 gamma - theta keep only channel 0
+    unsmoothed, which is what the reference's np.where(np.all(...)) selects;
+    whole_view_exception=True keeps those whole views unsmoothed instead."""
+    return _shortscan(reconNet, N.RN_WEIGHT_RIESS, sigma, theta, 1 if whole_view_exception else 0)

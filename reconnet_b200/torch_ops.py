@@ -17,42 +17,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-
-
-@dataclass
-class FanGeometry:
-    """Fan-beam geometry; field meaning follows Projector (Projector.h:10-37).
-
-    ``da`` is the angular detector pitch in radians (du_mm / dsd)."""
-    nx: int = 512
-    ny: int = 512
-    nz: int = 1
-    dx: float = 1.0
-    dy: float = 1.0
-    dz: float = 1.0
-    nu: int = 736
-    nv: int = 1
-    da: float = 1.2858 / 1085.6
-    dv: float = 1.0
-    off_a: float = 0.0
-    off_v: float = 0.0
-    dsd: float = 1085.6
-    dso: float = 595.0
-    cx: float = 0.0
-    cy: float = 0.0
-    cz: float = 0.0
-
-    def native(self, nbatches: int, nchannels: int, nview: int) -> N.RnFanGeom:
-        g = N.RnFanGeom()
-        g.nBatches, g.nChannels = int(nbatches), int(nchannels)
-        g.nx, g.ny, g.nz = int(self.nx), int(self.ny), int(self.nz)
-        g.dx, g.dy, g.dz = float(self.dx), float(self.dy), float(self.dz)
-        g.cx, g.cy, g.cz = float(self.cx), float(self.cy), float(self.cz)
-        g.nu, g.nview, g.nv = int(self.nu), int(nview), int(self.nv)
-        g.du, g.dv = float(self.da), float(self.dv)
-        g.off_u, g.off_v = float(self.off_a), float(self.off_v)
-        g.dsd, g.dso = float(self.dsd), float(self.dso)
-        return g
+from .geometry import FanGeometry  # noqa: F401  (re-exported)
 
 
 def _stream_ptr(device: torch.device) -> int:
@@ -425,16 +390,45 @@ class ConePlan:
         return int(N.lib.rn_cone_plan_launches(self._plan))
 
 
+def shortscan_weights(angles: torch.Tensor, geom: FanGeometry, kind: str = "parker", sigma: float = 30.0,
+                      theta: float = 10 * np.pi / 180, whole_view_exception: bool = False) -> torch.Tensor:
+    """Short-scan redundancy weights [nu, nview] on the device for the view
+    angles of a float32 CUDA tensor (rn_fan_shortscan_weights): Parker or
+    Riess, as the reference's ParkerWeighting / RiessWeighting
+    (python/ReconNet_no_tf.py:640-693)."""
+    ang = angles.detach().to(torch.float32).contiguous().reshape(-1)
+    if not ang.is_cuda:
+        raise ValueError("angles must be a CUDA tensor")
+    w = torch.empty((geom.nu, ang.numel()), dtype=torch.float32, device=ang.device)
+    k = {"parker": N.RN_WEIGHT_PARKER, "riess": N.RN_WEIGHT_RIESS}[kind]
+    N.check(N.lib.rn_fan_shortscan_weights(_dev_ptr(w), _dev_ptr(ang), int(geom.nu), int(ang.numel()),
+                                           float(geom.da), float(geom.off_a), k, float(sigma), float(theta),
+                                           int(bool(whole_view_exception)), _stream_ptr(ang.device)))
+    return w
+
+
 def fbp(sino: torch.Tensor, plan: "FanPlan", geom: FanGeometry, type_filter: int = 0,
         weights: Optional[torch.Tensor] = None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Fan-beam FBP on the device: optional short-scan weights (Parker /
-    Riess, multiplied into the sinogram), the ramp filter (cFilterFan), then
-    the pixel-driven backprojection with the dso^2 / L^2 weight
-    (cPixelDrivenFan) -- the reference's FBP chain (ReconNet_no_tf.py:84-131,
-    640-693).  sino is [B, nu, nview, nv, C] in the plan's layout."""
-    if weights is not None:
-        sino = sino * weights
-    return plan.backproject(filter_sino(sino, geom, type_filter), N.RN_TYPE_PIXEL, out=out)
+    Riess, [nu, nview] from `shortscan_weights`, or any shape holding nu x
+    nview values), multiplied into the sinogram inside the ramp filter's load
+    (rn_filter_weighted), then the pixel-driven backprojection with the
+    dso^2 / L^2 weight (cPixelDrivenFan) -- the reference's FBP chain
+    (ReconNet_no_tf.py:84-131, 640-693).  sino is [B, nu, nview, nv, C] in the
+    plan's layout."""
+    if weights is None:
+        filt = filter_sino(sino, geom, type_filter)
+    else:
+        B, nu, nview, nv, C = sino.shape
+        w = weights.to(device=sino.device, dtype=torch.float32).contiguous()
+        if w.numel() != nu * nview:
+            raise ValueError(f"weights must hold nu x nview = {nu} x {nview} values, got shape {tuple(w.shape)}")
+        sino = sino.contiguous()
+        filt = torch.empty_like(sino)
+        N.check(N.lib.rn_filter_weighted(_dev_ptr(filt), _dev_ptr(sino), _dev_ptr(w), B, C, nu, nview, nv,
+                                          float(geom.da), float(geom.off_a), float(geom.dsd), float(geom.dso),
+                                          int(type_filter), 1, _stream_ptr(sino.device)))
+    return plan.backproject(filt, N.RN_TYPE_PIXEL, out=out)
 
 
 def tv_iso_sqs(img: torch.Tensor, ndim: int, eps: float = 1e-8, want_var: bool = True):

@@ -173,6 +173,38 @@ def test_filter_matches_oracle(tf, rng):
     assert rel_l2(got_p, O.filter_sino(s, g, tf, fan=False)) <= TOL
 
 
+# Channel counts whose transform lengths N = 2^logN >= 2nu - 1 cover every
+# residue of logN mod 3 (the FFT fuses radix-2 levels three at a time, so the
+# remainder picks the radix-4 / radix-2 passes and which pass carries the
+# spectrum product) and the largest lengths (N = 8192 and 16384, one signal
+# per CTA).  Odd view counts leave the last CTA partly filled.
+@pytest.mark.parametrize("nu", [40, 150, 300, 1500, 3000, 5000, 8000])
+def test_filter_fft_lengths_match_oracle(nu, rng):
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200.torch_ops import filter_sino
+    g = small_fan(nu=nu, da=0.9 / nu, off_a=0.3)
+    nview = 7 if nu >= 3000 else 13
+    s = rng.random((1, nu, nview, 1, 1)).astype(np.float32)
+    for tf in (0, 2):
+        got = filter_sino(torch.from_numpy(s).cuda(), to_geometry(g), tf).cpu().numpy()
+        assert rel_l2(got, O.filter_sino(s, g, tf)) <= TOL, (nu, tf)
+
+
+def test_filter_more_planes_than_grid_rows(rng):
+    """More (batch, row, channel) planes than one grid dimension holds
+    (65,535): the kernels loop over the planes."""
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200.torch_ops import filter_sino
+    g = small_fan(nu=16, da=0.01, nv=65600)
+    s = rng.random((1, 16, 3, 65600, 1)).astype(np.float32)
+    got = filter_sino(torch.from_numpy(s).cuda(), to_geometry(g), 0).cpu().numpy()
+    ref = O.filter_sino(s, g, 0)
+    assert rel_l2(got, ref) <= TOL
+    assert rel_l2(got[..., -100:, :], ref[..., -100:, :]) <= TOL     # the planes past the first grid pass
+
+
 def test_filter_host_api_full_size(rng):
     from oracle import oracle as O
     from reconnet_b200 import phantom as P

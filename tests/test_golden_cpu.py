@@ -187,3 +187,26 @@ def test_cone_vs_reference(path):
     bp = O.cone_bp(d["prj_in"], *geo, g, (n["nx"], n["ny"], n["nz"]))
     assert rel_l2(fp, d["fp"]) < 1e-5      # measured 1.1e-6 - 1.3e-6
     assert rel_l2(bp, d["bp"]) < 1e-5      # measured 1.8e-6 - 2.7e-6
+
+
+SHORTSCAN = os.path.join(GOLDEN, "ref_shortscan.npz")
+
+
+@pytest.mark.parametrize("case", ["c736", "c736_off", "c96", "c200_wide"])
+def test_shortscan_weights_vs_reference(case):
+    """The oracle's Parker / Riess weights against the reference's own
+    ParkerWeighting / RiessWeighting run on the same angles
+    (tests/golden/make_shortscan_golden.py); the fixtures are float32, so the
+    bound is their rounding."""
+    d = np.load(SHORTSCAN)
+    nu, da, off = d[f"{case}_geom"]
+    ang = d[f"{case}_angles"]
+    nu = int(nu)
+    assert np.abs(O.shortscan_weights(ang, nu, da, off, "parker") - d[f"{case}_parker"]).max() < 1.2e-7
+    riess = O.shortscan_weights(ang, nu, da, off, "riess")
+    assert np.abs(riess - d[f"{case}_riess"]).max() < 1.2e-7
+    assert np.abs(O.shortscan_weights(ang, nu, da, off, "riess", 12, 0.1) - d[f"{case}_riess_s12"]).max() < 1.2e-7
+    # the reference keeps only channel 0 of the middle views unsmoothed; the
+    # whole-view reading of the method gives different weights
+    whole = O.shortscan_weights(ang, nu, da, off, "riess", mask_all=True)
+    assert np.abs(whole - d[f"{case}_riess"]).max() > 0.1

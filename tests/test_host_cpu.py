@@ -27,16 +27,17 @@ def test_reconnet_defaults_and_from_file(tmp_path):
     assert len(rn.angles) == 1152
 
 
-def test_parker_weights_shape_and_range():
-    from reconnet_b200.reconnet import ParkerWeighting, ReconNet
-    rn = ReconNet()
-    rn.nu = 64
-    rn.da = 0.01
-    rn.rotview = 300
-    rn.angles = list(np.linspace(0, np.pi + 2 * 0.4, 300))
-    w = ParkerWeighting(rn)
-    assert w.shape == (1, 64, 300, 1)
-    assert np.all(w >= 0) and np.all(w <= 1 + 1e-6)
+def test_shortscan_weights_oracle_shape_and_range():
+    """The oracle's Parker weights lie in [0, 1] and sum, over a ray and its
+    conjugate, to one; Riess weights lie in [0, 2]."""
+    from oracle import oracle as O
+    nu, da = 64, 0.01
+    ang = np.linspace(0, np.pi + 2 * 0.4, 300).astype(np.float32)
+    w = O.shortscan_weights(ang, nu, da, 0.0, "parker")
+    assert w.shape == (64, 300)
+    assert np.all(w >= 0) and np.all(w <= 1 + 1e-12)
+    r = O.shortscan_weights(ang, nu, da, 0.0, "riess")
+    assert np.all(r >= -1e-12) and np.all(r <= 2 + 1e-12)
 
 
 def test_interleaved_subsets_cover_views_once():
