@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-ossqs", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis, cone and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
-    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs"],
+    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs", "cyl"],
                     help="run only this extra measurement (one GPU) and print its JSON object")
     return ap.parse_args()
 
@@ -489,6 +489,66 @@ def tomo_run(dev, cpu_sample=True):
     return out
 
 
+def cyl_run(dev, cpu_sample=True):
+    """The cone-beam workload: the cylindrical-detector DD pair (csrc/cyl.cu)
+    on 512x512x128 voxels of 0.8x0.8x1.0 mm, 736 x 64 cells (1.2858 mm x
+    1.0 mm at the detector), 984 views over 360 degrees, source at 595 mm and
+    the detector at 1085.6 mm; random ellipsoids of 0-0.04/mm.  Updates:
+    FP = views x cells x planes (984 x 736 x 64 x 512), BP = voxels x views.
+    The bound is not HBM: the FP streams each voxel column's z-run through
+    warp scans and the BP reads per-view row tables, both from L2; the
+    compulsory-bytes fraction is reported beside the time."""
+    import torch
+
+    from reconnet_b200.phantom import ellipsoid_phantom
+    from reconnet_b200.torch_ops import CylGeometry, CylPlan
+    g = CylGeometry()
+    nview = 984
+    ang = (np.arange(nview) * 2 * np.pi / nview).astype(np.float32)
+    plan = CylPlan(g, ang, device=dev)
+    vol = ellipsoid_phantom(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, np.random.default_rng(21), device=dev)[None].contiguous()
+    prj = torch.empty(plan.prj_shape, device=dev)
+    back = torch.empty(plan.vol_shape, device=dev)
+    peak, kind = measured_peaks()
+    vol_b, prj_b = vol.numel() * 4, prj.numel() * 4
+    tab_b = nview * g.nu * (g.nv + 1) * 8
+    out = {"workload": "cylindrical-detector cone-beam DD pair: 512x512x128 @0.8x0.8x1.0 mm, 736x64 cells "
+                       "(1.2858 x 1.0 mm at the detector), 984 views over 360 deg, dso 595 / dsd 1085.6 mm",
+           "data": "synthetic: 10 seeded random ellipsoids, 0-0.04/mm"}
+    fp_upd = nview * g.nu * g.nv * g.ny       # planes per ray: ny (X-class) or nx (Y-class), equal here
+    bp_upd = g.nx * g.ny * g.nz * nview
+    for name, f, upd, hbm in (("fp", lambda: plan.project(vol, out=prj), fp_upd, vol_b + prj_b),
+                              ("bp", lambda: plan.backproject(prj, out=back), bp_upd, prj_b + 2 * tab_b + vol_b)):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        ach = hbm / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "updates": upd, "gupd_s": upd / ms / 1e6,
+                     "roofline": {"bound": "hbm (compulsory bytes)", "achieved": ach, "peak": peak, "unit": "GB/s",
+                                  "frac": ach / peak, "peak_kind": kind, "bytes_per_launch": hbm}}
+    y = torch.rand(plan.prj_shape, device=dev)
+    aty = plan.backproject(y)
+    ax = plan.project(vol)
+    lhs, rhs = float((ax.double() * y.double()).sum()), float((vol.double() * aty.double()).sum())
+    out["adjoint_rel"] = abs(lhs - rhs) / abs(lhs)
+    if cpu_sample:
+        from oracle import oracle as O
+        O.set_threads(os.cpu_count() or 1)
+        v = vol.cpu().numpy()
+        t0 = time.perf_counter()
+        O.cyl_fp(v, ang[:1], g)
+        t1 = time.perf_counter()
+        out["cpu_baseline"] = {"fp_gupd_s": g.nu * g.nv * g.ny / (t1 - t0) / 1e9, "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": "1 of the 984 views, FP64 OpenMP oracle (no reference CPU path)"}
+    return out
+
+
 def siddon_run(plan, x, p, b, geom, angles, counts, cpu_sample=True):
     """Siddon fan pair (Siddon.cu, the reference OS-SQS projector) on the
     bench's slice batch: FP of every view of every slice, then the Siddon
@@ -837,6 +897,7 @@ def run_b200(args):
         extras["tomo"] = tomo_run(dev, cpu_sample=world == 1)
         extras["siddon_cone"] = cone_run(dev, cpu_sample=world == 1)
         extras["filter"] = filter_run(dev, cpu_sample=world == 1)
+        extras["cone_cyl"] = cyl_run(dev, cpu_sample=world == 1)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -885,6 +946,8 @@ def run_extra(args):
         out = tomo_run(dev, cpu_sample=cpu)
     elif args.extra == "cone":
         out = cone_run(dev, cpu_sample=cpu)
+    elif args.extra == "cyl":
+        out = cyl_run(dev, cpu_sample=cpu)
     else:
         out = filter_run(dev, cpu_sample=cpu)
     print(json.dumps({args.extra: out}), flush=True)

@@ -387,6 +387,62 @@ int rn_tomo_backproject(float* d_img, const float* d_prj, const float* d_detCent
                         float cy, float cz, int nu, int nview, int nv, float du, float dv, float off_u, float off_v,
                         int weightAllViews, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Cylindrical-detector cone-beam DD pair on a circular orbit (no counterpart
+ * in the reference: its DistanceDriven3D.cu:139-227 / 519-559 is a flat,
+ * axis-aligned tomosynthesis pair with z as the main axis; this generalises
+ * that rectangle-footprint DD and the fan geometry of DistanceDriven.cu:64-196
+ * to a 360-degree orbit).  Source (dso sin t, -dso cos t, 0); detector a
+ * cylinder of radius dsd about the source, cell (u, v) at fan angle
+ * a_u = (-(u - (nu-1)/2) - off_a) da and height v_c = (v - (nv-1)/2 + off_v) dv
+ * at the detector; volume of nx x ny x nz voxels (dx, dy, dz mm) centred at
+ * (cx, cy, cz).  Volumes are [nBatches][nx][ny][nz], projections
+ * [nBatches][nu][nview][nv] (the reference's layouts without channels).  The
+ * backprojection is the exact transpose and overwrites its output.  The plan
+ * owns the view tables and the backprojection's row tables
+ * (nBatches * nview * nu * (nv + 1) float2). */
+typedef struct RnCylGeom {
+    int nBatches;
+    int nx, ny, nz;
+    float dx, dy, dz, cx, cy, cz;
+    int nu, nview, nv;
+    float da, dv, off_a, off_v, dsd, dso;
+} RnCylGeom;
+typedef struct rn_cyl_plan rn_cyl_plan;
+int rn_cyl_plan_create(rn_cyl_plan** plan, const RnCylGeom* geom, const float* host_deg, void* stream);
+int rn_cyl_plan_destroy(rn_cyl_plan* plan);
+int rn_cyl_project(rn_cyl_plan* plan, float* d_prj, const float* d_vol, void* stream);
+int rn_cyl_backproject(rn_cyl_plan* plan, float* d_vol, const float* d_prj, void* stream);
+long long rn_cyl_plan_launches(const rn_cyl_plan* plan);
+
+/* ---------------------------------------------------------------------------
+ * BF16 3x3 convolutions of the learned prior (no counterpart in the
+ * reference, whose learned path is TensorFlow's: python/ReconNet.py:773-830).
+ * tcgen05 tensor-core kernels with FP32 accumulation; activations are bf16
+ * "blocked" [N][C/8][H][W][8], 16-byte aligned.  d_wpack is the weight
+ * operand image: chunk kc of 8 input channels x NPAD output rows x 8 bf16
+ * (NPAD = 32, or 16 for one output channel), kc = tap * (cin/8) + ci/8 for
+ * cin = 32, kc = tap for cin = 8 (plus a zero tenth chunk).
+ * mode 0: d_out blocked bf16 = relu(conv + bias), cout 32;
+ * mode 1: d_out fp32 [N][H][W] = conv + bias + d_aux (fp32 residual), cout 1;
+ * mode 2: d_out blocked bf16 = conv * (d_aux > 0), d_aux the blocked
+ *         activation (the input gradient through a ReLU), cout 32;
+ * mode 3: d_out fp32 [N][cout][H][W] = conv (+ bias if given).
+ * A device wait that runs out records RN_ERR_TIMEOUT in *d_err. */
+int rn_conv3x3(void* d_out, const void* d_in, const void* d_wpack, const float* d_bias, const void* d_aux, int N,
+               int H, int W, int cin, int cout, int mode, int* d_err, void* stream);
+/* Weight gradient: d_dw [32][ncols] fp32, ncols = rn_conv3x3_wgrad_cols(cin):
+ * column tap * 32 + ci (cin 32) or (tap / 2) * 16 + (tap % 2) * 8 + ci (cin 8),
+ * then 16 columns of the bias gradient sum_p dY[p][co]; rows >= cout are 0.
+ * d_partial: scratch of at least (number of SMs) * 32 * ncols floats. */
+int rn_conv3x3_wgrad_cols(int cin);
+int rn_conv3x3_wgrad(float* d_dw, float* d_partial, size_t partial_bytes, const void* d_x, const void* d_dy, int N,
+                     int H, int W, int cin, int cout, int* d_err, void* stream);
+/* fp32 [N][H][W] -> blocked bf16 with 8 channels: channel 0 = (img - sub) * scale
+ * (d_sub may be NULL), channels 1..7 zero. */
+int rn_conv_pack_image(void* d_out, const float* d_img, const float* d_sub, float scale, int N, int H, int W,
+                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif

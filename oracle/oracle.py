@@ -28,6 +28,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 
 _FAN = [_i, _i, _i, _i, _i, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f, _f, _f]
 _TOMO = [_i, _i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f]
+_CYL = [_i, _i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _i, _f, _f, _f, _f, _f, _f]
 
 
 def build(force: bool = False) -> str:
@@ -65,6 +66,9 @@ def lib():
         L.oracle_cone_bp_f64.argtypes = [_dp, _fp, _fp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_fp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO + [_i]
+        L.oracle_cyl_fp_f64.argtypes = [_dp, _fp, _fp] + _CYL
+        L.oracle_cyl_fp_f32.argtypes = [_fp, _fp, _fp] + _CYL
+        L.oracle_cyl_bp_f64.argtypes = [_dp, _fp, _fp] + _CYL
         _lib = L
     return _lib
 
@@ -356,3 +360,80 @@ def shortscan_weights(angles, nu, da, off_a, kind="parker", sigma=30.0, theta=10
     if not mask_all:
         keep[1:, :] = False
     return np.where(keep, w, smooth)
+
+
+def _cyl_args(g, nb, vol_shape, nview):
+    nx, ny, nz = vol_shape
+    return (nb, nx, ny, nz, g.dx, g.dy, g.dz, g.cx, g.cy, g.cz, g.nu, nview, g.nv, g.da, g.dv, g.off_a, g.off_v,
+            g.dsd, g.dso)
+
+
+def cyl_fp(vol, angles, g, dtype=np.float64):
+    """Cylindrical-detector cone-beam DD forward projection (definition in
+    oracle.cpp, section "Cylindrical-detector cone-beam DD pair"): vol is
+    [B, nx, ny, nz], returns [B, nu, nview, nv]."""
+    vol = _f32(vol)
+    ang = _f32(angles)
+    B, nx, ny, nz = vol.shape
+    out = np.zeros((B, g.nu, ang.size, g.nv), dtype)
+    fn = lib().oracle_cyl_fp_f64 if dtype == np.float64 else lib().oracle_cyl_fp_f32
+    ct = ctypes.c_double if dtype == np.float64 else _f
+    fn(_ptr(out, ct), _ptr(vol, _f), _ptr(ang, _f), *_cyl_args(g, B, (nx, ny, nz), ang.size))
+    return out
+
+
+def cyl_bp(prj, angles, g, vol_shape):
+    """Exact transpose of cyl_fp: prj [B, nu, nview, nv] -> [B, nx, ny, nz]."""
+    prj = _f32(prj)
+    ang = _f32(angles)
+    B = prj.shape[0]
+    out = np.zeros((B,) + tuple(vol_shape), np.float64)
+    lib().oracle_cyl_bp_f64(_ptr(out, ctypes.c_double), _ptr(prj, _f), _ptr(ang, _f),
+                            *_cyl_args(g, B, vol_shape, ang.size))
+    return out
+
+
+# ---- the learned prior's 3x3 convolutions (FP64 numpy) -------------------------
+# Tap (dy, dx) of output pixel (h, w) reads input pixel (h + dy - 1, w + dx - 1),
+# zero outside the image; weights are [cout, 3, 3, cin].
+
+def bf16_round(a):
+    """Round float32 values to bfloat16 (nearest even), returned as float64."""
+    a = np.ascontiguousarray(a, np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def conv3x3(x, w, b=None):
+    """x [N, cin, H, W], w [cout, 3, 3, cin] -> [N, cout, H, W] in FP64."""
+    x = np.asarray(x, np.float64)
+    w = np.asarray(w, np.float64)
+    N, C, H, W = x.shape
+    xp = np.pad(x, ((0, 0), (0, 0), (1, 1), (1, 1)))
+    y = np.zeros((N, w.shape[0], H, W))
+    for dy in range(3):
+        for dx in range(3):
+            y += np.einsum("nchw,oc->nohw", xp[:, :, dy:dy + H, dx:dx + W], w[:, dy, dx, :], optimize=True)
+    if b is not None:
+        y += np.asarray(b, np.float64)[None, :, None, None]
+    return y
+
+
+def conv3x3_dgrad(dy, w):
+    """Gradient with respect to the input: dy [N, cout, H, W] -> [N, cin, H, W]."""
+    w = np.asarray(w, np.float64)
+    return conv3x3(dy, w[:, ::-1, ::-1, :].transpose(3, 1, 2, 0))
+
+
+def conv3x3_wgrad(x, dy):
+    """Gradients with respect to the weights [cout, 3, 3, cin] and bias [cout]."""
+    x = np.asarray(x, np.float64)
+    dy = np.asarray(dy, np.float64)
+    N, C, H, W = x.shape
+    xp = np.pad(x, ((0, 0), (0, 0), (1, 1), (1, 1)))
+    dw = np.zeros((dy.shape[1], 3, 3, C))
+    for a in range(3):
+        for c in range(3):
+            dw[:, a, c, :] = np.einsum("nohw,nchw->oc", dy, xp[:, :, a:a + H, c:c + W], optimize=True)
+    return dw, dy.sum(axis=(0, 2, 3))

@@ -47,6 +47,14 @@ class RnConeGeom(ctypes.Structure):
                 ("du", _f), ("dv", _f), ("off_u", _f), ("off_v", _f)]
 
 
+class RnCylGeom(ctypes.Structure):
+    """Mirror of ``RnCylGeom`` (cylindrical-detector cone-beam DD, circular orbit)."""
+    _fields_ = [("nBatches", _i), ("nx", _i), ("ny", _i), ("nz", _i),
+                ("dx", _f), ("dy", _f), ("dz", _f), ("cx", _f), ("cy", _f), ("cz", _f),
+                ("nu", _i), ("nview", _i), ("nv", _i),
+                ("da", _f), ("dv", _f), ("off_a", _f), ("off_v", _f), ("dsd", _f), ("dso", _f)]
+
+
 class ReconNetError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"reconnet_b200 error {code}: {msg}")
@@ -110,6 +118,15 @@ SIGNATURES = {
                                ctypes.POINTER(ctypes.c_size_t)]),
     "rn_tomo_project": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),
     "rn_tomo_backproject": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_i, _vp]),
+    "rn_cyl_plan_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnCylGeom), _fp, _vp]),
+    "rn_cyl_plan_destroy": (_i, [_vp]),
+    "rn_cyl_project": (_i, [_vp, _vp, _vp, _vp]),
+    "rn_cyl_backproject": (_i, [_vp, _vp, _vp, _vp]),
+    "rn_cyl_plan_launches": (ctypes.c_longlong, [_vp]),
+    "rn_conv3x3": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp]),
+    "rn_conv3x3_wgrad_cols": (_i, [_i]),
+    "rn_conv3x3_wgrad": (_i, [_vp, _vp, ctypes.c_size_t, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
+    "rn_conv_pack_image": (_i, [_vp, _vp, _vp, _f, _i, _i, _i, _vp]),
 }
 
 

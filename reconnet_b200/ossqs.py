@@ -151,17 +151,28 @@ def tv_terms(x: torch.Tensor, eps: float = 1e-6):
 
 def unrolled_ossqs(x0: torch.Tensor, subset_plans: Sequence[FanPlan], sub_b: Sequence[torch.Tensor],
                    sub_w: Sequence[torch.Tensor], norm_img: torch.Tensor, step_scales: torch.Tensor,
-                   tv_weights: torch.Tensor, checkpoint: bool = True) -> torch.Tensor:
+                   tv_weights: torch.Tensor, checkpoint: bool = True, bp_type: int = N.RN_TYPE_MATCHED,
+                   project=None, backproject=None) -> torch.Tensor:
     """Unrolled OS-SQS in reference layout ([B, nx, ny, 1, 1] images, subset
     sinograms [B, nu, nview_s, 1, 1]); iteration k uses step scale
     step_scales[k] and TV weight tv_weights[k].  Differentiable w.r.t. x0, the
-    measured data and both parameter vectors."""
+    measured data and both parameter vectors.
+
+    bp_type is the backprojection of the update and the gradient of the
+    projection: the matched transpose (exact gradients) or the reference's
+    iterative backprojection (type 0, the reference's own registration,
+    python/ReconNet.py:773-830).  `project(x, m)` / `backproject(r, m)`
+    replace the pair (any autograd functions over subset m)."""
     M = len(subset_plans)
+    if project is None:
+        project = lambda x, m: fan_project(x, subset_plans[m], bp_type)
+    if backproject is None:
+        backproject = lambda r, m: fan_backproject(r, subset_plans[m], bp_type)
 
     def one_iter(x, lam, beta):
         for m in range(M):
-            r = (fan_project(x, subset_plans[m]) - sub_b[m]) * sub_w[m]
-            bp = fan_backproject(r, subset_plans[m])
+            r = (project(x, m) - sub_b[m]) * sub_w[m]
+            bp = backproject(r, m)
             g, n = tv_terms(x[..., 0, 0])
             g, n = g[..., None, None], n[..., None, None]
             x = x - lam * (M * bp + beta * g) / (norm_img + beta * n + 1e-6)

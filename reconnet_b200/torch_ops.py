@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .geometry import FanGeometry  # noqa: F401  (re-exported)
+from .geometry import CylGeometry, FanGeometry  # noqa: F401  (re-exported)
 
 
 def _stream_ptr(device: torch.device) -> int:
@@ -262,37 +262,44 @@ class StreamedFanPair:
 
 
 class FanProjectFn(torch.autograd.Function):
-    """y = A x with dL/dx = A^T dL/dy (A^T = matched backprojection)."""
+    """y = A x with dL/dx = B dL/dy, B the backprojection of type `grad_type`:
+    the matched transpose A^T by default (the exact gradient), or the
+    reference's iterative backprojection (type 0), which is how the
+    reference registers the gradient of its projection op
+    (python/ReconNet.py:773-800)."""
 
     @staticmethod
-    def forward(ctx, img, plan: FanPlan):
+    def forward(ctx, img, plan: FanPlan, grad_type: int = N.RN_TYPE_MATCHED):
         ctx.plan = plan
+        ctx.grad_type = grad_type
         return plan.project(img.contiguous())
 
     @staticmethod
     def backward(ctx, gy):
-        return ctx.plan.backproject(gy.contiguous(), N.RN_TYPE_MATCHED), None
+        return ctx.plan.backproject(gy.contiguous(), ctx.grad_type), None, None
 
 
 class FanBackprojectFn(torch.autograd.Function):
-    """x = A^T y (matched) with dL/dy = A dL/dx."""
+    """x = B y (backprojection of type `bp_type`, matched by default) with
+    dL/dy = A dL/dx (python/ReconNet.py:801-830 registers the projection as
+    the backprojection's gradient)."""
 
     @staticmethod
-    def forward(ctx, sino, plan: FanPlan):
+    def forward(ctx, sino, plan: FanPlan, bp_type: int = N.RN_TYPE_MATCHED):
         ctx.plan = plan
-        return plan.backproject(sino.contiguous(), N.RN_TYPE_MATCHED)
+        return plan.backproject(sino.contiguous(), bp_type)
 
     @staticmethod
     def backward(ctx, gx):
-        return ctx.plan.project(gx.contiguous()), None
+        return ctx.plan.project(gx.contiguous()), None, None
 
 
-def fan_project(img: torch.Tensor, plan: FanPlan) -> torch.Tensor:
-    return FanProjectFn.apply(img, plan)
+def fan_project(img: torch.Tensor, plan: FanPlan, grad_type: int = N.RN_TYPE_MATCHED) -> torch.Tensor:
+    return FanProjectFn.apply(img, plan, grad_type)
 
 
-def fan_backproject(sino: torch.Tensor, plan: FanPlan) -> torch.Tensor:
-    return FanBackprojectFn.apply(sino, plan)
+def fan_backproject(sino: torch.Tensor, plan: FanPlan, bp_type: int = N.RN_TYPE_MATCHED) -> torch.Tensor:
+    return FanBackprojectFn.apply(sino, plan, bp_type)
 
 
 def filter_sino(sino: torch.Tensor, geom: FanGeometry, type_filter: int = 0, fan: bool = True) -> torch.Tensor:
@@ -456,3 +463,49 @@ def tv_sqs(img: torch.Tensor, want_tv: bool = True):
     N.check(N.lib.rn_tv_sqs(_dev_ptr(grad), _dev_ptr(norm), tv.data_ptr() if tv is not None else None,
                             _dev_ptr(img), S, nx, ny, _stream_ptr(img.device)))
     return grad, norm, tv
+
+
+class CylPlan:
+    """Native plan of the cylindrical-detector cone-beam DD pair (rn_cyl_*):
+    volumes [B, nx, ny, nz], projections [B, nu, nview, nv], float32 CUDA
+    tensors; kernels run on the current stream of the plan's device."""
+
+    def __init__(self, geom: CylGeometry, angles, nbatches: int = 1, device=None):
+        self.geom = geom
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.angles = np.ascontiguousarray(np.asarray(angles, np.float32).ravel())
+        self.nbatches = int(nbatches)
+        self._plan = ctypes.c_void_p()
+        g = geom.native(self.nbatches, self.angles.size)
+        with torch.cuda.device(self.device):
+            N.check(N.lib.rn_cyl_plan_create(ctypes.byref(self._plan), ctypes.byref(g),
+                                             self.angles.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                             _stream_ptr(self.device)))
+        self.vol_shape = (self.nbatches, geom.nx, geom.ny, geom.nz)
+        self.prj_shape = (self.nbatches, geom.nu, self.angles.size, geom.nv)
+
+    def __del__(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            N.lib.rn_cyl_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def _check(self, t, shape):
+        if tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_contiguous() or t.device != self.device:
+            raise ValueError(f"expected a contiguous float32 tensor of shape {shape} on {self.device}")
+
+    def project(self, vol: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        self._check(vol, self.vol_shape)
+        out = torch.empty(self.prj_shape, device=self.device) if out is None else out
+        self._check(out, self.prj_shape)
+        N.check(N.lib.rn_cyl_project(self._plan, _dev_ptr(out), _dev_ptr(vol), _stream_ptr(self.device)))
+        return out
+
+    def backproject(self, prj: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        self._check(prj, self.prj_shape)
+        out = torch.empty(self.vol_shape, device=self.device) if out is None else out
+        self._check(out, self.vol_shape)
+        N.check(N.lib.rn_cyl_backproject(self._plan, _dev_ptr(out), _dev_ptr(prj), _stream_ptr(self.device)))
+        return out
+
+    def launches(self) -> int:
+        return int(N.lib.rn_cyl_plan_launches(self._plan))

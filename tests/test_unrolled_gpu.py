@@ -1,0 +1,167 @@
+"""The differentiable unrolled OS-SQS at the size it is specified for: a batch
+of 8 slices of 256 x 256 (1.0 mm pixels; 736 channels at 1.2858 mm, 720 views
+over 360 degrees, 12 ordered subsets), 10 unrolled iterations, each with a
+learnable step scale and TV weight, checkpointed per iteration.
+
+* Gradients with respect to the 20 parameters and the starting image against
+  central finite differences (eps = 1e-3), relative error <= 5e-3.
+* The same unrolled loop built on the reference library's own
+  cDistanceDrivenFan{Projection,Backprojection} (oracle/_ref, when present),
+  with the reference's gradient registration (python/ReconNet.py:773-830:
+  the projection's gradient is the backprojection and vice versa), against
+  this library with the same registration (bp_type 0): relative difference of
+  the gradients <= 1e-2 (the reference reads its prefix sums through 8-bit
+  texture weights, ~1e-3 per projection).
+* Peak device memory with and without per-iteration checkpoints is printed."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+B, M, K = 8, 12, 10
+
+
+def _setup():
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200 import phantom as P
+    from reconnet_b200.torch_ops import FanPlan
+    geom = P.geom_fan256()
+    nview = 720
+    ang = P.uniform_angles(nview)
+    rng = np.random.default_rng(31)
+    truth = np.stack([P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng) for _ in range(B)]).astype(np.float32)
+    t = torch.from_numpy(truth[:, :, :, None, None]).cuda()
+    full = FanPlan(geom, ang, nbatches=B)
+    sino = full.project(t)
+    cnt = P.poisson_sinogram(sino.cpu().numpy(), 1e5, rng)
+    b = torch.from_numpy(cnt[0].astype(np.float32)).cuda()
+    w = torch.from_numpy(cnt[1].astype(np.float32)).cuda()
+    w = w / w.mean()
+    norm = full.backproject(full.project(torch.ones(full.img_shape, device="cuda")) * w, 2)
+    plans, bs, ws = [], [], []
+    for m in range(M):
+        v = np.arange(m, nview, M)
+        plans.append(FanPlan(geom, ang[v], nbatches=B))
+        bs.append(b[:, :, v].contiguous())
+        ws.append(w[:, :, v].contiguous())
+    return geom, ang, plans, bs, ws, norm, t
+
+
+def test_unrolled_config_gradients_match_finite_differences():
+    import torch
+    from reconnet_b200.ossqs import unrolled_ossqs
+    geom, ang, plans, bs, ws, norm, truth = _setup()
+    x0 = torch.zeros_like(truth)
+
+    def loss(step, tvw, x_init=x0, checkpoint=True):
+        x = unrolled_ossqs(x_init, plans, bs, ws, norm, step, tvw, checkpoint=checkpoint)
+        return ((x - truth).double() ** 2).sum()
+
+    step = torch.linspace(0.9, 1.0, K, device="cuda").requires_grad_(True)
+    tvw = torch.linspace(0.02, 0.002, K, device="cuda").requires_grad_(True)
+    peaks = {}
+    for ck in (True, False):
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        base = torch.cuda.memory_allocated()
+        g = torch.autograd.grad(loss(step, tvw, checkpoint=ck), (step, tvw))
+        torch.cuda.synchronize()
+        peaks[ck] = torch.cuda.max_memory_allocated() - base
+        if ck:
+            gs, gt = g
+    print(f"\nunrolled OS-SQS (8 x 256^2, 720 views, 12 subsets, 10 iterations): peak memory above the inputs "
+          f"{peaks[True] / 2**20:.1f} MiB with per-iteration checkpoints, {peaks[False] / 2**20:.1f} MiB without")
+    assert peaks[True] < peaks[False]
+    eps = 1e-3
+    with torch.no_grad():
+        for vec, grad, other, first in ((step, gs, tvw, True), (tvw, gt, step, False)):
+            for i in range(K):
+                d = torch.zeros_like(vec)
+                d[i] = eps
+                lp = loss(vec + d, other) if first else loss(other, vec + d)
+                lm = loss(vec - d, other) if first else loss(other, vec - d)
+                fd = float(lp - lm) / (2 * eps)
+                assert abs(fd - float(grad[i])) <= 5e-3 * abs(fd) + 1e-9, (first, i, fd, float(grad[i]))
+    x_init = (0.01 * torch.rand_like(truth)).requires_grad_(True)
+    gx, = torch.autograd.grad(loss(step.detach(), tvw.detach(), x_init), (x_init,))
+    v = gx / gx.abs().max() * 1e-5
+    with torch.no_grad():
+        fd = float(loss(step, tvw, x_init + v) - loss(step, tvw, x_init - v)) / 2
+    assert abs(fd - float((gx * v).sum())) <= 5e-3 * abs(fd)
+
+
+REF = os.path.join(ROOT, "oracle", "_ref", "libreconnet_ref.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference library not built (make -C oracle ref)")
+def test_unrolled_gradients_match_reference_registration():
+    import torch
+    from reconnet_b200 import _native as N
+    from reconnet_b200.ossqs import unrolled_ossqs
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    lib = make_golden.load_ref(REF)
+    geom, ang, plans, bs, ws, norm, truth = _setup()
+    nview = ang.size
+
+    def args(nv):
+        return (B, 1, geom.nx, geom.ny, 1, geom.dx, geom.dy, geom.dz, geom.nu, nv, 1, geom.da, geom.dv, 0.0, 0.0,
+                geom.dsd, geom.dso, 0)
+
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+    def ref_fp(x, m):
+        a = np.ascontiguousarray(ang[m::M])
+        img = np.ascontiguousarray(x.detach().cpu().numpy())
+        out = np.zeros((B, geom.nu, a.size, 1, 1), np.float32)
+        lib.cDistanceDrivenFanProjection(p(out), p(img), p(a), *args(a.size))
+        return torch.from_numpy(out).cuda()
+
+    def ref_bp(y, m):
+        a = np.ascontiguousarray(ang[m::M])
+        s = np.ascontiguousarray(y.detach().cpu().numpy())
+        out = np.zeros((B, geom.nx, geom.ny, 1, 1), np.float32)     # the reference's BP accumulates
+        lib.cDistanceDrivenFanBackprojection(p(out), p(s), p(a), *args(a.size))
+        return torch.from_numpy(out).cuda()
+
+    class RefFP(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, x, m):
+            ctx.m = m
+            return ref_fp(x, m)
+
+        @staticmethod
+        def backward(ctx, g):
+            return ref_bp(g, ctx.m), None
+
+    class RefBP(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, y, m):
+            ctx.m = m
+            return ref_bp(y, m)
+
+        @staticmethod
+        def backward(ctx, g):
+            return ref_fp(g, ctx.m), None
+
+    step = torch.linspace(0.9, 1.0, K, device="cuda").requires_grad_(True)
+    tvw = torch.linspace(0.02, 0.002, K, device="cuda").requires_grad_(True)
+    x0 = torch.zeros_like(truth)
+
+    def grads(**kw):
+        x = unrolled_ossqs(x0, plans, bs, ws, norm, step, tvw, **kw)
+        L = ((x - truth).double() ** 2).sum()
+        return torch.cat([g.reshape(-1) for g in torch.autograd.grad(L, (step, tvw))])
+
+    ours = grads(bp_type=N.RN_TYPE_ITERATIVE)
+    ref = grads(project=lambda x, m: RefFP.apply(x, m), backproject=lambda r, m: RefBP.apply(r, m))
+    rel = float((ours - ref).norm() / ref.norm())
+    print(f"\nunrolled OS-SQS gradients, this library vs the reference library (same registration): {rel:.2e}")
+    assert rel <= 1e-2
