@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-ossqs", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis, cone and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
-    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs", "cyl"],
+    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs", "cyl", "cfg0", "prior"],
                     help="run only this extra measurement (one GPU) and print its JSON object")
     return ap.parse_args()
 
@@ -416,6 +416,170 @@ def ossqs_run(plan, geom, counts, angles, truth, n_iter, dev, n_subsets=24, I0=5
             "note": "graph replay of one full iteration (24 subset updates: FP, residual, matched BP, "
                     "TV + SQS step); includes the start-up copy of x0.  Rays with at most one photon "
                     "(starved_ray_fraction) carry a clipped, biased line integral, which bounds the noisy RMSE"}
+
+
+def cfg0_run(dev, cpu_sample=True, n_iter=20, n_subsets=12, I0=1e5):
+    """The 2D fan workload end to end: a 256x256 random-ellipse phantom (1.0 mm
+    pixels), 736 channels at 1.2858 mm, 720 views over 360 degrees; its DD
+    projection, Poisson counts at I0 = 1e5, the ramp-filtered FBP (Ram-Lak,
+    pixel-driven backprojection) and 20 iterations of TV OS-SQS with 12
+    subsets started from the FBP image.  The same pipeline runs on the host
+    cores as the FP32 OpenMP port of the oracle (the reference has no CPU DD
+    path; this is the "host C++ build" of the workload)."""
+    import torch
+
+    from reconnet_b200 import phantom as P
+    from reconnet_b200.ossqs import BatchedOSSQS, interleaved_subsets, tv_terms
+    from reconnet_b200.torch_ops import FanPlan, fbp
+    geom = P.geom_fan256()
+    nview = 720
+    ang = P.uniform_angles(nview)
+    truth = P.ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, np.random.default_rng(2)).astype(np.float32)
+    t = torch.from_numpy(truth[None, :, :, None, None]).to(dev)
+    plan = FanPlan(geom, ang, device=dev)
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    times = {}
+
+    def timed(name, fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = ev()
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        times[name] = e0.elapsed_time(e1)
+        return r
+
+    line = timed("fp_ms", lambda: plan.project(t))
+    rng = np.random.default_rng(3)
+    b_np, cnt_np = P.poisson_sinogram(line.cpu().numpy(), I0, rng)
+    b, w = torch.from_numpy(b_np).to(dev), torch.from_numpy(cnt_np).to(dev)
+    timed("bp_ms", lambda: plan.backproject(b, 2))
+    x_fbp = timed("fbp_ms", lambda: fbp(b, plan, geom, 0))
+    solver = BatchedOSSQS(geom, [nview], ang, b.reshape(-1), w.reshape(-1), n_subsets=n_subsets, lb=0.0, device=dev)
+    _, n_flat = tv_terms(torch.zeros((1, 8, 8), device=dev))
+    solver.beta = float(0.05 * solver.norm_img.median() / n_flat[0, 4, 4])
+    x0 = x_fbp[:, :, :, 0, 0].clamp_min(0).contiguous()
+    x = timed("ossqs_ms", lambda: solver.run(x0, n_iter))
+    solver.check()
+    rmse = lambda a: float(np.sqrt(np.mean((np.asarray(a, np.float64) - truth) ** 2)) / P.HU)
+    out = {"workload": "256x256 @1.0 mm, 736 ch @1.2858 mm, 720 views over 360 deg: DD FP, matched BP, Ram-Lak FBP, "
+                       f"{n_iter} TV OS-SQS iterations ({n_subsets} subsets) from the FBP image, I0 = {I0:g}",
+           "gpu_ms": times, "gpu_pipeline_ms": times["fp_ms"] + times["fbp_ms"] + times["ossqs_ms"],
+           "rmse_hu_fbp": rmse(x_fbp[0, :, :, 0, 0].cpu().numpy()), "rmse_hu_ossqs": rmse(x[0].cpu().numpy()),
+           "beta": solver.beta}
+    if cpu_sample:
+        from oracle import oracle as O
+        O.set_threads(os.cpu_count() or 1)
+        c = {}
+        t0 = time.perf_counter()
+        O.fan_fp(truth[None, :, :, None, None], ang, geom, geom.nu, 1, dtype=np.float32)
+        c["fp_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        filt = O.filter_sino(b_np, geom, 0).astype(np.float32)
+        xf = O.pixel_bp(filt, ang, geom, (geom.nx, geom.ny, 1), dtype=np.float32)[0, :, :, 0, 0]
+        c["fbp_s"] = time.perf_counter() - t0
+        sino, wsn = b_np[0, :, :, 0, 0], cnt_np[0, :, :, 0, 0]
+        ones = np.ones((1, geom.nx, geom.ny, 1, 1), np.float32)
+        a1 = (O.fan_fp(ones, ang, geom, geom.nu, 1, dtype=np.float32)[0, :, :, 0, 0] * wsn).astype(np.float32)
+        norm = O.fan_bp(a1[None, :, :, None, None], ang, geom, (geom.nx, geom.ny, 1), 2,
+                        dtype=np.float32)[0, :, :, 0, 0]
+        xc = np.maximum(xf, 0).astype(np.float32)
+        t0 = time.perf_counter()
+        iters = 0
+        while iters < n_iter:
+            for views in interleaved_subsets(nview, n_subsets):
+                xc = O.sqs_subset_update(xc, sino, wsn, norm, ang, views, geom, n_subsets, beta=solver.beta, lb=0.0,
+                                         dtype=np.float32).astype(np.float32)
+            iters += 1
+            if time.perf_counter() - t0 > 20.0:
+                break
+        c["ossqs_s_per_iteration"] = (time.perf_counter() - t0) / iters
+        c["ossqs_iterations_run"] = iters
+        c["pipeline_s"] = c["fp_s"] + c["fbp_s"] + c["ossqs_s_per_iteration"] * n_iter
+        c["rmse_hu_after_run"] = rmse(xc)
+        out["cpu_baseline"] = {"value": c["pipeline_s"], "unit": "s", "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"the same pipeline on the host, FP32 OpenMP oracle; OS-SQS timed over "
+                                         f"{iters} of the {n_iter} iterations (capped at ~20 s) and scaled",
+                               "stages": c}
+        out["speedup_vs_cpu"] = c["pipeline_s"] * 1e3 / out["gpu_pipeline_ms"]
+    return out
+
+
+def prior_run(dev, n_train=128, n_eval=32, train_steps=600, tv_iters=100):
+    """The learned prior against plain TV-SQS (the learned-prior workload at
+    reduced slice counts): 512x512 slices @0.7 mm, 888 channels, 1152 views;
+    the CNN (5 layers, 32 channels, BF16 tcgen05 convolutions) is trained here
+    on n_train pairs (inputs: 4 OS-SQS iterations at I0 = 1e4; targets: 100
+    TV-SQS iterations at I0 = 1e6), then n_eval held-out slices at I0 = 1e4
+    are reconstructed by (a) TV-SQS for tv_iters iterations and (b) 4 OS-SQS
+    iterations + the network.  Time-to-RMSE: the target is TV-SQS's final
+    RMSE + 1 HU; TV's time is that of its first iteration within the target."""
+    import torch
+
+    from reconnet_b200 import learned_prior as LP
+    from reconnet_b200.phantom import HU, ellipse_phantom, geom_fan512
+    geom = geom_fan512()
+    nview = 1152
+    t0 = time.perf_counter()
+    x_in, x_tg, _ = LP.make_training_pairs(geom, nview, n_train, seed=5)
+    gen_s = time.perf_counter() - t0
+    net = LP.PriorCNN(dev, seed=0)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    losses = net.train(x_in, x_tg, steps=train_steps, batch=8, lr=1e-3, log_every=100)
+    torch.cuda.synchronize(dev)
+    train_s = time.perf_counter() - t0
+    rng = np.random.default_rng(77)
+    truth = torch.from_numpy(np.stack([ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)
+                                       for _ in range(n_eval)]).astype(np.float32)).to(dev)
+    ang, b, w = LP.simulate(geom, nview, truth, 1e4, seed=99)
+    rmse = lambda a: float(torch.sqrt(((a - truth) ** 2).mean())) / HU
+    # TV-SQS trajectory (untimed), then its timing (graph replay, CUDA events)
+    from reconnet_b200.ossqs import BatchedOSSQS
+    solver = BatchedOSSQS(geom, [nview] * n_eval, ang, b, w, n_subsets=24, lb=0.0, device=dev)
+    solver.beta = LP.tv_weight(solver)
+    x = torch.zeros_like(truth)
+    traj = []
+    for k in range(tv_iters):
+        x = solver.run(x, 1)
+        traj.append(rmse(x))
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    e0, e1 = ev()
+    e0.record()
+    solver.run(torch.zeros_like(truth), tv_iters)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    tv_ms_per_iter = e0.elapsed_time(e1) / tv_iters
+    solver.check()
+    target = traj[-1] + 1.0
+    # learned: 4 OS-SQS iterations (same solver, no TV) + the network
+    solver.beta = 0.0
+    x4 = solver.run(torch.zeros_like(truth), 4)
+    y = net.denoise(x4).clamp_min_(0.0)
+    e0, e1 = ev()
+    e0.record()
+    x4 = solver.run(torch.zeros_like(truth), 4)
+    y = net.denoise(x4).clamp_min_(0.0)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    learned_ms = e0.elapsed_time(e1)
+    net.k.check()
+    r_learned = rmse(y)
+    k_reach = next((k for k, r in enumerate(traj) if r <= target), None)
+    tv_ms_to_target = None if k_reach is None else (k_reach + 1) * tv_ms_per_iter
+    speedup = None if (tv_ms_to_target is None or r_learned > target) else tv_ms_to_target / learned_ms
+    return {"workload": f"512x512 @0.7 mm, 888 ch, {nview} views; train {n_train} slices (4-iteration OS-SQS at "
+                        f"I0=1e4 -> 100-iteration TV-SQS at I0=1e6), evaluate {n_eval} held-out slices at I0=1e4",
+            "scaled_from": "4,000 training and 256 held-out slices in the workload's definition",
+            "data_generation_s": gen_s, "train_s": train_s, "train_steps": train_steps, "train_loss": losses,
+            "tv_iterations": tv_iters, "tv_ms_per_iteration": tv_ms_per_iter, "tv_rmse_hu_final": traj[-1],
+            "tv_rmse_hu_at": {str(k + 1): traj[k] for k in (0, 3, 9, 19, 49, tv_iters - 1) if k < tv_iters},
+            "rmse_target_hu": target, "tv_ms_to_target": tv_ms_to_target,
+            "learned_ms": learned_ms, "learned_rmse_hu": r_learned, "os_sqs4_rmse_hu": rmse(x4),
+            "speedup_time_to_rmse": speedup,
+            "target_met": bool(speedup is not None and speedup >= 3.0)}
 
 
 def tomo_run(dev, cpu_sample=True):
@@ -898,6 +1062,8 @@ def run_b200(args):
         extras["siddon_cone"] = cone_run(dev, cpu_sample=world == 1)
         extras["filter"] = filter_run(dev, cpu_sample=world == 1)
         extras["cone_cyl"] = cyl_run(dev, cpu_sample=world == 1)
+        extras["fan2d_pipeline"] = cfg0_run(dev, cpu_sample=world == 1)
+        extras["learned_prior"] = prior_run(dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -948,6 +1114,10 @@ def run_extra(args):
         out = cone_run(dev, cpu_sample=cpu)
     elif args.extra == "cyl":
         out = cyl_run(dev, cpu_sample=cpu)
+    elif args.extra == "cfg0":
+        out = cfg0_run(dev, cpu_sample=cpu)
+    elif args.extra == "prior":
+        out = prior_run(dev)
     else:
         out = filter_run(dev, cpu_sample=cpu)
     print(json.dumps({args.extra: out}), flush=True)

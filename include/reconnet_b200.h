@@ -197,6 +197,13 @@ int rn_fan_backproject(rn_fan_plan* plan, float* d_img, const float* d_prj, int 
  * synchronises `stream`, returns RN_OK or RN_ERR_TIMEOUT, clears the word. */
 int rn_fan_plan_check(rn_fan_plan* plan, void* stream);
 
+/* Polls each chunk wait of the plan's projection and backprojection kernels
+ * makes before it gives up (records RN_ERR_TIMEOUT, waits for its own bulk
+ * copy in flight, and returns); -1 restores the default of 2^22.  A limit of
+ * 0 makes every wait give up at once: the failure path runs, without any
+ * fault, for tests. */
+int rn_fan_plan_set_spin_limit(rn_fan_plan* plan, long long polls);
+
 /* Instrumentation.  rn_fan_plan_set_timing(plan, 1) brackets every kernel
  * launch of the plan with CUDA events on its stream; rn_fan_plan_read_timing
  * synchronises on them and returns, per kernel kind (0 line prologue,

@@ -282,7 +282,7 @@ def tomo_bp(prj, det_center, src, g, img_shape, weight_mode=0):
 # term from TotalVariation.cu, explicit subset view lists).
 # ---------------------------------------------------------------------------
 def sqs_subset_update(x, sino, wsino, norm_img, angles, views, g, n_subsets, lam=1.0, beta=0.0,
-                      lb=-np.inf, ub=np.inf, bp_type=2, projector="dd"):
+                      lb=-np.inf, ub=np.inf, bp_type=2, projector="dd", dtype=np.float64):
     """One ordered-subset SQS step on a [nx, ny] slice (2D, B = C = 1),
     ossqs.cu:91-149 with the TV terms of the TV-regularised variant.
 
@@ -300,13 +300,13 @@ def sqs_subset_update(x, sino, wsino, norm_img, angles, views, g, n_subsets, lam
     if projector == "siddon":
         fp = siddon_fp(x[None, :, :, None, None], ang, g, nu, 1)[0, :, :, 0, 0]
     else:
-        fp = fan_fp(x[None, :, :, None, None], ang, g, nu, 1)[0, :, :, 0, 0]
+        fp = fan_fp(x[None, :, :, None, None], ang, g, nu, 1, dtype=dtype)[0, :, :, 0, 0]
     r = (fp - sino[:, views].astype(np.float64)) * wsino[:, views].astype(np.float64)
     r = r.astype(np.float32)[None, :, :, None, None]
     if projector == "siddon":
         bp = siddon_bp(r, ang, g, (nx, ny, 1))[0, :, :, 0, 0]
     else:
-        bp = fan_bp(r, ang, g, (nx, ny, 1), bp_type)[0, :, :, 0, 0]
+        bp = fan_bp(r, ang, g, (nx, ny, 1), bp_type, dtype=dtype)[0, :, :, 0, 0]
     num = n_subsets * bp
     den = np.asarray(norm_img, np.float64) + 1e-6
     if beta > 0:

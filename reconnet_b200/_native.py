@@ -118,6 +118,7 @@ SIGNATURES = {
                                ctypes.POINTER(ctypes.c_size_t)]),
     "rn_tomo_project": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_vp]),
     "rn_tomo_backproject": (_i, [_vp, _vp, _vp, _vp, _vp] + _TOMO + [_i, _vp]),
+    "rn_fan_plan_set_spin_limit": (_i, [_vp, ctypes.c_longlong]),
     "rn_cyl_plan_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(RnCylGeom), _fp, _vp]),
     "rn_cyl_plan_destroy": (_i, [_vp]),
     "rn_cyl_project": (_i, [_vp, _vp, _vp, _vp]),

@@ -207,6 +207,7 @@ struct FpParams {
     FanDims d;
     int R;             // lines per chunk
     int vt;            // views per CTA (size of the per-edge table)
+    long long spin;    // polls of a chunk wait before it gives up (the plan's spin limit)
 };
 
 // Active line range [lb, le) of the footprint between edge slopes ra, rb
@@ -349,9 +350,15 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         const int b = c & 1;
         const int l0 = c * R;
         const int rc = min(R, nlines - l0);
-        if (!mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1))) ok = false;
+        if (!mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1), p.spin)) ok = false;
         if (!__syncthreads_and(ok)) {
-            if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
+            // chunk c's bulk copy is the only one in flight (chunk c + 1 is
+            // issued after this barrier): the issuing thread waits for it,
+            // bounded, so no copy lands in shared memory after the CTA exits
+            if (tid == 0) {
+                atomicExch(p.err, RN_ERR_TIMEOUT);
+                mbar_wait(&bars[b], (uint32_t)((c >> 1) & 1));
+            }
             ok = false;
             break;
         }
@@ -592,6 +599,7 @@ struct BpParams {
     int accumulate;
     int type;
     int tiles_x, tiles_y;
+    long long spin;    // polls of a chunk wait before it gives up (the plan's spin limit)
     int win;           // staged table entries per view
     // view split for small batches: CTA part k of a tile takes the k-th
     // share of the views and writes its partial image to parts + k *
@@ -1187,10 +1195,15 @@ __global__ void __launch_bounds__(kBpThreads, (kMode == 2 || kMode == 0) ? 3 : 0
     bool ok = true;
     for (int c = 0; c < nchunks; c++) {
         const int b = c & 1;
-        if (!mbar_wait(&sh->bars[b], (uint32_t)((c >> 1) & 1))) ok = false;
+        if (!mbar_wait(&sh->bars[b], (uint32_t)((c >> 1) & 1), p.spin)) ok = false;
         if (tid < 32 && c + 1 < nchunks) prep(c + 1, sh->rec[(c + 1) & 1]);
         if (!__syncthreads_and(ok)) {
-            if (tid == 0) atomicExch(p.err, RN_ERR_TIMEOUT);
+            // chunk c's copies are the only ones in flight: wait for them
+            // (bounded) before the CTA gives its shared memory back
+            if (tid == 0) {
+                atomicExch(p.err, RN_ERR_TIMEOUT);
+                mbar_wait(&sh->bars[b], (uint32_t)((c >> 1) & 1));
+            }
             ok = false;
             break;
         }
@@ -1457,6 +1470,7 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
             fp.d = d;
             fp.R = R;
             fp.vt = fan_fp_views(d.nu);
+            fp.spin = p->spin_limit;
             LaunchScope ls1(p, st, 1);
             if (siddon) fan_fp_kernel<true><<<wend - wbeg, kFpThreads, smem, st>>>(fp);
             else fan_fp_kernel<false><<<wend - wbeg, kFpThreads, smem, st>>>(fp);
@@ -1565,6 +1579,7 @@ int fan_backproject(rn_fan_plan* p, float* d_img, const float* d_prj, int type, 
         bp.d = d;
         bp.accumulate = accumulate;
         bp.type = type;
+        bp.spin = p->spin_limit;
         bp.tiles_x = tiles_x;
         bp.tiles_y = tiles_y;
         bp.win = win;
@@ -1824,6 +1839,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     fp.d = d;
     fp.R = R;
     fp.vt = VT;
+    fp.spin = kSpinLimit;
     fan_fp_kernel<false><<<nwork, kFpThreads, smem, st>>>(fp);
     RN_CUDA_TRY(cudaGetLastError());
     int herr = 0;

@@ -490,17 +490,18 @@ __global__ void sqs_update_kernel(float* __restrict__ xo, const float* __restric
     const int ix = blockIdx.y, bb = blockIdx.z;
     const long long isx = (long long)ny * nzc;
     const long long i = ((long long)bb * nx + ix) * isx + j;
-    float num = M * bp[i];
-    float den = nimg[i] + 1e-6f;
+    // numerator and denominator of the surrogate step in FP64
+    double num = (double)M * bp[i];
+    double den = (double)nimg[i] + 1e-6;
     if (beta != 0.f) {
         const int iy = nzc == 1 ? j : j / nzc;
         const int zc = j - iy * nzc;
         const float* plane = xi + (long long)bb * nx * isx + zc;
         TvTerms t = tv_terms(plane, ix, iy, nx, ny, isx, nzc);
-        num += beta * t.grad;
-        den += beta * t.norm;
+        num += (double)beta * t.grad;
+        den += (double)beta * t.norm;
     }
-    float v = xi[i] - lam * num / den;
+    float v = (float)((double)xi[i] - (double)lam * num / den);
     if (clamp) v = fminf(fmaxf(v, lb), ub);
     xo[i] = v;
 }
@@ -515,8 +516,6 @@ int sqs_update(rn_fan_plan* p, float* x_out, const float* x_in, const float* prj
         if (g.nBatches > 65535 || (long long)g.ny * nzc >= (1LL << 31))
             return set_error(RN_ERR_ARG, "sqs update: more than 65535 batches, or an image row above 2^31 elements");
     }
-    if (!p->d_tmp_prj) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_prj, sizeof(float) * p->prj_elems));
-    if (!p->d_tmp_img) RN_CUDA_TRY(cudaMalloc(&p->d_tmp_img, sizeof(float) * p->img_elems));
     RN_TRY(fan_project(p, p->d_tmp_prj, x_in, st, type == RN_TYPE_SIDDON));
     long long n = p->prj_elems;
     residual_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(p->d_tmp_prj, prj_s,

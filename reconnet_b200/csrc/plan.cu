@@ -254,6 +254,10 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     device(&p->d_la, sizeof(float) * p->fp_slots * p->line_slot_elems);
     device(&p->d_tab, sizeof(float4) * p->tab_elems);
     if (p->bp_parts_cap > 0) device(&p->d_bp_parts, sizeof(float) * p->bp_parts_cap);
+    // residual and backprojection scratch of the SQS step and the autotuner:
+    // part of the plan, so a step never allocates
+    device(&p->d_tmp_prj, sizeof(float) * (size_t)p->prj_elems);
+    device(&p->d_tmp_img, sizeof(float) * (size_t)p->img_elems);
 
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
     size_t upload_bytes = 0;
@@ -343,8 +347,6 @@ int rn_fan_plan_destroy(rn_fan_plan* p) {
         else cudaFree(p->d_arena);
         if (cur >= 0 && cur != p->device) cudaSetDevice(cur);
     }
-    cudaFree(p->d_tmp_img);
-    cudaFree(p->d_tmp_prj);
     for (auto& t : p->timed) {
         cudaEventDestroy(t.start);
         cudaEventDestroy(t.stop);
@@ -688,10 +690,6 @@ int rn_fan_plan_autotune(rn_fan_plan* p, float* d_prj, const float* d_img, int t
     }
     // the view split of the backprojection, where the plan can split it
     if (s == RN_OK && p->bp_parts_cap > 0) {
-        if (!p->d_tmp_img) {
-            cudaError_t e = cudaMalloc(&p->d_tmp_img, sizeof(float) * p->img_elems);
-            if (e != cudaSuccess) s = set_cuda_error(e, "autotune: cudaMalloc");
-        }
         best = 1e30f;
         for (int parts = 1; parts <= kBpMaxParts && s == RN_OK; parts *= 2) {
             if ((long long)parts * p->img_elems > p->bp_parts_cap && parts > 1) break;
@@ -717,6 +715,14 @@ int rn_fan_plan_autotune(rn_fan_plan* p, float* d_prj, const float* d_img, int t
         g_tuned[key] = {best_vt, best_R, best_parts};
     }
     return apply_tuning(p, best_vt, best_R, best_parts, st);
+}
+
+int rn_fan_plan_set_spin_limit(rn_fan_plan* p, long long polls) {
+    clear_error();
+    if (!p) return set_error(RN_ERR_ARG, "null plan");
+    if (polls < -1) return set_error(RN_ERR_ARG, "spin limit must be >= 0 (-1 restores the default)");
+    p->spin_limit = polls == -1 ? kSpinLimit : polls;
+    return RN_OK;
 }
 
 int rn_fan_plan_check(rn_fan_plan* p, void* stream) {

@@ -34,10 +34,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 }
 
 // Returns true when the phase with the given parity has completed, false if
-// the bounded spin ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// the bounded spin (`limit` polls) ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = kSpinLimit) {
     uint32_t addr = smem_u32(bar);
-    for (long long it = 0; it < kSpinLimit; ++it) {
+    for (long long it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

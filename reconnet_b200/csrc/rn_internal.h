@@ -155,7 +155,7 @@ struct rn_fan_plan {
     int table_win_m = 0;            // staged table entries per view (BP tiles of 31 x 128 pixels)
     float4* d_tab = nullptr;        // BP edge tables
     long long tab_elems = 0;
-    float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, lazily allocated)
+    float* d_tmp_img = nullptr;     // image-sized scratch (SQS update, autotuner)
     float* d_bp_parts = nullptr;    // partial images of a view-split backprojection
     long long bp_parts_cap = 0;     // elements
     // launch parameters (0 = the built-in choice); set by rn_fan_plan_set_tuning
@@ -165,9 +165,9 @@ struct rn_fan_plan {
     int bp_nparts = 0;              // view parts of a split backprojection (single-launch batches)
     int fp_vt_used = 0;             // views per work item of the current work list
     int fp_work_cap = 0;            // work items the device list holds (one view each)
-    float* d_tmp_prj = nullptr;     // sinogram-sized scratch (SQS update, lazily allocated)
-    // every device table and scratch above except the two lazily allocated
-    // ones lives in this one allocation
+    long long spin_limit = rn::kSpinLimit;   // polls of a chunk wait before it gives up
+    float* d_tmp_prj = nullptr;     // sinogram-sized scratch (SQS update)
+    // every device table and scratch above lives in this one allocation
     void* d_arena = nullptr;
     size_t arena_bytes = 0;
 

@@ -234,3 +234,71 @@ class PriorCNN:
                 losses.append(loss)
         self.k.check()
         return losses
+
+
+# ---------------------------------------------------------------------------
+# Data and the learned-prior reconstruction
+# ---------------------------------------------------------------------------
+def simulate(geom, nview: int, truth: torch.Tensor, I0: float, seed: int):
+    """Projections of a batch of slices [S, nx, ny] over nview uniform views
+    with Poisson counts at I0: (solver angles, b, w) in the ragged packed
+    layout of BatchedOSSQS (flat [S * nu * nview])."""
+    from .phantom import uniform_angles
+    from .torch_ops import FanPlan
+    S = truth.shape[0]
+    ang = np.tile(uniform_angles(nview), S)
+    plan = FanPlan(geom, ang, nbatches=S, nview_per_slice=[nview] * S, device=truth.device)
+    gen = torch.Generator(device=truth.device).manual_seed(seed)
+    with torch.no_grad():
+        line = plan.project(truth.contiguous())
+        counts = torch.poisson(I0 * torch.exp(-line.double()), generator=gen).clamp_min(1.0)
+        b = (-torch.log(counts / I0)).float()
+    return ang, b, counts.float()
+
+
+def tv_weight(solver) -> float:
+    """TV weight of the OS-SQS runs: 5% of the median data curvature against
+    the TV curvature of a flat image (the weight the benchmark's OS-SQS uses)."""
+    from .ossqs import tv_terms
+    _, n_flat = tv_terms(torch.zeros((1, 8, 8), device=solver.norm_img.device))
+    return float(0.05 * solver.norm_img.median() / n_flat[0, 4, 4])
+
+
+def os_sqs(geom, nview, ang, b, w, S, n_iter, n_subsets=24, beta=None, x0=None):
+    """TV OS-SQS (BatchedOSSQS, graph-replayed iterations) on S slices."""
+    from .ossqs import BatchedOSSQS
+    solver = BatchedOSSQS(geom, [nview] * S, ang, b, w, n_subsets=n_subsets, lb=0.0, device=b.device)
+    solver.beta = tv_weight(solver) if beta is None else beta
+    x0 = torch.zeros((S, geom.nx, geom.ny), device=b.device) if x0 is None else x0
+    x = solver.run(x0, n_iter)
+    solver.check()
+    return x, solver
+
+
+def make_training_pairs(geom, nview: int, n_slices: int, seed: int, I0_in=1e4, I0_target=1e6, it_in=4,
+                        it_target=100, n_subsets=24, chunk=32):
+    """(inputs, targets, truths) [n_slices, nx, ny]: inputs = it_in OS-SQS
+    iterations at I0_in, targets = it_target TV-SQS iterations at I0_target,
+    on seeded random-ellipse slices."""
+    from .phantom import ellipse_phantom
+    rng = np.random.default_rng(seed)
+    ins, tgs, tru = [], [], []
+    for c0 in range(0, n_slices, chunk):
+        S = min(chunk, n_slices - c0)
+        truth = torch.from_numpy(np.stack([ellipse_phantom(geom.nx, geom.ny, geom.dx, geom.dy, rng)
+                                           for _ in range(S)]).astype(np.float32)).cuda()
+        ang, b, w = simulate(geom, nview, truth, I0_in, seed * 1000 + c0)
+        x_in, _ = os_sqs(geom, nview, ang, b, w, S, it_in, n_subsets)
+        ang, b, w = simulate(geom, nview, truth, I0_target, seed * 1000 + c0 + 1)
+        x_tg, _ = os_sqs(geom, nview, ang, b, w, S, it_target, n_subsets)
+        ins.append(x_in)
+        tgs.append(x_tg)
+        tru.append(truth)
+    return torch.cat(ins), torch.cat(tgs), torch.cat(tru)
+
+
+def learned_ossqs(net: PriorCNN, geom, nview, ang, b, w, S, n_iter=4, n_subsets=24):
+    """A few OS-SQS iterations, then the network in place of the TV prior's
+    remaining work; returns (image, the OS-SQS image)."""
+    x, _ = os_sqs(geom, nview, ang, b, w, S, n_iter, n_subsets)
+    return net.denoise(x).clamp_min_(0.0), x

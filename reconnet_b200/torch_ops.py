@@ -142,6 +142,10 @@ class FanPlan:
         """Synchronise and raise if a device-side bounded wait gave up."""
         N.check(N.lib.rn_fan_plan_check(self._plan, _stream_ptr(self.device)))
 
+    def set_spin_limit(self, polls: int = -1) -> None:
+        """Polls each device-side chunk wait makes before giving up (-1: the default)."""
+        N.check(N.lib.rn_fan_plan_set_spin_limit(self._plan, int(polls)))
+
     def autotune(self, img: torch.Tensor, type_projector: int = N.RN_TYPE_MATCHED,
                  sino: Optional[torch.Tensor] = None) -> Tuple[int, int, int]:
         """Time the launch-parameter candidates of this plan's forward

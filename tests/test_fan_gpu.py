@@ -360,3 +360,32 @@ def test_streamed_pair_matches_single_plan(rng):
         pair.check()
         ref = plan.backproject(plan.project(imgs.cuda()), 2).cpu()
         assert torch.equal(out, ref), call
+
+
+@pytest.mark.parametrize("op", ["project", "backproject"])
+def test_device_wait_timeout_is_reported_and_recoverable(op, rng):
+    """A spin limit of zero polls makes every chunk wait of the kernels give
+    up at once: the kernels record RN_ERR_TIMEOUT, wait (bounded) for their
+    own bulk copies in flight and return, with no fault.  check() reports it;
+    with the default limit the same plan then computes the right result."""
+    import torch
+    from oracle import oracle as O
+    from reconnet_b200 import _native as N
+    from reconnet_b200.torch_ops import FanPlan
+    g = small_fan()
+    ang = (np.arange(40) * 2 * np.pi / 40).astype(np.float32)
+    plan = FanPlan(to_geometry(g), ang)
+    x = rng.random((1, g.nx, g.ny, 1, 1)).astype(np.float32)
+    y = rng.random((1, g.nu, ang.size, 1, 1)).astype(np.float32)
+    run = (lambda: plan.project(torch.from_numpy(x).cuda())) if op == "project" else \
+        (lambda: plan.backproject(torch.from_numpy(y).cuda(), 2))
+    plan.set_spin_limit(0)
+    run()
+    with pytest.raises(N.ReconNetError) as e:
+        plan.check()
+    assert e.value.code == N.RN_ERR_TIMEOUT
+    plan.set_spin_limit(-1)
+    got = run().cpu().numpy()
+    plan.check()
+    ref = O.fan_fp(x, ang, g, g.nu, 1) if op == "project" else O.fan_bp(y, ang, g, (g.nx, g.ny, 1), 2)
+    assert rel_l2(got, ref) <= TOL
