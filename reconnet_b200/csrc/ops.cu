@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <list>
 #include <map>
 #include <mutex>
 #include <string>
@@ -559,11 +560,22 @@ struct DevBuf {
 struct HostCtx {
     std::mutex mu;
     cudaStream_t st = nullptr;
-    rn_fan_plan* plan = nullptr;
-    RnFanGeom key{};
-    std::vector<float> key_deg;
+    rn_fan_plan* plan = nullptr;    // the plan of the current call (owned by `cache`)
+    // plans of recent (geometry, angles) pairs, most recent first: a caller
+    // that cycles through the same slices (each with its own angles) finds
+    // its plans here instead of rebuilding one per call
+    struct Cached {
+        RnFanGeom key;
+        std::vector<float> deg;
+        uint64_t hash;
+        rn_fan_plan* plan;
+    };
+    std::list<Cached> cache;
+    size_t cache_bytes = 0;
     DevBuf a, b, c, d, e;
 };
+constexpr size_t kHostPlanCacheCount = 128;
+constexpr size_t kHostPlanCacheBytes = (size_t)4 << 30;
 static std::mutex g_ctx_mu;
 static std::map<int, HostCtx*> g_ctx;
 
@@ -579,15 +591,40 @@ static HostCtx* host_ctx() {
     return c;
 }
 
+static uint64_t angle_hash(const RnFanGeom& g, const float* deg, int nview) {
+    uint64_t h = 1469598103934665603ull;   // FNV-1a over the geometry and the angle bits
+    auto mix = [&](const void* d, size_t n) {
+        const unsigned char* q = static_cast<const unsigned char*>(d);
+        for (size_t i = 0; i < n; i++) {
+            h ^= q[i];
+            h *= 1099511628211ull;
+        }
+    };
+    mix(&g, sizeof(g));
+    mix(deg, sizeof(float) * (size_t)nview);
+    return h;
+}
+
 static int ctx_plan(HostCtx* c, const RnFanGeom& g, const float* deg, int nview) {
-    if (c->plan && memcmp(&c->key, &g, sizeof(g)) == 0 && (int)c->key_deg.size() == nview &&
-        memcmp(c->key_deg.data(), deg, sizeof(float) * nview) == 0)
-        return RN_OK;
-    if (c->plan) rn_fan_plan_destroy(c->plan);
-    c->plan = nullptr;
-    RN_TRY(rn_fan_plan_create(&c->plan, &g, deg, c->st));
-    c->key = g;
-    c->key_deg.assign(deg, deg + nview);
+    const uint64_t h = angle_hash(g, deg, nview);
+    for (auto it = c->cache.begin(); it != c->cache.end(); ++it) {
+        if (it->hash == h && memcmp(&it->key, &g, sizeof(g)) == 0 && (int)it->deg.size() == nview &&
+            memcmp(it->deg.data(), deg, sizeof(float) * nview) == 0) {
+            c->cache.splice(c->cache.begin(), c->cache, it);   // most recently used first
+            c->plan = it->plan;
+            return RN_OK;
+        }
+    }
+    rn_fan_plan* p = nullptr;
+    RN_TRY(rn_fan_plan_create(&p, &g, deg, c->st));
+    c->cache.push_front(HostCtx::Cached{g, std::vector<float>(deg, deg + nview), h, p});
+    c->cache_bytes += p->arena_bytes;
+    while (c->cache.size() > 1 && (c->cache.size() > kHostPlanCacheCount || c->cache_bytes > kHostPlanCacheBytes)) {
+        c->cache_bytes -= c->cache.back().plan->arena_bytes;
+        rn_fan_plan_destroy(c->cache.back().plan);
+        c->cache.pop_back();
+    }
+    c->plan = p;
     return RN_OK;
 }
 
