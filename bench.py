@@ -325,6 +325,15 @@ def reference_gpu_extras(geom, counts, angles, imgs):
     for name, fn, upd in pairs:
         ms = timed(fn)
         out[name] = {"ms": ms, "gupd_s_host_call": upd / ms / 1e6, "workload": "the tomosynthesis workload"}
+    # the ramp filter on the filter extra's workload (64 sinograms of 888 x 1152,
+    # Ram-Lak): cFilterFanFilter plans cuFFT and stages host arrays per call
+    fB, fview = 64, 1152
+    fs = np.random.default_rng(12).random((fB, geom.nu, fview, 1, 1), dtype=np.float32)
+    fo = np.zeros_like(fs)
+    fargs = (fB, 1, geom.nu, fview, 1, geom.da, geom.dv, 0.0, 0.0, geom.dsd, geom.dso, 0, 0)
+    ms = timed(lambda: lib.cFilterFanFilter(p(fo), p(fs), *fargs))
+    out["filter"] = {"ms": ms, "views_per_s_host_call": fB * fview / (ms * 1e-3),
+                     "workload": "64 fan sinograms of 888 channels x 1152 views, Ram-Lak (host arrays, cuFFT)"}
     out["note"] = ("reference CUDA library (oracle/_ref) through its C entry points with host arrays: wall time "
                    "of the second of two calls, including its allocations and copies")
     return out
