@@ -262,13 +262,14 @@ int rn_filter_weighted(float* d_out, const float* d_prj, const float* d_w, int n
  * int(4 sigma + 0.5)) outside theta < beta < pi + 2 gamma - theta.  riessMask
  * 0 keeps only channel 0 of those middle views unsmoothed, as the reference's
  * np.where(np.all(...)) does; 1 keeps the whole view unsmoothed.  d_angles is
- * a device array; the _host variant takes and returns host arrays. */
+ * a device array; the _host variant takes and returns host arrays.  Pitch,
+ * offset, sigma and theta are doubles, as the reference's Python holds them. */
 #define RN_WEIGHT_PARKER 0
 #define RN_WEIGHT_RIESS 1
-int rn_fan_shortscan_weights(float* d_w, const float* d_angles, int nu, int nview, float da, float off_a, int kind,
-                             float sigma, float theta, int riessMask, void* stream);
-int rn_fan_shortscan_weights_host(float* w, const float* angles, int nu, int nview, float da, float off_a, int kind,
-                                  float sigma, float theta, int riessMask);
+int rn_fan_shortscan_weights(float* d_w, const float* d_angles, int nu, int nview, double da, double off_a, int kind,
+                             double sigma, double theta, int riessMask, void* stream);
+int rn_fan_shortscan_weights_host(float* w, const float* angles, int nu, int nview, double da, double off_a, int kind,
+                                  double sigma, double theta, int riessMask);
 
 /* TV surrogate on a batch of S slices [S][nx][ny]; grad/norm may be NULL;
  * d_tv (may be NULL) receives S FP64 TV values. */

@@ -71,14 +71,20 @@ inline double chan_angle(const Fan& g, double iu) {
 // to compare against the reference's own texture-based kernels.
 //
 // Mode 3 (measured on a B200 with impulse textures, every 1/256 step of two
-// fractional coordinates, plus random-valued textures): each dimension's
+// fractional coordinates, random-valued textures, and every fetch of the
+// reference's X-class forward kernel on two golden cases, which it
+// reproduces to FP32 rounding): in a clamp-addressed dimension the
+// coordinate is first clamped to the texel centres' range; each dimension's
 // fraction is rounded half-up to A = round(256 a) in [0, 256]; the outermost
-// dimension's two weights (256 - A2, A2) are kept exactly; each is split
-// between the two texels of the next dimension as w1 = round-half-down(A1 X /
-// 256), w0 = X - w1.  All corner weights are thus multiples of 1/256 summing
-// to 1, and a dimension at weight 1/2 does not split an odd X evenly.  The
-// innermost dimension is split the same way (assumed: the measurement had it
-// at a texel centre, as every fetch of the reference's 2D kernels does).
+// (depth) dimension's two weights (256 - A2, A2) are kept exactly; each is
+// split between the two texels of the next dimension as w1 =
+// round-half-down(A1 X / 256), w0 = X - w1.  All corner weights are thus
+// multiples of 1/256 summing to 1, and a dimension at weight 1/2 does not
+// split an odd X evenly -- which is why the reference's X-class views (rows
+// blended 50/50 in the height dimension, prefix fraction in depth) carry ten
+// times the texture error of its Y-class views.  The innermost (width)
+// dimension is split the same way (assumed: the measurement had it at a
+// texel centre, as every fetch of the reference's 2D kernels does).
 static int g_tex_quant = 0;
 
 inline int tex_hw_split(int a, int x) { return (a * x + 127) >> 8; }   // round half down of a*x/256
@@ -163,8 +169,14 @@ struct Tex3 {
         int i0[3];
         int A[3];
         const double c[3] = {cw, ch, cd};
+        const int ext[3] = {W, H, D};
         for (int k = 0; k < 3; k++) {
-            double b = c[k] - 0.5, f = std::floor(b);
+            double b = c[k] - 0.5;
+            // clamp addressing clamps the coordinate itself (so a fetch past
+            // the last texel takes it with weight 1); border addressing
+            // keeps the coordinate and reads zeros outside
+            if (mode[k] == 1) b = std::min(std::max(b, 0.0), (double)(ext[k] - 1));
+            const double f = std::floor(b);
             i0[k] = (int)f;
             A[k] = (int)std::floor((b - f) * 256.0 + 0.5);
         }
@@ -1189,6 +1201,16 @@ void oracle_set_num_threads(int n) {
 int oracle_view_is_x(float deg) { return x_class(deg) ? 1 : 0; }
 
 void oracle_set_tex_quant(int mode) { g_tex_quant = mode; }
+
+// Fetches of the emulated texture unit at the current quantisation mode:
+// table [D][H][W], modes (0 border, 1 clamp) per dimension, coords [n][3].
+void oracle_tex_fetch(double* out, const float* table, int W, int H, int D, int m0, int m1, int m2,
+                      const float* coords, int n) {
+    std::vector<double> t((size_t)W * H * D);
+    for (size_t i = 0; i < t.size(); i++) t[i] = table[i];
+    Tex3<double> tx{t.data(), W, H, D, {m0, m1, m2}};
+    for (int i = 0; i < n; i++) out[i] = tx.fetch(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]);
+}
 
 void oracle_fan_fp_f64(double* prj, const float* img, const float* deg, FAN_ARGS) {
     fan_fp<double>(prj, img, deg, make_fan(FAN_PASS));

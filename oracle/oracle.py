@@ -66,6 +66,7 @@ def lib():
         L.oracle_cone_bp_f64.argtypes = [_dp, _fp, _fp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_fp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO
         L.oracle_tomo_bp_f64.argtypes = [_dp, _fp, _fp, _fp] + _TOMO + [_i]
+        L.oracle_tex_fetch.argtypes = [_dp, _fp, _i, _i, _i, _i, _i, _i, _fp, _i]
         L.oracle_cyl_fp_f64.argtypes = [_dp, _fp, _fp] + _CYL
         L.oracle_cyl_fp_f32.argtypes = [_fp, _fp, _fp] + _CYL
         L.oracle_cyl_bp_f64.argtypes = [_dp, _fp, _fp] + _CYL
@@ -92,6 +93,21 @@ def num_threads() -> int:
 def set_tex_quant(mode: int) -> None:
     """0 exact texture weights (default), 1 rounded / 2 truncated to 1/256."""
     lib().oracle_set_tex_quant(int(mode))
+
+
+def tex_fetch(table, modes, coords, quant=3):
+    """Linear-filtered fetches of the emulated texture unit: table [D, H, W],
+    modes (border 0 / clamp 1) per dimension (w, h, d), coords [n, 3]."""
+    t = _f32(table)
+    c = _f32(coords)
+    D, H, W = t.shape
+    out = np.zeros(c.shape[0], np.float64)
+    set_tex_quant(quant)
+    try:
+        lib().oracle_tex_fetch(_ptr(out, ctypes.c_double), _ptr(t, _f), W, H, D, *modes, _ptr(c, _f), c.shape[0])
+    finally:
+        set_tex_quant(0)
+    return out
 
 
 def view_is_x(deg: float) -> bool:

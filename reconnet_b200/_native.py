@@ -29,6 +29,7 @@ _f = ctypes.c_float
 _i = ctypes.c_int
 _fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
+_d = ctypes.c_double
 
 
 class RnFanGeom(ctypes.Structure):
@@ -107,8 +108,8 @@ SIGNATURES = {
     "rn_fan_plan_read_timing": (_i, [_vp, _fp, ctypes.POINTER(_i), _i, ctypes.POINTER(ctypes.c_longlong)]),
     "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
     "rn_filter_weighted": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
-    "rn_fan_shortscan_weights": (_i, [_vp, _vp, _i, _i, _f, _f, _i, _f, _f, _i, _vp]),
-    "rn_fan_shortscan_weights_host": (_i, [_fp, _fp, _i, _i, _f, _f, _i, _f, _f, _i]),
+    "rn_fan_shortscan_weights": (_i, [_vp, _vp, _i, _i, _d, _d, _i, _d, _d, _i, _vp]),
+    "rn_fan_shortscan_weights_host": (_i, [_fp, _fp, _i, _i, _d, _d, _i, _d, _d, _i]),
     "rn_tv_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
     "rn_tv_iso_sqs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _i, _vp]),
     "rn_tv_iso_sqs_host": (_i, [_fp, _fp, _fp, _fp, _i, _i, _i, _i, _i, _f, _i]),

@@ -28,7 +28,10 @@
 // reference); riessMask = 1 applies the exception to the whole view, the
 // behaviour the published method describes.
 //
-// Parker weights are evaluated in FP64 (the reference uses float64 numpy).
+// Parker weights are evaluated in FP64 (the reference uses float64 numpy),
+// from FP64 pitch and offset: the Riess continuations jump where a wedge
+// ends, so a channel angle rounded to FP32 can move a channel across that
+// edge.
 // The Riess pre-smoothing weights are rounded to FP32, as the reference
 // stores them in a float32 array, and smoothed in FP64.
 #include <cuda_runtime.h>
@@ -118,25 +121,25 @@ __global__ void riess_weights_kernel(float* __restrict__ w, const float* __restr
     }
 }
 
-int shortscan_weights_device(float* d_w, const float* d_ang, int nu, int nview, float da, float off_a, int kind,
-                             float sigma, float theta, int riessMask, cudaStream_t st) {
+int shortscan_weights_device(float* d_w, const float* d_ang, int nu, int nview, double da, double off_a, int kind,
+                             double sigma, double theta, int riessMask, cudaStream_t st) {
     if (!d_w || !d_ang) return set_error(RN_ERR_ARG, "shortscan weights: null argument");
     if (nu <= 0 || nview <= 0 || !(da > 0)) return set_error(RN_ERR_ARG, "shortscan weights: sizes and pitch must be positive");
     if (kind == RN_WEIGHT_PARKER) {
         dim3 grid((unsigned)((nu + 255) / 256), (unsigned)std::min(nview, 65535));
-        parker_weights_kernel<<<grid, 256, 0, st>>>(d_w, d_ang, nu, nview, (double)da, (double)off_a);
+        parker_weights_kernel<<<grid, 256, 0, st>>>(d_w, d_ang, nu, nview, da, off_a);
         RN_CUDA_TRY(cudaGetLastError());
         return RN_OK;
     }
     if (kind != RN_WEIGHT_RIESS) return set_error(RN_ERR_ARG, "shortscan weights: kind must be Parker (0) or Riess (1)");
     if (!(sigma > 0)) return set_error(RN_ERR_ARG, "shortscan weights: sigma must be positive");
     // scipy.ndimage.gaussian_filter1d's default reach: radius = int(4 sigma + 0.5)
-    const int radius = (int)(4.0 * (double)sigma + 0.5);
+    const int radius = (int)(4.0 * sigma + 0.5);
     const size_t smem = sizeof(double) * (2 * (size_t)radius + 1) + sizeof(float) * (size_t)nu;
     if (smem > 200 * 1024) return set_error(RN_ERR_ARG, "shortscan weights: too many channels or too wide a smoothing");
     RN_CUDA_TRY(cudaFuncSetAttribute(riess_weights_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     riess_weights_kernel<<<(unsigned)std::min(nview, 65535), 256, smem, st>>>(
-        d_w, d_ang, nu, nview, (double)da, (double)off_a, (double)sigma, radius, (double)theta, riessMask ? 1 : 0);
+        d_w, d_ang, nu, nview, da, off_a, sigma, radius, theta, riessMask ? 1 : 0);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
@@ -145,15 +148,15 @@ int shortscan_weights_device(float* d_w, const float* d_ang, int nu, int nview, 
 
 using namespace rn;
 
-extern "C" int rn_fan_shortscan_weights(float* d_w, const float* d_angles, int nu, int nview, float da, float off_a,
-                                        int kind, float sigma, float theta, int riessMask, void* stream) {
+extern "C" int rn_fan_shortscan_weights(float* d_w, const float* d_angles, int nu, int nview, double da, double off_a,
+                                        int kind, double sigma, double theta, int riessMask, void* stream) {
     clear_error();
     return shortscan_weights_device(d_w, d_angles, nu, nview, da, off_a, kind, sigma, theta, riessMask,
                                     (cudaStream_t)stream);
 }
 
-extern "C" int rn_fan_shortscan_weights_host(float* w, const float* angles, int nu, int nview, float da, float off_a,
-                                             int kind, float sigma, float theta, int riessMask) {
+extern "C" int rn_fan_shortscan_weights_host(float* w, const float* angles, int nu, int nview, double da,
+                                             double off_a, int kind, double sigma, double theta, int riessMask) {
     clear_error();
     if (!w || !angles) return set_error(RN_ERR_ARG, "shortscan weights: null argument");
     if (nu <= 0 || nview <= 0) return set_error(RN_ERR_ARG, "shortscan weights: sizes must be positive");

@@ -123,14 +123,14 @@ class ConvKernels:
 
 
 def unpack_wgrad(g: torch.Tensor, cin: int, cout: int):
-    """rn_conv3x3_wgrad columns -> (dW [cout, 3, 3, cin_real], db [cout])."""
+    """rn_conv3x3_wgrad columns -> (dW [cout, 3, 3, cin], db [cout])."""
     if cin == 32:
         dw = g[:cout, :288].reshape(cout, 9, 32)
         db = g[:cout, 288]
     else:
-        t = torch.arange(9, device=g.device)
-        cols = (t // 2) * 16 + (t % 2) * 8
-        dw = g[:cout, cols][:, :, None]
+        t = torch.arange(9, device=g.device)[:, None]
+        cols = (t // 2) * 16 + (t % 2) * 8 + torch.arange(8, device=g.device)[None, :]
+        dw = g[:cout, cols.reshape(-1)].reshape(cout, 9, 8)
         db = g[:cout, 80]
     return dw.reshape(cout, 3, 3, -1).contiguous(), db.contiguous()
 
@@ -196,6 +196,7 @@ class PriorCNN:
             d = self.k.conv(d, self.pkd[li], None, CH, CH, 2, aux=acts[li])
         g = self.k.wgrad(acts[0], d, 8, CH)
         dws[0], dbs[0] = unpack_wgrad(g, 8, CH)
+        dws[0] = dws[0][..., :1].contiguous()     # the image is channel 0 of the 8-channel input
         return dws, dbs
 
     def adam_step(self, dws, dbs, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):

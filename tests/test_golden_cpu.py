@@ -2,15 +2,19 @@
 kernels (tests/golden/make_golden.py, run on a B200 with the reference
 library built from its sources).
 
-The reference reads its prefix sums through linear-filtering textures whose
-weights are rounded to 1/256, so the oracle is compared twice:
+The reference reads its prefix sums through linear-filtering textures, so the
+oracle is compared twice:
   * with exact weights (the oracle proper): bounded by the texture error;
-  * with weights rounded to 1/256 (texture emulation): the reference-mode
-    backprojectors then agree to ~5e-5, the residual being the reference's
-    __sinf/__cosf/atanf and FP32 arithmetic.
-The forward projector of X-class views keeps a per-ray noise floor of ~3e-3
-against the reference kernel that no weight model removes (Y-class views sit
-at ~3e-4); the bounds below are the measured ones with a small margin.
+  * with the B200 texture unit's weights as measured (oracle mode 3: 8-bit
+    fractions after the coordinate clamp, exact depth marginals, round-half-
+    down splits in the other dimensions; pinned to hardware fetches by
+    tests/golden/ref_texfetch.npz).  What then remains is the reference's
+    __sinf/__cosf: a replica of its forward kernel with accurate sinf/cosf
+    and hardware textures differs from it by 3.8e-4 (fan2d) and 1.0e-3
+    (fan256) on X-class views, and the residuals below sit at those figures.
+The X-class views carry ten times the Y-class texture error because their
+rows are blended 50/50 in the texture's height dimension, which the unit
+splits unevenly when the depth weight is odd.
 Tomosynthesis, filter and TV paths use no textures and agree to ~1e-6."""
 import glob
 import os
@@ -50,10 +54,14 @@ def test_fan_fp_vs_reference(path):
     d, g, n = _fan(path)
     fp = O.fan_fp(d["img"], d["angles"], g, n["nu"], n["nv"])
     assert rel_l2(fp, d["fp"]) < 4e-3
-    # per class: Y-class views sit an order of magnitude closer
     xv = np.array([O.view_is_x(a) for a in d["angles"]])
+    # with the measured texture weights only the reference's __sinf/__cosf remain
+    O.set_tex_quant(3)
+    emu = O.fan_fp(d["img"], d["angles"], g, n["nu"], n["nv"])
+    x_bound = 1.2e-3 if "fan256" in path else 6e-4      # fan256: its trig floor is 1.02e-3
+    assert rel_l2(emu[:, :, xv], d["fp"][:, :, xv]) < x_bound
     if (~xv).any():
-        assert rel_l2(fp[:, :, ~xv], d["fp"][:, :, ~xv]) < 6e-4
+        assert rel_l2(emu[:, :, ~xv], d["fp"][:, :, ~xv]) < 1.5e-4
 
 
 @pytest.mark.parametrize("path", FAN, ids=[os.path.basename(p)[4:-4] for p in FAN])
@@ -66,6 +74,8 @@ def test_fan_bp_vs_reference(path, ptype):
     O.set_tex_quant(1)     # texture emulation: weights rounded to 1/256
     emu = O.fan_bp(d["sino_in"], d["angles"], g, shape, ptype)
     assert rel_l2(emu, d[f"bp{ptype}"]) < 1.2e-4
+    O.set_tex_quant(3)     # the measured weights (the backprojection fetches vary one coordinate)
+    assert rel_l2(O.fan_bp(d["sino_in"], d["angles"], g, shape, ptype), d[f"bp{ptype}"]) < 1.2e-4
     # rounding fits the hardware better than truncation
     O.set_tex_quant(2)
     trunc = O.fan_bp(d["sino_in"], d["angles"], g, shape, ptype)
@@ -210,3 +220,26 @@ def test_shortscan_weights_vs_reference(case):
     # whole-view reading of the method gives different weights
     whole = O.shortscan_weights(ang, nu, da, off, "riess", mask_all=True)
     assert np.abs(whole - d[f"{case}_riess"]).max() > 0.1
+
+
+TEXFETCH = os.path.join(GOLDEN, "ref_texfetch.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(TEXFETCH), reason="texture-fetch golden vectors not generated")
+def test_texture_model_vs_hardware_fetches():
+    """The oracle's texture model (mode 3) against fetches made by the B200's
+    texture unit (tests/golden/texfetch.cu): the fan2d prefix tables with the
+    reference's layouts and addressing at X- and Y-class coordinates across
+    and beyond the image, and an impulse texture at pairs of fractional
+    coordinates.  Equal to FP32 rounding."""
+    d = np.load(TEXFETCH)
+    mx = O.tex_fetch(d["px"][:, :, None], (0, 0, 1), d["cx"])
+    assert np.max(np.abs(mx - d["vx"]) / np.maximum(np.abs(d["vx"]), 1e-3)) < 2e-7
+    my = O.tex_fetch(d["py"][:, :, None], (0, 1, 0), d["cy"])
+    assert np.max(np.abs(my - d["vy"]) / np.maximum(np.abs(d["vy"]), 1e-3)) < 2e-7
+    imp = np.zeros((8, 8, 1), np.float32)
+    imp[4, 4, 0] = 1.0
+    mi = O.tex_fetch(imp, (0, 0, 1), d["ci"])
+    assert np.array_equal(mi.astype(np.float32), d["vi"])
+    # the same fetches with each dimension's weight rounded alone miss by up to 1/256
+    assert np.abs(O.tex_fetch(imp, (0, 0, 1), d["ci"], quant=1) - d["vi"]).max() > 1e-3

@@ -41,6 +41,17 @@ def test_fan_vs_reference_kernels(ref, name, rng):
         setattr(rn, k, out[k].item() if k not in ("nx", "ny", "nz", "nu", "nv") else int(out[k]))
     fp = rn.cDDFanProjection4d(out["img"], out["angles"])
     assert rel_l2(fp, out["fp"]) <= REF_TOL
+    # the definition, with the texture unit's measured weights, against the
+    # live reference: only its __sinf/__cosf remain (fan256's floor 1.0e-3)
+    from oracle import oracle as O
+    from types import SimpleNamespace
+    g = SimpleNamespace(**{k: float(out[k]) for k in ("dx", "dy", "dz", "da", "dv", "off_a", "off_v", "dsd", "dso")})
+    O.set_tex_quant(3)
+    try:
+        emu = O.fan_fp(out["img"], out["angles"], g, int(out["nu"]), int(out["nv"]))
+    finally:
+        O.set_tex_quant(0)
+    assert rel_l2(emu, out["fp"]) <= (1.2e-3 if name == "fan256" else 6e-4)
     for t in (0, 1):
         bp = rn.cDDFanBackprojection4d(out["sino_in"], out["angles"], type_projector=t)
         assert rel_l2(bp, out[f"bp{t}"]) <= REF_TOL
