@@ -516,6 +516,44 @@ def cfg0_run(dev, cpu_sample=True, n_iter=20, n_subsets=12, I0=1e5):
     return out
 
 
+def conv_roofline(dev, n=16, hw=512):
+    """The 32 -> 32 channel BF16 3x3 convolution layer of the prior (the
+    dominant layer: 3 of 5) forward, input-gradient and weight-gradient
+    kernels on n images of hw x hw, timed with CUDA events; FLOPs 2 * pixels
+    * 32 * 288 per kernel, against the measured dense BF16 peak."""
+    import torch
+
+    from reconnet_b200.learned_prior import ConvKernels, pack_dgrad_weights, pack_weights
+    k = ConvKernels(dev)
+    x = (torch.rand((n, 4, hw, hw, 8), device=dev) - 0.5).to(torch.bfloat16)
+    w = torch.randn(32, 3, 3, 32, device=dev) * 0.05
+    b = torch.zeros(32, device=dev)
+    pk, pkd = pack_weights(w), pack_dgrad_weights(w)
+    out = torch.empty_like(x)
+    flops = 2.0 * n * hw * hw * 32 * 288
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(p))["bf16_tflops"] if os.path.exists(p) else 1590.0
+    res = {"workload": f"{n} images {hw}x{hw}, 32 -> 32 channels, BF16 in / FP32 accumulation",
+           "flops_per_launch": flops, "peak_tflops": peak}
+    for name, fn in (("forward", lambda: k.conv(x, pk, b, 32, 32, 0, out=out)),
+                     ("input_gradient", lambda: k.conv(x, pkd, None, 32, 32, 2, aux=x, out=out)),
+                     ("weight_gradient", lambda: k.wgrad(x, x, 32, 32))):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 5
+        tf = flops / (ms * 1e-3) / 1e12
+        hbm = 2 * x.numel() * 2 / (ms * 1e-3) / 1e9
+        res[name] = {"ms": ms, "tflops": tf, "frac_of_bf16_peak": tf / peak, "activation_gbs": hbm}
+    k.check()
+    return res
+
+
 def prior_run(dev, n_train=128, n_eval=32, train_steps=600, tv_iters=100):
     """The learned prior against plain TV-SQS (the learned-prior workload at
     reduced slice counts): 512x512 slices @0.7 mm, 888 channels, 1152 views;
@@ -579,7 +617,9 @@ def prior_run(dev, n_train=128, n_eval=32, train_steps=600, tv_iters=100):
     k_reach = next((k for k, r in enumerate(traj) if r <= target), None)
     tv_ms_to_target = None if k_reach is None else (k_reach + 1) * tv_ms_per_iter
     speedup = None if (tv_ms_to_target is None or r_learned > target) else tv_ms_to_target / learned_ms
-    return {"workload": f"512x512 @0.7 mm, 888 ch, {nview} views; train {n_train} slices (4-iteration OS-SQS at "
+    conv = conv_roofline(dev)
+    return {"conv_32x32": conv,
+            "workload": f"512x512 @0.7 mm, 888 ch, {nview} views; train {n_train} slices (4-iteration OS-SQS at "
                         f"I0=1e4 -> 100-iteration TV-SQS at I0=1e6), evaluate {n_eval} held-out slices at I0=1e4",
             "scaled_from": "4,000 training and 256 held-out slices in the workload's definition",
             "data_generation_s": gen_s, "train_s": train_s, "train_steps": train_steps, "train_loss": losses,
