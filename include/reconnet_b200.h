@@ -244,6 +244,13 @@ int rn_fan_plan_get_tuning(const rn_fan_plan* plan, int* fp_views, int* fp_lines
 int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int nu, int nview, int nv, float da,
               float off_a, float dsd, float dso, int typeFilter, int fan, void* stream);
 
+/* Which ramp-filter kernel rn_filter and the host filters run (process-wide):
+ * 0 (default) the register four-step FFT where the transform length is 512,
+ * 1024 or 2048 (nu <= 1024), else the shared-memory FFT; 1 the
+ * shared-memory FFT; 2 the direct Toeplitz product.  All give the same
+ * result to FP32 rounding; the choice exists for comparisons. */
+int rn_filter_set_form(int form);
+
 /* The same filter with short-scan weights d_w [nu][nview] (broadcast over
  * batches, detector rows and channels) multiplied into the sinogram as it is
  * loaded: the reference's FBP chain multiplies its Parker / Riess weights

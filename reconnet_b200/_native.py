@@ -107,6 +107,7 @@ SIGNATURES = {
     "rn_fan_plan_get_tuning": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "rn_fan_plan_read_timing": (_i, [_vp, _fp, ctypes.POINTER(_i), _i, ctypes.POINTER(ctypes.c_longlong)]),
     "rn_filter": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
+    "rn_filter_set_form": (_i, [_i]),
     "rn_filter_weighted": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _f, _i, _i, _vp]),
     "rn_fan_shortscan_weights": (_i, [_vp, _vp, _i, _i, _d, _d, _i, _d, _d, _i, _vp]),
     "rn_fan_shortscan_weights_host": (_i, [_fp, _fp, _i, _i, _d, _d, _i, _d, _d, _i]),

@@ -99,6 +99,10 @@ struct FilterVal {
     int logN = 0;
     float2* d_H = nullptr;  // [N]
     float2* d_tw = nullptr; // [N/2] exp(-2 pi i q / N)
+    // register four-step form (N = 512, 1024, 2048): the spectrum and the
+    // middle twiddles in the registers' order, [N/32][32] (entry [r][lane])
+    float2* d_Hp = nullptr;
+    float2* d_Tw = nullptr;
 };
 
 // In-place radix-2 FFT in FP64 (host; the filter spectrum).
@@ -164,6 +168,29 @@ static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cu
             twf[q] = make_float2((float)w.real(), (float)w.imag());
         }
         v.logN = logN;
+        if (N >= 512 && N <= 2048) {
+            // lane l, register r of the four-step transform holds frequency
+            // bitrev(r) + (N/32) bitrev5(l) after the forward pass; its middle
+            // twiddle is exp(-2 pi i l bitrev(r) / N)
+            const int L = N / 32, bits = logN - 5;
+            auto brev = [](int x, int nb) {
+                int r = 0;
+                for (int i = 0; i < nb; i++) r = (r << 1) | ((x >> i) & 1);
+                return r;
+            };
+            std::vector<float2> Hp((size_t)N), Tw((size_t)N);
+            for (int r = 0; r < L; r++)
+                for (int l = 0; l < 32; l++) {
+                    const int k2 = brev(r, bits), k = k2 + L * brev(l, 5);
+                    Hp[(size_t)r * 32 + l] = Hf[k];
+                    const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * (double)(l * k2) / (double)N);
+                    Tw[(size_t)r * 32 + l] = make_float2((float)w.real(), (float)w.imag());
+                }
+            RN_CUDA_TRY(cudaMalloc(&v.d_Hp, sizeof(float2) * N));
+            RN_CUDA_TRY(cudaMalloc(&v.d_Tw, sizeof(float2) * N));
+            RN_CUDA_TRY(cudaMemcpyAsync(v.d_Hp, Hp.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
+            RN_CUDA_TRY(cudaMemcpyAsync(v.d_Tw, Tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
+        }
         RN_CUDA_TRY(cudaMalloc(&v.d_H, sizeof(float2) * N));
         RN_CUDA_TRY(cudaMalloc(&v.d_tw, sizeof(float2) * (N / 2)));
         RN_CUDA_TRY(cudaMemcpyAsync(v.d_H, Hf.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
@@ -381,6 +408,174 @@ __global__ void __launch_bounds__(kFftThreads, 2) filter_fft_kernel(float* __res
     }
 }
 
+// Register four-step FFT filter (N = 32 L, L = 16, 32 or 64 values per
+// lane): a warp holds one complex signal (two views as real and imaginary
+// parts), element n = lane + 32 r in register r of its lane.  Forward: an
+// L-point decimation-in-frequency transform in each lane's registers, the
+// middle twiddles exp(-2 pi i lane k2 / N), and a 32-point
+// decimation-in-frequency transform across the lanes by shuffles; the
+// spectrum then sits in bit-reversed order in both indices, where it is
+// multiplied by the kernel's spectrum stored in that order.  The inverse runs
+// the same steps backwards (decimation in time, conjugate twiddles) and
+// returns the signal in its original registers.  No shared-memory passes: a
+// CTA stages 16 views of its sinogram plane through shared memory only to
+// load and store them coalesced.
+constexpr int kRegViews = 16;   // views per CTA (8 warps, two views each)
+
+template <int L>
+struct RegFftTw {
+    float2 local[L / 2];   // exp(-2 pi i k / L), k < L/2
+    float2 w32[16];        // exp(-2 pi i k / 32), k < 16
+};
+
+template <int L>
+__device__ __forceinline__ void reg_local_dif(float2 (&v)[L], const RegFftTw<L>& t) {
+#pragma unroll
+    for (int h = L / 2; h >= 1; h >>= 1) {
+#pragma unroll
+        for (int i = 0; i < L; i++) {
+            if (i & h) continue;
+            const float2 a = v[i], b = v[i + h];
+            v[i] = c_add(a, b);
+            const int k = (i & (h - 1)) * (L / (2 * h));
+            v[i + h] = k == 0 ? c_sub(a, b) : c_mul(c_sub(a, b), t.local[k]);
+        }
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void reg_local_dit_inv(float2 (&v)[L], const RegFftTw<L>& t) {
+#pragma unroll
+    for (int h = 1; h < L; h <<= 1) {
+#pragma unroll
+        for (int i = 0; i < L; i++) {
+            if (i & h) continue;
+            const int k = (i & (h - 1)) * (L / (2 * h));
+            const float2 a = v[i], b = k == 0 ? v[i + h] : c_mulc(v[i + h], t.local[k]);
+            v[i] = c_add(a, b);
+            v[i + h] = c_sub(a, b);
+        }
+    }
+}
+
+__device__ __forceinline__ float2 shfl_xor2(float2 a, int m) {
+    return make_float2(__shfl_xor_sync(0xffffffffu, a.x, m), __shfl_xor_sync(0xffffffffu, a.y, m));
+}
+
+template <int L>
+__global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ out, const float* __restrict__ prj,
+                                                           const float2* __restrict__ Hp,
+                                                           const float2* __restrict__ Tw,
+                                                           const float* __restrict__ pw,
+                                                           const float* __restrict__ sw, int nu, int nview, int nv,
+                                                           int nc, int nplane_total, float scale, RegFftTw<L> tw) {
+    extern __shared__ float tile[];            // [nu][kRegViews + 1]
+    constexpr int TS = kRegViews + 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // this lane's twiddle in each cross-lane stage: exp(-2 pi i (lane mod h) / 2h)
+    float2 wl[5];
+#pragma unroll
+    for (int s = 0; s < 5; s++) {
+        const int h = 1 << s;
+        wl[s] = tw.w32[(lane & (h - 1)) * (16 / h)];
+    }
+    const long long su = (long long)nview * nv * nc, sview = (long long)nv * nc;
+    const int v0 = blockIdx.x * kRegViews;
+    for (int plane = blockIdx.y; plane < nplane_total; plane += gridDim.y) {
+        const int b = plane / (nv * nc);
+        const int rem = plane - b * nv * nc;
+        const long long off = (long long)b * nu * nview * nv * nc + rem;
+        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
+            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
+            float x = 0.f;
+            if (view < nview) {
+                x = prj[off + (long long)n * su + (long long)view * sview] * pw[n];
+                if (sw) x *= sw[(long long)n * nview + view];
+            }
+            tile[n * TS + vv] = x;
+        }
+        __syncthreads();
+        float2 v[L];
+#pragma unroll
+        for (int r = 0; r < L; r++) {
+            const int n = lane + 32 * r;
+            v[r] = n < nu ? make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1]) : make_float2(0.f, 0.f);
+        }
+        // forward
+        reg_local_dif<L>(v, tw);
+#pragma unroll
+        for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
+#pragma unroll
+        for (int s = 4; s >= 0; s--) {
+            const int h = 1 << s;
+            const bool up = (lane & h) != 0;
+#pragma unroll
+            for (int r = 0; r < L; r++) {
+                const float2 p = shfl_xor2(v[r], h);
+                v[r] = up ? c_mul(c_sub(p, v[r]), wl[s]) : c_add(v[r], p);
+            }
+        }
+        // the kernel's spectrum (scaled by 1/N), then the inverse
+#pragma unroll
+        for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Hp + r * 32 + lane));
+#pragma unroll
+        for (int s = 0; s < 5; s++) {
+            const int h = 1 << s;
+            const bool up = (lane & h) != 0;
+#pragma unroll
+            for (int r = 0; r < L; r++) {
+                const float2 t = up ? c_mulc(v[r], wl[s]) : v[r];
+                const float2 p = shfl_xor2(t, h);
+                v[r] = up ? c_sub(p, t) : c_add(v[r], p);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < L; r++) v[r] = c_mulc(v[r], __ldg(Tw + r * 32 + lane));
+        reg_local_dit_inv<L>(v, tw);
+        // each warp writes back only its own two columns
+#pragma unroll
+        for (int r = 0; r < L; r++) {
+            const int n = lane + 32 * r;
+            if (n < nu) {
+                tile[n * TS + 2 * warp] = v[r].x * scale;
+                tile[n * TS + 2 * warp + 1] = v[r].y * scale;
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
+            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
+            if (view < nview) out[off + (long long)n * su + (long long)view * sview] = tile[n * TS + vv];
+        }
+        __syncthreads();   // the next plane refills the tile
+    }
+}
+
+template <int L>
+static int launch_filter_reg(float* d_out, const float* d_prj, const FilterVal& fv, const float* d_sw, int nu,
+                             int nview, int nv, int nc, int nplanes, unsigned grid_planes, float scale,
+                             cudaStream_t st) {
+    RegFftTw<L> tw;
+    for (int k = 0; k < L / 2; k++) {
+        const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / (double)L);
+        tw.local[k] = make_float2((float)w.real(), (float)w.imag());
+    }
+    for (int k = 0; k < 16; k++) {
+        const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / 32.0);
+        tw.w32[k] = make_float2((float)w.real(), (float)w.imag());
+    }
+    const size_t smem = sizeof(float) * (size_t)nu * (kRegViews + 1);
+    RN_CUDA_TRY(cudaFuncSetAttribute(filter_reg_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((nview + kRegViews - 1) / kRegViews), grid_planes);
+    filter_reg_kernel<L><<<grid, 256, smem, st>>>(d_out, d_prj, fv.d_Hp, fv.d_Tw, fv.d_pw, d_sw, nu, nview, nv, nc,
+                                                  nplanes, scale, tw);
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+// 0 = the register four-step kernel where it applies (the default), 1 = the
+// shared-memory FFT kernel, 2 = the direct product (for comparisons)
+static int g_filter_form = 0;
+
 int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int nview, int nv, float da,
                   float off_a, float dsd, float dso, int typeFilter, int fan, cudaStream_t st,
                   const float* d_sw = nullptr) {
@@ -397,7 +592,13 @@ int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int 
     const long long nplanes = (long long)nb * nv * nc;
     if (nplanes > INT_MAX) return set_error(RN_ERR_ARG, "filter: too many sinogram planes");
     const unsigned grid_planes = (unsigned)std::min<long long>(nplanes, 65535);
-    if (fv.logN > 0) {
+    if (g_filter_form == 0 && fv.d_Hp) {
+        const int N = 1 << fv.logN;
+        if (N == 2048) return launch_filter_reg<64>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        if (N == 1024) return launch_filter_reg<32>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        return launch_filter_reg<16>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+    }
+    if (fv.logN > 0 && g_filter_form <= 1) {
         // S signals (2S views) per CTA: ~64 KB of shared memory at N = 2048
         const int N = 1 << fv.logN;
         const int S = std::max(1, std::min(16, 8192 / N));
@@ -771,6 +972,13 @@ int rn_filter(float* d_out, const float* d_prj, int nBatches, int nChannels, int
     if (!d_out || !d_prj) return set_error(RN_ERR_ARG, "null argument");
     return filter_device(d_out, d_prj, nBatches, nChannels, nu, nview, nv, da, off_a, dsd, dso, typeFilter, fan,
                          (cudaStream_t)stream);
+}
+
+int rn_filter_set_form(int form) {
+    clear_error();
+    if (form < 0 || form > 2) return set_error(RN_ERR_ARG, "filter form must be 0, 1 or 2");
+    g_filter_form = form;
+    return RN_OK;
 }
 
 int rn_filter_weighted(float* d_out, const float* d_prj, const float* d_w, int nBatches, int nChannels, int nu,

@@ -228,6 +228,7 @@ class StreamedFanPair:
         self.h2d_stream = torch.cuda.Stream(self.device)
         self.d2h_stream = torch.cuda.Stream(self.device)
         self.done = torch.cuda.Event()
+        self.inputs_read = torch.cuda.Event()
         self.calls = 0
 
     def updates(self) -> int:
@@ -235,8 +236,11 @@ class StreamedFanPair:
 
     def __call__(self, host_img: torch.Tensor, host_out: torch.Tensor) -> torch.cuda.Event:
         """host_img, host_out: pinned float32 [S, nx, ny] host tensors.  Enqueues
-        the work and returns an event that completes when host_out is written;
-        host_img may be reused once the call after next has been enqueued."""
+        the work and returns an event that completes when host_out is written.
+        The copies are asynchronous: host_img may be overwritten only after
+        ``self.inputs_read`` (recorded after this call's host-to-device copies)
+        or the returned event has completed, and host_out read only after the
+        returned event has."""
         if host_img.shape[0] != self.nslices or host_out.shape[0] != self.nslices:
             raise ValueError("host tensors must hold one [nx, ny] image per slice")
         comp = torch.cuda.current_stream(self.device)
@@ -257,6 +261,7 @@ class StreamedFanPair:
             with torch.cuda.stream(self.d2h_stream):
                 host_out[g.s0:g.s1].copy_(bf.b, non_blocking=True)
                 bf.d2h.record(self.d2h_stream)
+        self.inputs_read.record(self.h2d_stream)
         self.done.record(self.d2h_stream)
         return self.done
 

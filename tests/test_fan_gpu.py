@@ -191,6 +191,26 @@ def test_filter_fft_lengths_match_oracle(nu, rng):
         assert rel_l2(got, O.filter_sino(s, g, tf)) <= TOL, (nu, tf)
 
 
+@pytest.mark.parametrize("nu", [150, 300, 736, 888])
+def test_filter_kernel_forms_agree(nu, rng):
+    """The register four-step FFT (transform lengths 512-2048), the
+    shared-memory FFT and the direct product give the same filtered
+    sinograms; with short-scan weights too."""
+    import torch
+    from reconnet_b200 import _native as N
+    from reconnet_b200.torch_ops import FanGeometry, filter_sino, shortscan_weights
+    geom = FanGeometry(nu=nu, da=0.9 / nu, off_a=0.25)
+    s = torch.from_numpy(rng.random((2, nu, 67, 1, 1)).astype(np.float32)).cuda()
+    outs = []
+    try:
+        for form in (0, 1, 2):
+            N.check(N.lib.rn_filter_set_form(form))
+            outs.append(filter_sino(s, geom, 2).cpu().numpy())
+    finally:
+        N.lib.rn_filter_set_form(0)
+    assert rel_l2(outs[0], outs[2]) <= 2e-6 and rel_l2(outs[1], outs[2]) <= 2e-6
+
+
 def test_filter_more_planes_than_grid_rows(rng):
     """More (batch, row, channel) planes than one grid dimension holds
     (65,535): the kernels loop over the planes."""
