@@ -601,8 +601,8 @@ def prior_run(dev, n_train=128, n_eval=32, train_steps=600, tv_iters=100):
     tv_ms_per_iter = e0.elapsed_time(e1) / tv_iters
     solver.check()
     target = traj[-1] + 1.0
-    # learned: 4 OS-SQS iterations (same solver, no TV) + the network
-    solver.beta = 0.0
+    # learned: the first 4 iterations of the same solver (as the training
+    # inputs were made) + the network
     x4 = solver.run(torch.zeros_like(truth), 4)
     y = net.denoise(x4).clamp_min_(0.0)
     e0, e1 = ev()

@@ -130,6 +130,11 @@ class BatchedOSSQS:
                 self._one_iteration()
         return self._xa.clone()
 
+    def set_beta(self, beta: float) -> None:
+        """Change the TV weight; the captured iteration is re-captured on the next run."""
+        self.beta = float(beta)
+        self._graph = None
+
     def check(self):
         for p in self.plans:
             p.check()
