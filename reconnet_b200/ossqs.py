@@ -61,8 +61,8 @@ class BatchedOSSQS:
         angles = np.asarray(angles, np.float32)
         offs = np.concatenate([[0], np.cumsum(self.counts)])
         nu = geom.nu
-        # full plan (normaliser) and one ragged plan per subset
-        self.full = FanPlan(geom, angles, nbatches=self.S, nview_per_slice=self.counts, device=self.device)
+        # one ragged plan per subset
+        self.img_shape = (self.S, geom.nx, geom.ny)
         self.plans, self.sub_b, self.sub_w = [], [], []
         for m in range(self.M):
             cnt, ang, idx = [], [], []
@@ -85,14 +85,20 @@ class BatchedOSSQS:
             self.tuning = choice
         else:
             self.tuning = self.plans[0].tuning()
-        # normImg = A^T W A 1 over all views (the same pair)
-        ones = torch.ones(self.full.img_shape, device=self.device)
-        a1 = self.full.project(ones, siddon=self.type == N.RN_TYPE_SIDDON)
-        self.norm_img = self.full.backproject(a1 * weights.reshape(-1), self.type)
+        # normImg = A^T W A 1 over all views (the same pair), summed over the
+        # subsets in FP64: each subset's backprojection accumulates its own
+        # ~1/M of the views in FP32 registers, the sum across subsets is FP64
+        ones = torch.ones(self.img_shape, device=self.device)
+        siddon = self.type == N.RN_TYPE_SIDDON
+        norm = torch.zeros(self.img_shape, dtype=torch.float64, device=self.device)
+        for m in range(self.M):
+            a1 = self.plans[m].project(ones, siddon=siddon)
+            norm += self.plans[m].backproject(a1 * self.sub_w[m], self.type).double()
+        self.norm_img = norm.float()
         self.use_graph = use_graph
         self._graph = None
-        self._xa = torch.zeros(self.full.img_shape, device=self.device)
-        self._xb = torch.zeros(self.full.img_shape, device=self.device)
+        self._xa = torch.zeros(self.img_shape, device=self.device)
+        self._xb = torch.zeros(self.img_shape, device=self.device)
 
     def _one_iteration(self):
         src, dst = self._xa, self._xb
