@@ -22,17 +22,21 @@
 // The FP64 CPU oracle (oracle/oracle.cpp, cyl_view_terms) evaluates the same
 // sum voxel by voxel.
 //
-// Forward projection: a warp owns one detector column u and 31 rows (32 row
-// edges on its lanes).  On each plane the column's lateral footprint covers
-// 1-3 voxel columns, the same for every lane; for each of them the warp loads
-// the z-run of voxels its rows span (coalesced), scans it (FP32 prefix sums
-// relative to the run's start) and evaluates the prefix at each lane's row
-// edge; a row's integral over z is the difference of two neighbouring lanes'
-// values (one shuffle), so every edge is evaluated once and no prefix table
-// is kept in memory.  The volume itself stays in L2 between views.
+// Forward projection: a warp owns one detector column u and 32 rows: its
+// lanes hold the rows' lower edges, and the 33rd edge, closing lane 31's row,
+// is evaluated by every lane alongside (it needs two more shuffles).  On each
+// plane the column's lateral footprint covers 1-3 voxel columns, the same
+// for every lane; for each of them the warp loads the z-run of voxels its
+// rows span (coalesced), scans it (FP32 prefix sums relative to the run's
+// start) and evaluates the prefix at each lane's row edge; a row's integral
+// over z is the difference of two neighbouring lanes' values (one shuffle),
+// so every edge is evaluated once and no prefix table is kept in memory.  The
+// volume itself stays in L2 between views.
 //
 // Backprojection: per view, the sinogram column u becomes a row table of
-// prefix sums of L p along v (cyl_table_kernel).  A thread owns a voxel; a
+// prefix sums of L p along v (cyl_table_kernel).  The gather runs in
+// launches over chunks of views whose tables stay in L2 (each voxel adds its
+// chunk's sum to the previous chunks').  A thread owns a voxel; a
 // warp owns 32 consecutive voxels along z of one (x, y) column, so the
 // candidate cells u (the columns whose footprint meets the voxel's lateral
 // extent on its plane) are the same for every lane and the loop over them
@@ -64,7 +68,7 @@ struct CylDims {
 };
 
 constexpr int kCylFpWarps = 8;   // detector columns per forward-projection CTA
-constexpr int kCylRows = 31;     // detector rows per warp (32 row edges)
+constexpr int kCylRows = 32;     // detector rows per warp (its 32 lanes' edges and one more)
 constexpr int kCylBpWarps = 8;   // voxel columns per backprojection CTA
 
 __device__ __forceinline__ float warp_scan_f(float v, int lane) {
@@ -89,6 +93,7 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
     const int g0 = blockIdx.y * kCylRows;
     const int e = g0 + lane;
     const float s_lane = sedge[min(e, d.nv)];
+    const float s_top = sedge[min(g0 + 32, d.nv)];           // the 33rd edge, closing lane 31's row
     for (int bz = blockIdx.z; bz < d.nview * d.nb; bz += gridDim.z) {
         const int iv = bz % d.nview, b = bz / d.nview;
         const CylView V = views[iv];
@@ -99,46 +104,57 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
         const double smain = xc ? V.sy : V.sx, slat = xc ? V.sx : V.sy;
         const double R0 = redge[(long long)iv * (d.nu + 1) + u], R1 = redge[(long long)iv * (d.nu + 1) + u + 1];
         const float inp = inplane[(long long)iv * d.nu + u];
-        const double lat_off = nlat / 2.0 - clat / dlat;
+        const double inv_dlat = 1.0 / dlat;
+        const double lat_off = nlat / 2.0 - clat * inv_dlat;
         const float inv_dz = (float)(1.0 / d.dz), zoff = (float)(d.nz / 2.0 - d.cz / d.dz);
+        // footprint width x in-plane distance: |R1 - R0| inp D^2 / dlat
+        const float wfac = (float)(fabs(R1 - R0) * inv_dlat) * inp;
         const float* vb = vol + (long long)b * d.vol_stride;
         float acc = 0.f;
         for (int k = 0; k < nplane; k++) {
             const double D = (k + 0.5 - nplane / 2.0) * dmain + cmain - smain;
-            const double la = (slat + R0 * D) / dlat + lat_off, lb = (slat + R1 * D) / dlat + lat_off;
+            const double la = fma(R0, D, slat) * inv_dlat + lat_off, lb = fma(R1, D, slat) * inv_dlat + lat_off;
             const double lo = fmin(la, lb), hi = fmax(la, lb);
             const int i0 = (int)fmax(floor(lo), 0.0), i1 = (int)fmin(floor(hi), (double)(nlat - 1));
             if (i0 > i1) continue;
-            const float dc = (float)fabs(D) * inp;
+            const float aD = (float)fabs(D);
+            const float dc = aD * inp;
             const float zeta = s_lane * dc * inv_dz + zoff;
-            const float z_first = __shfl_sync(0xffffffffu, zeta, 0), z_last = __shfl_sync(0xffffffffu, zeta, 31);
-            if (z_last <= 0.f || z_first >= (float)d.nz) continue;   // every row edge outside the volume
-            const float zf = floorf(zeta);
+            const float ztop = s_top * dc * inv_dz + zoff;
+            const float z_first = __shfl_sync(0xffffffffu, zeta, 0);
+            if (ztop <= 0.f || z_first >= (float)d.nz) continue;   // every row edge outside the volume
+            const float zf = floorf(zeta), ztf = floorf(ztop);
             const int mabs = (int)fminf(fmaxf(zf, -1.f), (float)d.nz);
+            const int mtop = (int)fminf(fmaxf(ztf, -1.f), (float)d.nz);
             const int jlo = (int)fmaxf(floorf(z_first), 0.f);
-            const int jhi = min(d.nz, __shfl_sync(0xffffffffu, mabs, 31) + 1);
-            float Q = 0.f;
+            const int jhi = min(d.nz, mtop + 1);
+            float Q = 0.f, Qt = 0.f;
             for (int i = i0; i <= i1; i++) {
                 const float ox = (float)(fmin(hi, i + 1.0) - fmax(lo, (double)i));
                 const float* col = vb + (long long)(xc ? (i * d.ny + k) : (k * d.ny + i)) * d.nz;
-                float P = 0.f, carry = 0.f;
+                float P = 0.f, Pt = 0.f, carry = 0.f;
                 for (int jw = jlo; jw < jhi; jw += 32) {
                     const int j = jw + lane;
                     const float f = j < jhi ? __ldg(col + j) : 0.f;
                     const float I = warp_scan_f(f, lane);
                     const float tot = __shfl_sync(0xffffffffu, I, 31);
-                    const int m = mabs - jw;
+                    const int m = mabs - jw, mt = mtop - jw;
                     const float Im = __shfl_sync(0xffffffffu, I, m & 31), fm = __shfl_sync(0xffffffffu, f, m & 31);
+                    const float It = __shfl_sync(0xffffffffu, I, mt & 31), ft = __shfl_sync(0xffffffffu, f, mt & 31);
                     if (m >= 0 && m < 32 && mabs < d.nz) P = carry + (Im - fm) + (zeta - zf) * fm;
+                    if (mt >= 0 && mt < 32 && mtop < d.nz) Pt = carry + (It - ft) + (ztop - ztf) * ft;
                     carry += tot;
                 }
                 if (mabs >= d.nz) P = carry;
+                if (mtop >= d.nz) Pt = carry;
                 Q = fmaf(ox, P, Q);
+                Qt = fmaf(ox, Pt, Qt);
             }
-            const float Qn = __shfl_down_sync(0xffffffffu, Q, 1);
-            acc = fmaf(Qn - Q, 1.0f / ((float)(hi - lo) * dc), acc);
+            float Qn = __shfl_down_sync(0xffffffffu, Q, 1);
+            if (lane == 31) Qn = Qt;
+            acc = fmaf(Qn - Q, __frcp_rn(wfac * aD * aD), acc);
         }
-        if (lane < kCylRows && e < d.nv) {
+        if (e < d.nv) {
             const float ds = sedge[e + 1] - sedge[e];
             const float L = (float)dmain * inp * rowlen[e];
             prj[(long long)b * d.prj_stride + ((long long)u * d.nview + iv) * d.nv + e] = acc * L * (float)d.dz / ds;
@@ -180,7 +196,9 @@ __device__ __forceinline__ float row_prefix(const float2* __restrict__ t, float 
 __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restrict__ vol, const float2* __restrict__ tab,
                                                                  const CylView* __restrict__ views,
                                                                  const double* __restrict__ redge,
-                                                                 const float* __restrict__ inplane, CylDims d) {
+                                                                 const double* __restrict__ inv_dr,
+                                                                 const float* __restrict__ inv_inp, CylDims d,
+                                                                 int v_begin, int v_end, int accumulate) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long column = (long long)blockIdx.x * kCylBpWarps + warp;
     if (column >= (long long)d.nx * d.ny) return;              // whole warp
@@ -193,7 +211,7 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
     const float dsd_dv = (float)(d.dsd / d.dv);
     const double two_pi = 6.283185307179586;
     float acc = 0.f;
-    for (int iv = 0; iv < d.nview; iv++) {
+    for (int iv = v_begin; iv < v_end; iv++) {
         const CylView V = views[iv];
         const bool xc = V.xcls != 0;
         const int k = xc ? iy : ix, i = xc ? ix : iy;
@@ -215,18 +233,21 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
             e01[q] = -a / (float)d.da - (float)d.off_a + (d.nu - 1) * 0.5f + 0.5f;
         }
         const float elo = fminf(e01[0], e01[1]) - 0.01f, ehi = fmaxf(e01[0], e01[1]) + 0.01f;
-        const int ulo = (int)fmaxf(floorf(elo), 0.f), uhi = (int)fminf(floorf(ehi), (float)(d.nu - 1));
-        const double lat_off = nlat / 2.0 - clat / dlat;
+        const int ulo = (int)fmaxf(floorf(elo), 0.f), uhi = (int)fminf(floorf(ehi), (double)(d.nu - 1));
+        const double inv_dlat = 1.0 / dlat;
+        const double lat_off = nlat / 2.0 - clat * inv_dlat;
+        // footprint width on this plane: |R1 - R0| |D| / dlat
+        const double wD = dlat / fabs(D);
+        const float inv_aD = (float)(1.0 / fabs(D));
         const double* Rv = redge + (long long)iv * (d.nu + 1);
         const float2* tv = tab + ((long long)b * d.nview + iv) * (long long)d.nu * (d.nv + 1);
         for (int u = ulo; u <= uhi; u++) {
-            const double la = (slat + Rv[u] * D) / dlat + lat_off, lb = (slat + Rv[u + 1] * D) / dlat + lat_off;
+            const double la = fma(Rv[u], D, slat) * inv_dlat + lat_off, lb = fma(Rv[u + 1], D, slat) * inv_dlat + lat_off;
             const double lo = fmin(la, lb), hi = fmax(la, lb);
             const double ov = fmin(hi, i + 1.0) - fmax(lo, (double)i);
             if (ov <= 0) continue;
-            const float w = (float)(ov / (hi - lo));
-            const float dc = (float)fabs(D) * inplane[(long long)iv * d.nu + u];
-            const float inv = dsd_dv / dc;
+            const float w = (float)(ov * wD * inv_dr[(long long)iv * d.nu + u]);
+            const float inv = dsd_dv * inv_aD * inv_inp[(long long)iv * d.nu + u];
             const float r_lo = fmaf(z_lo, inv, rho0), r_hi = fmaf(z_hi, inv, rho0);
             // the warp's z run against the detector rows: skip if it misses them
             const float first = __shfl_sync(0xffffffffu, r_lo, 0), last = __shfl_sync(0xffffffffu, r_hi, 31);
@@ -235,7 +256,10 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
             acc = fmaf(w, row_prefix(t, r_hi, d.nv) - row_prefix(t, r_lo, d.nv), acc);
         }
     }
-    if (j < d.nz) vol[(long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz + j] = acc;
+    if (j < d.nz) {
+        float* o = vol + (long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz + j;
+        *o = accumulate ? *o + acc : acc;
+    }
 }
 
 }  // namespace rn
@@ -251,6 +275,9 @@ struct rn_cyl_plan {
     float* d_inplane = nullptr;   // [nview][nu] sqrt(1 + R_c^2) of each cell's central ray
     float* d_sedge = nullptr;     // [nv+1] row-edge rise per mm of in-plane distance
     float* d_rowlen = nullptr;    // [nv] sqrt(1 + s_c^2) of each row's central ray
+    double* d_invdr = nullptr;    // [nview][nu] 1 / |R_{u+1} - R_u|
+    float* d_invinp = nullptr;    // [nview][nu] 1 / sqrt(1 + R_c^2)
+    int bp_chunk = 0;             // views per backprojection launch (their row tables stay in L2)
     float2* d_tab = nullptr;      // backprojection row tables [nb][nview][nu][nv+1]
     long long launches = 0;
 };
@@ -288,7 +315,8 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
     const int nu = g->nu, nv = g->nv, nview = g->nview;
     std::vector<CylView> views(nview);
     std::vector<double> redge((size_t)nview * (nu + 1));
-    std::vector<float> inplane((size_t)nview * nu), sedge(nv + 1), rowlen(nv);
+    std::vector<float> inplane((size_t)nview * nu), sedge(nv + 1), rowlen(nv), invinp((size_t)nview * nu);
+    std::vector<double> invdr((size_t)nview * nu);
     for (int iv = 0; iv < nview; iv++) {
         const float tf = host_deg[iv];
         const double t = (double)tf;
@@ -303,6 +331,9 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
         for (int u = 0; u < nu; u++) {
             const double Rc = slope((-(u - (nu - 1) / 2.0) - g->off_a) * g->da);
             inplane[(size_t)iv * nu + u] = (float)std::sqrt(1 + Rc * Rc);
+            invinp[(size_t)iv * nu + u] = (float)(1.0 / std::sqrt(1 + Rc * Rc));
+            invdr[(size_t)iv * nu + u] =
+                1.0 / std::fabs(redge[(size_t)iv * (nu + 1) + u + 1] - redge[(size_t)iv * (nu + 1) + u]);
         }
     }
     for (int e = 0; e <= nv; e++) sedge[e] = (float)(((e - 0.5) - (nv - 1) / 2.0 + g->off_v) * g->dv / g->dsd);
@@ -322,12 +353,19 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
     if ((e = cudaMalloc(&p->d_sedge, sizeof(float) * sedge.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_rowlen, sizeof(float) * rowlen.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_tab, sizeof(float2) * tab_elems)) != cudaSuccess) return fail(e, "cyl: row tables");
+    if ((e = cudaMalloc(&p->d_invdr, sizeof(double) * invdr.size())) != cudaSuccess) return fail(e, "cyl: cells");
+    if ((e = cudaMalloc(&p->d_invinp, sizeof(float) * invinp.size())) != cudaSuccess) return fail(e, "cyl: cells");
     if ((e = cudaMemcpyAsync(p->d_views, views.data(), sizeof(CylView) * nview, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_redge, redge.data(), sizeof(double) * redge.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_inplane, inplane.data(), sizeof(float) * inplane.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_sedge, sedge.data(), sizeof(float) * sedge.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(p->d_rowlen, rowlen.data(), sizeof(float) * rowlen.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        (e = cudaMemcpyAsync(p->d_rowlen, rowlen.data(), sizeof(float) * rowlen.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(p->d_invdr, invdr.data(), sizeof(double) * invdr.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(p->d_invinp, invinp.data(), sizeof(float) * invinp.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return fail(e, "cyl: table upload");
+    // backprojection launches take views in chunks whose row tables (nu x
+    // (nv + 1) float2 each) fill about 24 MB, well inside the 126 MB L2
+    p->bp_chunk = (int)std::max<long long>(1, (24ll << 20) / ((long long)nu * (nv + 1) * 8 * g->nBatches));
     // the host vectors go out of scope: finish the copies first
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cyl: table upload");
     *out = p;
@@ -342,6 +380,8 @@ extern "C" int rn_cyl_plan_destroy(rn_cyl_plan* p) {
     cudaFree(p->d_sedge);
     cudaFree(p->d_rowlen);
     cudaFree(p->d_tab);
+    cudaFree(p->d_invdr);
+    cudaFree(p->d_invinp);
     delete p;
     return RN_OK;
 }
@@ -375,8 +415,12 @@ extern "C" int rn_cyl_backproject(rn_cyl_plan* p, float* d_vol, const float* d_p
     if (d.nb > 65535) return set_error(RN_ERR_ARG, "cyl: too many batches");
     dim3 grid((unsigned)(((long long)d.nx * d.ny + kCylBpWarps - 1) / kCylBpWarps), (unsigned)((d.nz + 31) / 32),
               (unsigned)d.nb);
-    cyl_bp_kernel<<<grid, 32 * kCylBpWarps, 0, st>>>(d_vol, p->d_tab, p->d_views, p->d_redge, p->d_inplane, d);
-    p->launches++;
-    RN_CUDA_TRY(cudaGetLastError());
+    for (int v0 = 0; v0 < d.nview; v0 += p->bp_chunk) {
+        const int v1 = std::min(d.nview, v0 + p->bp_chunk);
+        cyl_bp_kernel<<<grid, 32 * kCylBpWarps, 0, st>>>(d_vol, p->d_tab, p->d_views, p->d_redge, p->d_invdr,
+                                                        p->d_invinp, d, v0, v1, v0 > 0 ? 1 : 0);
+        p->launches++;
+        RN_CUDA_TRY(cudaGetLastError());
+    }
     return RN_OK;
 }

@@ -99,8 +99,11 @@ struct FilterVal {
     int logN = 0;
     float2* d_H = nullptr;  // [N]
     float2* d_tw = nullptr; // [N/2] exp(-2 pi i q / N)
-    // register four-step form (N = 512, 1024, 2048): the spectrum and the
-    // middle twiddles in the registers' order, [N/32][32] (entry [r][lane])
+    // register four-step form (N = 512, 1024, 2048, run as two transforms of
+    // M = N/2 points): the even- and odd-frequency halves of the spectrum in
+    // the registers' order, [2][M/32][32] (entry [half][r][lane]); then the
+    // M-point middle twiddles [M/32][32] followed by the odd half's
+    // pre-twiddles exp(-2 pi i n / N), n = lane + 32 r < M
     float2* d_Hp = nullptr;
     float2* d_Tw = nullptr;
 };
@@ -169,10 +172,13 @@ static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cu
         }
         v.logN = logN;
         if (N >= 512 && N <= 2048) {
-            // lane l, register r of the four-step transform holds frequency
-            // bitrev(r) + (N/32) bitrev5(l) after the forward pass; its middle
-            // twiddle is exp(-2 pi i l bitrev(r) / N)
-            const int L = N / 32, bits = logN - 5;
+            // the signal occupies n < nu <= M = N/2, so the N-point spectrum
+            // splits into X[2k] = FFT_M(x)[k] and X[2k+1] = FFT_M(x
+            // exp(-2 pi i n / N))[k].  Lane l, register r of the M-point
+            // four-step transform holds frequency bitrev(r) + (M/32) bitrev5(l)
+            // after the forward pass; its middle twiddle is
+            // exp(-2 pi i l bitrev(r) / M)
+            const int M = N / 2, L = M / 32, bits = logN - 6;
             auto brev = [](int x, int nb) {
                 int r = 0;
                 for (int i = 0; i < nb; i++) r = (r << 1) | ((x >> i) & 1);
@@ -182,9 +188,12 @@ static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cu
             for (int r = 0; r < L; r++)
                 for (int l = 0; l < 32; l++) {
                     const int k2 = brev(r, bits), k = k2 + L * brev(l, 5);
-                    Hp[(size_t)r * 32 + l] = Hf[k];
-                    const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * (double)(l * k2) / (double)N);
+                    Hp[(size_t)r * 32 + l] = Hf[2 * k];
+                    Hp[(size_t)M + r * 32 + l] = Hf[2 * k + 1];
+                    const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * (double)(l * k2) / (double)M);
                     Tw[(size_t)r * 32 + l] = make_float2((float)w.real(), (float)w.imag());
+                    const std::complex<double> q = std::polar(1.0, -2.0 * M_PI * (double)(l + 32 * r) / (double)N);
+                    Tw[(size_t)M + r * 32 + l] = make_float2((float)q.real(), (float)q.imag());
                 }
             RN_CUDA_TRY(cudaMalloc(&v.d_Hp, sizeof(float2) * N));
             RN_CUDA_TRY(cudaMalloc(&v.d_Tw, sizeof(float2) * N));
@@ -408,11 +417,16 @@ __global__ void __launch_bounds__(kFftThreads, 2) filter_fft_kernel(float* __res
     }
 }
 
-// Register four-step FFT filter (N = 32 L, L = 16, 32 or 64 values per
-// lane): a warp holds one complex signal (two views as real and imaginary
-// parts), element n = lane + 32 r in register r of its lane.  Forward: an
-// L-point decimation-in-frequency transform in each lane's registers, the
-// middle twiddles exp(-2 pi i lane k2 / N), and a 32-point
+// Register four-step FFT filter.  The zero-padded signal of N points (N =
+// 512, 1024, 2048) is nonzero on its first half only, so its spectrum is two
+// M = N/2 point transforms: the even frequencies are FFT_M(x) and the odd ones
+// FFT_M(x w), w = exp(-2 pi i n / N).  Each is filtered by its half of the
+// kernel's spectrum and inverted, and the outputs (needed for n < nu <= M
+// only) are y = y_even + conj(w) y_odd.  A warp runs both halves in turn on
+// one complex signal (two views as real and imaginary parts), element n =
+// lane + 32 r in register r of its lane (M = 32 L).  An M-point transform:
+// an L-point decimation-in-frequency transform in each lane's registers, the
+// middle twiddles exp(-2 pi i lane k2 / M), and a 32-point
 // decimation-in-frequency transform across the lanes by shuffles; the
 // spectrum then sits in bit-reversed order in both indices, where it is
 // multiplied by the kernel's spectrum stored in that order.  The inverse runs
@@ -469,9 +483,12 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
                                                            const float* __restrict__ pw,
                                                            const float* __restrict__ sw, int nu, int nview, int nv,
                                                            int nc, int nplane_total, float scale, RegFftTw<L> tw) {
-    extern __shared__ float tile[];            // [nu][kRegViews + 1]
-    constexpr int TS = kRegViews + 1;
+    extern __shared__ float tile[];            // [nu][kRegViews + 1], then [8 warps][nu] float2
+    constexpr int TS = kRegViews + 1, M = 32 * L;
+    const float2* __restrict__ Pre = Tw + M;   // exp(-2 pi i n / N), n < M
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the even half's output, held while the odd half runs
+    float2* ybuf = reinterpret_cast<float2*>(tile + ((nu * TS + 1) & ~1)) + (long long)warp * nu;
     // this lane's twiddle in each cross-lane stage: exp(-2 pi i (lane mod h) / 2h)
     float2 wl[5];
 #pragma unroll
@@ -485,6 +502,7 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
         const int b = plane / (nv * nc);
         const int rem = plane - b * nv * nc;
         const long long off = (long long)b * nu * nview * nv * nc + rem;
+#pragma unroll 4
         for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
             const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
             float x = 0.f;
@@ -495,53 +513,66 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
             tile[n * TS + vv] = x;
         }
         __syncthreads();
-        float2 v[L];
-#pragma unroll
-        for (int r = 0; r < L; r++) {
-            const int n = lane + 32 * r;
-            v[r] = n < nu ? make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1]) : make_float2(0.f, 0.f);
-        }
-        // forward
-        reg_local_dif<L>(v, tw);
-#pragma unroll
-        for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
-#pragma unroll
-        for (int s = 4; s >= 0; s--) {
-            const int h = 1 << s;
-            const bool up = (lane & h) != 0;
+#pragma unroll 1
+        for (int half = 0; half < 2; half++) {
+            float2 v[L];
 #pragma unroll
             for (int r = 0; r < L; r++) {
-                const float2 p = shfl_xor2(v[r], h);
-                v[r] = up ? c_mul(c_sub(p, v[r]), wl[s]) : c_add(v[r], p);
+                const int n = lane + 32 * r;
+                v[r] = n < nu ? make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1])
+                              : make_float2(0.f, 0.f);
+                if (half) v[r] = c_mul(v[r], __ldg(Pre + r * 32 + lane));
             }
-        }
-        // the kernel's spectrum (scaled by 1/N), then the inverse
+            // forward
+            reg_local_dif<L>(v, tw);
 #pragma unroll
-        for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Hp + r * 32 + lane));
+            for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
 #pragma unroll
-        for (int s = 0; s < 5; s++) {
-            const int h = 1 << s;
-            const bool up = (lane & h) != 0;
+            for (int s = 4; s >= 0; s--) {
+                const int h = 1 << s;
+                const bool up = (lane & h) != 0;
 #pragma unroll
-            for (int r = 0; r < L; r++) {
-                const float2 t = up ? c_mulc(v[r], wl[s]) : v[r];
-                const float2 p = shfl_xor2(t, h);
-                v[r] = up ? c_sub(p, t) : c_add(v[r], p);
+                for (int r = 0; r < L; r++) {
+                    const float2 p = shfl_xor2(v[r], h);
+                    v[r] = up ? c_mul(c_sub(p, v[r]), wl[s]) : c_add(v[r], p);
+                }
             }
-        }
+            // this half of the kernel's spectrum (scaled by 1/N), then the inverse
 #pragma unroll
-        for (int r = 0; r < L; r++) v[r] = c_mulc(v[r], __ldg(Tw + r * 32 + lane));
-        reg_local_dit_inv<L>(v, tw);
-        // each warp writes back only its own two columns
+            for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Hp + half * M + r * 32 + lane));
 #pragma unroll
-        for (int r = 0; r < L; r++) {
-            const int n = lane + 32 * r;
-            if (n < nu) {
-                tile[n * TS + 2 * warp] = v[r].x * scale;
-                tile[n * TS + 2 * warp + 1] = v[r].y * scale;
+            for (int s = 0; s < 5; s++) {
+                const int h = 1 << s;
+                const bool up = (lane & h) != 0;
+#pragma unroll
+                for (int r = 0; r < L; r++) {
+                    const float2 t = up ? c_mulc(v[r], wl[s]) : v[r];
+                    const float2 p = shfl_xor2(t, h);
+                    v[r] = up ? c_sub(p, t) : c_add(v[r], p);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < L; r++) v[r] = c_mulc(v[r], __ldg(Tw + r * 32 + lane));
+            reg_local_dit_inv<L>(v, tw);
+            if (half == 0) {
+#pragma unroll
+                for (int r = 0; r < L; r++)
+                    if (lane + 32 * r < nu) ybuf[lane + 32 * r] = v[r];
+            } else {
+                // each warp writes back only its own two columns
+#pragma unroll
+                for (int r = 0; r < L; r++) {
+                    const int n = lane + 32 * r;
+                    if (n < nu) {
+                        const float2 y = c_add(ybuf[n], c_mulc(v[r], __ldg(Pre + r * 32 + lane)));
+                        tile[n * TS + 2 * warp] = y.x * scale;
+                        tile[n * TS + 2 * warp + 1] = y.y * scale;
+                    }
+                }
             }
         }
         __syncthreads();
+#pragma unroll 4
         for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
             const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
             if (view < nview) out[off + (long long)n * su + (long long)view * sview] = tile[n * TS + vv];
@@ -563,7 +594,7 @@ static int launch_filter_reg(float* d_out, const float* d_prj, const FilterVal& 
         const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / 32.0);
         tw.w32[k] = make_float2((float)w.real(), (float)w.imag());
     }
-    const size_t smem = sizeof(float) * (size_t)nu * (kRegViews + 1);
+    const size_t smem = sizeof(float) * (((size_t)nu * (kRegViews + 1) + 1) & ~(size_t)1) + sizeof(float2) * 8 * nu;
     RN_CUDA_TRY(cudaFuncSetAttribute(filter_reg_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)((nview + kRegViews - 1) / kRegViews), grid_planes);
     filter_reg_kernel<L><<<grid, 256, smem, st>>>(d_out, d_prj, fv.d_Hp, fv.d_Tw, fv.d_pw, d_sw, nu, nview, nv, nc,
@@ -594,9 +625,9 @@ int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int 
     const unsigned grid_planes = (unsigned)std::min<long long>(nplanes, 65535);
     if (g_filter_form == 0 && fv.d_Hp) {
         const int N = 1 << fv.logN;
-        if (N == 2048) return launch_filter_reg<64>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
-        if (N == 1024) return launch_filter_reg<32>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
-        return launch_filter_reg<16>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        if (N == 2048) return launch_filter_reg<32>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        if (N == 1024) return launch_filter_reg<16>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        return launch_filter_reg<8>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
     }
     if (fv.logN > 0 && g_filter_form <= 1) {
         // S signals (2S views) per CTA: ~64 KB of shared memory at N = 2048

@@ -5,7 +5,8 @@ The kernels multiply BF16 operands exactly and accumulate in FP32, so with the
 oracle fed the same BF16-rounded operands: FP32 outputs agree to relative L2
 <= 1e-5; BF16 outputs agree with the oracle's result rounded to BF16 except
 where the two sides of a rounding boundary differ (<= 1e-3 relative L2, about
-one BF16 ulp on a few elements); the full network's gradients, which pass
+one BF16 ulp on a few elements); the full network's output, whose hidden
+activations are BF16, agrees to 1e-4; its gradients, which pass
 through BF16 activations and BF16 output gradients, agree to 2e-2."""
 import numpy as np
 import pytest
@@ -122,7 +123,10 @@ def test_network_gradients_match_oracle_chain(rng):
     for li in range(4):
         a.append(O.bf16_round(np.maximum(O.conv3x3(a[-1], W[li], B[li]), 0).astype(np.float32)))
     ref_out = O.conv3x3(a[4], W[4], B[4])[:, 0] + u
-    assert rel_l2(out.cpu().numpy(), ref_out) <= 1e-5
+    # the hidden activations are rounded to BF16 between layers, so an FP32
+    # accumulation that lands on the other side of a rounding boundary from
+    # the FP64 sum moves that activation by one BF16 ulp: 1e-4, not 1e-5
+    assert rel_l2(out.cpu().numpy(), ref_out) <= 1e-4
     d = O.bf16_round(((2.0 / u.size) * (ref_out - t)).astype(np.float32))[:, None]
     for li in (4, 3, 2, 1, 0):
         rdw, rdb = O.conv3x3_wgrad(a[li], d)
