@@ -22,27 +22,30 @@
 // The FP64 CPU oracle (oracle/oracle.cpp, cyl_view_terms) evaluates the same
 // sum voxel by voxel.
 //
-// Forward projection: a warp owns one detector column u and 32 rows: its
-// lanes hold the rows' lower edges, and the 33rd edge, closing lane 31's row,
-// is evaluated by every lane alongside (it needs two more shuffles).  On each
+// Forward projection: the volume's z prefix sums (one FP64-accumulated
+// table per call, cyl_zprefix_kernel) turn a row's integral over z on one
+// voxel column into the difference of the prefix at its two edges, read with
+// linear interpolation inside a voxel.  A warp owns one detector column u
+// and 32 rows: its lanes hold the rows' lower edges, and the 33rd edge,
+// closing lane 31's row, is evaluated by every lane alongside.  On each
 // plane the column's lateral footprint covers 1-3 voxel columns, the same
-// for every lane; for each of them the warp loads the z-run of voxels its
-// rows span (coalesced), scans it (FP32 prefix sums relative to the run's
-// start) and evaluates the prefix at each lane's row edge; a row's integral
-// over z is the difference of two neighbouring lanes' values (one shuffle),
-// so every edge is evaluated once and no prefix table is kept in memory.  The
-// volume itself stays in L2 between views.
+// for every lane; each lane reads the prefix at its edge on each of them
+// (lanes read neighbouring entries of one column: two or three sectors per
+// warp), weights it by the lateral overlap, and a row's value is the
+// difference of two neighbouring lanes' sums (one shuffle), so every edge is
+// evaluated once per plane.
 //
 // Backprojection: per view, the sinogram column u becomes a row table of
 // prefix sums of L p along v (cyl_table_kernel).  The gather runs in
 // launches over chunks of views whose tables stay in L2 (each voxel adds its
-// chunk's sum to the previous chunks').  A thread owns a voxel; a
-// warp owns 32 consecutive voxels along z of one (x, y) column, so the
-// candidate cells u (the columns whose footprint meets the voxel's lateral
-// extent on its plane) are the same for every lane and the loop over them
-// does not diverge.  For each candidate the voxel's z extent maps linearly to
-// a range of detector-row coordinates, and the row table gives the integral
-// of L p over it exactly.
+// chunk's sum to the previous chunks').  A warp owns 128 voxels along z of
+// one (x, y) column, four per lane, so the lateral work of a view (the
+// voxel's fan-angle range, the candidate cells u whose footprint meets its
+// lateral extent on its plane, their overlaps) is done once for the whole
+// column and the loop over candidates does not diverge.  For each candidate
+// the voxel edges map linearly to detector-row coordinates, the row table
+// gives the prefix of L p at each edge, and a voxel's share is the
+// difference of its two edges' prefixes (one shuffle).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -70,6 +73,7 @@ struct CylDims {
 constexpr int kCylFpWarps = 8;   // detector columns per forward-projection CTA
 constexpr int kCylRows = 32;     // detector rows per warp (its 32 lanes' edges and one more)
 constexpr int kCylBpWarps = 8;   // voxel columns per backprojection CTA
+constexpr int kCylBpZ = 4;       // voxels per lane along z (a warp covers 128)
 
 __device__ __forceinline__ float warp_scan_f(float v, int lane) {
 #pragma unroll
@@ -80,8 +84,43 @@ __device__ __forceinline__ float warp_scan_f(float v, int lane) {
     return v;
 }
 
+// z prefix sums of the volume, one column (b, x, y) per warp: entry j of
+// nz + 1 holds the sum of voxels j' < j, accumulated in FP64.
+__global__ void cyl_zprefix_kernel(float* __restrict__ zp, const float* __restrict__ vol, CylDims d) {
+    const int lane = threadIdx.x & 31;
+    const long long col = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (col >= (long long)d.nb * d.nx * d.ny) return;   // whole warp
+    const long long b = col / ((long long)d.nx * d.ny), xy = col % ((long long)d.nx * d.ny);
+    const float* v = vol + b * d.vol_stride + xy * d.nz;
+    float* o = zp + col * (d.nz + 1);
+    double carry = 0;
+    for (int j0 = 0; j0 < d.nz; j0 += 32) {
+        const int j = j0 + lane;
+        double x = j < d.nz ? (double)v[j] : 0.0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double t = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += t;
+        }
+        // inclusive sum up to j -> the prefix before j + 1
+        if (j < d.nz) o[j + 1] = (float)(carry + x);
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) o[0] = 0.f;
+}
+
+// The prefix of a z column at zeta (voxel units from the volume's bottom),
+// linear inside each voxel.
+__device__ __forceinline__ float z_prefix(const float* __restrict__ c, float zeta, int nz) {
+    if (zeta <= 0.f) return 0.f;
+    if (zeta >= (float)nz) return __ldg(c + nz);
+    const int m = (int)zeta;
+    const float a = __ldg(c + m), b = __ldg(c + m + 1);
+    return fmaf(zeta - (float)m, b - a, a);
+}
+
 __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restrict__ prj,
-                                                                 const float* __restrict__ vol,
+                                                                 const float* __restrict__ zp,
                                                                  const CylView* __restrict__ views,
                                                                  const double* __restrict__ redge,
                                                                  const float* __restrict__ inplane,
@@ -94,6 +133,7 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
     const int e = g0 + lane;
     const float s_lane = sedge[min(e, d.nv)];
     const float s_top = sedge[min(g0 + 32, d.nv)];           // the 33rd edge, closing lane 31's row
+    const float inv_dz = (float)(1.0 / d.dz), zoff = (float)(d.nz / 2.0 - d.cz / d.dz);
     for (int bz = blockIdx.z; bz < d.nview * d.nb; bz += gridDim.z) {
         const int iv = bz % d.nview, b = bz / d.nview;
         const CylView V = views[iv];
@@ -106,10 +146,14 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
         const float inp = inplane[(long long)iv * d.nu + u];
         const double inv_dlat = 1.0 / dlat;
         const double lat_off = nlat / 2.0 - clat * inv_dlat;
-        const float inv_dz = (float)(1.0 / d.dz), zoff = (float)(d.nz / 2.0 - d.cz / d.dz);
         // footprint width x in-plane distance: |R1 - R0| inp D^2 / dlat
         const float wfac = (float)(fabs(R1 - R0) * inv_dlat) * inp;
-        const float* vb = vol + (long long)b * d.vol_stride;
+        const float* zb = zp + (long long)b * d.nx * d.ny * (d.nz + 1);
+        // the columns of plane k along the lateral axis: x-class planes are
+        // rows y = k (columns x = i), y-class planes columns x = k
+        const long long cstride = (long long)(xc ? d.ny : 1) * (d.nz + 1);
+        const long long pstride = (long long)(xc ? 1 : d.ny) * (d.nz + 1);
+        const float szl = s_lane * inp * inv_dz, szt = s_top * inp * inv_dz;
         float acc = 0.f;
         for (int k = 0; k < nplane; k++) {
             const double D = (k + 0.5 - nplane / 2.0) * dmain + cmain - smain;
@@ -118,37 +162,17 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
             const int i0 = (int)fmax(floor(lo), 0.0), i1 = (int)fmin(floor(hi), (double)(nlat - 1));
             if (i0 > i1) continue;
             const float aD = (float)fabs(D);
-            const float dc = aD * inp;
-            const float zeta = s_lane * dc * inv_dz + zoff;
-            const float ztop = s_top * dc * inv_dz + zoff;
+            const float zeta = fmaf(szl, aD, zoff);
+            const float ztop = fmaf(szt, aD, zoff);
             const float z_first = __shfl_sync(0xffffffffu, zeta, 0);
             if (ztop <= 0.f || z_first >= (float)d.nz) continue;   // every row edge outside the volume
-            const float zf = floorf(zeta), ztf = floorf(ztop);
-            const int mabs = (int)fminf(fmaxf(zf, -1.f), (float)d.nz);
-            const int mtop = (int)fminf(fmaxf(ztf, -1.f), (float)d.nz);
-            const int jlo = (int)fmaxf(floorf(z_first), 0.f);
-            const int jhi = min(d.nz, mtop + 1);
+            const float* cp = zb + k * pstride;
             float Q = 0.f, Qt = 0.f;
             for (int i = i0; i <= i1; i++) {
                 const float ox = (float)(fmin(hi, i + 1.0) - fmax(lo, (double)i));
-                const float* col = vb + (long long)(xc ? (i * d.ny + k) : (k * d.ny + i)) * d.nz;
-                float P = 0.f, Pt = 0.f, carry = 0.f;
-                for (int jw = jlo; jw < jhi; jw += 32) {
-                    const int j = jw + lane;
-                    const float f = j < jhi ? __ldg(col + j) : 0.f;
-                    const float I = warp_scan_f(f, lane);
-                    const float tot = __shfl_sync(0xffffffffu, I, 31);
-                    const int m = mabs - jw, mt = mtop - jw;
-                    const float Im = __shfl_sync(0xffffffffu, I, m & 31), fm = __shfl_sync(0xffffffffu, f, m & 31);
-                    const float It = __shfl_sync(0xffffffffu, I, mt & 31), ft = __shfl_sync(0xffffffffu, f, mt & 31);
-                    if (m >= 0 && m < 32 && mabs < d.nz) P = carry + (Im - fm) + (zeta - zf) * fm;
-                    if (mt >= 0 && mt < 32 && mtop < d.nz) Pt = carry + (It - ft) + (ztop - ztf) * ft;
-                    carry += tot;
-                }
-                if (mabs >= d.nz) P = carry;
-                if (mtop >= d.nz) Pt = carry;
-                Q = fmaf(ox, P, Q);
-                Qt = fmaf(ox, Pt, Qt);
+                const float* c = cp + i * cstride;
+                Q = fmaf(ox, z_prefix(c, zeta, d.nz), Q);
+                Qt = fmaf(ox, z_prefix(c, ztop, d.nz), Qt);
             }
             float Qn = __shfl_down_sync(0xffffffffu, Q, 1);
             if (lane == 31) Qn = Qt;
@@ -199,18 +223,26 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
                                                                  const double* __restrict__ inv_dr,
                                                                  const float* __restrict__ inv_inp, CylDims d,
                                                                  int v_begin, int v_end, int accumulate) {
+    constexpr int Z = kCylBpZ;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long column = (long long)blockIdx.x * kCylBpWarps + warp;
     if (column >= (long long)d.nx * d.ny) return;              // whole warp
     const int ix = (int)(column / d.ny), iy = (int)(column % d.ny);
     const int b = blockIdx.z;
-    const int j = blockIdx.y * 32 + lane;
-    const float z_lo = (float)((j - d.nz / 2.0) * d.dz + d.cz);   // voxel's lower z face (mm)
-    const float z_hi = z_lo + (float)d.dz;
+    const int zbase = blockIdx.y * 32 * Z;
+    // z (mm) of the voxel edges zbase + lane + 32 q and of the warp's top edge
+    float ze[Z];
+#pragma unroll
+    for (int q = 0; q < Z; q++) ze[q] = (float)((zbase + lane + 32 * q - d.nz / 2.0) * d.dz + d.cz);
+    const float ztop = (float)((zbase + 32 * Z - d.nz / 2.0) * d.dz + d.cz);
+    const float zlast = (float)((min(d.nz, zbase + 32 * Z) - d.nz / 2.0) * d.dz + d.cz);
+    const float zfirst = (float)((zbase - d.nz / 2.0) * d.dz + d.cz);
     const float rho0 = (float)(d.nv / 2.0 - d.off_v);
     const float dsd_dv = (float)(d.dsd / d.dv);
     const double two_pi = 6.283185307179586;
-    float acc = 0.f;
+    float acc[Z];
+#pragma unroll
+    for (int q = 0; q < Z; q++) acc[q] = 0.f;
     for (int iv = v_begin; iv < v_end; iv++) {
         const CylView V = views[iv];
         const bool xc = V.xcls != 0;
@@ -246,19 +278,32 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
             const double lo = fmin(la, lb), hi = fmax(la, lb);
             const double ov = fmin(hi, i + 1.0) - fmax(lo, (double)i);
             if (ov <= 0) continue;
-            const float w = (float)(ov * wD * inv_dr[(long long)iv * d.nu + u]);
             const float inv = dsd_dv * inv_aD * inv_inp[(long long)iv * d.nu + u];
-            const float r_lo = fmaf(z_lo, inv, rho0), r_hi = fmaf(z_hi, inv, rho0);
             // the warp's z run against the detector rows: skip if it misses them
-            const float first = __shfl_sync(0xffffffffu, r_lo, 0), last = __shfl_sync(0xffffffffu, r_hi, 31);
-            if (last <= 0.f || first >= (float)d.nv) continue;
+            if (fmaf(zlast, inv, rho0) <= 0.f || fmaf(zfirst, inv, rho0) >= (float)d.nv) continue;
+            const float w = (float)(ov * wD * inv_dr[(long long)iv * d.nu + u]);
             const float2* t = tv + (long long)u * (d.nv + 1);
-            acc = fmaf(w, row_prefix(t, r_hi, d.nv) - row_prefix(t, r_lo, d.nv), acc);
+            // prefixes at every edge; a voxel's integral is the next edge's minus its own
+            float P[Z];
+#pragma unroll
+            for (int q = 0; q < Z; q++) P[q] = row_prefix(t, fmaf(ze[q], inv, rho0), d.nv);
+            const float Ptop = row_prefix(t, fmaf(ztop, inv, rho0), d.nv);
+#pragma unroll
+            for (int q = 0; q < Z; q++) {
+                float Pn = __shfl_down_sync(0xffffffffu, P[q], 1);
+                const float P0 = __shfl_sync(0xffffffffu, q + 1 < Z ? P[q + 1 < Z ? q + 1 : q] : Ptop, 0);
+                if (lane == 31) Pn = q + 1 < Z ? P0 : Ptop;
+                acc[q] = fmaf(w, Pn - P[q], acc[q]);
+            }
         }
     }
-    if (j < d.nz) {
-        float* o = vol + (long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz + j;
-        *o = accumulate ? *o + acc : acc;
+#pragma unroll
+    for (int q = 0; q < Z; q++) {
+        const int j = zbase + lane + 32 * q;
+        if (j < d.nz) {
+            float* o = vol + (long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz + j;
+            *o = accumulate ? *o + acc[q] : acc[q];
+        }
     }
 }
 
@@ -279,6 +324,7 @@ struct rn_cyl_plan {
     float* d_invinp = nullptr;    // [nview][nu] 1 / sqrt(1 + R_c^2)
     int bp_chunk = 0;             // views per backprojection launch (their row tables stay in L2)
     float2* d_tab = nullptr;      // backprojection row tables [nb][nview][nu][nv+1]
+    float* d_zp = nullptr;        // forward-projection z prefix sums [nb][nx][ny][nz+1]
     long long launches = 0;
 };
 
@@ -353,6 +399,8 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
     if ((e = cudaMalloc(&p->d_sedge, sizeof(float) * sedge.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_rowlen, sizeof(float) * rowlen.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_tab, sizeof(float2) * tab_elems)) != cudaSuccess) return fail(e, "cyl: row tables");
+    if ((e = cudaMalloc(&p->d_zp, sizeof(float) * (size_t)g->nBatches * g->nx * g->ny * (g->nz + 1))) != cudaSuccess)
+        return fail(e, "cyl: z prefix sums");
     if ((e = cudaMalloc(&p->d_invdr, sizeof(double) * invdr.size())) != cudaSuccess) return fail(e, "cyl: cells");
     if ((e = cudaMalloc(&p->d_invinp, sizeof(float) * invinp.size())) != cudaSuccess) return fail(e, "cyl: cells");
     if ((e = cudaMemcpyAsync(p->d_views, views.data(), sizeof(CylView) * nview, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
@@ -380,6 +428,7 @@ extern "C" int rn_cyl_plan_destroy(rn_cyl_plan* p) {
     cudaFree(p->d_sedge);
     cudaFree(p->d_rowlen);
     cudaFree(p->d_tab);
+    cudaFree(p->d_zp);
     cudaFree(p->d_invdr);
     cudaFree(p->d_invinp);
     delete p;
@@ -393,10 +442,14 @@ extern "C" int rn_cyl_project(rn_cyl_plan* p, float* d_prj, const float* d_vol, 
     if (!p || !d_prj || !d_vol) return set_error(RN_ERR_ARG, "cyl: null argument");
     cudaStream_t st = (cudaStream_t)stream;
     const CylDims& d = p->d;
+    const long long ncol = (long long)d.nb * d.nx * d.ny;
+    cyl_zprefix_kernel<<<(unsigned)((ncol * 32 + 255) / 256), 256, 0, st>>>(p->d_zp, d_vol, d);
+    p->launches++;
+    RN_CUDA_TRY(cudaGetLastError());
     dim3 grid((unsigned)((d.nu + kCylFpWarps - 1) / kCylFpWarps), (unsigned)((d.nv + kCylRows - 1) / kCylRows),
               (unsigned)std::min<long long>((long long)d.nview * d.nb, 65535));
-    cyl_fp_kernel<<<grid, 32 * kCylFpWarps, 0, st>>>(d_prj, d_vol, p->d_views, p->d_redge, p->d_inplane, p->d_sedge,
-                                                    p->d_rowlen, d);
+    cyl_fp_kernel<<<grid, 32 * kCylFpWarps, 0, st>>>(d_prj, p->d_zp, p->d_views, p->d_redge, p->d_inplane,
+                                                    p->d_sedge, p->d_rowlen, d);
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
@@ -413,8 +466,8 @@ extern "C" int rn_cyl_backproject(rn_cyl_plan* p, float* d_vol, const float* d_p
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     if (d.nb > 65535) return set_error(RN_ERR_ARG, "cyl: too many batches");
-    dim3 grid((unsigned)(((long long)d.nx * d.ny + kCylBpWarps - 1) / kCylBpWarps), (unsigned)((d.nz + 31) / 32),
-              (unsigned)d.nb);
+    dim3 grid((unsigned)(((long long)d.nx * d.ny + kCylBpWarps - 1) / kCylBpWarps),
+              (unsigned)((d.nz + 32 * kCylBpZ - 1) / (32 * kCylBpZ)), (unsigned)d.nb);
     for (int v0 = 0; v0 < d.nview; v0 += p->bp_chunk) {
         const int v1 = std::min(d.nview, v0 + p->bp_chunk);
         cyl_bp_kernel<<<grid, 32 * kCylBpWarps, 0, st>>>(d_vol, p->d_tab, p->d_views, p->d_redge, p->d_invdr,

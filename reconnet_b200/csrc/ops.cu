@@ -101,7 +101,8 @@ struct FilterVal {
     float2* d_tw = nullptr; // [N/2] exp(-2 pi i q / N)
     // register four-step form (N = 512, 1024, 2048, run as two transforms of
     // M = N/2 points): the even- and odd-frequency halves of the spectrum in
-    // the registers' order, [2][M/32][32] (entry [half][r][lane]); then the
+    // the registers' order, [2][M/32][32] (entry [half][r][lane]; at M = 1024
+    // in the order of the transposing kernel); then the
     // M-point middle twiddles [M/32][32] followed by the odd half's
     // pre-twiddles exp(-2 pi i n / N), n = lane + 32 r < M
     float2* d_Hp = nullptr;
@@ -188,8 +189,11 @@ static int get_filter(int nu, float da, float off_a, int typeFilter, int fan, cu
             for (int r = 0; r < L; r++)
                 for (int l = 0; l < 32; l++) {
                     const int k2 = brev(r, bits), k = k2 + L * brev(l, 5);
-                    Hp[(size_t)r * 32 + l] = Hf[2 * k];
-                    Hp[(size_t)M + r * 32 + l] = Hf[2 * k + 1];
+                    // at M = 1024 the transposing kernel holds frequency k2 +
+                    // 32 k1 in lane bitrev5^-1(k2), register bitrev5^-1(k1)
+                    const size_t at = M == 1024 ? (size_t)l * 32 + r : (size_t)r * 32 + l;
+                    Hp[at] = Hf[2 * k];
+                    Hp[(size_t)M + at] = Hf[2 * k + 1];
                     const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * (double)(l * k2) / (double)M);
                     Tw[(size_t)r * 32 + l] = make_float2((float)w.real(), (float)w.imag());
                     const std::complex<double> q = std::polar(1.0, -2.0 * M_PI * (double)(l + 32 * r) / (double)N);
@@ -452,7 +456,9 @@ __device__ __forceinline__ void reg_local_dif(float2 (&v)[L], const RegFftTw<L>&
             const float2 a = v[i], b = v[i + h];
             v[i] = c_add(a, b);
             const int k = (i & (h - 1)) * (L / (2 * h));
-            v[i + h] = k == 0 ? c_sub(a, b) : c_mul(c_sub(a, b), t.local[k]);
+            const float2 d = c_sub(a, b);
+            // exp(-2 pi i k / L): 1 at k = 0, -i at k = L/4
+            v[i + h] = k == 0 ? d : 4 * k == L ? make_float2(d.y, -d.x) : c_mul(d, t.local[k]);
         }
     }
 }
@@ -465,7 +471,8 @@ __device__ __forceinline__ void reg_local_dit_inv(float2 (&v)[L], const RegFftTw
         for (int i = 0; i < L; i++) {
             if (i & h) continue;
             const int k = (i & (h - 1)) * (L / (2 * h));
-            const float2 a = v[i], b = k == 0 ? v[i + h] : c_mulc(v[i + h], t.local[k]);
+            const float2 c = v[i + h];
+            const float2 a = v[i], b = k == 0 ? c : 4 * k == L ? make_float2(-c.y, c.x) : c_mulc(c, t.local[k]);
             v[i] = c_add(a, b);
             v[i + h] = c_sub(a, b);
         }
@@ -581,6 +588,103 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
     }
 }
 
+// The N = 2048 case (M = 1024 = 32 x 32) with both 32-point stages in
+// registers: lane l first transforms its 32 registers (n2 -> k2, register r
+// holding k2 = bitrev(r)), applies the middle twiddle exp(-2 pi i l k2 / M),
+// and the warp transposes the 32 x 32 block through shared memory, after which
+// lane l holds row k2 = bitrev(l) and transforms n1 -> k1 in its registers
+// (register c holding k1 = bitrev(c)); frequency k2 + 32 k1 then sits in lane
+// l, register c.  The inverse runs the same steps backwards.  Two transposes
+// (64 conflict-free shared-memory accesses per lane) replace ten cross-lane
+// shuffle stages.
+constexpr int kTrStride = 33;   // float2 row stride of a warp's transpose block
+
+__global__ void __launch_bounds__(256, 1) filter_tr_kernel(float* __restrict__ out, const float* __restrict__ prj,
+                                                          const float2* __restrict__ Hq,
+                                                          const float2* __restrict__ Tw,
+                                                          const float* __restrict__ pw,
+                                                          const float* __restrict__ sw, int nu, int nview, int nv,
+                                                          int nc, int nplane_total, float scale, RegFftTw<32> tw) {
+    constexpr int L = 32, M = 1024, TS = kRegViews + 1;
+    // [nu][kRegViews + 1] floats, then [8 warps][nu] float2 (the even half's
+    // output), then [8 warps][32][33] float2 (the transpose blocks)
+    extern __shared__ float tile[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float2* __restrict__ Pre = Tw + M;
+    float2* ybuf = reinterpret_cast<float2*>(tile + ((nu * TS + 1) & ~1)) + (long long)warp * nu;
+    float2* tr = reinterpret_cast<float2*>(tile + ((nu * TS + 1) & ~1)) + 8 * nu + warp * (32 * kTrStride);
+    const long long su = (long long)nview * nv * nc, sview = (long long)nv * nc;
+    const int v0 = blockIdx.x * kRegViews;
+    for (int plane = blockIdx.y; plane < nplane_total; plane += gridDim.y) {
+        const int b = plane / (nv * nc);
+        const int rem = plane - b * nv * nc;
+        const long long off = (long long)b * nu * nview * nv * nc + rem;
+#pragma unroll 4
+        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
+            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
+            float x = 0.f;
+            if (view < nview) {
+                x = prj[off + (long long)n * su + (long long)view * sview] * pw[n];
+                if (sw) x *= sw[(long long)n * nview + view];
+            }
+            tile[n * TS + vv] = x;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int half = 0; half < 2; half++) {
+            float2 v[L];
+#pragma unroll
+            for (int r = 0; r < L; r++) {
+                const int n = lane + 32 * r;
+                v[r] = n < nu ? make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1])
+                              : make_float2(0.f, 0.f);
+                if (half) v[r] = c_mul(v[r], __ldg(Pre + r * 32 + lane));
+            }
+            reg_local_dif<L>(v, tw);
+#pragma unroll
+            for (int r = 0; r < L; r++) tr[r * kTrStride + lane] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < L; c++) v[c] = tr[lane * kTrStride + c];
+            reg_local_dif<L>(v, tw);
+            // this half of the kernel's spectrum (scaled by 1/N), then the inverse
+#pragma unroll
+            for (int c = 0; c < L; c++) v[c] = c_mul(v[c], __ldg(Hq + half * M + c * 32 + lane));
+            reg_local_dit_inv<L>(v, tw);
+            __syncwarp();   // every lane has read its row of the block
+#pragma unroll
+            for (int c = 0; c < L; c++) tr[lane * kTrStride + c] = v[c];
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < L; r++) v[r] = c_mulc(tr[r * kTrStride + lane], __ldg(Tw + r * 32 + lane));
+            reg_local_dit_inv<L>(v, tw);
+            __syncwarp();   // the block is free for the next half
+            if (half == 0) {
+#pragma unroll
+                for (int r = 0; r < L; r++)
+                    if (lane + 32 * r < nu) ybuf[lane + 32 * r] = v[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < L; r++) {
+                    const int n = lane + 32 * r;
+                    if (n < nu) {
+                        const float2 y = c_add(ybuf[n], c_mulc(v[r], __ldg(Pre + r * 32 + lane)));
+                        tile[n * TS + 2 * warp] = y.x * scale;
+                        tile[n * TS + 2 * warp + 1] = y.y * scale;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
+            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
+            if (view < nview) out[off + (long long)n * su + (long long)view * sview] = tile[n * TS + vv];
+        }
+        __syncthreads();   // the next plane refills the tile
+    }
+}
+
 template <int L>
 static int launch_filter_reg(float* d_out, const float* d_prj, const FilterVal& fv, const float* d_sw, int nu,
                              int nview, int nv, int nc, int nplanes, unsigned grid_planes, float scale,
@@ -599,6 +703,24 @@ static int launch_filter_reg(float* d_out, const float* d_prj, const FilterVal& 
     dim3 grid((unsigned)((nview + kRegViews - 1) / kRegViews), grid_planes);
     filter_reg_kernel<L><<<grid, 256, smem, st>>>(d_out, d_prj, fv.d_Hp, fv.d_Tw, fv.d_pw, d_sw, nu, nview, nv, nc,
                                                   nplanes, scale, tw);
+    RN_CUDA_TRY(cudaGetLastError());
+    return RN_OK;
+}
+
+static int launch_filter_tr(float* d_out, const float* d_prj, const FilterVal& fv, const float* d_sw, int nu,
+                            int nview, int nv, int nc, int nplanes, unsigned grid_planes, float scale,
+                            cudaStream_t st) {
+    RegFftTw<32> tw;
+    for (int k = 0; k < 16; k++) {
+        const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / 32.0);
+        tw.local[k] = tw.w32[k] = make_float2((float)w.real(), (float)w.imag());
+    }
+    const size_t smem = sizeof(float) * (((size_t)nu * (kRegViews + 1) + 1) & ~(size_t)1) +
+                        sizeof(float2) * 8 * ((size_t)nu + 32 * kTrStride);
+    RN_CUDA_TRY(cudaFuncSetAttribute(filter_tr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((nview + kRegViews - 1) / kRegViews), grid_planes);
+    filter_tr_kernel<<<grid, 256, smem, st>>>(d_out, d_prj, fv.d_Hp, fv.d_Tw, fv.d_pw, d_sw, nu, nview, nv, nc,
+                                              nplanes, scale, tw);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
@@ -625,7 +747,7 @@ int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int 
     const unsigned grid_planes = (unsigned)std::min<long long>(nplanes, 65535);
     if (g_filter_form == 0 && fv.d_Hp) {
         const int N = 1 << fv.logN;
-        if (N == 2048) return launch_filter_reg<32>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        if (N == 2048) return launch_filter_tr(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
         if (N == 1024) return launch_filter_reg<16>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
         return launch_filter_reg<8>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
     }

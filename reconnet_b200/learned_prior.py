@@ -216,21 +216,35 @@ class PriorCNN:
         return self.forward(img.contiguous() * self.scale) / self.scale
 
     def train(self, inputs: torch.Tensor, targets: torch.Tensor, steps: int, batch: int = 8, lr: float = 1e-3,
-              seed: int = 0, log_every: int = 0) -> List[float]:
-        """Adam on the mean squared error of u_in -> u_target (normalised)."""
+              seed: int = 0, log_every: int = 0, lr_final: float = 0.01, augment: bool = True) -> List[float]:
+        """Adam on the mean squared error of u_in -> u_target (normalised).
+        The learning rate decays from lr to lr * lr_final on a cosine; with
+        augment, each batch is taken in one of the square's eight orientations
+        (a full-circle scan with uniform views treats them alike)."""
         g = torch.Generator(device="cpu").manual_seed(seed)
         n = inputs.shape[0]
+        square = inputs.shape[1] == inputs.shape[2]
         losses = []
         for s in range(steps):
             idx = torch.randint(0, n, (batch,), generator=g).to(self.device)
-            u = (inputs[idx] * self.scale).contiguous()
-            t = (targets[idx] * self.scale).contiguous()
+            u = inputs[idx] * self.scale
+            t = targets[idx] * self.scale
+            if augment:
+                o = int(torch.randint(0, 8 if square else 4, (1,), generator=g))
+                if o & 1:
+                    u, t = u.flip(1), t.flip(1)
+                if o & 2:
+                    u, t = u.flip(2), t.flip(2)
+                if o & 4:
+                    u, t = u.transpose(1, 2), t.transpose(1, 2)
+            u, t = u.contiguous(), t.contiguous()
             out, acts = self.forward(u, keep=True)
             diff = out - t
             loss = float((diff * diff).mean()) if (log_every and s % log_every == 0) or s == steps - 1 else None
             d_out = (2.0 / diff.numel()) * diff
             dws, dbs = self.backward(acts, d_out.contiguous())
-            self.adam_step(dws, dbs, lr=lr)
+            frac = s / max(steps - 1, 1)
+            self.adam_step(dws, dbs, lr=lr * (lr_final + (1 - lr_final) * 0.5 * (1 + math.cos(math.pi * frac))))
             if loss is not None:
                 losses.append(loss)
         self.k.check()
