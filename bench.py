@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-ossqs", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the Siddon, tomosynthesis, cone and filter measurements")
     ap.add_argument("--ossqs-iters", type=int, default=30)
-    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs", "cyl", "cfg0", "prior"],
+    ap.add_argument("--extra", choices=["siddon", "tomo", "cone", "filter", "ossqs", "cyl", "cfg0", "prior", "conv"],
                     help="run only this extra measurement (one GPU) and print its JSON object")
     return ap.parse_args()
 
@@ -1197,6 +1197,8 @@ def run_extra(args):
         out = cfg0_run(dev, cpu_sample=cpu)
     elif args.extra == "prior":
         out = prior_run(dev)
+    elif args.extra == "conv":
+        out = conv_roofline(dev)
     else:
         out = filter_run(dev, cpu_sample=cpu)
     print(json.dumps({args.extra: out}), flush=True)

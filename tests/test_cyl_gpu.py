@@ -53,7 +53,7 @@ def test_cyl_pair_matches_oracle(name, rng):
     lhs = float((ax.double() * torch.from_numpy(y).cuda().double()).sum())
     rhs = float((torch.from_numpy(x).cuda().double() * aty.double()).sum())
     assert abs(lhs - rhs) / abs(lhs) <= TOL
-    assert plan.launches() == 3          # FP; BP row tables + BP
+    assert plan.launches() == 4          # FP: z prefix table + FP; BP: row tables + BP
 
 
 def test_cyl_views_on_class_boundaries(rng):
