@@ -71,69 +71,75 @@ struct CylDims {
 };
 
 constexpr int kCylFpWarps = 8;   // detector columns per forward-projection CTA
-constexpr int kCylRows = 32;     // detector rows per warp (its 32 lanes' edges and one more)
+constexpr int kCylRows = 64;     // detector rows per forward-projection warp (two per lane)
 constexpr int kCylBpWarps = 8;   // voxel columns per backprojection CTA
 constexpr int kCylBpZ = 4;       // voxels per lane along z (a warp covers 128)
+constexpr float kCylFloorBias = 12582912.0f;   // 1.5 * 2^23: adding it rounds to an integer
+constexpr int kCylFloorBiasBits = 0x4B400000;
 
-__device__ __forceinline__ float warp_scan_f(float v, int lane) {
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
-
-// z prefix sums of the volume, one column (b, x, y) per warp: entry j of
-// nz + 1 holds the sum of voxels j' < j, accumulated in FP64.
-__global__ void cyl_zprefix_kernel(float* __restrict__ zp, const float* __restrict__ vol, CylDims d) {
+// Band-limited z prefix sums of the volume, one column (b, x, y) per warp.
+// Entry j of the band (nbz entries) holds the sum of the column's voxels
+// between z = max(zlo, 0) and z = clamp(zlo + j, 0, nz) (voxel units), so that
+// linear interpolation between entries is the column's exact integral up to
+// any height, constant below the volume and above it.  The band [zlo, zlo +
+// nbz - 1] covers every row edge of every view (the plan bounds it on the
+// host), and accumulation is FP64.
+__global__ void cyl_zprefix_kernel(float* __restrict__ zp, const float* __restrict__ vol, CylDims d, int zlo,
+                                   int nbz) {
     const int lane = threadIdx.x & 31;
     const long long col = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (col >= (long long)d.nb * d.nx * d.ny) return;   // whole warp
     const long long b = col / ((long long)d.nx * d.ny), xy = col % ((long long)d.nx * d.ny);
     const float* v = vol + b * d.vol_stride + xy * d.nz;
-    float* o = zp + col * (d.nz + 1);
+    float* o = zp + col * nbz;
+    const int z0 = max(zlo, 0), z1 = min(zlo + nbz - 1, d.nz);   // heights stored as running sums
     double carry = 0;
-    for (int j0 = 0; j0 < d.nz; j0 += 32) {
-        const int j = j0 + lane;
-        double x = j < d.nz ? (double)v[j] : 0.0;
+    for (int j0 = z0; j0 < z1; j0 += 32) {
+        const int j = j0 + lane;   // voxel j: the entry at height j + 1 holds the sum up to it
+        double x = j < z1 ? (double)v[j] : 0.0;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
             const double t = __shfl_up_sync(0xffffffffu, x, off);
             if (lane >= off) x += t;
         }
-        // inclusive sum up to j -> the prefix before j + 1
-        if (j < d.nz) o[j + 1] = (float)(carry + x);
+        if (j < z1) o[j + 1 - zlo] = (float)(carry + x);
         carry += __shfl_sync(0xffffffffu, x, 31);
     }
-    if (lane == 0) o[0] = 0.f;
+    // heights at or below max(zlo, 0) hold 0, heights above min(zhi, nz) the total
+    const float tot = (float)carry;
+    for (int j = lane; j < nbz; j += 32) {
+        const int z = zlo + j;
+        if (z <= z0) o[j] = 0.f;
+        else if (z > z1) o[j] = tot;
+    }
 }
 
-// The prefix of a z column at zeta (voxel units from the volume's bottom),
-// linear inside each voxel.
-__device__ __forceinline__ float z_prefix(const float* __restrict__ c, float zeta, int nz) {
-    if (zeta <= 0.f) return 0.f;
-    if (zeta >= (float)nz) return __ldg(c + nz);
-    const int m = (int)zeta;
-    const float a = __ldg(c + m), b = __ldg(c + m + 1);
-    return fmaf(zeta - (float)m, b - a, a);
-}
-
+// Forward projection.  A warp owns one detector column u and 64 rows; lane l
+// holds rows 2l and 2l + 1, so it evaluates their three edges.  Per plane k
+// the column's lateral footprint [lo, hi] (voxel units) is affine in k, and
+// so is each edge's height on the plane; the heights' cells and fractions are
+// computed once per plane and serve every voxel column the footprint meets.
 __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restrict__ prj,
                                                                  const float* __restrict__ zp,
                                                                  const CylView* __restrict__ views,
                                                                  const double* __restrict__ redge,
                                                                  const float* __restrict__ inplane,
                                                                  const float* __restrict__ sedge,
-                                                                 const float* __restrict__ rowlen, CylDims d) {
+                                                                 const float* __restrict__ rowlen, CylDims d,
+                                                                 int zlo, int nbz) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int u = blockIdx.x * kCylFpWarps + warp;
     if (u >= d.nu) return;                                   // whole warp
     const int g0 = blockIdx.y * kCylRows;
-    const int e = g0 + lane;
-    const float s_lane = sedge[min(e, d.nv)];
-    const float s_top = sedge[min(g0 + 32, d.nv)];           // the 33rd edge, closing lane 31's row
-    const float inv_dz = (float)(1.0 / d.dz), zoff = (float)(d.nz / 2.0 - d.cz / d.dz);
+    const int e0 = g0 + 2 * lane;
+    float sl[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) sl[q] = sedge[min(e0 + q, d.nv)];
+    const float s_bot = sedge[min(g0, d.nv)], s_top = sedge[min(g0 + kCylRows, d.nv)];
+    const float inv_dz = (float)(1.0 / d.dz);
+    const float zoffb = (float)(d.nz / 2.0 - d.cz / d.dz) - (float)zlo;   // band coordinates
+    const float zvol0 = -(float)zlo, zvol1 = (float)(d.nz - zlo);         // the volume's bottom and top
+    const unsigned mmax = (unsigned)(nbz - 2);
     for (int bz = blockIdx.z; bz < d.nview * d.nb; bz += gridDim.z) {
         const int iv = bz % d.nview, b = bz / d.nview;
         const CylView V = views[iv];
@@ -146,48 +152,82 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
         const float inp = inplane[(long long)iv * d.nu + u];
         const double inv_dlat = 1.0 / dlat;
         const double lat_off = nlat / 2.0 - clat * inv_dlat;
+        // plane k sits at D(k) = D0 + k dmain from the source along the main
+        // axis (one sign for every plane: the source is outside the volume);
+        // the footprint's edges are affine in D
+        const double D0 = (0.5 - nplane / 2.0) * dmain + cmain - smain;
+        const double la0 = fma(R0, D0, slat) * inv_dlat + lat_off, dla = R0 * dmain * inv_dlat;
+        const double lb0 = fma(R1, D0, slat) * inv_dlat + lat_off, dlb = R1 * dmain * inv_dlat;
+        const bool aless = la0 < lb0;
+        const double lo0 = aless ? la0 : lb0, dlo = aless ? dla : dlb;
+        const double hi0 = aless ? lb0 : la0, dhi = aless ? dlb : dla;
         // footprint width x in-plane distance: |R1 - R0| inp D^2 / dlat
         const float wfac = (float)(fabs(R1 - R0) * inv_dlat) * inp;
-        const float* zb = zp + (long long)b * d.nx * d.ny * (d.nz + 1);
-        // the columns of plane k along the lateral axis: x-class planes are
-        // rows y = k (columns x = i), y-class planes columns x = k
-        const long long cstride = (long long)(xc ? d.ny : 1) * (d.nz + 1);
-        const long long pstride = (long long)(xc ? 1 : d.ny) * (d.nz + 1);
-        const float szl = s_lane * inp * inv_dz, szt = s_top * inp * inv_dz;
-        float acc = 0.f;
+        const float* zb = zp + (long long)b * d.nx * d.ny * nbz;
+        // voxel column (lateral i, plane k): x-class planes are rows y = k
+        const long long cstride = (long long)(xc ? d.ny : 1) * nbz;
+        const long long pstride = (long long)(xc ? 1 : d.ny) * nbz;
+        float sz[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) sz[q] = sl[q] * inp * inv_dz;
+        const float szb = s_bot * inp * inv_dz, szt = s_top * inp * inv_dz;
+        float acc0 = 0.f, acc1 = 0.f;
         for (int k = 0; k < nplane; k++) {
-            const double D = (k + 0.5 - nplane / 2.0) * dmain + cmain - smain;
-            const double la = fma(R0, D, slat) * inv_dlat + lat_off, lb = fma(R1, D, slat) * inv_dlat + lat_off;
-            const double lo = fmin(la, lb), hi = fmax(la, lb);
-            const int i0 = (int)fmax(floor(lo), 0.0), i1 = (int)fmin(floor(hi), (double)(nlat - 1));
-            if (i0 > i1) continue;
+            const double D = fma((double)k, dmain, D0);
+            const double lo = fma((double)k, dlo, lo0), hi = fma((double)k, dhi, hi0);
+            const double flo_d = floor(lo), fhi_d = floor(hi);
+            const int ilo = (int)flo_d, ihi = (int)fhi_d;
+            const int i0 = max(ilo, 0), i1 = min(ihi, nlat - 1);
+            if (i0 > i1) continue;                                   // warp-uniform
             const float aD = (float)fabs(D);
-            const float zeta = fmaf(szl, aD, zoff);
-            const float ztop = fmaf(szt, aD, zoff);
-            const float z_first = __shfl_sync(0xffffffffu, zeta, 0);
-            if (ztop <= 0.f || z_first >= (float)d.nz) continue;   // every row edge outside the volume
-            const float* cp = zb + k * pstride;
-            float Q = 0.f, Qt = 0.f;
-            for (int i = i0; i <= i1; i++) {
-                const float ox = (float)(fmin(hi, i + 1.0) - fmax(lo, (double)i));
-                const float* c = cp + i * cstride;
-                Q = fmaf(ox, z_prefix(c, zeta, d.nz), Q);
-                Qt = fmaf(ox, z_prefix(c, ztop, d.nz), Qt);
+            // the warp's rows against the volume's z extent
+            if (fmaf(szt, aD, zoffb) <= zvol0 || fmaf(szb, aD, zoffb) >= zvol1) continue;
+            const float flo = (float)(lo - flo_d), fhi = (float)(hi - fhi_d);
+            // each edge's cell m and fraction f in the band
+            unsigned m[3];
+            float f[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const float z = fmaf(sz[q], aD, zoffb);
+                const float y = __fadd_rd(z, kCylFloorBias);
+                const int mi = __float_as_int(y) - kCylFloorBiasBits;
+                f[q] = z - (y - kCylFloorBias);
+                m[q] = min((unsigned)max(mi, 0), mmax);
             }
-            float Qn = __shfl_down_sync(0xffffffffu, Q, 1);
-            if (lane == 31) Qn = Qt;
-            acc = fmaf(Qn - Q, __frcp_rn(wfac * aD * aD), acc);
+            const float* cp = zb + k * pstride;
+            float Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
+            for (int i = i0; i <= i1; i++) {
+                const float ox = (i == ihi ? fhi : 1.f) - (i == ilo ? flo : 0.f);
+                const float* c = cp + i * cstride;
+                float a0 = __ldg(c + m[0]), b0 = __ldg(c + m[0] + 1);
+                float a1 = __ldg(c + m[1]), b1 = __ldg(c + m[1] + 1);
+                float a2 = __ldg(c + m[2]), b2 = __ldg(c + m[2] + 1);
+                Q0 = fmaf(ox, fmaf(f[0], b0 - a0, a0), Q0);
+                Q1 = fmaf(ox, fmaf(f[1], b1 - a1, a1), Q1);
+                Q2 = fmaf(ox, fmaf(f[2], b2 - a2, a2), Q2);
+            }
+            const float w = __frcp_rn(wfac * aD * aD);
+            acc0 = fmaf(Q1 - Q0, w, acc0);
+            acc1 = fmaf(Q2 - Q1, w, acc1);
         }
-        if (e < d.nv) {
-            const float ds = sedge[e + 1] - sedge[e];
-            const float L = (float)dmain * inp * rowlen[e];
-            prj[(long long)b * d.prj_stride + ((long long)u * d.nview + iv) * d.nv + e] = acc * L * (float)d.dz / ds;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int e = e0 + q;
+            if (e < d.nv) {
+                const float ds = sedge[e + 1] - sedge[e];
+                const float L = (float)dmain * inp * rowlen[e];
+                prj[(long long)b * d.prj_stride + ((long long)u * d.nview + iv) * d.nv + e] =
+                    (q ? acc1 : acc0) * L * (float)d.dz / ds;
+            }
         }
     }
 }
 
-// Row tables of the backprojection: per (batch, view, column u), entry r of
-// nv + 1 holds (sum over rows v < r of L p, L p of row r), built in FP64.
+// Row tables of the backprojection: per (batch, view, column u), nv + 2
+// entries: entry r + 1 holds (sum over rows v < r of L p, L p of row r) for
+// r < nv, built in FP64; entry 0 = (0, 0) and entry nv + 1 = (total, 0) are
+// guards, so that a height below the detector reads 0 and one above it the
+// total without a branch.
 __global__ void cyl_table_kernel(float2* __restrict__ tab, const float* __restrict__ prj, const CylView* __restrict__ views,
                                  const float* __restrict__ inplane, const float* __restrict__ rowlen, CylDims d) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -199,28 +239,30 @@ __global__ void cyl_table_kernel(float2* __restrict__ tab, const float* __restri
     const double dmain = views[iv].xcls ? d.dy : d.dx;
     const double lu = dmain * inplane[(long long)iv * d.nu + u];
     const float* p = prj + (long long)b * d.prj_stride + ((long long)u * d.nview + iv) * d.nv;
-    float2* out = tab + (((long long)b * d.nview + iv) * d.nu + u) * (d.nv + 1);
+    float2* out = tab + (((long long)b * d.nview + iv) * d.nu + u) * (d.nv + 2);
     double C = 0;
+    out[0] = make_float2(0.f, 0.f);
     for (int v = 0; v < d.nv; v++) {
         const double w = lu * rowlen[v] * (double)p[v];
-        out[v] = make_float2((float)C, (float)w);
+        out[v + 1] = make_float2((float)C, (float)w);
         C += w;
     }
-    out[d.nv] = make_float2((float)C, 0.f);
+    out[d.nv + 1] = make_float2((float)C, 0.f);
 }
 
+// The prefix of L p at detector-row coordinate rho of a row table (linear
+// inside each row, 0 below the detector, the total above it).
 __device__ __forceinline__ float row_prefix(const float2* __restrict__ t, float rho, int nv) {
-    if (rho <= 0.f) return 0.f;
-    if (rho >= (float)nv) return __ldg(&t[nv].x);
-    const int r = (int)rho;
-    const float2 c = __ldg(&t[r]);
-    return fmaf(c.y, rho - (float)r, c.x);
+    const float y = __fadd_rd(rho, kCylFloorBias);
+    const int m = min(max(__float_as_int(y) - kCylFloorBiasBits, -1), nv);
+    const float2 c = __ldg(&t[m + 1]);
+    return fmaf(c.y, rho - (y - kCylFloorBias), c.x);
 }
 
 __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restrict__ vol, const float2* __restrict__ tab,
                                                                  const CylView* __restrict__ views,
                                                                  const double* __restrict__ redge,
-                                                                 const double* __restrict__ inv_dr,
+                                                                 const float* __restrict__ inv_dr,
                                                                  const float* __restrict__ inv_inp, CylDims d,
                                                                  int v_begin, int v_end, int accumulate) {
     constexpr int Z = kCylBpZ;
@@ -230,15 +272,15 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
     const int ix = (int)(column / d.ny), iy = (int)(column % d.ny);
     const int b = blockIdx.z;
     const int zbase = blockIdx.y * 32 * Z;
-    // z (mm) of the voxel edges zbase + lane + 32 q and of the warp's top edge
-    float ze[Z];
+    // lane holds voxels zbase + Z lane + q; z (mm) of their Z + 1 edges
+    float ze[Z + 1];
 #pragma unroll
-    for (int q = 0; q < Z; q++) ze[q] = (float)((zbase + lane + 32 * q - d.nz / 2.0) * d.dz + d.cz);
-    const float ztop = (float)((zbase + 32 * Z - d.nz / 2.0) * d.dz + d.cz);
+    for (int q = 0; q <= Z; q++) ze[q] = (float)((zbase + Z * lane + q - d.nz / 2.0) * d.dz + d.cz);
     const float zlast = (float)((min(d.nz, zbase + 32 * Z) - d.nz / 2.0) * d.dz + d.cz);
     const float zfirst = (float)((zbase - d.nz / 2.0) * d.dz + d.cz);
     const float rho0 = (float)(d.nv / 2.0 - d.off_v);
     const float dsd_dv = (float)(d.dsd / d.dv);
+    const float inv_da = (float)(1.0 / d.da), e_off = (float)(-d.off_a + (d.nu - 1) * 0.5 + 0.5);
     const double two_pi = 6.283185307179586;
     float acc[Z];
 #pragma unroll
@@ -251,55 +293,56 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
         const double dmain = xc ? d.dy : d.dx, dlat = xc ? d.dx : d.dy;
         const double cmain = xc ? d.cy : d.cx, clat = xc ? d.cx : d.cy;
         const double smain = xc ? V.sy : V.sx, slat = xc ? V.sx : V.sy;
-        const double pm = (k + 0.5 - nplane / 2.0) * dmain + cmain;
-        const double D = pm - smain;
-        const double lat0 = (i - nlat / 2.0) * dlat + clat;
-        // fan angles of the rays through the voxel's lateral faces -> edge coordinates
-        float e01[2];
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-            const double lat = lat0 + q * dlat;
-            const float px = (float)((xc ? lat : pm) - V.sx), py = (float)((xc ? pm : lat) - V.sy);
-            float a = atan2f(px, py) + V.theta;
-            a -= (float)two_pi * rintf(a * (float)(1.0 / two_pi));
-            e01[q] = -a / (float)d.da - (float)d.off_a + (d.nu - 1) * 0.5f + 0.5f;
-        }
-        const float elo = fminf(e01[0], e01[1]) - 0.01f, ehi = fmaxf(e01[0], e01[1]) + 0.01f;
-        const int ulo = (int)fmaxf(floorf(elo), 0.f), uhi = (int)fminf(floorf(ehi), (double)(d.nu - 1));
+        const double D = (k + 0.5 - nplane / 2.0) * dmain + cmain - smain;
+        // the voxel's lower lateral face, relative to the source
+        const double lf = (i - nlat / 2.0) * dlat + clat - slat;
+        // fan angle of the ray through the voxel's lateral centre, and the
+        // half-width of the voxel's angular range to first order: |D| / r^2
+        // per mm of lateral offset.  The candidate range is widened by the
+        // bound of the second-order term, (dlat / 2)^2 / (2 r^2) rad, twice
+        // over, and 0.01 cells; every candidate's overlap is then exact.
+        const float pl = (float)(lf + 0.5 * dlat), pD = (float)D;
+        const float px = xc ? pl : pD, py = xc ? pD : pl;
+        float a = atan2f(px, py) + V.theta;
+        a -= (float)two_pi * rintf(a * (float)(1.0 / two_pi));
+        const float inv_r2 = __frcp_rn(fmaf(px, px, py * py));
+        const float dl = (float)dlat;
+        const float half = 0.5f * dl * fabsf(pD) * inv_r2 * inv_da;
+        const float slack = fmaf(0.25f * dl * dl * inv_r2, inv_da, 0.01f);
+        const float ec = fmaf(-a, inv_da, e_off);
+        const int ulo = (int)fmaxf(floorf(ec - half - slack), 0.f);
+        const int uhi = (int)fminf(floorf(ec + half + slack), (float)(d.nu - 1));
+        const float inv_aD = __frcp_rn(fabsf(pD));
+        const float wD = (float)dlat * inv_aD;
         const double inv_dlat = 1.0 / dlat;
-        const double lat_off = nlat / 2.0 - clat * inv_dlat;
-        // footprint width on this plane: |R1 - R0| |D| / dlat
-        const double wD = dlat / fabs(D);
-        const float inv_aD = (float)(1.0 / fabs(D));
         const double* Rv = redge + (long long)iv * (d.nu + 1);
-        const float2* tv = tab + ((long long)b * d.nview + iv) * (long long)d.nu * (d.nv + 1);
+        const float2* tv = tab + ((long long)b * d.nview + iv) * (long long)d.nu * (d.nv + 2);
+        // lateral position of edge e on this plane relative to the voxel's
+        // lower face, in voxel units
+        float xe = (float)((fma(Rv[ulo], D, -lf)) * inv_dlat);
         for (int u = ulo; u <= uhi; u++) {
-            const double la = fma(Rv[u], D, slat) * inv_dlat + lat_off, lb = fma(Rv[u + 1], D, slat) * inv_dlat + lat_off;
-            const double lo = fmin(la, lb), hi = fmax(la, lb);
-            const double ov = fmin(hi, i + 1.0) - fmax(lo, (double)i);
-            if (ov <= 0) continue;
+            const float xn = (float)((fma(Rv[u + 1], D, -lf)) * inv_dlat);
+            const float lo = fminf(xe, xn), hi = fmaxf(xe, xn);
+            xe = xn;
+            const float ov = fminf(hi, 1.f) - fmaxf(lo, 0.f);
+            if (ov <= 0.f) continue;
             const float inv = dsd_dv * inv_aD * inv_inp[(long long)iv * d.nu + u];
             // the warp's z run against the detector rows: skip if it misses them
             if (fmaf(zlast, inv, rho0) <= 0.f || fmaf(zfirst, inv, rho0) >= (float)d.nv) continue;
-            const float w = (float)(ov * wD * inv_dr[(long long)iv * d.nu + u]);
-            const float2* t = tv + (long long)u * (d.nv + 1);
-            // prefixes at every edge; a voxel's integral is the next edge's minus its own
-            float P[Z];
+            const float w = ov * wD * inv_dr[(long long)iv * d.nu + u];
+            const float2* t = tv + (long long)u * (d.nv + 2);
+            // prefixes at the lane's Z + 1 edges; a voxel's integral is the
+            // difference of its two edges'
+            float P[Z + 1];
 #pragma unroll
-            for (int q = 0; q < Z; q++) P[q] = row_prefix(t, fmaf(ze[q], inv, rho0), d.nv);
-            const float Ptop = row_prefix(t, fmaf(ztop, inv, rho0), d.nv);
+            for (int q = 0; q <= Z; q++) P[q] = row_prefix(t, fmaf(ze[q], inv, rho0), d.nv);
 #pragma unroll
-            for (int q = 0; q < Z; q++) {
-                float Pn = __shfl_down_sync(0xffffffffu, P[q], 1);
-                const float P0 = __shfl_sync(0xffffffffu, q + 1 < Z ? P[q + 1 < Z ? q + 1 : q] : Ptop, 0);
-                if (lane == 31) Pn = q + 1 < Z ? P0 : Ptop;
-                acc[q] = fmaf(w, Pn - P[q], acc[q]);
-            }
+            for (int q = 0; q < Z; q++) acc[q] = fmaf(w, P[q + 1] - P[q], acc[q]);
         }
     }
 #pragma unroll
     for (int q = 0; q < Z; q++) {
-        const int j = zbase + lane + 32 * q;
+        const int j = zbase + Z * lane + q;
         if (j < d.nz) {
             float* o = vol + (long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz + j;
             *o = accumulate ? *o + acc[q] : acc[q];
@@ -320,11 +363,12 @@ struct rn_cyl_plan {
     float* d_inplane = nullptr;   // [nview][nu] sqrt(1 + R_c^2) of each cell's central ray
     float* d_sedge = nullptr;     // [nv+1] row-edge rise per mm of in-plane distance
     float* d_rowlen = nullptr;    // [nv] sqrt(1 + s_c^2) of each row's central ray
-    double* d_invdr = nullptr;    // [nview][nu] 1 / |R_{u+1} - R_u|
+    float* d_invdr = nullptr;     // [nview][nu] 1 / |R_{u+1} - R_u|
     float* d_invinp = nullptr;    // [nview][nu] 1 / sqrt(1 + R_c^2)
     int bp_chunk = 0;             // views per backprojection launch (their row tables stay in L2)
-    float2* d_tab = nullptr;      // backprojection row tables [nb][nview][nu][nv+1]
-    float* d_zp = nullptr;        // forward-projection z prefix sums [nb][nx][ny][nz+1]
+    float2* d_tab = nullptr;      // backprojection row tables [nb][nview][nu][nv+2]
+    float* d_zp = nullptr;        // forward-projection z prefix band [nb][nx][ny][nbz]
+    int zlo = 0, nbz = 0;         // the band: heights zlo .. zlo + nbz - 1 (voxel units)
     long long launches = 0;
 };
 
@@ -362,7 +406,7 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
     std::vector<CylView> views(nview);
     std::vector<double> redge((size_t)nview * (nu + 1));
     std::vector<float> inplane((size_t)nview * nu), sedge(nv + 1), rowlen(nv), invinp((size_t)nview * nu);
-    std::vector<double> invdr((size_t)nview * nu);
+    std::vector<float> invdr((size_t)nview * nu);
     for (int iv = 0; iv < nview; iv++) {
         const float tf = host_deg[iv];
         const double t = (double)tf;
@@ -379,7 +423,7 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
             inplane[(size_t)iv * nu + u] = (float)std::sqrt(1 + Rc * Rc);
             invinp[(size_t)iv * nu + u] = (float)(1.0 / std::sqrt(1 + Rc * Rc));
             invdr[(size_t)iv * nu + u] =
-                1.0 / std::fabs(redge[(size_t)iv * (nu + 1) + u + 1] - redge[(size_t)iv * (nu + 1) + u]);
+                (float)(1.0 / std::fabs(redge[(size_t)iv * (nu + 1) + u + 1] - redge[(size_t)iv * (nu + 1) + u]));
         }
     }
     for (int e = 0; e <= nv; e++) sedge[e] = (float)(((e - 0.5) - (nv - 1) / 2.0 + g->off_v) * g->dv / g->dsd);
@@ -387,7 +431,7 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
         const double sc = ((double)v - (nv - 1) / 2.0 + g->off_v) * g->dv / g->dsd;
         rowlen[v] = (float)std::sqrt(1 + sc * sc);
     }
-    const size_t tab_elems = (size_t)g->nBatches * nview * nu * (nv + 1);
+    const size_t tab_elems = (size_t)g->nBatches * nview * nu * (nv + 2);
     auto fail = [&](cudaError_t e, const char* what) {
         rn_cyl_plan_destroy(p);
         return set_cuda_error(e, what);
@@ -399,21 +443,53 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
     if ((e = cudaMalloc(&p->d_sedge, sizeof(float) * sedge.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_rowlen, sizeof(float) * rowlen.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_tab, sizeof(float2) * tab_elems)) != cudaSuccess) return fail(e, "cyl: row tables");
-    if ((e = cudaMalloc(&p->d_zp, sizeof(float) * (size_t)g->nBatches * g->nx * g->ny * (g->nz + 1))) != cudaSuccess)
+    // The forward projection's z prefix band: the heights (voxel units) of
+    // every row edge on every plane of every view lie within s inp |D| / dz +
+    // zoff for s in the row-edge rises, inp in the cells' in-plane factors and
+    // |D| in the planes' distances from the source, so the band spans the
+    // extremes of that product (one cell of margin each side), cut to one
+    // height below and above the volume, where the prefix is constant.
+    {
+        double Dmin = 1e300, Dmax = 0.0;
+        for (int iv = 0; iv < nview; iv++) {
+            const bool xc = views[iv].xcls != 0;
+            const int np = xc ? g->ny : g->nx;
+            const double dm = xc ? g->dy : g->dx, cm = xc ? g->cy : g->cx, sm = xc ? views[iv].sy : views[iv].sx;
+            for (int k : {0, np - 1}) {
+                const double D = std::fabs((k + 0.5 - np / 2.0) * dm + cm - sm);
+                Dmin = std::min(Dmin, D);
+                Dmax = std::max(Dmax, D);
+            }
+        }
+        const double imin = *std::min_element(inplane.begin(), inplane.end()) * (1 - 1e-6);
+        const double imax = *std::max_element(inplane.begin(), inplane.end()) * (1 + 1e-6);
+        const double smin = sedge[0], smax = sedge[nv];
+        const double pmin = smin * (smin < 0 ? imax * Dmax : imin * Dmin);
+        const double pmax = smax * (smax > 0 ? imax * Dmax : imin * Dmin);
+        const double zoff = g->nz / 2.0 - g->cz / g->dz;
+        long long zlo = (long long)std::floor(pmin / g->dz + zoff) - 1;
+        long long zhi = (long long)std::ceil(pmax / g->dz + zoff) + 1;
+        zlo = std::max<long long>(zlo, -1);
+        zhi = std::min<long long>(zhi, (long long)g->nz + 1);
+        if (zhi < zlo + 1) zhi = zlo + 1;
+        p->zlo = (int)zlo;
+        p->nbz = (int)(zhi - zlo + 1);
+    }
+    if ((e = cudaMalloc(&p->d_zp, sizeof(float) * (size_t)g->nBatches * g->nx * g->ny * p->nbz)) != cudaSuccess)
         return fail(e, "cyl: z prefix sums");
-    if ((e = cudaMalloc(&p->d_invdr, sizeof(double) * invdr.size())) != cudaSuccess) return fail(e, "cyl: cells");
+    if ((e = cudaMalloc(&p->d_invdr, sizeof(float) * invdr.size())) != cudaSuccess) return fail(e, "cyl: cells");
     if ((e = cudaMalloc(&p->d_invinp, sizeof(float) * invinp.size())) != cudaSuccess) return fail(e, "cyl: cells");
     if ((e = cudaMemcpyAsync(p->d_views, views.data(), sizeof(CylView) * nview, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_redge, redge.data(), sizeof(double) * redge.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_inplane, inplane.data(), sizeof(float) * inplane.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_sedge, sedge.data(), sizeof(float) * sedge.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_rowlen, rowlen.data(), sizeof(float) * rowlen.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(p->d_invdr, invdr.data(), sizeof(double) * invdr.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(p->d_invdr, invdr.data(), sizeof(float) * invdr.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(p->d_invinp, invinp.data(), sizeof(float) * invinp.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return fail(e, "cyl: table upload");
     // backprojection launches take views in chunks whose row tables (nu x
-    // (nv + 1) float2 each) fill about 24 MB, well inside the 126 MB L2
-    p->bp_chunk = (int)std::max<long long>(1, (24ll << 20) / ((long long)nu * (nv + 1) * 8 * g->nBatches));
+    // (nv + 2) float2 each) fill about 24 MB, well inside the 126 MB L2
+    p->bp_chunk = (int)std::max<long long>(1, (24ll << 20) / ((long long)nu * (nv + 2) * 8 * g->nBatches));
     // the host vectors go out of scope: finish the copies first
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e, "cyl: table upload");
     *out = p;
@@ -443,13 +519,13 @@ extern "C" int rn_cyl_project(rn_cyl_plan* p, float* d_prj, const float* d_vol, 
     cudaStream_t st = (cudaStream_t)stream;
     const CylDims& d = p->d;
     const long long ncol = (long long)d.nb * d.nx * d.ny;
-    cyl_zprefix_kernel<<<(unsigned)((ncol * 32 + 255) / 256), 256, 0, st>>>(p->d_zp, d_vol, d);
+    cyl_zprefix_kernel<<<(unsigned)((ncol * 32 + 255) / 256), 256, 0, st>>>(p->d_zp, d_vol, d, p->zlo, p->nbz);
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     dim3 grid((unsigned)((d.nu + kCylFpWarps - 1) / kCylFpWarps), (unsigned)((d.nv + kCylRows - 1) / kCylRows),
               (unsigned)std::min<long long>((long long)d.nview * d.nb, 65535));
     cyl_fp_kernel<<<grid, 32 * kCylFpWarps, 0, st>>>(d_prj, p->d_zp, p->d_views, p->d_redge, p->d_inplane,
-                                                    p->d_sedge, p->d_rowlen, d);
+                                                    p->d_sedge, p->d_rowlen, d, p->zlo, p->nbz);
     p->launches++;
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;

@@ -483,19 +483,88 @@ __device__ __forceinline__ float2 shfl_xor2(float2 a, int m) {
     return make_float2(__shfl_xor_sync(0xffffffffu, a.x, m), __shfl_xor_sync(0xffffffffu, a.y, m));
 }
 
+// Tiles of 16 views x nu channels of one sinogram plane pass through shared
+// memory so that global loads and stores stay coalesced.  The kernels are
+// persistent: a CTA walks work items (plane, block of 16 views) with a stride
+// of the grid, and while it transforms one item the next item's tile arrives
+// by cp.async (4-byte copies, zero-filled beyond the last view) in the other
+// of two tile buffers, so the load latency is hidden behind the arithmetic.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+struct FiltTiles {
+    const float* prj;
+    float* out;
+    const float* pw;
+    const float* sw;
+    int nu, nview, nvb;      // nvb: view blocks per plane
+    long long su, sview, plane_elems;
+    int nv, nc;
+};
+
+// element offset of work item `it` (plane it / nvb, first view 16 (it % nvb))
+__device__ __forceinline__ long long filt_item(const FiltTiles& f, long long it, int& v0) {
+    const long long plane = it / f.nvb;
+    v0 = (int)(it - plane * f.nvb) * kRegViews;
+    const long long b = plane / ((long long)f.nv * f.nc), rem = plane - b * f.nv * f.nc;
+    return b * f.plane_elems + rem;
+}
+
+__device__ __forceinline__ void filt_issue(const FiltTiles& f, float* tile, long long it) {
+    constexpr int TS = kRegViews + 1;
+    int v0;
+    const long long off = filt_item(f, it, v0);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < f.nu * kRegViews; e += blockDim.x) {
+        const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
+        const bool ok = view < f.nview;
+        cp_async4(tile + n * TS + vv, ok ? f.prj + off + (long long)n * f.su + (long long)view * f.sview : f.prj, ok);
+    }
+}
+
+__device__ __forceinline__ void filt_store(const FiltTiles& f, const float* tile, long long it) {
+    constexpr int TS = kRegViews + 1;
+    int v0;
+    const long long off = filt_item(f, it, v0);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < f.nu * kRegViews; e += blockDim.x) {
+        const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
+        if (view < f.nview) f.out[off + (long long)n * f.su + (long long)view * f.sview] = tile[n * TS + vv];
+    }
+}
+
+// channel n of this warp's two views (columns 2 warp, 2 warp + 1 of the tile),
+// pre-weighted (and short-scan weighted) as the filter's input
+__device__ __forceinline__ float2 filt_input(const FiltTiles& f, const float* tile, int n, int warp, int v0) {
+    constexpr int TS = kRegViews + 1;
+    const float p = __ldg(f.pw + n);
+    float a = tile[n * TS + 2 * warp] * p, b = tile[n * TS + 2 * warp + 1] * p;
+    if (f.sw) {
+        const int va = v0 + 2 * warp;
+        a *= va < f.nview ? __ldg(f.sw + (long long)n * f.nview + va) : 0.f;
+        b *= va + 1 < f.nview ? __ldg(f.sw + (long long)n * f.nview + va + 1) : 0.f;
+    }
+    return make_float2(a, b);
+}
+
+// Per work item, each warp transforms one complex signal (its two views)
+// through both halves.  The even half's output y0 is parked in the tile in
+// place of the input, which the odd half no longer needs once it has read it.
 template <int L>
-__global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ out, const float* __restrict__ prj,
-                                                           const float2* __restrict__ Hp,
-                                                           const float2* __restrict__ Tw,
-                                                           const float* __restrict__ pw,
-                                                           const float* __restrict__ sw, int nu, int nview, int nv,
-                                                           int nc, int nplane_total, float scale, RegFftTw<L> tw) {
-    extern __shared__ float tile[];            // [nu][kRegViews + 1], then [8 warps][nu] float2
+__global__ void __launch_bounds__(256, 1) filter_reg_kernel(FiltTiles f, const float2* __restrict__ Hp,
+                                                           const float2* __restrict__ Tw, long long nitems,
+                                                           float scale, RegFftTw<L> tw) {
+    extern __shared__ float tiles[];           // two tiles of [nu][kRegViews + 1]
     constexpr int TS = kRegViews + 1, M = 32 * L;
     const float2* __restrict__ Pre = Tw + M;   // exp(-2 pi i n / N), n < M
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // the even half's output, held while the odd half runs
-    float2* ybuf = reinterpret_cast<float2*>(tile + ((nu * TS + 1) & ~1)) + (long long)warp * nu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile_floats = (f.nu * TS + 1) & ~1;
+    const int nu = f.nu;
     // this lane's twiddle in each cross-lane stage: exp(-2 pi i (lane mod h) / 2h)
     float2 wl[5];
 #pragma unroll
@@ -503,75 +572,79 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
         const int h = 1 << s;
         wl[s] = tw.w32[(lane & (h - 1)) * (16 / h)];
     }
-    const long long su = (long long)nview * nv * nc, sview = (long long)nv * nc;
-    const int v0 = blockIdx.x * kRegViews;
-    for (int plane = blockIdx.y; plane < nplane_total; plane += gridDim.y) {
-        const int b = plane / (nv * nc);
-        const int rem = plane - b * nv * nc;
-        const long long off = (long long)b * nu * nview * nv * nc + rem;
-#pragma unroll 4
-        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
-            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
-            float x = 0.f;
-            if (view < nview) {
-                x = prj[off + (long long)n * su + (long long)view * sview] * pw[n];
-                if (sw) x *= sw[(long long)n * nview + view];
-            }
-            tile[n * TS + vv] = x;
-        }
-        __syncthreads();
-#pragma unroll 1
-        for (int half = 0; half < 2; half++) {
-            float2 v[L];
+    auto forward = [&](float2 (&v)[L], int half) {
+        reg_local_dif<L>(v, tw);
+#pragma unroll
+        for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
+#pragma unroll
+        for (int s = 4; s >= 0; s--) {
+            const int h = 1 << s;
+            const bool up = (lane & h) != 0;
 #pragma unroll
             for (int r = 0; r < L; r++) {
-                const int n = lane + 32 * r;
-                v[r] = n < nu ? make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1])
-                              : make_float2(0.f, 0.f);
-                if (half) v[r] = c_mul(v[r], __ldg(Pre + r * 32 + lane));
+                const float2 p = shfl_xor2(v[r], h);
+                v[r] = up ? c_mul(c_sub(p, v[r]), wl[s]) : c_add(v[r], p);
             }
-            // forward
-            reg_local_dif<L>(v, tw);
+        }
+        // this half of the kernel's spectrum (scaled by 1/N), then the inverse
 #pragma unroll
-            for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
+        for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Hp + half * M + r * 32 + lane));
 #pragma unroll
-            for (int s = 4; s >= 0; s--) {
-                const int h = 1 << s;
-                const bool up = (lane & h) != 0;
+        for (int s = 0; s < 5; s++) {
+            const int h = 1 << s;
+            const bool up = (lane & h) != 0;
 #pragma unroll
-                for (int r = 0; r < L; r++) {
-                    const float2 p = shfl_xor2(v[r], h);
-                    v[r] = up ? c_mul(c_sub(p, v[r]), wl[s]) : c_add(v[r], p);
-                }
+            for (int r = 0; r < L; r++) {
+                const float2 t = up ? c_mulc(v[r], wl[s]) : v[r];
+                const float2 p = shfl_xor2(t, h);
+                v[r] = up ? c_sub(p, t) : c_add(v[r], p);
             }
-            // this half of the kernel's spectrum (scaled by 1/N), then the inverse
+        }
 #pragma unroll
-            for (int r = 0; r < L; r++) v[r] = c_mul(v[r], __ldg(Hp + half * M + r * 32 + lane));
+        for (int r = 0; r < L; r++) v[r] = c_mulc(v[r], __ldg(Tw + r * 32 + lane));
+        reg_local_dit_inv<L>(v, tw);
+    };
+    long long it = blockIdx.x;
+    if (it < nitems) filt_issue(f, tiles, it);
+    cp_async_commit();
+    for (int b = 0; it < nitems; it += gridDim.x, b ^= 1) {
+        float* tile = tiles + b * tile_floats;
+        if (it + gridDim.x < nitems) filt_issue(f, tiles + (b ^ 1) * tile_floats, it + gridDim.x);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();
+        int v0;
+        filt_item(f, it, v0);
+        float2 v[L];
 #pragma unroll
-            for (int s = 0; s < 5; s++) {
-                const int h = 1 << s;
-                const bool up = (lane & h) != 0;
-#pragma unroll
-                for (int r = 0; r < L; r++) {
-                    const float2 t = up ? c_mulc(v[r], wl[s]) : v[r];
-                    const float2 p = shfl_xor2(t, h);
-                    v[r] = up ? c_sub(p, t) : c_add(v[r], p);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < L; r++) v[r] = c_mulc(v[r], __ldg(Tw + r * 32 + lane));
-            reg_local_dit_inv<L>(v, tw);
+        for (int r = 0; r < L; r++) {
+            const int n = lane + 32 * r;
+            v[r] = n < nu ? filt_input(f, tile, n, warp, v0) : make_float2(0.f, 0.f);
+        }
+#pragma unroll 1
+        for (int half = 0; half < 2; half++) {
+            forward(v, half);
             if (half == 0) {
-#pragma unroll
-                for (int r = 0; r < L; r++)
-                    if (lane + 32 * r < nu) ybuf[lane + 32 * r] = v[r];
-            } else {
-                // each warp writes back only its own two columns
+                // park y0 in the tile, take the odd half's input
 #pragma unroll
                 for (int r = 0; r < L; r++) {
                     const int n = lane + 32 * r;
                     if (n < nu) {
-                        const float2 y = c_add(ybuf[n], c_mulc(v[r], __ldg(Pre + r * 32 + lane)));
+                        const float2 x = filt_input(f, tile, n, warp, v0);
+                        tile[n * TS + 2 * warp] = v[r].x;
+                        tile[n * TS + 2 * warp + 1] = v[r].y;
+                        v[r] = c_mul(x, __ldg(Pre + r * 32 + lane));
+                    } else {
+                        v[r] = make_float2(0.f, 0.f);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < L; r++) {
+                    const int n = lane + 32 * r;
+                    if (n < nu) {
+                        const float2 y0 = make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1]);
+                        const float2 y = c_add(y0, c_mulc(v[r], __ldg(Pre + r * 32 + lane)));
                         tile[n * TS + 2 * warp] = y.x * scale;
                         tile[n * TS + 2 * warp + 1] = y.y * scale;
                     }
@@ -579,12 +652,8 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
             }
         }
         __syncthreads();
-#pragma unroll 4
-        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
-            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
-            if (view < nview) out[off + (long long)n * su + (long long)view * sview] = tile[n * TS + vv];
-        }
-        __syncthreads();   // the next plane refills the tile
+        filt_store(f, tile, it);
+        __syncthreads();   // the item after next refills this tile
     }
 }
 
@@ -599,76 +668,80 @@ __global__ void __launch_bounds__(256, 1) filter_reg_kernel(float* __restrict__ 
 // shuffle stages.
 constexpr int kTrStride = 33;   // float2 row stride of a warp's transpose block
 
-__global__ void __launch_bounds__(256, 1) filter_tr_kernel(float* __restrict__ out, const float* __restrict__ prj,
-                                                          const float2* __restrict__ Hq,
-                                                          const float2* __restrict__ Tw,
-                                                          const float* __restrict__ pw,
-                                                          const float* __restrict__ sw, int nu, int nview, int nv,
-                                                          int nc, int nplane_total, float scale, RegFftTw<32> tw) {
+__global__ void __launch_bounds__(256, 1) filter_tr_kernel(FiltTiles f, const float2* __restrict__ Hq,
+                                                          const float2* __restrict__ Tw, long long nitems,
+                                                          float scale, RegFftTw<32> tw) {
     constexpr int L = 32, M = 1024, TS = kRegViews + 1;
-    // [nu][kRegViews + 1] floats, then [8 warps][nu] float2 (the even half's
-    // output), then [8 warps][32][33] float2 (the transpose blocks)
-    extern __shared__ float tile[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // two tiles of [nu][kRegViews + 1] floats, then [8 warps][32][33] float2
+    // (the transpose blocks)
+    extern __shared__ float tiles[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nu = f.nu;
     const float2* __restrict__ Pre = Tw + M;
-    float2* ybuf = reinterpret_cast<float2*>(tile + ((nu * TS + 1) & ~1)) + (long long)warp * nu;
-    float2* tr = reinterpret_cast<float2*>(tile + ((nu * TS + 1) & ~1)) + 8 * nu + warp * (32 * kTrStride);
-    const long long su = (long long)nview * nv * nc, sview = (long long)nv * nc;
-    const int v0 = blockIdx.x * kRegViews;
-    for (int plane = blockIdx.y; plane < nplane_total; plane += gridDim.y) {
-        const int b = plane / (nv * nc);
-        const int rem = plane - b * nv * nc;
-        const long long off = (long long)b * nu * nview * nv * nc + rem;
-#pragma unroll 4
-        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
-            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
-            float x = 0.f;
-            if (view < nview) {
-                x = prj[off + (long long)n * su + (long long)view * sview] * pw[n];
-                if (sw) x *= sw[(long long)n * nview + view];
-            }
-            tile[n * TS + vv] = x;
-        }
+    const int tile_floats = (nu * TS + 1) & ~1;
+    float2* tr = reinterpret_cast<float2*>(tiles + 2 * tile_floats) + warp * (32 * kTrStride);
+    auto forward = [&](float2 (&v)[L], int half) {
+        reg_local_dif<L>(v, tw);
+#pragma unroll
+        for (int r = 0; r < L; r++) tr[r * kTrStride + lane] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < L; c++) v[c] = tr[lane * kTrStride + c];
+        reg_local_dif<L>(v, tw);
+        // this half of the kernel's spectrum (scaled by 1/N), then the inverse
+#pragma unroll
+        for (int c = 0; c < L; c++) v[c] = c_mul(v[c], __ldg(Hq + half * M + c * 32 + lane));
+        reg_local_dit_inv<L>(v, tw);
+        __syncwarp();   // every lane has read its row of the block
+#pragma unroll
+        for (int c = 0; c < L; c++) tr[lane * kTrStride + c] = v[c];
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < L; r++) v[r] = c_mulc(tr[r * kTrStride + lane], __ldg(Tw + r * 32 + lane));
+        reg_local_dit_inv<L>(v, tw);
+        __syncwarp();   // the block is free for the next half
+    };
+    long long it = blockIdx.x;
+    if (it < nitems) filt_issue(f, tiles, it);
+    cp_async_commit();
+    for (int b = 0; it < nitems; it += gridDim.x, b ^= 1) {
+        float* tile = tiles + b * tile_floats;
+        if (it + gridDim.x < nitems) filt_issue(f, tiles + (b ^ 1) * tile_floats, it + gridDim.x);
+        cp_async_commit();
+        cp_async_wait_prev();
         __syncthreads();
+        int v0;
+        filt_item(f, it, v0);
+        float2 v[L];
+#pragma unroll
+        for (int r = 0; r < L; r++) {
+            const int n = lane + 32 * r;
+            v[r] = n < nu ? filt_input(f, tile, n, warp, v0) : make_float2(0.f, 0.f);
+        }
 #pragma unroll 1
         for (int half = 0; half < 2; half++) {
-            float2 v[L];
-#pragma unroll
-            for (int r = 0; r < L; r++) {
-                const int n = lane + 32 * r;
-                v[r] = n < nu ? make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1])
-                              : make_float2(0.f, 0.f);
-                if (half) v[r] = c_mul(v[r], __ldg(Pre + r * 32 + lane));
-            }
-            reg_local_dif<L>(v, tw);
-#pragma unroll
-            for (int r = 0; r < L; r++) tr[r * kTrStride + lane] = c_mul(v[r], __ldg(Tw + r * 32 + lane));
-            __syncwarp();
-#pragma unroll
-            for (int c = 0; c < L; c++) v[c] = tr[lane * kTrStride + c];
-            reg_local_dif<L>(v, tw);
-            // this half of the kernel's spectrum (scaled by 1/N), then the inverse
-#pragma unroll
-            for (int c = 0; c < L; c++) v[c] = c_mul(v[c], __ldg(Hq + half * M + c * 32 + lane));
-            reg_local_dit_inv<L>(v, tw);
-            __syncwarp();   // every lane has read its row of the block
-#pragma unroll
-            for (int c = 0; c < L; c++) tr[lane * kTrStride + c] = v[c];
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < L; r++) v[r] = c_mulc(tr[r * kTrStride + lane], __ldg(Tw + r * 32 + lane));
-            reg_local_dit_inv<L>(v, tw);
-            __syncwarp();   // the block is free for the next half
+            forward(v, half);
             if (half == 0) {
+                // park y0 in the tile, take the odd half's input
 #pragma unroll
-                for (int r = 0; r < L; r++)
-                    if (lane + 32 * r < nu) ybuf[lane + 32 * r] = v[r];
+                for (int r = 0; r < L; r++) {
+                    const int n = lane + 32 * r;
+                    if (n < nu) {
+                        const float2 x = filt_input(f, tile, n, warp, v0);
+                        tile[n * TS + 2 * warp] = v[r].x;
+                        tile[n * TS + 2 * warp + 1] = v[r].y;
+                        v[r] = c_mul(x, __ldg(Pre + r * 32 + lane));
+                    } else {
+                        v[r] = make_float2(0.f, 0.f);
+                    }
+                }
             } else {
 #pragma unroll
                 for (int r = 0; r < L; r++) {
                     const int n = lane + 32 * r;
                     if (n < nu) {
-                        const float2 y = c_add(ybuf[n], c_mulc(v[r], __ldg(Pre + r * 32 + lane)));
+                        const float2 y0 = make_float2(tile[n * TS + 2 * warp], tile[n * TS + 2 * warp + 1]);
+                        const float2 y = c_add(y0, c_mulc(v[r], __ldg(Pre + r * 32 + lane)));
                         tile[n * TS + 2 * warp] = y.x * scale;
                         tile[n * TS + 2 * warp + 1] = y.y * scale;
                     }
@@ -676,19 +749,53 @@ __global__ void __launch_bounds__(256, 1) filter_tr_kernel(float* __restrict__ o
             }
         }
         __syncthreads();
-#pragma unroll 4
-        for (int e = tid; e < nu * kRegViews; e += blockDim.x) {
-            const int n = e / kRegViews, vv = e - n * kRegViews, view = v0 + vv;
-            if (view < nview) out[off + (long long)n * su + (long long)view * sview] = tile[n * TS + vv];
-        }
-        __syncthreads();   // the next plane refills the tile
+        filt_store(f, tile, it);
+        __syncthreads();   // the item after next refills this tile
     }
+}
+
+static int sm_count_cached() {
+    static int sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && sms[dev] > 0) return sms[dev];
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    if (dev < 64) sms[dev] = n;
+    return n;
+}
+
+static FiltTiles filt_tiles(float* d_out, const float* d_prj, const FilterVal& fv, const float* d_sw, int nu,
+                            int nview, int nv, int nc) {
+    FiltTiles f;
+    f.prj = d_prj;
+    f.out = d_out;
+    f.pw = fv.d_pw;
+    f.sw = d_sw;
+    f.nu = nu;
+    f.nview = nview;
+    f.nvb = (nview + kRegViews - 1) / kRegViews;
+    f.su = (long long)nview * nv * nc;
+    f.sview = (long long)nv * nc;
+    f.plane_elems = (long long)nu * nview * nv * nc;
+    f.nv = nv;
+    f.nc = nc;
+    return f;
+}
+
+template <class K>
+static int launch_persistent(K kernel, size_t smem, long long nitems, unsigned& grid) {
+    RN_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    RN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
+    if (per_sm <= 0) return set_error(RN_ERR_ARG, "filter: sinogram rows too long for shared memory");
+    grid = (unsigned)std::min<long long>(nitems, (long long)per_sm * sm_count_cached());
+    return RN_OK;
 }
 
 template <int L>
 static int launch_filter_reg(float* d_out, const float* d_prj, const FilterVal& fv, const float* d_sw, int nu,
-                             int nview, int nv, int nc, int nplanes, unsigned grid_planes, float scale,
-                             cudaStream_t st) {
+                             int nview, int nv, int nc, long long nplanes, float scale, cudaStream_t st) {
     RegFftTw<L> tw;
     for (int k = 0; k < L / 2; k++) {
         const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / (double)L);
@@ -698,29 +805,30 @@ static int launch_filter_reg(float* d_out, const float* d_prj, const FilterVal& 
         const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / 32.0);
         tw.w32[k] = make_float2((float)w.real(), (float)w.imag());
     }
-    const size_t smem = sizeof(float) * (((size_t)nu * (kRegViews + 1) + 1) & ~(size_t)1) + sizeof(float2) * 8 * nu;
-    RN_CUDA_TRY(cudaFuncSetAttribute(filter_reg_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)((nview + kRegViews - 1) / kRegViews), grid_planes);
-    filter_reg_kernel<L><<<grid, 256, smem, st>>>(d_out, d_prj, fv.d_Hp, fv.d_Tw, fv.d_pw, d_sw, nu, nview, nv, nc,
-                                                  nplanes, scale, tw);
+    const FiltTiles f = filt_tiles(d_out, d_prj, fv, d_sw, nu, nview, nv, nc);
+    const long long nitems = (long long)f.nvb * nplanes;
+    const size_t smem = sizeof(float) * 2 * (((size_t)nu * (kRegViews + 1) + 1) & ~(size_t)1);
+    unsigned grid = 0;
+    RN_TRY(launch_persistent(filter_reg_kernel<L>, smem, nitems, grid));
+    filter_reg_kernel<L><<<grid, 256, smem, st>>>(f, fv.d_Hp, fv.d_Tw, nitems, scale, tw);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
 
 static int launch_filter_tr(float* d_out, const float* d_prj, const FilterVal& fv, const float* d_sw, int nu,
-                            int nview, int nv, int nc, int nplanes, unsigned grid_planes, float scale,
-                            cudaStream_t st) {
+                            int nview, int nv, int nc, long long nplanes, float scale, cudaStream_t st) {
     RegFftTw<32> tw;
     for (int k = 0; k < 16; k++) {
         const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / 32.0);
         tw.local[k] = tw.w32[k] = make_float2((float)w.real(), (float)w.imag());
     }
-    const size_t smem = sizeof(float) * (((size_t)nu * (kRegViews + 1) + 1) & ~(size_t)1) +
-                        sizeof(float2) * 8 * ((size_t)nu + 32 * kTrStride);
-    RN_CUDA_TRY(cudaFuncSetAttribute(filter_tr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)((nview + kRegViews - 1) / kRegViews), grid_planes);
-    filter_tr_kernel<<<grid, 256, smem, st>>>(d_out, d_prj, fv.d_Hp, fv.d_Tw, fv.d_pw, d_sw, nu, nview, nv, nc,
-                                              nplanes, scale, tw);
+    const FiltTiles f = filt_tiles(d_out, d_prj, fv, d_sw, nu, nview, nv, nc);
+    const long long nitems = (long long)f.nvb * nplanes;
+    const size_t smem = sizeof(float) * 2 * (((size_t)nu * (kRegViews + 1) + 1) & ~(size_t)1) +
+                        sizeof(float2) * 8 * 32 * kTrStride;
+    unsigned grid = 0;
+    RN_TRY(launch_persistent(filter_tr_kernel, smem, nitems, grid));
+    filter_tr_kernel<<<grid, 256, smem, st>>>(f, fv.d_Hp, fv.d_Tw, nitems, scale, tw);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
@@ -747,9 +855,9 @@ int filter_device(float* d_out, const float* d_prj, int nb, int nc, int nu, int 
     const unsigned grid_planes = (unsigned)std::min<long long>(nplanes, 65535);
     if (g_filter_form == 0 && fv.d_Hp) {
         const int N = 1 << fv.logN;
-        if (N == 2048) return launch_filter_tr(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
-        if (N == 1024) return launch_filter_reg<16>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
-        return launch_filter_reg<8>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, (int)nplanes, grid_planes, (float)scale, st);
+        if (N == 2048) return launch_filter_tr(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, nplanes, (float)scale, st);
+        if (N == 1024) return launch_filter_reg<16>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, nplanes, (float)scale, st);
+        return launch_filter_reg<8>(d_out, d_prj, fv, d_sw, nu, nview, nv, nc, nplanes, (float)scale, st);
     }
     if (fv.logN > 0 && g_filter_form <= 1) {
         // S signals (2S views) per CTA: ~64 KB of shared memory at N = 2048
