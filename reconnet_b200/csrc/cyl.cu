@@ -73,7 +73,7 @@ struct CylDims {
 constexpr int kCylFpWarps = 8;   // detector columns per forward-projection CTA
 constexpr int kCylRows = 64;     // detector rows per forward-projection warp (two per lane)
 constexpr int kCylBpWarps = 8;   // voxel columns per backprojection CTA
-constexpr int kCylBpZ = 4;       // voxels per lane along z (a warp covers 128)
+constexpr int kCylBpZ = 2;       // voxels per lane along z (a warp covers 64)
 constexpr float kCylFloorBias = 12582912.0f;   // 1.5 * 2^23: adding it rounds to an integer
 constexpr int kCylFloorBiasBits = 0x4B400000;
 
@@ -264,19 +264,28 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
                                                                  const double* __restrict__ redge,
                                                                  const float* __restrict__ inv_dr,
                                                                  const float* __restrict__ inv_inp, CylDims d,
-                                                                 int v_begin, int v_end, int accumulate) {
+                                                                 int v_begin, int v_end, int accumulate, int vz0,
+                                                                 int vz1) {
     constexpr int Z = kCylBpZ;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long column = (long long)blockIdx.x * kCylBpWarps + warp;
     if (column >= (long long)d.nx * d.ny) return;              // whole warp
     const int ix = (int)(column / d.ny), iy = (int)(column % d.ny);
     const int b = blockIdx.z;
-    const int zbase = blockIdx.y * 32 * Z;
+    // Only voxels vz0 <= j < vz1 can meet a detector row (the plan bounds the
+    // rows' heights over every view and plane); the first launch of a
+    // backprojection writes 0 to the rest of the column.
+    if (!accumulate && blockIdx.y == 0) {
+        float* o = vol + (long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz;
+        for (int j = lane; j < d.nz; j += 32)
+            if (j < vz0 || j >= vz1) o[j] = 0.f;
+    }
+    const int zbase = vz0 + blockIdx.y * 32 * Z;
     // lane holds voxels zbase + Z lane + q; z (mm) of their Z + 1 edges
     float ze[Z + 1];
 #pragma unroll
     for (int q = 0; q <= Z; q++) ze[q] = (float)((zbase + Z * lane + q - d.nz / 2.0) * d.dz + d.cz);
-    const float zlast = (float)((min(d.nz, zbase + 32 * Z) - d.nz / 2.0) * d.dz + d.cz);
+    const float zlast = (float)((min(vz1, zbase + 32 * Z) - d.nz / 2.0) * d.dz + d.cz);
     const float zfirst = (float)((zbase - d.nz / 2.0) * d.dz + d.cz);
     const float rho0 = (float)(d.nv / 2.0 - d.off_v);
     const float dsd_dv = (float)(d.dsd / d.dv);
@@ -343,7 +352,7 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
 #pragma unroll
     for (int q = 0; q < Z; q++) {
         const int j = zbase + Z * lane + q;
-        if (j < d.nz) {
+        if (j < vz1) {
             float* o = vol + (long long)b * d.vol_stride + ((long long)ix * d.ny + iy) * d.nz + j;
             *o = accumulate ? *o + acc[q] : acc[q];
         }
@@ -369,6 +378,7 @@ struct rn_cyl_plan {
     float2* d_tab = nullptr;      // backprojection row tables [nb][nview][nu][nv+2]
     float* d_zp = nullptr;        // forward-projection z prefix band [nb][nx][ny][nbz]
     int zlo = 0, nbz = 0;         // the band: heights zlo .. zlo + nbz - 1 (voxel units)
+    int vz0 = 0, vz1 = 0;         // voxels that can meet a detector row: vz0 <= j < vz1
     long long launches = 0;
 };
 
@@ -443,29 +453,37 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
     if ((e = cudaMalloc(&p->d_sedge, sizeof(float) * sedge.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_rowlen, sizeof(float) * rowlen.size())) != cudaSuccess) return fail(e, "cyl: rows");
     if ((e = cudaMalloc(&p->d_tab, sizeof(float2) * tab_elems)) != cudaSuccess) return fail(e, "cyl: row tables");
-    // The forward projection's z prefix band: the heights (voxel units) of
-    // every row edge on every plane of every view lie within s inp |D| / dz +
-    // zoff for s in the row-edge rises, inp in the cells' in-plane factors and
-    // |D| in the planes' distances from the source, so the band spans the
-    // extremes of that product (one cell of margin each side), cut to one
-    // height below and above the volume, where the prefix is constant.
+    // The forward projection's z prefix band.  A row edge of rise s sits, on
+    // a plane, at height s r / dz + zoff, r the in-plane distance from the
+    // source to where the cell's central ray meets the plane.  Both passes
+    // use a plane only where the cell's footprint meets the volume, so r is
+    // at most the distance from the source to the volume's in-plane box
+    // grown by one voxel and one footprint width (and at least the distance
+    // to that box); the band spans s r / dz + zoff over those extremes, with
+    // one cell of margin each side, cut to one height below and above the
+    // volume, where the prefix is constant.
     {
-        double Dmin = 1e300, Dmax = 0.0;
+        // a footprint's lateral width on a plane is |D| da (1 + R^2) to first
+        // order, R the lateral slope of its rays
+        double rsl = 0.0;
+        for (double r : redge) rsl = std::max(rsl, std::fabs(r));
+        const double grow = std::max(g->dx, g->dy) + (g->dso + std::hypot(0.5 * g->nx * g->dx + std::fabs(g->cx),
+                                                                          0.5 * g->ny * g->dy + std::fabs(g->cy))) *
+                                                        g->da * (1 + rsl * rsl) * 1.5;
+        const double bx0 = -0.5 * g->nx * g->dx + g->cx - grow, bx1 = 0.5 * g->nx * g->dx + g->cx + grow;
+        const double by0 = -0.5 * g->ny * g->dy + g->cy - grow, by1 = 0.5 * g->ny * g->dy + g->cy + grow;
+        double rmin = 1e300, rmax = 0.0;
         for (int iv = 0; iv < nview; iv++) {
-            const bool xc = views[iv].xcls != 0;
-            const int np = xc ? g->ny : g->nx;
-            const double dm = xc ? g->dy : g->dx, cm = xc ? g->cy : g->cx, sm = xc ? views[iv].sy : views[iv].sx;
-            for (int k : {0, np - 1}) {
-                const double D = std::fabs((k + 0.5 - np / 2.0) * dm + cm - sm);
-                Dmin = std::min(Dmin, D);
-                Dmax = std::max(Dmax, D);
-            }
+            const double sx = views[iv].sx, sy = views[iv].sy;
+            for (double x : {bx0, bx1})
+                for (double y : {by0, by1}) rmax = std::max(rmax, std::hypot(x - sx, y - sy));
+            const double qx = std::min(std::max(sx, bx0), bx1), qy = std::min(std::max(sy, by0), by1);
+            rmin = std::min(rmin, std::hypot(qx - sx, qy - sy));
         }
-        const double imin = *std::min_element(inplane.begin(), inplane.end()) * (1 - 1e-6);
-        const double imax = *std::max_element(inplane.begin(), inplane.end()) * (1 + 1e-6);
         const double smin = sedge[0], smax = sedge[nv];
-        const double pmin = smin * (smin < 0 ? imax * Dmax : imin * Dmin);
-        const double pmax = smax * (smax > 0 ? imax * Dmax : imin * Dmin);
+        double pmin = std::min(smin * rmin, smin * rmax), pmax = std::max(smax * rmin, smax * rmax);
+        if (!(pmin > -1e9)) pmin = -1e9;   // unbounded footprints: the whole volume
+        if (!(pmax < 1e9)) pmax = 1e9;
         const double zoff = g->nz / 2.0 - g->cz / g->dz;
         long long zlo = (long long)std::floor(pmin / g->dz + zoff) - 1;
         long long zhi = (long long)std::ceil(pmax / g->dz + zoff) + 1;
@@ -474,6 +492,9 @@ extern "C" int rn_cyl_plan_create(rn_cyl_plan** out, const RnCylGeom* g, const f
         if (zhi < zlo + 1) zhi = zlo + 1;
         p->zlo = (int)zlo;
         p->nbz = (int)(zhi - zlo + 1);
+        // voxel j spans heights [j, j + 1]: those inside the band's heights
+        p->vz0 = (int)std::max<long long>(zlo, 0);
+        p->vz1 = (int)std::max<long long>(std::min<long long>(zhi, g->nz), p->vz0 + 1);
     }
     if ((e = cudaMalloc(&p->d_zp, sizeof(float) * (size_t)g->nBatches * g->nx * g->ny * p->nbz)) != cudaSuccess)
         return fail(e, "cyl: z prefix sums");
@@ -543,11 +564,11 @@ extern "C" int rn_cyl_backproject(rn_cyl_plan* p, float* d_vol, const float* d_p
     RN_CUDA_TRY(cudaGetLastError());
     if (d.nb > 65535) return set_error(RN_ERR_ARG, "cyl: too many batches");
     dim3 grid((unsigned)(((long long)d.nx * d.ny + kCylBpWarps - 1) / kCylBpWarps),
-              (unsigned)((d.nz + 32 * kCylBpZ - 1) / (32 * kCylBpZ)), (unsigned)d.nb);
+              (unsigned)((p->vz1 - p->vz0 + 32 * kCylBpZ - 1) / (32 * kCylBpZ)), (unsigned)d.nb);
     for (int v0 = 0; v0 < d.nview; v0 += p->bp_chunk) {
         const int v1 = std::min(d.nview, v0 + p->bp_chunk);
         cyl_bp_kernel<<<grid, 32 * kCylBpWarps, 0, st>>>(d_vol, p->d_tab, p->d_views, p->d_redge, p->d_invdr,
-                                                        p->d_invinp, d, v0, v1, v0 > 0 ? 1 : 0);
+                                                        p->d_invinp, d, v0, v1, v0 > 0 ? 1 : 0, p->vz0, p->vz1);
         p->launches++;
         RN_CUDA_TRY(cudaGetLastError());
     }

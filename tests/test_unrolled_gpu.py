@@ -4,9 +4,11 @@ over 360 degrees, 12 ordered subsets), 10 unrolled iterations, each with a
 learnable step scale and TV weight, checkpointed per iteration.
 
 * Gradients with respect to the 20 parameters and the starting image against
-  central finite differences (eps = 1e-3 for the parameters, a step of 1e-4
-  along the gradient for the starting image, each Richardson-combined with
-  half the step), relative error <= 5e-3.
+  central finite differences (eps = 1e-3 for the parameters; for the starting
+  image a step along the gradient whose largest pixel is 1e-6, small against
+  the TV terms' sqrt(d^2 + 1e-6) curvature in pixels whose data weights are
+  photon-starved; each Richardson-combined with half the step), relative
+  error <= 5e-3.
 * The same unrolled loop built on the reference library's own
   cDistanceDrivenFan{Projection,Backprojection} (oracle/_ref, when present),
   with the reference's gradient registration (python/ReconNet.py:773-830:
@@ -98,12 +100,16 @@ def test_unrolled_config_gradients_match_finite_differences():
                 assert abs(fd - float(grad[i])) <= 5e-3 * abs(fd) + 1e-9, (first, i, fd, float(grad[i]))
     x_init = (0.01 * torch.rand_like(truth)).requires_grad_(True)
     gx, = torch.autograd.grad(loss(step.detach(), tvw.detach(), x_init), (x_init,))
-    v = gx / gx.abs().max() * 1e-4
+    # The ten iterations are strongly nonlinear along the gradient: it is
+    # largest where photon-starved rays leave the SQS denominator to the TV
+    # terms, whose curvature scale is sqrt(1e-6) = 1e-3.  Steps with a largest
+    # pixel of 1e-4 / 1e-5 / 1e-6 give 9% / 1.6% / 0.07% errors on this
+    # workload (measured), while the FP32 roundoff of the loss difference stays
+    # below 1e-3 of it at 1e-6.
+    v = gx / gx.abs().max() * 1e-6
     with torch.no_grad():
         def central_x(h):
             return float(loss(step, tvw, x_init + h * v) - loss(step, tvw, x_init - h * v)) / (2 * h)
-        # Richardson-combined as for the parameters: a step small enough for
-        # the plain difference drowns in the FP32 roundoff of ten iterations
         fd = (4 * central_x(0.5) - central_x(1.0)) / 3
     assert abs(fd - float((gx * v).sum())) <= 5e-3 * abs(fd), (fd, float((gx * v).sum()))
 
