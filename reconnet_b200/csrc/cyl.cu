@@ -172,43 +172,68 @@ __global__ void __launch_bounds__(32 * kCylFpWarps) cyl_fp_kernel(float* __restr
         for (int q = 0; q < 3; q++) sz[q] = sl[q] * inp * inv_dz;
         const float szb = s_bot * inp * inv_dz, szt = s_top * inp * inv_dz;
         float acc0 = 0.f, acc1 = 0.f;
-        for (int k = 0; k < nplane; k++) {
-            const double D = fma((double)k, dmain, D0);
-            const double lo = fma((double)k, dlo, lo0), hi = fma((double)k, dhi, hi0);
-            const double flo_d = floor(lo), fhi_d = floor(hi);
-            const int ilo = (int)flo_d, ihi = (int)fhi_d;
-            const int i0 = max(ilo, 0), i1 = min(ihi, nlat - 1);
-            if (i0 > i1) continue;                                   // warp-uniform
-            const float aD = (float)fabs(D);
-            // the warp's rows against the volume's z extent
-            if (fmaf(szt, aD, zoffb) <= zvol0 || fmaf(szb, aD, zoffb) >= zvol1) continue;
-            const float flo = (float)(lo - flo_d), fhi = (float)(hi - fhi_d);
-            // each edge's cell m and fraction f in the band
-            unsigned m[3];
-            float f[3];
+        // Planes go in groups of 32: lane l first works out plane k0 + l's
+        // lateral terms (the footprint's voxel columns and end fractions, the
+        // distance |D| and the plane weight), which are the same for every
+        // row, and the warp then walks the group's planes with them
+        // broadcast by shuffles.
+        for (int k0 = 0; k0 < nplane; k0 += 32) {
+            int l_lo = 0, l_hi = -1;     // footprint cells: floor(lo), floor(hi); l_hi < l_lo: skip
+            float l_flo = 0.f, l_fhi = 0.f, l_aD = 1.f, l_w = 0.f;
+            {
+                const int k = k0 + lane;
+                if (k < nplane) {
+                    const double D = fma((double)k, dmain, D0);
+                    const double lo = fma((double)k, dlo, lo0), hi = fma((double)k, dhi, hi0);
+                    const double flo_d = floor(lo), fhi_d = floor(hi);
+                    const int ilo = (int)flo_d, ihi = (int)fhi_d;
+                    const float aD = (float)fabs(D);
+                    // the footprint meets the volume laterally, and the
+                    // warp's rows meet its z extent
+                    if (max(ilo, 0) <= min(ihi, nlat - 1) && fmaf(szt, aD, zoffb) > zvol0 &&
+                        fmaf(szb, aD, zoffb) < zvol1) {
+                        l_lo = ilo;
+                        l_hi = ihi;
+                        l_flo = (float)(lo - flo_d);
+                        l_fhi = (float)(hi - fhi_d);
+                        l_aD = aD;
+                        l_w = __frcp_rn(wfac * aD * aD);
+                    }
+                }
+            }
+            const int nk = min(32, nplane - k0);
+            for (int j = 0; j < nk; j++) {
+                const int ilo = __shfl_sync(0xffffffffu, l_lo, j), ihi = __shfl_sync(0xffffffffu, l_hi, j);
+                if (ihi < ilo) continue;                                 // warp-uniform
+                const int i0 = max(ilo, 0), i1 = min(ihi, nlat - 1);
+                const float flo = __shfl_sync(0xffffffffu, l_flo, j), fhi = __shfl_sync(0xffffffffu, l_fhi, j);
+                const float aD = __shfl_sync(0xffffffffu, l_aD, j), w = __shfl_sync(0xffffffffu, l_w, j);
+                // each edge's cell m and fraction f in the band
+                unsigned m[3];
+                float f[3];
 #pragma unroll
-            for (int q = 0; q < 3; q++) {
-                const float z = fmaf(sz[q], aD, zoffb);
-                const float y = __fadd_rd(z, kCylFloorBias);
-                const int mi = __float_as_int(y) - kCylFloorBiasBits;
-                f[q] = z - (y - kCylFloorBias);
-                m[q] = min((unsigned)max(mi, 0), mmax);
+                for (int q = 0; q < 3; q++) {
+                    const float z = fmaf(sz[q], aD, zoffb);
+                    const float y = __fadd_rd(z, kCylFloorBias);
+                    const int mi = __float_as_int(y) - kCylFloorBiasBits;
+                    f[q] = z - (y - kCylFloorBias);
+                    m[q] = min((unsigned)max(mi, 0), mmax);
+                }
+                const float* cp = zb + (k0 + j) * pstride;
+                float Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
+                for (int i = i0; i <= i1; i++) {
+                    const float ox = (i == ihi ? fhi : 1.f) - (i == ilo ? flo : 0.f);
+                    const float* c = cp + i * cstride;
+                    float a0 = __ldg(c + m[0]), b0 = __ldg(c + m[0] + 1);
+                    float a1 = __ldg(c + m[1]), b1 = __ldg(c + m[1] + 1);
+                    float a2 = __ldg(c + m[2]), b2 = __ldg(c + m[2] + 1);
+                    Q0 = fmaf(ox, fmaf(f[0], b0 - a0, a0), Q0);
+                    Q1 = fmaf(ox, fmaf(f[1], b1 - a1, a1), Q1);
+                    Q2 = fmaf(ox, fmaf(f[2], b2 - a2, a2), Q2);
+                }
+                acc0 = fmaf(Q1 - Q0, w, acc0);
+                acc1 = fmaf(Q2 - Q1, w, acc1);
             }
-            const float* cp = zb + k * pstride;
-            float Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
-            for (int i = i0; i <= i1; i++) {
-                const float ox = (i == ihi ? fhi : 1.f) - (i == ilo ? flo : 0.f);
-                const float* c = cp + i * cstride;
-                float a0 = __ldg(c + m[0]), b0 = __ldg(c + m[0] + 1);
-                float a1 = __ldg(c + m[1]), b1 = __ldg(c + m[1] + 1);
-                float a2 = __ldg(c + m[2]), b2 = __ldg(c + m[2] + 1);
-                Q0 = fmaf(ox, fmaf(f[0], b0 - a0, a0), Q0);
-                Q1 = fmaf(ox, fmaf(f[1], b1 - a1, a1), Q1);
-                Q2 = fmaf(ox, fmaf(f[2], b2 - a2, a2), Q2);
-            }
-            const float w = __frcp_rn(wfac * aD * aD);
-            acc0 = fmaf(Q1 - Q0, w, acc0);
-            acc1 = fmaf(Q2 - Q1, w, acc1);
         }
 #pragma unroll
         for (int q = 0; q < 2; q++) {
@@ -259,6 +284,74 @@ __device__ __forceinline__ float row_prefix(const float2* __restrict__ t, float 
     return fmaf(c.y, rho - (y - kCylFloorBias), c.x);
 }
 
+// The candidate cells u of one view for the voxel column (ix, iy): those
+// whose footprint on the column's plane overlaps the voxel laterally and whose
+// rows reach the warp's z run [zfirst, zlast] (mm).  For each, emit(u, w,
+// inv) with w the lateral overlap weight and inv the detector rows per mm of
+// height on the plane.
+template <class Emit>
+__device__ __forceinline__ void cyl_bp_candidates(const CylView& V, int iv, int ix, int iy, const CylDims& d,
+                                                  const double* __restrict__ redge, const float* __restrict__ inv_dr,
+                                                  const float* __restrict__ inv_inp, float zfirst, float zlast,
+                                                  Emit&& emit) {
+    const float rho0 = (float)(d.nv / 2.0 - d.off_v);
+    const float dsd_dv = (float)(d.dsd / d.dv);
+    const float inv_da = (float)(1.0 / d.da), e_off = (float)(-d.off_a + (d.nu - 1) * 0.5 + 0.5);
+    const double two_pi = 6.283185307179586;
+    const bool xc = V.xcls != 0;
+    const int k = xc ? iy : ix, i = xc ? ix : iy;
+    const int nplane = xc ? d.ny : d.nx, nlat = xc ? d.nx : d.ny;
+    const double dmain = xc ? d.dy : d.dx, dlat = xc ? d.dx : d.dy;
+    const double cmain = xc ? d.cy : d.cx, clat = xc ? d.cx : d.cy;
+    const double smain = xc ? V.sy : V.sx, slat = xc ? V.sx : V.sy;
+    const double D = (k + 0.5 - nplane / 2.0) * dmain + cmain - smain;
+    // the voxel's lower lateral face, relative to the source
+    const double lf = (i - nlat / 2.0) * dlat + clat - slat;
+    // fan angle of the ray through the voxel's lateral centre, and the
+    // half-width of the voxel's angular range to first order: |D| / r^2 per
+    // mm of lateral offset.  The candidate range is widened by the bound of
+    // the second-order term, (dlat / 2)^2 / (2 r^2) rad, twice over, and 0.01
+    // cells; every candidate's overlap is then exact.
+    const float pl = (float)(lf + 0.5 * dlat), pD = (float)D;
+    const float px = xc ? pl : pD, py = xc ? pD : pl;
+    float a = atan2f(px, py) + V.theta;
+    a -= (float)two_pi * rintf(a * (float)(1.0 / two_pi));
+    const float inv_r2 = __frcp_rn(fmaf(px, px, py * py));
+    const float dl = (float)dlat;
+    const float half = 0.5f * dl * fabsf(pD) * inv_r2 * inv_da;
+    const float slack = fmaf(0.25f * dl * dl * inv_r2, inv_da, 0.01f);
+    const float ec = fmaf(-a, inv_da, e_off);
+    const int ulo = (int)fmaxf(floorf(ec - half - slack), 0.f);
+    const int uhi = (int)fminf(floorf(ec + half + slack), (float)(d.nu - 1));
+    const float inv_aD = __frcp_rn(fabsf(pD));
+    const float wD = dl * inv_aD;
+    const double inv_dlat = 1.0 / dlat;
+    const double* Rv = redge + (long long)iv * (d.nu + 1);
+    // lateral position of edge e on this plane relative to the voxel's lower
+    // face, in voxel units
+    float xe = (float)((fma(Rv[ulo], D, -lf)) * inv_dlat);
+    for (int u = ulo; u <= uhi; u++) {
+        const float xn = (float)((fma(Rv[u + 1], D, -lf)) * inv_dlat);
+        const float lo = fminf(xe, xn), hi = fmaxf(xe, xn);
+        xe = xn;
+        const float ov = fminf(hi, 1.f) - fmaxf(lo, 0.f);
+        if (ov <= 0.f) continue;
+        const float inv = dsd_dv * inv_aD * inv_inp[(long long)iv * d.nu + u];
+        // the warp's z run against the detector rows: skip if it misses them
+        if (fmaf(zlast, inv, rho0) <= 0.f || fmaf(zfirst, inv, rho0) >= (float)d.nv) continue;
+        emit(u, ov * wD * inv_dr[(long long)iv * d.nu + u], inv);
+    }
+}
+
+constexpr int kCylBpSlots = 8;   // candidates kept per (voxel column, view)
+
+// Backprojection.  A warp owns the voxels vz0 + 64 blockIdx.y + [0, 64) of
+// one (x, y) column, two per lane.  Views go in groups of 32: first each lane
+// finds the candidate cells of one view of the group (the lateral work, once
+// per view instead of once per lane), into a per-warp list in shared memory;
+// then the warp walks the group's views and candidates together, each lane
+// reading the row tables at its voxels' edges.  A view with more candidates
+// than the list holds is redone by the whole warp.
 __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restrict__ vol, const float2* __restrict__ tab,
                                                                  const CylView* __restrict__ views,
                                                                  const double* __restrict__ redge,
@@ -267,6 +360,8 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
                                                                  int v_begin, int v_end, int accumulate, int vz0,
                                                                  int vz1) {
     constexpr int Z = kCylBpZ;
+    __shared__ float4 s_cand[kCylBpWarps][kCylBpSlots][32];   // (w, inv, view * nu + u) per slot and view
+    __shared__ int s_cnt[kCylBpWarps][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long column = (long long)blockIdx.x * kCylBpWarps + warp;
     if (column >= (long long)d.nx * d.ny) return;              // whole warp
@@ -288,66 +383,53 @@ __global__ void __launch_bounds__(32 * kCylBpWarps) cyl_bp_kernel(float* __restr
     const float zlast = (float)((min(vz1, zbase + 32 * Z) - d.nz / 2.0) * d.dz + d.cz);
     const float zfirst = (float)((zbase - d.nz / 2.0) * d.dz + d.cz);
     const float rho0 = (float)(d.nv / 2.0 - d.off_v);
-    const float dsd_dv = (float)(d.dsd / d.dv);
-    const float inv_da = (float)(1.0 / d.da), e_off = (float)(-d.off_a + (d.nu - 1) * 0.5 + 0.5);
-    const double two_pi = 6.283185307179586;
+    const long long tab_b = (long long)b * d.nview * d.nu;
     float acc[Z];
 #pragma unroll
     for (int q = 0; q < Z; q++) acc[q] = 0.f;
-    for (int iv = v_begin; iv < v_end; iv++) {
-        const CylView V = views[iv];
-        const bool xc = V.xcls != 0;
-        const int k = xc ? iy : ix, i = xc ? ix : iy;
-        const int nplane = xc ? d.ny : d.nx, nlat = xc ? d.nx : d.ny;
-        const double dmain = xc ? d.dy : d.dx, dlat = xc ? d.dx : d.dy;
-        const double cmain = xc ? d.cy : d.cx, clat = xc ? d.cx : d.cy;
-        const double smain = xc ? V.sy : V.sx, slat = xc ? V.sx : V.sy;
-        const double D = (k + 0.5 - nplane / 2.0) * dmain + cmain - smain;
-        // the voxel's lower lateral face, relative to the source
-        const double lf = (i - nlat / 2.0) * dlat + clat - slat;
-        // fan angle of the ray through the voxel's lateral centre, and the
-        // half-width of the voxel's angular range to first order: |D| / r^2
-        // per mm of lateral offset.  The candidate range is widened by the
-        // bound of the second-order term, (dlat / 2)^2 / (2 r^2) rad, twice
-        // over, and 0.01 cells; every candidate's overlap is then exact.
-        const float pl = (float)(lf + 0.5 * dlat), pD = (float)D;
-        const float px = xc ? pl : pD, py = xc ? pD : pl;
-        float a = atan2f(px, py) + V.theta;
-        a -= (float)two_pi * rintf(a * (float)(1.0 / two_pi));
-        const float inv_r2 = __frcp_rn(fmaf(px, px, py * py));
-        const float dl = (float)dlat;
-        const float half = 0.5f * dl * fabsf(pD) * inv_r2 * inv_da;
-        const float slack = fmaf(0.25f * dl * dl * inv_r2, inv_da, 0.01f);
-        const float ec = fmaf(-a, inv_da, e_off);
-        const int ulo = (int)fmaxf(floorf(ec - half - slack), 0.f);
-        const int uhi = (int)fminf(floorf(ec + half + slack), (float)(d.nu - 1));
-        const float inv_aD = __frcp_rn(fabsf(pD));
-        const float wD = (float)dlat * inv_aD;
-        const double inv_dlat = 1.0 / dlat;
-        const double* Rv = redge + (long long)iv * (d.nu + 1);
-        const float2* tv = tab + ((long long)b * d.nview + iv) * (long long)d.nu * (d.nv + 2);
-        // lateral position of edge e on this plane relative to the voxel's
-        // lower face, in voxel units
-        float xe = (float)((fma(Rv[ulo], D, -lf)) * inv_dlat);
-        for (int u = ulo; u <= uhi; u++) {
-            const float xn = (float)((fma(Rv[u + 1], D, -lf)) * inv_dlat);
-            const float lo = fminf(xe, xn), hi = fmaxf(xe, xn);
-            xe = xn;
-            const float ov = fminf(hi, 1.f) - fmaxf(lo, 0.f);
-            if (ov <= 0.f) continue;
-            const float inv = dsd_dv * inv_aD * inv_inp[(long long)iv * d.nu + u];
-            // the warp's z run against the detector rows: skip if it misses them
-            if (fmaf(zlast, inv, rho0) <= 0.f || fmaf(zfirst, inv, rho0) >= (float)d.nv) continue;
-            const float w = ov * wD * inv_dr[(long long)iv * d.nu + u];
-            const float2* t = tv + (long long)u * (d.nv + 2);
-            // prefixes at the lane's Z + 1 edges; a voxel's integral is the
-            // difference of its two edges'
-            float P[Z + 1];
+    // one candidate: the prefixes at the lane's Z + 1 edges; a voxel's
+    // integral is the difference of its two edges'
+    auto add = [&](int vu, float w, float inv) {
+        const float2* t = tab + (tab_b + vu) * (d.nv + 2);
+        float P[Z + 1];
 #pragma unroll
-            for (int q = 0; q <= Z; q++) P[q] = row_prefix(t, fmaf(ze[q], inv, rho0), d.nv);
+        for (int q = 0; q <= Z; q++) P[q] = row_prefix(t, fmaf(ze[q], inv, rho0), d.nv);
 #pragma unroll
-            for (int q = 0; q < Z; q++) acc[q] = fmaf(w, P[q + 1] - P[q], acc[q]);
+        for (int q = 0; q < Z; q++) acc[q] = fmaf(w, P[q + 1] - P[q], acc[q]);
+    };
+    for (int v0 = v_begin; v0 < v_end; v0 += 32) {
+        // lateral work: lane l takes view v0 + l
+        {
+            const int iv = v0 + lane;
+            int n = 0;
+            if (iv < v_end) {
+                const CylView V = views[iv];
+                cyl_bp_candidates(V, iv, ix, iy, d, redge, inv_dr, inv_inp, zfirst, zlast,
+                                  [&](int u, float w, float inv) {
+                                      if (n < kCylBpSlots)
+                                          s_cand[warp][n][lane] = make_float4(w, inv, __int_as_float(iv * d.nu + u), 0.f);
+                                      n++;
+                                  });
+            }
+            s_cnt[warp][lane] = n <= kCylBpSlots ? n : -1;
         }
+        __syncwarp();
+        const int nj = min(32, v_end - v0);
+        for (int j = 0; j < nj; j++) {
+            const int cnt = s_cnt[warp][j];
+            if (cnt >= 0) {
+                for (int c = 0; c < cnt; c++) {
+                    const float4 e = s_cand[warp][c][j];
+                    add(__float_as_int(e.z), e.x, e.y);
+                }
+            } else {   // more candidates than the list holds: the warp redoes the view
+                const int iv = v0 + j;
+                const CylView V = views[iv];
+                cyl_bp_candidates(V, iv, ix, iy, d, redge, inv_dr, inv_inp, zfirst, zlast,
+                                  [&](int u, float w, float inv) { add(iv * d.nu + u, w, inv); });
+            }
+        }
+        __syncwarp();   // the list is rewritten for the next group
     }
 #pragma unroll
     for (int q = 0; q < Z; q++) {
