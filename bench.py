@@ -738,9 +738,12 @@ def cyl_run(dev, cpu_sample=True):
     1.0 mm at the detector), 984 views over 360 degrees, source at 595 mm and
     the detector at 1085.6 mm; random ellipsoids of 0-0.04/mm.  Updates:
     FP = views x cells x planes (984 x 736 x 64 x 512), BP = voxels x views.
-    The bound is not HBM: the FP streams each voxel column's z-run through
-    warp scans and the BP reads per-view row tables, both from L2; the
-    compulsory-bytes fraction is reported beside the time."""
+    The bound is instruction issue, not HBM: the FP reads a band of z
+    prefix sums per voxel column and the BP per-view row tables, both from
+    L2.  `roofline` is the kernel's warp instructions per projection (ncu,
+    profiles/ncu_counts_bench.txt) over its CUDA-event time against one warp
+    instruction per clock on each scheduler at the sampled SM clock; the
+    compulsory-bytes fraction of HBM is reported beside it."""
     import torch
 
     from reconnet_b200.phantom import ellipsoid_phantom
@@ -760,21 +763,36 @@ def cyl_run(dev, cpu_sample=True):
            "data": "synthetic: 10 seeded random ellipsoids, 0-0.04/mm"}
     fp_upd = nview * g.nu * g.nv * g.ny       # planes per ray: ny (X-class) or nx (Y-class), equal here
     bp_upd = g.nx * g.ny * g.nz * nview
-    for name, f, upd, hbm in (("fp", lambda: plan.project(vol, out=prj), fp_upd, vol_b + prj_b),
-                              ("bp", lambda: plan.backproject(prj, out=back), bp_upd, prj_b + 2 * tab_b + vol_b)):
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    for name, kern, f, upd, hbm in (("fp", "cyl_fp_kernel", lambda: plan.project(vol, out=prj), fp_upd, vol_b + prj_b),
+                                    ("bp", "cyl_bp_kernel", lambda: plan.backproject(prj, out=back), bp_upd,
+                                     prj_b + 2 * tab_b + vol_b)):
         f()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(3):
-            f()
-        e1.record()
-        torch.cuda.synchronize()
+        with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+            e0.record()
+            for _ in range(3):
+                f()
+            e1.record()
+            torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / 3
-        ach = hbm / (ms * 1e-3) / 1e9
-        out[name] = {"ms": ms, "updates": upd, "gupd_s": upd / ms / 1e6,
-                     "roofline": {"bound": "hbm (compulsory bytes)", "achieved": ach, "peak": peak, "unit": "GB/s",
-                                  "frac": ach / peak, "peak_kind": kind, "bytes_per_launch": hbm}}
+        t = ms * 1e-3
+        clocks = clk.summary()
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+        counts = ncu_counts(kern)
+        roof = {"bound": "issue", "kernel": kern, "unit": "Gwarp-inst/s", "achieved": None, "peak": None, "frac": None,
+                "traffic": None, "peak_source": f"{n_sm} SMs x 4 schedulers x 1 warp instruction per clock at the "
+                                                "sampled SM clock", "sm_mhz": mhz,
+                "compulsory_hbm": {"bytes": hbm, "achieved": hbm / t / 1e9, "peak": peak, "unit": "GB/s",
+                                   "frac": hbm / t / 1e9 / peak, "peak_kind": kind}}
+        if counts is not None:
+            roof["traffic"] = counts["dram_bytes"]
+            if mhz:
+                roof["achieved"] = counts["warp_inst"] / t / 1e9
+                roof["peak"] = n_sm * 4 * mhz * 1e6 / 1e9
+                roof["frac"] = roof["achieved"] / roof["peak"]
+        out[name] = {"ms": ms, "updates": upd, "gupd_s": upd / ms / 1e6, "roofline": roof, "clocks": clocks}
     y = torch.rand(plan.prj_shape, device=dev)
     aty = plan.backproject(y)
     ax = plan.project(vol)

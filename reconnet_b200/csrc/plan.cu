@@ -109,6 +109,29 @@ static void build_fp_work(rn_fan_plan* p) {
         }
     }
     p->n_fp_work = (int)(p->h_fp_work.size() / 4);
+    // Within each wave of slices that share the line scratch, items with more
+    // views go first: the block scheduler hands out CTAs in index order, so
+    // the short items fill the last wave instead of trailing it (a longest-
+    // processing-time-first list schedule).  The order within equal view
+    // counts stays by slice, so CTAs running together read the same slices'
+    // lines.
+    const int slots = (int)std::max<long long>(1, p->fp_slots);
+    int* w = p->h_fp_work.data();
+    for (int b = 0; b < p->n_fp_work;) {
+        const int s_end = (w[4 * b] / slots + 1) * slots;   // the wave of fan_project holding item b
+        int e = b;
+        while (e < p->n_fp_work && w[4 * e] < s_end) e++;
+        std::vector<int4> wave(e - b);
+        for (int i = b; i < e; i++) wave[i - b] = make_int4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+        std::stable_sort(wave.begin(), wave.end(), [](const int4& x, const int4& y) { return x.w > y.w; });
+        for (int i = b; i < e; i++) {
+            w[4 * i] = wave[i - b].x;
+            w[4 * i + 1] = wave[i - b].y;
+            w[4 * i + 2] = wave[i - b].z;
+            w[4 * i + 3] = wave[i - b].w;
+        }
+        b = e;
+    }
 }
 
 // Table window (entries per view staged by the BP kernels): the detector
@@ -195,6 +218,10 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
     RN_TRY(fan_kernel_attributes());
     FanGeoHost gh;
     RN_TRY(fan_build_geometry(p, host_deg, gh));
+    // line scratch: slices whose lines fit the budget form one wave of FP work
+    p->line_slot_elems = (long long)p->dims.ny * p->dims.spx + (long long)p->dims.nx * p->dims.spy;
+    p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(),
+                                         kLineBudget / (p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float)))));
     build_fp_work(p);
     {
         long long cap = 0;   // one view per item: room for any tuning
@@ -202,11 +229,6 @@ static int finish_plan(rn_fan_plan* p, const float* host_deg, cudaStream_t st) {
         p->fp_work_cap = (int)std::max<long long>(cap, p->n_fp_work);
     }
 
-    // line scratch
-    const FanDims& d = p->dims;
-    p->line_slot_elems = (long long)d.ny * d.spx + (long long)d.nx * d.spy;
-    long long slot_bytes = p->line_slot_elems * (long long)(sizeof(float2) + sizeof(float));
-    p->fp_slots = std::max(1ll, std::min((long long)p->h_fp.size(), kLineBudget / slot_bytes));
     // table scratch: all slices if within budget, else at least the largest slice
     long long need = 0, largest = 0;
     for (const BpSlice& b : p->h_bp) {
