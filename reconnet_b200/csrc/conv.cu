@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -67,6 +68,9 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
@@ -147,154 +151,187 @@ struct ConvArgs {
     int* err;
 };
 
+// Warp-specialised pipeline.  Warp 4 (one elected lane) is the producer: it
+// keeps kConvStages - 1 TMA boxes in flight ahead of the tile whose MMAs it
+// issues, and commits each tile's MMA group twice, to the box's "empty"
+// barrier (the box may be refilled) and to the accumulator's "full" barrier.
+// Warps 0-3 are the epilogue: thread t reads TMEM lane t (output pixel w0 + t
+// of the tile's row) from one of two accumulators of 32 columns, releases the
+// accumulator (one arrival per warp on its "empty" barrier) and stores.  So
+// the TMA copies, the MMAs of tile i and the epilogue of tile i - 1 overlap.
+constexpr int kConvStages = 3;
+constexpr int kConvWsThreads = kConvThreads + 32;
+
 template <int CH, int NPAD>
-__global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __grid_constant__ CUtensorMap tm_in, ConvArgs a) {
+__global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_constant__ CUtensorMap tm_in, ConvArgs a) {
     constexpr int KSTEPS = CH == 4 ? 18 : 5;
     constexpr int KCH = 2 * KSTEPS;                              // B chunks (the last one of an 8-channel layer is zero)
     constexpr uint32_t BOX_BYTES = CH * 3 * kBoxW * 16;
     constexpr uint32_t BOX_ALLOC = (BOX_BYTES + kZeroBytes + 1023) & ~1023u;
     constexpr uint32_t B_BYTES = KCH * NPAD * 16;
+    constexpr int S = kConvStages;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // TMA destinations on a 1024-byte boundary (the allocation has 1 KB of slack)
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-    unsigned char* box0 = smem;
-    unsigned char* box1 = smem + BOX_ALLOC;
-    unsigned char* bsm = smem + 2 * BOX_ALLOC;
-    __shared__ __align__(8) uint64_t bar_tma[2];
-    __shared__ __align__(8) uint64_t bar_mma;
+    unsigned char* bsm = smem + S * BOX_ALLOC;
+    __shared__ __align__(8) uint64_t bar_full[S], bar_empty[S], bar_accf[2], bar_acce[2];
     __shared__ uint32_t tmem_slot;
-    __shared__ int s_fail;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ volatile int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_w = (a.W + kConvTile - 1) / kConvTile;
     const long long ntiles = (long long)a.N * a.H * tiles_w;
+    const long long nmine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     // zero rows, weights (B operand image), barriers, accumulator columns
-    for (int i = tid; i < kZeroBytes / 16; i += kConvThreads) {
-        reinterpret_cast<uint4*>(box0 + BOX_BYTES)[i] = make_uint4(0, 0, 0, 0);
-        reinterpret_cast<uint4*>(box1 + BOX_BYTES)[i] = make_uint4(0, 0, 0, 0);
-    }
-    for (int i = tid; i < (int)(B_BYTES / 16); i += kConvThreads) reinterpret_cast<uint4*>(bsm)[i] = a.wpack[i];
+    for (int s = 0; s < S; s++)
+        for (int i = tid; i < kZeroBytes / 16; i += kConvWsThreads)
+            reinterpret_cast<uint4*>(smem + s * BOX_ALLOC + BOX_BYTES)[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < (int)(B_BYTES / 16); i += kConvWsThreads) reinterpret_cast<uint4*>(bsm)[i] = a.wpack[i];
     if (tid == 0) {
-        mbar_init(&bar_tma[0], 1);
-        mbar_init(&bar_tma[1], 1);
-        mbar_init(&bar_mma, 1);
+        for (int s = 0; s < S; s++) {
+            mbar_init(&bar_full[s], 1);
+            mbar_init(&bar_empty[s], 1);
+        }
+        for (int k = 0; k < 2; k++) {
+            mbar_init(&bar_accf[k], 1);
+            mbar_init(&bar_acce[k], kConvThreads / 32);
+        }
         fence_mbar_init();
         s_fail = 0;
     }
-    if (warp == 0) tmem_alloc(&tmem_slot, 32);
+    if (warp == 0) tmem_alloc(&tmem_slot, 64);
     fence_proxy_async();   // generic-proxy writes (zero rows, weights) before tensor-core reads
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    const uint32_t idesc = umma_idesc(NPAD, false, false);
 
-    auto tile_coords = [&](long long t, int& n, int& h, int& w0) {
+    auto tile_coords = [&](long long i, int& n, int& h, int& w0) {
+        const long long t = blockIdx.x + i * gridDim.x;
         const int tw = (int)(t % tiles_w);
         const long long r = t / tiles_w;
         h = (int)(r % a.H);
         n = (int)(r / a.H);
         w0 = tw * kConvTile;
     };
-    long long t = blockIdx.x;
-    if (tid == 0 && t < ntiles) {
-        int n, h, w0;
-        tile_coords(t, n, h, w0);
-        mbar_arrive_expect_tx(&bar_tma[0], BOX_BYTES);
-        tma_load_5d(box0, &tm_in, 0, w0 - 1, h - 1, 0, n, &bar_tma[0]);
-    }
-    for (int it = 0; t < ntiles; t += gridDim.x, it++) {
-        const int buf = it & 1;
-        unsigned char* box = buf ? box1 : box0;
-        int n, h, w0;
-        tile_coords(t, n, h, w0);
-        bool ok = mbar_wait(&bar_tma[buf], (it >> 1) & 1);
-        if (tid == 0) {
-            if (ok) {
+
+    if (warp == kConvThreads / 32) {
+        if (lane == 0) {
+            // ---- producer ----
+            long long tma_next = 0, full_seen = 0, mma_done = 0;   // TMA issued / consumed; MMA groups issued
+            bool ok = true;
+            auto issue_tma = [&](long long i) -> bool {
+                const int s = (int)(i % S);
+                if (i >= S && !mbar_wait(&bar_empty[s], (uint32_t)((i / S - 1) & 1))) return false;
+                int n, h, w0;
+                tile_coords(i, n, h, w0);
+                mbar_arrive_expect_tx(&bar_full[s], BOX_BYTES);
+                tma_load_5d(smem + s * BOX_ALLOC, &tm_in, 0, w0 - 1, h - 1, 0, n, &bar_full[s]);
+                return true;
+            };
+            while (tma_next < nmine && tma_next < S - 1) issue_tma(tma_next++);
+            const uint32_t idesc = umma_idesc(NPAD, false, false), bbase = smem_u32(bsm);
+            for (long long j = 0; j < nmine; j++) {
+                const int s = (int)(j % S), acc = (int)(j & 1);
+                if (!mbar_wait(&bar_full[s], (uint32_t)((j / S) & 1))) { ok = false; break; }
+                full_seen = j + 1;
+                if (j >= 2 && !mbar_wait(&bar_acce[acc], (uint32_t)(((j >> 1) - 1) & 1))) { ok = false; break; }
                 tc_fence_after();
-                const uint32_t abase = smem_u32(box), bbase = smem_u32(bsm);
+                const uint32_t abase = smem_u32(smem + s * BOX_ALLOC);
 #pragma unroll
-                for (int s = 0; s < KSTEPS; s++) {
+                for (int k = 0; k < KSTEPS; k++) {
                     uint32_t aoff, lbo;
                     if (CH == 4) {
-                        const int tap = s >> 1, c0 = (s & 1) * 2;
+                        const int tap = k >> 1, c0 = (k & 1) * 2;
                         aoff = tap_off(tap, CH) + (uint32_t)(c0 * 3 * kBoxW * 16);
                         lbo = 3 * kBoxW * 16;
                     } else {
-                        aoff = tap_off(2 * s, CH);
-                        lbo = tap_off(2 * s + 1, CH) - aoff;
+                        aoff = tap_off(2 * k, CH);
+                        lbo = tap_off(2 * k + 1, CH) - aoff;
                     }
                     const uint64_t da = umma_desc(abase + aoff, lbo, 128);
-                    const uint64_t db = umma_desc(bbase + (uint32_t)(2 * s * NPAD * 16), NPAD * 16, 128);
-                    umma_bf16(tmem, da, db, idesc, s > 0 ? 1u : 0u);
+                    const uint64_t db = umma_desc(bbase + (uint32_t)(2 * k * NPAD * 16), NPAD * 16, 128);
+                    umma_bf16(tmem + (uint32_t)(acc * 32), da, db, idesc, k > 0 ? 1u : 0u);
                 }
-                umma_commit(&bar_mma);
+                umma_commit(&bar_empty[s]);
+                umma_commit(&bar_accf[acc]);
+                mma_done = j + 1;
+                // the box after the ones in flight goes into the stage that
+                // tile j - 1's group is releasing
+                if (tma_next < nmine) {
+                    if (!issue_tma(tma_next)) { ok = false; break; }
+                    tma_next++;
+                }
             }
-            // the next tile's box goes into the other buffer, whose last
-            // reader (the previous tile's MMAs) has completed
-            const long long tn = t + gridDim.x;
-            if (tn < ntiles) {
-                int n2, h2, w2;
-                tile_coords(tn, n2, h2, w2);
-                unsigned char* nb = buf ? box0 : box1;
-                mbar_arrive_expect_tx(&bar_tma[buf ^ 1], BOX_BYTES);
-                tma_load_5d(nb, &tm_in, 0, w2 - 1, h2 - 1, 0, n2, &bar_tma[buf ^ 1]);
+            if (!ok) {
+                s_fail = 1;
+                // before the shared memory and the accumulator columns are
+                // released: the copies issued and not yet seen, and the last
+                // MMA group (its barrier completes after every earlier group)
+                for (long long i = full_seen; i < tma_next; i++)
+                    mbar_wait(&bar_full[i % S], (uint32_t)((i / S) & 1));
+                if (mma_done > 0)
+                    mbar_wait(&bar_empty[(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
             }
-            if (!ok) s_fail = 1;
         }
-        __syncthreads();
-        if (s_fail) break;
-        ok = mbar_wait(&bar_mma, it & 1);
-        if (!ok) {
-            if (tid == 0) s_fail = 1;
-            __syncthreads();
-            break;
-        }
-        tc_fence_after();
-        // epilogue: thread tid owns output pixel w0 + tid of row h
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16), v);
-        const int w = w0 + tid;
-        if (w < a.W) {
-            const long long pix = ((long long)n * a.H + h) * a.W + w;   // pixel index within one channel plane
-            const long long plane = (long long)a.H * a.W;
-            if (a.mode == 0 || a.mode == 2) {
-                uint4* o = reinterpret_cast<uint4*>(a.out);
-                const uint4* act = reinterpret_cast<const uint4*>(a.aux);
-                const int cho = a.cout / 8;
+    } else {
+        // ---- epilogue: thread tid owns output pixel w0 + tid ----
+        for (long long j = 0; j < nmine; j++) {
+            const int acc = (int)(j & 1);
+            if (!mbar_wait(&bar_accf[acc], (uint32_t)((j >> 1) & 1))) {
+                s_fail = 1;
+                break;
+            }
+            tc_fence_after();
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * 32), v);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_acce[acc]);
+            int n, h, w0;
+            tile_coords(j, n, h, w0);
+            const int w = w0 + tid;
+            if (w < a.W) {
+                const long long pix = ((long long)n * a.H + h) * a.W + w;   // pixel index within one channel plane
+                const long long plane = (long long)a.H * a.W;
+                if (a.mode == 0 || a.mode == 2) {
+                    uint4* o = reinterpret_cast<uint4*>(a.out);
+                    const uint4* act = reinterpret_cast<const uint4*>(a.aux);
+                    const int cho = a.cout / 8;
 #pragma unroll
-                for (int c = 0; c < NPAD / 8; c++) {
-                    if (c >= cho) break;
-                    float q[8];
+                    for (int c = 0; c < NPAD / 8; c++) {
+                        if (c >= cho) break;
+                        float q[8];
 #pragma unroll
-                    for (int i = 0; i < 8; i++) q[i] = v[c * 8 + i];
-                    const long long idx = ((long long)n * cho + c) * plane + (long long)h * a.W + w;
-                    if (a.mode == 0) {
+                        for (int i = 0; i < 8; i++) q[i] = v[c * 8 + i];
+                        const long long idx = ((long long)n * cho + c) * plane + (long long)h * a.W + w;
+                        if (a.mode == 0) {
 #pragma unroll
-                        for (int i = 0; i < 8; i++) q[i] = fmaxf(q[i] + a.bias[c * 8 + i], 0.f);
-                    } else {
-                        float m[8];
-                        unpack_bf16x8(act[idx], m);
+                            for (int i = 0; i < 8; i++) q[i] = fmaxf(q[i] + a.bias[c * 8 + i], 0.f);
+                        } else {
+                            float m[8];
+                            unpack_bf16x8(act[idx], m);
 #pragma unroll
-                        for (int i = 0; i < 8; i++) q[i] = m[i] > 0.f ? q[i] : 0.f;
+                            for (int i = 0; i < 8; i++) q[i] = m[i] > 0.f ? q[i] : 0.f;
+                        }
+                        o[idx] = pack_bf16x8(q);
                     }
-                    o[idx] = pack_bf16x8(q);
+                } else if (a.mode == 1) {
+                    const float* res = reinterpret_cast<const float*>(a.aux);
+                    reinterpret_cast<float*>(a.out)[pix] = v[0] + a.bias[0] + res[pix];
+                } else {
+                    float* o = reinterpret_cast<float*>(a.out);
+                    for (int c = 0; c < a.cout; c++)
+                        o[((long long)n * a.cout + c) * plane + (long long)h * a.W + w] = v[c] + (a.bias ? a.bias[c] : 0.f);
                 }
-            } else if (a.mode == 1) {
-                const float* res = reinterpret_cast<const float*>(a.aux);
-                reinterpret_cast<float*>(a.out)[pix] = v[0] + a.bias[0] + res[pix];
-            } else {
-                float* o = reinterpret_cast<float*>(a.out);
-                for (int c = 0; c < a.cout; c++)
-                    o[((long long)n * a.cout + c) * plane + (long long)h * a.W + w] = v[c] + (a.bias ? a.bias[c] : 0.f);
             }
         }
-        tc_fence_before();
-        __syncthreads();   // accumulator reads done before the next tile's MMAs
     }
-    if (s_fail && tid == 0) atomicExch(a.err, RN_ERR_TIMEOUT);
+    tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 32);
+    if (tid == 0 && s_fail) atomicExch(a.err, RN_ERR_TIMEOUT);
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, 64);
 }
 
 // ---- weight gradient -------------------------------------------------------------
@@ -491,11 +528,16 @@ static int launch_conv(const CUtensorMap& m, const ConvArgs& a, cudaStream_t st)
     constexpr int KSTEPS = CH == 4 ? 18 : 5;
     constexpr uint32_t BOX_BYTES = CH * 3 * kBoxW * 16;
     constexpr uint32_t BOX_ALLOC = (BOX_BYTES + kZeroBytes + 1023) & ~1023u;
-    const size_t smem = 2 * BOX_ALLOC + 2 * KSTEPS * NPAD * 16 + 1024;
+    const size_t smem = kConvStages * BOX_ALLOC + 2 * KSTEPS * NPAD * 16 + 1024;
     RN_CUDA_TRY(cudaFuncSetAttribute(conv3x3_kernel<CH, NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long ntiles = (long long)a.N * a.H * ((a.W + kConvTile - 1) / kConvTile);
-    const int grid = (int)std::min<long long>(ntiles, 2LL * sm_count());
-    conv3x3_kernel<CH, NPAD><<<grid, kConvThreads, smem, st>>>(m, a);
+    // as many CTAs per SM as shared memory allows (64 of the SM's 512 TMEM
+    // columns each), at most four
+    int per_sm = 0;
+    RN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_kernel<CH, NPAD>, kConvWsThreads, smem));
+    per_sm = std::max(1, std::min(per_sm, 4));
+    const int grid = (int)std::min<long long>(ntiles, (long long)per_sm * sm_count());
+    conv3x3_kernel<CH, NPAD><<<grid, kConvWsThreads, smem, st>>>(m, a);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
