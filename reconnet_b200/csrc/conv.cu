@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <string>
 
 #include "rn_device.cuh"
@@ -128,11 +129,11 @@ __device__ __forceinline__ void unpack_bf16x8(uint4 u, float* v) {
     }
 }
 
-// Offset (bytes) in a box [CH][3][kBoxW][16 B] of tap t's first chunk for
+// Offset (bytes) in a box [CH][3][boxw][16 B] of tap t's first chunk for
 // output pixel 0; tap 9 (the padding of an 8-channel layer) is the zero rows.
-__device__ __forceinline__ uint32_t tap_off(int t, int ch) {
-    if (t >= 9) return (uint32_t)(ch * 3 * kBoxW * 16);
-    return (uint32_t)(((t / 3) * kBoxW + (t % 3)) * 16);
+__device__ __forceinline__ uint32_t tap_off(int t, int ch, int boxw = kBoxW) {
+    if (t >= 9) return (uint32_t)(ch * 3 * boxw * 16);
+    return (uint32_t)(((t / 3) * boxw + (t % 3)) * 16);
 }
 
 // ---- forward / input-gradient convolution --------------------------------------
@@ -159,14 +160,22 @@ struct ConvArgs {
 // of the tile's row) from one of two accumulators of 32 columns, releases the
 // accumulator (one arrival per warp on its "empty" barrier) and stores.  So
 // the TMA copies, the MMAs of tile i and the epilogue of tile i - 1 overlap.
+//
+// Boxes: the tensor map views each image row as groups of PIX pixels (16 PIX
+// bytes; PIX = 8 when the width allows, else 2, else 1), so a TMA row is a
+// whole 128-byte line rather than half a 32-byte sector.  A box then starts
+// PIX - 1 pixels before the halo pixel w0 - 1 (128 + 2 PIX pixels) and the
+// operands start 16 (PIX - 1) bytes into each box row.
 constexpr int kConvStages = 3;
 constexpr int kConvWsThreads = kConvThreads + 32;
 
-template <int CH, int NPAD>
+template <int CH, int NPAD, int PIX>
 __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_constant__ CUtensorMap tm_in, ConvArgs a) {
     constexpr int KSTEPS = CH == 4 ? 18 : 5;
     constexpr int KCH = 2 * KSTEPS;                              // B chunks (the last one of an 8-channel layer is zero)
-    constexpr uint32_t BOX_BYTES = CH * 3 * kBoxW * 16;
+    constexpr int BOXW = kConvTile + 2 * PIX;                    // pixels per box row
+    constexpr uint32_t A0 = 16 * (PIX - 1);                      // the operands' first pixel within a box row
+    constexpr uint32_t BOX_BYTES = CH * 3 * BOXW * 16;
     constexpr uint32_t BOX_ALLOC = (BOX_BYTES + kZeroBytes + 1023) & ~1023u;
     constexpr uint32_t B_BYTES = KCH * NPAD * 16;
     constexpr int S = kConvStages;
@@ -177,6 +186,7 @@ __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_co
     __shared__ __align__(8) uint64_t bar_full[S], bar_empty[S], bar_accf[2], bar_acce[2];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int s_fail;
+    __shared__ float s_bias[NPAD];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_w = (a.W + kConvTile - 1) / kConvTile;
     const long long ntiles = (long long)a.N * a.H * tiles_w;
@@ -187,6 +197,7 @@ __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_co
         for (int i = tid; i < kZeroBytes / 16; i += kConvWsThreads)
             reinterpret_cast<uint4*>(smem + s * BOX_ALLOC + BOX_BYTES)[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < (int)(B_BYTES / 16); i += kConvWsThreads) reinterpret_cast<uint4*>(bsm)[i] = a.wpack[i];
+    if (tid < NPAD) s_bias[tid] = (a.bias && tid < a.cout) ? a.bias[tid] : 0.f;
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
             mbar_init(&bar_full[s], 1);
@@ -226,7 +237,7 @@ __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_co
                 int n, h, w0;
                 tile_coords(i, n, h, w0);
                 mbar_arrive_expect_tx(&bar_full[s], BOX_BYTES);
-                tma_load_5d(smem + s * BOX_ALLOC, &tm_in, 0, w0 - 1, h - 1, 0, n, &bar_full[s]);
+                tma_load_5d(smem + s * BOX_ALLOC, &tm_in, 0, w0 / PIX - 1, h - 1, 0, n, &bar_full[s]);
                 return true;
             };
             while (tma_next < nmine && tma_next < S - 1) issue_tma(tma_next++);
@@ -237,17 +248,19 @@ __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_co
                 full_seen = j + 1;
                 if (j >= 2 && !mbar_wait(&bar_acce[acc], (uint32_t)(((j >> 1) - 1) & 1))) { ok = false; break; }
                 tc_fence_after();
-                const uint32_t abase = smem_u32(smem + s * BOX_ALLOC);
+                const uint32_t abase = smem_u32(smem + s * BOX_ALLOC) + A0;
 #pragma unroll
                 for (int k = 0; k < KSTEPS; k++) {
                     uint32_t aoff, lbo;
                     if (CH == 4) {
                         const int tap = k >> 1, c0 = (k & 1) * 2;
-                        aoff = tap_off(tap, CH) + (uint32_t)(c0 * 3 * kBoxW * 16);
-                        lbo = 3 * kBoxW * 16;
+                        aoff = tap_off(tap, CH, BOXW) + (uint32_t)(c0 * 3 * BOXW * 16);
+                        lbo = 3 * BOXW * 16;
                     } else {
-                        aoff = tap_off(2 * k, CH);
-                        lbo = tap_off(2 * k + 1, CH) - aoff;
+                        // tap 9 is the zero rows after the box (from the
+                        // operands' shifted start: the same offset minus A0)
+                        aoff = tap_off(2 * k, CH, BOXW) - (2 * k >= 9 ? A0 : 0);
+                        lbo = tap_off(2 * k + 1, CH, BOXW) - (2 * k + 1 >= 9 ? A0 : 0) - aoff;
                     }
                     const uint64_t da = umma_desc(abase + aoff, lbo, 128);
                     const uint64_t db = umma_desc(bbase + (uint32_t)(2 * k * NPAD * 16), NPAD * 16, 128);
@@ -307,7 +320,7 @@ __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_co
                         const long long idx = ((long long)n * cho + c) * plane + (long long)h * a.W + w;
                         if (a.mode == 0) {
 #pragma unroll
-                            for (int i = 0; i < 8; i++) q[i] = fmaxf(q[i] + a.bias[c * 8 + i], 0.f);
+                            for (int i = 0; i < 8; i++) q[i] = fmaxf(q[i] + s_bias[c * 8 + i], 0.f);
                         } else {
                             float m[8];
                             unpack_bf16x8(act[idx], m);
@@ -318,11 +331,11 @@ __global__ void __launch_bounds__(kConvWsThreads) conv3x3_kernel(const __grid_co
                     }
                 } else if (a.mode == 1) {
                     const float* res = reinterpret_cast<const float*>(a.aux);
-                    reinterpret_cast<float*>(a.out)[pix] = v[0] + a.bias[0] + res[pix];
+                    reinterpret_cast<float*>(a.out)[pix] = v[0] + s_bias[0] + res[pix];
                 } else {
                     float* o = reinterpret_cast<float*>(a.out);
                     for (int c = 0; c < a.cout; c++)
-                        o[((long long)n * a.cout + c) * plane + (long long)h * a.W + w] = v[c] + (a.bias ? a.bias[c] : 0.f);
+                        o[((long long)n * a.cout + c) * plane + (long long)h * a.W + w] = v[c] + s_bias[c];
                 }
             }
         }
@@ -499,15 +512,18 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// Tensor map over a blocked activation [N][ch][H][W][8] bf16 with a box of
-// (8, box_w, box_h, ch, 1).
-static int make_act_map(CUtensorMap* m, const void* base, int N, int ch, int H, int W, int box_w, int box_h) {
+// Tensor map over a blocked activation [N][ch][H][W][8] bf16 with the pixels
+// taken in groups of `pix` (W a multiple of pix): a box of (8 pix, box_w /
+// pix, box_h, ch, 1), each of its rows 16 pix bytes.
+static int make_act_map(CUtensorMap* m, const void* base, int N, int ch, int H, int W, int box_w, int box_h,
+                        int pix = 1) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return set_error(RN_ERR_CUDA, "conv: cuTensorMapEncodeTiled unavailable");
     if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return set_error(RN_ERR_ARG, "conv: activations must be 16-byte aligned");
-    cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)ch, (cuuint64_t)N};
-    cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)ch * H * W * 16};
-    cuuint32_t box[5] = {8, (cuuint32_t)box_w, (cuuint32_t)box_h, (cuuint32_t)ch, 1};
+    const int p = pix;
+    cuuint64_t dims[5] = {(cuuint64_t)(8 * p), (cuuint64_t)(W / p), (cuuint64_t)H, (cuuint64_t)ch, (cuuint64_t)N};
+    cuuint64_t strides[4] = {(cuuint64_t)(16 * p), (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)ch * H * W * 16};
+    cuuint32_t box[5] = {(cuuint32_t)(8 * p), (cuuint32_t)(box_w / p), (cuuint32_t)box_h, (cuuint32_t)ch, 1};
     cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -523,21 +539,26 @@ static int sm_count() {
     return n;
 }
 
-template <int CH, int NPAD>
+template <int CH, int NPAD, int PIX>
 static int launch_conv(const CUtensorMap& m, const ConvArgs& a, cudaStream_t st) {
     constexpr int KSTEPS = CH == 4 ? 18 : 5;
-    constexpr uint32_t BOX_BYTES = CH * 3 * kBoxW * 16;
+    constexpr uint32_t BOX_BYTES = CH * 3 * (kConvTile + 2 * PIX) * 16;
     constexpr uint32_t BOX_ALLOC = (BOX_BYTES + kZeroBytes + 1023) & ~1023u;
     const size_t smem = kConvStages * BOX_ALLOC + 2 * KSTEPS * NPAD * 16 + 1024;
-    RN_CUDA_TRY(cudaFuncSetAttribute(conv3x3_kernel<CH, NPAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = conv3x3_kernel<CH, NPAD, PIX>;
+    RN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     const long long ntiles = (long long)a.N * a.H * ((a.W + kConvTile - 1) / kConvTile);
     // as many CTAs per SM as shared memory allows (64 of the SM's 512 TMEM
     // columns each), at most four
-    int per_sm = 0;
-    RN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_kernel<CH, NPAD>, kConvWsThreads, smem));
-    per_sm = std::max(1, std::min(per_sm, 4));
+    int per_sm = 0, dev = 0, smem_sm = 0;
+    RN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConvWsThreads, smem));
+    RN_CUDA_TRY(cudaGetDevice(&dev));
+    RN_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    // (the per-CTA reservation and the static barriers: 2 KB)
+    per_sm = std::max(1, std::min(std::max(per_sm, smem_sm / (int)(smem + 2048)), 4));
     const int grid = (int)std::min<long long>(ntiles, (long long)per_sm * sm_count());
-    conv3x3_kernel<CH, NPAD><<<grid, kConvWsThreads, smem, st>>>(m, a);
+    kern<<<grid, kConvWsThreads, smem, st>>>(m, a);
     RN_CUDA_TRY(cudaGetLastError());
     return RN_OK;
 }
@@ -559,11 +580,17 @@ extern "C" int rn_conv3x3(void* d_out, const void* d_in, const void* d_wpack, co
     if ((mode == 0 || mode == 1) && !d_bias) return set_error(RN_ERR_ARG, "conv: bias required");
     if ((mode == 1 || mode == 2) && !d_aux) return set_error(RN_ERR_ARG, "conv: aux input required");
     CUtensorMap m;
-    RN_TRY(make_act_map(&m, d_in, N, cin / 8, H, W, kBoxW, 3));
     ConvArgs a{d_out, reinterpret_cast<const uint4*>(d_wpack), d_bias, d_aux, N, H, W, cout, mode, d_err};
     cudaStream_t st = (cudaStream_t)stream;
-    if (cin == 32) return cout == 32 ? launch_conv<4, 32>(m, a, st) : launch_conv<4, 16>(m, a, st);
-    return cout == 32 ? launch_conv<1, 32>(m, a, st) : launch_conv<1, 16>(m, a, st);
+    auto run = [&](auto pix) {
+        constexpr int P = decltype(pix)::value;
+        RN_TRY(make_act_map(&m, d_in, N, cin / 8, H, W, kConvTile + 2 * P, 3, P));
+        if (cin == 32) return cout == 32 ? launch_conv<4, 32, P>(m, a, st) : launch_conv<4, 16, P>(m, a, st);
+        return cout == 32 ? launch_conv<1, 32, P>(m, a, st) : launch_conv<1, 16, P>(m, a, st);
+    };
+    if (W % 8 == 0) return run(std::integral_constant<int, 8>{});
+    if (W % 2 == 0) return run(std::integral_constant<int, 2>{});
+    return run(std::integral_constant<int, 1>{});
 }
 
 extern "C" int rn_conv3x3_wgrad_cols(int cin) { return cin == 32 ? 288 + 16 : 80 + 16; }

@@ -27,7 +27,8 @@ def _kern():
 
 
 @pytest.mark.parametrize("cin,cout", [(32, 32), (8, 32), (32, 1)])
-@pytest.mark.parametrize("hw", [(5, 200), (3, 128)])
+# widths of 8k, 2k and odd pixels: 8, 2 and 1 pixels per TMA box row
+@pytest.mark.parametrize("hw", [(5, 200), (3, 128), (4, 131), (3, 150)])
 def test_conv_forward_fp32_matches_oracle(cin, cout, hw, rng):
     import torch
     from oracle import oracle as O
