@@ -359,40 +359,51 @@ struct WgradArgs {
     int* err;
 };
 
-template <int CH, int CHO>
+// Thread 0 keeps kWgStages - 1 tiles' loads (a dY box and an X box each) in
+// flight ahead of the tile whose MMA group it issues; each group commits to
+// its stage's "empty" barrier, which the load kWgStages - 1 tiles later waits
+// for.  Boxes take PIX pixels per TMA row as in the forward kernel.
+// The A operand (dY, M = 128 output-channel rows of which the first 8 CHO are
+// real) spans 16 groups of 8 rows 2048 bytes apart: groups past the dY box
+// read whatever shared memory follows it (more boxes), which only feeds
+// accumulator rows that are never read.
+constexpr int kWgStages = 4;
+
+template <int CH, int CHO, int PIX>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x,
                                                                     const __grid_constant__ CUtensorMap tm_dy,
                                                                     WgradArgs a) {
-    constexpr uint32_t XBOX = CH * 3 * kBoxW * 16;
+    constexpr int S = kWgStages;
+    constexpr int BOXW = kConvTile + 2 * PIX;
+    constexpr uint32_t A0 = 16 * (PIX - 1);
+    constexpr uint32_t XBOX = CH * 3 * BOXW * 16;
     constexpr uint32_t DYBOX = CHO * kConvTile * 16;
-    // the A operand (dY, 128 rows of which the first 8 * CHO are real) walks
-    // 16 groups of rows 2048 bytes apart: keep 32 KB of shared memory after it
-    constexpr uint32_t DY_ALLOC = 32768 + 1024;
+    constexpr uint32_t DY_ALLOC = (DYBOX + 1023) & ~1023u;
     constexpr uint32_t X_ALLOC = (XBOX + kZeroBytes + 1023) & ~1023u;
-    constexpr uint32_t STAGE = DY_ALLOC + X_ALLOC;
     constexpr int NCOLS_TMEM = CH == 4 ? 512 : 128;
     constexpr int BIAS_COL = CH == 4 ? 288 : 80;
+    static_assert(DY_ALLOC + S * X_ALLOC >= 16 * 2048, "the A operand's 16 row groups must stay in shared memory");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-    unsigned char* ones = smem + 2 * STAGE;   // 512 B of bf16 ones: the bias-gradient B operand
-    __shared__ __align__(8) uint64_t bar_tma[2];
-    __shared__ __align__(8) uint64_t bar_mma;
+    unsigned char* xbox0 = smem + S * DY_ALLOC;
+    unsigned char* ones = xbox0 + S * X_ALLOC;   // 512 B of bf16 ones: the bias-gradient B operand
+    __shared__ __align__(8) uint64_t bar_full[S], bar_empty[S];
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int tiles_w = (a.W + kConvTile - 1) / kConvTile;
     const long long ntiles = (long long)a.N * a.H * tiles_w;
-    for (int s = 0; s < 2; s++) {
-        unsigned char* st = smem + s * STAGE;
-        for (int i = tid; i < (int)(DY_ALLOC / 16); i += kConvThreads) reinterpret_cast<uint4*>(st)[i] = make_uint4(0, 0, 0, 0);
+    const long long nmine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    for (int i = tid; i < (int)(S * DY_ALLOC / 16); i += kConvThreads) reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+    for (int s = 0; s < S; s++)
         for (int i = tid; i < kZeroBytes / 16; i += kConvThreads)
-            reinterpret_cast<uint4*>(st + DY_ALLOC + XBOX)[i] = make_uint4(0, 0, 0, 0);
-    }
+            reinterpret_cast<uint4*>(xbox0 + s * X_ALLOC + XBOX)[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 512 / 4; i += kConvThreads) reinterpret_cast<uint32_t*>(ones)[i] = 0x3F803F80u;   // bf16 1.0 pairs
     if (tid == 0) {
-        mbar_init(&bar_tma[0], 1);
-        mbar_init(&bar_tma[1], 1);
-        mbar_init(&bar_mma, 1);
+        for (int s = 0; s < S; s++) {
+            mbar_init(&bar_full[s], 1);
+            mbar_init(&bar_empty[s], 1);
+        }
         fence_mbar_init();
         s_fail = 0;
     }
@@ -402,44 +413,52 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    auto tile_coords = [&](long long t, int& n, int& h, int& w0) {
+    auto tile_coords = [&](long long i, int& n, int& h, int& w0) {
+        const long long t = blockIdx.x + i * gridDim.x;
         const int tw = (int)(t % tiles_w);
         const long long r = t / tiles_w;
         h = (int)(r % a.H);
         n = (int)(r / a.H);
         w0 = tw * kConvTile;
     };
-    auto issue_loads = [&](long long t, int buf) {
-        int n, h, w0;
-        tile_coords(t, n, h, w0);
-        unsigned char* st = smem + buf * STAGE;
-        mbar_arrive_expect_tx(&bar_tma[buf], XBOX + DYBOX);
-        tma_load_5d(st, &tm_dy, 0, w0, h, 0, n, &bar_tma[buf]);
-        tma_load_5d(st + DY_ALLOC, &tm_x, 0, w0 - 1, h - 1, 0, n, &bar_tma[buf]);
-    };
-    long long t = blockIdx.x;
     if (tid == 0) {
-        if (t < ntiles) issue_loads(t, 0);
+        long long tma_next = 0, full_seen = 0, mma_done = 0;
         bool ok = true;
+        auto issue_loads = [&](long long i) -> bool {
+            const int s = (int)(i % S);
+            if (i >= S && !mbar_wait(&bar_empty[s], (uint32_t)((i / S - 1) & 1))) return false;
+            int n, h, w0;
+            tile_coords(i, n, h, w0);
+            mbar_arrive_expect_tx(&bar_full[s], XBOX + DYBOX);
+            tma_load_5d(smem + s * DY_ALLOC, &tm_dy, 0, w0 / PIX, h, 0, n, &bar_full[s]);
+            tma_load_5d(xbox0 + s * X_ALLOC, &tm_x, 0, w0 / PIX - 1, h - 1, 0, n, &bar_full[s]);
+            return true;
+        };
+        while (tma_next < nmine && tma_next < S - 1) issue_loads(tma_next++);
+        const uint32_t ob = smem_u32(ones);
         uint32_t accum = 0;
-        for (int it = 0; t < ntiles && ok; t += gridDim.x, it++) {
-            const int buf = it & 1;
-            ok = mbar_wait(&bar_tma[buf], (it >> 1) & 1);
-            if (!ok) break;
+        for (long long j = 0; j < nmine; j++) {
+            const int s = (int)(j % S);
+            if (!mbar_wait(&bar_full[s], (uint32_t)((j / S) & 1))) { ok = false; break; }
+            full_seen = j + 1;
             tc_fence_after();
-            const uint32_t dyb = smem_u32(smem + buf * STAGE), xb = dyb + DY_ALLOC, ob = smem_u32(ones);
+            const uint32_t dyb = smem_u32(smem + s * DY_ALLOC), xb = smem_u32(xbox0 + s * X_ALLOC) + A0;
             for (int k0 = 0; k0 < kConvTile; k0 += 16) {
                 const uint64_t da = umma_desc(dyb + (uint32_t)(k0 * 16), 128, kConvTile * 16);
                 if (CH == 4) {
 #pragma unroll
                     for (int tap = 0; tap < 9; tap++) {
-                        const uint64_t db = umma_desc(xb + tap_off(tap, CH) + (uint32_t)(k0 * 16), 128, 3 * kBoxW * 16);
+                        const uint64_t db =
+                            umma_desc(xb + tap_off(tap, CH, BOXW) + (uint32_t)(k0 * 16), 128, 3 * BOXW * 16);
                         umma_bf16(tmem + (uint32_t)(tap * 32), da, db, umma_idesc(32, true, true), accum);
                     }
                 } else {
 #pragma unroll
                     for (int p = 0; p < 5; p++) {
-                        const uint32_t o0 = tap_off(2 * p, CH), o1 = tap_off(2 * p + 1, CH);
+                        // tap 9 is the zero rows after the box (the offset from
+                        // the shifted start is the plain one minus A0)
+                        const uint32_t o0 = tap_off(2 * p, CH, BOXW) - (2 * p >= 9 ? A0 : 0);
+                        const uint32_t o1 = tap_off(2 * p + 1, CH, BOXW) - (2 * p + 1 >= 9 ? A0 : 0);
                         const uint64_t db = umma_desc(xb + o0 + (uint32_t)(k0 * 16), 128, o1 - o0);
                         umma_bf16(tmem + (uint32_t)(p * 16), da, db, umma_idesc(16, true, true), accum);
                     }
@@ -448,14 +467,22 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
                 umma_bf16(tmem + (uint32_t)BIAS_COL, da, dbo, umma_idesc(16, true, true), accum);
                 accum = 1;
             }
-            umma_commit(&bar_mma);
-            const long long tn = t + gridDim.x;
-            // this tile's MMAs must finish reading its buffer before the one
-            // after next is loaded into it; the next tile uses the other buffer
-            if (tn < ntiles) issue_loads(tn, buf ^ 1);
-            ok = mbar_wait(&bar_mma, it & 1);
+            umma_commit(&bar_empty[s]);
+            mma_done = j + 1;
+            if (tma_next < nmine) {
+                if (!issue_loads(tma_next)) { ok = false; break; }
+                tma_next++;
+            }
         }
-        if (!ok) s_fail = 1;
+        // the last group completes after every earlier one
+        if (ok && mma_done > 0) ok = mbar_wait(&bar_empty[(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
+        if (!ok) {
+            s_fail = 1;
+            // give what is in flight its own bounded wait before the shared
+            // memory and the accumulator columns are released
+            for (long long i = full_seen; i < tma_next; i++) mbar_wait(&bar_full[i % S], (uint32_t)((i / S) & 1));
+            if (mma_done > 0) mbar_wait(&bar_empty[(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -463,7 +490,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
     if (!s_fail && warp == 0) {
         // lanes 0..31 hold output channels 0..31; columns in blocks of 32
         float* dst = a.partial + (long long)blockIdx.x * 32 * a.ncols;
-        const bool any = blockIdx.x < ntiles;
+        const bool any = nmine > 0;
         for (int cb = 0; cb < a.ncols; cb += 32) {
             float v[32];
             tmem_ld32(tmem + (uint32_t)cb, v);
@@ -607,26 +634,29 @@ extern "C" int rn_conv3x3_wgrad(float* d_dw, float* d_partial, size_t partial_by
     if (partial_bytes < (size_t)grid * 32 * ncols * sizeof(float))
         return set_error(RN_ERR_ARG, "conv wgrad: partial buffer too small (" + std::to_string((size_t)grid * 32 * ncols * 4) +
                                          " bytes needed)");
-    CUtensorMap mx, mdy;
-    RN_TRY(make_act_map(&mx, d_x, N, cin / 8, H, W, kBoxW, 3));
-    RN_TRY(make_act_map(&mdy, d_dy, N, cout / 8, H, W, kConvTile, 1));
     WgradArgs a{d_partial, N, H, W, ncols, d_err};
     cudaStream_t st = (cudaStream_t)stream;
-    const uint32_t xbox = (cin / 8) * 3 * kBoxW * 16;
-    const size_t stage = (32768 + 1024) + ((xbox + kZeroBytes + 1023) & ~1023u);
-    const size_t smem = 2 * stage + 512 + 1024;
-    if (cin == 32 && cout == 32) {
-        RN_CUDA_TRY(cudaFuncSetAttribute(conv3x3_wgrad_kernel<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        conv3x3_wgrad_kernel<4, 4><<<grid, kConvThreads, smem, st>>>(mx, mdy, a);
-    } else if (cin == 32 && cout == 8) {
-        RN_CUDA_TRY(cudaFuncSetAttribute(conv3x3_wgrad_kernel<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        conv3x3_wgrad_kernel<4, 1><<<grid, kConvThreads, smem, st>>>(mx, mdy, a);
-    } else if (cin == 8 && cout == 32) {
-        RN_CUDA_TRY(cudaFuncSetAttribute(conv3x3_wgrad_kernel<1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        conv3x3_wgrad_kernel<1, 4><<<grid, kConvThreads, smem, st>>>(mx, mdy, a);
-    } else {
+    auto run = [&](auto pix) -> int {
+        constexpr int P = decltype(pix)::value;
+        CUtensorMap mx, mdy;
+        RN_TRY(make_act_map(&mx, d_x, N, cin / 8, H, W, kConvTile + 2 * P, 3, P));
+        RN_TRY(make_act_map(&mdy, d_dy, N, cout / 8, H, W, kConvTile, 1, P));
+        const uint32_t xbox = (cin / 8) * 3 * (kConvTile + 2 * P) * 16;
+        const uint32_t dyb = (cout / 8) * kConvTile * 16;
+        const size_t smem = kWgStages * (((dyb + 1023) & ~1023u) + ((xbox + kZeroBytes + 1023) & ~1023u)) + 512 + 1024;
+        auto launch = [&](auto kern) -> int {
+            RN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kern<<<grid, kConvThreads, smem, st>>>(mx, mdy, a);
+            return RN_OK;
+        };
+        if (cin == 32 && cout == 32) return launch(conv3x3_wgrad_kernel<4, 4, P>);
+        if (cin == 32 && cout == 8) return launch(conv3x3_wgrad_kernel<4, 1, P>);
+        if (cin == 8 && cout == 32) return launch(conv3x3_wgrad_kernel<1, 4, P>);
         return set_error(RN_ERR_ARG, "conv wgrad: unsupported channel pair");
-    }
+    };
+    if (W % 8 == 0) RN_TRY(run(std::integral_constant<int, 8>{}));
+    else if (W % 2 == 0) RN_TRY(run(std::integral_constant<int, 2>{}));
+    else RN_TRY(run(std::integral_constant<int, 1>{}));
     RN_CUDA_TRY(cudaGetLastError());
     const int n = 32 * ncols;
     conv_wgrad_reduce<<<(n + 255) / 256, 256, 0, st>>>(d_dw, d_partial, grid, n);
