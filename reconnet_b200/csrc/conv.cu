@@ -359,15 +359,16 @@ struct WgradArgs {
     int* err;
 };
 
-// Thread 0 keeps kWgStages - 1 tiles' loads (a dY box and an X box each) in
-// flight ahead of the tile whose MMA group it issues; each group commits to
-// its stage's "empty" barrier, which the load kWgStages - 1 tiles later waits
-// for.  Boxes take PIX pixels per TMA row as in the forward kernel.
+// kWgStages - 1 tiles' loads (a dY box and an X box each) stay in flight
+// ahead of the tile whose MMAs are issued; each tile's MMA groups commit to
+// its stage's "empty" barriers, which the load kWgStages - 1 tiles later
+// waits for.  Boxes take PIX pixels per TMA row as in the forward kernel.
 // The A operand (dY, M = 128 output-channel rows of which the first 8 CHO are
 // real) spans 16 groups of 8 rows 2048 bytes apart: groups past the dY box
 // read whatever shared memory follows it (more boxes), which only feeds
 // accumulator rows that are never read.
 constexpr int kWgStages = 4;
+constexpr int kWgIssuers = 2;   // MMA-issuing threads (lane 0 of warps 0 and 1)
 
 template <int CH, int CHO, int PIX>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x,
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     unsigned char* xbox0 = smem + S * DY_ALLOC;
     unsigned char* ones = xbox0 + S * X_ALLOC;   // 512 B of bf16 ones: the bias-gradient B operand
-    __shared__ __align__(8) uint64_t bar_full[S], bar_empty[S];
+    __shared__ __align__(8) uint64_t bar_full[S], bar_empty[kWgIssuers][S];
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -402,7 +403,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
             mbar_init(&bar_full[s], 1);
-            mbar_init(&bar_empty[s], 1);
+            for (int q = 0; q < kWgIssuers; q++) mbar_init(&bar_empty[q][s], 1);
         }
         fence_mbar_init();
         s_fail = 0;
@@ -421,12 +422,22 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
         n = (int)(r / a.H);
         w0 = tw * kConvTile;
     };
-    if (tid == 0) {
+    // kWgIssuers issuers, lane 0 of warps 0, 1, .. (warp 0's also issues the
+    // loads), split each K step's MMA slots (k < 9: tap k with 32 channels;
+    // CH = 1: k < 5 a pair of taps; the last slot the bias columns) into
+    // contiguous runs, one per issuer.  Each commits to its own "empty"
+    // barrier of the stage; a stage is refilled once every issuer's group has
+    // read it.  (Two issuers: 0.59 ms per 32-channel layer against 0.77 for
+    // one; four, dealing slots round-robin, 0.71.)
+    if ((tid & 31) == 0 && warp < kWgIssuers) {
+        const int q = warp;
         long long tma_next = 0, full_seen = 0, mma_done = 0;
         bool ok = true;
         auto issue_loads = [&](long long i) -> bool {
             const int s = (int)(i % S);
-            if (i >= S && !mbar_wait(&bar_empty[s], (uint32_t)((i / S - 1) & 1))) return false;
+            if (i >= S)
+                for (int r = 0; r < kWgIssuers; r++)
+                    if (!mbar_wait(&bar_empty[r][s], (uint32_t)((i / S - 1) & 1))) return false;
             int n, h, w0;
             tile_coords(i, n, h, w0);
             mbar_arrive_expect_tx(&bar_full[s], XBOX + DYBOX);
@@ -434,7 +445,8 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
             tma_load_5d(xbox0 + s * X_ALLOC, &tm_x, 0, w0 / PIX - 1, h - 1, 0, n, &bar_full[s]);
             return true;
         };
-        while (tma_next < nmine && tma_next < S - 1) issue_loads(tma_next++);
+        if (q == 0)
+            while (tma_next < nmine && tma_next < S - 1) issue_loads(tma_next++);
         const uint32_t ob = smem_u32(ones);
         uint32_t accum = 0;
         for (long long j = 0; j < nmine; j++) {
@@ -445,43 +457,45 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_kernel(const __gri
             const uint32_t dyb = smem_u32(smem + s * DY_ALLOC), xb = smem_u32(xbox0 + s * X_ALLOC) + A0;
             for (int k0 = 0; k0 < kConvTile; k0 += 16) {
                 const uint64_t da = umma_desc(dyb + (uint32_t)(k0 * 16), 128, kConvTile * 16);
-                if (CH == 4) {
+                constexpr int NSLOT = CH == 4 ? 10 : 6;   // taps (or tap pairs), then the bias
 #pragma unroll
-                    for (int tap = 0; tap < 9; tap++) {
-                        const uint64_t db =
-                            umma_desc(xb + tap_off(tap, CH, BOXW) + (uint32_t)(k0 * 16), 128, 3 * BOXW * 16);
-                        umma_bf16(tmem + (uint32_t)(tap * 32), da, db, umma_idesc(32, true, true), accum);
-                    }
-                } else {
-#pragma unroll
-                    for (int p = 0; p < 5; p++) {
-                        // tap 9 is the zero rows after the box (the offset from
-                        // the shifted start is the plain one minus A0)
-                        const uint32_t o0 = tap_off(2 * p, CH, BOXW) - (2 * p >= 9 ? A0 : 0);
-                        const uint32_t o1 = tap_off(2 * p + 1, CH, BOXW) - (2 * p + 1 >= 9 ? A0 : 0);
+                for (int k = 0; k < NSLOT; k++) {
+                    constexpr int PER = (NSLOT + kWgIssuers - 1) / kWgIssuers;
+                    if (k / PER != q) continue;
+                    if (k == NSLOT - 1) {
+                        const uint64_t dbo = umma_desc(ob, 128, 256);
+                        umma_bf16(tmem + (uint32_t)BIAS_COL, da, dbo, umma_idesc(16, true, true), accum);
+                    } else if (CH == 4) {
+                        const uint64_t db = umma_desc(xb + tap_off(k, CH, BOXW) + (uint32_t)(k0 * 16), 128, 3 * BOXW * 16);
+                        umma_bf16(tmem + (uint32_t)(k * 32), da, db, umma_idesc(32, true, true), accum);
+                    } else {
+                        // tap 9 is the zero rows after the box (the offset
+                        // from the shifted start is the plain one minus A0)
+                        const uint32_t o0 = tap_off(2 * k, CH, BOXW) - (2 * k >= 9 ? A0 : 0);
+                        const uint32_t o1 = tap_off(2 * k + 1, CH, BOXW) - (2 * k + 1 >= 9 ? A0 : 0);
                         const uint64_t db = umma_desc(xb + o0 + (uint32_t)(k0 * 16), 128, o1 - o0);
-                        umma_bf16(tmem + (uint32_t)(p * 16), da, db, umma_idesc(16, true, true), accum);
+                        umma_bf16(tmem + (uint32_t)(k * 16), da, db, umma_idesc(16, true, true), accum);
                     }
                 }
-                const uint64_t dbo = umma_desc(ob, 128, 256);
-                umma_bf16(tmem + (uint32_t)BIAS_COL, da, dbo, umma_idesc(16, true, true), accum);
                 accum = 1;
             }
-            umma_commit(&bar_empty[s]);
+            umma_commit(&bar_empty[q][s]);
             mma_done = j + 1;
-            if (tma_next < nmine) {
+            if (q == 0 && tma_next < nmine) {
                 if (!issue_loads(tma_next)) { ok = false; break; }
                 tma_next++;
             }
         }
-        // the last group completes after every earlier one
-        if (ok && mma_done > 0) ok = mbar_wait(&bar_empty[(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
+        // the last group of this issuer completes after every earlier one
+        if (ok && mma_done > 0)
+            ok = mbar_wait(&bar_empty[q][(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
         if (!ok) {
             s_fail = 1;
             // give what is in flight its own bounded wait before the shared
             // memory and the accumulator columns are released
-            for (long long i = full_seen; i < tma_next; i++) mbar_wait(&bar_full[i % S], (uint32_t)((i / S) & 1));
-            if (mma_done > 0) mbar_wait(&bar_empty[(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
+            if (q == 0)
+                for (long long i = full_seen; i < tma_next; i++) mbar_wait(&bar_full[i % S], (uint32_t)((i / S) & 1));
+            if (mma_done > 0) mbar_wait(&bar_empty[q][(mma_done - 1) % S], (uint32_t)(((mma_done - 1) / S) & 1));
         }
     }
     tc_fence_before();
