@@ -563,11 +563,11 @@ def prior_run(dev, n_train=256, n_eval=32, train_steps=4000, tv_iters=100):
     are reconstructed by (a) TV-SQS for tv_iters iterations and (b) 4 OS-SQS
     iterations + the network.  Time-to-RMSE: the target is TV-SQS's final
     RMSE + 1 HU; TV's time is that of its first iteration within the target.
-    Two judges: the high-dose reconstruction of the held-out slices (100 TV-SQS
+    Two references for the RMSE: the high-dose reconstruction of the held-out slices (100 TV-SQS
     iterations at I0 = 1e6, the training targets' definition), and the
     phantom itself; at I0 = 1e4 a part of the rays through these phantoms is
     photon-starved, which leaves every reconstruction hundreds of HU from the
-    phantom, so the high-dose judge is the one the 1 HU margin is read on."""
+    phantom, so the high-dose reference is the one the 1 HU margin is read on."""
     import torch
 
     from reconnet_b200 import learned_prior as LP
@@ -625,16 +625,16 @@ def prior_run(dev, n_train=256, n_eval=32, train_steps=4000, tv_iters=100):
     net.k.check()
     r_learned = rmse(y)
 
-    def judge(tr, r_l):
+    def time_to_target(tr, r_l):
         tgt = tr[-1] + 1.0
         k_reach = next((k for k, r in enumerate(tr) if r <= tgt), None)
         t_ms = None if k_reach is None else (k_reach + 1) * tv_ms_per_iter
         sp = None if (t_ms is None or r_l > tgt) else t_ms / learned_ms
         return tgt, t_ms, sp
 
-    target, tv_ms_to_target, speedup = judge(traj, r_learned)
+    target, tv_ms_to_target, speedup = time_to_target(traj, r_learned)
     r_learned_hd = rmse_hd(y)
-    target_hd, tv_ms_to_target_hd, speedup_hd = judge(traj_hd, r_learned_hd)
+    target_hd, tv_ms_to_target_hd, speedup_hd = time_to_target(traj_hd, r_learned_hd)
     conv = conv_roofline(dev)
     return {"conv_32x32": conv,
             "workload": f"512x512 @0.7 mm, 888 ch, {nview} views; train {n_train} slices (4-iteration OS-SQS at "
@@ -645,7 +645,7 @@ def prior_run(dev, n_train=256, n_eval=32, train_steps=4000, tv_iters=100):
             "tv_rmse_hu_at": {str(k + 1): traj[k] for k in (0, 3, 9, 19, 49, tv_iters - 1) if k < tv_iters},
             "lr_schedule": "Adam, 1e-3 cosine-decayed to 1e-5, batch 8, the eight orientations of the square",
             "learned_ms": learned_ms,
-            "judge_high_dose": {
+            "against_high_dose": {
                 "reference": "100-iteration TV-SQS at I0=1e6 of the held-out slices",
                 "tv_rmse_hu_final": traj_hd[-1],
                 "tv_rmse_hu_at": {str(k + 1): traj_hd[k] for k in (0, 3, 9, 19, 49, tv_iters - 1) if k < tv_iters},
@@ -653,7 +653,7 @@ def prior_run(dev, n_train=256, n_eval=32, train_steps=4000, tv_iters=100):
                 "learned_rmse_hu": r_learned_hd, "os_sqs4_rmse_hu": rmse_hd(x4),
                 "speedup_time_to_rmse": speedup_hd,
                 "target_met": bool(speedup_hd is not None and speedup_hd >= 3.0)},
-            "judge_phantom": {
+            "against_phantom": {
                 "rmse_target_hu": target, "tv_ms_to_target": tv_ms_to_target,
                 "learned_rmse_hu": r_learned, "os_sqs4_rmse_hu": rmse(x4),
                 "speedup_time_to_rmse": speedup,

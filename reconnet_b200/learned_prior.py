@@ -6,7 +6,7 @@ accumulation, BF16 weights and activations).
 
 It stands in for the TV proximal step of OS-SQS: a few OS-SQS iterations
 followed by the network (``learned_ossqs``) against plain TV-SQS, which stays
-the fallback and the judge of the image RMSE.  The reference has no CNN; its
+the fallback and the yardstick of the image RMSE.  The reference has no CNN; its
 learned use of the projectors runs through TensorFlow with the projector pair
 as differentiable ops (python/ReconNet.py:773-830).
 
