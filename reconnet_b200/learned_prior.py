@@ -317,3 +317,40 @@ def learned_ossqs(net: PriorCNN, geom, nview, ang, b, w, S, n_iter=4, n_subsets=
     remaining work; returns (image, the OS-SQS image)."""
     x, _ = os_sqs(geom, nview, ang, b, w, S, n_iter, n_subsets)
     return net.denoise(x).clamp_min_(0.0), x
+
+
+# The schedules the learned path chooses from: OS-SQS iteration counts with
+# "N" marking a pass of the network (its output is the next iteration's
+# start).  The first entry is the path the network is trained for (its inputs
+# are 4-iteration images).
+SCHEDULES = ((4, "N"), (4, "N", 2, "N"), (4, "N", 2, "N", 2), (4, "N", 3, "N", 2), (4, "N", 4, "N", 2),
+             (4, "N", 2, "N", 2, "N", 2))
+
+
+def schedule_cost(schedule):
+    """(OS-SQS iterations, network passes) of a schedule."""
+    return sum(t for t in schedule if t != "N"), sum(1 for t in schedule if t == "N")
+
+
+def run_schedule(net: PriorCNN, solver, x0: torch.Tensor, schedule) -> torch.Tensor:
+    """Learned-prior OS-SQS: the solver's TV OS-SQS iterations (BatchedOSSQS,
+    graph-replayed) interleaved with passes of the network, in the order
+    `schedule` gives (see SCHEDULES)."""
+    x = x0
+    for t in schedule:
+        x = net.denoise(x).clamp_min_(0.0) if t == "N" else solver.run(x, t)
+    return x
+
+
+def choose_schedule(net: PriorCNN, solver, x_ref: torch.Tensor, target_rmse: float, schedules=SCHEDULES):
+    """The cheapest schedule (fewest iterations, then fewest network passes)
+    whose RMSE against x_ref on the solver's slices (a validation set, not the
+    slices the result is reported on) is within target_rmse; the one with the
+    lowest RMSE if none is.  Returns (schedule, {schedule: rmse})."""
+    errs = {}
+    for sch in schedules:
+        x = run_schedule(net, solver, torch.zeros_like(x_ref), sch)
+        errs[sch] = float(torch.sqrt(((x - x_ref) ** 2).mean()))
+    ok = [sch for sch in schedules if errs[sch] <= target_rmse]
+    best = min(ok, key=schedule_cost) if ok else min(schedules, key=lambda sch: errs[sch])
+    return best, errs

@@ -110,3 +110,33 @@ def test_bench_shards_independent_batches_per_rank():
     assert c0 != c1 and s0 != s1                  # different batches per rank
     assert tot0 == tot1 == sum(c0) + sum(c1)      # all-reduce reaches every rank
     assert ms0 == ms1 == 11.0                      # max over ranks
+
+
+def test_learned_schedule_choice_is_cheapest_within_target():
+    """choose_schedule takes the schedule with the fewest OS-SQS iterations
+    (then network passes) whose RMSE is within the target, and the lowest-RMSE
+    one when none is; run_schedule applies iterations and network passes in
+    the order given.  Checked with stand-ins for the solver and the network."""
+    import torch
+    from reconnet_b200 import learned_prior as LP
+
+    class Net:
+        def denoise(self, x):
+            return x * 0.5
+
+    class Solver:
+        def run(self, x, k):
+            return x + k
+
+    x0 = torch.zeros(2, 3)
+    assert float(LP.run_schedule(Net(), Solver(), x0, (4, "N", 2, "N", 2))[0, 0]) == 4.0   # ((4/2)+2)/2+2
+    assert LP.schedule_cost((4, "N", 3, "N", 2)) == (9, 2)
+    ref = torch.full((2, 3), 2.0)
+    sch, errs = LP.choose_schedule(Net(), Solver(), ref, 0.5)
+    assert sch == (4, "N") and errs[(4, "N")] == 0.0
+    # only the schedules ending in 2 iterations after two passes reach 4.0
+    sch, errs = LP.choose_schedule(Net(), Solver(), torch.full((2, 3), 4.0), 0.1)
+    assert sch == (4, "N", 2, "N", 2)
+    # none within the target: the lowest RMSE
+    sch, errs = LP.choose_schedule(Net(), Solver(), torch.full((2, 3), 100.0), 0.1)
+    assert errs[sch] == min(errs.values())
