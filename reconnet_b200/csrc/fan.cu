@@ -73,7 +73,12 @@ __global__ void edge_slope_kernel(double* edges, const double2* view_cs, const i
 // ---------------------------------------------------------------------------
 // Line prologue: for each FP slice, X lines (image rows, boundary l between
 // rows l-1 and l) and Y lines (columns).  Entry k of a line holds the prefix
-// P[k] = sum_{i<k} a_i as (hi, lo) and the value a_k (a_n = 0).
+// P[k] = sum_{i<k} a_i (summed in FP64) and the value a_k (a_n = 0).
+// Band mode (Siddon): P as (hi, lo) floats in `hl`, a_k in `la`; the band
+// integrals need prefix differences across a fraction of one cell.  DD mode:
+// (P rounded to FP32, a_k) packed in `hl`, `la` unused; a DD footprint spans
+// about a cell, so the prefix's FP32 rounding moves a projection by ~1e-7
+// relative (independent roundings over the lines a ray crosses).
 // ---------------------------------------------------------------------------
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
                                  FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems,
@@ -144,22 +149,26 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
         for (int c = 0; c < 4; c++) {
             const int k = k0 + 32 * c + lane;
             if (k < n) {
-                ohl[line_pos(k + M)] = split_double(sp[32 * c + lane]);
-                ola[line_pos(k + M)] = v[c];
+                if (band) {
+                    ohl[line_pos(k + M)] = split_double(sp[32 * c + lane]);
+                    ola[line_pos(k + M)] = v[c];
+                } else {
+                    ohl[line_pos(k + M)] = make_float2((float)sp[32 * c + lane], v[c]);
+                }
             }
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
         __syncwarp();   // the next block overwrites sa and sp
     }
     // margins: P = 0 before the line, P = total from position n on
-    float2 tot = split_double(carry);
+    const float2 tot = band ? split_double(carry) : make_float2((float)carry, 0.f);
     for (int j = lane; j < M; j += 32) {
         ohl[line_pos(j)] = make_float2(0.f, 0.f);
-        ola[line_pos(j)] = 0.f;
+        if (band) ola[line_pos(j)] = 0.f;
     }
     for (int j = n + M + lane; j < lp; j += 32) {
         ohl[line_pos(j)] = tot;
-        ola[line_pos(j)] = 0.f;
+        if (band) ola[line_pos(j)] = 0.f;
     }
 }
 
@@ -253,8 +262,9 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
     float4* s_edge = reinterpret_cast<float4*>(smem + kFpHeader);
     size_t off = kFpHeader + sizeof(float4) * (size_t)p.vt * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    // double buffer: buffer b holds R lines of (hi, lo) then R lines of values
-    const size_t hl_bytes = (size_t)R * sp * sizeof(float2), la_bytes = (size_t)R * sp * sizeof(float);
+    // double buffer: buffer b holds R lines of float2 entries ((P, a) packed
+    // for DD; (hi, lo) then R lines of values for Siddon)
+    const size_t hl_bytes = (size_t)R * sp * sizeof(float2), la_bytes = kSiddon ? (size_t)R * sp * sizeof(float) : 0;
     unsigned char* const buf0 = smem + off;
     const size_t buf_bytes = hl_bytes + la_bytes;
 
@@ -324,12 +334,12 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         int l0 = c * R;
         int rc = min(R, nlines - l0);
         uint32_t bh = (uint32_t)((size_t)rc * sp * sizeof(float2));
-        uint32_t ba = (uint32_t)((size_t)rc * sp * sizeof(float));
+        uint32_t ba = kSiddon ? (uint32_t)((size_t)rc * sp * sizeof(float)) : 0u;
         unsigned char* dst = buf0 + b * buf_bytes;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bars[b], bh + ba);
         bulk_g2s(dst, ghl + (long long)l0 * sp, bh, &bars[b]);
-        bulk_g2s(dst + hl_bytes, gla + (long long)l0 * sp, ba, &bars[b]);
+        if (kSiddon) bulk_g2s(dst + hl_bytes, gla + (long long)l0 * sp, ba, &bars[b]);
     };
     // per-line factors 1 / (l - perp) of chunk c into slot c & 1
     auto line_factors = [&](int c) {
@@ -384,21 +394,19 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
         };
         // prefix integral at this lane's edge on line j and the footprint
         // difference with the next lane's edge: cell kk and fraction f of the
-        // padded position, floored by a round-down add against 1.5*2^23.
-        // Positions beyond the padded line clamp to its ends, where the prefix
-        // is 0 or the line total and the value 0, so a ray that misses line j
-        // adds exactly 0.
-        auto footprint = [&](float jf, int Xi, float Xf, float r, const float2* hrow, const float* arow) -> float {
+        // padded position, floored by a round-down add against 1.5*2^23, and
+        // one packed (P, a) entry read.  Positions beyond the padded line
+        // clamp to its ends, where the prefix is 0 or the line total and the
+        // value 0, so a ray that misses line j adds exactly 0.
+        auto footprint = [&](float jf, int Xi, float Xf, float r, const float2* hrow) -> float {
             const float x = fmaf(r, jf, Xf);
             const float y = __fadd_rd(x, kFloorBias);
             const unsigned kk = min((unsigned)max(__float_as_int(y) + Xi, 0), lpm1);
             const unsigned pos = kk + (kk >> 4);   // line_pos
             const float f = x - (y - kFloorBias);
             const float2 h = hrow[pos];
-            const float hi = h.x, rest = fmaf(f, arow[pos], h.y);
-            const float nhi = __shfl_down_sync(0xffffffffu, hi, 1);
-            const float nrest = __shfl_down_sync(0xffffffffu, rest, 1);
-            return (nhi - hi) + (nrest - rest);
+            const float P = fmaf(f, h.y, h.x);
+            return __shfl_down_sync(0xffffffffu, P, 1) - P;
         };
         // Siddon (kSiddon): lane = ray.  On band j (image row / column j, not
         // blended) the ray runs from its position at boundary j to boundary
@@ -438,8 +446,8 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                 for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp)
                     a += band(jf, Xi, Xf, r, ir, hrow, arow);
             } else {
-                for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp)
-                    a = fmaf(footprint(jf, Xi, Xf, r, hrow, arow), g[j], a);
+                for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp)
+                    a = fmaf(footprint(jf, Xi, Xf, r, hrow), g[j], a);
             }
             acc[k] = a;
         };
@@ -468,9 +476,9 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
                         ab += band(jf, Xib, Xfb, rb, irb, hrow, arow);
                     }
                 } else {
-                    for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp, arow += sp) {
-                        aa = fmaf(footprint(jf, Xia, Xfa, ra, hrow, arow), ga[j], aa);
-                        ab = fmaf(footprint(jf, Xib, Xfb, rb, hrow, arow), gb[j], ab);
+                    for (int j = J0; j < J1; j++, jf += 1.f, hrow += sp) {
+                        aa = fmaf(footprint(jf, Xia, Xfa, ra, hrow), ga[j], aa);
+                        ab = fmaf(footprint(jf, Xib, Xfb, rb, hrow), gb[j], ab);
                     }
                 }
                 acc[k] = aa;
@@ -1257,10 +1265,11 @@ int fan_fp_views(int nu) {
     return std::min(kFpViews, (kFpGroups * (kFpThreads / 32)) / ngpv);
 }
 
-static size_t fp_smem_bytes(int nu, int sp, int R) {
+// DD lines are packed (P, a) float2 entries; Siddon lines add a value array
+static size_t fp_smem_bytes(int nu, int sp, int R, bool siddon) {
     size_t off = kFpHeader + sizeof(float4) * (size_t)fan_fp_views(nu) * (nu + 1);
     off = (off + 127) & ~size_t(127);
-    return off + 2 * (size_t)R * sp * (sizeof(float2) + sizeof(float));
+    return off + 2 * (size_t)R * sp * (sizeof(float2) + (siddon ? sizeof(float) : 0));
 }
 
 static size_t bp_smem_bytes(int win) {
@@ -1419,24 +1428,27 @@ int fan_slope_tables(rn_fan_plan* p, const double2* d_vcs, const int* d_vx, cons
     return RN_OK;
 }
 
-static int fp_lines_for_smem(int nu, int sp) {
+static int fp_lines_for_smem(int nu, int sp, bool siddon) {
     int R = kFpMaxLines;
-    while (R > 1 && fp_smem_bytes(nu, sp, R) > (size_t)kSmemBudget) R--;
+    while (R > 1 && fp_smem_bytes(nu, sp, R, siddon) > (size_t)kSmemBudget) R--;
     return R;
 }
 
-int fan_fp_lines_max(const rn_fan_plan* p) {
-    return std::min(fp_lines_for_smem(p->dims.nu, p->dims.spx), fp_lines_for_smem(p->dims.nu, p->dims.spy));
+static int fp_lines_max(const rn_fan_plan* p, bool siddon) {
+    return std::min(fp_lines_for_smem(p->dims.nu, p->dims.spx, siddon),
+                    fp_lines_for_smem(p->dims.nu, p->dims.spy, siddon));
 }
+
+int fan_fp_lines_max(const rn_fan_plan* p) { return fp_lines_max(p, false); }
 
 int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t st, bool siddon) {
     const FanDims& d = p->dims;
     const int nfp = (int)p->h_fp.size();
-    const int Rmax = fan_fp_lines_max(p);
+    const int Rmax = fp_lines_max(p, siddon);
     const int R = p->fp_R > 0 ? std::min(p->fp_R, Rmax) : Rmax;
-    if (fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R) > (size_t)kSmemBudget)
+    if (fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R, siddon) > (size_t)kSmemBudget)
         return set_error(RN_ERR_ARG, "fan projection: image lines too long for shared memory");
-    const size_t smem = fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R);
+    const size_t smem = fp_smem_bytes(d.nu, std::max(d.spx, d.spy), R, siddon);
     // slices are processed in waves of at most `slots` line buffers
     const long long slot = p->line_slot_elems;
     const int slots = (int)std::max<long long>(1, std::min<long long>(nfp, p->fp_slots));
@@ -1732,8 +1744,8 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
         return set_error(RN_ERR_ARG, "rn_fan_project_noalloc: this geometry needs " + std::to_string(off) +
                                          " bytes of scratch, more than its fixed " +
                                          std::to_string(kNoAllocScratchBytes) + " bytes");
-    const int R = std::min(fp_lines_for_smem(nu, d.spx), fp_lines_for_smem(nu, d.spy));
-    const size_t smem = fp_smem_bytes(nu, std::max(d.spx, d.spy), R);
+    const int R = std::min(fp_lines_for_smem(nu, d.spx, false), fp_lines_for_smem(nu, d.spy, false));
+    const size_t smem = fp_smem_bytes(nu, std::max(d.spx, d.spy), R, false);
     if (smem > (size_t)kSmemBudget) return set_error(RN_ERR_ARG, "image lines too long for shared memory");
 
     // host-side tables, same quantities as fan_build_geometry
