@@ -40,9 +40,9 @@ namespace rn {
 // ---------------------------------------------------------------------------
 // Tunables.
 // ---------------------------------------------------------------------------
-constexpr int kFpThreads = 512;
+constexpr int kFpThreads = 768;
 constexpr int kFpViews = 4;          // views per FP CTA (at most)
-constexpr int kFpGroups = 8;         // groups of 31 rays per FP warp (at most)
+constexpr int kFpGroups = 6;         // groups of 31 rays per FP warp (at most)
 constexpr int kFpMaxLines = 16;      // lines per staged chunk (upper bound)
 constexpr int kSmemBudget = 227 * 1024;
 
