@@ -4,7 +4,8 @@ over 360 degrees, 12 ordered subsets), 10 unrolled iterations, each with a
 learnable step scale and TV weight, checkpointed per iteration.
 
 * Gradients with respect to the 20 parameters and the starting image against
-  central finite differences (eps = 1e-3 for the parameters; for the starting
+  central finite differences (eps = 2e-3 for the step scales and 1e-3 for the
+  TV weights; for the starting
   image a step along the gradient whose largest pixel is 1e-6, small against
   the TV terms' sqrt(d^2 + 1e-6) curvature in pixels whose data weights are
   photon-starved; each Richardson-combined with half the step), relative
@@ -82,9 +83,14 @@ def test_unrolled_config_gradients_match_finite_differences():
     print(f"\nunrolled OS-SQS (8 x 256^2, 720 views, 12 subsets, 10 iterations): peak memory above the inputs "
           f"{peaks[True] / 2**20:.1f} MiB with per-iteration checkpoints, {peaks[False] / 2**20:.1f} MiB without")
     assert peaks[True] < peaks[False]
-    eps = 1e-3
+    # The loss of ten iterations in FP32 kernels scatters by ~3e-7 (std, at a
+    # loss of ~260) around a smooth curve when step[0] moves in steps of 2e-4
+    # (measured).  The step-scale gradients are ~0.2: at eps / 2 = 1e-3 that
+    # scatter is ~0.1% of them (at 5e-4, ~0.3%, too close to the tolerance).
+    # The TV-weight gradients are ~25, and the loss is curved more strongly
+    # in them, so they keep eps = 1e-3.
     with torch.no_grad():
-        for vec, grad, other, first in ((step, gs, tvw, True), (tvw, gt, step, False)):
+        for vec, grad, other, first, eps in ((step, gs, tvw, True, 2e-3), (tvw, gt, step, False, 1e-3)):
             for i in range(K):
                 def central(h):
                     d = torch.zeros_like(vec)
