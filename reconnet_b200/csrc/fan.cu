@@ -40,9 +40,15 @@ namespace rn {
 // ---------------------------------------------------------------------------
 // Tunables.
 // ---------------------------------------------------------------------------
-constexpr int kFpThreads = 768;
+// FP CTA shape per mode: DD runs 24 warps of 6 ray groups (80 registers),
+// Siddon, whose band step needs more registers, 16 warps of 8 groups
+template <bool kSiddon>
+struct FpCfg {
+    static constexpr int threads = kSiddon ? 512 : 768;
+    static constexpr int groups = kSiddon ? 8 : 6;   // groups of 31 rays per warp (at most)
+    static constexpr int warps = threads / 32;
+};
 constexpr int kFpViews = 4;          // views per FP CTA (at most)
-constexpr int kFpGroups = 6;         // groups of 31 rays per FP warp (at most)
 constexpr int kFpMaxLines = 16;      // lines per staged chunk (upper bound)
 constexpr int kSmemBudget = 227 * 1024;
 
@@ -74,11 +80,13 @@ __global__ void edge_slope_kernel(double* edges, const double2* view_cs, const i
 // Line prologue: for each FP slice, X lines (image rows, boundary l between
 // rows l-1 and l) and Y lines (columns).  Entry k of a line holds the prefix
 // P[k] = sum_{i<k} a_i (summed in FP64) and the value a_k (a_n = 0).
-// Band mode (Siddon): P as (hi, lo) floats in `hl`, a_k in `la`; the band
-// integrals need prefix differences across a fraction of one cell.  DD mode:
-// (P rounded to FP32, a_k) packed in `hl`, `la` unused; a DD footprint spans
-// about a cell, so the prefix's FP32 rounding moves a projection by ~1e-7
-// relative (independent roundings over the lines a ray crosses).
+// Band mode (Siddon): P as (hi, lo) floats in `hl`, a_k in `la`, entry j at
+// line_pos(j) (one unused slot per 16 entries, against bank conflicts); the
+// band integrals need prefix differences across a fraction of one cell.  DD
+// mode: (P rounded to FP32, a_k) packed in `hl` at entry j, `la` unused; a DD
+// footprint spans about a cell, so the prefix's FP32 rounding moves a
+// projection by ~1e-7 relative (independent roundings over the lines a ray
+// crosses).
 // ---------------------------------------------------------------------------
 __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* __restrict__ fps, int s_begin, int ns,
                                  FanDims d, float2* __restrict__ hl, float* __restrict__ la, long long slot_elems,
@@ -98,7 +106,7 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
     int lp = xl ? d.lpx : d.lpy;
     const int M = d.margin;
     long long base = (long long)si * slot_elems + (xl ? (long long)l * d.spx : (long long)d.ny * d.spx + (long long)l * d.spy);
-    float2* ohl = hl + base;    // entry j (at line_pos(j)) holds position k = j - M
+    float2* ohl = hl + base;    // entry j (at line_pos(j) in band mode, j for DD) holds position k = j - M
     float* ola = la + base;
     // blended value of rows (l-1, l) [X] or columns (l-1, l) [Y] at position k;
     // band mode (Siddon): row / column l itself
@@ -153,7 +161,7 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
                     ohl[line_pos(k + M)] = split_double(sp[32 * c + lane]);
                     ola[line_pos(k + M)] = v[c];
                 } else {
-                    ohl[line_pos(k + M)] = make_float2((float)sp[32 * c + lane], v[c]);
+                    ohl[k + M] = make_float2((float)sp[32 * c + lane], v[c]);
                 }
             }
         }
@@ -163,11 +171,11 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
     // margins: P = 0 before the line, P = total from position n on
     const float2 tot = band ? split_double(carry) : make_float2((float)carry, 0.f);
     for (int j = lane; j < M; j += 32) {
-        ohl[line_pos(j)] = make_float2(0.f, 0.f);
+        ohl[band ? line_pos(j) : j] = make_float2(0.f, 0.f);
         if (band) ola[line_pos(j)] = 0.f;
     }
     for (int j = n + M + lane; j < lp; j += 32) {
-        ohl[line_pos(j)] = tot;
+        ohl[band ? line_pos(j) : j] = tot;
         if (band) ola[line_pos(j)] = 0.f;
     }
 }
@@ -190,7 +198,6 @@ __global__ void fan_lines_kernel(const float* __restrict__ img, const FpSlice* _
 // positions beyond them clamp to the ends, so a footprint that misses a line
 // adds exactly zero and no per-ray masking is needed.
 // ---------------------------------------------------------------------------
-constexpr int kFpWarps = kFpThreads / 32;
 constexpr int kFpGroupRays = 31;
 // shared-memory header: barriers and view data (128 B), then the per-line
 // factors 1 / (l - perp) of two chunks; the per-edge table follows
@@ -238,7 +245,9 @@ __device__ __forceinline__ int fp_ray_range(double ra, double rb, double par, do
 }
 
 template <bool kSiddon>
-__global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
+__global__ void __launch_bounds__(FpCfg<kSiddon>::threads, 1) fan_fp_kernel(FpParams p) {
+    constexpr int kFpThreads = FpCfg<kSiddon>::threads, kFpGroups = FpCfg<kSiddon>::groups;
+    constexpr int kFpWarps = FpCfg<kSiddon>::warps;
     extern __shared__ __align__(128) unsigned char smem[];
     const int4 w = p.work[blockIdx.x];
     const int s = w.x, xcls = w.y, vbegin = w.z, vcount = w.w;
@@ -402,7 +411,7 @@ __global__ void __launch_bounds__(kFpThreads, 1) fan_fp_kernel(FpParams p) {
             const float x = fmaf(r, jf, Xf);
             const float y = __fadd_rd(x, kFloorBias);
             const unsigned kk = min((unsigned)max(__float_as_int(y) + Xi, 0), lpm1);
-            const unsigned pos = kk + (kk >> 4);   // line_pos
+            const unsigned pos = kk;
             const float f = x - (y - kFloorBias);
             const float2 h = hrow[pos];
             const float P = fmaf(f, h.y, h.x);
@@ -1262,7 +1271,9 @@ __global__ void __launch_bounds__(kBpThreads, (kMode == 2 || kMode == 0) ? 3 : 0
 // ---------------------------------------------------------------------------
 int fan_fp_views(int nu) {
     const int ngpv = (std::max(nu, 1) + 30) / 31;   // groups of 31 rays per view
-    return std::min(kFpViews, (kFpGroups * (kFpThreads / 32)) / ngpv);
+    // the group slots of the smaller of the two CTA shapes (work items serve both modes)
+    constexpr int slots = std::min(FpCfg<false>::groups * FpCfg<false>::warps, FpCfg<true>::groups * FpCfg<true>::warps);
+    return std::min(kFpViews, slots / ngpv);
 }
 
 // DD lines are packed (P, a) float2 entries; Siddon lines add a value array
@@ -1484,8 +1495,8 @@ int fan_project(rn_fan_plan* p, float* d_prj, const float* d_img, cudaStream_t s
             fp.vt = fan_fp_views(d.nu);
             fp.spin = p->spin_limit;
             LaunchScope ls1(p, st, 1);
-            if (siddon) fan_fp_kernel<true><<<wend - wbeg, kFpThreads, smem, st>>>(fp);
-            else fan_fp_kernel<false><<<wend - wbeg, kFpThreads, smem, st>>>(fp);
+            if (siddon) fan_fp_kernel<true><<<wend - wbeg, FpCfg<true>::threads, smem, st>>>(fp);
+            else fan_fp_kernel<false><<<wend - wbeg, FpCfg<false>::threads, smem, st>>>(fp);
             RN_CUDA_TRY(cudaGetLastError());
         }
         wbeg = wend;
@@ -1852,7 +1863,7 @@ extern "C" int rn_fan_project_noalloc(float* d_prj, const float* d_img, const fl
     fp.R = R;
     fp.vt = VT;
     fp.spin = kSpinLimit;
-    fan_fp_kernel<false><<<nwork, kFpThreads, smem, st>>>(fp);
+    fan_fp_kernel<false><<<nwork, FpCfg<false>::threads, smem, st>>>(fp);
     RN_CUDA_TRY(cudaGetLastError());
     int herr = 0;
     RN_CUDA_TRY(cudaMemcpyAsync(&herr, base + o_err, sizeof(int), cudaMemcpyDeviceToHost, st));
