@@ -342,15 +342,26 @@ def run_schedule(net: PriorCNN, solver, x0: torch.Tensor, schedule) -> torch.Ten
     return x
 
 
-def choose_schedule(net: PriorCNN, solver, x_ref: torch.Tensor, target_rmse: float, schedules=SCHEDULES):
+def choose_schedule(net: PriorCNN, solver, x_ref: torch.Tensor, x_tv: torch.Tensor, allowance: float = 0.0,
+                    schedules=SCHEDULES):
     """The cheapest schedule (fewest iterations, then fewest network passes)
     whose RMSE against x_ref on the solver's slices (a validation set, not the
-    slices the result is reported on) is within target_rmse; the one with the
-    lowest RMSE if none is.  Returns (schedule, {schedule: rmse})."""
-    errs = {}
+    slices the result is reported on) exceeds that of the TV reconstruction
+    x_tv by at most `allowance`; the one with the lowest RMSE if none does.
+    Returns (schedule, {schedule: rmse}, {schedule: rmse - TV's rmse}).
+
+    With the default allowance of 0 a schedule must match TV on the
+    validation slices, which leaves a target of "TV + 1 HU" on other slices
+    its whole tolerance as margin: a schedule's excess over TV moves from one
+    set of slices to another (by ~0.6 HU between 8 validation and 32
+    held-out slices here), so a schedule chosen just inside the target on
+    the validation slices can miss it on the held-out ones."""
+    tv = float(torch.sqrt(((x_tv - x_ref) ** 2).mean()))
+    errs, excess = {}, {}
     for sch in schedules:
         x = run_schedule(net, solver, torch.zeros_like(x_ref), sch)
         errs[sch] = float(torch.sqrt(((x - x_ref) ** 2).mean()))
-    ok = [sch for sch in schedules if errs[sch] <= target_rmse]
+        excess[sch] = errs[sch] - tv
+    ok = [sch for sch in schedules if excess[sch] <= allowance]
     best = min(ok, key=schedule_cost) if ok else min(schedules, key=lambda sch: errs[sch])
-    return best, errs
+    return best, errs, excess

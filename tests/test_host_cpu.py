@@ -114,8 +114,9 @@ def test_bench_shards_independent_batches_per_rank():
 
 def test_learned_schedule_choice_is_cheapest_within_target():
     """choose_schedule takes the schedule with the fewest OS-SQS iterations
-    (then network passes) whose RMSE is within the target, and the lowest-RMSE
-    one when none is; run_schedule applies iterations and network passes in
+    (then network passes) whose RMSE exceeds the TV reconstruction's by at
+    most the allowance (0 by default: matching TV), and the lowest-RMSE one
+    when none does; run_schedule applies iterations and network passes in
     the order given.  Checked with stand-ins for the solver and the network."""
     import torch
     from reconnet_b200 import learned_prior as LP
@@ -132,11 +133,17 @@ def test_learned_schedule_choice_is_cheapest_within_target():
     assert float(LP.run_schedule(Net(), Solver(), x0, (4, "N", 2, "N", 2))[0, 0]) == 4.0   # ((4/2)+2)/2+2
     assert LP.schedule_cost((4, "N", 3, "N", 2)) == (9, 2)
     ref = torch.full((2, 3), 2.0)
-    sch, errs = LP.choose_schedule(Net(), Solver(), ref, 0.5)
-    assert sch == (4, "N") and errs[(4, "N")] == 0.0
-    # only the schedules ending in 2 iterations after two passes reach 4.0
-    sch, errs = LP.choose_schedule(Net(), Solver(), torch.full((2, 3), 4.0), 0.1)
+    sch, errs, excess = LP.choose_schedule(Net(), Solver(), ref, ref + 0.25)
+    assert sch == (4, "N") and errs[(4, "N")] == 0.0 and abs(excess[(4, "N")] + 0.25) < 1e-6
+    # only the schedules ending in 2 iterations after two passes reach 4.0;
+    # with TV 0.05 off, they alone match it
+    ref4 = torch.full((2, 3), 4.0)
+    sch, errs, excess = LP.choose_schedule(Net(), Solver(), ref4, ref4 + 0.05)
     assert sch == (4, "N", 2, "N", 2)
-    # none within the target: the lowest RMSE
-    sch, errs = LP.choose_schedule(Net(), Solver(), torch.full((2, 3), 100.0), 0.1)
+    # an allowance of 2 admits the cheapest, (4, N): 2.0 off, TV 0.05 off
+    sch, errs, excess = LP.choose_schedule(Net(), Solver(), ref4, ref4 + 0.05, allowance=2.0)
+    assert sch == (4, "N") and abs(excess[sch] - 1.95) < 1e-6
+    # none within: the lowest RMSE
+    ref100 = torch.full((2, 3), 100.0)
+    sch, errs, excess = LP.choose_schedule(Net(), Solver(), ref100, ref100)
     assert errs[sch] == min(errs.values())
