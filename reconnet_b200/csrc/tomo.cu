@@ -8,10 +8,12 @@
 //       and the sum is scaled by dz / |dz_src-det| * |src - det|;
 //   BP: the sinogram is pre-weighted by the same length factor, and every
 //       voxel integrates the detector rectangle spanned by its projected faces.
-// Here both integrals come from FP64 row-prefix tables (rows_integral): the
-// rows a rectangle overlaps, each weighted by its overlap, the same quantity
-// in exact arithmetic as the reference's summed-area-table corner form.  Each
-// (b, c) volume is processed by one launch sequence on the caller's stream.
+// The FP integral comes from FP64 row-prefix tables (rows_integral): the rows
+// a rectangle overlaps, each weighted by its overlap, the same quantity in
+// exact arithmetic as the reference's summed-area-table corner form.  The BP
+// reads the FP64 (u, v) summed-area table, as the reference does, with the
+// corners shared between neighbouring voxels.  Each (b, c) volume is
+// processed by one launch sequence on the caller's stream.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -38,8 +40,9 @@ struct TomoDims {
 // sum over the rows it overlaps (rows_integral), which equals the reference's
 // summed-area-table corner form.  BP: per view, row prefixes along u of the
 // length-weighted projections, layout [view][v + 1][u] (u fastest, u in
-// [0, nu]), integrated the same way over detector rows.  Rows run along the
-// axis that the lanes of the main kernels walk, so their reads are coalesced.
+// [0, nu]), then summed along v in place (tomo_bp_sat_v) into the (u, v)
+// summed-area table.  Rows run along the axis that the lanes of the main
+// kernels walk, so their reads are coalesced.
 // Row prefixes are built by a tiled pass that reads the source along its
 // contiguous axis, transposes 32 x 32 tiles through shared memory and scans
 // along the row with warp scans (carry across tiles).
@@ -139,6 +142,35 @@ __global__ void __launch_bounds__(256) tomo_bp_sat_u(double* __restrict__ sat, c
         for (int u = lane + 32 * w; u <= d.nu; u += 256) S[u] = 0.0;
 }
 
+// In place along v: T[view][k][u] = sum_{k' <= k} R[view][k'][u], the (u, v)
+// summed-area table of the weighted projections (row 0 stays 0), the
+// quantity of the reference's AccumulateUVAlongVKernel (DistanceDriven3D.cu:459-475).
+// A warp scans 32 u columns (lanes along u, coalesced) down all rows, loading
+// 8 rows ahead of the running sum.  Block (32, 4): blockIdx.x * 4 + warp = a
+// strip of 32 columns, blockIdx.y = view.
+__global__ void __launch_bounds__(128) tomo_bp_sat_v(double* __restrict__ sat, TomoDims d) {
+    const int u = (blockIdx.x * 4 + threadIdx.y) * 32 + threadIdx.x;
+    // the two pad entries after the last view's table (read with weight 0
+    // by the backprojection's u + 1 neighbour at u = nu)
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.y == 0 && threadIdx.x < 2)
+        sat[(long long)d.nview * (d.nu + 1) * (d.nv + 1) + threadIdx.x] = 0.0;
+    if (u > d.nu) return;
+    const long long row = d.nu + 1;
+    double* T = sat + (long long)blockIdx.y * row * (d.nv + 1) + u;
+    double acc = 0.0;
+    for (int k0 = 1; k0 <= d.nv; k0 += 8) {
+        double v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = k0 + i <= d.nv ? T[(k0 + i) * row] : 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (k0 + i <= d.nv) {
+                acc += v[i];
+                T[(k0 + i) * row] = acc;
+            }
+    }
+}
+
 // Clamp_float + the index / weight of one coordinate of InterpolateXY /
 // InterpolateUV (DistanceDriven3D.cu:75-135, :493-517) on a grid of n points.
 struct Lerp {
@@ -229,15 +261,21 @@ __global__ void __launch_bounds__(128) tomo_fp_kernel(float* __restrict__ prj, c
     }
 }
 
-// BP: lane i of a warp owns voxel column ix = 31 blockIdx.x + i and its left
+// BP: lane i of a warp owns voxel column ix = 31 blockIdx.y + i and its left
 // face; lane 31 only supplies the right face of lane 30's voxel.  A warp
-// handles one (y, z) row.  Per view each lane evaluates D = S(u_e, v2) -
-// S(u_e, v1) at its face's detector coordinate (ProjectConeToDetCart,
-// DistanceDriven3D.cu:478-489), S being the (u, v) summed-area table of the
-// reference, from the detector rows that [v1, v2] overlaps (the same for
-// every lane of the warp): two row-prefix reads per row, two or three rows,
-// instead of the reference's 16 corner reads.  The voxel's rectangle integral
-// is D(next lane) - D(this lane); its area is r^2 dx dy / (du dv).
+// handles kTomoBpRows consecutive voxels y0 .. y0 + 7 of one z plane.  Per
+// view each lane evaluates the (u, v) summed-area table T of the weighted
+// projections, bilinearly (InterpolateUV, DistanceDriven3D.cu:493-517), at
+// its face's detector coordinate u_e (ProjectConeToDetCart, :478-489) and the
+// detector coordinates f_0 .. f_8 of the 8 voxels' v faces (the same for
+// every lane of the warp): D_j = T(u_e, f_(j+1)) - T(u_e, f_j), and the
+// voxel's rectangle integral is D_j(next lane) - D_j(this lane), divided by
+// its area r^2 dx dy / (du dv).  The reference reads 4 corners of 4 bilinear
+// samples per voxel and view; sharing corners between neighbouring voxels
+// in x (shuffles) and in y (the face between them) leaves 4 table reads per
+// voxel and view, all independent of one another.
+constexpr int kTomoBpRows = 8;
+
 __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, const double* __restrict__ sat,
                                                       const float* __restrict__ detCenter,
                                                       const float* __restrict__ src, TomoDims d, int b, int c) {
@@ -246,32 +284,72 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
     const int lane = threadIdx.x;
     const int iz = blockIdx.x;
     const int ix = blockIdx.y * 31 + lane;
-    const int iy = blockIdx.z * blockDim.y + threadIdx.y;
-    if (iy >= d.ny) return;   // warp-uniform
+    const int y0 = (blockIdx.z * blockDim.y + threadIdx.y) * kTomoBpRows;
+    if (y0 >= d.ny) return;   // warp-uniform
+    const int ny_w = min(kTomoBpRows, d.ny - y0);
     const float xf = (ix - (d.nx - 1) / 2.0f) * d.dx + d.cx - d.dx / 2;
-    const float y = (iy - (d.ny - 1) / 2.0f) * d.dy + d.cy;
+    const float yb = (y0 - (d.ny - 1) / 2.0f) * d.dy + d.cy - d.dy / 2;   // lower face of voxel y0
     const float z = (iz - (d.nz - 1) / 2.0f) * d.dz + d.cz;
     const float cu = d.off_u + (d.nu - 1) / 2.0f, cv = d.off_v + (d.nv - 1) / 2.0f;
     const float aunit = d.dx * d.dy / (d.du * d.dv);
     const float idu = 1.0f / d.du, idv = 1.0f / d.dv;
-    const long long vplane = (long long)(d.nu + 1) * (d.nv + 1), row = d.nu + 1;
-    float val = 0.f;
-    // two views per iteration: their table reads are in flight together
-#pragma unroll 2
+    const long long vplane = (long long)(d.nu + 1) * (d.nv + 1);
+    const int row = d.nu + 1;
+    float acc[kTomoBpRows];
+#pragma unroll
+    for (int j = 0; j < kTomoBpRows; j++) acc[j] = 0.f;
     for (int view = 0; view < d.nview; view++) {
         const float* dc = detCenter + 3 * view;
         const float* sp = src + 3 * view;
         const float r = (dc[2] - sp[2]) / (z - sp[2]);
         const float ue = fmaf(sp[0] - dc[0] + r * (xf - sp[0]), idu, cu);
-        const float v1 = fmaf(sp[1] - dc[1] + r * (y - d.dy / 2 - sp[1]), idv, cv);
-        const float v2 = fmaf(sp[1] - dc[1] + r * (y + d.dy / 2 - sp[1]), idv, cv);
-        const Lerp lu = lerp_at(ue, d.nu + 1);
-        const double D = rows_integral(sat + view * vplane, lu, v1, v2, d.nv, row);
-        const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
-        val = fmaf((float)q, __fdividef(1.0f, r * r * aunit), val);
+        const float ov0 = sp[1] - dc[1], wgt = __fdividef(1.0f, r * r * aunit);
+        // u_e clamped to [0, nu]: column iu and its neighbour iu + 1 with
+        // weight wu (at u_e = nu the neighbour is the next row's zero column
+        // or a pad entry, with weight 0)
+        const float uc = fminf(fmaxf(ue, 0.f), (float)d.nu);
+        const float uy = __fadd_rd(uc, 12582912.0f);
+        const double wu = (double)(uc - (uy - 12582912.0f)), wu1 = 1.0 - wu;
+        const double* Tu = sat + view * vplane + (__float_as_int(uy) - 0x4B400000);
+        // T(u_e, f_j) at the lower face of voxel y0 + j, from table rows k0
+        // and k1 = k0 + 1 (clamped); a face whose k0 is the previous face's
+        // k1 (the row index is the same for the whole warp) reuses that row
+        int kp = -1;
+        double ep = 0.0;
+        auto tface = [&](int j) {
+            const float f = fmaf(ov0 + r * (fmaf((float)j, d.dy, yb) - sp[1]), idv, cv);
+            const Lerp lv = lerp_at(f, d.nv + 1);
+            double a;
+            if (lv.i0 == kp) {
+                a = ep;
+            } else {
+                const double* t0 = Tu + lv.i0 * row;
+                a = t0[0] * wu1 + t0[1] * wu;
+            }
+            const double* t1 = Tu + lv.i1 * row;
+            const double e = t1[0] * wu1 + t1[1] * wu;
+            kp = lv.i1;
+            ep = e;
+            return fma(e - a, lv.w, a);
+        };
+        double tprev = tface(0);
+#pragma unroll
+        for (int j = 0; j < kTomoBpRows; j++) {
+            if (j < ny_w) {   // warp-uniform
+                const double t = tface(j + 1);
+                const double D = t - tprev;
+                const double q = __shfl_down_sync(0xffffffffu, D, 1) - D;
+                acc[j] = fmaf((float)q, wgt, acc[j]);
+                tprev = t;
+            }
+        }
     }
-    if (lane < 31 && ix < d.nx)
-        img[(long long)b * d.nx * d.ny * d.nz * d.nc + (((long long)ix * d.ny + iy) * d.nz + iz) * d.nc + c] = val;
+    if (lane < 31 && ix < d.nx) {
+        float* out = img + (long long)b * d.nx * d.ny * d.nz * d.nc + (((long long)ix * d.ny + y0) * d.nz + iz) * d.nc + c;
+#pragma unroll
+        for (int j = 0; j < kTomoBpRows; j++)
+            if (j < ny_w) out[(long long)j * d.nz * d.nc] = acc[j];
+    }
 }
 
 static int tomo_validate(const TomoDims& d) {
@@ -303,8 +381,9 @@ int tomo_backproject(float* d_img, const float* d_prj, const float* d_dc, const 
         for (int c = 0; c < d.nc; c++) {
             tomo_bp_sat_u<<<dim3((d.nv + 31) / 32, d.nview), dim3(32, 8), 0, st>>>(d_sat, d_prj, d_dc, d_src, d, b,
                                                                                     c, weight_all);
+            tomo_bp_sat_v<<<dim3((d.nu + 1 + 127) / 128, d.nview), dim3(32, 4), 0, st>>>(d_sat, d);
             dim3 blk(32, 8);
-            dim3 grd(d.nz, (d.nx + 30) / 31, (d.ny + 7) / 8);
+            dim3 grd(d.nz, (d.nx + 30) / 31, (d.ny + 8 * kTomoBpRows - 1) / (8 * kTomoBpRows));
             tomo_bp_kernel<<<grd, blk, 0, st>>>(d_img, d_sat, d_dc, d_src, d, b, c);
         }
     RN_CUDA_TRY(cudaGetLastError());
@@ -346,7 +425,7 @@ static int host_tomo(bool fp, float* out, const float* in, const float* dc, cons
     if (!g_tomo.st) RN_CUDA_TRY(cudaStreamCreateWithFlags(&g_tomo.st, cudaStreamNonBlocking));
     cudaStream_t st = g_tomo.st;
     size_t ni = (size_t)d.nb * d.nx * d.ny * d.nz * d.nc, np = (size_t)d.nb * d.nu * d.nview * d.nv * d.nc;
-    size_t nsat = fp ? (size_t)d.nz * (d.nx + 1) * (d.ny + 1) : (size_t)d.nview * (d.nu + 1) * (d.nv + 1);
+    size_t nsat = fp ? (size_t)d.nz * (d.nx + 1) * (d.ny + 1) : (size_t)d.nview * (d.nu + 1) * (d.nv + 1) + 2;
     RN_TRY(g_tomo.ensure(0, ni * 4));
     RN_TRY(g_tomo.ensure(1, np * 4));
     RN_TRY(g_tomo.ensure(2, (size_t)d.nview * 12));
@@ -378,7 +457,7 @@ extern "C" {
 
 int rn_tomo_sat_bytes(int nx, int ny, int nz, int nu, int nview, int nv, size_t* fp_bytes, size_t* bp_bytes) {
     if (fp_bytes) *fp_bytes = (size_t)nz * (nx + 1) * (ny + 1) * 8;
-    if (bp_bytes) *bp_bytes = (size_t)nview * (nu + 1) * (nv + 1) * 8;
+    if (bp_bytes) *bp_bytes = ((size_t)nview * (nu + 1) * (nv + 1) + 2) * 8;   // + 2 pad entries
     return RN_OK;
 }
 

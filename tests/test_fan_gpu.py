@@ -345,6 +345,27 @@ def test_tomo_matches_oracle(rng):
         assert rel_l2(out.cpu().numpy(), O.tomo_bp(prj, dc, src, g, (16, 14, 6), mode)) <= TOL
 
 
+def test_tomo_negative_magnification_matches_oracle(rng):
+    """A detector beyond the source (magnification r < 0): the voxels' detector
+    faces then run against y, and the backprojection sweeps its rows in the
+    reverse order; ny = 21 leaves a warp with 5 of its 8 voxel rows."""
+    from oracle import oracle as O
+    from reconnet_b200.reconnet import ReconNet
+    from test_oracle_cpu import _tomo_setup
+    g, dc, src = _tomo_setup(rng)
+    dc[:, 2] = 700.0
+    rn = ReconNet()
+    rn.nx, rn.ny, rn.nz, rn.nu, rn.nv = 16, 21, 6, 24, 20
+    for k in ("dx", "dy", "dz", "cx", "cy", "cz", "du", "dv", "off_u", "off_v"):
+        setattr(rn, k, getattr(g, k))
+    img = rng.random((1, 16, 21, 6, 1)).astype(np.float32)
+    got = rn.cDDTomoProjection4d(img, dc, src)
+    assert rel_l2(got, O.tomo_fp(img, dc, src, g, 24, 20)) <= TOL
+    prj = rng.random(got.shape).astype(np.float32)
+    gb = rn.cDDTomoBackprojection4d(prj, dc, src)
+    assert rel_l2(gb, O.tomo_bp(prj, dc, src, g, (16, 21, 6), 0)) <= TOL
+
+
 def test_invalid_arguments_raise():
     import torch
     from reconnet_b200 import _native as N
