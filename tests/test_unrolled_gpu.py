@@ -4,8 +4,8 @@ over 360 degrees, 12 ordered subsets), 10 unrolled iterations, each with a
 learnable step scale and TV weight, checkpointed per iteration.
 
 * Gradients with respect to the 20 parameters and the starting image against
-  central finite differences (eps = 2e-3 for the step scales and 1e-3 for the
-  TV weights; for the starting
+  central finite differences (eps = 1e-3; for the TV weights Richardson-
+  combined with eps / 2; for the starting
   image a step along the gradient whose largest pixel is 1e-6, small against
   the TV terms' sqrt(d^2 + 1e-6) curvature in pixels whose data weights are
   photon-starved; each Richardson-combined with half the step), relative
@@ -83,14 +83,18 @@ def test_unrolled_config_gradients_match_finite_differences():
     print(f"\nunrolled OS-SQS (8 x 256^2, 720 views, 12 subsets, 10 iterations): peak memory above the inputs "
           f"{peaks[True] / 2**20:.1f} MiB with per-iteration checkpoints, {peaks[False] / 2**20:.1f} MiB without")
     assert peaks[True] < peaks[False]
-    # The loss of ten iterations in FP32 kernels scatters by ~3e-7 (std, at a
-    # loss of ~260) around a smooth curve when step[0] moves in steps of 2e-4
-    # (measured).  The step-scale gradients are ~0.2: at eps / 2 = 1e-3 that
-    # scatter is ~0.1% of them (at 5e-4, ~0.3%, too close to the tolerance).
-    # The TV-weight gradients are ~25, and the loss is curved more strongly
-    # in them, so they keep eps = 1e-3.
+    # Central differences at eps = 1e-3.  For the step scales that is the
+    # check itself: their gradients are ~0.2 and the loss of ten iterations in
+    # FP32 kernels scatters by ~3e-7 (std, at a loss of ~260) around a smooth
+    # curve (measured), ~0.1% of the difference quotient at this eps, while a
+    # half step would leave ~0.3%.  The TV weights act through
+    # sqrt(d^2 + 1e-6), strongly curved on the scale of eps, so the plain
+    # difference carries an O(eps^2) error of a few per cent there: it is
+    # Richardson-combined with eps / 2 (their gradients are ~25, so the
+    # scatter does not matter).
+    eps = 1e-3
     with torch.no_grad():
-        for vec, grad, other, first, eps in ((step, gs, tvw, True, 2e-3), (tvw, gt, step, False, 1e-3)):
+        for vec, grad, other, first in ((step, gs, tvw, True), (tvw, gt, step, False)):
             for i in range(K):
                 def central(h):
                     d = torch.zeros_like(vec)
@@ -98,11 +102,7 @@ def test_unrolled_config_gradients_match_finite_differences():
                     lp = loss(vec + d, other) if first else loss(other, vec + d)
                     lm = loss(vec - d, other) if first else loss(other, vec - d)
                     return float(lp - lm) / (2 * h)
-                # central differences at eps and eps / 2, Richardson-combined:
-                # the TV weights act through sqrt(d^2 + 1e-6), strongly curved
-                # on the scale of eps, so the plain difference carries an
-                # O(eps^2) error of a few per cent there
-                fd = (4 * central(eps / 2) - central(eps)) / 3
+                fd = central(eps) if first else (4 * central(eps / 2) - central(eps)) / 3
                 assert abs(fd - float(grad[i])) <= 5e-3 * abs(fd) + 1e-9, (first, i, fd, float(grad[i]))
     x_init = (0.01 * torch.rand_like(truth)).requires_grad_(True)
     gx, = torch.autograd.grad(loss(step.detach(), tvw.detach(), x_init), (x_init,))
