@@ -640,10 +640,11 @@ __global__ void bp_parts_sum_kernel(float* __restrict__ out, const float* __rest
 
 
 // Per-view parameters the BP inner loop reads, staged in shared memory.
-// Siddon BP table: per view, entry u + 1 holds the slope of ray u as hi / lo
-// floats, c_u = w_u * (ray length per band), w_u the sinogram value mixed
-// over the slice's detector rows, and 1 / |r_u| (0 for rays within 1e-6 of
-// the line normal).
+// Siddon BP table: per view, entry e holds the slope of ray e - 1 as hi / lo
+// floats and the prefix C_e = sum_{u < e} c_u as hi / lo floats (FP64 scan),
+// c_u = w_u * (ray length per band), w_u the sinogram value mixed over the
+// slice's detector rows; entry 0 is a guard (C = 0) and entry nu + 1 holds
+// the total.  c_u is C_(u+1) - C_u of two neighbouring entries.
 __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice* __restrict__ bps, int s_begin,
                                     int ns, const GeoSet* __restrict__ sets, const ViewGeo* __restrict__ views,
                                     const double* __restrict__ cslopes, FanDims d, float4* __restrict__ tab,
@@ -659,22 +660,33 @@ __global__ void siddon_table_kernel(const float* __restrict__ prj, const BpSlice
     const int nu = d.nu;
     const double along = views[gv].xcls ? d.dx : d.dy, across = views[gv].xcls ? d.dy : d.dx;
     float4* out = tab + (bs.table_off - tab_base) + (long long)vl * (nu + 2);
-    for (int u = lane; u < nu; u += 32) {
-        float w = 0.f;
+    double carry = 0.0;
+    for (int u0 = 0; u0 < nu; u0 += 32) {
+        const int u = u0 + lane;
+        double c = 0.0, r = 0.0;
+        if (u < nu) {
+            float w = 0.f;
 #pragma unroll
-        for (int k = 0; k < kBpMix; k++) {
-            const float wk = bs.prj_w[k];
-            if (wk == 0.f) continue;
-            w += wk * __ldg(prj + bs.prj_off[k] + (long long)u * bs.su + (long long)vl * bs.sview);
+            for (int k = 0; k < kBpMix; k++) {
+                const float wk = bs.prj_w[k];
+                if (wk == 0.f) continue;
+                w += wk * __ldg(prj + bs.prj_off[k] + (long long)u * bs.su + (long long)vl * bs.sview);
+            }
+            r = cslopes[(long long)gv * (nu + 1) + u];
+            c = (double)(w * (float)sqrt(r * r * along * along + across * across));
         }
-        const double r = cslopes[(long long)gv * (nu + 1) + u];
-        const float c = w * (float)sqrt(r * r * along * along + across * across);
-        const float rh = (float)r;
-        out[u + 1] = make_float4(rh, (float)(r - (double)rh), c, fabs(r) > 1e-6 ? (float)(1.0 / fabs(r)) : 0.f);
+        const double incl = carry + warp_incl_scan(c);
+        if (u < nu) {
+            const float rh = (float)r;
+            const float2 q = split_double(incl);
+            out[u + 1] = make_float4(rh, (float)(r - (double)rh), q.x, q.y);
+        }
+        carry = __shfl_sync(0xffffffffu, incl, 31);
     }
     if (lane == 0) {
+        const float2 q = split_double(carry);
         out[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-        out[nu + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        out[nu + 1] = make_float4(0.f, 0.f, q.x, q.y);
     }
 }
 
@@ -730,7 +742,7 @@ __global__ void pd_table_kernel(const float* __restrict__ prj, const BpSlice* __
 
 struct BpView {
     double pard, perpd;   // source coordinates (Siddon band positions)
-    float par, perp, kappa, tA, tB;
+    float par, perp, kappa, tA, tB, sigma;
     int xcls;
 };
 
@@ -839,29 +851,31 @@ __device__ __forceinline__ void bp_matched_y(float (&acc)[kBmRows], const BpView
 
 // Siddon backprojection (kMode 2), the exact transpose of the Siddon forward
 // projection: pixel column q-range [q, q + 1] on the band between lattice
-// lines l and l + 1 receives, from every ray u that crosses it, c_u (its
-// sinogram value times its length per band) times the fraction of the ray's
-// band interval [pos_u(l), pos_u(l + 1)] inside [q, q + 1], where pos_u(l) =
-// par + r_u (l - perp).  The candidate rays are those whose centre index
-// u + 1/2 lies between the edge indices t at the pixel's four lattice corners
-// (widened by 1e-3 against the cubic's truncation; a ray that misses the
-// pixel adds a zero fraction).  Table entry u + 1 holds r_u as a double and
-// c_u.  X-class: lane column q = x on lines y0 + j; Y-class: line l = x and
-// positions q = y0 + j; the corners on the neighbour column / line come from
-// the next lane.
-// Contribution of one candidate ray: its position at line l relative to the
-// pixel, x = (par - q) + r (l - perp), from hi / lo parts (A = par - q and D =
-// l - perp as hi / lo floats, r from the table), to ~1e-7 cells.
-// The fraction of the band interval inside [0, 1] is 1 exactly when the
-// interval lies inside, and its overlap times 1 / |r| (E.w) otherwise; rays
-// within 1e-6 of the line normal (E.w = 0) take the point test.
-__device__ __forceinline__ float siddon_candidate(const float4 E, float Ah, float Al, float Dh, float Dl) {
+// lines l and l + 1 receives, from every ray u, c_u (its sinogram value times
+// its length per band) times the fraction of the ray's band interval
+// [pos_u(l), pos_u(l + 1)] inside [q, q + 1], where pos_u(l) = par +
+// r_u (l - perp).  Written as F(q + 1) - F(q), with F(q) = sum_u c_u b_u(q)
+// and b_u(q) the fraction of ray u's band interval below q: rays wholly below
+// q give the table prefix C (hi / lo), so F needs the exact fraction only for
+// the rays whose centre index u + 1/2 lies between the edge indices t of the
+// lattice points (q, l) and (q, l + 1) (widened by 1e-3 against the cubic's
+// truncation: a ray taken in that is wholly below or above q gets the
+// fraction 1 or 0 exactly), usually one.  Positions increase with u where
+// sigma > 0: the rays below q are then u < ua, else u > ub, whose sum is the
+// total minus C_(ub+1); the total cancels in F(q + 1) - F(q).  X class: lane
+// column q = x on lines y0 + j (F(x + 1) from the next lane); Y class: line l
+// = x, positions q = y0 + j (the band's second line x + 1 from the next lane).
+// The fraction of ray u below q: its position at line l relative to q, x_a =
+// (par - q) + r (l - perp), from hi / lo parts (A = par - q and D = l - perp
+// as hi / lo floats, r from the table) to ~1e-7 cells, x_b = x_a + r; the
+// fraction is min(max(-min(x_a, x_b) / |r|, 0), 1), and a ray within 1e-6 of
+// the line normal takes the point test x_a < 0.
+__device__ __forceinline__ float siddon_below(const float4 E, float Ah, float Al, float Dh, float Dl) {
     const float xa = fmaf(E.x, Dh, Ah) + fmaf(E.y, Dh, fmaf(E.x, Dl, Al));
-    const float xb = xa + E.x;
-    const float lo = fminf(xa, xb), hi = fmaxf(xa, xb);
-    const float ov = fmaxf(0.f, fminf(hi, 1.f) - fmaxf(lo, 0.f));
-    const float fr = (lo >= 0.f && hi <= 1.f) ? 1.f : ov * E.w;
-    return E.z * (E.w != 0.f ? fr : ((xa >= 0.f && xa < 1.f) ? 1.f : 0.f));
+    const float ar = fabsf(E.x);
+    const float lo = fminf(xa, xa + E.x);
+    const float fr = fminf(fmaxf(__fdividef(-lo, ar), 0.f), 1.f);
+    return ar > 1e-6f ? fr : (xa < 0.f ? 1.f : 0.f);
 }
 
 // floor(x) for |x| < 2^22 on the FMA / ALU pipes (round-down add of 1.5 * 2^23).
@@ -869,20 +883,42 @@ __device__ __forceinline__ int floor_small(float x) {
     return __float_as_int(__fadd_rd(x, 12582912.0f)) - 0x4B400000;
 }
 
-// Sum over the candidate rays of a pixel: the first two unrolled (most pixels
-// have at most two), the rest in a loop.
-__device__ __forceinline__ float siddon_pixel(const float4* T, int ilo, int imax, int nu, float t00, float t01,
-                                              float t10, float t11, float Ah, float Al, float Dh, float Dl) {
-    const float tmin = fminf(fminf(t00, t01), fminf(t10, t11)), tmax = fmaxf(fmaxf(t00, t01), fmaxf(t10, t11));
-    const int u0 = max(max(-floor_small(0.5f + 1e-3f - tmin), 0), ilo - 1);
-    const int u1 = min(min(floor_small(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
-    // the first two without branches: evaluated at indices clamped into the
-    // staged window [ilo, imax] and kept only when they are candidates
-    const float va = siddon_candidate(T[min(u0 + 1, imax) - ilo], Ah, Al, Dh, Dl);
-    const float vb = siddon_candidate(T[min(u0 + 2, imax) - ilo], Ah, Al, Dh, Dl);
-    float v = (u0 <= u1 ? va : 0.f) + (u0 + 1 <= u1 ? vb : 0.f);
-    for (int u = u0 + 2; u <= u1; u++) v += siddon_candidate(T[u + 1 - ilo], Ah, Al, Dh, Dl);
-    return v;
+// F(q) = sum_u c_u b_u(q) (up to the total, for sigma < 0) as hi + rest, for
+// the band between the lattice points with edge indices ta and tb.  Table
+// indices clamp into the staged window [ilo, imax].
+__device__ __forceinline__ void siddon_F(const float4* T, int ilo, int imax, int nu, float sigma, float ta, float tb,
+                                         float Ah, float Al, float Dh, float Dl, float& fhi, float& frest) {
+    const float tmin = fminf(ta, tb), tmax = fmaxf(ta, tb);
+    // first and last ray taken in (the staged window covers the tile's rays;
+    // the clamps to it only keep the reads inside it)
+    const int ua = max(max(-floor_small(0.5f + 1e-3f - tmin), 0), ilo - 1);
+    const int ub = min(min(floor_small(tmax - 0.5f + 1e-3f), nu - 1), imax - 1);
+    const float4 E0 = T[min(max(min(ua, nu), ilo), imax) - ilo];  // C_ua
+    float ch = E0.z, cl = E0.w, part = 0.f;
+    {   // the first ray taken in, without a branch: read at an index clamped
+        // into the window, kept only when taken in
+        const float4 E = T[min(ua + 1, imax) - ilo];
+        const bool in = ua <= ub;
+        const float c = (E.z - ch) + (E.w - cl);
+        part = in ? c * siddon_below(E, Ah, Al, Dh, Dl) : 0.f;
+        ch = in ? E.z : ch;
+        cl = in ? E.w : cl;
+    }
+    for (int u = ua + 1; u <= ub; u++) {   // the rare further ones
+        const float4 E = T[min(u + 1, imax) - ilo];
+        const float c = (E.z - ch) + (E.w - cl);
+        part = fmaf(c, siddon_below(E, Ah, Al, Dh, Dl), part);
+        ch = E.z;
+        cl = E.w;
+    }
+    // C_(ub+1) is the last entry read (C_ua when no ray was taken in)
+    if (sigma > 0.f) {
+        fhi = E0.z;
+        frest = E0.w + part;
+    } else {
+        fhi = -ch;
+        frest = part - cl;
+    }
 }
 
 __device__ __forceinline__ void split_hilo(double v, float& h, float& l) {
@@ -904,20 +940,21 @@ __device__ __forceinline__ void bp_siddon_x(float (&acc)[kBmRows], const BpView&
     float Ah, Al, Dh0, Dl0;
     split_hilo(vg.pard - (double)x, Ah, Al);
     split_hilo((double)y0 - vg.perpd, Dh0, Dl0);
-    float tp = 0.f, tnp = 0.f;
+    float tp = 0.f;
 #pragma unroll
     for (int j = 0; j <= kBmRows; j++) {
         const float h = A * __fdividef(1.0f, (float)(y0 + j) - vg.perp) - c.rt;
         const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
-        const float tn = __shfl_down_sync(0xffffffffu, t, 1);
         if (j > 0) {
-            // line y0 + j - 1 minus perp, stepped exactly from the first line
-            float Dh, e;
+            // band y0 + j - 1: line y0 + j - 1 minus perp, stepped exactly from the first line
+            float Dh, e, fhi, frest;
             two_sum(Dh0, (float)(j - 1), Dh, e);
-            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al, Dh, Dl0 + e);
+            siddon_F(T, ilo, imax, nu, vg.sigma, tp, t, Ah, Al, Dh, Dl0 + e, fhi, frest);
+            const float nhi = __shfl_down_sync(0xffffffffu, fhi, 1);
+            const float nrest = __shfl_down_sync(0xffffffffu, frest, 1);
+            acc[j - 1] += (nhi - fhi) + (nrest - frest);
         }
         tp = t;
-        tnp = tn;
     }
 }
 
@@ -929,20 +966,19 @@ __device__ __forceinline__ void bp_siddon_y(float (&acc)[kBmRows], const BpView&
     float Dh, Dl, Ah0, Al0;
     split_hilo((double)x - vg.perpd, Dh, Dl);
     split_hilo(vg.pard - (double)y0, Ah0, Al0);
-    float tp = 0.f, tnp = 0.f;
+    float hp = 0.f, rp = 0.f;
 #pragma unroll
     for (int j = 0; j <= kBmRows; j++) {
         const float h = fmaf((float)j, g, r0) - c.rt;
         const float t = fmaf(h, fmaf(h, fmaf(h, c.c3, c.c2), c.c1), c.c0);
-        const float tn = __shfl_down_sync(0xffffffffu, t, 1);
-        if (j > 0) {
-            // par minus position y0 + j - 1, stepped exactly from the first
-            float Ah, e;
-            two_sum(Ah0, -(float)(j - 1), Ah, e);
-            acc[j - 1] += siddon_pixel(T, ilo, imax, nu, tp, tnp, t, tn, Ah, Al0 + e, Dh, Dl);
-        }
-        tp = t;
-        tnp = tn;
+        const float tn = __shfl_down_sync(0xffffffffu, t, 1);   // the band's second line, x + 1
+        // position y0 + j: par minus it, stepped exactly from the first
+        float Ah, e, fhi, frest;
+        two_sum(Ah0, -(float)j, Ah, e);
+        siddon_F(T, ilo, imax, nu, vg.sigma, t, tn, Ah, Al0 + e, Dh, Dl, fhi, frest);
+        if (j > 0) acc[j - 1] += (fhi - hp) + (frest - rp);
+        hp = fhi;
+        rp = frest;
     }
 }
 
@@ -1123,6 +1159,7 @@ __device__ __noinline__ void bp_prep(BpShared* sh, const ViewGeo* src, int c, in
         w.kappa = vg.kappa;
         w.tA = vg.tA;
         w.tB = vg.tB;
+        w.sigma = vg.sigma;
         w.xcls = vg.xcls;
     }
 }
