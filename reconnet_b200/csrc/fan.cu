@@ -885,8 +885,10 @@ __device__ __forceinline__ int floor_small(float x) {
 
 // F(q) = sum_u c_u b_u(q) (up to the total, for sigma < 0) as hi + rest, for
 // the band between the lattice points with edge indices ta and tb.  Table
-// indices clamp into the staged window [ilo, imax].
-__device__ __forceinline__ void siddon_F(const float4* T, int ilo, int imax, int nu, float sigma, float ta, float tb,
+// indices clamp into the staged window [ilo, imax].  Kept out of line: the
+// kernel's two unrolled 17-point loops with it inlined overflow the
+// instruction cache (59.0 against 52.6 ms on the bench batch).
+__device__ __noinline__ void siddon_F(const float4* T, int ilo, int imax, int nu, float sigma, float ta, float tb,
                                          float Ah, float Al, float Dh, float Dl, float& fhi, float& frest) {
     const float tmin = fminf(ta, tb), tmax = fmaxf(ta, tb);
     // first and last ray taken in (the staged window covers the tile's rays;
