@@ -377,12 +377,12 @@ int rn_fan_sqs_update(rn_fan_plan* subset_plan, float* d_x_out, const float* d_x
  * 16*(ny*(nx+1+2m) + nx*(ny+1+2m)) + small tables, m ~ 12 line padding
  * entries, e.g. 512x512 with up to about 1000 views of 888 channels) is
  * rejected with RN_ERR_ARG and a message giving the bytes needed.  The
- * first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current.  Every call shares the
- * one array and overwrites it (the device error word is cleared by each
- * call), so calls that overlap on the GPU -- from several host threads or
- * streams -- race; serialise them.  The call synchronises `stream` before
- * returning. */
+ * first call on a device sets up that device: it looks up the array's device
+ * address (cudaGetSymbolAddress) with the device current, so make that first
+ * call before any stream capture.  Every call shares the one array and
+ * overwrites it (the device error word is cleared by each call), so calls
+ * that overlap on the GPU -- from several host threads or streams -- race;
+ * serialise them.  The call synchronises `stream` before returning. */
 int rn_fan_project_noalloc(float* d_prj, const float* d_img, const float* host_deg, int nx, int ny, float dx,
                            float dy, int nu, int nview, float da, float off_a, float dsd, float dso, void* stream);
 
