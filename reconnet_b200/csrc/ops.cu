@@ -1016,6 +1016,13 @@ struct DevBuf {
     }
 };
 
+// Host arrays cross PCIe through a pinned staging buffer in chunks, so the
+// host's copy of one chunk into (or out of) the staging buffer overlaps the
+// DMA of another; pageable copies of the same arrays run at about half the
+// rate (the driver stages them itself, one piece after the other).
+constexpr int kStageChunksMax = 32;
+constexpr size_t kStageChunkMin = (size_t)512 << 10;
+
 // One cached plan and a set of grow-only device buffers per device, guarded
 // by a mutex: repeated host calls with the same geometry and angles reuse the
 // geometry tables and scratch instead of rebuilding them.
@@ -1035,6 +1042,10 @@ struct HostCtx {
     std::list<Cached> cache;
     size_t cache_bytes = 0;
     DevBuf a, b, c, d, e;
+    // pinned staging for the host arrays of a call, and one event per chunk
+    void* pin = nullptr;
+    size_t pin_n = 0;
+    cudaEvent_t ev[kStageChunksMax] = {};
 };
 constexpr size_t kHostPlanCacheCount = 128;
 constexpr size_t kHostPlanCacheBytes = (size_t)4 << 30;
@@ -1051,6 +1062,62 @@ static HostCtx* host_ctx() {
         cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     }
     return c;
+}
+
+static int stage_ensure(HostCtx* c, size_t bytes) {
+    if (!c->ev[0])
+        for (int k = 0; k < kStageChunksMax; k++)
+            RN_CUDA_TRY(cudaEventCreateWithFlags(&c->ev[k], cudaEventDisableTiming));
+    if (bytes <= c->pin_n) return RN_OK;
+    if (c->pin) cudaFreeHost(c->pin);
+    c->pin = nullptr;
+    c->pin_n = 0;
+    RN_CUDA_TRY(cudaHostAlloc(&c->pin, bytes, cudaHostAllocDefault));
+    c->pin_n = bytes;
+    return RN_OK;
+}
+
+static size_t stage_chunk(size_t bytes) {
+    size_t ch = (bytes + kStageChunksMax - 1) / kStageChunksMax;
+    ch = std::max(ch, kStageChunkMin);
+    return (ch + 255) & ~(size_t)255;
+}
+
+// host -> device through the staging buffer: the host copies chunk k while
+// the DMA of chunk k - 1 runs.  The staging buffer is free on entry (every
+// call ends with its stream synchronised).
+static int h2d_staged(HostCtx* c, void* dst, const void* src, size_t bytes) {
+    RN_TRY(stage_ensure(c, bytes));
+    const size_t ch = stage_chunk(bytes);
+    for (size_t off = 0; off < bytes; off += ch) {
+        const size_t n = std::min(ch, bytes - off);
+        memcpy(static_cast<char*>(c->pin) + off, static_cast<const char*>(src) + off, n);
+        RN_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(dst) + off, static_cast<char*>(c->pin) + off, n,
+                                    cudaMemcpyHostToDevice, c->st));
+    }
+    return RN_OK;
+}
+
+// device -> host: every chunk's DMA is queued behind the stream's work with an
+// event after it; the host copies chunk k out as soon as its event completes,
+// while the later chunks are still crossing.
+static int d2h_staged(HostCtx* c, void* dst, const void* src, size_t bytes) {
+    RN_TRY(stage_ensure(c, bytes));
+    const size_t ch = stage_chunk(bytes);
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += ch, k++) {
+        const size_t n = std::min(ch, bytes - off);
+        RN_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(c->pin) + off, static_cast<const char*>(src) + off, n,
+                                    cudaMemcpyDeviceToHost, c->st));
+        RN_CUDA_TRY(cudaEventRecord(c->ev[k], c->st));
+    }
+    k = 0;
+    for (size_t off = 0; off < bytes; off += ch, k++) {
+        const size_t n = std::min(ch, bytes - off);
+        RN_CUDA_TRY(cudaEventSynchronize(c->ev[k]));
+        memcpy(static_cast<char*>(dst) + off, static_cast<char*>(c->pin) + off, n);
+    }
+    return RN_OK;
 }
 
 static uint64_t angle_hash(const RnFanGeom& g, const float* deg, int nview) {
@@ -1127,9 +1194,9 @@ static int host_fan_fp(float* prj, const float* img, const float* deg, const RnF
     size_t ni = (size_t)c->plan->img_elems, np = (size_t)c->plan->prj_elems;
     RN_TRY(c->a.ensure(ni * 4));
     RN_TRY(c->b.ensure(np * 4));
-    RN_CUDA_TRY(cudaMemcpyAsync(c->a.p, img, ni * 4, cudaMemcpyHostToDevice, c->st));
+    RN_TRY(h2d_staged(c, c->a.p, img, ni * 4));
     RN_TRY(fan_project(c->plan, c->b.as<float>(), c->a.as<float>(), c->st, siddon));
-    RN_CUDA_TRY(cudaMemcpyAsync(prj, c->b.p, np * 4, cudaMemcpyDeviceToHost, c->st));
+    RN_TRY(d2h_staged(c, prj, c->b.p, np * 4));
     return finish_sync(c, c->plan);
 }
 
@@ -1140,9 +1207,9 @@ static int host_fan_bp(float* img, const float* prj, const float* deg, const RnF
     size_t ni = (size_t)c->plan->img_elems, np = (size_t)c->plan->prj_elems;
     RN_TRY(c->a.ensure(ni * 4));
     RN_TRY(c->b.ensure(np * 4));
-    RN_CUDA_TRY(cudaMemcpyAsync(c->b.p, prj, np * 4, cudaMemcpyHostToDevice, c->st));
+    RN_TRY(h2d_staged(c, c->b.p, prj, np * 4));
     RN_TRY(fan_backproject(c->plan, c->a.as<float>(), c->b.as<float>(), type, 0, c->st));
-    RN_CUDA_TRY(cudaMemcpyAsync(img, c->a.p, ni * 4, cudaMemcpyDeviceToHost, c->st));
+    RN_TRY(d2h_staged(c, img, c->a.p, ni * 4));
     return finish_sync(c, c->plan);
 }
 
